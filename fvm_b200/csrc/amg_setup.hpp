@@ -1,0 +1,92 @@
+// AMG hierarchy construction on the host.
+//
+// The integer work (greedy pairwise aggregation, coarse-to-fine map,
+// coarse sparsity pattern) and the FP64 Galerkin coarse matrices follow
+// the reference's CRMatrix routines operation for operation, so level
+// sizes, aggregation indices and coarse coefficients are bit-identical to
+// the reference on the same fine matrix. On top of that each level gets a
+// deterministic greedy colouring and a colour-major row permutation, and
+// is packed into SELL-32 slices for the GPU smoothers.
+#pragma once
+
+#include <vector>
+
+#include "common.hpp"
+
+namespace fvm {
+
+// One level in the reference's row order: self rows only, implicit
+// diagonal, columns restricted to self rows (ghost couplings of the
+// finest level are zero after boundary elimination and are dropped).
+struct RefLevel {
+  int n = 0;
+  CSR conn;
+  std::vector<double> diag;
+  std::vector<double> off;
+  // to the next coarser level (empty on the coarsest)
+  std::vector<int> coarseIndex;  // fine row -> coarse row (reference CRMatrix.h:468-586)
+  int nCoarse = 0;
+};
+
+// Greedy aggregation (reference CRMatrix::createCoarsening). Returns the
+// number of coarse rows.
+int create_coarsening(const RefLevel& a, int groupSize, double weightRatioThreshold,
+                      std::vector<int>& coarseIndex);
+
+// Coarse-to-fine rows (MultiFieldMatrix::createCoarseToFineMapping), coarse
+// connectivity (CRMatrix::createCoarseConnectivity) and Galerkin values
+// (CRMatrix::createCoarseMatrix).
+void create_coarse_level(const RefLevel& fine, RefLevel& coarse, CSR& coarseToFine);
+
+struct HierarchyOptions {
+  int maxCoarseLevels = 30;
+  int groupSize = 2;
+  double weightRatioThreshold = 0.65;
+  // stop once a kept level has at most this many rows (0: the reference's
+  // rule only -- stop when a level fails to shrink or reaches <= 3 rows)
+  int coarsestSize = 0;
+  // count of rows+ghosts of the finest system, used by the reference's
+  // "did this level shrink" test on level 0
+  int finestLocalSize = 0;
+};
+
+// Builds levels[1..] from levels[0]; levels.size() - 1 coarse levels are
+// kept, following AMG::createCoarseLevels (serial build, AMG.cpp:150-210).
+void build_hierarchy(std::vector<RefLevel>& levels, const HierarchyOptions& opt,
+                     std::vector<CSR>& coarseToFine);
+
+// Packed, colour-permuted form of one level for the GPU.
+struct PackedLevel {
+  int n = 0;
+  int nColors = 0;
+  std::vector<int> colorStart;       // nColors+1 row offsets (permuted order)
+  std::vector<int> colorSliceStart;  // nColors+1 slice offsets
+  std::vector<int> sliceRow;         // first row of each slice
+  std::vector<int> sliceRows;        // rows in each slice (<= 32)
+  std::vector<int> sliceOff;         // nSlices+1 offsets into cols/vals (32 per width unit)
+  std::vector<int> cols;             // permuted columns, slice-column-major; padding = own row
+  std::vector<double> vals;          // padding = 0
+  std::vector<double> diag;          // permuted
+  std::vector<int> perm;             // reference row -> permuted row
+  std::vector<int> iperm;            // permuted row -> reference row
+  // transfer to the next coarser level, in permuted numbering of both
+  std::vector<int> coarseIndex;      // fine row -> coarse row
+  std::vector<int> c2fRow, c2fCol;   // coarse row -> fine rows, ascending reference order
+  int maxWidth = 0;
+};
+
+enum SmootherOrdering { kMulticolor = 0, kSequential = 1 };
+
+// Greedy colouring in reference row order: each row takes the smallest
+// colour unused by its already-coloured neighbours.
+int greedy_coloring(const CSR& conn, std::vector<int>& color);
+
+void pack_level(const RefLevel& lv, SmootherOrdering ordering, PackedLevel& out);
+void pack_transfer(const RefLevel& fine, const CSR& coarseToFine, PackedLevel& pf,
+                   const PackedLevel& pc);
+
+// Dense inverse of a (small) level matrix by Gauss-Jordan elimination with
+// partial pivoting, in the level's permuted numbering, row-major.
+void dense_inverse(const PackedLevel& lv, std::vector<double>& inv);
+
+}  // namespace fvm

@@ -1,0 +1,486 @@
+// The C ABI (include/fvm_b200.h) over the host mesh, the GPU thermal model
+// and the GPU AMG solvers.
+#include "../../include/fvm_b200.h"
+
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <memory>
+#include <string>
+
+#include "amg_setup.hpp"
+#include "mesh.hpp"
+#include "solver.hpp"
+#include "thermal.hpp"
+
+using namespace fvm;
+
+struct fvm_mesh {
+  std::shared_ptr<HostMesh> m;
+};
+struct fvm_thermal {
+  std::unique_ptr<ThermalModel> model;
+};
+
+namespace fvm {
+namespace {
+thread_local std::string g_error;
+}
+void set_last_error(const std::string& msg) { g_error = msg; }
+const char* last_error() { return g_error.c_str(); }
+}  // namespace fvm
+
+namespace {
+
+template <class F>
+int guarded(F f) {
+  try {
+    f();
+    return FVM_OK;
+  } catch (const Error& e) {
+    set_last_error(e.what());
+    return e.status;
+  } catch (const std::bad_alloc&) {
+    set_last_error("out of host memory");
+    return FVM_ERR_TOO_LARGE;
+  } catch (const std::exception& e) {
+    set_last_error(e.what());
+    return FVM_ERR_BAD_ARGUMENT;
+  } catch (...) {
+    set_last_error("unknown error");
+    return FVM_ERR_BAD_ARGUMENT;
+  }
+}
+
+SolverOptions to_solver(const fvm_linear_options& o) {
+  SolverOptions s;
+  FVM_REQUIRE(o.solver >= 0 && o.solver <= 2, kBadArgument, "solver must be 0 (AMG), 1 (CG) or 2 (BCGStab)");
+  FVM_REQUIRE(o.cycleType >= 0 && o.cycleType <= 2, kBadArgument, "cycleType must be 0 (V), 1 (W) or 2 (F)");
+  FVM_REQUIRE(o.smootherType == 0 || o.smootherType == 1, kBadArgument, "smootherType must be 0 or 1");
+  FVM_REQUIRE(o.nMaxIterations >= 0 && o.maxCoarseLevels >= 0 && o.nPreSweeps >= 0 &&
+                  o.nPostSweeps >= 0 && o.coarseGroupSize >= 1,
+              kBadArgument, "negative iteration/sweep/level count");
+  s.solver = (SolverKind)o.solver;
+  s.nMaxIterations = o.nMaxIterations;
+  s.relativeTolerance = o.relativeTolerance;
+  s.absoluteTolerance = o.absoluteTolerance;
+  s.verbosity = o.verbosity;
+  s.maxCoarseLevels = o.maxCoarseLevels;
+  s.nPreSweeps = o.nPreSweeps;
+  s.nPostSweeps = o.nPostSweeps;
+  s.coarseGroupSize = o.coarseGroupSize;
+  s.weightRatioThreshold = o.weightRatioThreshold;
+  s.cycleType = (CycleType)o.cycleType;
+  s.smootherType = (SmootherType)o.smootherType;
+  s.scaleCorrections = o.scaleCorrections != 0;
+  s.ordering = o.smootherOrdering == 1 ? kSequential : kMulticolor;
+  s.coarsestSize = o.coarsestSize;
+  s.coarseSolver = o.coarseSolver == 1 ? kCoarseDirect : kCoarseSmooth;
+  s.precision = o.precision == 1 ? kMixed : kFP64;
+  s.useGraphs = o.useGraphs != 0;
+  return s;
+}
+
+void from_solver(const SolverOptions& s, fvm_linear_options& o) {
+  o.solver = s.solver;
+  o.nMaxIterations = s.nMaxIterations;
+  o.relativeTolerance = s.relativeTolerance;
+  o.absoluteTolerance = s.absoluteTolerance;
+  o.verbosity = s.verbosity;
+  o.maxCoarseLevels = s.maxCoarseLevels;
+  o.nPreSweeps = s.nPreSweeps;
+  o.nPostSweeps = s.nPostSweeps;
+  o.coarseGroupSize = s.coarseGroupSize;
+  o.weightRatioThreshold = s.weightRatioThreshold;
+  o.cycleType = s.cycleType;
+  o.smootherType = s.smootherType;
+  o.scaleCorrections = s.scaleCorrections ? 1 : 0;
+  o.smootherOrdering = s.ordering == kSequential ? 1 : 0;
+  o.coarsestSize = s.coarsestSize;
+  o.coarseSolver = s.coarseSolver == kCoarseDirect ? 1 : 0;
+  o.precision = s.precision == kMixed ? 1 : 0;
+  o.useGraphs = s.useGraphs ? 1 : 0;
+}
+
+RefLevel level_from_csr(int n, const int* row, const int* col, const double* diag, const double* off) {
+  FVM_REQUIRE(n > 0 && row && col && diag && off, kBadArgument, "empty or null matrix");
+  FVM_REQUIRE(row[0] == 0, kBadArgument, "row[0] must be 0");
+  RefLevel l;
+  l.n = n;
+  l.conn.nRows = n;
+  l.conn.row.assign(row, row + n + 1);
+  for (int i = 0; i < n; i++)
+    FVM_REQUIRE(row[i + 1] >= row[i], kBadArgument, "row offsets must be non-decreasing");
+  const int nnz = row[n];
+  l.conn.col.assign(col, col + nnz);
+  for (int k = 0; k < nnz; k++)
+    FVM_REQUIRE(col[k] >= 0 && col[k] < n, kBadArgument, "column index out of range");
+  l.diag.assign(diag, diag + n);
+  l.off.assign(off, off + nnz);
+  return l;
+}
+
+void fill_report(fvm_report* rep, const SolveReport& s) {
+  if (!rep) return;
+  std::memset(rep, 0, sizeof(*rep));
+  rep->iterations = s.iterations;
+  rep->linearIterations = s.iterations;
+  rep->initialNorm = s.initialNorm;
+  rep->lastNorm = s.finalNorm;
+  rep->converged = s.converged ? 1 : 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* fvm_last_error(void) { return last_error(); }
+
+void fvm_default_linear_options(fvm_linear_options* o) {
+  if (!o) return;
+  SolverOptions s;
+  from_solver(s, *o);
+}
+
+void fvm_default_thermal_options(fvm_thermal_options* o) {
+  if (!o) return;
+  ThermalOptions t;
+  o->relativeTolerance = t.relativeTolerance;
+  o->absoluteTolerance = t.absoluteTolerance;
+  o->transient = t.transient ? 1 : 0;
+  o->timeDiscretizationOrder = t.timeDiscretizationOrder;
+  o->initialTemperature = t.initialTemperature;
+  o->timeStep = t.timeStep;
+  o->thermalConductivity = t.thermalConductivity;
+  o->density = t.density;
+  o->specificHeat = t.specificHeat;
+  from_solver(t.linear, o->linear);
+}
+
+int fvm_mesh_create(int dim, int nCells, int nNodes, const double* xyz, int nFaces,
+                    const int* faceCells, const int* faceNodes, const int* faceNodeCount,
+                    int nGroups, const int* groupSize, fvm_mesh** out) {
+  return guarded([&] {
+    FVM_REQUIRE(out, kBadArgument, "null output handle");
+    *out = nullptr;
+    std::shared_ptr<HostMesh> m(make_mesh(dim, nCells, nNodes, xyz, nFaces, faceCells, faceNodes,
+                                          faceNodeCount, nGroups, groupSize));
+    *out = new fvm_mesh{m};
+  });
+}
+
+int fvm_mesh_set_group(fvm_mesh* h, int group, int id, const char* type) {
+  return guarded([&] {
+    FVM_REQUIRE(h && type, kBadArgument, "null argument");
+    HostMesh& m = *h->m;
+    FVM_REQUIRE(group >= 1 && group < (int)m.groups.size(), kBadArgument, "no such boundary group");
+    const std::string t(type);
+    const bool geomChange = (t == "symmetry") != (m.groups[group].type == "symmetry");
+    m.groups[group].id = id;
+    m.groups[group].type = t;
+    if (geomChange) m.build();  // ghost centroids depend on the group type
+  });
+}
+
+int fvm_mesh_sizes(const fvm_mesh* h, int* out) {
+  return guarded([&] {
+    FVM_REQUIRE(h && out, kBadArgument, "null argument");
+    const HostMesh& m = *h->m;
+    out[0] = m.dim;
+    out[1] = m.nCells;
+    out[2] = m.nGhost;
+    out[3] = m.nNodes;
+    out[4] = m.nFaces;
+    out[5] = m.cellCells.nnz();
+    out[6] = (int)m.groups.size();
+  });
+}
+
+int fvm_mesh_connectivity(const fvm_mesh* h, int* row, int* col, int* pairToCol) {
+  return guarded([&] {
+    FVM_REQUIRE(h, kBadArgument, "null mesh");
+    const HostMesh& m = *h->m;
+    if (row) std::memcpy(row, m.cellCells.row.data(), sizeof(int) * m.cellCells.row.size());
+    if (col) std::memcpy(col, m.cellCells.col.data(), sizeof(int) * m.cellCells.col.size());
+    if (pairToCol) std::memcpy(pairToCol, m.pairToCol.data(), sizeof(int) * m.pairToCol.size());
+  });
+}
+
+int fvm_mesh_geometry(const fvm_mesh* h, double* fa, double* fam, double* fc, double* cc, double* vol) {
+  return guarded([&] {
+    FVM_REQUIRE(h, kBadArgument, "null mesh");
+    const HostMesh& m = *h->m;
+    if (fa) std::memcpy(fa, m.faceArea.data(), sizeof(double) * m.faceArea.size());
+    if (fam) std::memcpy(fam, m.faceAreaMag.data(), sizeof(double) * m.faceAreaMag.size());
+    if (fc) std::memcpy(fc, m.faceCentroid.data(), sizeof(double) * m.faceCentroid.size());
+    if (cc) std::memcpy(cc, m.cellCentroid.data(), sizeof(double) * m.cellCentroid.size());
+    if (vol) std::memcpy(vol, m.cellVolume.data(), sizeof(double) * m.cellVolume.size());
+  });
+}
+
+int fvm_mesh_destroy(fvm_mesh* h) {
+  delete h;
+  return FVM_OK;
+}
+
+int fvm_thermal_create(fvm_mesh* const* meshes, int nMesh, fvm_thermal** out) {
+  return guarded([&] {
+    FVM_REQUIRE(out && meshes, kBadArgument, "null argument");
+    *out = nullptr;
+    FVM_REQUIRE(nMesh == 1, kUnsupported, "one mesh per thermal model");
+    FVM_REQUIRE(meshes[0], kBadArgument, "null mesh");
+    std::unique_ptr<ThermalModel> t(new ThermalModel(meshes[0]->m));
+    *out = new fvm_thermal{std::move(t)};
+  });
+}
+
+int fvm_thermal_set_options(fvm_thermal* h, const fvm_thermal_options* o) {
+  return guarded([&] {
+    FVM_REQUIRE(h && o, kBadArgument, "null argument");
+    ThermalOptions& t = h->model->options();
+    FVM_REQUIRE(!o->transient || o->timeStep > 0, kBadArgument, "timeStep must be positive");
+    t.relativeTolerance = o->relativeTolerance;
+    t.absoluteTolerance = o->absoluteTolerance;
+    t.transient = o->transient != 0;
+    t.timeDiscretizationOrder = o->timeDiscretizationOrder;
+    t.initialTemperature = o->initialTemperature;
+    t.timeStep = o->timeStep;
+    t.thermalConductivity = o->thermalConductivity;
+    t.density = o->density;
+    t.specificHeat = o->specificHeat;
+    t.linear = to_solver(o->linear);
+    h->model->optionsChanged();
+  });
+}
+
+int fvm_thermal_get_options(const fvm_thermal* h, fvm_thermal_options* o) {
+  return guarded([&] {
+    FVM_REQUIRE(h && o, kBadArgument, "null argument");
+    const ThermalOptions& t = h->model->options();
+    o->relativeTolerance = t.relativeTolerance;
+    o->absoluteTolerance = t.absoluteTolerance;
+    o->transient = t.transient ? 1 : 0;
+    o->timeDiscretizationOrder = t.timeDiscretizationOrder;
+    o->initialTemperature = t.initialTemperature;
+    o->timeStep = t.timeStep;
+    o->thermalConductivity = t.thermalConductivity;
+    o->density = t.density;
+    o->specificHeat = t.specificHeat;
+    from_solver(t.linear, o->linear);
+  });
+}
+
+int fvm_thermal_set_bc(fvm_thermal* h, int mesh, int groupId, int bcType, const double* values) {
+  return guarded([&] {
+    FVM_REQUIRE(h, kBadArgument, "null model");
+    FVM_REQUIRE(mesh == 0, kBadArgument, "mesh index out of range");
+    FVM_REQUIRE(bcType >= 0 && bcType <= 5, kBadArgument, "unknown bcType");
+    GroupBC& b = h->model->bc(groupId);
+    if (b.type != (BcType)bcType) h->model->bcChanged();
+    b.type = (BcType)bcType;
+    if (values)
+      for (int i = 0; i < 5; i++) b.values[i] = values[i];
+  });
+}
+
+int fvm_thermal_get_bc(const fvm_thermal* h, int mesh, int groupId, int* bcType, double* values) {
+  return guarded([&] {
+    FVM_REQUIRE(h, kBadArgument, "null model");
+    FVM_REQUIRE(mesh == 0, kBadArgument, "mesh index out of range");
+    const GroupBC& b = h->model->bc(groupId);
+    if (bcType) *bcType = b.type;
+    if (values)
+      for (int i = 0; i < 5; i++) values[i] = b.values[i];
+  });
+}
+
+int fvm_thermal_init(fvm_thermal* h) {
+  return guarded([&] {
+    FVM_REQUIRE(h, kBadArgument, "null model");
+    h->model->init();
+  });
+}
+
+int fvm_thermal_set_cell_field(fvm_thermal* h, int mesh, int field, const double* values, int count) {
+  return guarded([&] {
+    FVM_REQUIRE(h && values, kBadArgument, "null argument");
+    FVM_REQUIRE(mesh == 0, kBadArgument, "mesh index out of range");
+    h->model->setCellField(field, values, count);
+  });
+}
+
+int fvm_thermal_get_cell_field(fvm_thermal* h, int mesh, int field, double* out, int count) {
+  return guarded([&] {
+    FVM_REQUIRE(h && out, kBadArgument, "null argument");
+    FVM_REQUIRE(mesh == 0, kBadArgument, "mesh index out of range");
+    h->model->getCellField(field, out, count);
+  });
+}
+
+int fvm_thermal_advance(fvm_thermal* h, int niter, fvm_report* rep) {
+  return guarded([&] {
+    FVM_REQUIRE(h, kBadArgument, "null model");
+    FVM_REQUIRE(niter >= 0, kBadArgument, "niter must be non-negative");
+    AdvanceReport r;
+    h->model->advance(niter, r);
+    if (rep) {
+      rep->iterations = r.iterations;
+      rep->linearIterations = r.linearIterations;
+      rep->initialNorm = r.initialNorm;
+      rep->lastNorm = r.lastNorm;
+      rep->converged = r.converged ? 1 : 0;
+      rep->seconds = r.seconds;
+      rep->setupSeconds = r.setupSeconds;
+      rep->launches = r.launches;
+    }
+  });
+}
+
+int fvm_thermal_update_time(fvm_thermal* h) {
+  return guarded([&] {
+    FVM_REQUIRE(h, kBadArgument, "null model");
+    h->model->updateTime();
+  });
+}
+
+int fvm_thermal_history(const fvm_thermal* h, double* norms, int cap, int* n) {
+  return guarded([&] {
+    FVM_REQUIRE(h && n, kBadArgument, "null argument");
+    const std::vector<double>& hist = h->model->history();
+    *n = (int)hist.size();
+    if (norms)
+      for (int i = 0; i < (int)hist.size() && i < cap; i++) norms[i] = hist[i];
+  });
+}
+
+int fvm_thermal_linear_system(fvm_thermal* h, double* diag, double* off, double* b, int* nnz) {
+  return guarded([&] {
+    FVM_REQUIRE(h, kBadArgument, "null model");
+    std::vector<double> d, o, bb;
+    h->model->linearizeOnly(d, o, bb);
+    if (nnz) *nnz = (int)o.size();
+    if (diag) std::memcpy(diag, d.data(), sizeof(double) * d.size());
+    if (off) std::memcpy(off, o.data(), sizeof(double) * o.size());
+    if (b) std::memcpy(b, bb.data(), sizeof(double) * bb.size());
+  });
+}
+
+static void export_hierarchy(const std::vector<RefLevel>& lv, int* nLevels, int* sizes, int sizesCap,
+                             int* coarseIndex, int ciCap) {
+  const int L = (int)lv.size();
+  if (nLevels) *nLevels = L - 1;
+  int pos = 0;
+  for (int l = 1; l < L; l++) {
+    if (sizes && l - 1 < sizesCap) sizes[l - 1] = lv[l].n;
+    const std::vector<int>& ci = lv[l - 1].coarseIndex;
+    for (size_t i = 0; i < ci.size() && coarseIndex; i++, pos++)
+      if (pos < ciCap) coarseIndex[pos] = ci[i];
+  }
+}
+
+int fvm_thermal_hierarchy(fvm_thermal* h, int* nLevels, int* sizes, int sizesCap, int* coarseIndex,
+                          int ciCap) {
+  return guarded([&] {
+    FVM_REQUIRE(h, kBadArgument, "null model");
+    const AmgHierarchy& hier = h->model->hierarchy();
+    export_hierarchy(hier.refLevels(), nLevels, sizes, sizesCap, coarseIndex, ciCap);
+  });
+}
+
+int fvm_thermal_destroy(fvm_thermal* h) {
+  delete h;
+  return FVM_OK;
+}
+
+int fvm_amg_hierarchy_csr(int n, const int* row, const int* col, const double* diag, const double* off,
+                          const fvm_linear_options* o, int finestLocalSize, int* nLevels, int* sizes,
+                          int sizesCap, int* coarseIndex, int ciCap, int* colors, int colorsCap) {
+  return guarded([&] {
+    FVM_REQUIRE(o, kBadArgument, "null options");
+    const SolverOptions s = to_solver(*o);
+    std::vector<RefLevel> levels(1);
+    levels[0] = level_from_csr(n, row, col, diag, off);
+    HierarchyOptions ho;
+    ho.maxCoarseLevels = s.maxCoarseLevels;
+    ho.groupSize = s.coarseGroupSize;
+    ho.weightRatioThreshold = s.weightRatioThreshold;
+    ho.coarsestSize = s.coarsestSize;
+    ho.finestLocalSize = finestLocalSize > 0 ? finestLocalSize : n;
+    std::vector<CSR> c2f;
+    build_hierarchy(levels, ho, c2f);
+    export_hierarchy(levels, nLevels, sizes, sizesCap, coarseIndex, ciCap);
+    if (colors) {
+      int pos = 0;
+      for (const RefLevel& l : levels) {
+        std::vector<int> c;
+        greedy_coloring(l.conn, c);
+        for (int v : c) {
+          if (pos < colorsCap) colors[pos] = v;
+          pos++;
+        }
+      }
+    }
+  });
+}
+
+int fvm_amg_solve_csr(int n, const int* row, const int* col, const double* diag, const double* off,
+                      const double* b, double* x, const fvm_linear_options* o, fvm_report* rep,
+                      double* history, int historyCap, int* nHistory, int* levelSizes, int levelCap,
+                      int* nLevels) {
+  return guarded([&] {
+    FVM_REQUIRE(o && b && x, kBadArgument, "null argument");
+    const SolverOptions s = to_solver(*o);
+    std::vector<RefLevel> levels(1);
+    levels[0] = level_from_csr(n, row, col, diag, off);
+    AmgHierarchy hier;
+    hier.build(levels, n, s);
+    const int L = hier.numLevels();
+    if (nLevels) *nLevels = L - 1;
+    for (int l = 1; l < L && levelSizes; l++)
+      if (l - 1 < levelCap) levelSizes[l - 1] = hier.level(l).n;
+    cudaStream_t st;
+    if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess)
+      throw Error(kDeviceError, "cannot create a CUDA stream");
+    SolveReport sr;
+    try {
+      const PackedLevel& p0 = hier.packed(0);
+      std::vector<double> bp(n);
+      for (int i = 0; i < n; i++) bp[p0.perm[i]] = b[i];
+      DevLevel& d = hier.level(0);
+      if (cudaMemcpy(d.b, bp.data(), sizeof(double) * n, cudaMemcpyHostToDevice) != cudaSuccess)
+        throw Error(kDeviceError, "copy of b failed");
+      cudaEvent_t e0, e1;
+      cudaEventCreate(&e0);
+      cudaEventCreate(&e1);
+      cudaEventRecord(e0, st);
+      {
+        LinearSolve ls(hier);
+        sr = ls.solve(st);
+        if (rep) {
+          fill_report(rep, sr);
+          rep->launches = ls.launches;
+        }
+      }
+      cudaEventRecord(e1, st);
+      cudaEventSynchronize(e1);
+      float ms = 0;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (rep) rep->seconds = ms * 1e-3;
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      std::vector<double> xp(n);
+      if (cudaMemcpy(xp.data(), d.x, sizeof(double) * n, cudaMemcpyDeviceToHost) != cudaSuccess)
+        throw Error(kDeviceError, "copy of x failed");
+      for (int i = 0; i < n; i++) x[i] = xp[p0.perm[i]];
+    } catch (...) {
+      cudaStreamDestroy(st);
+      throw;
+    }
+    cudaStreamDestroy(st);
+    if (nHistory) *nHistory = (int)sr.history.size();
+    for (size_t i = 0; history && i < sr.history.size() && (int)i < historyCap; i++)
+      history[i] = sr.history[i];
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,51 @@
+// Shared host-side definitions for the fvm_b200 library: error reporting,
+// compressed-row (CSR) containers and CUDA call checking.
+#pragma once
+
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace fvm {
+
+// Status codes returned through the C ABI (mirrored in include/fvm_b200.h).
+enum Status {
+  kOk = 0,
+  kBadArgument = 1,
+  kBadMesh = 2,
+  kNotConverged = 3,
+  kNaN = 4,
+  kDeviceError = 5,
+  kLearnedRejected = 6,
+  kUnsupported = 7,
+  kTooLarge = 8,
+};
+
+// An error raised anywhere below the C ABI; the ABI turns it into a status
+// code plus a message readable through fvm_last_error(). This mirrors the
+// reference's CException, which SWIG maps onto RuntimeError.
+struct Error : std::runtime_error {
+  int status;
+  Error(int s, const std::string& m) : std::runtime_error(m), status(s) {}
+};
+
+void set_last_error(const std::string& msg);
+const char* last_error();
+
+#define FVM_REQUIRE(cond, status, msg)                 \
+  do {                                                 \
+    if (!(cond)) throw ::fvm::Error((status), (msg)); \
+  } while (0)
+
+// Compressed rows: row[i]..row[i+1] index col[] (and any value arrays kept
+// alongside). Matches the reference's CRConnectivity layout.
+struct CSR {
+  int nRows = 0;
+  std::vector<int> row;
+  std::vector<int> col;
+  int count(int i) const { return row[i + 1] - row[i]; }
+  int nnz() const { return row.empty() ? 0 : row[nRows]; }
+};
+
+}  // namespace fvm

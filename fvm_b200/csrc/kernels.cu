@@ -1,0 +1,539 @@
+// sm_100a kernels for the thermal linearization and the AMG / Krylov solve.
+//
+// Build note: this file is compiled with -fmad=false. Every FP64 product
+// and sum then rounds on its own, exactly as the reference's scalar C++
+// does on x86-64, which keeps the face coefficients, the matrix and the
+// right-hand side bit-identical to the reference and lets the sequential
+// Gauss-Seidel and Jacobi smoothers reproduce its iterates. The kernels are
+// memory-bound, so fused multiply-adds would buy no speed here.
+//
+// Layout: level matrices are colour-permuted SELL-32 (32 rows per slice,
+// entries stored column-major inside the slice, so a warp reads 32
+// consecutive cols/vals per step: fully coalesced 128 B / 256 B lines).
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "kernels.cuh"
+
+namespace fvm {
+namespace dev {
+
+namespace {
+
+constexpr int kBlock = 256;           // threads per block for row kernels
+constexpr int kSlicesPerBlock = kBlock / 32;
+constexpr int kReduceBlocks = 1184;   // 148 SMs x 8: vector reductions
+
+inline int ceil_div(long long a, long long b) { return (int)((a + b - 1) / b); }
+
+__device__ __forceinline__ double warp_sum(double v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Block-wide sum of one double per thread; result valid in thread 0.
+__device__ __forceinline__ double block_sum(double v) {
+  __shared__ double sh[32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  v = warp_sum(v);
+  if (lane == 0) sh[wid] = v;
+  __syncthreads();
+  const int nw = (blockDim.x + 31) >> 5;
+  v = (threadIdx.x < nw) ? sh[threadIdx.x] : 0.0;
+  if (wid == 0) v = warp_sum(v);
+  return v;
+}
+
+template <class T>
+__device__ __forceinline__ T row_sum(const SellView<T>& a, int s, int lane, const T* __restrict__ x,
+                                     T sum) {
+  const int o = a.sliceOff[s];
+  const int w = (a.sliceOff[s + 1] - o) >> 5;
+  for (int k = 0; k < w; k++) {
+    const int e = o + (k << 5) + lane;
+    sum = sum + a.vals[e] * x[a.cols[e]];
+  }
+  return sum;
+}
+
+// ---------------------------------------------------------------------------
+template <class T>
+__global__ void k_gs_color(SellView<T> a, int s0, int s1, T* x, const T* __restrict__ b) {
+  const int s = s0 + blockIdx.x * kSlicesPerBlock + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (s >= s1 || lane >= a.sliceRows[s]) return;
+  const int i = a.sliceRow[s] + lane;
+  const T sum = row_sum(a, s, lane, x, b[i]);
+  x[i] = -sum / a.diag[i];
+}
+
+template <class T>
+__global__ void k_gs_sequential(SellView<T> a, T* x, const T* __restrict__ b, int reverse) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  for (int t = 0; t < a.n; t++) {
+    const int i = reverse ? a.n - 1 - t : t;
+    const int s = i >> 5, lane = i & 31;  // one colour: slices are consecutive 32-row blocks
+    const T sum = row_sum(a, s, lane, x, b[i]);
+    x[i] = -sum / a.diag[i];
+  }
+}
+
+template <class T>
+__global__ void k_jacobi(SellView<T> a, int nSlices, const T* __restrict__ xold, T* xnew,
+                         const T* __restrict__ b) {
+  const int s = blockIdx.x * kSlicesPerBlock + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (s >= nSlices || lane >= a.sliceRows[s]) return;
+  const int i = a.sliceRow[s] + lane;
+  const T sum = row_sum(a, s, lane, xold, b[i]);
+  xnew[i] = -sum / a.diag[i];
+}
+
+template <class T>
+__global__ void k_residual(SellView<T> a, int nSlices, const T* __restrict__ x,
+                           const T* __restrict__ b, T* r, double* partials) {
+  const int s = blockIdx.x * kSlicesPerBlock + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  double l1 = 0.0;
+  if (s < nSlices && lane < a.sliceRows[s]) {
+    const int i = a.sliceRow[s] + lane;
+    // reference order: r = b + d x, then r += a_ij x_j
+    const T ri = row_sum(a, s, lane, x, b[i] + a.diag[i] * x[i]);
+    r[i] = ri;
+    l1 = fabs((double)ri);
+  }
+  if (partials) {
+    const double t = block_sum(l1);
+    if (threadIdx.x == 0) partials[blockIdx.x] = t;
+  }
+}
+
+__global__ void k_spmv(SellView<double> a, int nSlices, const double* __restrict__ x, double* y) {
+  const int s = blockIdx.x * kSlicesPerBlock + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (s >= nSlices || lane >= a.sliceRows[s]) return;
+  const int i = a.sliceRow[s] + lane;
+  y[i] = row_sum(a, s, lane, x, a.diag[i] * x[i]);
+}
+
+template <class T>
+__global__ void k_restrict(int nc, const int* __restrict__ c2fRow, const int* __restrict__ c2fCol,
+                           const T* __restrict__ r, T* bc) {
+  const int I = blockIdx.x * blockDim.x + threadIdx.x;
+  if (I >= nc) return;
+  T s = T(0);
+  for (int k = c2fRow[I]; k < c2fRow[I + 1]; k++) s = s + r[c2fCol[k]];
+  bc[I] = s;
+}
+
+// Fine-row residuals computed inside the restriction: rowSlice maps a fine
+// row to its slice (lane = row - sliceRow).
+template <class T>
+__global__ void k_residual_restrict(SellView<T> a, const int* __restrict__ rowSlice, int nc,
+                                    const int* __restrict__ c2fRow, const int* __restrict__ c2fCol,
+                                    const T* __restrict__ x, const T* __restrict__ b, T* bc) {
+  const int I = blockIdx.x * blockDim.x + threadIdx.x;
+  if (I >= nc) return;
+  T s = T(0);
+  for (int k = c2fRow[I]; k < c2fRow[I + 1]; k++) {
+    const int i = c2fCol[k];
+    const int sl = rowSlice[i];
+    const int lane = i - a.sliceRow[sl];
+    const T ri = row_sum(a, sl, lane, x, b[i] + a.diag[i] * x[i]);
+    s = s + ri;
+  }
+  bc[I] = s;
+}
+
+template <class T>
+__global__ void k_prolong(int n, const int* __restrict__ ci, const T* __restrict__ xc, T* x) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int c = ci[i];
+  if (c >= 0) x[i] = x[i] + xc[c];
+}
+
+template <class T>
+__global__ void k_dense_solve(int n, const double* __restrict__ ainv, const T* __restrict__ b, T* x) {
+  // one warp per row
+  const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (row >= n) return;
+  double s = 0.0;
+  for (int j = lane; j < n; j += 32) s += ainv[(size_t)row * n + j] * (double)b[j];
+  s = warp_sum(s);
+  if (lane == 0) x[row] = (T)(-s);
+}
+
+__global__ void k_convert_d2f(int n, const double* __restrict__ a, float* b) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) b[i] = (float)a[i];
+}
+__global__ void k_add_f2d(int n, const float* __restrict__ a, double* b) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) b[i] = b[i] + (double)a[i];
+}
+__global__ void k_l1_partials(int n, const double* __restrict__ a, double* partials) {
+  double s = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) s += fabs(a[i]);
+  s = block_sum(s);
+  if (threadIdx.x == 0) partials[blockIdx.x] = s;
+}
+__global__ void k_dot_partials(int n, const double* __restrict__ a, const double* __restrict__ b,
+                               double* partials) {
+  double s = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) s += a[i] * b[i];
+  s = block_sum(s);
+  if (threadIdx.x == 0) partials[blockIdx.x] = s;
+}
+__global__ void k_sum_partials(int np, const double* __restrict__ p, double* out) {
+  double s = 0.0;
+  for (int i = threadIdx.x; i < np; i += blockDim.x) s += p[i];
+  s = block_sum(s);
+  if (threadIdx.x == 0) out[0] = s;
+}
+__global__ void k_scalar_div(const double* num, const double* den, double* out) {
+  out[0] = num[0] / den[0];
+}
+__global__ void k_scalar_ratio_product(const double* a, const double* b, const double* c,
+                                       const double* d, double* out) {
+  out[0] = (a[0] / b[0]) * (c[0] / d[0]);
+}
+__global__ void k_axpy_dev(int n, const double* s, double sign, const double* __restrict__ x, double* y) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) y[i] = y[i] + (sign * s[0]) * x[i];
+}
+__global__ void k_xpby_dev(int n, const double* __restrict__ z, const double* beta, double* p) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) p[i] = p[i] * beta[0] + z[i];
+}
+__global__ void k_bicg_p(int n, const double* __restrict__ r, const double* __restrict__ v,
+                         const double* omega, const double* beta, double* p) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) p[i] = (p[i] - omega[0] * v[i]) * beta[0] + r[i];
+}
+__global__ void k_copy_d(int n, const double* __restrict__ a, double* b) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) b[i] = a[i];
+}
+
+// ---------------------------------------------------------------------------
+// thermal linearization
+__device__ __forceinline__ double harmonic_average(double x0, double x1) {
+  const double sum = x0 + x1;
+  if (x0 + x1 != 0.0) return 2.0 * x0 * x1 / sum;
+  return sum;
+}
+
+__global__ void k_face_coefficients(FaceGeom g, const double* __restrict__ k, double* coeff,
+                                    double* secCoeff) {
+  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= g.nFaces) return;
+  const int c0 = g.faceCells[2 * f], c1 = g.faceCells[2 * f + 1];
+  const double vol0 = g.cellVolume[c0], vol1 = g.cellVolume[c1];
+  double ds[3];
+  for (int d = 0; d < 3; d++) ds[d] = g.cellCentroid[3 * c1 + d] - g.cellCentroid[3 * c0 + d];
+  double kf;
+  if (vol0 == 0.)
+    kf = k[c1];
+  else if (vol1 == 0.)
+    kf = k[c0];
+  else
+    kf = harmonic_average(k[c0], k[c1]);
+  const double* A = &g.faceArea[3 * f];
+  const double am = g.faceAreaMag[f];
+  const double dm = am * am / (A[0] * ds[0] + A[1] * ds[1] + A[2] * ds[2]);
+  coeff[f] = kf * dm;
+  for (int d = 0; d < 3; d++) secCoeff[3 * f + d] = kf * (A[d] - ds[d] * dm);
+}
+
+__global__ void k_gradient(int nCells, const int* __restrict__ row, const int* __restrict__ col,
+                           const double* __restrict__ w, const double* __restrict__ x, double* grad) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nCells) return;
+  double g0 = 0.0, g1 = 0.0, g2 = 0.0;
+  const double xi = x[i];
+  for (int k = row[i]; k < row[i + 1]; k++) {
+    const double dx = x[col[k]] - xi;
+    g0 += w[3 * k] * dx;
+    g1 += w[3 * k + 1] * dx;
+    g2 += w[3 * k + 2] * dx;
+  }
+  grad[3 * i] = g0;
+  grad[3 * i + 1] = g1;
+  grad[3 * i + 2] = g2;
+}
+
+__global__ void k_ghost_gradient(int nB, const int* __restrict__ bFaces, const int* __restrict__ fc,
+                                 double* grad) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nB) return;
+  const int f = bFaces[t];
+  const int c0 = fc[2 * f], c1 = fc[2 * f + 1];
+  for (int d = 0; d < 3; d++) grad[3 * c1 + d] = grad[3 * c0 + d];
+}
+
+__global__ void k_face_flux(FaceGeom g, const double* __restrict__ coeff,
+                            const double* __restrict__ sec, const double* __restrict__ grad,
+                            const double* __restrict__ x, double* flux) {
+  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= g.nFaces) return;
+  const int c0 = g.faceCells[2 * f], c1 = g.faceCells[2 * f + 1];
+  const double vol0 = g.cellVolume[c0], vol1 = g.cellVolume[c1];
+  const double vs = vol0 + vol1;
+  double s = 0.0;
+  for (int d = 0; d < 3; d++) {
+    const double gF = (grad[3 * c0 + d] * vol0 + grad[3 * c1 + d] * vol1) / vs;
+    s += gF * sec[3 * f + d];
+  }
+  flux[f] = coeff[f] * (x[c1] - x[c0]) + s;
+}
+
+__global__ void k_assemble_rhs(int nCells, CellFaceView cf, const int* __restrict__ fc,
+                               const double* __restrict__ flux, const double* __restrict__ coeff,
+                               const double* __restrict__ am, const double* __restrict__ vol,
+                               const double* __restrict__ source, const double* __restrict__ rhoVdt,
+                               const double* __restrict__ xN1, BoundaryData bd,
+                               const int* __restrict__ bIndexOfFace, double* x, double* bGhost,
+                               const int* __restrict__ perm, double* b) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nCells) return;
+  // DiffusionDiscretization: r0 += flux, r1 -= flux, faces ascending
+  double r = 0.0;
+  for (int k = cf.row[i]; k < cf.row[i + 1]; k++) {
+    const int f = cf.col[k];
+    if (fc[2 * f] == i)
+      r += flux[f];
+    else
+      r -= flux[f];
+  }
+  // SourceDiscretization
+  r += vol[i] * source[i];
+  // TimeDerivativeDiscretization (first order)
+  if (rhoVdt) r -= rhoVdt[i] * (x[i] - xN1[i]);
+  // GenericBCS::applyDirichletBC: r0 += a01 (Tb - x1); ghost takes Tb
+  for (int k = cf.bRow[i]; k < cf.bRow[i + 1]; k++) {
+    const int f = cf.bCol[k];
+    const int t = bIndexOfFace[f];
+    if (bd.kind[t] == 0) {
+      const int c1 = fc[2 * f + 1];
+      const double dX = bd.value[t] - x[c1];
+      r += coeff[f] * dX;
+      x[c1] = bd.value[t];
+    }
+  }
+  // applyNeumannBC sets the ghost row's rhs; eliminateBoundaryEquations
+  // then folds it into the interior row: b_i -= a_ij (b_j / a_jj)
+  for (int k = cf.bRow[i]; k < cf.bRow[i + 1]; k++) {
+    const int f = cf.bCol[k];
+    const int t = bIndexOfFace[f];
+    if (bd.kind[t] == 1) {
+      const double fluxB = -(0.0 - flux[f]);
+      const double bj = bd.value[t] * am[f] - fluxB;
+      const double ajj = 0.0 - coeff[f];
+      bGhost[t] = bj;
+      r -= coeff[f] * (bj / ajj);
+    }
+  }
+  b[perm[i]] = r;
+}
+
+__global__ void k_assemble_matrix(int nCells, CellFaceView cf, const int* __restrict__ fc,
+                                  const double* __restrict__ coeff, const double* __restrict__ rhoVdt,
+                                  BoundaryData bd, const int* __restrict__ bIndexOfFace, double* diag) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nCells) return;
+  double d = 0.0;
+  for (int k = cf.row[i]; k < cf.row[i + 1]; k++) d -= coeff[cf.col[k]];
+  if (rhoVdt) d -= rhoVdt[i];
+  for (int k = cf.bRow[i]; k < cf.bRow[i + 1]; k++) {
+    const int f = cf.bCol[k];
+    if (bd.kind[bIndexOfFace[f]] == 1) {
+      const double aij = coeff[f];
+      const double ajj = 0.0 - coeff[f];
+      d -= aij * (aij / ajj);
+    }
+  }
+  diag[i] = d;
+}
+
+__global__ void k_transient_coeff(int n, const double* __restrict__ rc, const double* __restrict__ vol,
+                                  double dt, double* out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = rc[i] * vol[i] / dt;
+}
+
+__global__ void k_cast_d2f(int n, const double* __restrict__ a, float* b) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) b[i] = (float)a[i];
+}
+
+__global__ void k_update_self(int nCells, const int* __restrict__ perm, const double* __restrict__ delta,
+                              double* x) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < nCells) x[i] = x[i] + delta[perm[i]];
+}
+
+// Neumann ghost rows: delta_j = -(b_j + a_ji delta_i) / a_jj with
+// a_ji = c_f, a_jj = -c_f (CRMatrix::solveBoundary); Dirichlet ghosts keep
+// delta 0. Runs after k_update_self, so delta_i is read from the delta array.
+__global__ void k_update_ghosts(BoundaryData bd, const int* __restrict__ perm,
+                                const double* __restrict__ delta, const int* __restrict__ fc,
+                                const double* __restrict__ coeff, const double* __restrict__ bGhost,
+                                double* x) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= bd.nBFaces || bd.kind[t] != 1) return;
+  const int f = bd.bFace[t];
+  const int c0 = fc[2 * f], c1 = fc[2 * f + 1];
+  const double sum = bGhost[t] + coeff[f] * delta[perm[c0]];
+  const double dj = -sum / (0.0 - coeff[f]);
+  x[c1] = x[c1] + dj;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// wrappers
+template <class T>
+void gs_color(const SellView<T>& a, int s0, int s1, T* x, const T* b, cudaStream_t st) {
+  if (s1 <= s0) return;
+  k_gs_color<T><<<ceil_div(s1 - s0, kSlicesPerBlock), kBlock, 0, st>>>(a, s0, s1, x, b);
+}
+template <class T>
+void gs_sequential(const SellView<T>& a, T* x, const T* b, bool reverse, cudaStream_t st) {
+  k_gs_sequential<T><<<1, 32, 0, st>>>(a, x, b, reverse ? 1 : 0);
+}
+template <class T>
+void jacobi(const SellView<T>& a, int nSlices, const T* xold, T* xnew, const T* b, cudaStream_t st) {
+  k_jacobi<T><<<ceil_div(nSlices, kSlicesPerBlock), kBlock, 0, st>>>(a, nSlices, xold, xnew, b);
+}
+template <class T>
+void residual(const SellView<T>& a, int nSlices, const T* x, const T* b, T* r, double* partials,
+              cudaStream_t st) {
+  k_residual<T><<<ceil_div(nSlices, kSlicesPerBlock), kBlock, 0, st>>>(a, nSlices, x, b, r, partials);
+}
+int reduce_blocks(int nSlices) { return ceil_div(nSlices, kSlicesPerBlock); }
+void spmv(const SellView<double>& a, int nSlices, const double* x, double* y, cudaStream_t st) {
+  k_spmv<<<ceil_div(nSlices, kSlicesPerBlock), kBlock, 0, st>>>(a, nSlices, x, y);
+}
+template <class T>
+void restrict_sum(int nc, const int* c2fRow, const int* c2fCol, const T* r, T* bc, cudaStream_t st) {
+  k_restrict<T><<<ceil_div(nc, kBlock), kBlock, 0, st>>>(nc, c2fRow, c2fCol, r, bc);
+}
+template <class T>
+void residual_restrict(const SellView<T>& a, const int* rowSlice, int nc, const int* c2fRow,
+                       const int* c2fCol, const T* x, const T* b, T* bc, cudaStream_t st) {
+  k_residual_restrict<T><<<ceil_div(nc, kBlock), kBlock, 0, st>>>(a, rowSlice, nc, c2fRow, c2fCol, x, b, bc);
+}
+template <class T>
+void prolong(int n, const int* ci, const T* xc, T* x, cudaStream_t st) {
+  k_prolong<T><<<ceil_div(n, kBlock), kBlock, 0, st>>>(n, ci, xc, x);
+}
+template <class T>
+void dense_solve(int n, const double* ainv, const T* b, T* x, cudaStream_t st) {
+  k_dense_solve<T><<<ceil_div(n, kBlock / 32), kBlock, 0, st>>>(n, ainv, b, x);
+}
+void convert_d2f(int n, const double* a, float* b, cudaStream_t st) {
+  k_convert_d2f<<<ceil_div(n, kBlock), kBlock, 0, st>>>(n, a, b);
+}
+void add_f2d(int n, const float* a, double* b, cudaStream_t st) {
+  k_add_f2d<<<ceil_div(n, kBlock), kBlock, 0, st>>>(n, a, b);
+}
+int vec_blocks(int n) {
+  const int b = ceil_div(n, kBlock);
+  return b < kReduceBlocks ? (b < 1 ? 1 : b) : kReduceBlocks;
+}
+void l1_partials(int n, const double* a, double* partials, cudaStream_t st) {
+  k_l1_partials<<<vec_blocks(n), kBlock, 0, st>>>(n, a, partials);
+}
+void dot_partials(int n, const double* a, const double* b, double* partials, cudaStream_t st) {
+  k_dot_partials<<<vec_blocks(n), kBlock, 0, st>>>(n, a, b, partials);
+}
+void sum_partials(int np, const double* partials, double* out, cudaStream_t st) {
+  k_sum_partials<<<1, 1024, 0, st>>>(np, partials, out);
+}
+void scalar_div(const double* num, const double* den, double* out, cudaStream_t st) {
+  k_scalar_div<<<1, 1, 0, st>>>(num, den, out);
+}
+void scalar_ratio_product(const double* a, const double* b, const double* c, const double* d,
+                          double* out, cudaStream_t st) {
+  k_scalar_ratio_product<<<1, 1, 0, st>>>(a, b, c, d, out);
+}
+void axpy_dev(int n, const double* s, double sign, const double* x, double* y, cudaStream_t st) {
+  k_axpy_dev<<<ceil_div(n, kBlock), kBlock, 0, st>>>(n, s, sign, x, y);
+}
+void xpby_dev(int n, const double* z, const double* beta, double* p, cudaStream_t st) {
+  k_xpby_dev<<<ceil_div(n, kBlock), kBlock, 0, st>>>(n, z, beta, p);
+}
+void bicg_p_update(int n, const double* r, const double* v, const double* omega, const double* beta,
+                   double* p, cudaStream_t st) {
+  k_bicg_p<<<ceil_div(n, kBlock), kBlock, 0, st>>>(n, r, v, omega, beta, p);
+}
+void copy_d(int n, const double* a, double* b, cudaStream_t st) {
+  k_copy_d<<<ceil_div(n, kBlock), kBlock, 0, st>>>(n, a, b);
+}
+
+void face_coefficients(const FaceGeom& g, const double* k, double* coeff, double* secCoeff,
+                       cudaStream_t st) {
+  k_face_coefficients<<<ceil_div(g.nFaces, kBlock), kBlock, 0, st>>>(g, k, coeff, secCoeff);
+}
+void gradient(int nCells, const int* ccRow, const int* ccCol, const double* w, const double* x,
+              double* grad, cudaStream_t st) {
+  k_gradient<<<ceil_div(nCells, kBlock), kBlock, 0, st>>>(nCells, ccRow, ccCol, w, x, grad);
+}
+void ghost_gradient(int nB, const int* bFaces, const int* faceCells, double* grad, cudaStream_t st) {
+  if (nB > 0) k_ghost_gradient<<<ceil_div(nB, kBlock), kBlock, 0, st>>>(nB, bFaces, faceCells, grad);
+}
+void face_flux(const FaceGeom& g, const double* coeff, const double* secCoeff, const double* grad,
+               const double* x, double* flux, cudaStream_t st) {
+  k_face_flux<<<ceil_div(g.nFaces, kBlock), kBlock, 0, st>>>(g, coeff, secCoeff, grad, x, flux);
+}
+void assemble_rhs(int nCells, const CellFaceView& cf, const int* faceCells, const double* flux,
+                  const double* coeff, const double* faceAreaMag, const double* vol,
+                  const double* source, const double* rhoVdt, const double* xN1,
+                  const BoundaryData& bd, const int* bIndexOfFace, double* x, double* bGhost,
+                  const int* perm, double* b, cudaStream_t st) {
+  k_assemble_rhs<<<ceil_div(nCells, kBlock), kBlock, 0, st>>>(nCells, cf, faceCells, flux, coeff,
+                                                              faceAreaMag, vol, source, rhoVdt, xN1,
+                                                              bd, bIndexOfFace, x, bGhost, perm, b);
+}
+void assemble_matrix(int nCells, const CellFaceView& cf, const int* faceCells, const double* coeff,
+                     const double* rhoVdt, const BoundaryData& bd, const int* bIndexOfFace,
+                     double* diagOrig, cudaStream_t st) {
+  k_assemble_matrix<<<ceil_div(nCells, kBlock), kBlock, 0, st>>>(nCells, cf, faceCells, coeff, rhoVdt,
+                                                                 bd, bIndexOfFace, diagOrig);
+}
+void transient_coeff(int n, const double* rhoCp, const double* vol, double dt, double* out,
+                     cudaStream_t st) {
+  k_transient_coeff<<<ceil_div(n, kBlock), kBlock, 0, st>>>(n, rhoCp, vol, dt, out);
+}
+void cast_d2f_vals(int n, const double* a, float* b, cudaStream_t st) {
+  k_cast_d2f<<<ceil_div(n, kBlock), kBlock, 0, st>>>(n, a, b);
+}
+void update_solution(int nCells, const int* perm, const double* delta, const BoundaryData& bd,
+                     const int* faceCells, const double* coeff, const double* bGhost, double* x,
+                     cudaStream_t st) {
+  k_update_self<<<ceil_div(nCells, kBlock), kBlock, 0, st>>>(nCells, perm, delta, x);
+  if (bd.nBFaces > 0)
+    k_update_ghosts<<<ceil_div(bd.nBFaces, kBlock), kBlock, 0, st>>>(bd, perm, delta, faceCells, coeff,
+                                                                     bGhost, x);
+}
+
+// explicit instantiations
+#define FVM_INST(T)                                                                              \
+  template void gs_color<T>(const SellView<T>&, int, int, T*, const T*, cudaStream_t);           \
+  template void gs_sequential<T>(const SellView<T>&, T*, const T*, bool, cudaStream_t);          \
+  template void jacobi<T>(const SellView<T>&, int, const T*, T*, const T*, cudaStream_t);        \
+  template void residual<T>(const SellView<T>&, int, const T*, const T*, T*, double*, cudaStream_t); \
+  template void restrict_sum<T>(int, const int*, const int*, const T*, T*, cudaStream_t);        \
+  template void residual_restrict<T>(const SellView<T>&, const int*, int, const int*, const int*,   \
+                                     const T*, const T*, T*, cudaStream_t);                      \
+  template void prolong<T>(int, const int*, const T*, T*, cudaStream_t);                         \
+  template void dense_solve<T>(int, const double*, const T*, T*, cudaStream_t);
+FVM_INST(double)
+FVM_INST(float)
+#undef FVM_INST
+
+}  // namespace dev
+}  // namespace fvm

@@ -1,0 +1,152 @@
+// Launch wrappers for the sm_100a kernels of the thermal/AMG hot path.
+// Every wrapper enqueues on the given stream and never synchronises, so
+// sequences of them can be captured into CUDA graphs.
+#pragma once
+
+#include <cuda_runtime.h>
+
+namespace fvm {
+namespace dev {
+
+// A level matrix in colour-permuted SELL-32 form (see amg_setup.hpp).
+template <class T>
+struct SellView {
+  int n;
+  const int* sliceRow;
+  const int* sliceRows;
+  const int* sliceOff;
+  const int* cols;
+  const T* vals;
+  const T* diag;
+};
+
+// ---- smoothers -----------------------------------------------------------
+// One Gauss-Seidel pass over the rows of slices [s0, s1) (one colour block):
+// x_i = -(b_i + sum_j a_ij x_j) / a_ii
+template <class T>
+void gs_color(const SellView<T>& a, int s0, int s1, T* x, const T* b, cudaStream_t st);
+// Lexicographic Gauss-Seidel by a single thread in row order (reverse when
+// asked): the reference's CRMatrix::forwardGS / reverseGS, for parity runs.
+template <class T>
+void gs_sequential(const SellView<T>& a, T* x, const T* b, bool reverse, cudaStream_t st);
+// Jacobi: xnew_i = -(b_i + sum_j a_ij xold_j) / a_ii over all rows
+template <class T>
+void jacobi(const SellView<T>& a, int nSlices, const T* xold, T* xnew, const T* b, cudaStream_t st);
+
+// ---- residual / products ---------------------------------------------------
+// r = b + D x + O x over all rows; when partials != null each block also
+// writes the L1 sum of its rows' r to partials[blockIdx] (FP64).
+template <class T>
+void residual(const SellView<T>& a, int nSlices, const T* x, const T* b, T* r, double* partials,
+              cudaStream_t st);
+// y = D x + O x (FP64 only)
+void spmv(const SellView<double>& a, int nSlices, const double* x, double* y, cudaStream_t st);
+int reduce_blocks(int nSlices);  // number of partials residual() writes
+
+// ---- transfers ---------------------------------------------------------------
+// bc[I] = sum over fine rows i of aggregate I (ascending reference order) of r[i]
+template <class T>
+void restrict_sum(int nc, const int* c2fRow, const int* c2fCol, const T* r, T* bc, cudaStream_t st);
+// residual of the fine rows fused into the restriction (r never stored)
+template <class T>
+void residual_restrict(const SellView<T>& a, const int* rowSlice, int nc, const int* c2fRow,
+                       const int* c2fCol, const T* x, const T* b, T* bc, cudaStream_t st);
+// x[i] += xc[ci[i]]
+template <class T>
+void prolong(int n, const int* ci, const T* xc, T* x, cudaStream_t st);
+
+// ---- coarsest level --------------------------------------------------------
+// x = -Ainv b with a dense FP64 inverse (n x n, row-major)
+template <class T>
+void dense_solve(int n, const double* ainv, const T* b, T* x, cudaStream_t st);
+
+// ---- vector ops ------------------------------------------------------------
+void convert_d2f(int n, const double* a, float* b, cudaStream_t st);
+void add_f2d(int n, const float* a, double* b, cudaStream_t st);  // b += a
+// partial sums of |a| or a*b per block, finalised by sum_partials
+int vec_blocks(int n);
+void l1_partials(int n, const double* a, double* partials, cudaStream_t st);
+void dot_partials(int n, const double* a, const double* b, double* partials, cudaStream_t st);
+// out[0] = sum of the partials in a fixed order
+void sum_partials(int np, const double* partials, double* out, cudaStream_t st);
+// scalar recurrences for the Krylov solvers, all on the device:
+// out = num / den (out, num, den are device scalars)
+void scalar_div(const double* num, const double* den, double* out, cudaStream_t st);
+// out = (a / b) * (c / d)
+void scalar_ratio_product(const double* a, const double* b, const double* c, const double* d,
+                          double* out, cudaStream_t st);
+// y += s * x (s a device scalar, sign +1/-1)
+void axpy_dev(int n, const double* s, double sign, const double* x, double* y, cudaStream_t st);
+// p = z + beta * p
+void xpby_dev(int n, const double* z, const double* beta, double* p, cudaStream_t st);
+// p = (p - omega v) * beta + r   (BiCGStab direction update)
+void bicg_p_update(int n, const double* r, const double* v, const double* omega,
+                   const double* beta, double* p, cudaStream_t st);
+void copy_d(int n, const double* a, double* b, cudaStream_t st);
+
+// ---- thermal linearization (original cell order) -----------------------------
+struct FaceGeom {
+  int nFaces;
+  int nCells;  // self cells
+  const int* faceCells;       // 2 per face
+  const double* faceArea;     // 3 per face
+  const double* faceAreaMag;  // per face
+  const double* cellCentroid; // 3 per cell (self + ghost)
+  const double* cellVolume;   // per cell (self + ghost)
+};
+// c_f and the secondary (non-orthogonal) coefficient per face
+void face_coefficients(const FaceGeom& g, const double* k, double* coeff, double* secCoeff,
+                       cudaStream_t st);
+// least-squares gradient of x on self rows, then boundary ghosts copy c0
+void gradient(int nCells, const int* ccRow, const int* ccCol, const double* w, const double* x,
+              double* grad, cudaStream_t st);
+void ghost_gradient(int nBFaces, const int* bFaces, const int* faceCells, double* grad,
+                    cudaStream_t st);
+// flux_f = c_f (x1 - x0) + gradF . sec_f
+void face_flux(const FaceGeom& g, const double* coeff, const double* secCoeff,
+               const double* grad, const double* x, double* flux, cudaStream_t st);
+
+// Per boundary face: BC kind (0 Dirichlet, 1 Neumann/Symmetry) and value
+struct BoundaryData {
+  int nBFaces;
+  const int* bFace;     // face index of each boundary face
+  const int* kind;      // 0 Dirichlet, 1 Neumann
+  const double* value;  // specified temperature or heat flux
+};
+struct CellFaceView {
+  const int* row;  // cellFaces over self cells
+  const int* col;
+  const int* bRow;  // per self cell: range into the boundary-face list (ascending face)
+  const int* bCol;
+};
+// Assembles the delta-form right-hand side of every self cell exactly as
+// DiffusionDiscretization + Source + TimeDerivative + GenericBCS +
+// eliminateBoundaryEquations produce it, writing b[perm[i]]; also records
+// the Neumann ghost rhs (bGhost) and sets Dirichlet ghosts of x to the
+// boundary value. transient: rhoVdt != null.
+void assemble_rhs(int nCells, const CellFaceView& cf, const int* faceCells, const double* flux,
+                  const double* coeff, const double* faceAreaMag, const double* vol,
+                  const double* source, const double* rhoVdt, const double* xN1,
+                  const BoundaryData& bd, const int* bIndexOfFace, double* x, double* bGhost,
+                  const int* perm, double* b, cudaStream_t st);
+// The matrix part (constant while conductivity, geometry and time step are):
+// diagonal of every self cell and the off-diagonals through entryFace.
+void assemble_matrix(int nCells, const CellFaceView& cf, const int* faceCells, const double* coeff,
+                     const double* rhoVdt, const BoundaryData& bd, const int* bIndexOfFace,
+                     double* diagOrig, cudaStream_t st);
+// rhoVdt_i = rho c_i V_i / dt
+void transient_coeff(int nCells, const double* rhoCp, const double* vol, double dt, double* out,
+                     cudaStream_t st);
+// off-diagonal value of entry e = coeff[entryFace[e]] (gathered into the SELL layout)
+void gather_offdiag(int nEntries, const int* entryFace, const double* coeff, double* vals,
+                    cudaStream_t st);
+void gather_diag(int n, const int* iperm, const double* diagOrig, double* diag, cudaStream_t st);
+void cast_d2f_vals(int n, const double* a, float* b, cudaStream_t st);
+// T_i += delta[perm[i]] on self cells; Neumann ghosts solve their boundary
+// row and update too (LinearSystem::postSolve + updateSolution)
+void update_solution(int nCells, const int* perm, const double* delta, const BoundaryData& bd,
+                     const int* faceCells, const double* coeff, const double* bGhost, double* x,
+                     cudaStream_t st);
+
+}  // namespace dev
+}  // namespace fvm

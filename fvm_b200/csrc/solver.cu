@@ -1,0 +1,579 @@
+// GPU AMG hierarchy and the linear solvers built on it.
+#include "solver.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+
+namespace fvm {
+
+#define CUDA_OK(call)                                                                       \
+  do {                                                                                      \
+    cudaError_t e_ = (call);                                                                \
+    if (e_ != cudaSuccess)                                                                  \
+      throw ::fvm::Error(::fvm::kDeviceError, std::string(#call ": ") + cudaGetErrorString(e_)); \
+  } while (0)
+
+// ---------------------------------------------------------------------------
+DeviceArena::~DeviceArena() { release(); }
+
+void* DeviceArena::alloc(size_t bytes) {
+  void* p = nullptr;
+  if (bytes == 0) bytes = 16;
+  CUDA_OK(cudaMalloc(&p, bytes));
+  ptrs_.push_back(p);
+  bytes_ += bytes;
+  return p;
+}
+
+void DeviceArena::copy_h2d(void* d, const void* h, size_t n) {
+  CUDA_OK(cudaMemcpy(d, h, n, cudaMemcpyHostToDevice));
+}
+
+void DeviceArena::release() {
+  for (void* p : ptrs_) cudaFree(p);
+  ptrs_.clear();
+  bytes_ = 0;
+}
+
+// ---------------------------------------------------------------------------
+void AmgHierarchy::release() {
+  arena_.release();
+  lv_.clear();
+  packed_.clear();
+  ref_.clear();
+  coarseInv_ = nullptr;
+}
+
+std::vector<int> AmgHierarchy::sizes() const {
+  std::vector<int> s;
+  for (const DevLevel& l : lv_) s.push_back(l.n);
+  return s;
+}
+
+void AmgHierarchy::build(std::vector<RefLevel>& levels, int finestLocalSize, const SolverOptions& opt) {
+  release();
+  opt_ = opt;
+  ref_ = std::move(levels);
+  levels.clear();
+  HierarchyOptions ho;
+  ho.maxCoarseLevels = opt.maxCoarseLevels;
+  ho.groupSize = opt.coarseGroupSize;
+  ho.weightRatioThreshold = opt.weightRatioThreshold;
+  ho.coarsestSize = opt.coarsestSize;
+  ho.finestLocalSize = finestLocalSize;
+  std::vector<CSR> c2f;
+  build_hierarchy(ref_, ho, c2f);
+  const int L = (int)ref_.size();
+  packed_.resize(L);
+  for (int l = 0; l < L; l++) pack_level(ref_[l], opt.ordering, packed_[l]);
+  for (int l = 0; l + 1 < L; l++) pack_transfer(ref_[l], c2f[l], packed_[l], packed_[l + 1]);
+
+  const bool mixed = opt.precision == kMixed;
+  lv_.resize(L);
+  for (int l = 0; l < L; l++) {
+    const PackedLevel& p = packed_[l];
+    DevLevel& d = lv_[l];
+    d.n = p.n;
+    d.nColors = p.nColors;
+    d.nSlices = (int)p.sliceRow.size();
+    d.maxWidth = p.maxWidth;
+    d.colorSliceStart = p.colorSliceStart;
+    d.entries = p.cols.size();
+    d.sliceRow = arena_.upload(p.sliceRow);
+    d.sliceRows = arena_.upload(p.sliceRows);
+    d.sliceOff = arena_.upload(p.sliceOff);
+    d.cols = arena_.upload(p.cols);
+    d.vals = arena_.upload(p.vals);
+    d.diag = arena_.upload(p.diag);
+    std::vector<int> rs(p.n);
+    for (int s = 0; s < d.nSlices; s++)
+      for (int k = 0; k < p.sliceRows[s]; k++) rs[p.sliceRow[s] + k] = s;
+    d.rowSlice = arena_.upload(rs);
+    if (l + 1 < L) {
+      d.nCoarse = packed_[l + 1].n;
+      d.ci = arena_.upload(p.coarseIndex);
+      d.c2fRow = arena_.upload(p.c2fRow);
+      d.c2fCol = arena_.upload(p.c2fCol);
+    }
+    const size_t nb = (size_t)p.n * sizeof(double);
+    d.x = (double*)arena_.alloc(nb);
+    d.b = (double*)arena_.alloc(nb);
+    d.r = (double*)arena_.alloc(nb);
+    d.tmp = (double*)arena_.alloc(nb);
+    CUDA_OK(cudaMemset(d.x, 0, nb));
+    CUDA_OK(cudaMemset(d.b, 0, nb));
+    d.nPartials = dev::reduce_blocks(d.nSlices);
+    d.partials = (double*)arena_.alloc(sizeof(double) * (d.nPartials + 1));
+    if (mixed) {
+      std::vector<float> vf(p.vals.begin(), p.vals.end()), df(p.diag.begin(), p.diag.end());
+      d.valsF = arena_.upload(vf);
+      d.diagF = arena_.upload(df);
+      const size_t fb = (size_t)p.n * sizeof(float);
+      d.xF = (float*)arena_.alloc(fb);
+      d.bF = (float*)arena_.alloc(fb);
+      d.rF = (float*)arena_.alloc(fb);
+      d.tmpF = (float*)arena_.alloc(fb);
+      CUDA_OK(cudaMemset(d.xF, 0, fb));
+    }
+  }
+  if (opt.coarseSolver == kCoarseDirect) {
+    const PackedLevel& c = packed_[L - 1];
+    FVM_REQUIRE(c.n <= 8192, kTooLarge,
+                "coarsest level too large for the dense direct solve; set coarsestSize");
+    std::vector<double> inv;
+    dense_inverse(c, inv);
+    coarseInv_ = arena_.upload(inv);
+  }
+}
+
+template <class T>
+static T* vec_x(DevLevel& d);
+template <>
+double* vec_x<double>(DevLevel& d) { return d.x; }
+template <>
+float* vec_x<float>(DevLevel& d) { return d.xF; }
+template <class T>
+static T* vec_b(DevLevel& d);
+template <>
+double* vec_b<double>(DevLevel& d) { return d.b; }
+template <>
+float* vec_b<float>(DevLevel& d) { return d.bF; }
+template <class T>
+static T* vec_r(DevLevel& d);
+template <>
+double* vec_r<double>(DevLevel& d) { return d.r; }
+template <>
+float* vec_r<float>(DevLevel& d) { return d.rF; }
+template <class T>
+static T* vec_tmp(DevLevel& d);
+template <>
+double* vec_tmp<double>(DevLevel& d) { return d.tmp; }
+template <>
+float* vec_tmp<float>(DevLevel& d) { return d.tmpF; }
+template <class T>
+static dev::SellView<T> view(const DevLevel& d);
+template <>
+dev::SellView<double> view<double>(const DevLevel& d) { return d.view64(); }
+template <>
+dev::SellView<float> view<float>(const DevLevel& d) { return d.view32(); }
+
+template <class T>
+void AmgHierarchy::sweeps(int nSweeps, int l, cudaStream_t st) {
+  DevLevel& d = lv_[l];
+  const dev::SellView<T> a = view<T>(d);
+  T* x = vec_x<T>(d);
+  const T* b = vec_b<T>(d);
+  for (int s = 0; s < nSweeps; s++) {
+    if (opt_.smootherType == kGaussSeidel) {
+      if (opt_.ordering == kSequential) {
+        dev::gs_sequential<T>(a, x, b, false, st);
+        dev::gs_sequential<T>(a, x, b, true, st);
+      } else {
+        const int C = d.nColors;
+        for (int c = 0; c < C; c++)
+          dev::gs_color<T>(a, d.colorSliceStart[c], d.colorSliceStart[c + 1], x, b, st);
+        // reverse pass; its first colour would repeat the last update exactly
+        for (int c = C - 2; c >= 0; c--)
+          dev::gs_color<T>(a, d.colorSliceStart[c], d.colorSliceStart[c + 1], x, b, st);
+      }
+    } else {
+      T* t = vec_tmp<T>(d);
+      dev::jacobi<T>(a, d.nSlices, x, t, b, st);
+      dev::jacobi<T>(a, d.nSlices, t, x, b, st);
+    }
+  }
+}
+
+template <class T>
+void AmgHierarchy::cycle(CycleType t, int l, cudaStream_t st) {
+  const int L = (int)lv_.size();
+  DevLevel& d = lv_[l];
+  const bool coarsest = (l == L - 1);
+  if (coarsest && coarseInv_) {
+    dev::dense_solve<T>(d.n, coarseInv_, vec_b<T>(d), vec_x<T>(d), st);
+    return;
+  }
+  sweeps<T>(opt_.nPreSweeps, l, st);
+  if (!coarsest) {
+    DevLevel& c = lv_[l + 1];
+    dev::residual_restrict<T>(view<T>(d), d.rowSlice, c.n, d.c2fRow, d.c2fCol, vec_x<T>(d),
+                              vec_b<T>(d), vec_b<T>(c), st);
+    CUDA_OK(cudaMemsetAsync(vec_x<T>(c), 0, sizeof(T) * (size_t)c.n, st));
+    cycle<T>(t, l + 1, st);
+    if (t == kWCycle)
+      cycle<T>(kWCycle, l + 1, st);
+    else if (t == kFCycle)
+      cycle<T>(kVCycle, l + 1, st);
+    dev::prolong<T>(d.n, d.ci, vec_x<T>(c), vec_x<T>(d), st);
+  }
+  sweeps<T>(opt_.nPostSweeps, l, st);
+}
+
+void AmgHierarchy::apply(const double* r, double* z, cudaStream_t st) {
+  DevLevel& d = lv_[0];
+  if (opt_.precision == kMixed) {
+    dev::convert_d2f(d.n, r, d.bF, st);
+    CUDA_OK(cudaMemsetAsync(d.xF, 0, sizeof(float) * (size_t)d.n, st));
+    cycle<float>(opt_.cycleType, 0, st);
+    CUDA_OK(cudaMemsetAsync(z, 0, sizeof(double) * (size_t)d.n, st));
+    dev::add_f2d(d.n, d.xF, z, st);
+  } else {
+    dev::copy_d(d.n, r, d.b, st);
+    CUDA_OK(cudaMemsetAsync(d.x, 0, sizeof(double) * (size_t)d.n, st));
+    cycle<double>(opt_.cycleType, 0, st);
+    dev::copy_d(d.n, d.x, z, st);
+  }
+}
+
+double AmgHierarchy::fineSweepBytes() const {
+  // one pass over every row of level 0: b, diag, x (read+write) per row,
+  // col + val per stored entry
+  const DevLevel& d = lv_[0];
+  const double vb = opt_.precision == kMixed ? 4.0 : 8.0;
+  return d.n * (4.0 * vb) + d.entries * (4.0 + vb);
+}
+
+double AmgHierarchy::cycleBytes() const {
+  const double vb = opt_.precision == kMixed ? 4.0 : 8.0;
+  double total = 0;
+  const int L = (int)lv_.size();
+  const int passesPerSweep = opt_.smootherType == kGaussSeidel ? 2 : 2;
+  for (int l = 0; l < L; l++) {
+    const DevLevel& d = lv_[l];
+    const double pass = d.n * (4.0 * vb) + d.entries * (4.0 + vb);
+    const int sweeps = (l == L - 1) ? opt_.nPreSweeps + opt_.nPostSweeps
+                                    : opt_.nPreSweeps + opt_.nPostSweeps;
+    if (l == L - 1 && coarseInv_) {
+      total += (double)d.n * d.n * 8.0;
+      continue;
+    }
+    total += sweeps * passesPerSweep * pass;
+    if (l + 1 < L) {
+      const DevLevel& c = lv_[l + 1];
+      // fused residual+restriction reads the matrix once, writes coarse b
+      total += d.n * (3.0 * vb + 8.0) + d.entries * (4.0 + vb) + c.n * (vb + 4.0);
+      // zero coarse x, prolongation
+      total += c.n * vb + d.n * (2.0 * vb + 4.0);
+    }
+  }
+  return total;
+}
+
+int AmgHierarchy::kernelsPerCycle() const {
+  int k = 0;
+  const int L = (int)lv_.size();
+  for (int l = 0; l < L; l++) {
+    const DevLevel& d = lv_[l];
+    if (l == L - 1 && coarseInv_) {
+      k += 1;
+      continue;
+    }
+    const int perSweep = opt_.smootherType == kGaussSeidel
+                             ? (opt_.ordering == kSequential ? 2 : 2 * d.nColors - 1)
+                             : 2;
+    k += perSweep * (opt_.nPreSweeps + opt_.nPostSweeps);
+    if (l + 1 < L) k += 3;
+  }
+  return k;
+}
+
+template void AmgHierarchy::cycle<double>(CycleType, int, cudaStream_t);
+template void AmgHierarchy::cycle<float>(CycleType, int, cudaStream_t);
+
+// ---------------------------------------------------------------------------
+namespace {
+enum Scal {
+  kRho = 0,
+  kRhoPrev,
+  kPtq,
+  kAlpha,
+  kBeta,
+  kNorm,
+  kOmega,
+  kRtv,
+  kTdotr,
+  kTdott,
+  kOmegaPrev,
+  kAlphaPrev,
+  kNumScal
+};
+constexpr int kWorkVectors = 9;
+}  // namespace
+
+LinearSolve::LinearSolve(AmgHierarchy& h) : h_(h), n_(h.level(0).n) {
+  CUDA_OK(cudaMalloc(&work_, sizeof(double) * (size_t)n_ * kWorkVectors));
+  CUDA_OK(cudaMalloc(&scal_, sizeof(double) * 32));
+  CUDA_OK(cudaMalloc(&partials_, sizeof(double) * (dev::vec_blocks(n_) + 1)));
+  CUDA_OK(cudaMallocHost(&hostScal_, sizeof(double) * 32));
+}
+
+LinearSolve::~LinearSolve() {
+  if (g1_) cudaGraphExecDestroy(g1_);
+  if (g2_) cudaGraphExecDestroy(g2_);
+  if (g3_) cudaGraphExecDestroy(g3_);
+  cudaFree(work_);
+  cudaFree(scal_);
+  cudaFree(partials_);
+  cudaFreeHost(hostScal_);
+}
+
+void LinearSolve::norm_into(const double* v, double* scalar, cudaStream_t st) {
+  dev::l1_partials(n_, v, partials_, st);
+  dev::sum_partials(dev::vec_blocks(n_), partials_, scalar, st);
+}
+
+void LinearSolve::dot_into(const double* a, const double* b, double* scalar, cudaStream_t st) {
+  dev::dot_partials(n_, a, b, partials_, st);
+  dev::sum_partials(dev::vec_blocks(n_), partials_, scalar, st);
+}
+
+double LinearSolve::fetch(const double* scalar, cudaStream_t st) {
+  CUDA_OK(cudaMemcpyAsync(hostScal_, scalar, sizeof(double), cudaMemcpyDeviceToHost, st));
+  CUDA_OK(cudaStreamSynchronize(st));
+  return hostScal_[0];
+}
+
+void LinearSolve::run(cudaGraphExec_t& exec, cudaStream_t st, const std::function<void()>& body) {
+  if (!h_.options().useGraphs) {
+    body();
+    return;
+  }
+  if (!exec) {
+    cudaGraph_t g;
+    CUDA_OK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    try {
+      body();
+    } catch (...) {
+      cudaStreamEndCapture(st, &g);
+      if (g) cudaGraphDestroy(g);
+      throw;
+    }
+    CUDA_OK(cudaStreamEndCapture(st, &g));
+    size_t nodes = 0;
+    cudaGraphGetNodes(g, nullptr, &nodes);
+    CUDA_OK(cudaGraphInstantiate(&exec, g, 0));
+    cudaGraphDestroy(g);
+    nodeCounts_[&exec] = (long long)nodes;
+  }
+  CUDA_OK(cudaGraphLaunch(exec, st));
+  launches += nodeCounts_[&exec];
+}
+
+SolveReport LinearSolve::solve(cudaStream_t st) {
+  switch (h_.options().solver) {
+    case kSolverCG:
+      return solveCG(st);
+    case kSolverBCGStab:
+      return solveBCGStab(st);
+    default:
+      return solveAMG(st);
+  }
+}
+
+static bool stop_test(double rn, double r0, const SolverOptions& o) {
+  return rn < o.absoluteTolerance || rn / r0 < o.relativeTolerance;
+}
+
+// AMG::solve (AMG.cpp:220-282): r0 = |b + A x|, then cycles until the L1
+// ratio drops below relTol. With mixed precision each cycle runs in FP32
+// on the FP64 residual and its correction is added in FP64 (iterative
+// refinement), so the stopping test is always on the FP64 residual.
+SolveReport LinearSolve::solveAMG(cudaStream_t st) {
+  const SolverOptions& o = h_.options();
+  DevLevel& d = h_.level(0);
+  SolveReport rep;
+  CUDA_OK(cudaMemsetAsync(d.x, 0, sizeof(double) * (size_t)n_, st));
+  dev::residual<double>(d.view64(), d.nSlices, d.x, d.b, d.r, d.partials, st);
+  dev::sum_partials(d.nPartials, d.partials, scal_ + kNorm, st);
+  launches += 3;
+  const double r0 = fetch(scal_ + kNorm, st);
+  rep.initialNorm = r0;
+  rep.finalNorm = r0;
+  rep.history.push_back(r0);
+  if (o.verbosity > 0) printf("0: %g\n", r0);
+  if (!std::isfinite(r0)) throw Error(kNaN, "initial residual is not finite");
+  if (r0 < o.absoluteTolerance) {
+    rep.converged = true;
+    return rep;
+  }
+  for (int i = 1; i < o.nMaxIterations; i++) {
+    run(g1_, st, [&] {
+      if (o.precision == kMixed) {
+        dev::convert_d2f(n_, d.r, d.bF, st);
+        CUDA_OK(cudaMemsetAsync(d.xF, 0, sizeof(float) * (size_t)n_, st));
+        h_.cycle<float>(o.cycleType, 0, st);
+        dev::add_f2d(n_, d.xF, d.x, st);
+      } else {
+        h_.cycle<double>(o.cycleType, 0, st);
+      }
+      dev::residual<double>(d.view64(), d.nSlices, d.x, d.b, d.r, d.partials, st);
+      dev::sum_partials(d.nPartials, d.partials, scal_ + kNorm, st);
+      CUDA_OK(cudaMemcpyAsync(hostScal_, scal_ + kNorm, sizeof(double), cudaMemcpyDeviceToHost, st));
+    });
+    CUDA_OK(cudaStreamSynchronize(st));
+    const double rn = hostScal_[0];
+    rep.iterations = i;
+    rep.finalNorm = rn;
+    rep.history.push_back(rn);
+    if (o.verbosity > 0) printf("%d: %g\n", i, rn);
+    if (!std::isfinite(rn)) throw Error(kNaN, "residual became non-finite");
+    if (stop_test(rn, r0, o)) {
+      rep.converged = true;
+      break;
+    }
+  }
+  return rep;
+}
+
+// CG::solve (CG.cpp:26-139) with the AMG cycle as preconditioner.
+SolveReport LinearSolve::solveCG(cudaStream_t st) {
+  const SolverOptions& o = h_.options();
+  DevLevel& d = h_.level(0);
+  double* X = work_;
+  double* R = work_ + (size_t)n_;
+  double* Z = work_ + 2 * (size_t)n_;
+  double* P = work_ + 3 * (size_t)n_;
+  double* Q = work_ + 4 * (size_t)n_;
+  double* B = work_ + 5 * (size_t)n_;
+  SolveReport rep;
+  CUDA_OK(cudaMemsetAsync(X, 0, sizeof(double) * (size_t)n_, st));
+  CUDA_OK(cudaMemsetAsync(P, 0, sizeof(double) * (size_t)n_, st));
+  dev::copy_d(n_, d.b, B, st);
+  dev::residual<double>(d.view64(), d.nSlices, X, B, R, nullptr, st);
+  norm_into(R, scal_ + kNorm, st);
+  {
+    const double inf = std::numeric_limits<double>::infinity();
+    CUDA_OK(cudaMemcpyAsync(scal_ + kRho, &inf, sizeof(double), cudaMemcpyHostToDevice, st));
+  }
+  const double r0 = fetch(scal_ + kNorm, st);
+  rep.initialNorm = r0;
+  rep.finalNorm = r0;
+  rep.history.push_back(r0);
+  if (o.verbosity > 0) printf("0: %g\n", r0);
+  if (!std::isfinite(r0)) throw Error(kNaN, "initial residual is not finite");
+  for (int i = 0; i < o.nMaxIterations; i++) {
+    run(g1_, st, [&] {
+      h_.apply(R, Z, st);
+      dev::copy_d(1, scal_ + kRho, scal_ + kRhoPrev, st);
+      dot_into(R, Z, scal_ + kRho, st);
+      dev::scalar_div(scal_ + kRho, scal_ + kRhoPrev, scal_ + kBeta, st);  // 0 on the first pass
+      dev::xpby_dev(n_, Z, scal_ + kBeta, P, st);
+      dev::spmv(d.view64(), d.nSlices, P, Q, st);
+      dot_into(P, Q, scal_ + kPtq, st);
+      dev::scalar_div(scal_ + kRho, scal_ + kPtq, scal_ + kAlpha, st);
+      dev::axpy_dev(n_, scal_ + kAlpha, -1.0, P, X, st);
+      dev::axpy_dev(n_, scal_ + kAlpha, -1.0, Q, R, st);
+      norm_into(R, scal_ + kNorm, st);
+      CUDA_OK(cudaMemcpyAsync(hostScal_, scal_ + kNorm, sizeof(double), cudaMemcpyDeviceToHost, st));
+    });
+    CUDA_OK(cudaStreamSynchronize(st));
+    const double rn = hostScal_[0];
+    rep.iterations = i + 1;
+    rep.finalNorm = rn;
+    rep.history.push_back(rn);
+    if (o.verbosity > 0) printf("%d: %g\n", i + 1, rn);
+    if (!std::isfinite(rn)) throw Error(kNaN, "residual became non-finite");
+    if (stop_test(rn, r0, o)) {
+      rep.converged = true;
+      break;
+    }
+  }
+  // restore the system: delta = X, b = original
+  dev::copy_d(n_, X, d.x, st);
+  dev::copy_d(n_, B, d.b, st);
+  CUDA_OK(cudaStreamSynchronize(st));
+  return rep;
+}
+
+// BCGStab::solve (BCGStab.cpp:27-170) with the AMG cycle as preconditioner.
+SolveReport LinearSolve::solveBCGStab(cudaStream_t st) {
+  const SolverOptions& o = h_.options();
+  DevLevel& d = h_.level(0);
+  double* X = work_;
+  double* R = work_ + (size_t)n_;
+  double* RT = work_ + 2 * (size_t)n_;
+  double* P = work_ + 3 * (size_t)n_;
+  double* PH = work_ + 4 * (size_t)n_;
+  double* V = work_ + 5 * (size_t)n_;
+  double* Tt = work_ + 6 * (size_t)n_;
+  double* B = work_ + 7 * (size_t)n_;
+  SolveReport rep;
+  CUDA_OK(cudaMemsetAsync(X, 0, sizeof(double) * (size_t)n_, st));
+  CUDA_OK(cudaMemsetAsync(P, 0, sizeof(double) * (size_t)n_, st));
+  CUDA_OK(cudaMemsetAsync(V, 0, sizeof(double) * (size_t)n_, st));
+  dev::copy_d(n_, d.b, B, st);
+  dev::residual<double>(d.view64(), d.nSlices, X, B, R, nullptr, st);
+  dev::copy_d(n_, R, RT, st);
+  norm_into(R, scal_ + kNorm, st);
+  {
+    // first pass: beta = (rho / inf) * (alpha / omega) = 0, so p = r
+    const double init[3] = {std::numeric_limits<double>::infinity(), 0.0, 1.0};
+    CUDA_OK(cudaMemcpyAsync(scal_ + kRho, &init[0], sizeof(double), cudaMemcpyHostToDevice, st));
+    CUDA_OK(cudaMemcpyAsync(scal_ + kAlpha, &init[1], sizeof(double), cudaMemcpyHostToDevice, st));
+    CUDA_OK(cudaMemcpyAsync(scal_ + kOmega, &init[2], sizeof(double), cudaMemcpyHostToDevice, st));
+  }
+  const double r0 = fetch(scal_ + kNorm, st);
+  rep.initialNorm = r0;
+  rep.finalNorm = r0;
+  rep.history.push_back(r0);
+  if (o.verbosity > 0) printf("0: %g\n", r0);
+  if (!std::isfinite(r0)) throw Error(kNaN, "initial residual is not finite");
+  for (int i = 0; i < o.nMaxIterations; i++) {
+    run(g1_, st, [&] {
+      dev::copy_d(1, scal_ + kRho, scal_ + kRhoPrev, st);
+      dot_into(R, RT, scal_ + kRho, st);
+      dev::scalar_ratio_product(scal_ + kRho, scal_ + kRhoPrev, scal_ + kAlpha, scal_ + kOmega,
+                                scal_ + kBeta, st);
+      dev::bicg_p_update(n_, R, V, scal_ + kOmega, scal_ + kBeta, P, st);
+      h_.apply(P, PH, st);
+      dev::spmv(d.view64(), d.nSlices, PH, V, st);
+      dot_into(RT, V, scal_ + kRtv, st);
+      dev::scalar_div(scal_ + kRho, scal_ + kRtv, scal_ + kAlpha, st);
+      dev::axpy_dev(n_, scal_ + kAlpha, -1.0, PH, X, st);
+      dev::axpy_dev(n_, scal_ + kAlpha, -1.0, V, R, st);
+      norm_into(R, scal_ + kNorm, st);
+      CUDA_OK(cudaMemcpyAsync(hostScal_, scal_ + kNorm, sizeof(double), cudaMemcpyDeviceToHost, st));
+    });
+    CUDA_OK(cudaStreamSynchronize(st));
+    double rn = hostScal_[0];
+    rep.iterations = i + 1;
+    if (!std::isfinite(rn)) throw Error(kNaN, "residual became non-finite");
+    if (rn < o.absoluteTolerance) {
+      rep.finalNorm = rn;
+      rep.history.push_back(rn);
+      rep.converged = true;
+      break;
+    }
+    run(g2_, st, [&] {
+      double* SH = PH;
+      h_.apply(R, SH, st);
+      dev::spmv(d.view64(), d.nSlices, SH, Tt, st);
+      dot_into(Tt, R, scal_ + kTdotr, st);
+      dot_into(Tt, Tt, scal_ + kTdott, st);
+      dev::scalar_div(scal_ + kTdotr, scal_ + kTdott, scal_ + kOmega, st);
+      dev::axpy_dev(n_, scal_ + kOmega, -1.0, SH, X, st);
+      dev::axpy_dev(n_, scal_ + kOmega, -1.0, Tt, R, st);
+      norm_into(R, scal_ + kNorm, st);
+      CUDA_OK(cudaMemcpyAsync(hostScal_, scal_ + kNorm, sizeof(double), cudaMemcpyDeviceToHost, st));
+    });
+    CUDA_OK(cudaStreamSynchronize(st));
+    rn = hostScal_[0];
+    rep.finalNorm = rn;
+    rep.history.push_back(rn);
+    if (o.verbosity > 0) printf("%d: %g\n", i + 1, rn);
+    if (!std::isfinite(rn)) throw Error(kNaN, "residual became non-finite");
+    if (stop_test(rn, r0, o)) {
+      rep.converged = true;
+      break;
+    }
+  }
+  dev::copy_d(n_, X, d.x, st);
+  dev::copy_d(n_, B, d.b, st);
+  CUDA_OK(cudaStreamSynchronize(st));
+  return rep;
+}
+
+}  // namespace fvm

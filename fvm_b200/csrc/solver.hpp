@@ -1,0 +1,171 @@
+// GPU AMG hierarchy and linear solvers (AMG standalone, CG and BiCGStab
+// with an AMG preconditioner), FP64 or with an FP32 V-cycle under FP64
+// iterative refinement. Mirrors the reference's LinearSolver / AMG / CG /
+// BCGStab semantics: delta form r = b + A x, L1 residual norms over self
+// rows, stop when |r| < absTol or |r|/|r0| < relTol.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <functional>
+#include <map>
+#include <memory>
+#include <vector>
+
+#include "amg_setup.hpp"
+#include "kernels.cuh"
+
+namespace fvm {
+
+enum CycleType { kVCycle = 0, kWCycle = 1, kFCycle = 2 };
+enum SmootherType { kGaussSeidel = 0, kJacobi = 1 };
+enum CoarseSolver { kCoarseSmooth = 0, kCoarseDirect = 1 };
+enum Precision { kFP64 = 0, kMixed = 1 };
+enum SolverKind { kSolverAMG = 0, kSolverCG = 1, kSolverBCGStab = 2 };
+
+struct SolverOptions {
+  SolverKind solver = kSolverAMG;
+  int nMaxIterations = 100;
+  double relativeTolerance = 1e-8;
+  double absoluteTolerance = 1e-16;
+  int verbosity = 0;
+  // AMG knobs (reference AMG.h:74-81 and defaults AMG.cpp:15-22)
+  int maxCoarseLevels = 30;
+  int nPreSweeps = 0;
+  int nPostSweeps = 1;
+  int coarseGroupSize = 2;
+  double weightRatioThreshold = 0.65;
+  CycleType cycleType = kVCycle;
+  SmootherType smootherType = kGaussSeidel;
+  bool scaleCorrections = true;  // only acts on symmetric systems (never flagged here)
+  // additions of this implementation
+  SmootherOrdering ordering = kMulticolor;
+  int coarsestSize = 0;
+  CoarseSolver coarseSolver = kCoarseSmooth;
+  Precision precision = kFP64;
+  bool useGraphs = true;
+};
+
+struct SolveReport {
+  double initialNorm = 0;
+  double finalNorm = 0;
+  int iterations = 0;
+  bool converged = false;
+  std::vector<double> history;  // L1 norm after each iteration (index 0 = initial)
+};
+
+// Device copy of one level.
+struct DevLevel {
+  int n = 0, nColors = 0, nSlices = 0, nCoarse = 0, maxWidth = 0;
+  std::vector<int> colorSliceStart;  // host copy, launch bounds
+  int *sliceRow = nullptr, *sliceRows = nullptr, *sliceOff = nullptr, *cols = nullptr;
+  int* rowSlice = nullptr;
+  double *vals = nullptr, *diag = nullptr;
+  float *valsF = nullptr, *diagF = nullptr;
+  int *ci = nullptr, *c2fRow = nullptr, *c2fCol = nullptr;
+  double *x = nullptr, *b = nullptr, *r = nullptr, *tmp = nullptr;
+  float *xF = nullptr, *bF = nullptr, *rF = nullptr, *tmpF = nullptr;
+  double* partials = nullptr;
+  int nPartials = 0;
+  dev::SellView<double> view64() const {
+    return {n, sliceRow, sliceRows, sliceOff, cols, vals, diag};
+  }
+  dev::SellView<float> view32() const {
+    return {n, sliceRow, sliceRows, sliceOff, cols, valsF, diagF};
+  }
+  size_t entries = 0;
+};
+
+// Bytes of device memory allocated through this class (for reporting).
+class DeviceArena {
+ public:
+  ~DeviceArena();
+  void* alloc(size_t bytes);
+  template <class T>
+  T* upload(const std::vector<T>& v) {
+    T* p = (T*)alloc(v.size() * sizeof(T));
+    if (!v.empty()) copy_h2d(p, v.data(), v.size() * sizeof(T));
+    return p;
+  }
+  void release();
+  size_t bytes() const { return bytes_; }
+
+ private:
+  void copy_h2d(void* d, const void* h, size_t n);
+  std::vector<void*> ptrs_;
+  size_t bytes_ = 0;
+};
+
+class AmgHierarchy {
+ public:
+  // levels[0] is the finest matrix in reference order; the hierarchy
+  // (reference-exact aggregation) is built, packed and uploaded.
+  void build(std::vector<RefLevel>& levels, int finestLocalSize, const SolverOptions& opt);
+  void release();
+
+  int numLevels() const { return (int)lv_.size(); }
+  const DevLevel& level(int l) const { return lv_[l]; }
+  DevLevel& level(int l) { return lv_[l]; }
+  const PackedLevel& packed(int l) const { return packed_[l]; }
+  const std::vector<RefLevel>& refLevels() const { return ref_; }
+  std::vector<int> sizes() const;
+
+  // one cycle on level l of precision T (x, b of each level as stored)
+  template <class T>
+  void cycle(CycleType t, int l, cudaStream_t st);
+  template <class T>
+  void sweeps(int nSweeps, int l, cudaStream_t st);
+
+  // x = z <- M^-1 applied to r (FP64 in/out; runs the cycle in the
+  // configured precision): b0 <- r, x0 <- 0, cycle, z <- x0
+  void apply(const double* r, double* z, cudaStream_t st);
+
+  const SolverOptions& options() const { return opt_; }
+
+  size_t deviceBytes() const { return arena_.bytes(); }
+  // algorithmic bytes moved by one cycle (for roofline reporting)
+  double cycleBytes() const;
+  double fineSweepBytes() const;  // one GS pass over all colours of level 0
+  int kernelsPerCycle() const;
+
+ private:
+  SolverOptions opt_;
+  std::vector<RefLevel> ref_;
+  std::vector<PackedLevel> packed_;
+  std::vector<DevLevel> lv_;
+  double* coarseInv_ = nullptr;  // dense inverse of the coarsest level
+  DeviceArena arena_;
+};
+
+// Linear solve of the finest system held by the hierarchy: level 0's b is
+// the right-hand side, level 0's x the delta (zeroed on entry).
+class LinearSolve {
+ public:
+  explicit LinearSolve(AmgHierarchy& h);
+  ~LinearSolve();
+  SolveReport solve(cudaStream_t st);
+
+ private:
+  SolveReport solveAMG(cudaStream_t st);
+  SolveReport solveCG(cudaStream_t st);
+  SolveReport solveBCGStab(cudaStream_t st);
+  void norm_into(const double* v, double* scalar, cudaStream_t st);
+  void dot_into(const double* a, const double* b, double* scalar, cudaStream_t st);
+  double fetch(const double* scalar, cudaStream_t st);
+  // Runs body on st; with graphs enabled the first call captures it and
+  // later calls replay the instantiated graph.
+  void run(cudaGraphExec_t& exec, cudaStream_t st, const std::function<void()>& body);
+  AmgHierarchy& h_;
+  int n_;
+  double* work_ = nullptr;    // vectors
+  double* scal_ = nullptr;    // device scalars
+  double* partials_ = nullptr;
+  double* hostScal_ = nullptr;  // pinned
+  cudaGraphExec_t g1_ = nullptr, g2_ = nullptr, g3_ = nullptr;
+  std::map<const void*, long long> nodeCounts_;
+
+ public:
+  long long launches = 0;  // kernels + copies enqueued (graph nodes counted per replay)
+};
+
+}  // namespace fvm

@@ -1,0 +1,416 @@
+// ThermalModel on the GPU.
+#include "thermal.hpp"
+
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+
+namespace fvm {
+
+#define CUDA_OK(call)                                                                       \
+  do {                                                                                      \
+    cudaError_t e_ = (call);                                                                \
+    if (e_ != cudaSuccess)                                                                  \
+      throw ::fvm::Error(::fvm::kDeviceError, std::string(#call ": ") + cudaGetErrorString(e_)); \
+  } while (0)
+
+ThermalModel::ThermalModel(std::shared_ptr<HostMesh> mesh) : mesh_(std::move(mesh)) {
+  // ThermalModel_impl.h:41-82: wall/symmetry -> SpecifiedHeatFlux,
+  // velocity-inlet/pressure-outlet -> SpecifiedTemperature
+  for (size_t g = 1; g < mesh_->groups.size(); g++) {
+    const FaceGroup& fg = mesh_->groups[g];
+    GroupBC bc;
+    bc.id = fg.id;
+    if (fg.type == "wall" || fg.type == "symmetry")
+      bc.type = kBcSpecifiedHeatFlux;
+    else if (fg.type == "velocity-inlet" || fg.type == "pressure-outlet")
+      bc.type = kBcSpecifiedTemperature;
+    else
+      throw Error(kBadArgument, "ThermalModel: unknown face group type " + fg.type);
+    bcs_.push_back(bc);
+  }
+}
+
+ThermalModel::~ThermalModel() {
+  solver_.reset();
+  hier_.release();
+  freeDevice();
+}
+
+void ThermalModel::freeDevice() {
+  arena_.release();
+  if (dPerm_) cudaFree(dPerm_);
+  dPerm_ = nullptr;
+  if (stream_) cudaStreamDestroy(stream_);
+  stream_ = nullptr;
+  deviceReady_ = false;
+}
+
+GroupBC& ThermalModel::bc(int groupId) {
+  for (GroupBC& b : bcs_)
+    if (b.id == groupId) return b;
+  throw Error(kBadArgument, "no boundary face group with id " + std::to_string(groupId));
+}
+
+void ThermalModel::init() {
+  const int nAll = mesh_->nTotalCells();
+  T_.assign(nAll, opt_.initialTemperature);
+  k_.assign(nAll, opt_.thermalConductivity);
+  src_.assign(nAll, 0.0);
+  rc_.assign(nAll, opt_.density * opt_.specificHeat);
+  TN1_ = T_;
+  tDirty_ = kDirty_ = srcDirty_ = rcDirty_ = tn1Dirty_ = true;
+  matrixDirty_ = hierarchyDirty_ = true;
+  initialNorm_ = -1;
+  niters_ = 0;
+  history_.clear();
+  initialized_ = true;
+}
+
+static std::vector<double>& field_ref(int field, std::vector<double>& T, std::vector<double>& k,
+                                      std::vector<double>& s, std::vector<double>& rc,
+                                      std::vector<double>& tn1) {
+  switch (field) {
+    case kFieldTemperature:
+      return T;
+    case kFieldConductivity:
+      return k;
+    case kFieldSource:
+      return s;
+    case kFieldSpecificHeat:
+      return rc;
+    case kFieldTemperatureN1:
+      return tn1;
+  }
+  throw Error(kBadArgument, "unknown cell field");
+}
+
+void ThermalModel::setCellField(int field, const double* values, int count) {
+  FVM_REQUIRE(initialized_, kBadArgument, "ThermalModel.init() must be called before setting fields");
+  const int n = mesh_->nCells, nAll = mesh_->nTotalCells();
+  FVM_REQUIRE(count == nAll || count == n, kBadArgument,
+              "cell field length must be nCells or nCells + ghost cells");
+  if (field == kFieldTemperature && deviceReady_ && !tDirty_) {
+    // keep ghost values the device already holds when only self cells are given
+    CUDA_OK(cudaMemcpy(T_.data(), dT_, sizeof(double) * nAll, cudaMemcpyDeviceToHost));
+  }
+  std::vector<double>& f = field_ref(field, T_, k_, src_, rc_, TN1_);
+  std::copy(values, values + count, f.begin());
+  if (count == n && field != kFieldTemperature) {
+    // ghost cells take the value of their interior neighbour
+    const HostMesh& m = *mesh_;
+    for (size_t g = 1; g < m.groups.size(); g++)
+      for (int fc = m.groups[g].offset; fc < m.groups[g].offset + m.groups[g].size; fc++)
+        f[m.faceCells[2 * fc + 1]] = f[m.faceCells[2 * fc]];
+  }
+  switch (field) {
+    case kFieldTemperature:
+      tDirty_ = true;
+      break;
+    case kFieldConductivity:
+      kDirty_ = true;
+      matrixDirty_ = true;
+      break;
+    case kFieldSource:
+      srcDirty_ = true;
+      break;
+    case kFieldSpecificHeat:
+      rcDirty_ = true;
+      matrixDirty_ = true;
+      break;
+    case kFieldTemperatureN1:
+      tn1Dirty_ = true;
+      break;
+  }
+}
+
+void ThermalModel::getCellField(int field, double* out, int count) {
+  FVM_REQUIRE(initialized_, kBadArgument, "ThermalModel.init() must be called first");
+  const int nAll = mesh_->nTotalCells();
+  FVM_REQUIRE(count == nAll || count == mesh_->nCells, kBadArgument, "bad cell field length");
+  if (deviceReady_) {
+    if (field == kFieldTemperature && !tDirty_)
+      CUDA_OK(cudaMemcpy(T_.data(), dT_, sizeof(double) * nAll, cudaMemcpyDeviceToHost));
+    if (field == kFieldTemperatureN1 && !tn1Dirty_)
+      CUDA_OK(cudaMemcpy(TN1_.data(), dTN1_, sizeof(double) * nAll, cudaMemcpyDeviceToHost));
+  }
+  std::vector<double>& f = field_ref(field, T_, k_, src_, rc_, TN1_);
+  std::copy(f.begin(), f.begin() + count, out);
+}
+
+void ThermalModel::ensureDevice() {
+  if (deviceReady_) return;
+  HostMesh& m = *mesh_;
+  CUDA_OK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+  const int n = m.nCells, nAll = m.nTotalCells(), F = m.nFaces;
+  // boundary faces in face order and the per-cell lists
+  boundaryFaces_.clear();
+  std::vector<int> bIndexOfFace(F, -1);
+  for (size_t g = 1; g < m.groups.size(); g++)
+    for (int f = m.groups[g].offset; f < m.groups[g].offset + m.groups[g].size; f++) {
+      bIndexOfFace[f] = (int)boundaryFaces_.size();
+      boundaryFaces_.push_back(f);
+    }
+  std::vector<int> cfRow(n + 1), cfCol, bRow(n + 1, 0), bCol;
+  for (int i = 0; i < n; i++) {
+    cfRow[i] = (int)cfCol.size();
+    bRow[i] = (int)bCol.size();
+    for (int k = m.cellFaces.row[i]; k < m.cellFaces.row[i + 1]; k++) {
+      const int f = m.cellFaces.col[k];
+      cfCol.push_back(f);
+      if (bIndexOfFace[f] >= 0) bCol.push_back(f);
+    }
+  }
+  cfRow[n] = (int)cfCol.size();
+  bRow[n] = (int)bCol.size();
+  // self-row/self-column part of cellCells and the face behind each entry
+  std::vector<int> fullEntryFace(m.cellCells.nnz(), -1);
+  for (int f = 0; f < F; f++) {
+    fullEntryFace[m.pairToCol[2 * f]] = f;
+    fullEntryFace[m.pairToCol[2 * f + 1]] = f;
+  }
+  interiorConn_.nRows = n;
+  interiorConn_.row.assign(n + 1, 0);
+  interiorConn_.col.clear();
+  entryFace_.clear();
+  for (int i = 0; i < n; i++) {
+    for (int k = m.cellCells.row[i]; k < m.cellCells.row[i + 1]; k++) {
+      const int j = m.cellCells.col[k];
+      if (j < n) {
+        interiorConn_.col.push_back(j);
+        entryFace_.push_back(fullEntryFace[k]);
+      }
+    }
+    interiorConn_.row[i + 1] = (int)interiorConn_.col.size();
+  }
+  std::vector<int> ccRow(m.cellCells.row.begin(), m.cellCells.row.begin() + n + 1);
+  dFaceCells_ = arena_.upload(m.faceCells);
+  dCcRow_ = arena_.upload(ccRow);
+  dCcCol_ = arena_.upload(m.cellCells.col);
+  dGradW_ = arena_.upload(m.gradCoeff);
+  dArea_ = arena_.upload(m.faceArea);
+  dAreaMag_ = arena_.upload(m.faceAreaMag);
+  dCentroid_ = arena_.upload(m.cellCentroid);
+  dVol_ = arena_.upload(m.cellVolume);
+  dCfRow_ = arena_.upload(cfRow);
+  dCfCol_ = arena_.upload(cfCol);
+  dBRow_ = arena_.upload(bRow);
+  dBCol_ = arena_.upload(bCol);
+  dBFace_ = arena_.upload(boundaryFaces_);
+  dBIndexOfFace_ = arena_.upload(bIndexOfFace);
+  const int nB = (int)boundaryFaces_.size();
+  dBKind_ = (int*)arena_.alloc(sizeof(int) * (nB + 1));
+  dBValue_ = (double*)arena_.alloc(sizeof(double) * (nB + 1));
+  dBGhost_ = (double*)arena_.alloc(sizeof(double) * (nB + 1));
+  const size_t cb = sizeof(double) * (size_t)nAll;
+  dT_ = (double*)arena_.alloc(cb);
+  dK_ = (double*)arena_.alloc(cb);
+  dSrc_ = (double*)arena_.alloc(cb);
+  dRc_ = (double*)arena_.alloc(cb);
+  dTN1_ = (double*)arena_.alloc(cb);
+  dRhoVdt_ = (double*)arena_.alloc(cb);
+  dGrad_ = (double*)arena_.alloc(3 * cb);
+  dDiagOrig_ = (double*)arena_.alloc(cb);
+  dFlux_ = (double*)arena_.alloc(sizeof(double) * (size_t)F);
+  dCoeff_ = (double*)arena_.alloc(sizeof(double) * (size_t)F);
+  dSec_ = (double*)arena_.alloc(3 * sizeof(double) * (size_t)F);
+  CUDA_OK(cudaMemset(dGrad_, 0, 3 * cb));
+  deviceReady_ = true;
+  tDirty_ = kDirty_ = srcDirty_ = rcDirty_ = tn1Dirty_ = true;
+  matrixDirty_ = true;
+}
+
+void ThermalModel::uploadFields() {
+  const size_t cb = sizeof(double) * (size_t)mesh_->nTotalCells();
+  if (tDirty_) CUDA_OK(cudaMemcpyAsync(dT_, T_.data(), cb, cudaMemcpyHostToDevice, stream_));
+  if (kDirty_) CUDA_OK(cudaMemcpyAsync(dK_, k_.data(), cb, cudaMemcpyHostToDevice, stream_));
+  if (srcDirty_) CUDA_OK(cudaMemcpyAsync(dSrc_, src_.data(), cb, cudaMemcpyHostToDevice, stream_));
+  if (rcDirty_) CUDA_OK(cudaMemcpyAsync(dRc_, rc_.data(), cb, cudaMemcpyHostToDevice, stream_));
+  if (tn1Dirty_) CUDA_OK(cudaMemcpyAsync(dTN1_, TN1_.data(), cb, cudaMemcpyHostToDevice, stream_));
+  CUDA_OK(cudaStreamSynchronize(stream_));
+  tDirty_ = kDirty_ = srcDirty_ = rcDirty_ = tn1Dirty_ = false;
+  // boundary kinds and values (cheap; a change of kind changes the matrix)
+  const int nB = (int)boundaryFaces_.size();
+  std::vector<int> kind(nB + 1, 0);
+  std::vector<double> val(nB + 1, 0.0);
+  int t = 0;
+  for (size_t g = 1; g < mesh_->groups.size(); g++) {
+    const FaceGroup& fg = mesh_->groups[g];
+    const GroupBC& b = bc(fg.id);
+    int k;
+    double v;
+    switch (b.type) {
+      case kBcSpecifiedTemperature:
+        k = 0;
+        v = b.values[0];
+        break;
+      case kBcSpecifiedHeatFlux:
+        k = 1;
+        v = b.values[1];
+        break;
+      case kBcSymmetry:
+        k = 1;
+        v = 0.0;
+        break;
+      default:
+        throw Error(kUnsupported,
+                    "boundary condition type not available on the GPU path (Convective/Radiative/Mixed)");
+    }
+    for (int f = 0; f < fg.size; f++, t++) {
+      kind[t] = k;
+      val[t] = v;
+    }
+  }
+  CUDA_OK(cudaMemcpy(dBKind_, kind.data(), sizeof(int) * (nB + 1), cudaMemcpyHostToDevice));
+  CUDA_OK(cudaMemcpy(dBValue_, val.data(), sizeof(double) * (nB + 1), cudaMemcpyHostToDevice));
+  if (kind != bKindHost_) {
+    bKindHost_ = kind;
+    matrixDirty_ = true;
+  }
+}
+
+void ThermalModel::ensureMatrix() {
+  if (!matrixDirty_ && !hierarchyDirty_) return;
+  HostMesh& m = *mesh_;
+  const int n = m.nCells, F = m.nFaces;
+  dev::FaceGeom g{F, n, dFaceCells_, dArea_, dAreaMag_, dCentroid_, dVol_};
+  dev::face_coefficients(g, dK_, dCoeff_, dSec_, stream_);
+  const double* rhoVdt = nullptr;
+  if (opt_.transient) {
+    FVM_REQUIRE(opt_.timeDiscretizationOrder == 1, kUnsupported,
+                "only first-order time discretization is available on the GPU path");
+    dev::transient_coeff(n, dRc_, dVol_, opt_.timeStep, dRhoVdt_, stream_);
+    rhoVdt = dRhoVdt_;
+  }
+  dev::CellFaceView cf{dCfRow_, dCfCol_, dBRow_, dBCol_};
+  dev::BoundaryData bd{(int)boundaryFaces_.size(), dBFace_, dBKind_, dBValue_};
+  dev::assemble_matrix(n, cf, dFaceCells_, dCoeff_, rhoVdt, bd, dBIndexOfFace_, dDiagOrig_, stream_);
+  std::vector<double> coeff(F), diag(n);
+  CUDA_OK(cudaMemcpyAsync(coeff.data(), dCoeff_, sizeof(double) * F, cudaMemcpyDeviceToHost, stream_));
+  CUDA_OK(cudaMemcpyAsync(diag.data(), dDiagOrig_, sizeof(double) * n, cudaMemcpyDeviceToHost, stream_));
+  CUDA_OK(cudaStreamSynchronize(stream_));
+  std::vector<RefLevel> levels(1);
+  RefLevel& l0 = levels[0];
+  l0.n = n;
+  l0.conn = interiorConn_;
+  l0.diag = std::move(diag);
+  l0.off.resize(entryFace_.size());
+  for (size_t e = 0; e < entryFace_.size(); e++) l0.off[e] = coeff[entryFace_[e]];
+  solver_.reset();
+  hier_.build(levels, m.nTotalCells(), opt_.linear);
+  if (dPerm_) cudaFree(dPerm_);
+  dPerm_ = nullptr;
+  CUDA_OK(cudaMalloc(&dPerm_, sizeof(int) * (size_t)n));
+  CUDA_OK(cudaMemcpy(dPerm_, hier_.packed(0).perm.data(), sizeof(int) * (size_t)n,
+                     cudaMemcpyHostToDevice));
+  solver_.reset(new LinearSolve(hier_));
+  matrixDirty_ = hierarchyDirty_ = false;
+}
+
+void ThermalModel::linearize() {
+  HostMesh& m = *mesh_;
+  const int n = m.nCells, F = m.nFaces;
+  dev::gradient(n, dCcRow_, dCcCol_, dGradW_, dT_, dGrad_, stream_);
+  dev::ghost_gradient((int)boundaryFaces_.size(), dBFace_, dFaceCells_, dGrad_, stream_);
+  dev::FaceGeom g{F, n, dFaceCells_, dArea_, dAreaMag_, dCentroid_, dVol_};
+  dev::face_flux(g, dCoeff_, dSec_, dGrad_, dT_, dFlux_, stream_);
+  dev::CellFaceView cf{dCfRow_, dCfCol_, dBRow_, dBCol_};
+  dev::BoundaryData bd{(int)boundaryFaces_.size(), dBFace_, dBKind_, dBValue_};
+  dev::assemble_rhs(n, cf, dFaceCells_, dFlux_, dCoeff_, dAreaMag_, dVol_, dSrc_,
+                    opt_.transient ? dRhoVdt_ : nullptr, dTN1_, bd, dBIndexOfFace_, dT_, dBGhost_,
+                    dPerm_, hier_.level(0).b, stream_);
+}
+
+void ThermalModel::advance(int niter, AdvanceReport& rep) {
+  FVM_REQUIRE(initialized_, kBadArgument, "ThermalModel.init() must be called before advance()");
+  rep = AdvanceReport();
+  ensureDevice();
+  cudaEvent_t e0, e1, e2;
+  CUDA_OK(cudaEventCreate(&e0));
+  CUDA_OK(cudaEventCreate(&e1));
+  CUDA_OK(cudaEventCreate(&e2));
+  CUDA_OK(cudaEventRecord(e0, stream_));
+  uploadFields();
+  const auto s0 = std::chrono::steady_clock::now();
+  ensureMatrix();
+  const auto s1 = std::chrono::steady_clock::now();
+  rep.setupSeconds = std::chrono::duration<double>(s1 - s0).count();
+  CUDA_OK(cudaEventRecord(e1, stream_));
+  const long long launches0 = solver_->launches;
+  HostMesh& m = *mesh_;
+  dev::BoundaryData bd{(int)boundaryFaces_.size(), dBFace_, dBKind_, dBValue_};
+  for (int it = 0; it < niter; it++) {
+    linearize();
+    rep.launches += 4;
+    SolveReport sr = solver_->solve(stream_);
+    const double rNorm = sr.initialNorm;
+    if (initialNorm_ < 0) initialNorm_ = rNorm;
+    dev::update_solution(m.nCells, dPerm_, hier_.level(0).x, bd, dFaceCells_, dCoeff_, dBGhost_, dT_,
+                         stream_);
+    rep.launches += 2;
+    niters_++;
+    history_.push_back(rNorm);
+    rep.iterations++;
+    rep.linearIterations += sr.iterations;
+    rep.lastNorm = rNorm;
+    if (opt_.linear.verbosity >= 0 && opt_.linear.verbosity > 0) printf("%d: %g\n", niters_ - 1, rNorm);
+    const double ratio = initialNorm_ > 0 ? rNorm / initialNorm_ : 0.0;
+    if (rNorm < opt_.absoluteTolerance || ratio < opt_.relativeTolerance) {
+      rep.converged = true;
+      break;
+    }
+  }
+  CUDA_OK(cudaEventRecord(e2, stream_));
+  CUDA_OK(cudaEventSynchronize(e2));
+  float ms = 0;
+  CUDA_OK(cudaEventElapsedTime(&ms, e0, e2));
+  rep.seconds = ms * 1e-3;
+  rep.initialNorm = initialNorm_;
+  rep.launches += solver_->launches - launches0;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaEventDestroy(e2);
+  CUDA_OK(cudaGetLastError());
+}
+
+void ThermalModel::updateTime() {
+  FVM_REQUIRE(initialized_, kBadArgument, "ThermalModel.init() must be called first");
+  if (!deviceReady_ || tDirty_) {
+    TN1_ = T_;
+    tn1Dirty_ = true;
+    return;
+  }
+  CUDA_OK(cudaMemcpyAsync(dTN1_, dT_, sizeof(double) * (size_t)mesh_->nTotalCells(),
+                          cudaMemcpyDeviceToDevice, stream_));
+  CUDA_OK(cudaStreamSynchronize(stream_));
+  tn1Dirty_ = false;
+}
+
+void ThermalModel::linearizeOnly(std::vector<double>& diag, std::vector<double>& off,
+                                 std::vector<double>& b) {
+  FVM_REQUIRE(initialized_, kBadArgument, "ThermalModel.init() must be called first");
+  ensureDevice();
+  uploadFields();
+  ensureMatrix();
+  linearize();
+  const int n = mesh_->nCells;
+  std::vector<double> bp(n);
+  CUDA_OK(cudaMemcpyAsync(bp.data(), hier_.level(0).b, sizeof(double) * n, cudaMemcpyDeviceToHost,
+                          stream_));
+  CUDA_OK(cudaStreamSynchronize(stream_));
+  const PackedLevel& p0 = hier_.packed(0);
+  b.resize(n);
+  for (int i = 0; i < n; i++) b[i] = bp[p0.perm[i]];
+  diag = hier_.refLevels()[0].diag;
+  off = hier_.refLevels()[0].off;
+}
+
+const AmgHierarchy& ThermalModel::hierarchy() {
+  FVM_REQUIRE(initialized_, kBadArgument, "ThermalModel.init() must be called first");
+  ensureDevice();
+  uploadFields();
+  ensureMatrix();
+  return hier_;
+}
+
+}  // namespace fvm

@@ -1,0 +1,137 @@
+// ThermalModel<double> on the GPU: the reference's init / advance /
+// updateTime semantics (ThermalModel_impl.h:84-173, 424-456, 472-495) with
+// the linearization and the linear solve running as sm_100a kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <array>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "mesh.hpp"
+#include "solver.hpp"
+
+namespace fvm {
+
+enum BcType {
+  kBcSpecifiedTemperature = 0,
+  kBcSpecifiedHeatFlux = 1,
+  kBcSymmetry = 2,
+  kBcConvective = 3,
+  kBcRadiative = 4,
+  kBcMixed = 5,
+};
+
+enum CellField {
+  kFieldTemperature = 0,
+  kFieldConductivity = 1,
+  kFieldSource = 2,
+  kFieldSpecificHeat = 3,  // rho * cp
+  kFieldTemperatureN1 = 4,
+};
+
+struct ThermalOptions {
+  double relativeTolerance = 1e-8;   // ThermalBC.h:42
+  double absoluteTolerance = 1e-16;
+  bool transient = false;
+  int timeDiscretizationOrder = 1;
+  double initialTemperature = 300.0;
+  double timeStep = 1e-7;
+  // volume-condition constants (ThermalVC)
+  double thermalConductivity = 1.0;
+  double density = 1.0;
+  double specificHeat = 1.0;
+  SolverOptions linear;
+  ThermalOptions() {
+    // ThermalModelOptions::getLinearSolver default: AMG, relTol 0.1, 20 iterations
+    linear.relativeTolerance = 1e-1;
+    linear.nMaxIterations = 20;
+  }
+};
+
+struct GroupBC {
+  int id = 0;
+  BcType type = kBcSpecifiedHeatFlux;
+  // specifiedTemperature, specifiedHeatFlux, convectiveCoefficient,
+  // farFieldTemperature, surfaceEmissivity (ThermalBC defaults)
+  std::array<double, 5> values{{300.0, 0.0, 0.0, 300.0, 1.0}};
+};
+
+struct AdvanceReport {
+  int iterations = 0;
+  int linearIterations = 0;
+  double initialNorm = 0;  // of the model's first linear system
+  double lastNorm = 0;
+  bool converged = false;
+  double seconds = 0;      // device time (CUDA events) of the advance call
+  double setupSeconds = 0; // part spent rebuilding matrix + hierarchy
+  long long launches = 0;
+};
+
+class ThermalModel {
+ public:
+  explicit ThermalModel(std::shared_ptr<HostMesh> mesh);
+  ~ThermalModel();
+
+  HostMesh& mesh() { return *mesh_; }
+  std::vector<GroupBC>& bcs() { return bcs_; }
+  GroupBC& bc(int groupId);
+  ThermalOptions& options() { return opt_; }
+  void optionsChanged() { matrixDirty_ = true; hierarchyDirty_ = true; }
+  void bcChanged() { matrixDirty_ = true; hierarchyDirty_ = true; }
+
+  void init();
+  void setCellField(int field, const double* values, int count);
+  void getCellField(int field, double* out, int count);
+  void advance(int niter, AdvanceReport& rep);
+  void updateTime();
+
+  // parity hooks: the current linearization (matrix in reference order and
+  // rhs) and the AMG hierarchy built from it
+  void linearizeOnly(std::vector<double>& diag, std::vector<double>& off,
+                     std::vector<double>& b);
+  const AmgHierarchy& hierarchy();
+  const std::vector<double>& history() const { return history_; }
+  cudaStream_t stream() const { return stream_; }
+
+ private:
+  void ensureDevice();
+  void uploadFields();
+  void ensureMatrix();
+  void linearize();
+  void freeDevice();
+
+  std::shared_ptr<HostMesh> mesh_;
+  std::vector<GroupBC> bcs_;
+  ThermalOptions opt_;
+  bool initialized_ = false;
+  // host fields, self + ghost cells
+  std::vector<double> T_, k_, src_, rc_, TN1_;
+  bool tDirty_ = true, kDirty_ = true, srcDirty_ = true, rcDirty_ = true, tn1Dirty_ = true;
+  bool matrixDirty_ = true, hierarchyDirty_ = true;
+  double initialNorm_ = -1;
+  int niters_ = 0;
+  std::vector<double> history_;
+
+  // device state
+  cudaStream_t stream_ = nullptr;
+  bool deviceReady_ = false;
+  DeviceArena arena_;
+  int *dFaceCells_ = nullptr, *dCcRow_ = nullptr, *dCcCol_ = nullptr;
+  int *dCfRow_ = nullptr, *dCfCol_ = nullptr, *dBRow_ = nullptr, *dBCol_ = nullptr;
+  int *dBFace_ = nullptr, *dBKind_ = nullptr, *dBIndexOfFace_ = nullptr, *dPerm_ = nullptr;
+  double *dArea_ = nullptr, *dAreaMag_ = nullptr, *dCentroid_ = nullptr, *dVol_ = nullptr;
+  double *dGradW_ = nullptr, *dGrad_ = nullptr, *dFlux_ = nullptr, *dCoeff_ = nullptr, *dSec_ = nullptr;
+  double *dT_ = nullptr, *dK_ = nullptr, *dSrc_ = nullptr, *dRc_ = nullptr, *dTN1_ = nullptr;
+  double *dRhoVdt_ = nullptr, *dBValue_ = nullptr, *dBGhost_ = nullptr, *dDiagOrig_ = nullptr;
+  std::vector<int> boundaryFaces_;       // boundary faces in face order
+  std::vector<int> bKindHost_;           // boundary kinds last uploaded
+  std::vector<int> entryFace_;           // interior-only CSR entry -> face
+  CSR interiorConn_;                     // cellCells restricted to self rows / self columns
+  AmgHierarchy hier_;
+  std::unique_ptr<LinearSolve> solver_;
+};
+
+}  // namespace fvm

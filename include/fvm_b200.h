@@ -1,0 +1,187 @@
+/*
+ * fvm_b200: B200-native replacement for the FVM thermal diffusion + AMG
+ * hot path. Plain C ABI: opaque handles, plain pointers and sizes, int
+ * status codes (0 = success); the message of the last failure on the
+ * calling thread is returned by fvm_last_error().
+ *
+ * Each entry point names the reference interface it replaces (paths are
+ * inside the c-PRIMED/fvm project, src/fvm/src/modules/...).
+ *
+ * Ownership: input arrays are copied; the library owns device memory;
+ * handles are released with the matching *_destroy call.
+ * Threading: calls on one handle must be serialised; distinct handles may
+ * be used from different threads (each thermal model has its own CUDA
+ * stream on the device current at its first advance).
+ */
+#ifndef FVM_B200_H
+#define FVM_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define FVM_OK 0
+#define FVM_ERR_BAD_ARGUMENT 1
+#define FVM_ERR_BAD_MESH 2
+#define FVM_ERR_NOT_CONVERGED 3
+#define FVM_ERR_NAN 4
+#define FVM_ERR_DEVICE 5
+#define FVM_ERR_LEARNED_REJECTED 6
+#define FVM_ERR_UNSUPPORTED 7
+#define FVM_ERR_TOO_LARGE 8
+
+/* boundary condition types (ThermalBC::bcType strings, fvmbase/ThermalModel_impl.h:299-383) */
+#define FVM_BC_SPECIFIED_TEMPERATURE 0
+#define FVM_BC_SPECIFIED_HEAT_FLUX 1
+#define FVM_BC_SYMMETRY 2
+#define FVM_BC_CONVECTIVE 3
+#define FVM_BC_RADIATIVE 4
+#define FVM_BC_MIXED 5
+
+/* cell fields (ThermalFields, fvmbase/ThermalFields.h) */
+#define FVM_FIELD_TEMPERATURE 0
+#define FVM_FIELD_CONDUCTIVITY 1
+#define FVM_FIELD_SOURCE 2
+#define FVM_FIELD_SPECIFIC_HEAT 3 /* density * specific heat */
+#define FVM_FIELD_TEMPERATURE_N1 4
+
+typedef struct fvm_mesh fvm_mesh;
+typedef struct fvm_thermal fvm_thermal;
+
+/* Linear solver settings: LinearSolver fields (fvmbase/LinearSolver.h:19-24)
+ * and AMG knobs (fvmbase/AMG.h:74-81), plus this implementation's own. */
+typedef struct fvm_linear_options {
+  int solver;               /* 0 AMG, 1 CG with AMG preconditioner, 2 BCGStab with AMG */
+  int nMaxIterations;
+  double relativeTolerance;
+  double absoluteTolerance;
+  int verbosity;
+  int maxCoarseLevels;
+  int nPreSweeps;
+  int nPostSweeps;
+  int coarseGroupSize;
+  double weightRatioThreshold;
+  int cycleType;            /* 0 V, 1 W, 2 F */
+  int smootherType;         /* 0 Gauss-Seidel, 1 Jacobi */
+  int scaleCorrections;
+  /* additions */
+  int smootherOrdering;     /* 0 multicolour (parallel), 1 sequential (reference order, parity runs) */
+  int coarsestSize;         /* stop coarsening at this many rows (0: reference rule) */
+  int coarseSolver;         /* 0 smooth only (reference), 1 dense FP64 direct solve */
+  int precision;            /* 0 FP64, 1 FP32 V-cycle under FP64 refinement */
+  int useGraphs;            /* replay each iteration as a CUDA graph */
+} fvm_linear_options;
+
+/* ThermalModelOptions (fvmbase/ThermalBC.h:33-67) + volume-condition constants */
+typedef struct fvm_thermal_options {
+  double relativeTolerance;
+  double absoluteTolerance;
+  int transient;
+  int timeDiscretizationOrder;
+  double initialTemperature;
+  double timeStep;
+  double thermalConductivity;
+  double density;
+  double specificHeat;
+  fvm_linear_options linear;
+} fvm_thermal_options;
+
+typedef struct fvm_report {
+  int iterations;          /* outer (advance) iterations, or solver iterations */
+  int linearIterations;    /* total inner iterations */
+  double initialNorm;      /* L1 norm of the first linear system */
+  double lastNorm;         /* L1 norm of the last linear system / final residual */
+  int converged;
+  double seconds;          /* device time, CUDA events around the call */
+  double setupSeconds;     /* host+device time rebuilding matrix and AMG levels */
+  long long launches;      /* kernels and copies issued (graph nodes counted per replay) */
+} fvm_report;
+
+/* Reference AMG defaults (fvmbase/AMG.cpp:15-22) and LinearSolver defaults. */
+void fvm_default_linear_options(fvm_linear_options* o);
+/* ThermalModelOptions defaults; linear = AMG with relTol 0.1, 20 iterations
+ * (ThermalModelOptions::getLinearSolver, fvmbase/ThermalBC.h:56-67). */
+void fvm_default_thermal_options(fvm_thermal_options* o);
+
+/* Mesh(dimension, nCells, nodes, faceCells, faceNodes, faceNodeCount,
+ * faceGroupSize) -- fvmbase/Mesh.cpp:132-247, Python fvmbaseExt.Mesh
+ * (fvmbase/Mesh.i:95-120). xyz: 3*nNodes; faceCells: 2*nFaces; faceNodes:
+ * all face nodes back to back; groupSize[0] = interior faces, then one
+ * entry per boundary group (ids 1..k, type "wall"). */
+int fvm_mesh_create(int dim, int nCells, int nNodes, const double* xyz, int nFaces,
+                    const int* faceCells, const int* faceNodes, const int* faceNodeCount,
+                    int nGroups, const int* groupSize, fvm_mesh** out);
+/* FaceGroup id/type of group g (g >= 1), as imported meshes carry them
+ * (fvmbase/Mesh.h FaceGroup). */
+int fvm_mesh_set_group(fvm_mesh* m, int group, int id, const char* type);
+/* out: dim, nCells, nGhost, nNodes, nFaces, nnz(cellCells), nGroups */
+int fvm_mesh_sizes(const fvm_mesh* m, int* out7);
+/* Mesh::getCellCells + CRConnectivity::getPairToColMapping
+ * (fvmbase/Mesh.cpp:479-492, fvmbase/CRConnectivity.cpp:730-790). */
+int fvm_mesh_connectivity(const fvm_mesh* m, int* row, int* col, int* pairToCol);
+/* MeshMetricsCalculator<double>::init (fvmbase/MeshMetricsCalculator_impl.h:1944-2042) */
+int fvm_mesh_geometry(const fvm_mesh* m, double* faceArea, double* faceAreaMag,
+                      double* faceCentroid, double* cellCentroid, double* cellVolume);
+int fvm_mesh_destroy(fvm_mesh* m);
+
+/* ThermalModel<double>(geomFields, thermalFields, meshes)
+ * (fvmbase/ThermalModel.h:28-52). One mesh per model. */
+int fvm_thermal_create(fvm_mesh* const* meshes, int nMesh, fvm_thermal** out);
+int fvm_thermal_set_options(fvm_thermal* t, const fvm_thermal_options* o);
+int fvm_thermal_get_options(const fvm_thermal* t, fvm_thermal_options* o);
+/* getBCMap()[groupId]: bcType + FloatVarDict values [specifiedTemperature,
+ * specifiedHeatFlux, convectiveCoefficient, farFieldTemperature,
+ * surfaceEmissivity] (fvmbase/ThermalBC.h:8-20). values may be null. */
+int fvm_thermal_set_bc(fvm_thermal* t, int mesh, int groupId, int bcType, const double* values5);
+int fvm_thermal_get_bc(const fvm_thermal* t, int mesh, int groupId, int* bcType, double* values5);
+/* ThermalModel::init (fvmbase/ThermalModel_impl.h:84-173) */
+int fvm_thermal_init(fvm_thermal* t);
+/* thermalFields.<field>[cells] arrays; count = nCells (ghosts take their
+ * neighbour's value, temperature ghosts are kept) or nCells + nGhost. */
+int fvm_thermal_set_cell_field(fvm_thermal* t, int mesh, int field, const double* values, int count);
+int fvm_thermal_get_cell_field(fvm_thermal* t, int mesh, int field, double* out, int count);
+/* ThermalModel::advance (fvmbase/ThermalModel_impl.h:424-456) */
+int fvm_thermal_advance(fvm_thermal* t, int niter, fvm_report* rep);
+/* ThermalModel::updateTime (fvmbase/ThermalModel_impl.h:472-495) */
+int fvm_thermal_update_time(fvm_thermal* t);
+/* outer L1 norms printed by advance(), one per iteration since init() */
+int fvm_thermal_history(const fvm_thermal* t, double* norms, int cap, int* n);
+/* The linearization advance() solves (ThermalModel::dumpMatrix content,
+ * fvmbase/ThermalModel_impl.h:499-572): diag[nCells], off[nnz of the
+ * self-row/self-column cellCells pattern in reference order], b[nCells]
+ * in delta form (b = -rhs of the dump). */
+int fvm_thermal_linear_system(fvm_thermal* t, double* diag, double* off, double* b, int* nnz);
+/* The AMG hierarchy of the current linearization (LinearSystem::createCoarse
+ * per level, fvmbase/LinearSystem.cpp:67-248): number of coarse levels,
+ * their sizes, and the coarseIndex of each fine level concatenated. */
+int fvm_thermal_hierarchy(fvm_thermal* t, int* nLevels, int* sizes, int sizesCap,
+                          int* coarseIndex, int ciCap);
+int fvm_thermal_destroy(fvm_thermal* t);
+
+/* Raw system path (testLinearSolver / MMReader + AMG::solve,
+ * src/modules/importers/testLinearSolver.cpp): solves b + A x = 0 for x
+ * from x = 0, A given with implicit diagonal (row, col over n rows, diag,
+ * off). history receives the L1 norm after each iteration (index 0 =
+ * initial), levelSizes the coarse level sizes. */
+int fvm_amg_solve_csr(int n, const int* row, const int* col, const double* diag,
+                      const double* off, const double* b, double* x,
+                      const fvm_linear_options* o, fvm_report* rep, double* history,
+                      int historyCap, int* nHistory, int* levelSizes, int levelCap,
+                      int* nLevels);
+/* Host-only AMG setup of the same system (no device needed): coarse sizes
+ * and concatenated coarseIndex arrays (CRMatrix::createCoarsening,
+ * fvmbase/CRMatrix.h:468-586), plus, when colors != null, the greedy
+ * colour of every row of every level (concatenated). */
+int fvm_amg_hierarchy_csr(int n, const int* row, const int* col, const double* diag,
+                          const double* off, const fvm_linear_options* o, int finestLocalSize,
+                          int* nLevels, int* sizes, int sizesCap, int* coarseIndex, int ciCap,
+                          int* colors, int colorsCap);
+
+const char* fvm_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FVM_B200_H */

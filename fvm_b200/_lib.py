@@ -100,6 +100,7 @@ _SIGS = {
     "fvm_thermal_linear_system": (ctypes.c_int, [ctypes.c_void_p, c_double_p, c_double_p, c_double_p, c_int_p]),
     "fvm_thermal_hierarchy": (ctypes.c_int, [ctypes.c_void_p, c_int_p, c_int_p, ctypes.c_int, c_int_p,
                                              ctypes.c_int]),
+    "fvm_thermal_profile": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, c_double_p]),
     "fvm_thermal_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "fvm_amg_solve_csr": (ctypes.c_int, [ctypes.c_int, c_int_p, c_int_p, c_double_p, c_double_p, c_double_p,
                                          c_double_p, ctypes.POINTER(LinearOptions), ctypes.POINTER(Report),

@@ -387,6 +387,13 @@ int fvm_thermal_hierarchy(fvm_thermal* h, int* nLevels, int* sizes, int sizesCap
   });
 }
 
+int fvm_thermal_profile(fvm_thermal* h, int reps, double* out) {
+  return guarded([&] {
+    FVM_REQUIRE(h && out, kBadArgument, "null argument");
+    h->model->profile(reps, out);
+  });
+}
+
 int fvm_thermal_destroy(fvm_thermal* h) {
   delete h;
   return FVM_OK;

@@ -326,7 +326,7 @@ __global__ void k_assemble_rhs(int nCells, CellFaceView cf, const int* __restric
   // applyNeumannBC sets the ghost row's rhs; eliminateBoundaryEquations
   // then folds it into the interior row: b_i -= a_ij (b_j / a_jj)
   for (int k = cf.bRow[i]; k < cf.bRow[i + 1]; k++) {
-    const int f = cf.bCol[k];
+    const int f = cf.bColG[k];
     const int t = bIndexOfFace[f];
     if (bd.kind[t] == 1) {
       const double fluxB = -(0.0 - flux[f]);
@@ -348,7 +348,7 @@ __global__ void k_assemble_matrix(int nCells, CellFaceView cf, const int* __rest
   for (int k = cf.row[i]; k < cf.row[i + 1]; k++) d -= coeff[cf.col[k]];
   if (rhoVdt) d -= rhoVdt[i];
   for (int k = cf.bRow[i]; k < cf.bRow[i + 1]; k++) {
-    const int f = cf.bCol[k];
+    const int f = cf.bColG[k];
     if (bd.kind[bIndexOfFace[f]] == 1) {
       const double aij = coeff[f];
       const double ajj = 0.0 - coeff[f];

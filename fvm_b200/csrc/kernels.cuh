@@ -116,8 +116,9 @@ struct BoundaryData {
 struct CellFaceView {
   const int* row;  // cellFaces over self cells
   const int* col;
-  const int* bRow;  // per self cell: range into the boundary-face list (ascending face)
-  const int* bCol;
+  const int* bRow;   // per self cell: range into the boundary-face lists
+  const int* bCol;   // boundary faces, ascending face index (BC application order)
+  const int* bColG;  // the same faces by ascending ghost index (elimination order)
 };
 // Assembles the delta-form right-hand side of every self cell exactly as
 // DiffusionDiscretization + Source + TimeDerivative + GenericBCS +

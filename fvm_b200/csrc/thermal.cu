@@ -1,7 +1,9 @@
 // ThermalModel on the GPU.
 #include "thermal.hpp"
 
+#include <algorithm>
 #include <chrono>
+#include <functional>
 #include <cmath>
 #include <cstdio>
 
@@ -151,7 +153,10 @@ void ThermalModel::ensureDevice() {
       bIndexOfFace[f] = (int)boundaryFaces_.size();
       boundaryFaces_.push_back(f);
     }
-  std::vector<int> cfRow(n + 1), cfCol, bRow(n + 1, 0), bCol;
+  // per self cell: its faces ascending; its boundary faces ascending (the
+  // order BCs are applied in) and the same faces by ghost index (the order
+  // eliminateBoundaryEquations visits the ghost rows in)
+  std::vector<int> cfRow(n + 1), cfCol, bRow(n + 1, 0), bCol, bColG;
   for (int i = 0; i < n; i++) {
     cfRow[i] = (int)cfCol.size();
     bRow[i] = (int)bCol.size();
@@ -160,6 +165,9 @@ void ThermalModel::ensureDevice() {
       cfCol.push_back(f);
       if (bIndexOfFace[f] >= 0) bCol.push_back(f);
     }
+    std::vector<int> g(bCol.begin() + bRow[i], bCol.end());
+    std::sort(g.begin(), g.end(), [&](int a, int b) { return m.faceCells[2 * a + 1] < m.faceCells[2 * b + 1]; });
+    bColG.insert(bColG.end(), g.begin(), g.end());
   }
   cfRow[n] = (int)cfCol.size();
   bRow[n] = (int)bCol.size();
@@ -196,6 +204,7 @@ void ThermalModel::ensureDevice() {
   dCfCol_ = arena_.upload(cfCol);
   dBRow_ = arena_.upload(bRow);
   dBCol_ = arena_.upload(bCol);
+  dBColG_ = arena_.upload(bColG);
   dBFace_ = arena_.upload(boundaryFaces_);
   dBIndexOfFace_ = arena_.upload(bIndexOfFace);
   const int nB = (int)boundaryFaces_.size();
@@ -282,7 +291,7 @@ void ThermalModel::ensureMatrix() {
     dev::transient_coeff(n, dRc_, dVol_, opt_.timeStep, dRhoVdt_, stream_);
     rhoVdt = dRhoVdt_;
   }
-  dev::CellFaceView cf{dCfRow_, dCfCol_, dBRow_, dBCol_};
+  dev::CellFaceView cf{dCfRow_, dCfCol_, dBRow_, dBCol_, dBColG_};
   dev::BoundaryData bd{(int)boundaryFaces_.size(), dBFace_, dBKind_, dBValue_};
   dev::assemble_matrix(n, cf, dFaceCells_, dCoeff_, rhoVdt, bd, dBIndexOfFace_, dDiagOrig_, stream_);
   std::vector<double> coeff(F), diag(n);
@@ -314,7 +323,7 @@ void ThermalModel::linearize() {
   dev::ghost_gradient((int)boundaryFaces_.size(), dBFace_, dFaceCells_, dGrad_, stream_);
   dev::FaceGeom g{F, n, dFaceCells_, dArea_, dAreaMag_, dCentroid_, dVol_};
   dev::face_flux(g, dCoeff_, dSec_, dGrad_, dT_, dFlux_, stream_);
-  dev::CellFaceView cf{dCfRow_, dCfCol_, dBRow_, dBCol_};
+  dev::CellFaceView cf{dCfRow_, dCfCol_, dBRow_, dBCol_, dBColG_};
   dev::BoundaryData bd{(int)boundaryFaces_.size(), dBFace_, dBKind_, dBValue_};
   dev::assemble_rhs(n, cf, dFaceCells_, dFlux_, dCoeff_, dAreaMag_, dVol_, dSrc_,
                     opt_.transient ? dRhoVdt_ : nullptr, dTN1_, bd, dBIndexOfFace_, dT_, dBGhost_,
@@ -403,6 +412,68 @@ void ThermalModel::linearizeOnly(std::vector<double>& diag, std::vector<double>&
   for (int i = 0; i < n; i++) b[i] = bp[p0.perm[i]];
   diag = hier_.refLevels()[0].diag;
   off = hier_.refLevels()[0].off;
+}
+
+void ThermalModel::profile(int reps, double* out) {
+  FVM_REQUIRE(initialized_, kBadArgument, "ThermalModel.init() must be called first");
+  FVM_REQUIRE(reps > 0, kBadArgument, "reps must be positive");
+  ensureDevice();
+  uploadFields();
+  ensureMatrix();
+  linearize();
+  const size_t flushBytes = 512u << 20;  // > 126 MB L2
+  void* flush = nullptr;
+  CUDA_OK(cudaMalloc(&flush, flushBytes));
+  cudaEvent_t a, b;
+  CUDA_OK(cudaEventCreate(&a));
+  CUDA_OK(cudaEventCreate(&b));
+  DevLevel& d = hier_.level(0);
+  const bool mixed = opt_.linear.precision == kMixed;
+  auto timed = [&](const std::function<void()>& body) {
+    double total = 0;
+    for (int r = 0; r < reps; r++) {
+      CUDA_OK(cudaMemsetAsync(flush, r & 0xff, flushBytes, stream_));
+      CUDA_OK(cudaEventRecord(a, stream_));
+      body();
+      CUDA_OK(cudaEventRecord(b, stream_));
+      CUDA_OK(cudaEventSynchronize(b));
+      float ms = 0;
+      CUDA_OK(cudaEventElapsedTime(&ms, a, b));
+      total += ms;
+    }
+    return total / reps;
+  };
+  if (mixed) dev::convert_d2f(d.n, d.b, d.bF, stream_);
+  out[0] = timed([&] {
+    if (mixed) {
+      for (int c = 0; c < d.nColors; c++)
+        dev::gs_color<float>(d.view32(), d.colorSliceStart[c], d.colorSliceStart[c + 1], d.xF, d.bF, stream_);
+    } else {
+      for (int c = 0; c < d.nColors; c++)
+        dev::gs_color<double>(d.view64(), d.colorSliceStart[c], d.colorSliceStart[c + 1], d.x, d.b, stream_);
+    }
+  });
+  out[1] = hier_.fineSweepBytes();
+  out[2] = timed([&] { dev::residual<double>(d.view64(), d.nSlices, d.x, d.b, d.r, d.partials, stream_); });
+  out[3] = d.n * 32.0 + d.entries * 12.0;
+  out[4] = timed([&] {
+    if (mixed)
+      hier_.cycle<float>(opt_.linear.cycleType, 0, stream_);
+    else
+      hier_.cycle<double>(opt_.linear.cycleType, 0, stream_);
+  });
+  out[5] = hier_.cycleBytes();
+  out[6] = hier_.numLevels();
+  out[7] = d.n;
+  out[8] = (double)d.entries;
+  out[9] = hier_.kernelsPerCycle();
+  out[10] = d.nColors;
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  cudaFree(flush);
+  CUDA_OK(cudaMemsetAsync(d.x, 0, sizeof(double) * d.n, stream_));
+  if (d.xF) CUDA_OK(cudaMemsetAsync(d.xF, 0, sizeof(float) * d.n, stream_));
+  CUDA_OK(cudaStreamSynchronize(stream_));
 }
 
 const AmgHierarchy& ThermalModel::hierarchy() {

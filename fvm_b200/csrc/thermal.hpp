@@ -93,6 +93,13 @@ class ThermalModel {
   void linearizeOnly(std::vector<double>& diag, std::vector<double>& off,
                      std::vector<double>& b);
   const AmgHierarchy& hierarchy();
+  // CUDA-event timings (ms per launch) with an L2 flush before each timed
+  // launch: [0] one Gauss-Seidel pass over all colours of level 0 in the
+  // configured V-cycle precision, [1] its algorithmic bytes, [2] FP64
+  // residual of level 0, [3] its bytes, [4] one full cycle, [5] its bytes,
+  // [6] levels, [7] rows of level 0, [8] stored entries of level 0,
+  // [9] kernels per cycle, [10] colours of level 0
+  void profile(int reps, double* out);
   const std::vector<double>& history() const { return history_; }
   cudaStream_t stream() const { return stream_; }
 
@@ -120,7 +127,7 @@ class ThermalModel {
   bool deviceReady_ = false;
   DeviceArena arena_;
   int *dFaceCells_ = nullptr, *dCcRow_ = nullptr, *dCcCol_ = nullptr;
-  int *dCfRow_ = nullptr, *dCfCol_ = nullptr, *dBRow_ = nullptr, *dBCol_ = nullptr;
+  int *dCfRow_ = nullptr, *dCfCol_ = nullptr, *dBRow_ = nullptr, *dBCol_ = nullptr, *dBColG_ = nullptr;
   int *dBFace_ = nullptr, *dBKind_ = nullptr, *dBIndexOfFace_ = nullptr, *dPerm_ = nullptr;
   double *dArea_ = nullptr, *dAreaMag_ = nullptr, *dCentroid_ = nullptr, *dVol_ = nullptr;
   double *dGradW_ = nullptr, *dGrad_ = nullptr, *dFlux_ = nullptr, *dCoeff_ = nullptr, *dSec_ = nullptr;

@@ -266,6 +266,15 @@ class ThermalModelA:
             p += s[lvl]
         return list(sizes[: nl.value]), out
 
+    def profile(self, reps: int = 5) -> dict:
+        """CUDA-event timings of the finest-level kernels (see fvm_thermal_profile)."""
+        self._push()
+        out = np.zeros(11)
+        check(_lib.load().fvm_thermal_profile(self._h, int(reps), dptr(out)))
+        keys = ["gs_pass_ms", "gs_pass_bytes", "residual_ms", "residual_bytes", "cycle_ms", "cycle_bytes", "levels",
+                "rows", "entries", "kernels_per_cycle", "colors"]
+        return dict(zip(keys, out.tolist()))
+
     def lastReport(self):
         return self._lastReport
 

@@ -157,6 +157,14 @@ int fvm_thermal_linear_system(fvm_thermal* t, double* diag, double* off, double*
  * their sizes, and the coarseIndex of each fine level concatenated. */
 int fvm_thermal_hierarchy(fvm_thermal* t, int* nLevels, int* sizes, int sizesCap,
                           int* coarseIndex, int ciCap);
+/* Measurement hook (no reference counterpart): CUDA-event timings in ms
+ * per launch, each launch preceded by a write of 512 MB to flush L2.
+ * out[0] one Gauss-Seidel pass over all colours of the finest level in the
+ * V-cycle precision, out[1] its algorithmic bytes, out[2] the FP64 finest
+ * residual, out[3] its bytes, out[4] one full cycle, out[5] its bytes,
+ * out[6] levels, out[7] finest rows, out[8] finest stored entries,
+ * out[9] kernels per cycle, out[10] colours of the finest level. */
+int fvm_thermal_profile(fvm_thermal* t, int reps, double* out11);
 int fvm_thermal_destroy(fvm_thermal* t);
 
 /* Raw system path (testLinearSolver / MMReader + AMG::solve,

@@ -45,6 +45,7 @@
 #include "ThermalModel.h"
 #include "ThermalModel_impl.h"
 #include "AMG.h"
+#include "GradientModel.h"
 #include "CG.h"
 #include "BCGStab.h"
 #include "LinearSystem.h"
@@ -159,6 +160,10 @@ struct RefModel {
   BCGStab* bcg = nullptr;
   std::vector<double> history;  // outer rNorm per advance iteration
   ~RefModel() {
+    // the reference caches least-squares gradient matrices in a static map
+    // keyed by Mesh*; drop this mesh's entry so that a later mesh allocated
+    // at the same address does not pick it up
+    if (mesh) GradientModelBase::clearGradientMatrix(*mesh);
     delete model;
     delete metrics;
     delete amg;
@@ -596,6 +601,7 @@ int ref_thermal_hierarchy(void* h, int groupSize, double thr, int maxLevels, int
     impl.linearize(ls);
     ls.initSolve();
     AMG amg;
+    amg.verbosity = 0;
     amg.maxCoarseLevels = maxLevels;
     amg.coarseGroupSize = groupSize;
     amg.weightRatioThreshold = thr;

@@ -1,0 +1,240 @@
+"""GPU parity: the CUDA path against the reference oracle on identical
+inputs, through the C ABI (Python mirror of the reference API).
+
+Bars (stated per test):
+  * integer setup (aggregation) and the FP64 matrix: bit-exact;
+  * reference-ordered smoothers (sequential Gauss-Seidel, Jacobi): residual
+    histories equal to the reference's to 1e-12 relative (only the L1
+    reduction order differs);
+  * converged temperature fields: relative L2 error <= 1e-8 against the
+    reference's FP64 CPU solve, for every smoother / precision / solver.
+"""
+import numpy as np
+import pytest
+
+from fvm_b200 import fvmbaseExt, meshgen
+from helpers import gpu_model, load_fixture, ref_model, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+TOL_FIELD = 1e-8  # relative L2 against the reference FP64 solve
+
+
+def _amg(**kw):
+    a = fvmbaseExt.AMG()
+    for k, v in kw.items():
+        setattr(a, k, v)
+    return a
+
+
+# ---------------------------------------------------------------------------
+# raw AMG on the reference's MatrixMarket known-answer system
+
+
+def test_mm226_sequential_gs_matches_reference_history():
+    z = load_fixture("mm226.npz")
+    a = _amg(nMaxIterations=41, relativeTolerance=1e-30, absoluteTolerance=0.0,
+             smootherOrdering=fvmbaseExt.AMG.SEQUENTIAL, useGraphs=True)
+    x, info = a.solve_csr(z["row"], z["col"], z["diag"], z["off"], z["b"])
+    assert list(info["levelSizes"]) == [108, 48, 20, 8]
+    h = info["history"]
+    assert len(h) == 41
+    np.testing.assert_allclose(h, z["ref_hist"], rtol=1e-12, atol=0)
+    np.testing.assert_allclose(x, z["ref_x"], rtol=1e-12, atol=1e-12 * np.abs(z["ref_x"]).max())
+
+
+def test_mm226_jacobi_matches_reference_history(refo):
+    z = load_fixture("mm226.npz")
+    _, _, rh, _ = refo.amg_csr(z["row"], z["col"], z["diag"], z["off"], z["b"], max_iter=30, rel_tol=1e-30,
+                               smoother=1)
+    a = _amg(nMaxIterations=30, relativeTolerance=1e-30, absoluteTolerance=0.0, smootherType=fvmbaseExt.AMG.JACOBI)
+    _, info = a.solve_csr(z["row"], z["col"], z["diag"], z["off"], z["b"])
+    np.testing.assert_allclose(info["history"], rh, rtol=1e-12, atol=0)
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+@pytest.mark.parametrize("solver", ["AMG", "CG", "BCGStab"])
+def test_mm226_multicolor_converges_to_reference_solution(refo, solver, precision):
+    z = load_fixture("mm226.npz")
+    xr, _, _, _ = refo.amg_csr(z["row"], z["col"], z["diag"], z["off"], z["b"], max_iter=400, rel_tol=1e-13)
+    pre = _amg(precision=precision, coarseSolver=fvmbaseExt.AMG.COARSE_DIRECT)
+    if solver == "AMG":
+        s = pre
+    else:
+        s = fvmbaseExt.CG() if solver == "CG" else fvmbaseExt.BCGStab()
+        s.preconditioner = pre
+    s.nMaxIterations = 400
+    s.relativeTolerance = 1e-13
+    s.absoluteTolerance = 0.0
+    x, info = s.solve_csr(z["row"], z["col"], z["diag"], z["off"], z["b"])
+    assert info["converged"]
+    assert rel_l2(x, xr) <= 1e-10
+
+
+# ---------------------------------------------------------------------------
+# ThermalModel linearization and AMG setup on the reference's own meshes
+
+
+def test_cav32_linear_system_bit_exact_and_golden(refo):
+    m = load_fixture("cav32_matrix.npz")
+    bcs = {3: ("T", 400.0), 4: ("T", 0.0), 5: ("T", 0.0), 6: ("T", 0.0)}
+    tm, tf, mesh = gpu_model(m, bcs, solver=_amg(relativeTolerance=1e-9, nMaxIterations=2000, maxCoarseLevels=20),
+                             group_ids=m["groupId"], group_types=m["groupType"])
+    diag, off, b = tm.getLinearSystem()
+    r = ref_model(refo, m, bcs, group_ids=m["groupId"], group_types=m["groupType"], lin_rel=1e-9, max_iter=2000,
+                  max_levels=20)
+    d_ref, o_ref, b_ref, _ = r.linearize()
+    n = m["nCells"]
+    row, col = mesh.getCellCells()
+    o_ref_int = np.concatenate([o_ref[row[i]:row[i + 1]][col[row[i]:row[i + 1]] < n] for i in range(n)])
+    np.testing.assert_array_equal(diag, d_ref[:n])
+    np.testing.assert_array_equal(off, o_ref_int)
+    np.testing.assert_array_equal(b, b_ref[:n])
+    # and the THERMAL_MATRIX golden (printed with %lf: 1e-8 in its ptest.py)
+    gold = {(int(i), int(j)): v for i, j, v in zip(m["gold_i"], m["gold_j"], m["gold_v"])}
+    rows, cols = tm._interior_pattern()
+    for i in range(n):
+        assert abs(diag[i] - gold[(i, i)]) <= 1e-8
+        for k in range(rows[i], rows[i + 1]):
+            assert abs(off[k] - gold[(i, int(cols[k]))]) <= 1e-8
+    assert np.abs(-b - m["gold_rhs"]).max() <= 1e-8
+
+
+@pytest.mark.parametrize("ordering", ["sequential", "multicolor"])
+@pytest.mark.parametrize("case", ["quad_1024", "tri_894", "hexa_10k", "tetra_8k"])
+def test_parallel_thermal_golden_on_gpu(refo, case, ordering):
+    """PARALLEL_TESTS np=1: advance(1) -> within 1e-5 of the golden
+    temperatures; the AMG hierarchy (coarseIndex of every level) equals the
+    reference's. The golden run stops the inner AMG at relTol 1e-9 with the
+    reference's lexicographic Gauss-Seidel: the sequential ordering repeats
+    exactly that; the multicolour smoother (different iterates) is run to
+    relTol 1e-12 so that its remaining solver error is below the tolerance."""
+    m = load_fixture("ptest_%s.npz" % case)
+    bcs = {g: ("T", v) for g, v in ((3, 400.0), (4, 0.0), (5, 0.0), (6, 0.0)) if g in m["groupId"]}
+    if ordering == "sequential":
+        amg = _amg(relativeTolerance=1e-9, nMaxIterations=2000, maxCoarseLevels=20,
+                   smootherOrdering=fvmbaseExt.AMG.SEQUENTIAL)
+    else:
+        amg = _amg(relativeTolerance=1e-12, nMaxIterations=4000, maxCoarseLevels=20)
+    tm, tf, mesh = gpu_model(m, bcs, solver=amg, group_ids=m["groupId"], group_types=m["groupType"])
+    sizes, cis = tm.getHierarchy()
+    r = ref_model(refo, m, bcs, group_ids=m["groupId"], group_types=m["groupType"], lin_rel=1e-9, max_iter=2000,
+                  max_levels=20)
+    rsizes, rcis = r.hierarchy(max_levels=20)
+    assert sizes == rsizes
+    for a, b in zip(cis, rcis):
+        np.testing.assert_array_equal(a, b)
+    tm.advance(1)
+    T = tf.temperature[mesh.getCells()][: m["nCells"]]
+    assert np.abs(T - m["T_gold"]).max() <= 1e-5
+
+
+# ---------------------------------------------------------------------------
+# converged fields on jittered synthetic meshes (non-orthogonal correction)
+
+
+def _synthetic(kind):
+    if kind == "quad":
+        mesh, f = meshgen.config0(n=24, seed=0)
+    elif kind == "tet":
+        mesh, f = meshgen.config1(m=7, seed=1)
+    else:
+        mesh, f = meshgen.config3(n=8, seed=3)
+    return mesh, f
+
+
+def _converge(tm, n_outer=200):
+    tm.advance(n_outer)
+    rep = tm.lastReport()
+    assert rep.converged
+    return rep
+
+
+@pytest.mark.parametrize("kind", ["quad", "tet", "hex"])
+@pytest.mark.parametrize("variant", ["fp64-gs", "fp64-sequential", "mixed-direct", "cg-mixed", "bcgstab", "jacobi"])
+def test_converged_field_matches_reference(refo, kind, variant):
+    mesh, f = _synthetic(kind)
+    bcs = {gid: v for gid, v in f["bc"].items()}
+    fields = {"conductivity": f["k"], "source": f["s"]}
+    amg = _amg(nPreSweeps=1, nPostSweeps=1, relativeTolerance=1e-10, nMaxIterations=500)
+    solver = amg
+    if variant == "fp64-sequential":
+        amg.smootherOrdering = fvmbaseExt.AMG.SEQUENTIAL
+    elif variant == "mixed-direct":
+        amg.precision = fvmbaseExt.AMG.MIXED
+        amg.coarseSolver = fvmbaseExt.AMG.COARSE_DIRECT
+        amg.coarsestSize = 100
+    elif variant == "cg-mixed":
+        amg.precision = fvmbaseExt.AMG.MIXED
+        amg.coarseSolver = fvmbaseExt.AMG.COARSE_DIRECT
+        amg.coarsestSize = 100
+        solver = fvmbaseExt.CG()
+        solver.preconditioner = amg
+        solver.relativeTolerance = 1e-10
+        solver.nMaxIterations = 500
+    elif variant == "bcgstab":
+        solver = fvmbaseExt.BCGStab()
+        solver.preconditioner = amg
+        solver.relativeTolerance = 1e-10
+        solver.nMaxIterations = 500
+    elif variant == "jacobi":
+        amg.smootherType = fvmbaseExt.AMG.JACOBI
+    tm, tf, m = gpu_model(mesh, bcs, solver=solver, fields=fields, opts={"relativeTolerance": 1e-10})
+    _converge(tm)
+    T = tf.temperature[m.getCells()][: mesh["nCells"]]
+    r = ref_model(refo, mesh, bcs, fields=fields, n_pre=1, n_post=1, lin_rel=1e-10, max_iter=500, rel=1e-10)
+    norms, _ = r.advance(200)
+    assert norms[-1] / norms[0] < 1e-10
+    Tr = r.get_field(0)[: mesh["nCells"]]
+    assert rel_l2(T, Tr) <= TOL_FIELD
+
+
+@pytest.mark.parametrize("smoother", ["sequential-gs", "jacobi"])
+def test_linear_system_bit_exact_on_jittered_tets(refo, smoother):
+    """Matrix and right-hand side of the first three outer iterations are
+    bit-identical to the reference's. With the reference-ordered smoothers
+    the iterates themselves are identical, so the non-zero lagged gradients
+    of later linearizations are compared too."""
+    mesh, f = meshgen.config1(m=7, seed=1)
+    fields = {"conductivity": f["k"], "source": f["s"]}
+    if smoother == "jacobi":
+        amg = _amg(smootherType=fvmbaseExt.AMG.JACOBI, relativeTolerance=1e-1, nMaxIterations=20)
+        sm = 1
+    else:
+        amg = _amg(smootherOrdering=fvmbaseExt.AMG.SEQUENTIAL, relativeTolerance=1e-1, nMaxIterations=20)
+        sm = 0
+    tm, tf, m = gpu_model(mesh, f["bc"], solver=amg, fields=fields)
+    r = ref_model(refo, mesh, f["bc"], fields=fields, smoother=sm)
+    n = mesh["nCells"]
+    for it in range(3):  # later linearizations carry a non-zero gradient
+        diag, off, b = tm.getLinearSystem()
+        d_ref, o_ref, b_ref, _ = r.linearize()
+        np.testing.assert_array_equal(diag, d_ref[:n], err_msg="diag, outer iteration %d" % it)
+        np.testing.assert_array_equal(b, b_ref[:n], err_msg="b, outer iteration %d" % it)
+        tm.advance(1)
+        r.advance(1)
+    T = tf.temperature[m.getCells()]
+    np.testing.assert_array_equal(T[:n], r.get_field(0)[:n])
+
+
+def test_transient_steps_match_reference(refo):
+    mesh = meshgen.hex_mesh(6)
+    n = mesh["nCells"]
+    rng = np.random.default_rng(4)
+    k = rng.lognormal(0, 1, n)
+    rc = rng.uniform(0.5, 2.0, n)
+    bcs = {2: ("T", 400.0)}
+    fields = {"conductivity": k, "specificHeat": rc}
+    amg = _amg(relativeTolerance=1e-10, nMaxIterations=300, nPreSweeps=1, nPostSweeps=1)
+    tm, tf, m = gpu_model(mesh, bcs, solver=amg, fields=fields,
+                          opts={"transient": True, "timeStep": 1e-3, "relativeTolerance": 1e-10})
+    r = ref_model(refo, mesh, bcs, fields=fields, transient=True, dt=1e-3, rel=1e-10, lin_rel=1e-10, max_iter=300,
+                  n_pre=1, n_post=1)
+    for step in range(3):
+        tm.advance(50)
+        tm.updateTime()
+        r.advance(50)
+        r.update_time()
+    T = tf.temperature[m.getCells()][:n]
+    Tr = r.get_field(0)[:n]
+    assert rel_l2(T, Tr) <= TOL_FIELD

@@ -399,6 +399,33 @@ int fvm_thermal_destroy(fvm_thermal* h) {
   return FVM_OK;
 }
 
+int fvm_csr_residual(int n, const int* row, const int* col, const double* diag, const double* off,
+                     const double* x, const double* b, double* r, double* l1norm) {
+  return guarded([&] {
+    FVM_REQUIRE(x && b && l1norm, kBadArgument, "null argument");
+    RefLevel l = level_from_csr(n, row, col, diag, off);  // validates the pattern
+    const int nnz = l.conn.nnz();
+    const int np = dev::csr_residual_blocks(n);
+    DeviceArena arena;
+    int* dRow = arena.upload(l.conn.row);
+    int* dCol = arena.upload(l.conn.col);
+    double* dDiag = arena.upload(l.diag);
+    double* dOff = arena.upload(l.off);
+    std::vector<double> hx(x, x + n), hb(b, b + n);
+    double* dX = arena.upload(hx);
+    double* dB = arena.upload(hb);
+    double* dR = (double*)arena.alloc(sizeof(double) * (size_t)n);
+    double* dP = (double*)arena.alloc(sizeof(double) * (size_t)(np + 1));
+    (void)nnz;
+    dev::csr_residual(n, dRow, dCol, dDiag, dOff, dX, dB, dR, dP, 0);
+    dev::csr_residual_finish(np, dP, dP + np, 0);
+    if (cudaMemcpy(l1norm, dP + np, sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess)
+      throw Error(kDeviceError, "copy of the residual norm failed");
+    if (r && cudaMemcpy(r, dR, sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost) != cudaSuccess)
+      throw Error(kDeviceError, "copy of the residual failed");
+  });
+}
+
 int fvm_amg_hierarchy_csr(int n, const int* row, const int* col, const double* diag, const double* off,
                           const fvm_linear_options* o, int finestLocalSize, int* nLevels, int* sizes,
                           int sizesCap, int* coarseIndex, int ciCap, int* colors, int colorsCap) {

@@ -109,6 +109,22 @@ __global__ void k_residual(SellView<T> a, int nSlices, const T* __restrict__ x,
   }
 }
 
+__global__ void k_csr_residual(int n, const int* __restrict__ row, const int* __restrict__ col,
+                               const double* __restrict__ diag, const double* __restrict__ off,
+                               const double* __restrict__ x, const double* __restrict__ b, double* r,
+                               double* partials) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double l1 = 0.0;
+  if (i < n) {
+    double s = b[i] + diag[i] * x[i];
+    for (int k = row[i]; k < row[i + 1]; k++) s = s + off[k] * x[col[k]];
+    if (r) r[i] = s;
+    l1 = fabs(s);
+  }
+  const double t = block_sum(l1);
+  if (threadIdx.x == 0) partials[blockIdx.x] = t;
+}
+
 __global__ void k_spmv(SellView<double> a, int nSlices, const double* __restrict__ x, double* y) {
   const int s = blockIdx.x * kSlicesPerBlock + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
@@ -414,6 +430,14 @@ void residual(const SellView<T>& a, int nSlices, const T* x, const T* b, T* r, d
   k_residual<T><<<ceil_div(nSlices, kSlicesPerBlock), kBlock, 0, st>>>(a, nSlices, x, b, r, partials);
 }
 int reduce_blocks(int nSlices) { return ceil_div(nSlices, kSlicesPerBlock); }
+int csr_residual_blocks(int n) { return ceil_div(n, kBlock); }
+void csr_residual(int n, const int* row, const int* col, const double* diag, const double* off,
+                  const double* x, const double* b, double* r, double* partials, cudaStream_t st) {
+  k_csr_residual<<<csr_residual_blocks(n), kBlock, 0, st>>>(n, row, col, diag, off, x, b, r, partials);
+}
+void csr_residual_finish(int nPartials, const double* partials, double* l1, cudaStream_t st) {
+  k_sum_partials<<<1, 1024, 0, st>>>(nPartials, partials, l1);
+}
 void spmv(const SellView<double>& a, int nSlices, const double* x, double* y, cudaStream_t st) {
   k_spmv<<<ceil_div(nSlices, kSlicesPerBlock), kBlock, 0, st>>>(a, nSlices, x, y);
 }

@@ -43,6 +43,15 @@ void residual(const SellView<T>& a, int nSlices, const T* x, const T* b, T* r, d
 void spmv(const SellView<double>& a, int nSlices, const double* x, double* y, cudaStream_t st);
 int reduce_blocks(int nSlices);  // number of partials residual() writes
 
+// r = b + D x + O x on a plain CSR matrix (implicit diagonal, reference
+// column order), one thread per row; block k writes the L1 sum of its 256
+// rows to partials[k] (csr_residual_blocks(n) of them), then
+// csr_residual_finish sums them in a fixed order into *l1.
+int csr_residual_blocks(int n);
+void csr_residual(int n, const int* row, const int* col, const double* diag, const double* off,
+                  const double* x, const double* b, double* r, double* partials, cudaStream_t st);
+void csr_residual_finish(int nPartials, const double* partials, double* l1, cudaStream_t st);
+
 // ---- transfers ---------------------------------------------------------------
 // bc[I] = sum over fine rows i of aggregate I (ascending reference order) of r[i]
 template <class T>

@@ -299,6 +299,20 @@ def _solve_csr(opts, row, col, diag, off, b, solver):
     return x, info
 
 
+def csr_residual(row, col, diag, off, x, b):
+    """(r, |r|_1) with r = b + A x for a matrix with implicit diagonal
+    (CRMatrix::computeResidual + getOneNorm), computed on the GPU."""
+    lib = _lib.load()
+    row, col = as_i32(row), as_i32(col)
+    diag, off, x, b = as_f64(diag), as_f64(off), as_f64(x), as_f64(b)
+    n = len(diag)
+    r = np.zeros(n)
+    nrm = np.zeros(1)
+    check(lib.fvm_csr_residual(n, iptr(row), iptr(col), dptr(diag), dptr(off), dptr(x), dptr(b), dptr(r),
+                               dptr(nrm)))
+    return r, float(nrm[0])
+
+
 def hierarchy_csr(opts, row, col, diag, off, finestLocalSize: int = 0):
     lib = _lib.load()
     row, col = as_i32(row), as_i32(col)

@@ -177,6 +177,12 @@ int fvm_amg_solve_csr(int n, const int* row, const int* col, const double* diag,
                       const fvm_linear_options* o, fvm_report* rep, double* history,
                       int historyCap, int* nHistory, int* levelSizes, int levelCap,
                       int* nLevels);
+/* Residual of the raw system, host buffers: r = b + A x over n rows
+ * (CRMatrix::computeResidual, fvmbase/CRMatrix.h:407-426) and its L1 norm
+ * (Array::getOneNorm / MultiField::getOneNorm, fvmbase/Array.h:302-311,
+ * fvmbase/MultiField.cpp:216-230). r may be null. */
+int fvm_csr_residual(int n, const int* row, const int* col, const double* diag, const double* off,
+                     const double* x, const double* b, double* r, double* l1norm);
 /* Host-only AMG setup of the same system (no device needed): coarse sizes
  * and concatenated coarseIndex arrays (CRMatrix::createCoarsening,
  * fvmbase/CRMatrix.h:468-586), plus, when colors != null, the greedy

@@ -107,6 +107,10 @@ _SIGS = {
                                          c_double_p, ctypes.c_int, c_int_p, c_int_p, ctypes.c_int, c_int_p]),
     "fvm_csr_residual": (ctypes.c_int, [ctypes.c_int, c_int_p, c_int_p, c_double_p, c_double_p, c_double_p,
                                         c_double_p, c_double_p, c_double_p]),
+    "fvm_csr_residual_device_noalloc": (ctypes.c_int, [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                                                       ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                                       ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                                       ctypes.c_void_p]),
     "fvm_amg_hierarchy_csr": (ctypes.c_int, [ctypes.c_int, c_int_p, c_int_p, c_double_p, c_double_p,
                                              ctypes.POINTER(LinearOptions), ctypes.c_int, c_int_p, c_int_p,
                                              ctypes.c_int, c_int_p, ctypes.c_int, c_int_p, ctypes.c_int]),

@@ -183,6 +183,19 @@ int fvm_amg_solve_csr(int n, const int* row, const int* col, const double* diag,
  * fvmbase/MultiField.cpp:216-230). r may be null. */
 int fvm_csr_residual(int n, const int* row, const int* col, const double* diag, const double* off,
                      const double* x, const double* b, double* r, double* l1norm);
+/* fvm_csr_residual for callers that cannot allocate device memory (no
+ * counterpart in the reference, which has no device boundary): every
+ * pointer is DEVICE memory owned by the caller (row, col, diag, off, x, b
+ * in; r -- may be null -- and the single double *l1norm out), work is
+ * enqueued on `stream` (a cudaStream_t; null = default stream) and nothing
+ * is allocated: the reduction's block sums live in a fixed 512 KB device
+ * array inside the library, so n is limited to 16,777,216 rows (larger n
+ * returns FVM_ERR_TOO_LARGE). The first call on each device looks up that
+ * array's device address; make it outside any stream capture. Calls share
+ * the array: calls that overlap on one device race, so serialise them. */
+int fvm_csr_residual_device_noalloc(int n, const int* row, const int* col, const double* diag,
+                                    const double* off, const double* x, const double* b, double* r,
+                                    double* l1norm, void* stream);
 /* Host-only AMG setup of the same system (no device needed): coarse sizes
  * and concatenated coarseIndex arrays (CRMatrix::createCoarsening,
  * fvmbase/CRMatrix.h:468-586), plus, when colors != null, the greedy

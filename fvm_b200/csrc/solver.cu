@@ -5,6 +5,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <cstdlib>
 #include <limits>
 
 namespace fvm {
@@ -127,6 +128,142 @@ void AmgHierarchy::build(std::vector<RefLevel>& levels, int finestLocalSize, con
     dense_inverse(c, inv);
     coarseInv_ = arena_.upload(inv);
   }
+  buildProgram();
+}
+
+void AmgHierarchy::genSweeps(int n, int l, std::vector<dev::Phase>& out) const {
+  const DevLevel& d = lv_[l];
+  for (int s = 0; s < n; s++) {
+    if (opt_.smootherType == kGaussSeidel) {
+      const int C = d.nColors;
+      for (int c = 0; c < C; c++)
+        if (d.colorSliceStart[c + 1] > d.colorSliceStart[c])
+          out.push_back({dev::kPhaseGS, l, d.colorSliceStart[c], d.colorSliceStart[c + 1]});
+      for (int c = C - 2; c >= 0; c--)
+        if (d.colorSliceStart[c + 1] > d.colorSliceStart[c])
+          out.push_back({dev::kPhaseGS, l, d.colorSliceStart[c], d.colorSliceStart[c + 1]});
+    } else {
+      out.push_back({dev::kPhaseJacobi, l, 0, 0});
+      out.push_back({dev::kPhaseJacobi, l, 1, 0});
+    }
+  }
+}
+
+// Flattens AmgHierarchy::cycle into phases (same order of operations).
+void AmgHierarchy::genCycle(CycleType t, int l, std::vector<dev::Phase>& out) const {
+  const int L = (int)lv_.size();
+  const bool coarsest = (l == L - 1);
+  if (coarsest && coarseInv_) {
+    out.push_back({dev::kPhaseDense, l, 0, 0});
+    return;
+  }
+  genSweeps(opt_.nPreSweeps, l, out);
+  if (!coarsest) {
+    out.push_back({dev::kPhaseRestrict, l, 0, 0});
+    genCycle(t, l + 1, out);
+    if (t == kWCycle)
+      genCycle(kWCycle, l + 1, out);
+    else if (t == kFCycle)
+      genCycle(kVCycle, l + 1, out);
+    out.push_back({dev::kPhaseProlong, l, 0, 0});
+  }
+  genSweeps(opt_.nPostSweeps, l, out);
+}
+
+void AmgHierarchy::buildProgram() {
+  programReady_ = false;
+  // Opt-in (FVM_PERSISTENT_CYCLE=1): measured on B200 at 1.5M cells, a
+  // 296-block grid barrier per phase costs more than a graph-launched
+  // kernel per phase (3.8 vs 2.5 ms per FP32 V-cycle), so one launch per
+  // phase stays the default.
+  const char* env = getenv("FVM_PERSISTENT_CYCLE");
+  if (!env || env[0] != '1') return;
+  if (opt_.ordering == kSequential && opt_.smootherType == kGaussSeidel) return;
+  phases_.clear();
+  genCycle(opt_.cycleType, 0, phases_);
+  if (phases_.empty()) return;
+  dPhases_ = arena_.upload(phases_);
+  const int L = (int)lv_.size();
+  std::vector<dev::ProgLevel<double>> p64(L);
+  std::vector<dev::ProgLevel<float>> p32(L);
+  for (int l = 0; l < L; l++) {
+    const DevLevel& d = lv_[l];
+    dev::ProgLevel<double>& a = p64[l];
+    a.n = d.n;
+    a.nSlices = d.nSlices;
+    a.nCoarse = d.nCoarse;
+    a.sliceRow = d.sliceRow;
+    a.sliceRows = d.sliceRows;
+    a.sliceOff = d.sliceOff;
+    a.cols = d.cols;
+    a.rowSlice = d.rowSlice;
+    a.vals = d.vals;
+    a.diag = d.diag;
+    a.x = d.x;
+    a.b = d.b;
+    a.tmp = d.tmp;
+    a.ci = d.ci;
+    a.c2fRow = d.c2fRow;
+    a.c2fCol = d.c2fCol;
+    dev::ProgLevel<float>& f = p32[l];
+    f.n = d.n;
+    f.nSlices = d.nSlices;
+    f.nCoarse = d.nCoarse;
+    f.sliceRow = d.sliceRow;
+    f.sliceRows = d.sliceRows;
+    f.sliceOff = d.sliceOff;
+    f.cols = d.cols;
+    f.rowSlice = d.rowSlice;
+    f.vals = d.valsF;
+    f.diag = d.diagF;
+    f.x = d.xF;
+    f.b = d.bF;
+    f.tmp = d.tmpF;
+    f.ci = d.ci;
+    f.c2fRow = d.c2fRow;
+    f.c2fCol = d.c2fCol;
+  }
+  dProg64_ = arena_.upload(p64);
+  if (opt_.precision == kMixed) dProg32_ = arena_.upload(p32);
+  dBarrier_ = (dev::BarrierState*)arena_.alloc(sizeof(dev::BarrierState));
+  CUDA_OK(cudaMemset(dBarrier_, 0, sizeof(dev::BarrierState)));
+  grid64_ = dev::cycle_program_max_grid<double>();
+  grid32_ = dev::cycle_program_max_grid<float>();
+  FVM_REQUIRE(grid64_ > 0 && grid32_ > 0, kDeviceError, "cycle program cannot be made co-resident");
+  programReady_ = true;
+}
+
+template <>
+void AmgHierarchy::runCycle<double>(cudaStream_t st) {
+  if (!programReady_) {
+    cycle<double>(opt_.cycleType, 0, st);
+    return;
+  }
+  const int L = (int)lv_.size();
+  CUDA_OK(dev::run_cycle_program<double>(dPhases_, (int)phases_.size(), dProg64_, coarseInv_, lv_[L - 1].n,
+                                         dBarrier_, grid64_, st));
+}
+
+template <>
+void AmgHierarchy::runCycle<float>(cudaStream_t st) {
+  if (!programReady_) {
+    cycle<float>(opt_.cycleType, 0, st);
+    return;
+  }
+  const int L = (int)lv_.size();
+  CUDA_OK(dev::run_cycle_program<float>(dPhases_, (int)phases_.size(), dProg32_, coarseInv_, lv_[L - 1].n,
+                                        dBarrier_, grid32_, st));
+}
+
+void AmgHierarchy::checkProgram(cudaStream_t st) {
+  if (!programReady_) return;
+  dev::BarrierState bs;
+  CUDA_OK(cudaMemcpyAsync(&bs, dBarrier_, sizeof(bs), cudaMemcpyDeviceToHost, st));
+  CUDA_OK(cudaStreamSynchronize(st));
+  if (bs.error) {
+    CUDA_OK(cudaMemset(dBarrier_, 0, sizeof(dev::BarrierState)));
+    throw Error(kDeviceError, "a grid barrier of the cycle program exceeded its wait limit");
+  }
 }
 
 template <class T>
@@ -217,13 +354,13 @@ void AmgHierarchy::apply(const double* r, double* z, cudaStream_t st) {
   if (opt_.precision == kMixed) {
     dev::convert_d2f(d.n, r, d.bF, st);
     CUDA_OK(cudaMemsetAsync(d.xF, 0, sizeof(float) * (size_t)d.n, st));
-    cycle<float>(opt_.cycleType, 0, st);
+    runCycle<float>(st);
     CUDA_OK(cudaMemsetAsync(z, 0, sizeof(double) * (size_t)d.n, st));
     dev::add_f2d(d.n, d.xF, z, st);
   } else {
     dev::copy_d(d.n, r, d.b, st);
     CUDA_OK(cudaMemsetAsync(d.x, 0, sizeof(double) * (size_t)d.n, st));
-    cycle<double>(opt_.cycleType, 0, st);
+    runCycle<double>(st);
     dev::copy_d(d.n, d.x, z, st);
   }
 }
@@ -341,15 +478,24 @@ void LinearSolve::run(cudaGraphExec_t& exec, cudaStream_t st, const std::functio
     body();
     return;
   }
+  if (graphsFailed_) {
+    body();
+    return;
+  }
   if (!exec) {
-    cudaGraph_t g;
+    cudaGraph_t g = nullptr;
     CUDA_OK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
     try {
       body();
-    } catch (...) {
+    } catch (const Error&) {
+      // a launch that cannot be captured (e.g. cooperative launch on an
+      // older driver): drop graphs for this solver and run eagerly
       cudaStreamEndCapture(st, &g);
       if (g) cudaGraphDestroy(g);
-      throw;
+      cudaGetLastError();
+      graphsFailed_ = true;
+      body();
+      return;
     }
     CUDA_OK(cudaStreamEndCapture(st, &g));
     size_t nodes = 0;
@@ -363,14 +509,19 @@ void LinearSolve::run(cudaGraphExec_t& exec, cudaStream_t st, const std::functio
 }
 
 SolveReport LinearSolve::solve(cudaStream_t st) {
+  SolveReport r;
   switch (h_.options().solver) {
     case kSolverCG:
-      return solveCG(st);
+      r = solveCG(st);
+      break;
     case kSolverBCGStab:
-      return solveBCGStab(st);
+      r = solveBCGStab(st);
+      break;
     default:
-      return solveAMG(st);
+      r = solveAMG(st);
   }
+  h_.checkProgram(st);
+  return r;
 }
 
 static bool stop_test(double rn, double r0, const SolverOptions& o) {
@@ -404,10 +555,10 @@ SolveReport LinearSolve::solveAMG(cudaStream_t st) {
       if (o.precision == kMixed) {
         dev::convert_d2f(n_, d.r, d.bF, st);
         CUDA_OK(cudaMemsetAsync(d.xF, 0, sizeof(float) * (size_t)n_, st));
-        h_.cycle<float>(o.cycleType, 0, st);
+        h_.runCycle<float>(st);
         dev::add_f2d(n_, d.xF, d.x, st);
       } else {
-        h_.cycle<double>(o.cycleType, 0, st);
+        h_.runCycle<double>(st);
       }
       dev::residual<double>(d.view64(), d.nSlices, d.x, d.b, d.r, d.partials, st);
       dev::sum_partials(d.nPartials, d.partials, scal_ + kNorm, st);

@@ -13,6 +13,7 @@
 #include <vector>
 
 #include "amg_setup.hpp"
+#include "cycle_program.cuh"
 #include "kernels.cuh"
 
 namespace fvm {
@@ -116,6 +117,15 @@ class AmgHierarchy {
   template <class T>
   void sweeps(int nSweeps, int l, cudaStream_t st);
 
+  // one cycle from the finest level: the persistent program kernel when
+  // available (multicolour or Jacobi smoothing), else one launch per phase
+  template <class T>
+  void runCycle(cudaStream_t st);
+  bool usesProgram() const { return programReady_; }
+  int programPhases() const { return (int)phases_.size(); }
+  // raises if a program barrier ever exceeded its wait limit
+  void checkProgram(cudaStream_t st);
+
   // x = z <- M^-1 applied to r (FP64 in/out; runs the cycle in the
   // configured precision): b0 <- r, x0 <- 0, cycle, z <- x0
   void apply(const double* r, double* z, cudaStream_t st);
@@ -135,6 +145,17 @@ class AmgHierarchy {
   std::vector<DevLevel> lv_;
   double* coarseInv_ = nullptr;  // dense inverse of the coarsest level
   DeviceArena arena_;
+  // persistent cycle program
+  void buildProgram();
+  void genCycle(CycleType t, int l, std::vector<dev::Phase>& out) const;
+  void genSweeps(int n, int l, std::vector<dev::Phase>& out) const;
+  bool programReady_ = false;
+  std::vector<dev::Phase> phases_;
+  dev::Phase* dPhases_ = nullptr;
+  dev::ProgLevel<double>* dProg64_ = nullptr;
+  dev::ProgLevel<float>* dProg32_ = nullptr;
+  dev::BarrierState* dBarrier_ = nullptr;
+  int grid64_ = 0, grid32_ = 0;
 };
 
 // Linear solve of the finest system held by the hierarchy: level 0's b is
@@ -163,6 +184,7 @@ class LinearSolve {
   double* hostScal_ = nullptr;  // pinned
   cudaGraphExec_t g1_ = nullptr, g2_ = nullptr, g3_ = nullptr;
   std::map<const void*, long long> nodeCounts_;
+  bool graphsFailed_ = false;
 
  public:
   long long launches = 0;  // kernels + copies enqueued (graph nodes counted per replay)

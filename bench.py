@@ -166,8 +166,11 @@ def solver_for(variant: str, inner_rel: float):
     amg.relativeTolerance = inner_rel
     amg.nMaxIterations = 200
     if variant == "mixed":
+        # FP32 V-cycle under FP64 refinement; the coarsest level (<= 4096
+        # rows) is solved by a dense FP64-built inverse instead of smoothed
         amg.precision = fvmbaseExt.AMG.MIXED
         amg.coarseSolver = fvmbaseExt.AMG.COARSE_DIRECT
+        amg.coarsestSize = 4096
     return amg
 
 

@@ -4,8 +4,34 @@
 
 #include <algorithm>
 #include <cmath>
+#include <thread>
 
 namespace fvm {
+
+namespace {
+
+// Runs f(begin, end) over [0, n) split into contiguous chunks on the host's
+// cores (one chunk when n is small).
+template <class F>
+void parallel_chunks(int n, F f) {
+  int nt = (int)std::thread::hardware_concurrency();
+  if (nt < 1) nt = 1;
+  if (nt > 32) nt = 32;
+  if (n < 20000 || nt == 1) {
+    f(0, n);
+    return;
+  }
+  std::vector<std::thread> th;
+  const int chunk = (n + nt - 1) / nt;
+  for (int t = 0; t < nt; t++) {
+    const int b = t * chunk, e = std::min(n, b + chunk);
+    if (b >= e) break;
+    th.emplace_back([=] { f(b, e); });
+  }
+  for (auto& x : th) x.join();
+}
+
+}  // namespace
 
 int create_coarsening(const RefLevel& a, int groupSize, double thr, std::vector<int>& ci) {
   const int n = a.n;
@@ -79,45 +105,72 @@ void create_coarse_level(const RefLevel& fine, RefLevel& coarse, CSR& c2f) {
     for (int i = 0; i < fine.n; i++)
       if (ci[i] >= 0) c2f.col[cur[ci[i]]++] = i;
   }
-  // coarse pattern: neighbours in first-visit order
+  // Coarse pattern: each coarse row lists the coarse neighbours of its fine
+  // rows in first-visit order. Rows are independent, so they are built in
+  // parallel: a count pass, a prefix sum, a fill pass (rows are short, so a
+  // linear search replaces the reference's marker array).
   coarse.n = nc;
   coarse.conn.nRows = nc;
   coarse.conn.row.assign(nc + 1, 0);
-  coarse.conn.col.clear();
-  std::vector<int> stamp(nc, -1);
-  for (int I = 0; I < nc; I++) {
+  auto visit = [&](int I, int* out) {
+    int cnt = 0;
     for (int k = c2f.row[I]; k < c2f.row[I + 1]; k++) {
       const int i = c2f.col[k];
       for (int nb = row[i]; nb < row[i + 1]; nb++) {
         const int J = ci[col[nb]];
-        if (J >= 0 && J != I && stamp[J] != I) {
-          stamp[J] = I;
-          coarse.conn.col.push_back(J);
+        if (J < 0 || J == I) continue;
+        bool seen = false;
+        for (int q = 0; q < cnt; q++)
+          if (out[q] == J) {
+            seen = true;
+            break;
+          }
+        if (!seen) out[cnt++] = J;
+      }
+    }
+    return cnt;
+  };
+  int maxRow = 0;
+  for (int I = 0; I < nc; I++) {
+    int w = 0;
+    for (int k = c2f.row[I]; k < c2f.row[I + 1]; k++) w += row[c2f.col[k] + 1] - row[c2f.col[k]];
+    maxRow = std::max(maxRow, w);
+  }
+  parallel_chunks(nc, [&](int b, int e) {
+    std::vector<int> buf(maxRow + 1);
+    for (int I = b; I < e; I++) coarse.conn.row[I + 1] = visit(I, buf.data());
+  });
+  for (int I = 0; I < nc; I++) coarse.conn.row[I + 1] += coarse.conn.row[I];
+  coarse.conn.col.assign(coarse.conn.row[nc], 0);
+  parallel_chunks(nc, [&](int b, int e) {
+    for (int I = b; I < e; I++) visit(I, &coarse.conn.col[coarse.conn.row[I]]);
+  });
+  // Galerkin values with piecewise-constant prolongation; every coarse
+  // entry receives its fine contributions in the reference's order (fine
+  // rows ascending, their entries in stored order), so the sums round
+  // exactly as CRMatrix::createCoarseMatrix's do.
+  coarse.diag.assign(nc, 0.0);
+  coarse.off.assign(coarse.conn.col.size(), 0.0);
+  parallel_chunks(nc, [&](int b, int e) {
+    for (int I = b; I < e; I++) {
+      const int rb = coarse.conn.row[I], re = coarse.conn.row[I + 1];
+      for (int k = c2f.row[I]; k < c2f.row[I + 1]; k++) {
+        const int i = c2f.col[k];
+        coarse.diag[I] += fine.diag[i];
+        for (int nb = row[i]; nb < row[i + 1]; nb++) {
+          const int J = ci[col[nb]];
+          if (J < 0) continue;
+          if (J != I) {
+            int p = rb;
+            while (p < re && coarse.conn.col[p] != J) p++;
+            coarse.off[p] += fine.off[nb];
+          } else {
+            coarse.diag[I] += fine.off[nb];
+          }
         }
       }
     }
-    coarse.conn.row[I + 1] = (int)coarse.conn.col.size();
-  }
-  // Galerkin values with piecewise-constant prolongation
-  coarse.diag.assign(nc, 0.0);
-  coarse.off.assign(coarse.conn.col.size(), 0.0);
-  std::vector<int> pos(nc, -1);
-  for (int I = 0; I < nc; I++) {
-    for (int nb = coarse.conn.row[I]; nb < coarse.conn.row[I + 1]; nb++)
-      pos[coarse.conn.col[nb]] = nb;
-    for (int k = c2f.row[I]; k < c2f.row[I + 1]; k++) {
-      const int i = c2f.col[k];
-      coarse.diag[I] += fine.diag[i];
-      for (int nb = row[i]; nb < row[i + 1]; nb++) {
-        const int J = ci[col[nb]];
-        if (J < 0) continue;
-        if (J != I)
-          coarse.off[pos[J]] += fine.off[nb];
-        else
-          coarse.diag[I] += fine.off[nb];
-      }
-    }
-  }
+  });
 }
 
 void build_hierarchy(std::vector<RefLevel>& levels, const HierarchyOptions& opt,
@@ -142,6 +195,102 @@ void build_hierarchy(std::vector<RefLevel>& levels, const HierarchyOptions& opt,
   }
   levels.back().coarseIndex.clear();
   levels.back().nCoarse = 0;
+}
+
+namespace {
+
+// Greedy colouring visiting rows in `order`: each row takes the smallest
+// colour unused by its already-coloured neighbours.
+int greedy_in_order(const CSR& conn, const std::vector<int>& order, std::vector<int>& color) {
+  const int n = conn.nRows;
+  color.assign(n, -1);
+  std::vector<int> mark;
+  int nColors = 0;
+  for (int t = 0; t < n; t++) {
+    const int i = order[t];
+    for (int k = conn.row[i]; k < conn.row[i + 1]; k++) {
+      const int c = color[conn.col[k]];
+      if (c >= 0) {
+        if ((int)mark.size() <= c) mark.resize(c + 1, -1);
+        mark[c] = i;
+      }
+    }
+    int c = 0;
+    while (c < (int)mark.size() && mark[c] == i) c++;
+    color[i] = c;
+    nColors = std::max(nColors, c + 1);
+  }
+  return nColors;
+}
+
+// Smallest-last ordering (Matula & Beck): repeatedly remove a vertex of
+// minimum remaining degree (lowest index among equals); colouring in the
+// reverse removal order needs at most degeneracy + 1 colours.
+void smallest_last_order(const CSR& conn, std::vector<int>& order) {
+  const int n = conn.nRows;
+  std::vector<int> deg(n);
+  int maxDeg = 0;
+  for (int i = 0; i < n; i++) {
+    deg[i] = conn.count(i);
+    maxDeg = std::max(maxDeg, deg[i]);
+  }
+  // bucket lists by degree (doubly linked), kept in ascending index order
+  std::vector<int> head(maxDeg + 1, -1), next(n, -1), prev(n, -1);
+  for (int i = n - 1; i >= 0; i--) {
+    next[i] = head[deg[i]];
+    if (head[deg[i]] >= 0) prev[head[deg[i]]] = i;
+    head[deg[i]] = i;
+  }
+  std::vector<char> removed(n, 0);
+  std::vector<int> removal;
+  removal.reserve(n);
+  int d = 0;
+  for (int t = 0; t < n; t++) {
+    if (d > 0) d--;
+    while (head[d] < 0) d++;
+    const int v = head[d];
+    head[d] = next[v];
+    if (next[v] >= 0) prev[next[v]] = -1;
+    removed[v] = 1;
+    removal.push_back(v);
+    for (int k = conn.row[v]; k < conn.row[v + 1]; k++) {
+      const int u = conn.col[k];
+      if (removed[u]) continue;
+      // unlink u from bucket deg[u], push to the front of deg[u]-1
+      if (prev[u] >= 0)
+        next[prev[u]] = next[u];
+      else
+        head[deg[u]] = next[u];
+      if (next[u] >= 0) prev[next[u]] = prev[u];
+      deg[u]--;
+      prev[u] = -1;
+      next[u] = head[deg[u]];
+      if (head[deg[u]] >= 0) prev[head[deg[u]]] = u;
+      head[deg[u]] = u;
+    }
+  }
+  order.assign(removal.rbegin(), removal.rend());
+}
+
+}  // namespace
+
+// Deterministic colouring for the multicolour smoothers: greedy in row
+// order and greedy in smallest-last order, keeping whichever needs fewer
+// colours (row order on a tie). Fewer colours mean fewer dependent passes.
+int multicolor(const CSR& conn, std::vector<int>& color) {
+  const int n = conn.nRows;
+  std::vector<int> natural(n);
+  for (int i = 0; i < n; i++) natural[i] = i;
+  const int c1 = greedy_in_order(conn, natural, color);
+  if (c1 <= 2) return c1;
+  std::vector<int> order, color2;
+  smallest_last_order(conn, order);
+  const int c2 = greedy_in_order(conn, order, color2);
+  if (c2 < c1) {
+    color.swap(color2);
+    return c2;
+  }
+  return c1;
 }
 
 int greedy_coloring(const CSR& conn, std::vector<int>& color) {
@@ -174,7 +323,7 @@ void pack_level(const RefLevel& lv, SmootherOrdering ordering, PackedLevel& out)
     color.assign(n, 0);
     out.nColors = 1;
   } else {
-    out.nColors = greedy_coloring(lv.conn, color);
+    out.nColors = multicolor(lv.conn, color);
   }
   // colour-major permutation, stable in reference order
   out.colorStart.assign(out.nColors + 1, 0);
@@ -206,15 +355,24 @@ void pack_level(const RefLevel& lv, SmootherOrdering ordering, PackedLevel& out)
   const int nSlices = (int)out.sliceRow.size();
   out.sliceOff.assign(nSlices + 1, 0);
   out.maxWidth = 0;
+  parallel_chunks(nSlices, [&](int b, int e) {
+    for (int s = b; s < e; s++) {
+      int w = 0;
+      for (int l = 0; l < out.sliceRows[s]; l++) w = std::max(w, lv.conn.count(out.iperm[out.sliceRow[s] + l]));
+      out.sliceOff[s + 1] = w;
+    }
+  });
   for (int s = 0; s < nSlices; s++) {
-    int w = 0;
-    for (int l = 0; l < out.sliceRows[s]; l++) w = std::max(w, lv.conn.count(out.iperm[out.sliceRow[s] + l]));
-    out.maxWidth = std::max(out.maxWidth, w);
-    out.sliceOff[s + 1] = out.sliceOff[s] + 32 * w;
+    out.maxWidth = std::max(out.maxWidth, out.sliceOff[s + 1]);
+    out.sliceOff[s + 1] = out.sliceOff[s] + 32 * out.sliceOff[s + 1];
   }
-  out.cols.assign(out.sliceOff[nSlices], 0);
-  out.vals.assign(out.sliceOff[nSlices], 0.0);
-  for (int s = 0; s < nSlices; s++) {
+  out.cols.resize(out.sliceOff[nSlices]);
+  out.vals.resize(out.sliceOff[nSlices]);
+  parallel_chunks(nSlices, [&](int b, int e) { pack_slices(lv, out, b, e); });
+}
+
+void pack_slices(const RefLevel& lv, PackedLevel& out, int sBegin, int sEnd) {
+  for (int s = sBegin; s < sEnd; s++) {
     const int w = (out.sliceOff[s + 1] - out.sliceOff[s]) / 32;
     for (int l = 0; l < 32; l++) {
       const int p = out.sliceRow[s] + l;

@@ -80,8 +80,13 @@ enum SmootherOrdering { kMulticolor = 0, kSequential = 1 };
 // Greedy colouring in reference row order: each row takes the smallest
 // colour unused by its already-coloured neighbours.
 int greedy_coloring(const CSR& conn, std::vector<int>& color);
+// The colouring the multicolour smoothers use: the better (fewer colours)
+// of row-order greedy and smallest-last-order greedy; deterministic.
+int multicolor(const CSR& conn, std::vector<int>& color);
 
 void pack_level(const RefLevel& lv, SmootherOrdering ordering, PackedLevel& out);
+// fills cols/vals of slices [sBegin, sEnd) (pack_level runs it in parallel)
+void pack_slices(const RefLevel& lv, PackedLevel& out, int sBegin, int sEnd);
 void pack_transfer(const RefLevel& fine, const CSR& coarseToFine, PackedLevel& pf,
                    const PackedLevel& pc);
 

@@ -447,7 +447,7 @@ int fvm_amg_hierarchy_csr(int n, const int* row, const int* col, const double* d
       int pos = 0;
       for (const RefLevel& l : levels) {
         std::vector<int> c;
-        greedy_coloring(l.conn, c);
+        multicolor(l.conn, c);
         for (int v : c) {
           if (pos < colorsCap) colors[pos] = v;
           pos++;

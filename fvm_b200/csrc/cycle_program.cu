@@ -65,41 +65,43 @@ __device__ __forceinline__ T ldv(const T* p) {
   return __ldcg(p);
 }
 
-// Row sum over a SELL slice in stored order, 4 entries in flight.
+// Row sum over a SELL slice in stored order; all loads of up to 16
+// entries are in flight together (two dependent round trips per chunk).
 template <class T>
 __device__ __forceinline__ T row_sum(const ProgLevel<T>& L, int s, int lane, const T* x, T sum) {
   const int o = L.sliceOff[s];
   const int w = (L.sliceOff[s + 1] - o) >> 5;
-  int k = 0;
-  for (; k + 4 <= w; k += 4) {
-    const int e = o + (k << 5) + lane;
-    const int c0 = L.cols[e], c1 = L.cols[e + 32], c2 = L.cols[e + 64], c3 = L.cols[e + 96];
-    const T v0 = L.vals[e], v1 = L.vals[e + 32], v2 = L.vals[e + 64], v3 = L.vals[e + 96];
-    const T x0 = ldv(x + c0), x1 = ldv(x + c1), x2 = ldv(x + c2), x3 = ldv(x + c3);
-    sum = sum + v0 * x0;
-    sum = sum + v1 * x1;
-    sum = sum + v2 * x2;
-    sum = sum + v3 * x3;
-  }
-  for (; k < w; k++) {
-    const int e = o + (k << 5) + lane;
-    sum = sum + L.vals[e] * ldv(x + L.cols[e]);
+  for (int k0 = 0; k0 < w; k0 += 16) {
+    const int cnt = min(16, w - k0);
+    int c[16];
+    T v[16];
+    T xv[16];
+#pragma unroll
+    for (int k = 0; k < 16; k++)
+      if (k < cnt) {
+        const int e = o + ((k0 + k) << 5) + lane;
+        c[k] = L.cols[e];
+        v[k] = L.vals[e];
+      }
+#pragma unroll
+    for (int k = 0; k < 16; k++)
+      if (k < cnt) xv[k] = ldv(x + c[k]);
+#pragma unroll
+    for (int k = 0; k < 16; k++)
+      if (k < cnt) sum = sum + v[k] * xv[k];
   }
   return sum;
 }
 
+// Executes one phase with this thread's share (thread tid of nthreads).
 template <class T>
-__global__ void __launch_bounds__(kProgramBlock) k_cycle_program(const Phase* __restrict__ phases, int nPhases,
-                                                                  const ProgLevel<T>* __restrict__ levels,
-                                                                  const double* __restrict__ coarseInv,
-                                                                  int coarseN, BarrierState* bs) {
-  const int tid = blockIdx.x * blockDim.x + threadIdx.x;
-  const int nthreads = gridDim.x * blockDim.x;
+__device__ __forceinline__ void exec_phase(const Phase ph, const ProgLevel<T>* __restrict__ levels,
+                                           const double* __restrict__ coarseInv, const float* __restrict__ coarseInvF,
+                                           int coarseN, int tid, int nthreads) {
   const int gwarp = tid >> 5;
   const int nwarps = nthreads >> 5;
   const int lane = threadIdx.x & 31;
-  for (int p = 0; p < nPhases; p++) {
-    const Phase ph = phases[p];
+  {
     const ProgLevel<T> L = levels[ph.level];
     switch (ph.op) {
       case kPhaseGS: {
@@ -151,7 +153,12 @@ __global__ void __launch_bounds__(kProgramBlock) k_cycle_program(const Phase* __
       case kPhaseDense: {
         for (int row = gwarp; row < coarseN; row += nwarps) {
           double s = 0.0;
-          for (int j = lane; j < coarseN; j += 32) s += coarseInv[(size_t)row * coarseN + j] * (double)ldv(L.b + j);
+          if (coarseInvF) {
+            for (int j = lane; j < coarseN; j += 32)
+              s += (double)(coarseInvF[(size_t)row * coarseN + j] * (float)ldv(L.b + j));
+          } else {
+            for (int j = lane; j < coarseN; j += 32) s += coarseInv[(size_t)row * coarseN + j] * (double)ldv(L.b + j);
+          }
           for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
           if (lane == 0) L.x[row] = (T)(-s);
         }
@@ -160,8 +167,41 @@ __global__ void __launch_bounds__(kProgramBlock) k_cycle_program(const Phase* __
       default:
         break;
     }
+  }
+}
+
+template <class T>
+__global__ void __launch_bounds__(kProgramBlock) k_cycle_program(const Phase* __restrict__ phases, int nPhases,
+                                                                  const ProgLevel<T>* __restrict__ levels,
+                                                                  const double* __restrict__ coarseInv,
+                                                                  int coarseN, BarrierState* bs) {
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nthreads = gridDim.x * blockDim.x;
+  for (int p = 0; p < nPhases; p++) {
+    exec_phase<T>(phases[p], levels, coarseInv, nullptr, coarseN, tid, nthreads);
     if (p + 1 < nPhases) {
       if (!grid_barrier(bs)) return;
+    }
+  }
+}
+
+// The same phase list run by ONE thread-block cluster: the CTAs of the
+// cluster meet at the hardware cluster barrier (release/acquire at cluster
+// scope) between phases. Meant for the small coarse levels, whose phases
+// are too short to amortise a kernel launch each.
+template <class T>
+__global__ void __launch_bounds__(kClusterBlock, 1)
+    k_cluster_program(const Phase* __restrict__ phases, int nPhases, const ProgLevel<T>* __restrict__ levels,
+                      const double* __restrict__ coarseInv, const float* __restrict__ coarseInvF, int coarseN) {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nthreads = gridDim.x * blockDim.x;
+  for (int p = 0; p < nPhases; p++) {
+    exec_phase<T>(phases[p], levels, coarseInv, coarseInvF, coarseN, tid, nthreads);
+    if (p + 1 < nPhases) {
+      asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory");
+      asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory");
     }
   }
 }
@@ -196,6 +236,62 @@ cudaError_t run_cycle_program(const Phase* phases, int nPhases, const ProgLevel<
   return cudaLaunchKernelEx(&cfg, k_cycle_program<T>, phases, nPhases, levels, coarseInv, coarseN, barrier);
 }
 
+template <class T>
+int cluster_program_size() {
+  // the largest cluster (16 non-portable, else 8) of 1024-thread CTAs the
+  // device can place
+  for (int cs : {16, 8}) {
+    if (cs > 8 &&
+        cudaFuncSetAttribute(k_cluster_program<T>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
+            cudaSuccess) {
+      cudaGetLastError();
+      continue;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(cs);
+    cfg.blockDim = dim3(kClusterBlock);
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = cs;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int clusters = 0;
+    if (cudaOccupancyMaxActiveClusters(&clusters, k_cluster_program<T>, &cfg) == cudaSuccess && clusters > 0)
+      return cs;
+    cudaGetLastError();
+  }
+  return 0;
+}
+
+template <class T>
+cudaError_t run_cluster_program(const Phase* phases, int nPhases, const ProgLevel<T>* levels,
+                                const double* coarseInv, const float* coarseInvF, int coarseN, int clusterSize,
+                                cudaStream_t st) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(clusterSize);
+  cfg.blockDim = dim3(kClusterBlock);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[2];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = clusterSize;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  attr[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[1].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 2;
+  return cudaLaunchKernelEx(&cfg, k_cluster_program<T>, phases, nPhases, levels, coarseInv, coarseInvF, coarseN);
+}
+
+template int cluster_program_size<double>();
+template int cluster_program_size<float>();
+template cudaError_t run_cluster_program<double>(const Phase*, int, const ProgLevel<double>*, const double*,
+                                                 const float*, int, int, cudaStream_t);
+template cudaError_t run_cluster_program<float>(const Phase*, int, const ProgLevel<float>*, const double*,
+                                                const float*, int, int, cudaStream_t);
 template int cycle_program_max_grid<double>();
 template int cycle_program_max_grid<float>();
 template cudaError_t run_cycle_program<double>(const Phase*, int, const ProgLevel<double>*, const double*, int,

@@ -76,6 +76,18 @@ template <class T>
 int cycle_program_max_grid();
 
 constexpr int kProgramBlock = 512;
+constexpr int kClusterBlock = 1024;
+
+// The phase list run by a single thread-block cluster of clusterSize CTAs
+// (hardware cluster barrier between phases). coarseInvF, when set, is the
+// FP32 copy of the coarsest inverse used by dense phases.
+template <class T>
+cudaError_t run_cluster_program(const Phase* phases, int nPhases, const ProgLevel<T>* levels,
+                                const double* coarseInv, const float* coarseInvF, int coarseN, int clusterSize,
+                                cudaStream_t st);
+// largest usable cluster size (16 or 8), 0 if none
+template <class T>
+int cluster_program_size();
 
 }  // namespace dev
 }  // namespace fvm

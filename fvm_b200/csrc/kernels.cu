@@ -45,36 +45,94 @@ __device__ __forceinline__ double block_sum(double v) {
   return v;
 }
 
-template <class T>
-__device__ __forceinline__ T row_sum(const SellView<T>& a, int s, int lane, const T* __restrict__ x,
-                                     T sum) {
-  const int o = a.sliceOff[s];
-  const int w = (a.sliceOff[s + 1] - o) >> 5;
-  for (int k = 0; k < w; k++) {
-    const int e = o + (k << 5) + lane;
-    sum = sum + a.vals[e] * x[a.cols[e]];
-  }
+// Up to K entries of a row: every column and value load is issued, then
+// every x gather, then the products are accumulated in stored order -- two
+// dependent round trips to memory for the whole chunk.
+template <class T, int K>
+__device__ __forceinline__ T row_chunk(const SellView<T>& a, int e0, int cnt, const T* __restrict__ x, T sum) {
+  int c[K];
+  T v[K];
+  T xv[K];
+#pragma unroll
+  for (int k = 0; k < K; k++)
+    if (k < cnt) {
+      c[k] = a.cols[e0 + (k << 5)];
+      v[k] = a.vals[e0 + (k << 5)];
+    }
+#pragma unroll
+  for (int k = 0; k < K; k++)
+    if (k < cnt) xv[k] = x[c[k]];
+#pragma unroll
+  for (int k = 0; k < K; k++)
+    if (k < cnt) sum = sum + v[k] * xv[k];
   return sum;
+}
+
+// Sum over one row of a slice (m = the slice's packed metadata) in stored
+// order. Coarse-level rows hold 10-20 entries and their passes are latency
+// bound, so the row is processed in chunks of 16 with all loads of a chunk
+// in flight together; the summation order is the stored order.
+template <class T>
+__device__ __forceinline__ T row_sum(const SellView<T>& a, const int4 m, int lane, const T* __restrict__ x,
+                                     T sum) {
+  const int o = m.z + lane;
+  const int w = m.w;
+  if constexpr (sizeof(T) == 4) {
+    if (w <= 8) return row_chunk<T, 8>(a, o, w, x, sum);
+    for (int k0 = 0; k0 < w; k0 += 16) sum = row_chunk<T, 16>(a, o + (k0 << 5), min(16, w - k0), x, sum);
+    return sum;
+  } else {
+    // FP64: four entries in flight (measured faster than 8-entry chunks,
+    // which raised register use and cut occupancy on the finest level)
+    int k = 0;
+    for (; k + 4 <= w; k += 4) sum = row_chunk<T, 4>(a, o + (k << 5), 4, x, sum);
+    if (k < w) sum = row_chunk<T, 4>(a, o + (k << 5), w - k, x, sum);
+    return sum;
+  }
+}
+
+
+// Programmatic dependent launch: every hot-path kernel lets the next
+// kernel in the stream be scheduled as soon as all of its own blocks are
+// running (launch_dependents), and waits for its predecessor's completion
+// and memory before touching any data (griddepcontrol.wait). The launch
+// latency of the next kernel then overlaps this one. Kernels launched
+// without the attribute see both instructions as no-ops.
+#define FVM_PDL()                                                  \
+  do {                                                             \
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); \
+    asm volatile("griddepcontrol.wait;" ::: "memory");             \
+  } while (0)
+
+template <class T>
+__global__ void k_zero(int n, T* x) {
+  FVM_PDL();
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) x[i] = T(0);
 }
 
 // ---------------------------------------------------------------------------
 template <class T>
 __global__ void k_gs_color(SellView<T> a, int s0, int s1, T* x, const T* __restrict__ b) {
+  FVM_PDL();
   const int s = s0 + blockIdx.x * kSlicesPerBlock + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
-  if (s >= s1 || lane >= a.sliceRows[s]) return;
-  const int i = a.sliceRow[s] + lane;
-  const T sum = row_sum(a, s, lane, x, b[i]);
+  if (s >= s1) return;
+  const int4 m = a.meta[s];
+  if (lane >= m.y) return;
+  const int i = m.x + lane;
+  const T sum = row_sum(a, m, lane, x, b[i]);
   x[i] = -sum / a.diag[i];
 }
 
 template <class T>
 __global__ void k_gs_sequential(SellView<T> a, T* x, const T* __restrict__ b, int reverse) {
+  FVM_PDL();
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   for (int t = 0; t < a.n; t++) {
     const int i = reverse ? a.n - 1 - t : t;
     const int s = i >> 5, lane = i & 31;  // one colour: slices are consecutive 32-row blocks
-    const T sum = row_sum(a, s, lane, x, b[i]);
+    const T sum = row_sum(a, a.meta[s], lane, x, b[i]);
     x[i] = -sum / a.diag[i];
   }
 }
@@ -82,26 +140,33 @@ __global__ void k_gs_sequential(SellView<T> a, T* x, const T* __restrict__ b, in
 template <class T>
 __global__ void k_jacobi(SellView<T> a, int nSlices, const T* __restrict__ xold, T* xnew,
                          const T* __restrict__ b) {
+  FVM_PDL();
   const int s = blockIdx.x * kSlicesPerBlock + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
-  if (s >= nSlices || lane >= a.sliceRows[s]) return;
-  const int i = a.sliceRow[s] + lane;
-  const T sum = row_sum(a, s, lane, xold, b[i]);
+  if (s >= nSlices) return;
+  const int4 m = a.meta[s];
+  if (lane >= m.y) return;
+  const int i = m.x + lane;
+  const T sum = row_sum(a, m, lane, xold, b[i]);
   xnew[i] = -sum / a.diag[i];
 }
 
 template <class T>
 __global__ void k_residual(SellView<T> a, int nSlices, const T* __restrict__ x,
                            const T* __restrict__ b, T* r, double* partials) {
+  FVM_PDL();
   const int s = blockIdx.x * kSlicesPerBlock + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
   double l1 = 0.0;
-  if (s < nSlices && lane < a.sliceRows[s]) {
-    const int i = a.sliceRow[s] + lane;
-    // reference order: r = b + d x, then r += a_ij x_j
-    const T ri = row_sum(a, s, lane, x, b[i] + a.diag[i] * x[i]);
-    r[i] = ri;
-    l1 = fabs((double)ri);
+  if (s < nSlices) {
+    const int4 m = a.meta[s];
+    if (lane < m.y) {
+      const int i = m.x + lane;
+      // reference order: r = b + d x, then r += a_ij x_j
+      const T ri = row_sum(a, m, lane, x, b[i] + a.diag[i] * x[i]);
+      r[i] = ri;
+      l1 = fabs((double)ri);
+    }
   }
   if (partials) {
     const double t = block_sum(l1);
@@ -126,16 +191,20 @@ __global__ void k_csr_residual(int n, const int* __restrict__ row, const int* __
 }
 
 __global__ void k_spmv(SellView<double> a, int nSlices, const double* __restrict__ x, double* y) {
+  FVM_PDL();
   const int s = blockIdx.x * kSlicesPerBlock + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
-  if (s >= nSlices || lane >= a.sliceRows[s]) return;
-  const int i = a.sliceRow[s] + lane;
-  y[i] = row_sum(a, s, lane, x, a.diag[i] * x[i]);
+  if (s >= nSlices) return;
+  const int4 m = a.meta[s];
+  if (lane >= m.y) return;
+  const int i = m.x + lane;
+  y[i] = row_sum(a, m, lane, x, a.diag[i] * x[i]);
 }
 
 template <class T>
 __global__ void k_restrict(int nc, const int* __restrict__ c2fRow, const int* __restrict__ c2fCol,
                            const T* __restrict__ r, T* bc) {
+  FVM_PDL();
   const int I = blockIdx.x * blockDim.x + threadIdx.x;
   if (I >= nc) return;
   T s = T(0);
@@ -148,22 +217,25 @@ __global__ void k_restrict(int nc, const int* __restrict__ c2fRow, const int* __
 template <class T>
 __global__ void k_residual_restrict(SellView<T> a, const int* __restrict__ rowSlice, int nc,
                                     const int* __restrict__ c2fRow, const int* __restrict__ c2fCol,
-                                    const T* __restrict__ x, const T* __restrict__ b, T* bc) {
+                                    const T* __restrict__ x, const T* __restrict__ b, T* bc, T* xc) {
+  FVM_PDL();
   const int I = blockIdx.x * blockDim.x + threadIdx.x;
   if (I >= nc) return;
   T s = T(0);
   for (int k = c2fRow[I]; k < c2fRow[I + 1]; k++) {
     const int i = c2fCol[k];
-    const int sl = rowSlice[i];
-    const int lane = i - a.sliceRow[sl];
-    const T ri = row_sum(a, sl, lane, x, b[i] + a.diag[i] * x[i]);
+    const int4 m = a.meta[rowSlice[i]];
+    const int lane = i - m.x;
+    const T ri = row_sum(a, m, lane, x, b[i] + a.diag[i] * x[i]);
     s = s + ri;
   }
   bc[I] = s;
+  if (xc) xc[I] = T(0);
 }
 
 template <class T>
 __global__ void k_prolong(int n, const int* __restrict__ ci, const T* __restrict__ xc, T* x) {
+  FVM_PDL();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const int c = ci[i];
@@ -172,6 +244,7 @@ __global__ void k_prolong(int n, const int* __restrict__ ci, const T* __restrict
 
 template <class T>
 __global__ void k_dense_solve(int n, const double* __restrict__ ainv, const T* __restrict__ b, T* x) {
+  FVM_PDL();
   // one warp per row
   const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
@@ -182,15 +255,104 @@ __global__ void k_dense_solve(int n, const double* __restrict__ ainv, const T* _
   if (lane == 0) x[row] = (T)(-s);
 }
 
+__global__ void k_dense_solve_f32(int n, const float* __restrict__ ainv, const float* __restrict__ b,
+                                  float* x) {
+  FVM_PDL();
+  const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (row >= n) return;
+  float s = 0.0f;
+  for (int j = lane; j < n; j += 32) s += ainv[(size_t)row * n + j] * b[j];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if (lane == 0) x[row] = -s;
+}
+
+// Gauss-Jordan step k on the augmented matrix W = [A | I] (n x 2n): pick
+// the largest |W[r][k]|, r >= k, swap it into row k, record the pivot and
+// the column factors f[i] = W[i][k] (i != k) for the elimination.
+__global__ void k_gj_pivot(int n, int k, double* W, double* scratch) {
+  __shared__ double sv[1024];
+  __shared__ int si[1024];
+  const int w2 = 2 * n;
+  double best = -1.0;
+  int bi = k;
+  for (int r = k + threadIdx.x; r < n; r += blockDim.x) {
+    const double v = fabs(W[(size_t)r * w2 + k]);
+    if (v > best) {
+      best = v;
+      bi = r;
+    }
+  }
+  sv[threadIdx.x] = best;
+  si[threadIdx.x] = bi;
+  __syncthreads();
+  for (int o = blockDim.x >> 1; o > 0; o >>= 1) {
+    if (threadIdx.x < o) {
+      const double v2 = sv[threadIdx.x + o];
+      const int i2 = si[threadIdx.x + o];
+      if (v2 > sv[threadIdx.x] || (v2 == sv[threadIdx.x] && i2 < si[threadIdx.x])) {
+        sv[threadIdx.x] = v2;
+        si[threadIdx.x] = i2;
+      }
+    }
+    __syncthreads();
+  }
+  const int p = si[0];
+  if (p != k)
+    for (int j = threadIdx.x; j < w2; j += blockDim.x) {
+      const double t = W[(size_t)k * w2 + j];
+      W[(size_t)k * w2 + j] = W[(size_t)p * w2 + j];
+      W[(size_t)p * w2 + j] = t;
+    }
+  __syncthreads();
+  if (threadIdx.x == 0) scratch[n] = W[(size_t)k * w2 + k];
+  for (int i = threadIdx.x; i < n; i += blockDim.x) scratch[i] = (i == k) ? 0.0 : W[(size_t)i * w2 + k];
+}
+
+__global__ void k_gj_scale(int n, int k, double* W, const double* scratch) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j < 2 * n) W[(size_t)k * 2 * n + j] = W[(size_t)k * 2 * n + j] / scratch[n];
+}
+
+__global__ void k_gj_eliminate(int n, int k, double* W, const double* scratch) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = blockIdx.y;
+  if (j >= 2 * n || i == k) return;
+  const double f = scratch[i];
+  if (f != 0.0) W[(size_t)i * 2 * n + j] = W[(size_t)i * 2 * n + j] - f * W[(size_t)k * 2 * n + j];
+}
+
+__global__ void k_gj_init(int n, const double* __restrict__ a, double* W) {
+  const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (size_t)n * 2 * n) return;
+  const int i = (int)(t / (2 * n)), j = (int)(t % (2 * n));
+  W[t] = j < n ? a[(size_t)i * n + j] : (j - n == i ? 1.0 : 0.0);
+}
+
+__global__ void k_gj_extract(int n, const double* __restrict__ W, double* inv) {
+  const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (size_t)n * n) return;
+  const int i = (int)(t / n), j = (int)(t % n);
+  inv[t] = W[(size_t)i * 2 * n + n + j];
+}
+
+__global__ void k_cast_d2f_big(size_t n, const double* __restrict__ a, float* b) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) b[i] = (float)a[i];
+}
+
 __global__ void k_convert_d2f(int n, const double* __restrict__ a, float* b) {
+  FVM_PDL();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) b[i] = (float)a[i];
 }
 __global__ void k_add_f2d(int n, const float* __restrict__ a, double* b) {
+  FVM_PDL();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) b[i] = b[i] + (double)a[i];
 }
 __global__ void k_l1_partials(int n, const double* __restrict__ a, double* partials) {
+  FVM_PDL();
   double s = 0.0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) s += fabs(a[i]);
   s = block_sum(s);
@@ -198,38 +360,46 @@ __global__ void k_l1_partials(int n, const double* __restrict__ a, double* parti
 }
 __global__ void k_dot_partials(int n, const double* __restrict__ a, const double* __restrict__ b,
                                double* partials) {
+  FVM_PDL();
   double s = 0.0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) s += a[i] * b[i];
   s = block_sum(s);
   if (threadIdx.x == 0) partials[blockIdx.x] = s;
 }
 __global__ void k_sum_partials(int np, const double* __restrict__ p, double* out) {
+  FVM_PDL();
   double s = 0.0;
   for (int i = threadIdx.x; i < np; i += blockDim.x) s += p[i];
   s = block_sum(s);
   if (threadIdx.x == 0) out[0] = s;
 }
 __global__ void k_scalar_div(const double* num, const double* den, double* out) {
+  FVM_PDL();
   out[0] = num[0] / den[0];
 }
 __global__ void k_scalar_ratio_product(const double* a, const double* b, const double* c,
                                        const double* d, double* out) {
+  FVM_PDL();
   out[0] = (a[0] / b[0]) * (c[0] / d[0]);
 }
 __global__ void k_axpy_dev(int n, const double* s, double sign, const double* __restrict__ x, double* y) {
+  FVM_PDL();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) y[i] = y[i] + (sign * s[0]) * x[i];
 }
 __global__ void k_xpby_dev(int n, const double* __restrict__ z, const double* beta, double* p) {
+  FVM_PDL();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) p[i] = p[i] * beta[0] + z[i];
 }
 __global__ void k_bicg_p(int n, const double* __restrict__ r, const double* __restrict__ v,
                          const double* omega, const double* beta, double* p) {
+  FVM_PDL();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) p[i] = (p[i] - omega[0] * v[i]) * beta[0] + r[i];
 }
 __global__ void k_copy_d(int n, const double* __restrict__ a, double* b) {
+  FVM_PDL();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) b[i] = a[i];
 }
@@ -266,6 +436,7 @@ __global__ void k_face_coefficients(FaceGeom g, const double* __restrict__ k, do
 
 __global__ void k_gradient(int nCells, const int* __restrict__ row, const int* __restrict__ col,
                            const double* __restrict__ w, const double* __restrict__ x, double* grad) {
+  FVM_PDL();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nCells) return;
   double g0 = 0.0, g1 = 0.0, g2 = 0.0;
@@ -283,6 +454,7 @@ __global__ void k_gradient(int nCells, const int* __restrict__ row, const int* _
 
 __global__ void k_ghost_gradient(int nB, const int* __restrict__ bFaces, const int* __restrict__ fc,
                                  double* grad) {
+  FVM_PDL();
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= nB) return;
   const int f = bFaces[t];
@@ -293,6 +465,7 @@ __global__ void k_ghost_gradient(int nB, const int* __restrict__ bFaces, const i
 __global__ void k_face_flux(FaceGeom g, const double* __restrict__ coeff,
                             const double* __restrict__ sec, const double* __restrict__ grad,
                             const double* __restrict__ x, double* flux) {
+  FVM_PDL();
   const int f = blockIdx.x * blockDim.x + threadIdx.x;
   if (f >= g.nFaces) return;
   const int c0 = g.faceCells[2 * f], c1 = g.faceCells[2 * f + 1];
@@ -313,6 +486,7 @@ __global__ void k_assemble_rhs(int nCells, CellFaceView cf, const int* __restric
                                const double* __restrict__ xN1, BoundaryData bd,
                                const int* __restrict__ bIndexOfFace, double* x, double* bGhost,
                                const int* __restrict__ perm, double* b) {
+  FVM_PDL();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nCells) return;
   // DiffusionDiscretization: r0 += flux, r1 -= flux, faces ascending
@@ -387,6 +561,7 @@ __global__ void k_cast_d2f(int n, const double* __restrict__ a, float* b) {
 
 __global__ void k_update_self(int nCells, const int* __restrict__ perm, const double* __restrict__ delta,
                               double* x) {
+  FVM_PDL();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < nCells) x[i] = x[i] + delta[perm[i]];
 }
@@ -398,6 +573,7 @@ __global__ void k_update_ghosts(BoundaryData bd, const int* __restrict__ perm,
                                 const double* __restrict__ delta, const int* __restrict__ fc,
                                 const double* __restrict__ coeff, const double* __restrict__ bGhost,
                                 double* x) {
+  FVM_PDL();
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= bd.nBFaces || bd.kind[t] != 1) return;
   const int f = bd.bFace[t];
@@ -411,23 +587,40 @@ __global__ void k_update_ghosts(BoundaryData bd, const int* __restrict__ perm,
 
 // ---------------------------------------------------------------------------
 // wrappers
+
+namespace {
+template <typename... KArgs, typename... Args>
+void pdl_launch(void (*kernel)(KArgs...), dim3 grid, dim3 block, cudaStream_t st, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+}
+}  // namespace
 template <class T>
 void gs_color(const SellView<T>& a, int s0, int s1, T* x, const T* b, cudaStream_t st) {
   if (s1 <= s0) return;
-  k_gs_color<T><<<ceil_div(s1 - s0, kSlicesPerBlock), kBlock, 0, st>>>(a, s0, s1, x, b);
+  pdl_launch(k_gs_color<T>, ceil_div(s1 - s0, kSlicesPerBlock), kBlock, st, a, s0, s1, x, b);
 }
 template <class T>
 void gs_sequential(const SellView<T>& a, T* x, const T* b, bool reverse, cudaStream_t st) {
-  k_gs_sequential<T><<<1, 32, 0, st>>>(a, x, b, reverse ? 1 : 0);
+  pdl_launch(k_gs_sequential<T>, 1, 32, st, a, x, b, reverse ? 1 : 0);
 }
 template <class T>
 void jacobi(const SellView<T>& a, int nSlices, const T* xold, T* xnew, const T* b, cudaStream_t st) {
-  k_jacobi<T><<<ceil_div(nSlices, kSlicesPerBlock), kBlock, 0, st>>>(a, nSlices, xold, xnew, b);
+  pdl_launch(k_jacobi<T>, ceil_div(nSlices, kSlicesPerBlock), kBlock, st, a, nSlices, xold, xnew, b);
 }
 template <class T>
 void residual(const SellView<T>& a, int nSlices, const T* x, const T* b, T* r, double* partials,
               cudaStream_t st) {
-  k_residual<T><<<ceil_div(nSlices, kSlicesPerBlock), kBlock, 0, st>>>(a, nSlices, x, b, r, partials);
+  pdl_launch(k_residual<T>, ceil_div(nSlices, kSlicesPerBlock), kBlock, st, a, nSlices, x, b, r, partials);
 }
 int reduce_blocks(int nSlices) { return ceil_div(nSlices, kSlicesPerBlock); }
 int csr_residual_blocks(int n) { return ceil_div(n, kBlock); }
@@ -436,66 +629,89 @@ void csr_residual(int n, const int* row, const int* col, const double* diag, con
   k_csr_residual<<<csr_residual_blocks(n), kBlock, 0, st>>>(n, row, col, diag, off, x, b, r, partials);
 }
 void csr_residual_finish(int nPartials, const double* partials, double* l1, cudaStream_t st) {
-  k_sum_partials<<<1, 1024, 0, st>>>(nPartials, partials, l1);
+  pdl_launch(k_sum_partials, 1, 1024, st, nPartials, partials, l1);
 }
 void spmv(const SellView<double>& a, int nSlices, const double* x, double* y, cudaStream_t st) {
-  k_spmv<<<ceil_div(nSlices, kSlicesPerBlock), kBlock, 0, st>>>(a, nSlices, x, y);
+  pdl_launch(k_spmv, ceil_div(nSlices, kSlicesPerBlock), kBlock, st, a, nSlices, x, y);
 }
 template <class T>
 void restrict_sum(int nc, const int* c2fRow, const int* c2fCol, const T* r, T* bc, cudaStream_t st) {
-  k_restrict<T><<<ceil_div(nc, kBlock), kBlock, 0, st>>>(nc, c2fRow, c2fCol, r, bc);
+  pdl_launch(k_restrict<T>, ceil_div(nc, kBlock), kBlock, st, nc, c2fRow, c2fCol, r, bc);
 }
 template <class T>
 void residual_restrict(const SellView<T>& a, const int* rowSlice, int nc, const int* c2fRow,
-                       const int* c2fCol, const T* x, const T* b, T* bc, cudaStream_t st) {
-  k_residual_restrict<T><<<ceil_div(nc, kBlock), kBlock, 0, st>>>(a, rowSlice, nc, c2fRow, c2fCol, x, b, bc);
+                       const int* c2fCol, const T* x, const T* b, T* bc, T* xc, cudaStream_t st) {
+  pdl_launch(k_residual_restrict<T>, ceil_div(nc, kBlock), kBlock, st, a, rowSlice, nc, c2fRow, c2fCol, x, b, bc, xc);
+}
+template <class T>
+void zero(int n, T* x, cudaStream_t st) {
+  pdl_launch(k_zero<T>, ceil_div(n, kBlock), kBlock, st, n, x);
 }
 template <class T>
 void prolong(int n, const int* ci, const T* xc, T* x, cudaStream_t st) {
-  k_prolong<T><<<ceil_div(n, kBlock), kBlock, 0, st>>>(n, ci, xc, x);
+  pdl_launch(k_prolong<T>, ceil_div(n, kBlock), kBlock, st, n, ci, xc, x);
 }
 template <class T>
 void dense_solve(int n, const double* ainv, const T* b, T* x, cudaStream_t st) {
-  k_dense_solve<T><<<ceil_div(n, kBlock / 32), kBlock, 0, st>>>(n, ainv, b, x);
+  pdl_launch(k_dense_solve<T>, ceil_div(n, kBlock / 32), kBlock, st, n, ainv, b, x);
+}
+void dense_solve_f32(int n, const float* ainv, const float* b, float* x, cudaStream_t st) {
+  pdl_launch(k_dense_solve_f32, ceil_div(n, kBlock / 32), kBlock, st, n, ainv, b, x);
+}
+void gauss_jordan_inverse(int n, const double* a, double* work, double* inv, double* scratch,
+                          cudaStream_t st) {
+  const size_t aug = (size_t)n * 2 * n;
+  k_gj_init<<<(unsigned)((aug + kBlock - 1) / kBlock), kBlock, 0, st>>>(n, a, work);
+  const dim3 eg(ceil_div(2 * n, kBlock), n);
+  for (int k = 0; k < n; k++) {
+    k_gj_pivot<<<1, 1024, 0, st>>>(n, k, work, scratch);
+    k_gj_scale<<<ceil_div(2 * n, kBlock), kBlock, 0, st>>>(n, k, work, scratch);
+    k_gj_eliminate<<<eg, kBlock, 0, st>>>(n, k, work, scratch);
+  }
+  const size_t nn = (size_t)n * n;
+  k_gj_extract<<<(unsigned)((nn + kBlock - 1) / kBlock), kBlock, 0, st>>>(n, work, inv);
+}
+void cast_d2f(size_t n, const double* a, float* b, cudaStream_t st) {
+  k_cast_d2f_big<<<(unsigned)((n + kBlock - 1) / kBlock), kBlock, 0, st>>>(n, a, b);
 }
 void convert_d2f(int n, const double* a, float* b, cudaStream_t st) {
-  k_convert_d2f<<<ceil_div(n, kBlock), kBlock, 0, st>>>(n, a, b);
+  pdl_launch(k_convert_d2f, ceil_div(n, kBlock), kBlock, st, n, a, b);
 }
 void add_f2d(int n, const float* a, double* b, cudaStream_t st) {
-  k_add_f2d<<<ceil_div(n, kBlock), kBlock, 0, st>>>(n, a, b);
+  pdl_launch(k_add_f2d, ceil_div(n, kBlock), kBlock, st, n, a, b);
 }
 int vec_blocks(int n) {
   const int b = ceil_div(n, kBlock);
   return b < kReduceBlocks ? (b < 1 ? 1 : b) : kReduceBlocks;
 }
 void l1_partials(int n, const double* a, double* partials, cudaStream_t st) {
-  k_l1_partials<<<vec_blocks(n), kBlock, 0, st>>>(n, a, partials);
+  pdl_launch(k_l1_partials, vec_blocks(n), kBlock, st, n, a, partials);
 }
 void dot_partials(int n, const double* a, const double* b, double* partials, cudaStream_t st) {
-  k_dot_partials<<<vec_blocks(n), kBlock, 0, st>>>(n, a, b, partials);
+  pdl_launch(k_dot_partials, vec_blocks(n), kBlock, st, n, a, b, partials);
 }
 void sum_partials(int np, const double* partials, double* out, cudaStream_t st) {
-  k_sum_partials<<<1, 1024, 0, st>>>(np, partials, out);
+  pdl_launch(k_sum_partials, 1, 1024, st, np, partials, out);
 }
 void scalar_div(const double* num, const double* den, double* out, cudaStream_t st) {
-  k_scalar_div<<<1, 1, 0, st>>>(num, den, out);
+  pdl_launch(k_scalar_div, 1, 1, st, num, den, out);
 }
 void scalar_ratio_product(const double* a, const double* b, const double* c, const double* d,
                           double* out, cudaStream_t st) {
-  k_scalar_ratio_product<<<1, 1, 0, st>>>(a, b, c, d, out);
+  pdl_launch(k_scalar_ratio_product, 1, 1, st, a, b, c, d, out);
 }
 void axpy_dev(int n, const double* s, double sign, const double* x, double* y, cudaStream_t st) {
-  k_axpy_dev<<<ceil_div(n, kBlock), kBlock, 0, st>>>(n, s, sign, x, y);
+  pdl_launch(k_axpy_dev, ceil_div(n, kBlock), kBlock, st, n, s, sign, x, y);
 }
 void xpby_dev(int n, const double* z, const double* beta, double* p, cudaStream_t st) {
-  k_xpby_dev<<<ceil_div(n, kBlock), kBlock, 0, st>>>(n, z, beta, p);
+  pdl_launch(k_xpby_dev, ceil_div(n, kBlock), kBlock, st, n, z, beta, p);
 }
 void bicg_p_update(int n, const double* r, const double* v, const double* omega, const double* beta,
                    double* p, cudaStream_t st) {
-  k_bicg_p<<<ceil_div(n, kBlock), kBlock, 0, st>>>(n, r, v, omega, beta, p);
+  pdl_launch(k_bicg_p, ceil_div(n, kBlock), kBlock, st, n, r, v, omega, beta, p);
 }
 void copy_d(int n, const double* a, double* b, cudaStream_t st) {
-  k_copy_d<<<ceil_div(n, kBlock), kBlock, 0, st>>>(n, a, b);
+  pdl_launch(k_copy_d, ceil_div(n, kBlock), kBlock, st, n, a, b);
 }
 
 void face_coefficients(const FaceGeom& g, const double* k, double* coeff, double* secCoeff,
@@ -504,21 +720,21 @@ void face_coefficients(const FaceGeom& g, const double* k, double* coeff, double
 }
 void gradient(int nCells, const int* ccRow, const int* ccCol, const double* w, const double* x,
               double* grad, cudaStream_t st) {
-  k_gradient<<<ceil_div(nCells, kBlock), kBlock, 0, st>>>(nCells, ccRow, ccCol, w, x, grad);
+  pdl_launch(k_gradient, ceil_div(nCells, kBlock), kBlock, st, nCells, ccRow, ccCol, w, x, grad);
 }
 void ghost_gradient(int nB, const int* bFaces, const int* faceCells, double* grad, cudaStream_t st) {
-  if (nB > 0) k_ghost_gradient<<<ceil_div(nB, kBlock), kBlock, 0, st>>>(nB, bFaces, faceCells, grad);
+  if (nB > 0) pdl_launch(k_ghost_gradient, ceil_div(nB, kBlock), kBlock, st, nB, bFaces, faceCells, grad);
 }
 void face_flux(const FaceGeom& g, const double* coeff, const double* secCoeff, const double* grad,
                const double* x, double* flux, cudaStream_t st) {
-  k_face_flux<<<ceil_div(g.nFaces, kBlock), kBlock, 0, st>>>(g, coeff, secCoeff, grad, x, flux);
+  pdl_launch(k_face_flux, ceil_div(g.nFaces, kBlock), kBlock, st, g, coeff, secCoeff, grad, x, flux);
 }
 void assemble_rhs(int nCells, const CellFaceView& cf, const int* faceCells, const double* flux,
                   const double* coeff, const double* faceAreaMag, const double* vol,
                   const double* source, const double* rhoVdt, const double* xN1,
                   const BoundaryData& bd, const int* bIndexOfFace, double* x, double* bGhost,
                   const int* perm, double* b, cudaStream_t st) {
-  k_assemble_rhs<<<ceil_div(nCells, kBlock), kBlock, 0, st>>>(nCells, cf, faceCells, flux, coeff,
+  pdl_launch(k_assemble_rhs, ceil_div(nCells, kBlock), kBlock, st, nCells, cf, faceCells, flux, coeff,
                                                               faceAreaMag, vol, source, rhoVdt, xN1,
                                                               bd, bIndexOfFace, x, bGhost, perm, b);
 }
@@ -538,9 +754,9 @@ void cast_d2f_vals(int n, const double* a, float* b, cudaStream_t st) {
 void update_solution(int nCells, const int* perm, const double* delta, const BoundaryData& bd,
                      const int* faceCells, const double* coeff, const double* bGhost, double* x,
                      cudaStream_t st) {
-  k_update_self<<<ceil_div(nCells, kBlock), kBlock, 0, st>>>(nCells, perm, delta, x);
+  pdl_launch(k_update_self, ceil_div(nCells, kBlock), kBlock, st, nCells, perm, delta, x);
   if (bd.nBFaces > 0)
-    k_update_ghosts<<<ceil_div(bd.nBFaces, kBlock), kBlock, 0, st>>>(bd, perm, delta, faceCells, coeff,
+    pdl_launch(k_update_ghosts, ceil_div(bd.nBFaces, kBlock), kBlock, st, bd, perm, delta, faceCells, coeff,
                                                                      bGhost, x);
 }
 
@@ -552,7 +768,8 @@ void update_solution(int nCells, const int* perm, const double* delta, const Bou
   template void residual<T>(const SellView<T>&, int, const T*, const T*, T*, double*, cudaStream_t); \
   template void restrict_sum<T>(int, const int*, const int*, const T*, T*, cudaStream_t);        \
   template void residual_restrict<T>(const SellView<T>&, const int*, int, const int*, const int*,   \
-                                     const T*, const T*, T*, cudaStream_t);                      \
+                                     const T*, const T*, T*, T*, cudaStream_t);                  \
+  template void zero<T>(int, T*, cudaStream_t);                                                  \
   template void prolong<T>(int, const int*, const T*, T*, cudaStream_t);                         \
   template void dense_solve<T>(int, const double*, const T*, T*, cudaStream_t);
 FVM_INST(double)

@@ -18,6 +18,9 @@ struct SellView {
   const int* cols;
   const T* vals;
   const T* diag;
+  // per slice, packed for a single 16-byte load: first row, rows (<= 32),
+  // offset of its first entry, width (entries per row, padded)
+  const int4* meta;
 };
 
 // ---- smoothers -----------------------------------------------------------
@@ -56,10 +59,13 @@ void csr_residual_finish(int nPartials, const double* partials, double* l1, cuda
 // bc[I] = sum over fine rows i of aggregate I (ascending reference order) of r[i]
 template <class T>
 void restrict_sum(int nc, const int* c2fRow, const int* c2fCol, const T* r, T* bc, cudaStream_t st);
-// residual of the fine rows fused into the restriction (r never stored)
+// residual of the fine rows fused into the restriction (r never stored);
+// also zeroes the coarse x (xc may be null)
 template <class T>
 void residual_restrict(const SellView<T>& a, const int* rowSlice, int nc, const int* c2fRow,
-                       const int* c2fCol, const T* x, const T* b, T* bc, cudaStream_t st);
+                       const int* c2fCol, const T* x, const T* b, T* bc, T* xc, cudaStream_t st);
+template <class T>
+void zero(int n, T* x, cudaStream_t st);
 // x[i] += xc[ci[i]]
 template <class T>
 void prolong(int n, const int* ci, const T* xc, T* x, cudaStream_t st);
@@ -68,6 +74,15 @@ void prolong(int n, const int* ci, const T* xc, T* x, cudaStream_t st);
 // x = -Ainv b with a dense FP64 inverse (n x n, row-major)
 template <class T>
 void dense_solve(int n, const double* ainv, const T* b, T* x, cudaStream_t st);
+// same with an FP32 copy of the inverse (half the bytes; FP32 V-cycle)
+void dense_solve_f32(int n, const float* ainv, const float* b, float* x, cudaStream_t st);
+// Inverse of the dense n x n matrix a (row-major, FP64, device) by
+// Gauss-Jordan elimination with partial pivoting on the augmented n x 2n
+// matrix `work` (2 n^2 doubles); result in `inv` (n^2 doubles). scratch
+// needs n + 2 doubles. Returns false if a pivot is exactly zero.
+void gauss_jordan_inverse(int n, const double* a, double* work, double* inv, double* scratch,
+                          cudaStream_t st);
+void cast_d2f(size_t n, const double* a, float* b, cudaStream_t st);
 
 // ---- vector ops ------------------------------------------------------------
 void convert_d2f(int n, const double* a, float* b, cudaStream_t st);

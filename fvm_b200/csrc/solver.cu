@@ -2,11 +2,13 @@
 #include "solver.hpp"
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <cstdlib>
 #include <limits>
+#include <type_traits>
 
 namespace fvm {
 
@@ -18,13 +20,23 @@ namespace fvm {
   } while (0)
 
 // ---------------------------------------------------------------------------
-DeviceArena::~DeviceArena() { release(); }
+DeviceArena::~DeviceArena() {
+  release();
+  for (auto& kv : free_) cudaFree(kv.second);
+  free_.clear();
+}
 
 void* DeviceArena::alloc(size_t bytes) {
   void* p = nullptr;
   if (bytes == 0) bytes = 16;
-  CUDA_OK(cudaMalloc(&p, bytes));
-  ptrs_.push_back(p);
+  auto it = free_.find(bytes);
+  if (it != free_.end()) {
+    p = it->second;
+    free_.erase(it);
+  } else {
+    CUDA_OK(cudaMalloc(&p, bytes));
+  }
+  ptrs_.push_back({p, bytes});
   bytes_ += bytes;
   return p;
 }
@@ -34,7 +46,7 @@ void DeviceArena::copy_h2d(void* d, const void* h, size_t n) {
 }
 
 void DeviceArena::release() {
-  for (void* p : ptrs_) cudaFree(p);
+  for (auto& pb : ptrs_) free_.insert({pb.second, pb.first});
   ptrs_.clear();
   bytes_ = 0;
 }
@@ -46,6 +58,7 @@ void AmgHierarchy::release() {
   packed_.clear();
   ref_.clear();
   coarseInv_ = nullptr;
+  coarseInvF_ = nullptr;
 }
 
 std::vector<int> AmgHierarchy::sizes() const {
@@ -65,12 +78,23 @@ void AmgHierarchy::build(std::vector<RefLevel>& levels, int finestLocalSize, con
   ho.weightRatioThreshold = opt.weightRatioThreshold;
   ho.coarsestSize = opt.coarsestSize;
   ho.finestLocalSize = finestLocalSize;
+  const bool trace = getenv("FVM_TRACE") != nullptr;
+  auto t0 = std::chrono::steady_clock::now();
+  auto lap = [&](const char* what) {
+    if (!trace) return;
+    const auto t1 = std::chrono::steady_clock::now();
+    fprintf(stderr, "[fvm setup] %-28s %8.1f ms\n", what, std::chrono::duration<double, std::milli>(t1 - t0).count());
+    t0 = t1;
+  };
   std::vector<CSR> c2f;
   build_hierarchy(ref_, ho, c2f);
+  lap("aggregation + Galerkin");
   const int L = (int)ref_.size();
   packed_.resize(L);
   for (int l = 0; l < L; l++) pack_level(ref_[l], opt.ordering, packed_[l]);
+  lap("colouring + SELL packing");
   for (int l = 0; l + 1 < L; l++) pack_transfer(ref_[l], c2f[l], packed_[l], packed_[l + 1]);
+  lap("transfer maps");
 
   const bool mixed = opt.precision == kMixed;
   lv_.resize(L);
@@ -90,9 +114,13 @@ void AmgHierarchy::build(std::vector<RefLevel>& levels, int finestLocalSize, con
     d.vals = arena_.upload(p.vals);
     d.diag = arena_.upload(p.diag);
     std::vector<int> rs(p.n);
-    for (int s = 0; s < d.nSlices; s++)
+    std::vector<int4> meta(d.nSlices);
+    for (int s = 0; s < d.nSlices; s++) {
       for (int k = 0; k < p.sliceRows[s]; k++) rs[p.sliceRow[s] + k] = s;
+      meta[s] = make_int4(p.sliceRow[s], p.sliceRows[s], p.sliceOff[s], (p.sliceOff[s + 1] - p.sliceOff[s]) / 32);
+    }
     d.rowSlice = arena_.upload(rs);
+    d.meta = arena_.upload(meta);
     if (l + 1 < L) {
       d.nCoarse = packed_[l + 1].n;
       d.ci = arena_.upload(p.coarseIndex);
@@ -109,9 +137,10 @@ void AmgHierarchy::build(std::vector<RefLevel>& levels, int finestLocalSize, con
     d.nPartials = dev::reduce_blocks(d.nSlices);
     d.partials = (double*)arena_.alloc(sizeof(double) * (d.nPartials + 1));
     if (mixed) {
-      std::vector<float> vf(p.vals.begin(), p.vals.end()), df(p.diag.begin(), p.diag.end());
-      d.valsF = arena_.upload(vf);
-      d.diagF = arena_.upload(df);
+      d.valsF = (float*)arena_.alloc(sizeof(float) * p.vals.size());
+      d.diagF = (float*)arena_.alloc(sizeof(float) * p.diag.size());
+      dev::cast_d2f(p.vals.size(), d.vals, d.valsF, 0);
+      dev::cast_d2f(p.diag.size(), d.diag, d.diagF, 0);
       const size_t fb = (size_t)p.n * sizeof(float);
       d.xF = (float*)arena_.alloc(fb);
       d.bF = (float*)arena_.alloc(fb);
@@ -120,15 +149,49 @@ void AmgHierarchy::build(std::vector<RefLevel>& levels, int finestLocalSize, con
       CUDA_OK(cudaMemset(d.xF, 0, fb));
     }
   }
+  lap("uploads");
   if (opt.coarseSolver == kCoarseDirect) {
     const PackedLevel& c = packed_[L - 1];
-    FVM_REQUIRE(c.n <= 8192, kTooLarge,
-                "coarsest level too large for the dense direct solve; set coarsestSize");
-    std::vector<double> inv;
-    dense_inverse(c, inv);
-    coarseInv_ = arena_.upload(inv);
+    FVM_REQUIRE(c.n <= 4096, kTooLarge,
+                "coarsest level too large for the dense direct solve (max 4096 rows); set coarsestSize");
+    const size_t nn = (size_t)c.n * c.n;
+    if (c.n <= 128) {
+      std::vector<double> inv;
+      dense_inverse(c, inv);
+      coarseInv_ = arena_.upload(inv);
+    } else {
+      // dense copy of the level in its permuted numbering, inverted on the GPU
+      std::vector<double> a(nn, 0.0);
+      for (int p = 0; p < c.n; p++) a[(size_t)p * c.n + p] = c.diag[p];
+      for (size_t s = 0; s + 1 < c.sliceOff.size(); s++) {
+        const int w = (c.sliceOff[s + 1] - c.sliceOff[s]) / 32;
+        for (int l = 0; l < c.sliceRows[s]; l++)
+          for (int k = 0; k < w; k++) {
+            const size_t e = (size_t)c.sliceOff[s] + (size_t)k * 32 + l;
+            if (c.vals[e] != 0.0) a[(size_t)(c.sliceRow[s] + l) * c.n + c.cols[e]] += c.vals[e];
+          }
+      }
+      double* dA = arena_.upload(a);
+      DeviceArena tmp;
+      double* work = (double*)tmp.alloc(sizeof(double) * 2 * nn);
+      double* scratch = (double*)tmp.alloc(sizeof(double) * (c.n + 2));
+      coarseInv_ = (double*)arena_.alloc(sizeof(double) * nn);
+      dev::gauss_jordan_inverse(c.n, dA, work, coarseInv_, scratch, 0);
+      CUDA_OK(cudaDeviceSynchronize());
+    }
+    if (mixed) {
+      coarseInvF_ = (float*)arena_.alloc(sizeof(float) * nn);
+      dev::cast_d2f(nn, coarseInv_, coarseInvF_, 0);
+      CUDA_OK(cudaDeviceSynchronize());
+    }
+    lap("coarsest inverse");
   }
   buildProgram();
+  if (trace) {
+    fprintf(stderr, "[fvm setup] levels:");
+    for (int l = 0; l < L; l++) fprintf(stderr, " %d(%dc)", lv_[l].n, lv_[l].nColors);
+    fprintf(stderr, "\n");
+  }
 }
 
 void AmgHierarchy::genSweeps(int n, int l, std::vector<dev::Phase>& out) const {
@@ -172,17 +235,8 @@ void AmgHierarchy::genCycle(CycleType t, int l, std::vector<dev::Phase>& out) co
 
 void AmgHierarchy::buildProgram() {
   programReady_ = false;
-  // Opt-in (FVM_PERSISTENT_CYCLE=1): measured on B200 at 1.5M cells, a
-  // 296-block grid barrier per phase costs more than a graph-launched
-  // kernel per phase (3.8 vs 2.5 ms per FP32 V-cycle), so one launch per
-  // phase stays the default.
-  const char* env = getenv("FVM_PERSISTENT_CYCLE");
-  if (!env || env[0] != '1') return;
+  tailLevel_ = -1;
   if (opt_.ordering == kSequential && opt_.smootherType == kGaussSeidel) return;
-  phases_.clear();
-  genCycle(opt_.cycleType, 0, phases_);
-  if (phases_.empty()) return;
-  dPhases_ = arena_.upload(phases_);
   const int L = (int)lv_.size();
   std::vector<dev::ProgLevel<double>> p64(L);
   std::vector<dev::ProgLevel<float>> p32(L);
@@ -225,6 +279,44 @@ void AmgHierarchy::buildProgram() {
   }
   dProg64_ = arena_.upload(p64);
   if (opt_.precision == kMixed) dProg32_ = arena_.upload(p32);
+
+  // Coarse tail: from the first level (below the finest) with at most
+  // kTailRows rows down to the coarsest, a V-cycle is one cluster kernel.
+  // Those levels fit in L2 and their phases are latency bound; the
+  // cluster barrier between phases is far cheaper than a kernel launch.
+  // Off by default (FVM_TAIL_ROWS=<rows> enables): measured slower than one
+  // launch per phase at 1.5M cells (2.26 vs 1.37 ms per FP32 V-cycle).
+  int tailRows = 0;
+  if (const char* tr = getenv("FVM_TAIL_ROWS")) tailRows = atoi(tr);
+  if (opt_.cycleType == kVCycle && tailRows > 0) {
+    int lt = -1;
+    for (int l = 1; l < L; l++)
+      if (lv_[l].n <= tailRows) {
+        lt = l;
+        break;
+      }
+    const int cs = lt >= 0 ? (opt_.precision == kMixed ? dev::cluster_program_size<float>()
+                                                        : dev::cluster_program_size<double>())
+                           : 0;
+    if (lt >= 0 && cs > 0) {
+      tailPhases_.clear();
+      genCycle(kVCycle, lt, tailPhases_);
+      dTailPhases_ = arena_.upload(tailPhases_);
+      clusterSize_ = cs;
+      tailLevel_ = lt;
+    }
+  }
+
+  // Opt-in (FVM_PERSISTENT_CYCLE=1): the whole cycle as one cooperative
+  // kernel with grid barriers. Measured on B200 at 1.5M cells, a 296-block
+  // grid barrier per phase costs more than a kernel launch per phase (3.8 vs
+  // 2.5 ms per FP32 V-cycle), so it is not the default.
+  const char* env = getenv("FVM_PERSISTENT_CYCLE");
+  if (!env || env[0] != '1') return;
+  phases_.clear();
+  genCycle(opt_.cycleType, 0, phases_);
+  if (phases_.empty()) return;
+  dPhases_ = arena_.upload(phases_);
   dBarrier_ = (dev::BarrierState*)arena_.alloc(sizeof(dev::BarrierState));
   CUDA_OK(cudaMemset(dBarrier_, 0, sizeof(dev::BarrierState)));
   grid64_ = dev::cycle_program_max_grid<double>();
@@ -329,7 +421,22 @@ void AmgHierarchy::cycle(CycleType t, int l, cudaStream_t st) {
   const int L = (int)lv_.size();
   DevLevel& d = lv_[l];
   const bool coarsest = (l == L - 1);
+  if (l == tailLevel_ && t == kVCycle) {
+    if constexpr (std::is_same<T, float>::value)
+      CUDA_OK(dev::run_cluster_program<float>(dTailPhases_, (int)tailPhases_.size(), dProg32_, coarseInv_,
+                                              coarseInvF_, lv_[L - 1].n, clusterSize_, st));
+    else
+      CUDA_OK(dev::run_cluster_program<double>(dTailPhases_, (int)tailPhases_.size(), dProg64_, coarseInv_,
+                                               nullptr, lv_[L - 1].n, clusterSize_, st));
+    return;
+  }
   if (coarsest && coarseInv_) {
+    if constexpr (std::is_same<T, float>::value) {
+      if (coarseInvF_) {
+        dev::dense_solve_f32(d.n, coarseInvF_, d.bF, d.xF, st);
+        return;
+      }
+    }
     dev::dense_solve<T>(d.n, coarseInv_, vec_b<T>(d), vec_x<T>(d), st);
     return;
   }
@@ -337,8 +444,7 @@ void AmgHierarchy::cycle(CycleType t, int l, cudaStream_t st) {
   if (!coarsest) {
     DevLevel& c = lv_[l + 1];
     dev::residual_restrict<T>(view<T>(d), d.rowSlice, c.n, d.c2fRow, d.c2fCol, vec_x<T>(d),
-                              vec_b<T>(d), vec_b<T>(c), st);
-    CUDA_OK(cudaMemsetAsync(vec_x<T>(c), 0, sizeof(T) * (size_t)c.n, st));
+                              vec_b<T>(d), vec_b<T>(c), vec_x<T>(c), st);
     cycle<T>(t, l + 1, st);
     if (t == kWCycle)
       cycle<T>(kWCycle, l + 1, st);
@@ -353,13 +459,13 @@ void AmgHierarchy::apply(const double* r, double* z, cudaStream_t st) {
   DevLevel& d = lv_[0];
   if (opt_.precision == kMixed) {
     dev::convert_d2f(d.n, r, d.bF, st);
-    CUDA_OK(cudaMemsetAsync(d.xF, 0, sizeof(float) * (size_t)d.n, st));
+    dev::zero<float>(d.n, d.xF, st);
     runCycle<float>(st);
-    CUDA_OK(cudaMemsetAsync(z, 0, sizeof(double) * (size_t)d.n, st));
+    dev::zero<double>(d.n, z, st);
     dev::add_f2d(d.n, d.xF, z, st);
   } else {
     dev::copy_d(d.n, r, d.b, st);
-    CUDA_OK(cudaMemsetAsync(d.x, 0, sizeof(double) * (size_t)d.n, st));
+    dev::zero<double>(d.n, d.x, st);
     runCycle<double>(st);
     dev::copy_d(d.n, d.x, z, st);
   }
@@ -554,7 +660,7 @@ SolveReport LinearSolve::solveAMG(cudaStream_t st) {
     run(g1_, st, [&] {
       if (o.precision == kMixed) {
         dev::convert_d2f(n_, d.r, d.bF, st);
-        CUDA_OK(cudaMemsetAsync(d.xF, 0, sizeof(float) * (size_t)n_, st));
+        dev::zero<float>(n_, d.xF, st);
         h_.runCycle<float>(st);
         dev::add_f2d(n_, d.xF, d.x, st);
       } else {

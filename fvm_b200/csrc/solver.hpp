@@ -68,16 +68,20 @@ struct DevLevel {
   float *xF = nullptr, *bF = nullptr, *rF = nullptr, *tmpF = nullptr;
   double* partials = nullptr;
   int nPartials = 0;
+  int4* meta = nullptr;  // per slice: first row, rows, entry offset, width
   dev::SellView<double> view64() const {
-    return {n, sliceRow, sliceRows, sliceOff, cols, vals, diag};
+    return {n, sliceRow, sliceRows, sliceOff, cols, vals, diag, meta};
   }
   dev::SellView<float> view32() const {
-    return {n, sliceRow, sliceRows, sliceOff, cols, valsF, diagF};
+    return {n, sliceRow, sliceRows, sliceOff, cols, valsF, diagF, meta};
   }
   size_t entries = 0;
 };
 
-// Bytes of device memory allocated through this class (for reporting).
+// Device allocations of one owner. release() keeps the blocks for reuse by
+// later alloc() calls of the same size (a rebuilt AMG hierarchy on the same
+// mesh asks for the same sizes), so rebuilding does not pay cudaFree /
+// cudaMalloc again; the destructor frees everything.
 class DeviceArena {
  public:
   ~DeviceArena();
@@ -93,7 +97,8 @@ class DeviceArena {
 
  private:
   void copy_h2d(void* d, const void* h, size_t n);
-  std::vector<void*> ptrs_;
+  std::vector<std::pair<void*, size_t>> ptrs_;
+  std::multimap<size_t, void*> free_;
   size_t bytes_ = 0;
 };
 
@@ -144,12 +149,18 @@ class AmgHierarchy {
   std::vector<PackedLevel> packed_;
   std::vector<DevLevel> lv_;
   double* coarseInv_ = nullptr;  // dense inverse of the coarsest level
+  float* coarseInvF_ = nullptr;  // its FP32 copy for the FP32 cycle
   DeviceArena arena_;
   // persistent cycle program
   void buildProgram();
   void genCycle(CycleType t, int l, std::vector<dev::Phase>& out) const;
   void genSweeps(int n, int l, std::vector<dev::Phase>& out) const;
   bool programReady_ = false;
+  // coarse tail: levels >= tailLevel_ run as one cluster kernel per cycle
+  int tailLevel_ = -1;
+  int clusterSize_ = 0;
+  std::vector<dev::Phase> tailPhases_;
+  dev::Phase* dTailPhases_ = nullptr;
   std::vector<dev::Phase> phases_;
   dev::Phase* dPhases_ = nullptr;
   dev::ProgLevel<double>* dProg64_ = nullptr;

@@ -110,6 +110,7 @@ void create_coarse_level(const RefLevel& fine, RefLevel& coarse, CSR& c2f) {
   // parallel: a count pass, a prefix sum, a fill pass (rows are short, so a
   // linear search replaces the reference's marker array).
   coarse.n = nc;
+  coarse.symmetricPattern = fine.symmetricPattern;
   coarse.conn.nRows = nc;
   coarse.conn.row.assign(nc + 1, 0);
   auto visit = [&](int I, int* out) {
@@ -224,8 +225,11 @@ int greedy_in_order(const CSR& conn, const std::vector<int>& order, std::vector<
 }
 
 // Smallest-last ordering (Matula & Beck): repeatedly remove a vertex of
-// minimum remaining degree (lowest index among equals); colouring in the
-// reverse removal order needs at most degeneracy + 1 colours.
+// minimum remaining degree; colouring in the reverse removal order needs at
+// most degeneracy + 1 colours. Ties: each degree bucket is a list that
+// starts in ascending index order; a vertex whose degree drops moves to the
+// front of its new bucket, and the vertex removed is the front of the
+// lowest non-empty bucket.
 void smallest_last_order(const CSR& conn, std::vector<int>& order) {
   const int n = conn.nRows;
   std::vector<int> deg(n);
@@ -275,14 +279,64 @@ void smallest_last_order(const CSR& conn, std::vector<int>& order) {
 }  // namespace
 
 // Deterministic colouring for the multicolour smoothers: greedy in row
-// order and greedy in smallest-last order, keeping whichever needs fewer
-// colours (row order on a tie). Fewer colours mean fewer dependent passes.
-int multicolor(const CSR& conn, std::vector<int>& color) {
+// order; when that needs more than kFewColors colours, also greedy in
+// smallest-last order, keeping whichever needs fewer (row order on a tie).
+// Fewer colours mean fewer dependent passes per sweep; the smallest-last
+// pass costs several greedy passes and rarely improves a colouring that is
+// already this small (finest tetrahedral and hexahedral levels).
+bool pattern_is_symmetric(const CSR& a) {
+  for (int i = 0; i < a.nRows; i++)
+    for (int k = a.row[i]; k < a.row[i + 1]; k++) {
+      const int j = a.col[k];
+      bool found = false;
+      for (int q = a.row[j]; q < a.row[j + 1] && !found; q++) found = a.col[q] == i;
+      if (!found) return false;
+    }
+  return true;
+}
+
+bool symmetrize_pattern(const CSR& a, CSR& out) {
+  const int n = a.nRows;
+  // transpose, rows in ascending source order
+  std::vector<int> tr(n + 1, 0), tc(a.col.size());
+  for (int c : a.col) tr[c + 1]++;
+  for (int i = 0; i < n; i++) tr[i + 1] += tr[i];
+  {
+    std::vector<int> cur(tr.begin(), tr.end() - 1);
+    for (int i = 0; i < n; i++)
+      for (int k = a.row[i]; k < a.row[i + 1]; k++) tc[cur[a.col[k]]++] = i;
+  }
+  std::vector<int> mark(n, -1);
+  out.nRows = n;
+  out.row.assign(n + 1, 0);
+  out.col.clear();
+  out.col.reserve(2 * a.col.size());
+  bool extra = false;
+  for (int i = 0; i < n; i++) {
+    for (int k = a.row[i]; k < a.row[i + 1]; k++) {
+      out.col.push_back(a.col[k]);
+      mark[a.col[k]] = i;
+    }
+    for (int k = tr[i]; k < tr[i + 1]; k++)
+      if (mark[tc[k]] != i && tc[k] != i) {
+        out.col.push_back(tc[k]);
+        mark[tc[k]] = i;
+        extra = true;
+      }
+    out.row[i + 1] = (int)out.col.size();
+  }
+  return extra;
+}
+
+int multicolor(const CSR& connIn, std::vector<int>& color, bool symmetricPattern) {
+  CSR sym;
+  const CSR& conn = (!symmetricPattern && symmetrize_pattern(connIn, sym)) ? sym : connIn;
+  constexpr int kFewColors = 5;
   const int n = conn.nRows;
   std::vector<int> natural(n);
   for (int i = 0; i < n; i++) natural[i] = i;
   const int c1 = greedy_in_order(conn, natural, color);
-  if (c1 <= 2) return c1;
+  if (c1 <= kFewColors) return c1;
   std::vector<int> order, color2;
   smallest_last_order(conn, order);
   const int c2 = greedy_in_order(conn, order, color2);
@@ -323,7 +377,7 @@ void pack_level(const RefLevel& lv, SmootherOrdering ordering, PackedLevel& out)
     color.assign(n, 0);
     out.nColors = 1;
   } else {
-    out.nColors = multicolor(lv.conn, color);
+    out.nColors = multicolor(lv.conn, color, lv.symmetricPattern);
   }
   // colour-major permutation, stable in reference order
   out.colorStart.assign(out.nColors + 1, 0);

@@ -26,6 +26,10 @@ struct RefLevel {
   // to the next coarser level (empty on the coarsest)
   std::vector<int> coarseIndex;  // fine row -> coarse row (reference CRMatrix.h:468-586)
   int nCoarse = 0;
+  // the column pattern is known to be structurally symmetric (cellCells and
+  // the Galerkin levels built from a symmetric level); otherwise the
+  // colouring uses the pattern of A + A^T
+  bool symmetricPattern = false;
 };
 
 // Greedy aggregation (reference CRMatrix::createCoarsening). Returns the
@@ -80,9 +84,16 @@ enum SmootherOrdering { kMulticolor = 0, kSequential = 1 };
 // Greedy colouring in reference row order: each row takes the smallest
 // colour unused by its already-coloured neighbours.
 int greedy_coloring(const CSR& conn, std::vector<int>& color);
-// The colouring the multicolour smoothers use: the better (fewer colours)
-// of row-order greedy and smallest-last-order greedy; deterministic.
-int multicolor(const CSR& conn, std::vector<int>& color);
+// The colouring the multicolour smoothers use: row-order greedy, or when
+// that needs more than five colours the better (fewer colours) of it and
+// smallest-last-order greedy; deterministic.
+int multicolor(const CSR& conn, std::vector<int>& color, bool symmetricPattern = true);
+// Pattern of A + A^T: each row keeps its stored columns, followed by the
+// columns present only in the transpose, ascending. Returns false (and
+// leaves out untouched) when the pattern is already symmetric.
+bool symmetrize_pattern(const CSR& a, CSR& out);
+// true when every stored (i, j) has a stored (j, i)
+bool pattern_is_symmetric(const CSR& a);
 
 void pack_level(const RefLevel& lv, SmootherOrdering ordering, PackedLevel& out);
 // fills cols/vals of slices [sBegin, sEnd) (pack_level runs it in parallel)

@@ -117,6 +117,7 @@ RefLevel level_from_csr(int n, const int* row, const int* col, const double* dia
     FVM_REQUIRE(col[k] >= 0 && col[k] < n, kBadArgument, "column index out of range");
   l.diag.assign(diag, diag + n);
   l.off.assign(off, off + nnz);
+  l.symmetricPattern = pattern_is_symmetric(l.conn);
   return l;
 }
 
@@ -447,7 +448,7 @@ int fvm_amg_hierarchy_csr(int n, const int* row, const int* col, const double* d
       int pos = 0;
       for (const RefLevel& l : levels) {
         std::vector<int> c;
-        multicolor(l.conn, c);
+        multicolor(l.conn, c, l.symmetricPattern);
         for (int v : c) {
           if (pos < colorsCap) colors[pos] = v;
           pos++;

@@ -267,73 +267,144 @@ __global__ void k_dense_solve_f32(int n, const float* __restrict__ ainv, const f
   if (lane == 0) x[row] = -s;
 }
 
-// Gauss-Jordan step k on the augmented matrix W = [A | I] (n x 2n): pick
-// the largest |W[r][k]|, r >= k, swap it into row k, record the pivot and
-// the column factors f[i] = W[i][k] (i != k) for the elimination.
-__global__ void k_gj_pivot(int n, int k, double* W, double* scratch) {
-  __shared__ double sv[1024];
-  __shared__ int si[1024];
-  const int w2 = 2 * n;
-  double best = -1.0;
-  int bi = k;
-  for (int r = k + threadIdx.x; r < n; r += blockDim.x) {
-    const double v = fabs(W[(size_t)r * w2 + k]);
-    if (v > best) {
-      best = v;
-      bi = r;
-    }
+// Blocked in-place Gauss-Jordan inversion with partial (row) pivoting.
+// For each panel of B columns [k0, k0+nb): one CTA factors the panel (all n
+// rows, held column-major in shared memory), choosing pivot rows, applying
+// the row swaps to the panel and eliminating above and below each pivot;
+// the panel then holds the columns k0.. of the accumulated transform M.
+// The swaps are applied to the other columns and their pivot rows copied
+// out (k_gj_swap_rows); every other column j is then updated as
+// a'[i] = (i not a pivot row ? a[i] : 0) + sum_t M[i][t] a[k0+t]
+// (k_gj_update), a rank-nb update instead of nb sweeps over the matrix.
+// The row interchanges become a column permutation of the result
+// (k_gj_colperm, k_gj_gather).
+template <int B>
+__global__ void __launch_bounds__(1024) k_gj_panel(int n, int k0, int nb, double* __restrict__ A,
+                                                    int* __restrict__ piv, int* __restrict__ status) {
+  extern __shared__ double P[];  // P[t * n + i] = A[i][k0 + t]
+  __shared__ double redV[32];
+  __shared__ int redI[32];
+  __shared__ int sPiv;
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5, nw = blockDim.x >> 5;
+  for (int idx = tid; idx < n * B; idx += blockDim.x) {
+    const int t = idx / n, i = idx - t * n;
+    P[idx] = t < nb ? A[(size_t)i * n + k0 + t] : 0.0;
   }
-  sv[threadIdx.x] = best;
-  si[threadIdx.x] = bi;
   __syncthreads();
-  for (int o = blockDim.x >> 1; o > 0; o >>= 1) {
-    if (threadIdx.x < o) {
-      const double v2 = sv[threadIdx.x + o];
-      const int i2 = si[threadIdx.x + o];
-      if (v2 > sv[threadIdx.x] || (v2 == sv[threadIdx.x] && i2 < si[threadIdx.x])) {
-        sv[threadIdx.x] = v2;
-        si[threadIdx.x] = i2;
+  for (int t = 0; t < nb; t++) {
+    const int k = k0 + t;
+    double best = -1.0;
+    int bi = n;
+    for (int r = k + tid; r < n; r += blockDim.x) {
+      const double v = fabs(P[t * n + r]);
+      if (v > best) {  // rows visited in ascending order: ties keep the lowest
+        best = v;
+        bi = r;
+      }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      const double v2 = __shfl_down_sync(0xffffffffu, best, o);
+      const int i2 = __shfl_down_sync(0xffffffffu, bi, o);
+      if (v2 > best || (v2 == best && i2 < bi)) {
+        best = v2;
+        bi = i2;
+      }
+    }
+    if (lane == 0) {
+      redV[w] = best;
+      redI[w] = bi;
+    }
+    __syncthreads();
+    if (w == 0) {
+      best = lane < nw ? redV[lane] : -1.0;
+      bi = lane < nw ? redI[lane] : n;
+      for (int o = 16; o > 0; o >>= 1) {
+        const double v2 = __shfl_down_sync(0xffffffffu, best, o);
+        const int i2 = __shfl_down_sync(0xffffffffu, bi, o);
+        if (v2 > best || (v2 == best && i2 < bi)) {
+          best = v2;
+          bi = i2;
+        }
+      }
+      if (lane == 0) sPiv = (bi >= k && bi < n) ? bi : k;
+    }
+    __syncthreads();
+    const int p = sPiv;
+    if (tid == 0) piv[k] = p;
+    if (p != k && tid < nb) {
+      const double a = P[tid * n + k];
+      P[tid * n + k] = P[tid * n + p];
+      P[tid * n + p] = a;
+    }
+    __syncthreads();
+    const double pv = P[t * n + k];
+    if (pv == 0.0 && tid == 0) atomicExch(status, 1);
+    __syncthreads();
+    if (tid < nb) P[tid * n + k] = (tid == t ? 1.0 : P[tid * n + k]) / pv;
+    __syncthreads();
+    for (int i = tid; i < n; i += blockDim.x) {
+      if (i == k) continue;
+      const double f = P[t * n + i];
+      if (f != 0.0) {
+        P[t * n + i] = 0.0;
+        for (int s = 0; s < nb; s++) P[s * n + i] = P[s * n + i] - f * P[s * n + k];
       }
     }
     __syncthreads();
   }
-  const int p = si[0];
-  if (p != k)
-    for (int j = threadIdx.x; j < w2; j += blockDim.x) {
-      const double t = W[(size_t)k * w2 + j];
-      W[(size_t)k * w2 + j] = W[(size_t)p * w2 + j];
-      W[(size_t)p * w2 + j] = t;
-    }
-  __syncthreads();
-  if (threadIdx.x == 0) scratch[n] = W[(size_t)k * w2 + k];
-  for (int i = threadIdx.x; i < n; i += blockDim.x) scratch[i] = (i == k) ? 0.0 : W[(size_t)i * w2 + k];
+  for (int idx = tid; idx < n * nb; idx += blockDim.x) {
+    const int t = idx / n, i = idx - t * n;
+    A[(size_t)i * n + k0 + t] = P[idx];
+  }
 }
 
-__global__ void k_gj_scale(int n, int k, double* W, const double* scratch) {
+// Applies the panel's row swaps to every column outside the panel and
+// copies the pivot rows (old values) to Bt[t * n + j]; panel columns get 0.
+__global__ void k_gj_swap_rows(int n, int k0, int nb, double* __restrict__ A, const int* __restrict__ piv,
+                               double* __restrict__ Bt) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j < 2 * n) W[(size_t)k * 2 * n + j] = W[(size_t)k * 2 * n + j] / scratch[n];
+  if (j >= n) return;
+  const bool inPanel = j >= k0 && j < k0 + nb;
+  if (!inPanel)
+    for (int t = 0; t < nb; t++) {
+      const int k = k0 + t, p = piv[k];
+      if (p != k) {
+        const double a = A[(size_t)k * n + j];
+        A[(size_t)k * n + j] = A[(size_t)p * n + j];
+        A[(size_t)p * n + j] = a;
+      }
+    }
+  for (int t = 0; t < nb; t++) Bt[(size_t)t * n + j] = inPanel ? 0.0 : A[(size_t)(k0 + t) * n + j];
 }
 
-__global__ void k_gj_eliminate(int n, int k, double* W, const double* scratch) {
+__global__ void k_gj_update(int n, int k0, int nb, double* __restrict__ A, const double* __restrict__ Bt) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   const int i = blockIdx.y;
-  if (j >= 2 * n || i == k) return;
-  const double f = scratch[i];
-  if (f != 0.0) W[(size_t)i * 2 * n + j] = W[(size_t)i * 2 * n + j] - f * W[(size_t)k * 2 * n + j];
+  if (j >= n || (j >= k0 && j < k0 + nb)) return;
+  const double* Mi = A + (size_t)i * n + k0;
+  double s = 0.0;
+  for (int t = 0; t < nb; t++) s = s + Mi[t] * Bt[(size_t)t * n + j];
+  const size_t e = (size_t)i * n + j;
+  A[e] = (i >= k0 && i < k0 + nb) ? s : A[e] + s;
 }
 
-__global__ void k_gj_init(int n, const double* __restrict__ a, double* W) {
-  const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= (size_t)n * 2 * n) return;
-  const int i = (int)(t / (2 * n)), j = (int)(t % (2 * n));
-  W[t] = j < n ? a[(size_t)i * n + j] : (j - n == i ? 1.0 : 0.0);
+// column order of the inverse: the row swaps undone in reverse order
+__global__ void k_gj_colperm(int n, const int* __restrict__ piv, int* __restrict__ idx) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  for (int j = 0; j < n; j++) idx[j] = j;
+  for (int k = n - 1; k >= 0; k--) {
+    const int p = piv[k];
+    const int a = idx[k];
+    idx[k] = idx[p];
+    idx[p] = a;
+  }
 }
 
-__global__ void k_gj_extract(int n, const double* __restrict__ W, double* inv) {
-  const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= (size_t)n * n) return;
-  const int i = (int)(t / n), j = (int)(t % n);
-  inv[t] = W[(size_t)i * 2 * n + n + j];
+__global__ void k_gj_gather(int n, const double* __restrict__ X, const int* __restrict__ idx, double* inv) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = blockIdx.y;
+  if (j >= n) return;
+  inv[(size_t)i * n + j] = X[(size_t)i * n + idx[j]];
 }
 
 __global__ void k_cast_d2f_big(size_t n, const double* __restrict__ a, float* b) {
@@ -658,18 +729,47 @@ void dense_solve(int n, const double* ainv, const T* b, T* x, cudaStream_t st) {
 void dense_solve_f32(int n, const float* ainv, const float* b, float* x, cudaStream_t st) {
   pdl_launch(k_dense_solve_f32, ceil_div(n, kBlock / 32), kBlock, st, n, ainv, b, x);
 }
-void gauss_jordan_inverse(int n, const double* a, double* work, double* inv, double* scratch,
-                          cudaStream_t st) {
-  const size_t aug = (size_t)n * 2 * n;
-  k_gj_init<<<(unsigned)((aug + kBlock - 1) / kBlock), kBlock, 0, st>>>(n, a, work);
-  const dim3 eg(ceil_div(2 * n, kBlock), n);
-  for (int k = 0; k < n; k++) {
-    k_gj_pivot<<<1, 1024, 0, st>>>(n, k, work, scratch);
-    k_gj_scale<<<ceil_div(2 * n, kBlock), kBlock, 0, st>>>(n, k, work, scratch);
-    k_gj_eliminate<<<eg, kBlock, 0, st>>>(n, k, work, scratch);
+namespace {
+constexpr int kGjMaxPanel = 8;
+constexpr size_t kGjSmemLimit = 200 * 1024;
+size_t gj_align(size_t b) { return (b + 255) & ~size_t(255); }
+template <int B>
+void gj_run(int n, double* a, double* inv, double* Bt, int* piv, int* idx, int* status, cudaStream_t st) {
+  const size_t smem = sizeof(double) * (size_t)B * n;
+  cudaFuncSetAttribute(k_gj_panel<B>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  const dim3 ug(ceil_div(n, kBlock), n);
+  for (int k0 = 0; k0 < n; k0 += B) {
+    const int nb = n - k0 < B ? n - k0 : B;
+    k_gj_panel<B><<<1, 1024, smem, st>>>(n, k0, nb, a, piv, status);
+    k_gj_swap_rows<<<ceil_div(n, kBlock), kBlock, 0, st>>>(n, k0, nb, a, piv, Bt);
+    k_gj_update<<<ug, kBlock, 0, st>>>(n, k0, nb, a, Bt);
   }
-  const size_t nn = (size_t)n * n;
-  k_gj_extract<<<(unsigned)((nn + kBlock - 1) / kBlock), kBlock, 0, st>>>(n, work, inv);
+  k_gj_colperm<<<1, 1, 0, st>>>(n, piv, idx);
+  k_gj_gather<<<ug, kBlock, 0, st>>>(n, a, idx, inv);
+}
+}  // namespace
+
+size_t gauss_jordan_scratch_bytes(int n) {
+  return gj_align(sizeof(double) * kGjMaxPanel * (size_t)n) + 2 * gj_align(sizeof(int) * (size_t)n) +
+         gj_align(sizeof(int));
+}
+const int* gauss_jordan_status(int n, const void* scratch) {
+  const char* s = (const char*)scratch;
+  return (const int*)(s + gj_align(sizeof(double) * kGjMaxPanel * (size_t)n) + 2 * gj_align(sizeof(int) * (size_t)n));
+}
+void gauss_jordan_inverse(int n, double* a, double* inv, void* scratch, cudaStream_t st) {
+  char* s = (char*)scratch;
+  double* Bt = (double*)s;
+  int* piv = (int*)(s + gj_align(sizeof(double) * kGjMaxPanel * (size_t)n));
+  int* idx = piv + gj_align(sizeof(int) * (size_t)n) / sizeof(int);
+  int* status = (int*)gauss_jordan_status(n, scratch);
+  cudaMemsetAsync(status, 0, sizeof(int), st);
+  if (sizeof(double) * 8 * (size_t)n <= kGjSmemLimit)
+    gj_run<8>(n, a, inv, Bt, piv, idx, status, st);
+  else if (sizeof(double) * 4 * (size_t)n <= kGjSmemLimit)
+    gj_run<4>(n, a, inv, Bt, piv, idx, status, st);
+  else
+    gj_run<2>(n, a, inv, Bt, piv, idx, status, st);
 }
 void cast_d2f(size_t n, const double* a, float* b, cudaStream_t st) {
   k_cast_d2f_big<<<(unsigned)((n + kBlock - 1) / kBlock), kBlock, 0, st>>>(n, a, b);

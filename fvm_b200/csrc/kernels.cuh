@@ -76,12 +76,16 @@ template <class T>
 void dense_solve(int n, const double* ainv, const T* b, T* x, cudaStream_t st);
 // same with an FP32 copy of the inverse (half the bytes; FP32 V-cycle)
 void dense_solve_f32(int n, const float* ainv, const float* b, float* x, cudaStream_t st);
-// Inverse of the dense n x n matrix a (row-major, FP64, device) by
-// Gauss-Jordan elimination with partial pivoting on the augmented n x 2n
-// matrix `work` (2 n^2 doubles); result in `inv` (n^2 doubles). scratch
-// needs n + 2 doubles. Returns false if a pivot is exactly zero.
-void gauss_jordan_inverse(int n, const double* a, double* work, double* inv, double* scratch,
-                          cudaStream_t st);
+// Inverse of the dense n x n matrix `a` (row-major, FP64, device;
+// overwritten) by blocked in-place Gauss-Jordan elimination with partial
+// (row) pivoting; result in `inv` (n^2 doubles). scratch must hold
+// gauss_jordan_scratch_bytes(n); *status (device int inside scratch, see
+// gauss_jordan_status) becomes 1 if a pivot was exactly zero. Asynchronous
+// on st.
+size_t gauss_jordan_scratch_bytes(int n);
+void gauss_jordan_inverse(int n, double* a, double* inv, void* scratch, cudaStream_t st);
+// device address of the status flag inside scratch
+const int* gauss_jordan_status(int n, const void* scratch);
 void cast_d2f(size_t n, const double* a, float* b, cudaStream_t st);
 
 // ---- vector ops ------------------------------------------------------------

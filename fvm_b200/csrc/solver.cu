@@ -7,6 +7,8 @@
 #include <cstdio>
 #include <cstring>
 #include <cstdlib>
+#include <exception>
+#include <thread>
 #include <limits>
 #include <type_traits>
 
@@ -86,75 +88,66 @@ void AmgHierarchy::build(std::vector<RefLevel>& levels, int finestLocalSize, con
     fprintf(stderr, "[fvm setup] %-28s %8.1f ms\n", what, std::chrono::duration<double, std::milli>(t1 - t0).count());
     t0 = t1;
   };
+  const bool mixed = opt.precision == kMixed;
+  // Level 0 (the largest) is coloured, packed and uploaded on another
+  // thread while the coarse levels are aggregated; ref_ has room for every
+  // level, so appending coarse levels never moves level 0.
+  ref_.reserve((size_t)std::max(1, opt.maxCoarseLevels) + 2);
+  PackedLevel p0;
+  DevLevel d0;
+  std::exception_ptr err0;
+  std::thread level0([&] {
+    try {
+      pack_level(ref_[0], opt.ordering, p0);
+      uploadMatrix(p0, d0, mixed);
+    } catch (...) {
+      err0 = std::current_exception();
+    }
+  });
   std::vector<CSR> c2f;
-  build_hierarchy(ref_, ho, c2f);
+  try {
+    build_hierarchy(ref_, ho, c2f);
+  } catch (...) {
+    level0.join();
+    throw;
+  }
   lap("aggregation + Galerkin");
   const int L = (int)ref_.size();
   packed_.resize(L);
-  for (int l = 0; l < L; l++) pack_level(ref_[l], opt.ordering, packed_[l]);
-  lap("colouring + SELL packing");
+  lv_.resize(L);
+  {
+    std::vector<std::exception_ptr> errs(L);
+    std::vector<std::thread> th;
+    for (int l = 1; l < L; l++)
+      th.emplace_back([&, l] {
+        try {
+          pack_level(ref_[l], opt.ordering, packed_[l]);
+        } catch (...) {
+          errs[l] = std::current_exception();
+        }
+      });
+    for (auto& t : th) t.join();
+    level0.join();
+    if (err0) std::rethrow_exception(err0);
+    for (auto& e : errs)
+      if (e) std::rethrow_exception(e);
+  }
+  packed_[0] = std::move(p0);
+  lv_[0] = std::move(d0);
+  lap("colouring + packing (+ level 0 upload)");
   for (int l = 0; l + 1 < L; l++) pack_transfer(ref_[l], c2f[l], packed_[l], packed_[l + 1]);
   lap("transfer maps");
 
-  const bool mixed = opt.precision == kMixed;
-  lv_.resize(L);
-  for (int l = 0; l < L; l++) {
-    const PackedLevel& p = packed_[l];
-    DevLevel& d = lv_[l];
-    d.n = p.n;
-    d.nColors = p.nColors;
-    d.nSlices = (int)p.sliceRow.size();
-    d.maxWidth = p.maxWidth;
-    d.colorSliceStart = p.colorSliceStart;
-    d.entries = p.cols.size();
-    d.sliceRow = arena_.upload(p.sliceRow);
-    d.sliceRows = arena_.upload(p.sliceRows);
-    d.sliceOff = arena_.upload(p.sliceOff);
-    d.cols = arena_.upload(p.cols);
-    d.vals = arena_.upload(p.vals);
-    d.diag = arena_.upload(p.diag);
-    std::vector<int> rs(p.n);
-    std::vector<int4> meta(d.nSlices);
-    for (int s = 0; s < d.nSlices; s++) {
-      for (int k = 0; k < p.sliceRows[s]; k++) rs[p.sliceRow[s] + k] = s;
-      meta[s] = make_int4(p.sliceRow[s], p.sliceRows[s], p.sliceOff[s], (p.sliceOff[s + 1] - p.sliceOff[s]) / 32);
-    }
-    d.rowSlice = arena_.upload(rs);
-    d.meta = arena_.upload(meta);
-    if (l + 1 < L) {
-      d.nCoarse = packed_[l + 1].n;
-      d.ci = arena_.upload(p.coarseIndex);
-      d.c2fRow = arena_.upload(p.c2fRow);
-      d.c2fCol = arena_.upload(p.c2fCol);
-    }
-    const size_t nb = (size_t)p.n * sizeof(double);
-    d.x = (double*)arena_.alloc(nb);
-    d.b = (double*)arena_.alloc(nb);
-    d.r = (double*)arena_.alloc(nb);
-    d.tmp = (double*)arena_.alloc(nb);
-    CUDA_OK(cudaMemset(d.x, 0, nb));
-    CUDA_OK(cudaMemset(d.b, 0, nb));
-    d.nPartials = dev::reduce_blocks(d.nSlices);
-    d.partials = (double*)arena_.alloc(sizeof(double) * (d.nPartials + 1));
-    if (mixed) {
-      d.valsF = (float*)arena_.alloc(sizeof(float) * p.vals.size());
-      d.diagF = (float*)arena_.alloc(sizeof(float) * p.diag.size());
-      dev::cast_d2f(p.vals.size(), d.vals, d.valsF, 0);
-      dev::cast_d2f(p.diag.size(), d.diag, d.diagF, 0);
-      const size_t fb = (size_t)p.n * sizeof(float);
-      d.xF = (float*)arena_.alloc(fb);
-      d.bF = (float*)arena_.alloc(fb);
-      d.rF = (float*)arena_.alloc(fb);
-      d.tmpF = (float*)arena_.alloc(fb);
-      CUDA_OK(cudaMemset(d.xF, 0, fb));
-    }
-  }
-  lap("uploads");
+  // coarsest direct solve: the inverse runs on its own stream while the
+  // other levels upload
+  cudaStream_t gjStream = nullptr;
+  DeviceArena gjTmp;
+  void* gjScratch = nullptr;
+  const PackedLevel& c = packed_[L - 1];
+  const size_t nn = (size_t)c.n * c.n;
   if (opt.coarseSolver == kCoarseDirect) {
-    const PackedLevel& c = packed_[L - 1];
     FVM_REQUIRE(c.n <= 4096, kTooLarge,
                 "coarsest level too large for the dense direct solve (max 4096 rows); set coarsestSize");
-    const size_t nn = (size_t)c.n * c.n;
     if (c.n <= 128) {
       std::vector<double> inv;
       dense_inverse(c, inv);
@@ -171,19 +164,32 @@ void AmgHierarchy::build(std::vector<RefLevel>& levels, int finestLocalSize, con
             if (c.vals[e] != 0.0) a[(size_t)(c.sliceRow[s] + l) * c.n + c.cols[e]] += c.vals[e];
           }
       }
-      double* dA = arena_.upload(a);
-      DeviceArena tmp;
-      double* work = (double*)tmp.alloc(sizeof(double) * 2 * nn);
-      double* scratch = (double*)tmp.alloc(sizeof(double) * (c.n + 2));
+      double* dA = gjTmp.upload(a);
+      gjScratch = gjTmp.alloc(dev::gauss_jordan_scratch_bytes(c.n));
       coarseInv_ = (double*)arena_.alloc(sizeof(double) * nn);
-      dev::gauss_jordan_inverse(c.n, dA, work, coarseInv_, scratch, 0);
-      CUDA_OK(cudaDeviceSynchronize());
+      CUDA_OK(cudaStreamCreateWithFlags(&gjStream, cudaStreamNonBlocking));
+      dev::gauss_jordan_inverse(c.n, dA, coarseInv_, gjScratch, gjStream);
+    }
+  }
+  for (int l = 1; l < L; l++) uploadMatrix(packed_[l], lv_[l], mixed);
+  for (int l = 0; l + 1 < L; l++) uploadTransfer(packed_[l], lv_[l], packed_[l + 1].n);
+  lap("uploads");
+  if (opt.coarseSolver == kCoarseDirect) {
+    if (gjStream) {
+      int singular = 0;
+      const cudaError_t e1 = cudaMemcpyAsync(&singular, dev::gauss_jordan_status(c.n, gjScratch), sizeof(int),
+                                             cudaMemcpyDeviceToHost, gjStream);
+      const cudaError_t e2 = cudaStreamSynchronize(gjStream);
+      cudaStreamDestroy(gjStream);
+      CUDA_OK(e1);
+      CUDA_OK(e2);
+      FVM_REQUIRE(singular == 0, kBadArgument, "singular coarsest-level matrix");
     }
     if (mixed) {
       coarseInvF_ = (float*)arena_.alloc(sizeof(float) * nn);
       dev::cast_d2f(nn, coarseInv_, coarseInvF_, 0);
-      CUDA_OK(cudaDeviceSynchronize());
     }
+    CUDA_OK(cudaDeviceSynchronize());
     lap("coarsest inverse");
   }
   buildProgram();
@@ -192,6 +198,57 @@ void AmgHierarchy::build(std::vector<RefLevel>& levels, int finestLocalSize, con
     for (int l = 0; l < L; l++) fprintf(stderr, " %d(%dc)", lv_[l].n, lv_[l].nColors);
     fprintf(stderr, "\n");
   }
+}
+
+void AmgHierarchy::uploadMatrix(const PackedLevel& p, DevLevel& d, bool mixed) {
+  d.n = p.n;
+  d.nColors = p.nColors;
+  d.nSlices = (int)p.sliceRow.size();
+  d.maxWidth = p.maxWidth;
+  d.colorSliceStart = p.colorSliceStart;
+  d.entries = p.cols.size();
+  d.sliceRow = arena_.upload(p.sliceRow);
+  d.sliceRows = arena_.upload(p.sliceRows);
+  d.sliceOff = arena_.upload(p.sliceOff);
+  d.cols = arena_.upload(p.cols);
+  d.vals = arena_.upload(p.vals);
+  d.diag = arena_.upload(p.diag);
+  std::vector<int> rs(p.n);
+  std::vector<int4> meta(d.nSlices);
+  for (int s = 0; s < d.nSlices; s++) {
+    for (int k = 0; k < p.sliceRows[s]; k++) rs[p.sliceRow[s] + k] = s;
+    meta[s] = make_int4(p.sliceRow[s], p.sliceRows[s], p.sliceOff[s], (p.sliceOff[s + 1] - p.sliceOff[s]) / 32);
+  }
+  d.rowSlice = arena_.upload(rs);
+  d.meta = arena_.upload(meta);
+  const size_t nb = (size_t)p.n * sizeof(double);
+  d.x = (double*)arena_.alloc(nb);
+  d.b = (double*)arena_.alloc(nb);
+  d.r = (double*)arena_.alloc(nb);
+  d.tmp = (double*)arena_.alloc(nb);
+  CUDA_OK(cudaMemset(d.x, 0, nb));
+  CUDA_OK(cudaMemset(d.b, 0, nb));
+  d.nPartials = dev::reduce_blocks(d.nSlices);
+  d.partials = (double*)arena_.alloc(sizeof(double) * (d.nPartials + 1));
+  if (mixed) {
+    d.valsF = (float*)arena_.alloc(sizeof(float) * p.vals.size());
+    d.diagF = (float*)arena_.alloc(sizeof(float) * p.diag.size());
+    dev::cast_d2f(p.vals.size(), d.vals, d.valsF, 0);
+    dev::cast_d2f(p.diag.size(), d.diag, d.diagF, 0);
+    const size_t fb = (size_t)p.n * sizeof(float);
+    d.xF = (float*)arena_.alloc(fb);
+    d.bF = (float*)arena_.alloc(fb);
+    d.rF = (float*)arena_.alloc(fb);
+    d.tmpF = (float*)arena_.alloc(fb);
+    CUDA_OK(cudaMemset(d.xF, 0, fb));
+  }
+}
+
+void AmgHierarchy::uploadTransfer(const PackedLevel& p, DevLevel& d, int nCoarse) {
+  d.nCoarse = nCoarse;
+  d.ci = arena_.upload(p.coarseIndex);
+  d.c2fRow = arena_.upload(p.c2fRow);
+  d.c2fCol = arena_.upload(p.c2fCol);
 }
 
 void AmgHierarchy::genSweeps(int n, int l, std::vector<dev::Phase>& out) const {

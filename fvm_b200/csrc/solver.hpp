@@ -151,6 +151,10 @@ class AmgHierarchy {
   double* coarseInv_ = nullptr;  // dense inverse of the coarsest level
   float* coarseInvF_ = nullptr;  // its FP32 copy for the FP32 cycle
   DeviceArena arena_;
+  // device copy of one packed level (matrix, slice metadata, vectors) and
+  // of its transfer to the next coarser level
+  void uploadMatrix(const PackedLevel& p, DevLevel& d, bool mixed);
+  void uploadTransfer(const PackedLevel& p, DevLevel& d, int nCoarse);
   // persistent cycle program
   void buildProgram();
   void genCycle(CycleType t, int l, std::vector<dev::Phase>& out) const;

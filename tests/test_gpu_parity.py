@@ -151,7 +151,8 @@ def _converge(tm, n_outer=200):
 
 
 @pytest.mark.parametrize("kind", ["quad", "tet", "hex"])
-@pytest.mark.parametrize("variant", ["fp64-gs", "fp64-sequential", "mixed-direct", "cg-mixed", "bcgstab", "jacobi"])
+@pytest.mark.parametrize("variant", ["fp64-gs", "fp64-sequential", "mixed-direct", "mixed-direct-gpu-inverse",
+                                     "cg-mixed", "bcgstab", "jacobi"])
 def test_converged_field_matches_reference(refo, kind, variant):
     mesh, f = _synthetic(kind)
     bcs = {gid: v for gid, v in f["bc"].items()}
@@ -164,6 +165,11 @@ def test_converged_field_matches_reference(refo, kind, variant):
         amg.precision = fvmbaseExt.AMG.MIXED
         amg.coarseSolver = fvmbaseExt.AMG.COARSE_DIRECT
         amg.coarsestSize = 100
+    elif variant == "mixed-direct-gpu-inverse":
+        # first coarse level (> 128 rows) inverted by the blocked GPU Gauss-Jordan
+        amg.precision = fvmbaseExt.AMG.MIXED
+        amg.coarseSolver = fvmbaseExt.AMG.COARSE_DIRECT
+        amg.coarsestSize = 4096
     elif variant == "cg-mixed":
         amg.precision = fvmbaseExt.AMG.MIXED
         amg.coarseSolver = fvmbaseExt.AMG.COARSE_DIRECT
@@ -187,6 +193,25 @@ def test_converged_field_matches_reference(refo, kind, variant):
     assert norms[-1] / norms[0] < 1e-10
     Tr = r.get_field(0)[: mesh["nCells"]]
     assert rel_l2(T, Tr) <= TOL_FIELD
+
+
+def test_gpu_inverse_narrow_panels_matches_reference(refo):
+    """A coarsest level of more than 3200 rows takes the 4-column panels of
+    the blocked GPU Gauss-Jordan inverse (shared-memory bound)."""
+    mesh, f = meshgen.config0(n=90, seed=0)
+    bcs = {gid: v for gid, v in f["bc"].items()}
+    fields = {"conductivity": f["k"], "source": f["s"]}
+    amg = _amg(nPreSweeps=1, nPostSweeps=1, relativeTolerance=1e-10, nMaxIterations=500, coarsestSize=4096)
+    amg.precision = fvmbaseExt.AMG.MIXED
+    amg.coarseSolver = fvmbaseExt.AMG.COARSE_DIRECT
+    tm, tf, m = gpu_model(mesh, bcs, solver=amg, fields=fields, opts={"relativeTolerance": 1e-10})
+    sizes, _ = tm.getHierarchy()
+    assert 3200 < sizes[-1] <= 4096  # 3607 rows
+    _converge(tm)
+    T = tf.temperature[m.getCells()][: mesh["nCells"]]
+    r = ref_model(refo, mesh, bcs, fields=fields, n_pre=1, n_post=1, lin_rel=1e-10, max_iter=500, rel=1e-10)
+    r.advance(200)
+    assert rel_l2(T, r.get_field(0)[: mesh["nCells"]]) <= TOL_FIELD
 
 
 @pytest.mark.parametrize("smoother", ["sequential-gs", "jacobi"])

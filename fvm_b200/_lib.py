@@ -37,6 +37,8 @@ class LinearOptions(ctypes.Structure):
         ("coarseSolver", ctypes.c_int),
         ("precision", ctypes.c_int),
         ("useGraphs", ctypes.c_int),
+        ("coarseJacobiRows", ctypes.c_int),
+        ("jacobiWeight", ctypes.c_double),
     ]
 
 

@@ -78,6 +78,10 @@ SolverOptions to_solver(const fvm_linear_options& o) {
   s.coarseSolver = o.coarseSolver == 1 ? kCoarseDirect : kCoarseSmooth;
   s.precision = o.precision == 1 ? kMixed : kFP64;
   s.useGraphs = o.useGraphs != 0;
+  FVM_REQUIRE(o.coarseJacobiRows >= 0, kBadArgument, "coarseJacobiRows must be >= 0");
+  FVM_REQUIRE(o.jacobiWeight > 0.0 && o.jacobiWeight <= 1.0, kBadArgument, "jacobiWeight must be in (0, 1]");
+  s.coarseJacobiRows = o.coarseJacobiRows;
+  s.jacobiWeight = o.jacobiWeight;
   return s;
 }
 
@@ -100,6 +104,8 @@ void from_solver(const SolverOptions& s, fvm_linear_options& o) {
   o.coarseSolver = s.coarseSolver == kCoarseDirect ? 1 : 0;
   o.precision = s.precision == kMixed ? 1 : 0;
   o.useGraphs = s.useGraphs ? 1 : 0;
+  o.coarseJacobiRows = s.coarseJacobiRows;
+  o.jacobiWeight = s.jacobiWeight;
 }
 
 RefLevel level_from_csr(int n, const int* row, const int* col, const double* diag, const double* off) {

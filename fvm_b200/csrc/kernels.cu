@@ -151,6 +151,22 @@ __global__ void k_jacobi(SellView<T> a, int nSlices, const T* __restrict__ xold,
   xnew[i] = -sum / a.diag[i];
 }
 
+// damped Jacobi: xnew = xold + w (xJacobi - xold)
+template <class T>
+__global__ void k_jacobi_damped(SellView<T> a, int nSlices, const T* __restrict__ xold, T* xnew,
+                                const T* __restrict__ b, T w) {
+  FVM_PDL();
+  const int s = blockIdx.x * kSlicesPerBlock + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (s >= nSlices) return;
+  const int4 m = a.meta[s];
+  if (lane >= m.y) return;
+  const int i = m.x + lane;
+  const T sum = row_sum(a, m, lane, xold, b[i]);
+  const T xo = xold[i];
+  xnew[i] = xo + w * (-sum / a.diag[i] - xo);
+}
+
 template <class T>
 __global__ void k_residual(SellView<T> a, int nSlices, const T* __restrict__ x,
                            const T* __restrict__ b, T* r, double* partials) {
@@ -689,6 +705,10 @@ void jacobi(const SellView<T>& a, int nSlices, const T* xold, T* xnew, const T* 
   pdl_launch(k_jacobi<T>, ceil_div(nSlices, kSlicesPerBlock), kBlock, st, a, nSlices, xold, xnew, b);
 }
 template <class T>
+void jacobi_damped(const SellView<T>& a, int nSlices, const T* xold, T* xnew, const T* b, T w, cudaStream_t st) {
+  pdl_launch(k_jacobi_damped<T>, ceil_div(nSlices, kSlicesPerBlock), kBlock, st, a, nSlices, xold, xnew, b, w);
+}
+template <class T>
 void residual(const SellView<T>& a, int nSlices, const T* x, const T* b, T* r, double* partials,
               cudaStream_t st) {
   pdl_launch(k_residual<T>, ceil_div(nSlices, kSlicesPerBlock), kBlock, st, a, nSlices, x, b, r, partials);
@@ -865,6 +885,7 @@ void update_solution(int nCells, const int* perm, const double* delta, const Bou
   template void gs_color<T>(const SellView<T>&, int, int, T*, const T*, cudaStream_t);           \
   template void gs_sequential<T>(const SellView<T>&, T*, const T*, bool, cudaStream_t);          \
   template void jacobi<T>(const SellView<T>&, int, const T*, T*, const T*, cudaStream_t);        \
+  template void jacobi_damped<T>(const SellView<T>&, int, const T*, T*, const T*, T, cudaStream_t); \
   template void residual<T>(const SellView<T>&, int, const T*, const T*, T*, double*, cudaStream_t); \
   template void restrict_sum<T>(int, const int*, const int*, const T*, T*, cudaStream_t);        \
   template void residual_restrict<T>(const SellView<T>&, const int*, int, const int*, const int*,   \

@@ -35,6 +35,9 @@ void gs_sequential(const SellView<T>& a, T* x, const T* b, bool reverse, cudaStr
 // Jacobi: xnew_i = -(b_i + sum_j a_ij xold_j) / a_ii over all rows
 template <class T>
 void jacobi(const SellView<T>& a, int nSlices, const T* xold, T* xnew, const T* b, cudaStream_t st);
+// damped Jacobi: xnew = xold + w (Jacobi update - xold)
+template <class T>
+void jacobi_damped(const SellView<T>& a, int nSlices, const T* xold, T* xnew, const T* b, T w, cudaStream_t st);
 
 // ---- residual / products ---------------------------------------------------
 // r = b + D x + O x over all rows; when partials != null each block also

@@ -121,7 +121,8 @@ void AmgHierarchy::build(std::vector<RefLevel>& levels, int finestLocalSize, con
     for (int l = 1; l < L; l++)
       th.emplace_back([&, l] {
         try {
-          pack_level(ref_[l], opt.ordering, packed_[l]);
+          // levels smoothed by damped Jacobi need no colouring
+          pack_level(ref_[l], dampedLevel(l, ref_[l].n) ? kSequential : opt.ordering, packed_[l]);
         } catch (...) {
           errs[l] = std::current_exception();
         }
@@ -193,11 +194,17 @@ void AmgHierarchy::build(std::vector<RefLevel>& levels, int finestLocalSize, con
     lap("coarsest inverse");
   }
   buildProgram();
+  lap("cycle program");
   if (trace) {
     fprintf(stderr, "[fvm setup] levels:");
     for (int l = 0; l < L; l++) fprintf(stderr, " %d(%dc)", lv_[l].n, lv_[l].nColors);
     fprintf(stderr, "\n");
   }
+}
+
+bool AmgHierarchy::dampedLevel(int l, int n) const {
+  return l > 0 && opt_.coarseJacobiRows > 0 && n <= opt_.coarseJacobiRows && opt_.smootherType == kGaussSeidel &&
+         opt_.ordering == kMulticolor;
 }
 
 void AmgHierarchy::uploadMatrix(const PackedLevel& p, DevLevel& d, bool mixed) {
@@ -293,7 +300,8 @@ void AmgHierarchy::genCycle(CycleType t, int l, std::vector<dev::Phase>& out) co
 void AmgHierarchy::buildProgram() {
   programReady_ = false;
   tailLevel_ = -1;
-  if (opt_.ordering == kSequential && opt_.smootherType == kGaussSeidel) return;
+  // the program kernels implement the uniform smoothers only
+  if ((opt_.ordering == kSequential && opt_.smootherType == kGaussSeidel) || opt_.coarseJacobiRows > 0) return;
   const int L = (int)lv_.size();
   std::vector<dev::ProgLevel<double>> p64(L);
   std::vector<dev::ProgLevel<float>> p32(L);
@@ -452,8 +460,16 @@ void AmgHierarchy::sweeps(int nSweeps, int l, cudaStream_t st) {
   const dev::SellView<T> a = view<T>(d);
   T* x = vec_x<T>(d);
   const T* b = vec_b<T>(d);
+  const bool damped = dampedLevel(l, d.n);
   for (int s = 0; s < nSweeps; s++) {
-    if (opt_.smootherType == kGaussSeidel) {
+    if (damped) {
+      // small coarse levels: two damped Jacobi passes instead of 2C-1
+      // launch-bound colour passes
+      T* t = vec_tmp<T>(d);
+      const T w = (T)opt_.jacobiWeight;
+      dev::jacobi_damped<T>(a, d.nSlices, x, t, b, w, st);
+      dev::jacobi_damped<T>(a, d.nSlices, t, x, b, w, st);
+    } else if (opt_.smootherType == kGaussSeidel) {
       if (opt_.ordering == kSequential) {
         dev::gs_sequential<T>(a, x, b, false, st);
         dev::gs_sequential<T>(a, x, b, true, st);
@@ -571,11 +587,11 @@ int AmgHierarchy::kernelsPerCycle() const {
       k += 1;
       continue;
     }
-    const int perSweep = opt_.smootherType == kGaussSeidel
+    const int perSweep = (opt_.smootherType == kGaussSeidel && !dampedLevel(l, d.n))
                              ? (opt_.ordering == kSequential ? 2 : 2 * d.nColors - 1)
                              : 2;
     k += perSweep * (opt_.nPreSweeps + opt_.nPostSweeps);
-    if (l + 1 < L) k += 3;
+    if (l + 1 < L) k += 2;  // fused residual + restriction, prolongation
   }
   return k;
 }

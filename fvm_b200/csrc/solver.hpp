@@ -45,6 +45,10 @@ struct SolverOptions {
   CoarseSolver coarseSolver = kCoarseSmooth;
   Precision precision = kFP64;
   bool useGraphs = true;
+  // multicolour Gauss-Seidel levels below the finest with at most this many
+  // rows smooth with damped Jacobi (weight jacobiWeight) instead; 0 = never
+  int coarseJacobiRows = 0;
+  double jacobiWeight = 2.0 / 3.0;
 };
 
 struct SolveReport {
@@ -151,6 +155,8 @@ class AmgHierarchy {
   double* coarseInv_ = nullptr;  // dense inverse of the coarsest level
   float* coarseInvF_ = nullptr;  // its FP32 copy for the FP32 cycle
   DeviceArena arena_;
+  // level l (of n rows) smooths with damped Jacobi (coarseJacobiRows)
+  bool dampedLevel(int l, int n) const;
   // device copy of one packed level (matrix, slice metadata, vectors) and
   // of its transfer to the next coarser level
   void uploadMatrix(const PackedLevel& p, DevLevel& d, bool mixed);

@@ -280,6 +280,14 @@ void ThermalModel::uploadFields() {
 
 void ThermalModel::ensureMatrix() {
   if (!matrixDirty_ && !hierarchyDirty_) return;
+  const bool trace = getenv("FVM_TRACE") != nullptr;
+  auto t0 = std::chrono::steady_clock::now();
+  auto lap = [&](const char* what) {
+    if (!trace) return;
+    const auto t1 = std::chrono::steady_clock::now();
+    fprintf(stderr, "[fvm matrix] %-26s %8.1f ms\n", what, std::chrono::duration<double, std::milli>(t1 - t0).count());
+    t0 = t1;
+  };
   HostMesh& m = *mesh_;
   const int n = m.nCells, F = m.nFaces;
   dev::FaceGeom g{F, n, dFaceCells_, dArea_, dAreaMag_, dCentroid_, dVol_};
@@ -298,6 +306,7 @@ void ThermalModel::ensureMatrix() {
   CUDA_OK(cudaMemcpyAsync(coeff.data(), dCoeff_, sizeof(double) * F, cudaMemcpyDeviceToHost, stream_));
   CUDA_OK(cudaMemcpyAsync(diag.data(), dDiagOrig_, sizeof(double) * n, cudaMemcpyDeviceToHost, stream_));
   CUDA_OK(cudaStreamSynchronize(stream_));
+  lap("assembly + copy to host");
   std::vector<RefLevel> levels(1);
   RefLevel& l0 = levels[0];
   l0.n = n;
@@ -306,14 +315,18 @@ void ThermalModel::ensureMatrix() {
   l0.diag = std::move(diag);
   l0.off.resize(entryFace_.size());
   for (size_t e = 0; e < entryFace_.size(); e++) l0.off[e] = coeff[entryFace_[e]];
+  lap("finest level on host");
   solver_.reset();
+  lap("previous solver released");
   hier_.build(levels, m.nTotalCells(), opt_.linear);
+  lap("hierarchy");
   if (dPerm_) cudaFree(dPerm_);
   dPerm_ = nullptr;
   CUDA_OK(cudaMalloc(&dPerm_, sizeof(int) * (size_t)n));
   CUDA_OK(cudaMemcpy(dPerm_, hier_.packed(0).perm.data(), sizeof(int) * (size_t)n,
                      cudaMemcpyHostToDevice));
   solver_.reset(new LinearSolve(hier_));
+  lap("solver workspace");
   matrixDirty_ = hierarchyDirty_ = false;
 }
 

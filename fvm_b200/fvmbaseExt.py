@@ -187,6 +187,8 @@ class AMG(LinearSolver):
         self.coarseSolver = d.coarseSolver
         self.precision = d.precision
         self.useGraphs = bool(d.useGraphs)
+        self.coarseJacobiRows = d.coarseJacobiRows
+        self.jacobiWeight = d.jacobiWeight
         self._printFile = None
 
     def setMergeLevelSize(self, size: int) -> None:
@@ -219,6 +221,8 @@ class AMG(LinearSolver):
         o.coarseSolver = int(self.coarseSolver)
         o.precision = int(self.precision)
         o.useGraphs = int(bool(self.useGraphs))
+        o.coarseJacobiRows = int(self.coarseJacobiRows)
+        o.jacobiWeight = float(self.jacobiWeight)
 
     def options(self) -> _lib.LinearOptions:
         o = _lib.LinearOptions()

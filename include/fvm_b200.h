@@ -71,6 +71,9 @@ typedef struct fvm_linear_options {
   int coarseSolver;         /* 0 smooth only (reference), 1 dense FP64 direct solve */
   int precision;            /* 0 FP64, 1 FP32 V-cycle under FP64 refinement */
   int useGraphs;            /* replay each iteration as a CUDA graph */
+  int coarseJacobiRows;     /* levels below the finest with at most this many rows smooth with
+                               damped Jacobi instead of multicolour Gauss-Seidel (0: never) */
+  double jacobiWeight;      /* damping of that Jacobi smoother (default 2/3) */
 } fvm_linear_options;
 
 /* ThermalModelOptions (fvmbase/ThermalBC.h:33-67) + volume-condition constants */

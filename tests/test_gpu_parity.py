@@ -152,7 +152,7 @@ def _converge(tm, n_outer=200):
 
 @pytest.mark.parametrize("kind", ["quad", "tet", "hex"])
 @pytest.mark.parametrize("variant", ["fp64-gs", "fp64-sequential", "mixed-direct", "mixed-direct-gpu-inverse",
-                                     "cg-mixed", "bcgstab", "jacobi"])
+                                     "mixed-coarse-jacobi", "cg-mixed", "bcgstab", "jacobi"])
 def test_converged_field_matches_reference(refo, kind, variant):
     mesh, f = _synthetic(kind)
     bcs = {gid: v for gid, v in f["bc"].items()}
@@ -170,6 +170,12 @@ def test_converged_field_matches_reference(refo, kind, variant):
         amg.precision = fvmbaseExt.AMG.MIXED
         amg.coarseSolver = fvmbaseExt.AMG.COARSE_DIRECT
         amg.coarsestSize = 4096
+    elif variant == "mixed-coarse-jacobi":
+        # damped Jacobi on every level below the finest
+        amg.precision = fvmbaseExt.AMG.MIXED
+        amg.coarseSolver = fvmbaseExt.AMG.COARSE_DIRECT
+        amg.coarsestSize = 100
+        amg.coarseJacobiRows = 1 << 30
     elif variant == "cg-mixed":
         amg.precision = fvmbaseExt.AMG.MIXED
         amg.coarseSolver = fvmbaseExt.AMG.COARSE_DIRECT

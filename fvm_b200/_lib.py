@@ -15,6 +15,7 @@ LIB_PATH = os.path.join(HERE, "libfvm_b200.so")
 
 c_int_p = ctypes.POINTER(ctypes.c_int)
 c_double_p = ctypes.POINTER(ctypes.c_double)
+c_float_p = ctypes.POINTER(ctypes.c_float)
 
 
 class LinearOptions(ctypes.Structure):
@@ -67,6 +68,8 @@ class Report(ctypes.Structure):
         ("seconds", ctypes.c_double),
         ("setupSeconds", ctypes.c_double),
         ("launches", ctypes.c_longlong),
+        ("learnedSteps", ctypes.c_int),
+        ("learnedAccepted", ctypes.c_int),
     ]
 
 
@@ -116,6 +119,22 @@ _SIGS = {
     "fvm_amg_hierarchy_csr": (ctypes.c_int, [ctypes.c_int, c_int_p, c_int_p, c_double_p, c_double_p,
                                              ctypes.POINTER(LinearOptions), ctypes.c_int, c_int_p, c_int_p,
                                              ctypes.c_int, c_int_p, ctypes.c_int, c_int_p, ctypes.c_int]),
+    "fvm_learned_create": (ctypes.c_void_p, [ctypes.c_ulonglong]),
+    "fvm_learned_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "fvm_learned_num_params": (ctypes.c_int, []),
+    "fvm_learned_get_params": (ctypes.c_int, [ctypes.c_void_p, c_float_p, ctypes.c_int]),
+    "fvm_learned_set_params": (ctypes.c_int, [ctypes.c_void_p, c_float_p, ctypes.c_int]),
+    "fvm_learned_harvest": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                           ctypes.c_double, ctypes.c_int, c_int_p]),
+    "fvm_learned_num_pairs": (ctypes.c_int, [ctypes.c_void_p]),
+    "fvm_learned_train": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_float, ctypes.c_ulonglong,
+                                         c_double_p]),
+    "fvm_learned_evaluate": (ctypes.c_int, [ctypes.c_void_p, c_double_p]),
+    "fvm_thermal_set_learned": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "fvm_learned_forward_csr": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, c_int_p, c_int_p, c_double_p,
+                                               c_double_p, c_double_p, c_double_p]),
+    "fvm_learned_gradient_csr": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, c_int_p, c_int_p, c_double_p,
+                                                c_double_p, c_double_p, c_double_p, c_float_p, c_double_p]),
 }
 
 EXPORTED = tuple(_SIGS)

@@ -28,7 +28,7 @@ NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-fmad=false", "--expt-relaxed-c
               "-Xcompiler", "-fPIC,-ffp-contract=off"] + ARCH
 
 HOST_SOURCES = ["mesh.cpp", "amg_setup.cpp", "capi.cpp"]
-CUDA_SOURCES = ["kernels.cu", "solver.cu", "thermal.cu", "residual_noalloc.cu", "cycle_program.cu"]
+CUDA_SOURCES = ["kernels.cu", "solver.cu", "thermal.cu", "residual_noalloc.cu", "cycle_program.cu", "learned.cu"]
 
 
 def _nvcc() -> str:

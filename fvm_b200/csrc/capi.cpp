@@ -10,6 +10,7 @@
 
 #include "amg_setup.hpp"
 #include "mesh.hpp"
+#include "learned.hpp"
 #include "solver.hpp"
 #include "thermal.hpp"
 
@@ -20,6 +21,10 @@ struct fvm_mesh {
 };
 struct fvm_thermal {
   std::unique_ptr<ThermalModel> model;
+};
+
+struct fvm_learned {
+  std::unique_ptr<fvm::LearnedCorrection> lc;
 };
 
 namespace fvm {
@@ -339,6 +344,8 @@ int fvm_thermal_advance(fvm_thermal* h, int niter, fvm_report* rep) {
       rep->seconds = r.seconds;
       rep->setupSeconds = r.setupSeconds;
       rep->launches = r.launches;
+      rep->learnedSteps = r.learnedSteps;
+      rep->learnedAccepted = r.learnedAccepted;
     }
   });
 }
@@ -521,6 +528,139 @@ int fvm_amg_solve_csr(int n, const int* row, const int* col, const double* diag,
     if (nHistory) *nHistory = (int)sr.history.size();
     for (size_t i = 0; history && i < sr.history.size() && (int)i < historyCap; i++)
       history[i] = sr.history[i];
+  });
+}
+
+
+// ---- learned correction ------------------------------------------------------
+namespace {
+// A CSR graph packed in natural order (one colour) and uploaded, for the
+// network test hooks.
+struct CsrGraph {
+  fvm::DeviceArena arena;
+  fvm::nn::Graph g;
+  int n = 0;
+  CsrGraph(int n_, const int* row, const int* col, const double* diag, const double* off) {
+    using namespace fvm;
+    RefLevel l = level_from_csr(n_, row, col, diag, off);
+    PackedLevel p;
+    pack_level(l, kSequential, p);
+    n = n_;
+    std::vector<int> rs(n);
+    std::vector<int4> meta(p.sliceRow.size());
+    for (size_t s = 0; s < p.sliceRow.size(); s++) {
+      for (int k = 0; k < p.sliceRows[s]; k++) rs[p.sliceRow[s] + k] = (int)s;
+      meta[s] = make_int4(p.sliceRow[s], p.sliceRows[s], p.sliceOff[s], (p.sliceOff[s + 1] - p.sliceOff[s]) / 32);
+    }
+    g.a.n = n;
+    g.a.cols = arena.upload(p.cols);
+    g.a.vals = arena.upload(p.vals);
+    g.a.diag = arena.upload(p.diag);
+    g.a.meta = arena.upload(meta);
+    g.rowSlice = arena.upload(rs);
+    g.nSlices = (int)p.sliceRow.size();
+  }
+};
+}  // namespace
+
+fvm_learned* fvm_learned_create(unsigned long long seed) {
+  fvm_learned* l = nullptr;
+  const int rc = guarded([&] {
+    l = new fvm_learned;
+    l->lc.reset(new LearnedCorrection(seed));
+  });
+  if (rc != 0) {
+    delete l;
+    return nullptr;
+  }
+  return l;
+}
+
+int fvm_learned_destroy(fvm_learned* l) {
+  return guarded([&] { delete l; });
+}
+
+int fvm_learned_num_params(void) { return nn::kParams; }
+
+int fvm_learned_get_params(const fvm_learned* l, float* out, int cap) {
+  return guarded([&] {
+    FVM_REQUIRE(l && out && cap >= nn::kParams, kBadArgument, "null argument or capacity below num_params");
+    const std::vector<float> p = l->lc->params();
+    std::copy(p.begin(), p.end(), out);
+  });
+}
+
+int fvm_learned_set_params(fvm_learned* l, const float* p, int n) {
+  return guarded([&] {
+    FVM_REQUIRE(l && p && n == nn::kParams, kBadArgument, "null argument or wrong parameter count");
+    l->lc->setParams(std::vector<float>(p, p + n));
+  });
+}
+
+int fvm_learned_harvest(fvm_learned* l, fvm_thermal* t, int nOuter, int perSolve, double relTol, int maxCycles,
+                        int* nPairs) {
+  return guarded([&] {
+    FVM_REQUIRE(l && t, kBadArgument, "null argument");
+    const int k = t->model->harvest(*l->lc, nOuter, perSolve, relTol, maxCycles);
+    if (nPairs) *nPairs = k;
+  });
+}
+
+int fvm_learned_num_pairs(const fvm_learned* l) { return l ? l->lc->numPairs() : 0; }
+
+int fvm_learned_train(fvm_learned* l, int steps, float lr, unsigned long long seed, double* losses) {
+  return guarded([&] {
+    FVM_REQUIRE(l, kBadArgument, "null argument");
+    l->lc->train(steps, lr, seed, losses, 0);
+  });
+}
+
+int fvm_learned_evaluate(fvm_learned* l, double* meanLoss) {
+  return guarded([&] {
+    FVM_REQUIRE(l && meanLoss, kBadArgument, "null argument");
+    *meanLoss = l->lc->evaluate(0);
+  });
+}
+
+int fvm_thermal_set_learned(fvm_thermal* t, fvm_learned* l) {
+  return guarded([&] {
+    FVM_REQUIRE(t, kBadArgument, "null model");
+    t->model->setLearned(l ? l->lc.get() : nullptr);
+  });
+}
+
+int fvm_learned_forward_csr(fvm_learned* l, int n, const int* row, const int* col, const double* diag,
+                            const double* off, const double* r, double* out) {
+  return guarded([&] {
+    FVM_REQUIRE(l && r && out, kBadArgument, "null argument");
+    CsrGraph cg(n, row, col, diag, off);
+    DeviceArena tmp;
+    double* dr = tmp.upload(std::vector<double>(r, r + n));
+    double* dOut = (double*)tmp.alloc(sizeof(double) * (size_t)n);
+    double* scal = (double*)tmp.alloc(sizeof(double) * 8);
+    l->lc->prepare(n);
+    l->lc->apply(cg.g, dr, dOut, scal, 0);
+    if (cudaMemcpy(out, dOut, sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost) != cudaSuccess)
+      throw Error(kDeviceError, "copy of the network output failed");
+  });
+}
+
+int fvm_learned_gradient_csr(fvm_learned* l, int n, const int* row, const int* col, const double* diag,
+                             const double* off, const double* r, const double* e, float* grad, double* loss) {
+  return guarded([&] {
+    FVM_REQUIRE(l && r && e && grad && loss, kBadArgument, "null argument");
+    CsrGraph cg(n, row, col, diag, off);
+    DeviceArena tmp;
+    double* dr = tmp.upload(std::vector<double>(r, r + n));
+    double* de = tmp.upload(std::vector<double>(e, e + n));
+    float* dg = (float*)tmp.alloc(sizeof(float) * nn::kParams);
+    double* scal = (double*)tmp.alloc(sizeof(double) * 8);
+    nn::Workspace ws;
+    ws.allocate(n, true);
+    nn::forward_backward(cg.g, l->lc->deviceParams(), dr, de, dg, scal + 4, ws, scal, 0);
+    if (cudaMemcpy(grad, dg, sizeof(float) * nn::kParams, cudaMemcpyDeviceToHost) != cudaSuccess ||
+        cudaMemcpy(loss, scal + 4, sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess)
+      throw Error(kDeviceError, "copy of the gradient failed");
   });
 }
 

@@ -311,9 +311,12 @@ void run_forward(const Graph& g, const float* P, const double* r, Workspace& w, 
 }  // namespace
 
 void Workspace::allocate(int n_, bool training) {
-  if (n_ == n && (!training || M[0])) return;
+  if (n_ <= cap && (!training || M[0])) {
+    n = n_;
+    return;
+  }
   release();
-  n = n_;
+  n = cap = n_;
   const size_t hb = sizeof(float) * (size_t)n * 32;
   check(cudaMalloc(&u, sizeof(float) * (size_t)n), "cudaMalloc");
   for (int l = 0; l <= kLayers; l++) check(cudaMalloc(&H[l], hb), "cudaMalloc");
@@ -341,7 +344,7 @@ void Workspace::release() {
   partials = nullptr;
   for (auto& h : H) h = nullptr;
   for (auto& m : M) m = nullptr;
-  n = 0;
+  n = cap = 0;
 }
 
 void forward(const Graph& g, const float* params, const double* r, double* out, Workspace& w, double* scal,
@@ -403,4 +406,223 @@ std::vector<float> initial_parameters(uint64_t seed) {
 }
 
 }  // namespace nn
+}  // namespace fvm
+
+// ---------------------------------------------------------------------------
+// flexible step of the solve
+namespace fvm {
+namespace nn {
+namespace {
+
+__global__ void k_step_alpha(const double* rq, const double* qq, double* alpha) {
+  alpha[0] = qq[0] > 0.0 ? -rq[0] / qq[0] : 0.0;
+}
+
+__global__ void k_step_trial(int n, const double* __restrict__ r, const double* __restrict__ q,
+                             const double* __restrict__ alpha, double* __restrict__ rt, double* partials) {
+  const double a = alpha[0];
+  double s = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double v = r[i] + a * q[i];
+    rt[i] = v;
+    s += fabs(v);
+  }
+  s = block_sum(s);
+  if (threadIdx.x == 0) partials[blockIdx.x] = s;
+}
+
+__global__ void k_step_accept(int n, double* __restrict__ x, const double* __restrict__ d, double* __restrict__ r,
+                              const double* __restrict__ rt, const double* __restrict__ alpha,
+                              const double* __restrict__ norm, const double* __restrict__ trial) {
+  if (!(trial[0] < norm[0])) return;
+  const double a = alpha[0];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    x[i] += a * d[i];
+    r[i] = rt[i];
+  }
+}
+
+__global__ void k_step_finish(double* norm, const double* trial, double* accepted, double* steps) {
+  if (trial[0] < norm[0]) {
+    norm[0] = trial[0];
+    accepted[0] += 1.0;
+  }
+  steps[0] += 1.0;
+}
+
+}  // namespace
+
+void step_alpha(const double* rq, const double* qq, double* alpha, cudaStream_t st) {
+  k_step_alpha<<<1, 1, 0, st>>>(rq, qq, alpha);
+}
+void step_trial(int n, const double* r, const double* q, const double* alpha, double* rt, double* partials,
+                cudaStream_t st) {
+  k_step_trial<<<dev::vec_blocks(n), kBlock, 0, st>>>(n, r, q, alpha, rt, partials);
+}
+void step_accept(int n, double* x, const double* d, double* r, const double* rt, const double* alpha,
+                 const double* norm, const double* trialNorm, cudaStream_t st) {
+  k_step_accept<<<dev::vec_blocks(n), kBlock, 0, st>>>(n, x, d, r, rt, alpha, norm, trialNorm);
+}
+void step_finish(double* norm, const double* trialNorm, double* accepted, double* steps, cudaStream_t st) {
+  k_step_finish<<<1, 1, 0, st>>>(norm, trialNorm, accepted, steps);
+}
+
+}  // namespace nn
+
+// ---------------------------------------------------------------------------
+LearnedCorrection::LearnedCorrection(uint64_t seed) {
+  nn::check(cudaMalloc(&dParams_, sizeof(float) * nn::kParams), "cudaMalloc");
+  nn::check(cudaMalloc(&dGrad_, sizeof(float) * nn::kParams), "cudaMalloc");
+  nn::check(cudaMalloc(&dM_, sizeof(float) * nn::kParams), "cudaMalloc");
+  nn::check(cudaMalloc(&dV_, sizeof(float) * nn::kParams), "cudaMalloc");
+  nn::check(cudaMalloc(&dScal_, sizeof(double) * 16), "cudaMalloc");
+  nn::check(cudaMemset(dM_, 0, sizeof(float) * nn::kParams), "cudaMemset");
+  nn::check(cudaMemset(dV_, 0, sizeof(float) * nn::kParams), "cudaMemset");
+  setParams(nn::initial_parameters(seed));
+}
+
+LearnedCorrection::~LearnedCorrection() {
+  for (Instance& k : inst_) {
+    for (auto& pr : k.pairs) {
+      cudaFree(pr.first);
+      cudaFree(pr.second);
+    }
+    cudaFree(k.storage);
+  }
+  cudaFree(dParams_);
+  cudaFree(dGrad_);
+  cudaFree(dM_);
+  cudaFree(dV_);
+  cudaFree(dScal_);
+}
+
+std::vector<float> LearnedCorrection::params() const {
+  std::vector<float> p(nn::kParams);
+  nn::check(cudaMemcpy(p.data(), dParams_, sizeof(float) * nn::kParams, cudaMemcpyDeviceToHost), "cudaMemcpy");
+  return p;
+}
+
+void LearnedCorrection::setParams(const std::vector<float>& p) {
+  FVM_REQUIRE((int)p.size() == nn::kParams, kBadArgument, "learned correction: wrong parameter count");
+  nn::check(cudaMemcpy(dParams_, p.data(), sizeof(float) * nn::kParams, cudaMemcpyHostToDevice), "cudaMemcpy");
+  nn::check(cudaMemset(dM_, 0, sizeof(float) * nn::kParams), "cudaMemset");
+  nn::check(cudaMemset(dV_, 0, sizeof(float) * nn::kParams), "cudaMemset");
+  adamT_ = 0;
+}
+
+int LearnedCorrection::addInstance(const nn::Graph& g, int nEntries, cudaStream_t st) {
+  Instance k;
+  k.n = g.a.n;
+  const size_t bCols = sizeof(int) * (size_t)nEntries, bVals = sizeof(double) * (size_t)nEntries;
+  const size_t bDiag = sizeof(double) * (size_t)k.n, bMeta = sizeof(int4) * (size_t)g.nSlices;
+  const size_t bRs = sizeof(int) * (size_t)k.n;
+  auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
+  char* p = nullptr;
+  nn::check(cudaMalloc((void**)&p, al(bCols) + al(bVals) + al(bDiag) + al(bMeta) + al(bRs)), "cudaMalloc");
+  k.storage = p;
+  int* cols = (int*)p;
+  double* vals = (double*)(p + al(bCols));
+  double* diag = (double*)(p + al(bCols) + al(bVals));
+  int4* meta = (int4*)(p + al(bCols) + al(bVals) + al(bDiag));
+  int* rs = (int*)(p + al(bCols) + al(bVals) + al(bDiag) + al(bMeta));
+  nn::check(cudaMemcpyAsync(cols, g.a.cols, bCols, cudaMemcpyDeviceToDevice, st), "cudaMemcpy");
+  nn::check(cudaMemcpyAsync(vals, g.a.vals, bVals, cudaMemcpyDeviceToDevice, st), "cudaMemcpy");
+  nn::check(cudaMemcpyAsync(diag, g.a.diag, bDiag, cudaMemcpyDeviceToDevice, st), "cudaMemcpy");
+  nn::check(cudaMemcpyAsync(meta, g.a.meta, bMeta, cudaMemcpyDeviceToDevice, st), "cudaMemcpy");
+  nn::check(cudaMemcpyAsync(rs, g.rowSlice, bRs, cudaMemcpyDeviceToDevice, st), "cudaMemcpy");
+  k.g = g;
+  k.g.a.cols = cols;
+  k.g.a.vals = vals;
+  k.g.a.diag = diag;
+  k.g.a.meta = meta;
+  k.g.rowSlice = rs;
+  // slice-row arrays are not used by the network kernels
+  k.g.a.sliceRow = k.g.a.sliceRows = k.g.a.sliceOff = nullptr;
+  inst_.push_back(k);
+  return (int)inst_.size() - 1;
+}
+
+void LearnedCorrection::addPair(int k, const double* r, const double* e, cudaStream_t st) {
+  FVM_REQUIRE(k >= 0 && k < (int)inst_.size(), kBadArgument, "learned correction: no such instance");
+  Instance& in = inst_[k];
+  const size_t b = sizeof(double) * (size_t)in.n;
+  double *pr = nullptr, *pe = nullptr;
+  nn::check(cudaMalloc(&pr, b), "cudaMalloc");
+  nn::check(cudaMalloc(&pe, b), "cudaMalloc");
+  nn::check(cudaMemcpyAsync(pr, r, b, cudaMemcpyDeviceToDevice, st), "cudaMemcpy");
+  nn::check(cudaMemcpyAsync(pe, e, b, cudaMemcpyDeviceToDevice, st), "cudaMemcpy");
+  in.pairs.push_back({pr, pe});
+}
+
+int LearnedCorrection::numPairs() const {
+  int c = 0;
+  for (const Instance& k : inst_) c += (int)k.pairs.size();
+  return c;
+}
+
+void LearnedCorrection::train(int steps, float lr, uint64_t seed, double* losses, cudaStream_t st) {
+  const int np = numPairs();
+  FVM_REQUIRE(np > 0, kBadArgument, "learned correction: no training pairs (harvest first)");
+  FVM_REQUIRE(steps >= 0 && lr > 0.f, kBadArgument, "learned correction: bad training settings");
+  int maxN = 0;
+  std::vector<std::pair<int, int>> index;
+  for (int k = 0; k < (int)inst_.size(); k++) {
+    maxN = std::max(maxN, inst_[k].n);
+    for (int q = 0; q < (int)inst_[k].pairs.size(); q++) index.push_back({k, q});
+  }
+  trainWs_.allocate(maxN, true);
+  double* dLoss = nullptr;
+  nn::check(cudaMalloc(&dLoss, sizeof(double) * (size_t)std::max(steps, 1)), "cudaMalloc");
+  uint64_t x = seed * 0x9E3779B97F4A7C15ull + 0x51ull;
+  auto next = [&]() {
+    uint64_t z = (x += 0x9E3779B97F4A7C15ull);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+  };
+  for (int t = 0; t < steps; t++) {
+    const auto& ix = index[next() % index.size()];
+    Instance& in = inst_[ix.first];
+    trainWs_.allocate(in.n, true);
+    nn::forward_backward(in.g, dParams_, in.pairs[ix.second].first, in.pairs[ix.second].second, dGrad_,
+                         dLoss + t, trainWs_, dScal_, st);
+    nn::adam_step(dParams_, dGrad_, dM_, dV_, lr, ++adamT_, st);
+  }
+  if (losses && steps > 0)
+    nn::check(cudaMemcpyAsync(losses, dLoss, sizeof(double) * steps, cudaMemcpyDeviceToHost, st), "cudaMemcpy");
+  nn::check(cudaStreamSynchronize(st), "training");
+  cudaFree(dLoss);
+}
+
+double LearnedCorrection::evaluate(cudaStream_t st) {
+  const int np = numPairs();
+  FVM_REQUIRE(np > 0, kBadArgument, "learned correction: no pairs to evaluate");
+  int maxN = 0;
+  for (const Instance& k : inst_) maxN = std::max(maxN, k.n);
+  trainWs_.allocate(maxN, true);
+  double* dLoss = nullptr;
+  nn::check(cudaMalloc(&dLoss, sizeof(double) * (size_t)np), "cudaMalloc");
+  int q = 0;
+  for (Instance& in : inst_)
+    for (auto& pr : in.pairs) {
+      trainWs_.allocate(in.n, true);
+      nn::forward_backward(in.g, dParams_, pr.first, pr.second, dGrad_, dLoss + q++, trainWs_, dScal_, st);
+    }
+  std::vector<double> l(np);
+  nn::check(cudaMemcpyAsync(l.data(), dLoss, sizeof(double) * np, cudaMemcpyDeviceToHost, st), "cudaMemcpy");
+  nn::check(cudaStreamSynchronize(st), "evaluation");
+  cudaFree(dLoss);
+  double s = 0.0;
+  for (double v : l) s += v;
+  return s / np;
+}
+
+void LearnedCorrection::prepare(int n) { applyWs_.allocate(n, false); }
+
+void LearnedCorrection::apply(const nn::Graph& g, const double* r, double* out, double* scal, cudaStream_t st) {
+  FVM_REQUIRE(g.a.n <= applyWs_.cap, kBadArgument, "learned correction: prepare() was not called for this size");
+  applyWs_.n = g.a.n;
+  nn::forward(g, dParams_, r, out, applyWs_, scal, st);
+}
+
 }  // namespace fvm

@@ -47,7 +47,8 @@ struct Graph {
 
 // Device workspace for one graph size.
 struct Workspace {
-  int n = 0;
+  int n = 0;    // nodes of the current graph
+  int cap = 0;  // nodes the buffers hold
   float* u = nullptr;            // n
   float* H[kLayers + 1] = {};    // n x 32 each
   float* M[kLayers] = {};        // n x 32 each (training only)
@@ -78,6 +79,69 @@ void adam_step(float* params, const float* grad, float* m, float* v, float lr, i
 
 // Deterministic initial parameters (He-style uniform, seeded).
 std::vector<float> initial_parameters(uint64_t seed);
+
+// ---- the flexible step inside the solve (all device scalars, capturable) ----
+// alpha = -(r.q)/(q.q) (0 if q.q = 0)
+void step_alpha(const double* rq, const double* qq, double* alpha, cudaStream_t st);
+// rt = r + alpha q, with per-block L1 partials of rt (vec_blocks(n) of them)
+void step_trial(int n, const double* r, const double* q, const double* alpha, double* rt, double* partials,
+                cudaStream_t st);
+// if trialNorm < norm: x += alpha d, r = rt
+void step_accept(int n, double* x, const double* d, double* r, const double* rt, const double* alpha,
+                 const double* norm, const double* trialNorm, cudaStream_t st);
+// if trialNorm < norm: norm = trialNorm, accepted += 1; steps += 1
+void step_finish(double* norm, const double* trialNorm, double* accepted, double* steps, cudaStream_t st);
 }  // namespace nn
+
+// A trained (or training) learned correction: parameters, Adam state and
+// the training set. A training instance is one linear system's graph
+// (copied, so it outlives the model it came from) with its (residual,
+// error) pairs.
+class LearnedCorrection {
+ public:
+  explicit LearnedCorrection(uint64_t seed);
+  ~LearnedCorrection();
+  LearnedCorrection(const LearnedCorrection&) = delete;
+  LearnedCorrection& operator=(const LearnedCorrection&) = delete;
+
+  std::vector<float> params() const;
+  void setParams(const std::vector<float>& p);
+  const float* deviceParams() const { return dParams_; }
+
+  // a new instance with a copy of the graph; returns its index
+  int addInstance(const nn::Graph& g, int nEntries, cudaStream_t st);
+  // copies one (residual, error) pair (n doubles each, device) into instance k
+  void addPair(int k, const double* r, const double* e, cudaStream_t st);
+  int numPairs() const;
+  int numInstances() const { return (int)inst_.size(); }
+
+  // Adam on randomly drawn pairs; losses (optional, steps entries) gets the
+  // relative squared error of each step's pair before its update.
+  void train(int steps, float lr, uint64_t seed, double* losses, cudaStream_t st);
+  // mean relative squared error over all pairs (no update)
+  double evaluate(cudaStream_t st);
+
+  // correction for residual r on graph g (call prepare(n) first: apply
+  // allocates nothing, so it can run inside a captured graph)
+  void prepare(int n);
+  void apply(const nn::Graph& g, const double* r, double* out, double* scal, cudaStream_t st);
+
+ private:
+  struct Instance {
+    int n = 0;
+    nn::Graph g;
+    void* storage = nullptr;  // owns the graph copy
+    std::vector<std::pair<double*, double*>> pairs;
+  };
+  std::vector<Instance> inst_;
+  float* dParams_ = nullptr;
+  float* dGrad_ = nullptr;
+  float* dM_ = nullptr;
+  float* dV_ = nullptr;
+  double* dScal_ = nullptr;
+  int adamT_ = 0;
+  nn::Workspace trainWs_;
+  nn::Workspace applyWs_;
+};
 
 }  // namespace fvm

@@ -614,6 +614,14 @@ enum Scal {
   kTdott,
   kOmegaPrev,
   kAlphaPrev,
+  // learned step
+  kLsScale = 20,  // and kLsScale + 1 (input sum)
+  kLsRq = 22,
+  kLsQq,
+  kLsAlpha,
+  kLsTrial,
+  kLsAccepted,
+  kLsSteps,
   kNumScal
 };
 constexpr int kWorkVectors = 9;
@@ -622,6 +630,7 @@ constexpr int kWorkVectors = 9;
 LinearSolve::LinearSolve(AmgHierarchy& h) : h_(h), n_(h.level(0).n) {
   CUDA_OK(cudaMalloc(&work_, sizeof(double) * (size_t)n_ * kWorkVectors));
   CUDA_OK(cudaMalloc(&scal_, sizeof(double) * 32));
+  CUDA_OK(cudaMemset(scal_, 0, sizeof(double) * 32));
   CUDA_OK(cudaMalloc(&partials_, sizeof(double) * (dev::vec_blocks(n_) + 1)));
   CUDA_OK(cudaMallocHost(&hostScal_, sizeof(double) * 32));
 }
@@ -716,6 +725,7 @@ SolveReport LinearSolve::solveAMG(cudaStream_t st) {
   DevLevel& d = h_.level(0);
   SolveReport rep;
   CUDA_OK(cudaMemsetAsync(d.x, 0, sizeof(double) * (size_t)n_, st));
+  if (learned_) CUDA_OK(cudaMemsetAsync(scal_ + kLsAccepted, 0, 2 * sizeof(double), st));
   dev::residual<double>(d.view64(), d.nSlices, d.x, d.b, d.r, d.partials, st);
   dev::sum_partials(d.nPartials, d.partials, scal_ + kNorm, st);
   launches += 3;
@@ -741,6 +751,7 @@ SolveReport LinearSolve::solveAMG(cudaStream_t st) {
       }
       dev::residual<double>(d.view64(), d.nSlices, d.x, d.b, d.r, d.partials, st);
       dev::sum_partials(d.nPartials, d.partials, scal_ + kNorm, st);
+      if (learned_) learnedStep(st);
       CUDA_OK(cudaMemcpyAsync(hostScal_, scal_ + kNorm, sizeof(double), cudaMemcpyDeviceToHost, st));
     });
     CUDA_OK(cudaStreamSynchronize(st));
@@ -755,7 +766,92 @@ SolveReport LinearSolve::solveAMG(cudaStream_t st) {
       break;
     }
   }
+  if (learned_) {
+    CUDA_OK(cudaMemcpyAsync(hostScal_, scal_ + kLsAccepted, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CUDA_OK(cudaStreamSynchronize(st));
+    rep.learnedAccepted = (int)hostScal_[0];
+    rep.learnedSteps = (int)hostScal_[1];
+  }
   return rep;
+}
+
+void LinearSolve::setLearned(LearnedCorrection* lc) {
+  if (lc != learned_) {
+    // the captured iteration graph changes with the step
+    if (g1_) cudaGraphExecDestroy(g1_);
+    g1_ = nullptr;
+  }
+  learned_ = lc;
+  if (lc) lc->prepare(n_);
+}
+
+// Flexible learned step after an AMG refinement iteration: d = N(r),
+// q = A d, alpha = -(r.q)/(q.q), kept (x += alpha d, r += alpha q) only
+// when the FP64 L1 norm of r + alpha q is below that of r. Scalars stay on
+// the device, so the step is part of the captured iteration graph.
+void LinearSolve::learnedStep(cudaStream_t st) {
+  DevLevel& d = h_.level(0);
+  double* D = work_;
+  double* Q = work_ + (size_t)n_;
+  double* RT = work_ + 2 * (size_t)n_;
+  const nn::Graph g{d.view64(), d.rowSlice, d.nSlices};
+  learned_->apply(g, d.r, D, scal_ + kLsScale, st);
+  dev::spmv(d.view64(), d.nSlices, D, Q, st);
+  dot_into(d.r, Q, scal_ + kLsRq, st);
+  dot_into(Q, Q, scal_ + kLsQq, st);
+  nn::step_alpha(scal_ + kLsRq, scal_ + kLsQq, scal_ + kLsAlpha, st);
+  nn::step_trial(n_, d.r, Q, scal_ + kLsAlpha, RT, partials_, st);
+  dev::sum_partials(dev::vec_blocks(n_), partials_, scal_ + kLsTrial, st);
+  nn::step_accept(n_, d.x, D, d.r, RT, scal_ + kLsAlpha, scal_ + kNorm, scal_ + kLsTrial, st);
+  nn::step_finish(scal_ + kNorm, scal_ + kLsTrial, scal_ + kLsAccepted, scal_ + kLsSteps, st);
+  launches += 19;
+}
+
+int LinearSolve::solveRecording(cudaStream_t st, double relTol, int maxIter, int record,
+                                const std::vector<double*>& rs, const std::vector<double*>& xs, SolveReport& rep) {
+  const SolverOptions& o = h_.options();
+  DevLevel& d = h_.level(0);
+  const size_t nb = sizeof(double) * (size_t)n_;
+  rep = SolveReport();
+  CUDA_OK(cudaMemsetAsync(d.x, 0, nb, st));
+  dev::residual<double>(d.view64(), d.nSlices, d.x, d.b, d.r, d.partials, st);
+  dev::sum_partials(d.nPartials, d.partials, scal_ + kNorm, st);
+  const double r0 = fetch(scal_ + kNorm, st);
+  rep.initialNorm = rep.finalNorm = r0;
+  rep.history.push_back(r0);
+  int recorded = 0;
+  auto keep = [&]() {
+    if (recorded < record) {
+      CUDA_OK(cudaMemcpyAsync(rs[recorded], d.r, nb, cudaMemcpyDeviceToDevice, st));
+      CUDA_OK(cudaMemcpyAsync(xs[recorded], d.x, nb, cudaMemcpyDeviceToDevice, st));
+      recorded++;
+    }
+  };
+  if (!(r0 > 0.0)) return 0;
+  keep();
+  for (int i = 1; i < maxIter; i++) {
+    if (o.precision == kMixed) {
+      dev::convert_d2f(n_, d.r, d.bF, st);
+      dev::zero<float>(n_, d.xF, st);
+      h_.runCycle<float>(st);
+      dev::add_f2d(n_, d.xF, d.x, st);
+    } else {
+      h_.runCycle<double>(st);
+    }
+    dev::residual<double>(d.view64(), d.nSlices, d.x, d.b, d.r, d.partials, st);
+    dev::sum_partials(d.nPartials, d.partials, scal_ + kNorm, st);
+    const double rn = fetch(scal_ + kNorm, st);
+    rep.iterations = i;
+    rep.finalNorm = rn;
+    rep.history.push_back(rn);
+    if (!std::isfinite(rn)) throw Error(kNaN, "residual became non-finite");
+    if (rn / r0 < relTol) {
+      rep.converged = true;
+      break;
+    }
+    keep();
+  }
+  return recorded;
 }
 
 // CG::solve (CG.cpp:26-139) with the AMG cycle as preconditioner.

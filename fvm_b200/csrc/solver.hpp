@@ -15,6 +15,7 @@
 #include "amg_setup.hpp"
 #include "cycle_program.cuh"
 #include "kernels.cuh"
+#include "learned.hpp"
 
 namespace fvm {
 
@@ -57,6 +58,8 @@ struct SolveReport {
   int iterations = 0;
   bool converged = false;
   std::vector<double> history;  // L1 norm after each iteration (index 0 = initial)
+  int learnedSteps = 0;         // learned corrections tried / kept
+  int learnedAccepted = 0;
 };
 
 // Device copy of one level.
@@ -186,6 +189,14 @@ class LinearSolve {
   explicit LinearSolve(AmgHierarchy& h);
   ~LinearSolve();
   SolveReport solve(cudaStream_t st);
+  // Learned correction applied after every refinement iteration of the AMG
+  // solve (null disables); not owned.
+  void setLearned(LearnedCorrection* lc);
+  // AMG iterations to relTol (or maxIter) recording the residual and the
+  // iterate of iterations 0..record-1 into rs[q], xs[q] (device, n each);
+  // returns how many were recorded. The final iterate stays in level 0's x.
+  int solveRecording(cudaStream_t st, double relTol, int maxIter, int record, const std::vector<double*>& rs,
+                     const std::vector<double*>& xs, SolveReport& rep);
 
  private:
   SolveReport solveAMG(cudaStream_t st);
@@ -204,6 +215,8 @@ class LinearSolve {
   double* partials_ = nullptr;
   double* hostScal_ = nullptr;  // pinned
   cudaGraphExec_t g1_ = nullptr, g2_ = nullptr, g3_ = nullptr;
+  LearnedCorrection* learned_ = nullptr;
+  void learnedStep(cudaStream_t st);
   std::map<const void*, long long> nodeCounts_;
   bool graphsFailed_ = false;
 

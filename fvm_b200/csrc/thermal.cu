@@ -326,6 +326,7 @@ void ThermalModel::ensureMatrix() {
   CUDA_OK(cudaMemcpy(dPerm_, hier_.packed(0).perm.data(), sizeof(int) * (size_t)n,
                      cudaMemcpyHostToDevice));
   solver_.reset(new LinearSolve(hier_));
+  solver_->setLearned(learned_);
   lap("solver workspace");
   matrixDirty_ = hierarchyDirty_ = false;
 }
@@ -375,6 +376,8 @@ void ThermalModel::advance(int niter, AdvanceReport& rep) {
     history_.push_back(rNorm);
     rep.iterations++;
     rep.linearIterations += sr.iterations;
+    rep.learnedSteps += sr.learnedSteps;
+    rep.learnedAccepted += sr.learnedAccepted;
     rep.lastNorm = rNorm;
     if (opt_.linear.verbosity >= 0 && opt_.linear.verbosity > 0) printf("%d: %g\n", niters_ - 1, rNorm);
     const double ratio = initialNorm_ > 0 ? rNorm / initialNorm_ : 0.0;
@@ -394,6 +397,63 @@ void ThermalModel::advance(int niter, AdvanceReport& rep) {
   cudaEventDestroy(e1);
   cudaEventDestroy(e2);
   CUDA_OK(cudaGetLastError());
+}
+
+void ThermalModel::setLearned(LearnedCorrection* lc) {
+  learned_ = lc;
+  if (solver_) solver_->setLearned(lc);
+}
+
+namespace {
+__global__ void k_error(int n, const double* __restrict__ xs, const double* __restrict__ x, double* e) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) e[i] = xs[i] - x[i];
+}
+}  // namespace
+
+int ThermalModel::harvest(LearnedCorrection& lc, int nOuter, int perSolve, double relTol, int maxCycles) {
+  FVM_REQUIRE(initialized_, kBadArgument, "ThermalModel.init() must be called first");
+  FVM_REQUIRE(nOuter > 0 && perSolve > 0 && maxCycles > 1 && relTol > 0.0, kBadArgument,
+              "harvest: nOuter, perSolve > 0, maxCycles > 1, relTol > 0");
+  FVM_REQUIRE(opt_.linear.solver == kSolverAMG, kUnsupported, "harvest: the model's linear solver must be AMG");
+  ensureDevice();
+  uploadFields();
+  ensureMatrix();
+  HostMesh& m = *mesh_;
+  const int n = m.nCells;
+  DevLevel& d0 = hier_.level(0);
+  const nn::Graph g{d0.view64(), d0.rowSlice, d0.nSlices};
+  const int inst = lc.addInstance(g, (int)d0.entries, stream_);
+  std::vector<double*> rs(perSolve), xs(perSolve);
+  double* e = nullptr;
+  DeviceArena tmp;
+  for (int q = 0; q < perSolve; q++) {
+    rs[q] = (double*)tmp.alloc(sizeof(double) * (size_t)n);
+    xs[q] = (double*)tmp.alloc(sizeof(double) * (size_t)n);
+  }
+  e = (double*)tmp.alloc(sizeof(double) * (size_t)n);
+  dev::BoundaryData bd{(int)boundaryFaces_.size(), dBFace_, dBKind_, dBValue_};
+  int pairs = 0;
+  for (int it = 0; it < nOuter; it++) {
+    linearize();
+    SolveReport sr;
+    const int rec = solver_->solveRecording(stream_, relTol, maxCycles, perSolve, rs, xs, sr);
+    for (int q = 0; q < rec; q++) {
+      k_error<<<(n + 255) / 256, 256, 0, stream_>>>(n, d0.x, xs[q], e);
+      lc.addPair(inst, rs[q], e, stream_);
+      pairs++;
+    }
+    const double rNorm = sr.initialNorm;
+    if (initialNorm_ < 0) initialNorm_ = rNorm;
+    dev::update_solution(n, dPerm_, d0.x, bd, dFaceCells_, dCoeff_, dBGhost_, dT_, stream_);
+    niters_++;
+    history_.push_back(rNorm);
+    const double ratio = initialNorm_ > 0 ? rNorm / initialNorm_ : 0.0;
+    if (rNorm < opt_.absoluteTolerance || ratio < opt_.relativeTolerance) break;
+  }
+  CUDA_OK(cudaStreamSynchronize(stream_));
+  tDirty_ = false;
+  return pairs;
 }
 
 void ThermalModel::updateTime() {

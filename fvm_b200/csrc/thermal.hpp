@@ -68,6 +68,8 @@ struct AdvanceReport {
   double seconds = 0;      // device time (CUDA events) of the advance call
   double setupSeconds = 0; // part spent rebuilding matrix + hierarchy
   long long launches = 0;
+  int learnedSteps = 0;    // learned corrections tried / kept (all outer iterations)
+  int learnedAccepted = 0;
 };
 
 class ThermalModel {
@@ -102,6 +104,16 @@ class ThermalModel {
   void profile(int reps, double* out);
   const std::vector<double>& history() const { return history_; }
   cudaStream_t stream() const { return stream_; }
+
+  // Learned correction used by the AMG solve of advance() (null disables;
+  // not owned).
+  void setLearned(LearnedCorrection* lc);
+  // Runs up to nOuter outer iterations like advance(), each linear system
+  // solved to relTol (at most maxCycles cycles) with the configured AMG,
+  // and adds this linear system's graph as a training instance of lc with
+  // the pairs (residual, error) of the first perSolve iterates of every
+  // solve (error = final iterate - iterate). Returns the pairs added.
+  int harvest(LearnedCorrection& lc, int nOuter, int perSolve, double relTol, int maxCycles);
 
  private:
   void ensureDevice();
@@ -138,6 +150,7 @@ class ThermalModel {
   std::vector<int> entryFace_;           // interior-only CSR entry -> face
   CSR interiorConn_;                     // cellCells restricted to self rows / self columns
   AmgHierarchy hier_;
+  LearnedCorrection* learned_ = nullptr;
   std::unique_ptr<LinearSolve> solver_;
 };
 

@@ -202,6 +202,12 @@ class ThermalModelA:
     def updateTime(self) -> None:
         check(_lib.load().fvm_thermal_update_time(self._h))
 
+    def setLearnedCorrection(self, lc) -> None:
+        """Use a trained fvm_b200.learned.LearnedCorrection in the AMG solves
+        of advance() (None disables). The model keeps a reference to it."""
+        check(_lib.load().fvm_thermal_set_learned(self._h, lc.handle() if lc is not None else None))
+        self._learned = lc
+
     def printBCs(self) -> None:
         for k, bc in self._bcMap.items():
             print("Face Group %d:" % k)

@@ -99,6 +99,8 @@ typedef struct fvm_report {
   double seconds;          /* device time, CUDA events around the call */
   double setupSeconds;     /* host+device time rebuilding matrix and AMG levels */
   long long launches;      /* kernels and copies issued (graph nodes counted per replay) */
+  int learnedSteps;        /* learned corrections tried (0 without a learned correction) */
+  int learnedAccepted;     /* ... and kept because they lowered the FP64 residual */
 } fvm_report;
 
 /* Reference AMG defaults (fvmbase/AMG.cpp:15-22) and LinearSolver defaults. */
@@ -207,6 +209,43 @@ int fvm_amg_hierarchy_csr(int n, const int* row, const int* col, const double* d
                           const double* off, const fvm_linear_options* o, int finestLocalSize,
                           int* nLevels, int* sizes, int sizesCap, int* coarseIndex, int ciCap,
                           int* colors, int colorsCap);
+
+/* ---- learned correction (no reference counterpart) ----------------------
+ * A message-passing network on the finest level's cell graph (width 32,
+ * three layers, FP32 weights) predicting the solution error from the FP64
+ * residual; used as a flexible step after every AMG refinement iteration
+ * of advance(), kept only when it lowers the FP64 L1 residual norm. Trained
+ * on the GPU on (residual, error) pairs harvested from the plain solver. */
+typedef struct fvm_learned fvm_learned;
+fvm_learned* fvm_learned_create(unsigned long long seed);
+int fvm_learned_destroy(fvm_learned* l);
+int fvm_learned_num_params(void);
+int fvm_learned_get_params(const fvm_learned* l, float* out, int cap);
+int fvm_learned_set_params(fvm_learned* l, const float* p, int n);
+/* runs up to nOuter outer iterations of t (as fvm_thermal_advance), each
+ * linear system solved to relTol with at most maxCycles AMG cycles; adds
+ * t's finest graph as a training instance with the (residual, error) pairs
+ * of the first perSolve iterates of every solve; *nPairs = pairs added */
+int fvm_learned_harvest(fvm_learned* l, fvm_thermal* t, int nOuter, int perSolve, double relTol,
+                        int maxCycles, int* nPairs);
+int fvm_learned_num_pairs(const fvm_learned* l);
+/* Adam, steps updates on pairs drawn with the seed; losses (optional,
+ * steps entries) gets each step's relative squared error */
+int fvm_learned_train(fvm_learned* l, int steps, float lr, unsigned long long seed, double* losses);
+/* mean relative squared error over all harvested pairs */
+int fvm_learned_evaluate(fvm_learned* l, double* meanLoss);
+/* use l in t's solves (null disables); l must outlive its use by t */
+int fvm_thermal_set_learned(fvm_thermal* t, fvm_learned* l);
+/* The network on a plain CSR graph (implicit diagonal, symmetric
+ * couplings), host buffers: out = correction for residual r; and the
+ * gradient of the relative squared error against e (grad: num_params
+ * floats) with the loss. For checking the kernels against a CPU
+ * restatement. */
+int fvm_learned_forward_csr(fvm_learned* l, int n, const int* row, const int* col, const double* diag,
+                            const double* off, const double* r, double* out);
+int fvm_learned_gradient_csr(fvm_learned* l, int n, const int* row, const int* col, const double* diag,
+                             const double* off, const double* r, const double* e, float* grad,
+                             double* loss);
 
 const char* fvm_last_error(void);
 

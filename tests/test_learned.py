@@ -1,0 +1,194 @@
+"""Learned correction: the CPU restatement of the network (oracle/
+mpnn_oracle.py) against finite differences; the GPU forward and backward
+kernels against that restatement; training on the GPU on pairs harvested
+from the plain solver; and the solve with the learned step, whose converged
+field must still match the reference FP64 solve.
+
+Tolerances: the restatement's gradient matches central differences to 1e-6
+relative (FP64); the GPU kernels run in FP32 with FP32 accumulation, so the
+forward output is compared at 1e-4 relative (L2) and the gradient at 2e-3
+of its largest component; the converged field at 1e-8 relative L2."""
+import numpy as np
+import pytest
+
+from helpers import gpu_model, ref_model, rel_l2
+from oracle import mpnn_oracle as mo
+
+
+def _graph(nx=9, ny=7, seed=0):
+    """Symmetric M-matrix on an nx x ny grid with random couplings."""
+    rng = np.random.default_rng(seed)
+    n = nx * ny
+    idx = np.arange(n).reshape(ny, nx)
+    pairs = []
+    for y in range(ny):
+        for x in range(nx):
+            if x + 1 < nx:
+                pairs.append((idx[y, x], idx[y, x + 1]))
+            if y + 1 < ny:
+                pairs.append((idx[y, x], idx[y + 1, x]))
+    w = rng.uniform(0.1, 2.0, len(pairs))
+    rows = [[] for _ in range(n)]
+    for (a, b), c in zip(pairs, w):
+        rows[a].append((b, c))
+        rows[b].append((a, c))
+    row = np.zeros(n + 1, np.int32)
+    row[1:] = np.cumsum([len(r) for r in rows])
+    col = np.array([j for r in rows for j, _ in r], np.int32)
+    off = np.array([c for r in rows for _, c in r])
+    diag = -np.array([sum(c for _, c in r) for r in rows]) - rng.uniform(0.01, 0.5, n)
+    return row, col, diag, off
+
+
+def _params(seed=1, scale=1.0):
+    rng = np.random.default_rng(seed)
+    return rng.normal(0, 0.3 * scale, mo.N_PARAMS)
+
+
+def test_oracle_gradient_matches_finite_differences():
+    row, col, diag, off = _graph()
+    rng = np.random.default_rng(2)
+    r = rng.normal(size=len(diag))
+    e = rng.normal(size=len(diag))
+    P = _params()
+    loss, g = mo.loss_and_gradient(P, row, col, diag, off, r, e)
+    assert loss > 0
+    h = 1e-6
+    for k in rng.choice(mo.N_PARAMS, 60, replace=False).tolist() + [0, 40, mo.DEC_W, mo.N_PARAMS - 1]:
+        Pp, Pm = P.copy(), P.copy()
+        Pp[k] += h
+        Pm[k] -= h
+        fd = (mo.loss_and_gradient(Pp, row, col, diag, off, r, e)[0] -
+              mo.loss_and_gradient(Pm, row, col, diag, off, r, e)[0]) / (2 * h)
+        assert abs(fd - g[k]) <= 1e-6 * max(1.0, abs(g).max()) + 1e-5 * abs(g[k]), k
+
+
+def test_oracle_output_scales_with_residual():
+    """The input is normalised by the mean Jacobi-scaled residual and the
+    output rescaled by it: N(c r) = c N(r) for c > 0."""
+    row, col, diag, off = _graph(seed=3)
+    r = np.random.default_rng(4).normal(size=len(diag))
+    P = _params(seed=5)
+    a = mo.forward(P, row, col, diag, off, r)
+    b = mo.forward(P, row, col, diag, off, 37.5 * r)
+    np.testing.assert_allclose(b, 37.5 * a, rtol=1e-12, atol=1e-12 * np.abs(b).max())
+
+
+@pytest.mark.gpu
+def test_gpu_forward_matches_oracle():
+    from fvm_b200.learned import LearnedCorrection
+
+    row, col, diag, off = _graph(nx=23, ny=19, seed=6)
+    lc = LearnedCorrection(seed=3)
+    P = lc.getParams().astype(np.float64)
+    rng = np.random.default_rng(7)
+    for trial in range(3):
+        r = rng.normal(size=len(diag)) * 10.0 ** trial
+        out = lc.forward_csr(row, col, diag, off, r)
+        ref = mo.forward(P, row, col, diag, off, r)
+        assert rel_l2(out, ref) <= 1e-4
+
+
+@pytest.mark.gpu
+def test_gpu_gradient_matches_oracle():
+    from fvm_b200.learned import LearnedCorrection
+
+    row, col, diag, off = _graph(nx=31, ny=17, seed=8)
+    lc = LearnedCorrection(seed=4)
+    rng = np.random.default_rng(9)
+    # random parameters with a spread of signs so that every ReLU path is exercised
+    P = rng.normal(0, 0.25, mo.N_PARAMS).astype(np.float32)
+    lc.setParams(P)
+    r = rng.normal(size=len(diag))
+    e = rng.normal(size=len(diag))
+    g, loss = lc.gradient_csr(row, col, diag, off, r, e)
+    lref, gref = mo.loss_and_gradient(P.astype(np.float64), row, col, diag, off, r, e)
+    assert abs(loss - lref) <= 1e-4 * lref
+    assert np.abs(g - gref).max() <= 2e-3 * np.abs(gref).max()
+    # every block of the parameter vector carries gradient
+    for a, b in ((0, 64), (64, 64 + mo.LAYER), (mo.DEC_W, mo.N_PARAMS)):
+        assert np.abs(gref[a:b]).max() > 0
+        assert rel_l2(g[a:b], gref[a:b]) <= 5e-3
+
+
+def _plain(nPre=1, nPost=1):
+    from fvm_b200 import fvmbaseExt
+
+    a = fvmbaseExt.AMG()
+    a.nPreSweeps, a.nPostSweeps = nPre, nPost
+    a.relativeTolerance = 0.1
+    a.nMaxIterations = 200
+    return a
+
+
+def _mixed():
+    from fvm_b200 import fvmbaseExt
+
+    a = _plain(1, 2)
+    a.precision = fvmbaseExt.AMG.MIXED
+    a.coarseSolver = fvmbaseExt.AMG.COARSE_DIRECT
+    a.coarsestSize = 100
+    a.coarseJacobiRows = 1 << 30
+    return a
+
+
+def _case(seed, m=9):
+    from fvm_b200 import meshgen
+
+    mesh, f = meshgen.config1(m=m, seed=seed)
+    return mesh, f, {gid: v for gid, v in f["bc"].items()}, {"conductivity": f["k"], "source": f["s"]}
+
+
+@pytest.mark.gpu
+def test_training_on_harvested_pairs_and_exact_solve(refo):
+    from fvm_b200.learned import LearnedCorrection
+
+    lc = LearnedCorrection(seed=0)
+    # training instances: plain-solver runs on two conductivity draws
+    for seed in (11, 12):
+        mesh, f, bcs, fields = _case(seed)
+        tm, tf, m = gpu_model(mesh, bcs, solver=_plain(), fields=fields, opts={"relativeTolerance": 1e-10})
+        assert lc.harvest(tm, nOuter=6, perSolve=4, relativeTolerance=1e-10) > 0
+    assert lc.numPairs() >= 24
+    before = lc.evaluate()
+    losses = lc.train(steps=400, lr=2e-3, seed=1)
+    after = lc.evaluate()
+    assert np.isfinite(losses).all()
+    assert after < before
+    assert losses[-50:].mean() < losses[:50].mean()
+    # held-out draw: mixed solve with the learned step converges to the reference field
+    mesh, f, bcs, fields = _case(13)
+    tm, tf, m = gpu_model(mesh, bcs, solver=_mixed(), fields=fields, opts={"relativeTolerance": 1e-10})
+    tm.setLearnedCorrection(lc)
+    tm.advance(300)
+    rep = tm.lastReport()
+    assert rep.converged
+    assert rep.learnedSteps > 0
+    T = tf.temperature[m.getCells()][: mesh["nCells"]]
+    r = ref_model(refo, mesh, bcs, fields=fields, n_pre=1, n_post=1, lin_rel=1e-10, max_iter=500, rel=1e-10)
+    r.advance(300)
+    assert rel_l2(T, r.get_field(0)[: mesh["nCells"]]) <= 1e-8
+
+
+@pytest.mark.gpu
+def test_learned_step_never_raises_the_residual():
+    """With untrained (random) weights every step is judged by the FP64
+    residual: rejected steps leave the iteration as it was, so the solve
+    takes the same number of cycles as without the step."""
+    from fvm_b200.learned import LearnedCorrection
+
+    mesh, f, bcs, fields = _case(14, m=7)
+    counts = []
+    for use in (False, True):
+        tm, tf, m = gpu_model(mesh, bcs, solver=_mixed(), fields=fields, opts={"relativeTolerance": 1e-10})
+        if use:
+            lc = LearnedCorrection(seed=99)
+            tm.setLearnedCorrection(lc)
+        tm.advance(300)
+        rep = tm.lastReport()
+        assert rep.converged
+        counts.append((rep.iterations, rep.linearIterations, rep.learnedSteps, rep.learnedAccepted))
+    (o0, c0, s0, a0), (o1, c1, s1, a1) = counts
+    assert s0 == 0 and s1 == c1
+    if a1 == 0:
+        assert (o1, c1) == (o0, c0)

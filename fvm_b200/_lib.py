@@ -119,6 +119,8 @@ _SIGS = {
     "fvm_amg_hierarchy_csr": (ctypes.c_int, [ctypes.c_int, c_int_p, c_int_p, c_double_p, c_double_p,
                                              ctypes.POINTER(LinearOptions), ctypes.c_int, c_int_p, c_int_p,
                                              ctypes.c_int, c_int_p, ctypes.c_int, c_int_p, ctypes.c_int]),
+    "fvm_thermal_set_segments": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, c_int_p]),
+    "fvm_thermal_segments": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, c_double_p, c_double_p, c_int_p]),
     "fvm_learned_create": (ctypes.c_void_p, [ctypes.c_ulonglong]),
     "fvm_learned_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "fvm_learned_num_params": (ctypes.c_int, []),

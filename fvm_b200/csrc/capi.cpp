@@ -563,6 +563,31 @@ struct CsrGraph {
 };
 }  // namespace
 
+int fvm_thermal_set_segments(fvm_thermal* t, int nSeg, const int* cellOffsets) {
+  return guarded([&] {
+    FVM_REQUIRE(t, kBadArgument, "null model");
+    FVM_REQUIRE(nSeg >= 0 && (nSeg == 0 || cellOffsets), kBadArgument, "segments: null offsets");
+    std::vector<int> off;
+    if (nSeg > 0) off.assign(cellOffsets, cellOffsets + nSeg + 1);
+    t->model->setSegments(off);
+  });
+}
+
+int fvm_thermal_segments(const fvm_thermal* t, int cap, double* firstNorm, double* lastNorm, int* convergedAt) {
+  return guarded([&] {
+    FVM_REQUIRE(t, kBadArgument, "null model");
+    std::vector<double> f, l;
+    std::vector<int> c;
+    t->model->segmentStatus(f, l, c);
+    FVM_REQUIRE(cap >= (int)f.size(), kBadArgument, "segments: capacity below the number of segments");
+    for (size_t s = 0; s < f.size(); s++) {
+      if (firstNorm) firstNorm[s] = f[s];
+      if (lastNorm) lastNorm[s] = l[s];
+      if (convergedAt) convergedAt[s] = c[s];
+    }
+  });
+}
+
 fvm_learned* fvm_learned_create(unsigned long long seed) {
   fvm_learned* l = nullptr;
   const int rc = guarded([&] {

@@ -442,7 +442,9 @@ __global__ void k_step_accept(int n, double* __restrict__ x, const double* __res
   }
 }
 
-__global__ void k_step_finish(double* norm, const double* trial, double* accepted, double* steps) {
+__global__ void k_step_finish(double* norm, const double* trial, double* accepted, double* steps,
+                              double* useful, double usefulFactor) {
+  if (trial[0] < usefulFactor * norm[0]) useful[0] += 1.0;
   if (trial[0] < norm[0]) {
     norm[0] = trial[0];
     accepted[0] += 1.0;
@@ -463,8 +465,9 @@ void step_accept(int n, double* x, const double* d, double* r, const double* rt,
                  const double* norm, const double* trialNorm, cudaStream_t st) {
   k_step_accept<<<dev::vec_blocks(n), kBlock, 0, st>>>(n, x, d, r, rt, alpha, norm, trialNorm);
 }
-void step_finish(double* norm, const double* trialNorm, double* accepted, double* steps, cudaStream_t st) {
-  k_step_finish<<<1, 1, 0, st>>>(norm, trialNorm, accepted, steps);
+void step_finish(double* norm, const double* trialNorm, double* accepted, double* steps, double* useful,
+                 double usefulFactor, cudaStream_t st) {
+  k_step_finish<<<1, 1, 0, st>>>(norm, trialNorm, accepted, steps, useful, usefulFactor);
 }
 
 }  // namespace nn

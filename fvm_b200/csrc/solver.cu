@@ -622,6 +622,7 @@ enum Scal {
   kLsTrial,
   kLsAccepted,
   kLsSteps,
+  kLsUseful,
   kNumScal
 };
 constexpr int kWorkVectors = 9;
@@ -639,6 +640,7 @@ LinearSolve::~LinearSolve() {
   if (g1_) cudaGraphExecDestroy(g1_);
   if (g2_) cudaGraphExecDestroy(g2_);
   if (g3_) cudaGraphExecDestroy(g3_);
+  if (g4_) cudaGraphExecDestroy(g4_);
   cudaFree(work_);
   cudaFree(scal_);
   cudaFree(partials_);
@@ -725,7 +727,7 @@ SolveReport LinearSolve::solveAMG(cudaStream_t st) {
   DevLevel& d = h_.level(0);
   SolveReport rep;
   CUDA_OK(cudaMemsetAsync(d.x, 0, sizeof(double) * (size_t)n_, st));
-  if (learned_) CUDA_OK(cudaMemsetAsync(scal_ + kLsAccepted, 0, 2 * sizeof(double), st));
+  if (learned_) CUDA_OK(cudaMemsetAsync(scal_ + kLsAccepted, 0, 3 * sizeof(double), st));
   dev::residual<double>(d.view64(), d.nSlices, d.x, d.b, d.r, d.partials, st);
   dev::sum_partials(d.nPartials, d.partials, scal_ + kNorm, st);
   launches += 3;
@@ -740,7 +742,8 @@ SolveReport LinearSolve::solveAMG(cudaStream_t st) {
     return rep;
   }
   for (int i = 1; i < o.nMaxIterations; i++) {
-    run(g1_, st, [&] {
+    const bool useLs = learned_ && learnedActive_;
+    run(useLs ? g4_ : g1_, st, [&] {
       if (o.precision == kMixed) {
         dev::convert_d2f(n_, d.r, d.bF, st);
         dev::zero<float>(n_, d.xF, st);
@@ -751,11 +754,28 @@ SolveReport LinearSolve::solveAMG(cudaStream_t st) {
       }
       dev::residual<double>(d.view64(), d.nSlices, d.x, d.b, d.r, d.partials, st);
       dev::sum_partials(d.nPartials, d.partials, scal_ + kNorm, st);
-      if (learned_) learnedStep(st);
+      if (useLs) {
+        learnedStep(st);
+        CUDA_OK(cudaMemcpyAsync(hostScal_ + 1, scal_ + kLsAccepted, sizeof(double), cudaMemcpyDeviceToHost, st));
+        CUDA_OK(cudaMemcpyAsync(hostScal_ + 2, scal_ + kLsUseful, sizeof(double), cudaMemcpyDeviceToHost, st));
+      }
       CUDA_OK(cudaMemcpyAsync(hostScal_, scal_ + kNorm, sizeof(double), cudaMemcpyDeviceToHost, st));
     });
     CUDA_OK(cudaStreamSynchronize(st));
     const double rn = hostScal_[0];
+    if (useLs) {
+      // Any step that lowers the residual is kept. The step is retired for
+      // good once it has been tried kLsProbe times and fewer than a quarter
+      // of the tries cut the residual by the factor that pays for its cost
+      // (kLsUsefulFactor).
+      const int kept = (int)hostScal_[1], useful = (int)hostScal_[2];
+      rep.learnedSteps++;
+      lsTries_++;
+      lsKept_ += useful - rep.learnedUseful;
+      rep.learnedAccepted = kept;
+      rep.learnedUseful = useful;
+      if (lsTries_ >= kLsProbe && 4 * lsKept_ < lsTries_) learnedActive_ = false;
+    }
     rep.iterations = i;
     rep.finalNorm = rn;
     rep.history.push_back(rn);
@@ -766,22 +786,17 @@ SolveReport LinearSolve::solveAMG(cudaStream_t st) {
       break;
     }
   }
-  if (learned_) {
-    CUDA_OK(cudaMemcpyAsync(hostScal_, scal_ + kLsAccepted, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
-    CUDA_OK(cudaStreamSynchronize(st));
-    rep.learnedAccepted = (int)hostScal_[0];
-    rep.learnedSteps = (int)hostScal_[1];
-  }
   return rep;
 }
 
 void LinearSolve::setLearned(LearnedCorrection* lc) {
   if (lc != learned_) {
-    // the captured iteration graph changes with the step
-    if (g1_) cudaGraphExecDestroy(g1_);
-    g1_ = nullptr;
+    if (g4_) cudaGraphExecDestroy(g4_);
+    g4_ = nullptr;
   }
   learned_ = lc;
+  learnedActive_ = true;
+  lsTries_ = lsKept_ = 0;
   if (lc) lc->prepare(n_);
 }
 
@@ -803,7 +818,8 @@ void LinearSolve::learnedStep(cudaStream_t st) {
   nn::step_trial(n_, d.r, Q, scal_ + kLsAlpha, RT, partials_, st);
   dev::sum_partials(dev::vec_blocks(n_), partials_, scal_ + kLsTrial, st);
   nn::step_accept(n_, d.x, D, d.r, RT, scal_ + kLsAlpha, scal_ + kNorm, scal_ + kLsTrial, st);
-  nn::step_finish(scal_ + kNorm, scal_ + kLsTrial, scal_ + kLsAccepted, scal_ + kLsSteps, st);
+  nn::step_finish(scal_ + kNorm, scal_ + kLsTrial, scal_ + kLsAccepted, scal_ + kLsSteps, scal_ + kLsUseful,
+                  kLsUsefulFactor, st);
   launches += 19;
 }
 

@@ -58,8 +58,9 @@ struct SolveReport {
   int iterations = 0;
   bool converged = false;
   std::vector<double> history;  // L1 norm after each iteration (index 0 = initial)
-  int learnedSteps = 0;         // learned corrections tried / kept
-  int learnedAccepted = 0;
+  int learnedSteps = 0;         // learned corrections tried / kept /
+  int learnedAccepted = 0;      // kept with a residual cut that pays for the step
+  int learnedUseful = 0;
 };
 
 // Device copy of one level.
@@ -214,8 +215,15 @@ class LinearSolve {
   double* scal_ = nullptr;    // device scalars
   double* partials_ = nullptr;
   double* hostScal_ = nullptr;  // pinned
-  cudaGraphExec_t g1_ = nullptr, g2_ = nullptr, g3_ = nullptr;
+  cudaGraphExec_t g1_ = nullptr, g2_ = nullptr, g3_ = nullptr, g4_ = nullptr;
   LearnedCorrection* learned_ = nullptr;
+  // the learned step stays on while it pays: after kLsProbe tries it is
+  // retired if fewer than a quarter cut the FP64 L1 residual below
+  // kLsUsefulFactor times its value (the step costs several V-cycles)
+  static constexpr int kLsProbe = 8;
+  static constexpr double kLsUsefulFactor = 0.5;
+  bool learnedActive_ = true;
+  int lsTries_ = 0, lsKept_ = 0;
   void learnedStep(cudaStream_t st);
   std::map<const void*, long long> nodeCounts_;
   bool graphsFailed_ = false;

@@ -37,6 +37,8 @@ ThermalModel::~ThermalModel() {
   solver_.reset();
   hier_.release();
   freeDevice();
+  if (dSegOff_) cudaFree(dSegOff_);
+  if (dSegNorm_) cudaFree(dSegNorm_);
 }
 
 void ThermalModel::freeDevice() {
@@ -66,7 +68,76 @@ void ThermalModel::init() {
   initialNorm_ = -1;
   niters_ = 0;
   history_.clear();
+  segFirst_.assign(numSegments(), -1.0);
+  segLast_.assign(numSegments(), -1.0);
+  segConvergedAt_.assign(numSegments(), -1);
   initialized_ = true;
+}
+
+void ThermalModel::setSegments(const std::vector<int>& offsets) {
+  if (dSegOff_) cudaFree(dSegOff_);
+  if (dSegNorm_) cudaFree(dSegNorm_);
+  dSegOff_ = nullptr;
+  dSegNorm_ = nullptr;
+  segOff_.clear();
+  if (!offsets.empty()) {
+    FVM_REQUIRE(offsets.size() >= 2 && offsets.front() == 0 && offsets.back() == mesh_->nCells, kBadArgument,
+                "segments: offsets must start at 0 and end at the number of cells");
+    for (size_t s = 0; s + 1 < offsets.size(); s++)
+      FVM_REQUIRE(offsets[s + 1] > offsets[s], kBadArgument, "segments: offsets must increase");
+    segOff_ = offsets;
+    CUDA_OK(cudaMalloc(&dSegOff_, sizeof(int) * segOff_.size()));
+    CUDA_OK(cudaMemcpy(dSegOff_, segOff_.data(), sizeof(int) * segOff_.size(), cudaMemcpyHostToDevice));
+    CUDA_OK(cudaMalloc(&dSegNorm_, sizeof(double) * (segOff_.size() - 1)));
+  }
+  segFirst_.assign(numSegments(), -1.0);
+  segLast_.assign(numSegments(), -1.0);
+  segConvergedAt_.assign(numSegments(), -1);
+}
+
+void ThermalModel::segmentStatus(std::vector<double>& first, std::vector<double>& last,
+                                 std::vector<int>& convergedAt) const {
+  first = segFirst_;
+  last = segLast_;
+  convergedAt = segConvergedAt_;
+}
+
+namespace {
+// L1 norm of b over each block of cells (reference order; b is in the
+// solver's permuted order), one CUDA block per segment, fixed summation order
+__global__ void k_segment_l1(const int* __restrict__ off, const int* __restrict__ perm, const double* __restrict__ b,
+                             double* out) {
+  __shared__ double red[256];
+  const int s = blockIdx.x;
+  double acc = 0.0;
+  for (int i = off[s] + threadIdx.x; i < off[s + 1]; i += blockDim.x) acc += fabs(b[perm[i]]);
+  red[threadIdx.x] = acc;
+  __syncthreads();
+  for (int o = blockDim.x >> 1; o > 0; o >>= 1) {
+    if ((int)threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[s] = red[0];
+}
+}  // namespace
+
+// Per-block outer test on the L1 norm of this iteration's linear system
+// (b, the residual of the delta form at delta = 0).
+bool ThermalModel::segmentsConverged() {
+  const int ns = numSegments();
+  std::vector<double> v(ns);
+  CUDA_OK(cudaMemcpyAsync(v.data(), dSegNorm_, sizeof(double) * ns, cudaMemcpyDeviceToHost, stream_));
+  CUDA_OK(cudaStreamSynchronize(stream_));
+  bool all = true;
+  for (int s = 0; s < ns; s++) {
+    if (segFirst_[s] < 0) segFirst_[s] = v[s];
+    segLast_[s] = v[s];
+    const double ratio = segFirst_[s] > 0 ? v[s] / segFirst_[s] : 0.0;
+    const bool ok = v[s] < opt_.absoluteTolerance || ratio < opt_.relativeTolerance;
+    if (ok && segConvergedAt_[s] < 0) segConvergedAt_[s] = niters_ - 1;
+    all = all && ok;
+  }
+  return all;
 }
 
 static std::vector<double>& field_ref(int field, std::vector<double>& T, std::vector<double>& k,
@@ -366,6 +437,10 @@ void ThermalModel::advance(int niter, AdvanceReport& rep) {
   for (int it = 0; it < niter; it++) {
     linearize();
     rep.launches += 4;
+    if (dSegNorm_) {
+      k_segment_l1<<<numSegments(), 256, 0, stream_>>>(dSegOff_, dPerm_, hier_.level(0).b, dSegNorm_);
+      rep.launches += 1;
+    }
     SolveReport sr = solver_->solve(stream_);
     const double rNorm = sr.initialNorm;
     if (initialNorm_ < 0) initialNorm_ = rNorm;
@@ -381,7 +456,9 @@ void ThermalModel::advance(int niter, AdvanceReport& rep) {
     rep.lastNorm = rNorm;
     if (opt_.linear.verbosity >= 0 && opt_.linear.verbosity > 0) printf("%d: %g\n", niters_ - 1, rNorm);
     const double ratio = initialNorm_ > 0 ? rNorm / initialNorm_ : 0.0;
-    if (rNorm < opt_.absoluteTolerance || ratio < opt_.relativeTolerance) {
+    const bool done = dSegNorm_ ? segmentsConverged()
+                                : (rNorm < opt_.absoluteTolerance || ratio < opt_.relativeTolerance);
+    if (done) {
       rep.converged = true;
       break;
     }

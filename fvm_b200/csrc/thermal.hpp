@@ -105,6 +105,16 @@ class ThermalModel {
   const std::vector<double>& history() const { return history_; }
   cudaStream_t stream() const { return stream_; }
 
+  // Independent blocks of self cells (a batch of meshes packed into one
+  // model, offsets in cell order, nSeg + 1 entries; empty = one block): the
+  // outer loop of advance() then runs until every block meets the
+  // tolerances on its own L1 residual norm, relative to its own first one.
+  void setSegments(const std::vector<int>& offsets);
+  int numSegments() const { return segOff_.empty() ? 0 : (int)segOff_.size() - 1; }
+  // per block: first and last outer L1 norm, outer iteration (from 0) at
+  // which it first met the tolerances (-1: not yet)
+  void segmentStatus(std::vector<double>& first, std::vector<double>& last, std::vector<int>& convergedAt) const;
+
   // Learned correction used by the AMG solve of advance() (null disables;
   // not owned).
   void setLearned(LearnedCorrection* lc);
@@ -151,6 +161,13 @@ class ThermalModel {
   CSR interiorConn_;                     // cellCells restricted to self rows / self columns
   AmgHierarchy hier_;
   LearnedCorrection* learned_ = nullptr;
+  // blocks of cells with their own convergence test
+  std::vector<int> segOff_;
+  int* dSegOff_ = nullptr;
+  double* dSegNorm_ = nullptr;
+  std::vector<double> segFirst_, segLast_;
+  std::vector<int> segConvergedAt_;
+  bool segmentsConverged();
   std::unique_ptr<LinearSolve> solver_;
 };
 

@@ -457,3 +457,20 @@ def config4(n: int = 200, seed: int = 4) -> tuple[dict, dict]:
     k = lognormal_field(N, 1.0, seed + 100)
     rc = uniform_field(N, 0.5, 2.0, seed + 300)
     return mesh, {"k": k, "s": np.zeros(N), "rc": rc, "bc": {1: ("q", 0.0), 2: ("T", 400.0)}}
+
+
+def config2(n_meshes: int = 512, seed: int = 2, lo: int = 32, hi: int = 256) -> list[tuple[dict, dict]]:
+    """Batch of independent jittered quad meshes with sides drawn from
+    U{lo..hi}: mesh i uses seed + i for its jitter and fields; k ~
+    lognormal(0, 1.5), s ~ U[0,1], the boundary conditions of config0."""
+    rng = np.random.default_rng(seed)
+    sides = rng.integers(lo, hi + 1, n_meshes)
+    out = []
+    for i, n in enumerate(sides):
+        sd = seed + i
+        mesh = quad_mesh(int(n), jitter=0.2, seed=sd)
+        N = mesh["nCells"]
+        k = lognormal_field(N, 1.5, sd + 100)
+        s = uniform_field(N, 0.0, 1.0, sd + 200)
+        out.append((mesh, {"k": k, "s": s, "bc": {1: ("T", 300.0), 2: ("T", 400.0)}}))
+    return out

@@ -202,6 +202,25 @@ class ThermalModelA:
     def updateTime(self) -> None:
         check(_lib.load().fvm_thermal_update_time(self._h))
 
+    def setSegments(self, cellOffsets) -> None:
+        """Blocks of self cells (a batch of independent meshes packed into
+        this model) that must each meet the outer tolerances on their own
+        L1 residual norm; None or [] restores the combined test."""
+        if cellOffsets is None or len(cellOffsets) == 0:
+            check(_lib.load().fvm_thermal_set_segments(self._h, 0, None))
+            self._nseg = 0
+            return
+        off = np.ascontiguousarray(cellOffsets, dtype=np.int32)
+        check(_lib.load().fvm_thermal_set_segments(self._h, len(off) - 1, iptr(off)))
+        self._nseg = len(off) - 1
+
+    def getSegmentStatus(self):
+        """(first L1 norm, last L1 norm, outer iteration of convergence or -1) per block."""
+        n = getattr(self, "_nseg", 0)
+        f, l, c = np.zeros(max(n, 1)), np.zeros(max(n, 1)), np.zeros(max(n, 1), np.int32)
+        check(_lib.load().fvm_thermal_segments(self._h, max(n, 1), dptr(f), dptr(l), iptr(c)))
+        return f[:n], l[:n], c[:n]
+
     def setLearnedCorrection(self, lc) -> None:
         """Use a trained fvm_b200.learned.LearnedCorrection in the AMG solves
         of advance() (None disables). The model keeps a reference to it."""

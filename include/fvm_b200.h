@@ -210,6 +210,18 @@ int fvm_amg_hierarchy_csr(int n, const int* row, const int* col, const double* d
                           int* nLevels, int* sizes, int sizesCap, int* coarseIndex, int ciCap,
                           int* colors, int colorsCap);
 
+/* Batches (no reference counterpart): independent meshes packed into one
+ * model (their disjoint union) solve together; with nSeg blocks of self
+ * cells (cellOffsets: nSeg + 1 ascending offsets from 0 to nCells) the
+ * outer loop runs until EVERY block meets the tolerances on its own L1
+ * residual norm relative to its own first one, instead of the combined
+ * norm the reference's multi-mesh ThermalModel tests
+ * (fvmbase/MultiField.cpp:216-230). nSeg = 0 restores the combined test. */
+int fvm_thermal_set_segments(fvm_thermal* t, int nSeg, const int* cellOffsets);
+/* per block: first and last outer L1 norms and the outer iteration (from
+ * 0) at which it first met the tolerances (-1: not yet) */
+int fvm_thermal_segments(const fvm_thermal* t, int cap, double* firstNorm, double* lastNorm, int* convergedAt);
+
 /* ---- learned correction (no reference counterpart) ----------------------
  * A message-passing network on the finest level's cell graph (width 32,
  * three layers, FP32 weights) predicting the solution error from the FP64

@@ -174,7 +174,8 @@ def test_training_on_harvested_pairs_and_exact_solve(refo):
 def test_learned_step_never_raises_the_residual():
     """With untrained (random) weights every step is judged by the FP64
     residual: rejected steps leave the iteration as it was, so the solve
-    takes the same number of cycles as without the step."""
+    takes the same number of cycles as without the step, and a step that
+    keeps failing is retired."""
     from fvm_b200.learned import LearnedCorrection
 
     mesh, f, bcs, fields = _case(14, m=7)
@@ -189,6 +190,9 @@ def test_learned_step_never_raises_the_residual():
         assert rep.converged
         counts.append((rep.iterations, rep.linearIterations, rep.learnedSteps, rep.learnedAccepted))
     (o0, c0, s0, a0), (o1, c1, s1, a1) = counts
-    assert s0 == 0 and s1 == c1
+    # tried after every refinement iteration until it proves useless (kept
+    # in fewer than a quarter of its first tries), then retired
+    assert s0 == 0 and 0 < s1 <= c1
     if a1 == 0:
         assert (o1, c1) == (o0, c0)
+        assert s1 == 8

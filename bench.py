@@ -189,6 +189,12 @@ def train_learned(gen, inner_rel, seeds=(101, 102), n_outer=4, per_solve=3, step
 
 
 def solver_for(variant: str, inner_rel: float):
+    """plain: the reference's default solver on the GPU -- standalone FP64
+    AMG, V(1,1), multicolour Gauss-Seidel, coarsest level <= 100 rows
+    smoothed. plain-cg: CG preconditioned by that AMG (FP64). mixed /
+    learned: CG preconditioned by the FP32 V-cycle (FP64 refinement by the
+    CG, FP64 dense inverse on the coarsest level <= 4096 rows, damped Jacobi
+    below the finest level, V(1,2))."""
     from fvm_b200 import fvmbaseExt
 
     amg = fvmbaseExt.AMG()
@@ -197,17 +203,19 @@ def solver_for(variant: str, inner_rel: float):
     amg.coarsestSize = 100
     amg.relativeTolerance = inner_rel
     amg.nMaxIterations = 200
-    if variant == "mixed":
-        # FP32 V-cycle under FP64 refinement; the coarsest level (<= 4096
-        # rows) is solved by a dense FP64-built inverse instead of smoothed;
-        # the levels below the finest smooth with damped Jacobi (2 launches
-        # per sweep instead of 2C-1 colour passes); one pre-, two post-sweeps
+    if variant in ("mixed", "learned"):
         amg.precision = fvmbaseExt.AMG.MIXED
         amg.coarseSolver = fvmbaseExt.AMG.COARSE_DIRECT
         amg.coarsestSize = 4096
         amg.coarseJacobiRows = 1 << 30
         amg.jacobiWeight = 2.0 / 3.0
         amg.nPostSweeps = 2
+    if variant in ("plain-cg", "mixed", "learned"):
+        cg = fvmbaseExt.CG()
+        cg.preconditioner = amg
+        cg.relativeTolerance = inner_rel
+        cg.nMaxIterations = 200
+        return cg
     return amg
 
 
@@ -310,8 +318,8 @@ def main():
                     help="inner AMG relative tolerance (ThermalModel default 0.1)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-reps", type=int, default=5)
-    ap.add_argument("--variants", default="plain,mixed,learned",
-                    help="comma list of plain, mixed, learned (mixed + learned correction)")
+    ap.add_argument("--variants", default="plain,plain-cg,mixed,learned",
+                    help="comma list of plain, plain-cg, mixed, learned (mixed + learned correction)")
     ap.add_argument("--train-steps", type=int, default=600)
     args = ap.parse_args()
 
@@ -356,7 +364,7 @@ def main():
     if "learned" in variants:
         lc, learned_info = train_learned(gen, args.inner_rel, steps=args.train_steps)
     for variant in variants:
-        solve = Solve(mesh, fields, "mixed" if variant == "learned" else variant, args.inner_rel)
+        solve = Solve(mesh, fields, variant, args.inner_rel)
         if variant == "learned":
             solve.tm.setLearnedCorrection(lc)
         for _ in range(args.warmup):
@@ -450,15 +458,18 @@ def main():
             "config": {
                 "workload": desc,
                 "cells": n_cells,
-                "solver": ("mixed: FP32 AMG V(1,2) under FP64 refinement, multicolour GS on the finest level, "
-                           "damped Jacobi (w=2/3) below, dense FP64 inverse on the coarsest level (<= 4096 rows); "
-                           "plain: FP64 AMG V(1,1), multicolour GS on every level, coarsest <= 100 rows smoothed"),
+                "solver": ("mixed+learned: CG (FP64) preconditioned by an FP32 AMG V(1,2) -- multicolour GS on the "
+                           "finest level, damped Jacobi (w=2/3) below, dense FP64 inverse on the coarsest level "
+                           "(<= 4096 rows) -- with the learned initial correction (kept only when it lowers the FP64 "
+                           "residual, retired when it does not pay); plain: standalone FP64 AMG V(1,1), multicolour "
+                           "GS on every level, coarsest <= 100 rows smoothed (the reference's default solver)"),
                 "outer_rel": 1e-10,
                 "inner_rel": args.inner_rel,
                 "l2": "working set > 126 MB L2 (kernel timings flush L2 with a 512 MB write)",
                 "parallelism": "replicas" if args.gpus > 1 else "single GPU",
             },
             "plain_fp64_s": plain["dev"],
+            "plain_fp64_cg_s": results["plain-cg"]["dev"] if "plain-cg" in results else None,
             "mixed_without_learned_s": mixed["dev"],
             "speedup_vs_plain_fp64": plain["dev"] / head["dev"],
             "mixed_vs_plain_rel_l2": rel_err,

@@ -40,6 +40,7 @@ class LinearOptions(ctypes.Structure):
         ("useGraphs", ctypes.c_int),
         ("coarseJacobiRows", ctypes.c_int),
         ("jacobiWeight", ctypes.c_double),
+        ("preconditioner", ctypes.c_int),
     ]
 
 
@@ -101,6 +102,7 @@ _SIGS = {
                                                   ctypes.c_int]),
     "fvm_thermal_advance": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(Report)]),
     "fvm_thermal_update_time": (ctypes.c_int, [ctypes.c_void_p]),
+    "fvm_thermal_heat_flux_integral": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, c_double_p]),
     "fvm_thermal_history": (ctypes.c_int, [ctypes.c_void_p, c_double_p, ctypes.c_int, c_int_p]),
     "fvm_thermal_linear_system": (ctypes.c_int, [ctypes.c_void_p, c_double_p, c_double_p, c_double_p, c_int_p]),
     "fvm_thermal_hierarchy": (ctypes.c_int, [ctypes.c_void_p, c_int_p, c_int_p, ctypes.c_int, c_int_p,

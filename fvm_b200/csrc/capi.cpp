@@ -59,7 +59,10 @@ int guarded(F f) {
 
 SolverOptions to_solver(const fvm_linear_options& o) {
   SolverOptions s;
-  FVM_REQUIRE(o.solver >= 0 && o.solver <= 2, kBadArgument, "solver must be 0 (AMG), 1 (CG) or 2 (BCGStab)");
+  FVM_REQUIRE(o.solver >= 0 && o.solver <= 3, kBadArgument,
+              "solver must be 0 (AMG), 1 (CG), 2 (BCGStab) or 3 (Jacobi)");
+  FVM_REQUIRE(o.preconditioner == 0 || o.preconditioner == 1, kBadArgument,
+              "preconditioner must be 0 (AMG) or 1 (Jacobi)");
   FVM_REQUIRE(o.cycleType >= 0 && o.cycleType <= 2, kBadArgument, "cycleType must be 0 (V), 1 (W) or 2 (F)");
   FVM_REQUIRE(o.smootherType == 0 || o.smootherType == 1, kBadArgument, "smootherType must be 0 or 1");
   FVM_REQUIRE(o.nMaxIterations >= 0 && o.maxCoarseLevels >= 0 && o.nPreSweeps >= 0 &&
@@ -87,6 +90,7 @@ SolverOptions to_solver(const fvm_linear_options& o) {
   FVM_REQUIRE(o.jacobiWeight > 0.0 && o.jacobiWeight <= 1.0, kBadArgument, "jacobiWeight must be in (0, 1]");
   s.coarseJacobiRows = o.coarseJacobiRows;
   s.jacobiWeight = o.jacobiWeight;
+  s.preconditioner = o.preconditioner == 1 ? kPrecJacobi : kPrecAMG;
   return s;
 }
 
@@ -111,6 +115,7 @@ void from_solver(const SolverOptions& s, fvm_linear_options& o) {
   o.useGraphs = s.useGraphs ? 1 : 0;
   o.coarseJacobiRows = s.coarseJacobiRows;
   o.jacobiWeight = s.jacobiWeight;
+  o.preconditioner = s.preconditioner;
 }
 
 RefLevel level_from_csr(int n, const int* row, const int* col, const double* diag, const double* off) {
@@ -292,6 +297,14 @@ int fvm_thermal_set_bc(fvm_thermal* h, int mesh, int groupId, int bcType, const 
     b.type = (BcType)bcType;
     if (values)
       for (int i = 0; i < 5; i++) b.values[i] = values[i];
+  });
+}
+
+int fvm_thermal_heat_flux_integral(fvm_thermal* h, int mesh, int groupId, double* out) {
+  return guarded([&] {
+    FVM_REQUIRE(h && out, kBadArgument, "null argument");
+    FVM_REQUIRE(mesh == 0, kBadArgument, "mesh index out of range");
+    *out = h->model->heatFluxIntegral(groupId);
   });
 }
 

@@ -566,12 +566,49 @@ __global__ void k_face_flux(FaceGeom g, const double* __restrict__ coeff,
   flux[f] = coeff[f] * (x[c1] - x[c0]) + s;
 }
 
+// Ghost row of a flux-type boundary face as GenericBCS leaves it
+// (GenericBCS.h:111-323), from the face flux of the face loop: the ghost's
+// rhs bj and diagonal ajj, and the boundary heat flux with its derivative
+// with respect to the ghost value (the post-solve flux update).
+__device__ __forceinline__ void flux_bc(int kind, double q, const double* p, double x1, double flux, double am,
+                                        double c, double& bj, double& ajj, double& hfB, double& hfR) {
+  const double sb = 5.670373E-8;
+  const double fluxI = -(0.0 - flux);
+  ajj = 0.0 - c;
+  hfR = 0.0;
+  if (kind == kBkFlux) {
+    bj = q * am - fluxI;
+    hfB = q * am;
+  } else if (kind == kBkConvective) {
+    const double h = p[0], xi = p[1];
+    const double fb = -h * (x1 - xi) * am;
+    bj = fb - fluxI;
+    ajj -= h * am;
+    hfB = fb;
+    hfR = -h * am;
+  } else if (kind == kBkRadiative) {
+    const double xi = p[1], e = p[2];
+    const double fb = -e * sb * (x1 * x1 * x1 * x1 - xi * xi * xi * xi) * am;
+    bj = fb - fluxI;
+    ajj -= 4 * e * sb * x1 * x1 * x1 * am;
+    hfB = fb;
+    hfR = -4 * e * sb * x1 * x1 * x1 * am;
+  } else {  // mixed; its flux derivative omits h, as the reference's does
+    const double h = p[0], xi = p[1], e = p[2];
+    const double fb = (-e * sb * (x1 * x1 * x1 * x1 - xi * xi * xi * xi) - h * (x1 - xi)) * am;
+    bj = fb - fluxI;
+    ajj -= (4 * e * sb * x1 * x1 * x1 + h) * am;
+    hfB = fb;
+    hfR = -4 * e * sb * x1 * x1 * x1 * am;
+  }
+}
+
 __global__ void k_assemble_rhs(int nCells, CellFaceView cf, const int* __restrict__ fc,
                                const double* __restrict__ flux, const double* __restrict__ coeff,
                                const double* __restrict__ am, const double* __restrict__ vol,
                                const double* __restrict__ source, const double* __restrict__ rhoVdt,
                                const double* __restrict__ xN1, BoundaryData bd,
-                               const int* __restrict__ bIndexOfFace, double* x, double* bGhost,
+                               const int* __restrict__ bIndexOfFace, double* x,
                                const int* __restrict__ perm, double* b) {
   FVM_PDL();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -589,27 +626,38 @@ __global__ void k_assemble_rhs(int nCells, CellFaceView cf, const int* __restric
   r += vol[i] * source[i];
   // TimeDerivativeDiscretization (first order)
   if (rhoVdt) r -= rhoVdt[i] * (x[i] - xN1[i]);
-  // GenericBCS::applyDirichletBC: r0 += a01 (Tb - x1); ghost takes Tb
+  // GenericBCS::applyDirichletBC: r0 += a01 (Tb - x1); ghost takes Tb; the
+  // boundary heat flux is the face flux plus a01 (Tb - x1) - a01 dx0
   for (int k = cf.bRow[i]; k < cf.bRow[i + 1]; k++) {
     const int f = cf.bCol[k];
     const int t = bIndexOfFace[f];
-    if (bd.kind[t] == 0) {
+    if (bd.kind[t] == kBkDirichlet) {
       const int c1 = fc[2 * f + 1];
       const double dX = bd.value[t] - x[c1];
       r += coeff[f] * dX;
+      bd.hf[4 * t] = -(0.0 - flux[f]);
+      bd.hf[4 * t + 1] = -(0.0 - coeff[f]) * dX;
+      bd.hf[4 * t + 2] = -coeff[f];
+      bd.hf[4 * t + 3] = 0.0;
       x[c1] = bd.value[t];
     }
   }
-  // applyNeumannBC sets the ghost row's rhs; eliminateBoundaryEquations
-  // then folds it into the interior row: b_i -= a_ij (b_j / a_jj)
+  // flux-type conditions set the ghost row; eliminateBoundaryEquations then
+  // folds it into the interior row, ghosts by ascending index:
+  // b_i -= a_ij (b_j / a_jj)
   for (int k = cf.bRow[i]; k < cf.bRow[i + 1]; k++) {
     const int f = cf.bColG[k];
     const int t = bIndexOfFace[f];
-    if (bd.kind[t] == 1) {
-      const double fluxB = -(0.0 - flux[f]);
-      const double bj = bd.value[t] * am[f] - fluxB;
-      const double ajj = 0.0 - coeff[f];
-      bGhost[t] = bj;
+    const int kind = bd.kind[t];
+    if (kind != kBkDirichlet) {
+      double bj, ajj, hfB, hfR;
+      flux_bc(kind, bd.value[t], bd.param + 3 * t, x[fc[2 * f + 1]], flux[f], am[f], coeff[f], bj, ajj, hfB, hfR);
+      bd.ghostRhs[t] = bj;
+      bd.ghostDiag[t] = ajj;
+      bd.hf[4 * t] = hfB;
+      bd.hf[4 * t + 1] = 0.0;
+      bd.hf[4 * t + 2] = 0.0;
+      bd.hf[4 * t + 3] = hfR;
       r -= coeff[f] * (bj / ajj);
     }
   }
@@ -617,8 +665,10 @@ __global__ void k_assemble_rhs(int nCells, CellFaceView cf, const int* __restric
 }
 
 __global__ void k_assemble_matrix(int nCells, CellFaceView cf, const int* __restrict__ fc,
-                                  const double* __restrict__ coeff, const double* __restrict__ rhoVdt,
-                                  BoundaryData bd, const int* __restrict__ bIndexOfFace, double* diag) {
+                                  const double* __restrict__ coeff, const double* __restrict__ am,
+                                  const double* __restrict__ rhoVdt, BoundaryData bd,
+                                  const int* __restrict__ bIndexOfFace, const double* __restrict__ x,
+                                  double* diag) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nCells) return;
   double d = 0.0;
@@ -626,9 +676,12 @@ __global__ void k_assemble_matrix(int nCells, CellFaceView cf, const int* __rest
   if (rhoVdt) d -= rhoVdt[i];
   for (int k = cf.bRow[i]; k < cf.bRow[i + 1]; k++) {
     const int f = cf.bColG[k];
-    if (bd.kind[bIndexOfFace[f]] == 1) {
+    const int t = bIndexOfFace[f];
+    const int kind = bd.kind[t];
+    if (kind != kBkDirichlet) {
+      double bj, ajj, hfB, hfR;
+      flux_bc(kind, bd.value[t], bd.param + 3 * t, x[fc[2 * f + 1]], 0.0, am[f], coeff[f], bj, ajj, hfB, hfR);
       const double aij = coeff[f];
-      const double ajj = 0.0 - coeff[f];
       d -= aij * (aij / ajj);
     }
   }
@@ -653,21 +706,28 @@ __global__ void k_update_self(int nCells, const int* __restrict__ perm, const do
   if (i < nCells) x[i] = x[i] + delta[perm[i]];
 }
 
-// Neumann ghost rows: delta_j = -(b_j + a_ji delta_i) / a_jj with
-// a_ji = c_f, a_jj = -c_f (CRMatrix::solveBoundary); Dirichlet ghosts keep
-// delta 0. Runs after k_update_self, so delta_i is read from the delta array.
+// Ghost rows of flux-type conditions: delta_j = -(b_j + a_ji delta_i) / a_jj
+// with a_ji = c_f (CRMatrix::solveBoundary); Dirichlet ghosts keep delta 0.
+// Then the boundary heat flux: q += -(r_q + (L dx0 + R dx1)) / (-1)
+// (FluxJacobianMatrix::multiplyAndAdd, DiagonalMatrix::solveBoundary).
 __global__ void k_update_ghosts(BoundaryData bd, const int* __restrict__ perm,
                                 const double* __restrict__ delta, const int* __restrict__ fc,
-                                const double* __restrict__ coeff, const double* __restrict__ bGhost,
-                                double* x) {
+                                const double* __restrict__ coeff, double* x) {
   FVM_PDL();
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= bd.nBFaces || bd.kind[t] != 1) return;
+  if (t >= bd.nBFaces) return;
   const int f = bd.bFace[t];
   const int c0 = fc[2 * f], c1 = fc[2 * f + 1];
-  const double sum = bGhost[t] + coeff[f] * delta[perm[c0]];
-  const double dj = -sum / (0.0 - coeff[f]);
-  x[c1] = x[c1] + dj;
+  const double dx0 = delta[perm[c0]];
+  double dx1 = 0.0;
+  if (bd.kind[t] != kBkDirichlet) {
+    const double sum = bd.ghostRhs[t] + coeff[f] * dx0;
+    dx1 = -sum / bd.ghostDiag[t];
+    x[c1] = x[c1] + dx1;
+  }
+  const double* h = bd.hf + 4 * t;
+  const double rq = h[1] + (h[2] * dx0 + h[3] * dx1);
+  bd.heatFlux[t] = h[0] + (-rq / -1.0);
 }
 
 }  // namespace
@@ -852,17 +912,17 @@ void face_flux(const FaceGeom& g, const double* coeff, const double* secCoeff, c
 void assemble_rhs(int nCells, const CellFaceView& cf, const int* faceCells, const double* flux,
                   const double* coeff, const double* faceAreaMag, const double* vol,
                   const double* source, const double* rhoVdt, const double* xN1,
-                  const BoundaryData& bd, const int* bIndexOfFace, double* x, double* bGhost,
-                  const int* perm, double* b, cudaStream_t st) {
+                  const BoundaryData& bd, const int* bIndexOfFace, double* x, const int* perm, double* b,
+                  cudaStream_t st) {
   pdl_launch(k_assemble_rhs, ceil_div(nCells, kBlock), kBlock, st, nCells, cf, faceCells, flux, coeff,
                                                               faceAreaMag, vol, source, rhoVdt, xN1,
-                                                              bd, bIndexOfFace, x, bGhost, perm, b);
+                                                              bd, bIndexOfFace, x, perm, b);
 }
 void assemble_matrix(int nCells, const CellFaceView& cf, const int* faceCells, const double* coeff,
-                     const double* rhoVdt, const BoundaryData& bd, const int* bIndexOfFace,
-                     double* diagOrig, cudaStream_t st) {
-  k_assemble_matrix<<<ceil_div(nCells, kBlock), kBlock, 0, st>>>(nCells, cf, faceCells, coeff, rhoVdt,
-                                                                 bd, bIndexOfFace, diagOrig);
+                     const double* faceAreaMag, const double* rhoVdt, const BoundaryData& bd,
+                     const int* bIndexOfFace, const double* x, double* diagOrig, cudaStream_t st) {
+  k_assemble_matrix<<<ceil_div(nCells, kBlock), kBlock, 0, st>>>(nCells, cf, faceCells, coeff, faceAreaMag,
+                                                                 rhoVdt, bd, bIndexOfFace, x, diagOrig);
 }
 void transient_coeff(int n, const double* rhoCp, const double* vol, double dt, double* out,
                      cudaStream_t st) {
@@ -872,12 +932,10 @@ void cast_d2f_vals(int n, const double* a, float* b, cudaStream_t st) {
   k_cast_d2f<<<ceil_div(n, kBlock), kBlock, 0, st>>>(n, a, b);
 }
 void update_solution(int nCells, const int* perm, const double* delta, const BoundaryData& bd,
-                     const int* faceCells, const double* coeff, const double* bGhost, double* x,
-                     cudaStream_t st) {
+                     const int* faceCells, const double* coeff, double* x, cudaStream_t st) {
   pdl_launch(k_update_self, ceil_div(nCells, kBlock), kBlock, st, nCells, perm, delta, x);
   if (bd.nBFaces > 0)
-    pdl_launch(k_update_ghosts, ceil_div(bd.nBFaces, kBlock), kBlock, st, bd, perm, delta, faceCells, coeff,
-                                                                     bGhost, x);
+    pdl_launch(k_update_ghosts, ceil_div(bd.nBFaces, kBlock), kBlock, st, bd, perm, delta, faceCells, coeff, x);
 }
 
 // explicit instantiations

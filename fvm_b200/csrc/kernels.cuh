@@ -137,12 +137,20 @@ void ghost_gradient(int nBFaces, const int* bFaces, const int* faceCells, double
 void face_flux(const FaceGeom& g, const double* coeff, const double* secCoeff,
                const double* grad, const double* x, double* flux, cudaStream_t st);
 
-// Per boundary face: BC kind (0 Dirichlet, 1 Neumann/Symmetry) and value
+// Per boundary face (in face order): the condition and what the
+// linearization records for the post-solve update (GenericBCS.h:77-323,
+// LinearSystem::postSolve).
+enum BoundaryKind { kBkDirichlet = 0, kBkFlux = 1, kBkConvective = 2, kBkRadiative = 3, kBkMixed = 4 };
 struct BoundaryData {
   int nBFaces;
   const int* bFace;     // face index of each boundary face
-  const int* kind;      // 0 Dirichlet, 1 Neumann
+  const int* kind;      // BoundaryKind; Symmetry is a zero specified flux
   const double* value;  // specified temperature or heat flux
+  const double* param;  // 3 per face: convective coefficient, far-field temperature, emissivity
+  double* ghostRhs;     // per face: the ghost row's rhs after the condition (not Dirichlet)
+  double* ghostDiag;    // per face: the ghost row's diagonal after the condition (not Dirichlet)
+  double* hf;           // 4 per face: heat flux at linearization, its rhs, d/dx0, d/dx1
+  double* heatFlux;     // per face: heat flux after the update
 };
 struct CellFaceView {
   const int* row;  // cellFaces over self cells
@@ -159,13 +167,13 @@ struct CellFaceView {
 void assemble_rhs(int nCells, const CellFaceView& cf, const int* faceCells, const double* flux,
                   const double* coeff, const double* faceAreaMag, const double* vol,
                   const double* source, const double* rhoVdt, const double* xN1,
-                  const BoundaryData& bd, const int* bIndexOfFace, double* x, double* bGhost,
-                  const int* perm, double* b, cudaStream_t st);
+                  const BoundaryData& bd, const int* bIndexOfFace, double* x, const int* perm, double* b,
+                  cudaStream_t st);
 // The matrix part (constant while conductivity, geometry and time step are):
 // diagonal of every self cell and the off-diagonals through entryFace.
 void assemble_matrix(int nCells, const CellFaceView& cf, const int* faceCells, const double* coeff,
-                     const double* rhoVdt, const BoundaryData& bd, const int* bIndexOfFace,
-                     double* diagOrig, cudaStream_t st);
+                     const double* faceAreaMag, const double* rhoVdt, const BoundaryData& bd,
+                     const int* bIndexOfFace, const double* x, double* diagOrig, cudaStream_t st);
 // rhoVdt_i = rho c_i V_i / dt
 void transient_coeff(int nCells, const double* rhoCp, const double* vol, double dt, double* out,
                      cudaStream_t st);
@@ -174,11 +182,11 @@ void gather_offdiag(int nEntries, const int* entryFace, const double* coeff, dou
                     cudaStream_t st);
 void gather_diag(int n, const int* iperm, const double* diagOrig, double* diag, cudaStream_t st);
 void cast_d2f_vals(int n, const double* a, float* b, cudaStream_t st);
-// T_i += delta[perm[i]] on self cells; Neumann ghosts solve their boundary
-// row and update too (LinearSystem::postSolve + updateSolution)
+// T_i += delta[perm[i]] on self cells; the ghosts of flux-type conditions
+// solve their boundary row and update too, and every boundary face's heat
+// flux takes its update (LinearSystem::postSolve + updateSolution)
 void update_solution(int nCells, const int* perm, const double* delta, const BoundaryData& bd,
-                     const int* faceCells, const double* coeff, const double* bGhost, double* x,
-                     cudaStream_t st);
+                     const int* faceCells, const double* coeff, double* x, cudaStream_t st);
 
 }  // namespace dev
 }  // namespace fvm

@@ -75,7 +75,7 @@ void AmgHierarchy::build(std::vector<RefLevel>& levels, int finestLocalSize, con
   ref_ = std::move(levels);
   levels.clear();
   HierarchyOptions ho;
-  ho.maxCoarseLevels = opt.maxCoarseLevels;
+  ho.maxCoarseLevels = opt.finestOnly() ? 0 : opt.maxCoarseLevels;
   ho.groupSize = opt.coarseGroupSize;
   ho.weightRatioThreshold = opt.weightRatioThreshold;
   ho.coarsestSize = opt.coarsestSize;
@@ -98,7 +98,7 @@ void AmgHierarchy::build(std::vector<RefLevel>& levels, int finestLocalSize, con
   std::exception_ptr err0;
   std::thread level0([&] {
     try {
-      pack_level(ref_[0], opt.ordering, p0);
+      pack_level(ref_[0], opt.finestOnly() ? kSequential : opt.ordering, p0);
       uploadMatrix(p0, d0, mixed);
     } catch (...) {
       err0 = std::current_exception();
@@ -146,7 +146,7 @@ void AmgHierarchy::build(std::vector<RefLevel>& levels, int finestLocalSize, con
   void* gjScratch = nullptr;
   const PackedLevel& c = packed_[L - 1];
   const size_t nn = (size_t)c.n * c.n;
-  if (opt.coarseSolver == kCoarseDirect) {
+  if (opt.coarseSolver == kCoarseDirect && !opt.finestOnly()) {
     FVM_REQUIRE(c.n <= 4096, kTooLarge,
                 "coarsest level too large for the dense direct solve (max 4096 rows); set coarsestSize");
     if (c.n <= 128) {
@@ -175,7 +175,7 @@ void AmgHierarchy::build(std::vector<RefLevel>& levels, int finestLocalSize, con
   for (int l = 1; l < L; l++) uploadMatrix(packed_[l], lv_[l], mixed);
   for (int l = 0; l + 1 < L; l++) uploadTransfer(packed_[l], lv_[l], packed_[l + 1].n);
   lap("uploads");
-  if (opt.coarseSolver == kCoarseDirect) {
+  if (opt.coarseSolver == kCoarseDirect && !opt.finestOnly()) {
     if (gjStream) {
       int singular = 0;
       const cudaError_t e1 = cudaMemcpyAsync(&singular, dev::gauss_jordan_status(c.n, gjScratch), sizeof(int),
@@ -530,6 +530,13 @@ void AmgHierarchy::cycle(CycleType t, int l, cudaStream_t st) {
 
 void AmgHierarchy::apply(const double* r, double* z, cudaStream_t st) {
   DevLevel& d = lv_[0];
+  if (opt_.preconditioner == kPrecJacobi) {
+    // JacobiSolver::smooth: two Jacobi sweeps from zero with b = r
+    dev::zero<double>(d.n, z, st);
+    dev::jacobi<double>(d.view64(), d.nSlices, z, d.tmp, r, st);
+    dev::jacobi<double>(d.view64(), d.nSlices, d.tmp, z, r, st);
+    return;
+  }
   if (opt_.precision == kMixed) {
     dev::convert_d2f(d.n, r, d.bF, st);
     dev::zero<float>(d.n, d.xF, st);
@@ -641,6 +648,7 @@ LinearSolve::~LinearSolve() {
   if (g2_) cudaGraphExecDestroy(g2_);
   if (g3_) cudaGraphExecDestroy(g3_);
   if (g4_) cudaGraphExecDestroy(g4_);
+  if (g5_) cudaGraphExecDestroy(g5_);
   cudaFree(work_);
   cudaFree(scal_);
   cudaFree(partials_);
@@ -707,6 +715,9 @@ SolveReport LinearSolve::solve(cudaStream_t st) {
     case kSolverBCGStab:
       r = solveBCGStab(st);
       break;
+    case kSolverJacobi:
+      r = solveJacobi(st);
+      break;
     default:
       r = solveAMG(st);
   }
@@ -755,7 +766,7 @@ SolveReport LinearSolve::solveAMG(cudaStream_t st) {
       dev::residual<double>(d.view64(), d.nSlices, d.x, d.b, d.r, d.partials, st);
       dev::sum_partials(d.nPartials, d.partials, scal_ + kNorm, st);
       if (useLs) {
-        learnedStep(st);
+        learnedStep(st, d.x, d.r);
         CUDA_OK(cudaMemcpyAsync(hostScal_ + 1, scal_ + kLsAccepted, sizeof(double), cudaMemcpyDeviceToHost, st));
         CUDA_OK(cudaMemcpyAsync(hostScal_ + 2, scal_ + kLsUseful, sizeof(double), cudaMemcpyDeviceToHost, st));
       }
@@ -789,6 +800,47 @@ SolveReport LinearSolve::solveAMG(cudaStream_t st) {
   return rep;
 }
 
+// JacobiSolver::solve (fvmbase/JacobiSolver.cpp:42-80): one Jacobi sweep
+// per iteration, same stopping test as the AMG solve.
+SolveReport LinearSolve::solveJacobi(cudaStream_t st) {
+  const SolverOptions& o = h_.options();
+  DevLevel& d = h_.level(0);
+  SolveReport rep;
+  CUDA_OK(cudaMemsetAsync(d.x, 0, sizeof(double) * (size_t)n_, st));
+  dev::residual<double>(d.view64(), d.nSlices, d.x, d.b, d.r, d.partials, st);
+  dev::sum_partials(d.nPartials, d.partials, scal_ + kNorm, st);
+  launches += 3;
+  const double r0 = fetch(scal_ + kNorm, st);
+  rep.initialNorm = rep.finalNorm = r0;
+  rep.history.push_back(r0);
+  if (!std::isfinite(r0)) throw Error(kNaN, "initial residual is not finite");
+  if (r0 < o.absoluteTolerance) {
+    rep.converged = true;
+    return rep;
+  }
+  for (int i = 1; i < o.nMaxIterations; i++) {
+    run(g5_, st, [&] {
+      dev::jacobi<double>(d.view64(), d.nSlices, d.x, d.tmp, d.b, st);
+      dev::copy_d(n_, d.tmp, d.x, st);
+      dev::residual<double>(d.view64(), d.nSlices, d.x, d.b, d.r, d.partials, st);
+      dev::sum_partials(d.nPartials, d.partials, scal_ + kNorm, st);
+      CUDA_OK(cudaMemcpyAsync(hostScal_, scal_ + kNorm, sizeof(double), cudaMemcpyDeviceToHost, st));
+    });
+    CUDA_OK(cudaStreamSynchronize(st));
+    const double rn = hostScal_[0];
+    rep.iterations = i;
+    rep.finalNorm = rn;
+    rep.history.push_back(rn);
+    if (o.verbosity > 0) printf("%d: %g\n", i, rn);
+    if (!std::isfinite(rn)) throw Error(kNaN, "residual became non-finite");
+    if (stop_test(rn, r0, o)) {
+      rep.converged = true;
+      break;
+    }
+  }
+  return rep;
+}
+
 void LinearSolve::setLearned(LearnedCorrection* lc) {
   if (lc != learned_) {
     if (g4_) cudaGraphExecDestroy(g4_);
@@ -804,20 +856,20 @@ void LinearSolve::setLearned(LearnedCorrection* lc) {
 // q = A d, alpha = -(r.q)/(q.q), kept (x += alpha d, r += alpha q) only
 // when the FP64 L1 norm of r + alpha q is below that of r. Scalars stay on
 // the device, so the step is part of the captured iteration graph.
-void LinearSolve::learnedStep(cudaStream_t st) {
+void LinearSolve::learnedStep(cudaStream_t st, double* x, double* r) {
   DevLevel& d = h_.level(0);
-  double* D = work_;
-  double* Q = work_ + (size_t)n_;
-  double* RT = work_ + 2 * (size_t)n_;
+  double* D = work_ + 6 * (size_t)n_;
+  double* Q = work_ + 7 * (size_t)n_;
+  double* RT = work_ + 8 * (size_t)n_;
   const nn::Graph g{d.view64(), d.rowSlice, d.nSlices};
-  learned_->apply(g, d.r, D, scal_ + kLsScale, st);
+  learned_->apply(g, r, D, scal_ + kLsScale, st);
   dev::spmv(d.view64(), d.nSlices, D, Q, st);
-  dot_into(d.r, Q, scal_ + kLsRq, st);
+  dot_into(r, Q, scal_ + kLsRq, st);
   dot_into(Q, Q, scal_ + kLsQq, st);
   nn::step_alpha(scal_ + kLsRq, scal_ + kLsQq, scal_ + kLsAlpha, st);
-  nn::step_trial(n_, d.r, Q, scal_ + kLsAlpha, RT, partials_, st);
+  nn::step_trial(n_, r, Q, scal_ + kLsAlpha, RT, partials_, st);
   dev::sum_partials(dev::vec_blocks(n_), partials_, scal_ + kLsTrial, st);
-  nn::step_accept(n_, d.x, D, d.r, RT, scal_ + kLsAlpha, scal_ + kNorm, scal_ + kLsTrial, st);
+  nn::step_accept(n_, x, D, r, RT, scal_ + kLsAlpha, scal_ + kNorm, scal_ + kLsTrial, st);
   nn::step_finish(scal_ + kNorm, scal_ + kLsTrial, scal_ + kLsAccepted, scal_ + kLsSteps, scal_ + kLsUseful,
                   kLsUsefulFactor, st);
   launches += 19;
@@ -896,6 +948,20 @@ SolveReport LinearSolve::solveCG(cudaStream_t st) {
   rep.history.push_back(r0);
   if (o.verbosity > 0) printf("0: %g\n", r0);
   if (!std::isfinite(r0)) throw Error(kNaN, "initial residual is not finite");
+  if (learned_ && learnedActive_ && r0 > 0.0) {
+    // learned initial correction of the delta, kept only if it lowers the
+    // FP64 residual; CG then starts from it
+    CUDA_OK(cudaMemsetAsync(scal_ + kLsAccepted, 0, 3 * sizeof(double), st));
+    learnedStep(st, X, R);
+    CUDA_OK(cudaMemcpyAsync(hostScal_, scal_ + kLsAccepted, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CUDA_OK(cudaStreamSynchronize(st));
+    rep.learnedSteps = 1;
+    rep.learnedAccepted = (int)hostScal_[0];
+    rep.learnedUseful = (int)hostScal_[2];
+    lsTries_++;
+    lsKept_ += rep.learnedUseful;
+    if (lsTries_ >= kLsProbe && 4 * lsKept_ < lsTries_) learnedActive_ = false;
+  }
   for (int i = 0; i < o.nMaxIterations; i++) {
     run(g1_, st, [&] {
       h_.apply(R, Z, st);

@@ -23,7 +23,8 @@ enum CycleType { kVCycle = 0, kWCycle = 1, kFCycle = 2 };
 enum SmootherType { kGaussSeidel = 0, kJacobi = 1 };
 enum CoarseSolver { kCoarseSmooth = 0, kCoarseDirect = 1 };
 enum Precision { kFP64 = 0, kMixed = 1 };
-enum SolverKind { kSolverAMG = 0, kSolverCG = 1, kSolverBCGStab = 2 };
+enum SolverKind { kSolverAMG = 0, kSolverCG = 1, kSolverBCGStab = 2, kSolverJacobi = 3 };
+enum PreconditionerKind { kPrecAMG = 0, kPrecJacobi = 1 };
 
 struct SolverOptions {
   SolverKind solver = kSolverAMG;
@@ -50,6 +51,11 @@ struct SolverOptions {
   // rows smooth with damped Jacobi (weight jacobiWeight) instead; 0 = never
   int coarseJacobiRows = 0;
   double jacobiWeight = 2.0 / 3.0;
+  // preconditioner of CG / BCGStab: one AMG cycle, or two Jacobi sweeps
+  // (JacobiSolver::smooth, fvmbase/JacobiSolver.cpp:27-100)
+  PreconditionerKind preconditioner = kPrecAMG;
+  // only the finest level is needed (Jacobi solver or preconditioner)
+  bool finestOnly() const { return solver == kSolverJacobi || preconditioner == kPrecJacobi; }
 };
 
 struct SolveReport {
@@ -203,6 +209,7 @@ class LinearSolve {
   SolveReport solveAMG(cudaStream_t st);
   SolveReport solveCG(cudaStream_t st);
   SolveReport solveBCGStab(cudaStream_t st);
+  SolveReport solveJacobi(cudaStream_t st);
   void norm_into(const double* v, double* scalar, cudaStream_t st);
   void dot_into(const double* a, const double* b, double* scalar, cudaStream_t st);
   double fetch(const double* scalar, cudaStream_t st);
@@ -215,7 +222,7 @@ class LinearSolve {
   double* scal_ = nullptr;    // device scalars
   double* partials_ = nullptr;
   double* hostScal_ = nullptr;  // pinned
-  cudaGraphExec_t g1_ = nullptr, g2_ = nullptr, g3_ = nullptr, g4_ = nullptr;
+  cudaGraphExec_t g1_ = nullptr, g2_ = nullptr, g3_ = nullptr, g4_ = nullptr, g5_ = nullptr;
   LearnedCorrection* learned_ = nullptr;
   // the learned step stays on while it pays: after kLsProbe tries it is
   // retired if fewer than a quarter cut the FP64 L1 residual below
@@ -224,7 +231,7 @@ class LinearSolve {
   static constexpr double kLsUsefulFactor = 0.5;
   bool learnedActive_ = true;
   int lsTries_ = 0, lsKept_ = 0;
-  void learnedStep(cudaStream_t st);
+  void learnedStep(cudaStream_t st, double* x, double* r);
   std::map<const void*, long long> nodeCounts_;
   bool graphsFailed_ = false;
 

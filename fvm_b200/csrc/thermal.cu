@@ -282,6 +282,11 @@ void ThermalModel::ensureDevice() {
   dBKind_ = (int*)arena_.alloc(sizeof(int) * (nB + 1));
   dBValue_ = (double*)arena_.alloc(sizeof(double) * (nB + 1));
   dBGhost_ = (double*)arena_.alloc(sizeof(double) * (nB + 1));
+  dBParam_ = (double*)arena_.alloc(sizeof(double) * 3 * (nB + 1));
+  dBGhostDiag_ = (double*)arena_.alloc(sizeof(double) * (nB + 1));
+  dHf_ = (double*)arena_.alloc(sizeof(double) * 4 * (nB + 1));
+  dHeatFlux_ = (double*)arena_.alloc(sizeof(double) * (nB + 1));
+  CUDA_OK(cudaMemset(dHeatFlux_, 0, sizeof(double) * (nB + 1)));
   const size_t cb = sizeof(double) * (size_t)nAll;
   dT_ = (double*)arena_.alloc(cb);
   dK_ = (double*)arena_.alloc(cb);
@@ -309,40 +314,59 @@ void ThermalModel::uploadFields() {
   if (tn1Dirty_) CUDA_OK(cudaMemcpyAsync(dTN1_, TN1_.data(), cb, cudaMemcpyHostToDevice, stream_));
   CUDA_OK(cudaStreamSynchronize(stream_));
   tDirty_ = kDirty_ = srcDirty_ = rcDirty_ = tn1Dirty_ = false;
-  // boundary kinds and values (cheap; a change of kind changes the matrix)
+  // boundary kinds and values (cheap; a change of kind or of a value the
+  // matrix depends on changes the matrix)
   const int nB = (int)boundaryFaces_.size();
   std::vector<int> kind(nB + 1, 0);
-  std::vector<double> val(nB + 1, 0.0);
+  std::vector<double> val(nB + 1, 0.0), par(3 * (nB + 1), 0.0);
   int t = 0;
+  matrixDependsOnT_ = false;
   for (size_t g = 1; g < mesh_->groups.size(); g++) {
     const FaceGroup& fg = mesh_->groups[g];
     const GroupBC& b = bc(fg.id);
     int k;
-    double v;
+    double v = 0.0;
     switch (b.type) {
       case kBcSpecifiedTemperature:
-        k = 0;
+        k = dev::kBkDirichlet;
         v = b.values[0];
         break;
       case kBcSpecifiedHeatFlux:
-        k = 1;
+        k = dev::kBkFlux;
         v = b.values[1];
         break;
       case kBcSymmetry:
-        k = 1;
-        v = 0.0;
+        k = dev::kBkFlux;
+        break;
+      case kBcConvective:
+        k = dev::kBkConvective;
+        break;
+      case kBcRadiative:
+        k = dev::kBkRadiative;
+        matrixDependsOnT_ = true;
+        break;
+      case kBcMixed:
+        k = dev::kBkMixed;
+        matrixDependsOnT_ = true;
         break;
       default:
-        throw Error(kUnsupported,
-                    "boundary condition type not available on the GPU path (Convective/Radiative/Mixed)");
+        throw Error(kUnsupported, "unknown boundary condition type");
     }
     for (int f = 0; f < fg.size; f++, t++) {
       kind[t] = k;
       val[t] = v;
+      par[3 * t] = b.values[2];      // convectiveCoefficient
+      par[3 * t + 1] = b.values[3];  // farFieldTemperature
+      par[3 * t + 2] = b.values[4];  // surfaceEmissivity
     }
   }
   CUDA_OK(cudaMemcpy(dBKind_, kind.data(), sizeof(int) * (nB + 1), cudaMemcpyHostToDevice));
   CUDA_OK(cudaMemcpy(dBValue_, val.data(), sizeof(double) * (nB + 1), cudaMemcpyHostToDevice));
+  CUDA_OK(cudaMemcpy(dBParam_, par.data(), sizeof(double) * 3 * (nB + 1), cudaMemcpyHostToDevice));
+  if (par != bParamHost_) {
+    bParamHost_ = par;
+    matrixDirty_ = true;
+  }
   if (kind != bKindHost_) {
     bKindHost_ = kind;
     matrixDirty_ = true;
@@ -350,7 +374,9 @@ void ThermalModel::uploadFields() {
 }
 
 void ThermalModel::ensureMatrix() {
-  if (!matrixDirty_ && !hierarchyDirty_) return;
+  // a matrix that depends on T (radiative / mixed conditions) is rebuilt
+  // for every linearization
+  if (!matrixDirty_ && !hierarchyDirty_ && !matrixDependsOnT_) return;
   const bool trace = getenv("FVM_TRACE") != nullptr;
   auto t0 = std::chrono::steady_clock::now();
   auto lap = [&](const char* what) {
@@ -371,8 +397,8 @@ void ThermalModel::ensureMatrix() {
     rhoVdt = dRhoVdt_;
   }
   dev::CellFaceView cf{dCfRow_, dCfCol_, dBRow_, dBCol_, dBColG_};
-  dev::BoundaryData bd{(int)boundaryFaces_.size(), dBFace_, dBKind_, dBValue_};
-  dev::assemble_matrix(n, cf, dFaceCells_, dCoeff_, rhoVdt, bd, dBIndexOfFace_, dDiagOrig_, stream_);
+  const dev::BoundaryData bd = boundaryData();
+  dev::assemble_matrix(n, cf, dFaceCells_, dCoeff_, dAreaMag_, rhoVdt, bd, dBIndexOfFace_, dT_, dDiagOrig_, stream_);
   std::vector<double> coeff(F), diag(n);
   CUDA_OK(cudaMemcpyAsync(coeff.data(), dCoeff_, sizeof(double) * F, cudaMemcpyDeviceToHost, stream_));
   CUDA_OK(cudaMemcpyAsync(diag.data(), dDiagOrig_, sizeof(double) * n, cudaMemcpyDeviceToHost, stream_));
@@ -410,9 +436,9 @@ void ThermalModel::linearize() {
   dev::FaceGeom g{F, n, dFaceCells_, dArea_, dAreaMag_, dCentroid_, dVol_};
   dev::face_flux(g, dCoeff_, dSec_, dGrad_, dT_, dFlux_, stream_);
   dev::CellFaceView cf{dCfRow_, dCfCol_, dBRow_, dBCol_, dBColG_};
-  dev::BoundaryData bd{(int)boundaryFaces_.size(), dBFace_, dBKind_, dBValue_};
+  const dev::BoundaryData bd = boundaryData();
   dev::assemble_rhs(n, cf, dFaceCells_, dFlux_, dCoeff_, dAreaMag_, dVol_, dSrc_,
-                    opt_.transient ? dRhoVdt_ : nullptr, dTN1_, bd, dBIndexOfFace_, dT_, dBGhost_,
+                    opt_.transient ? dRhoVdt_ : nullptr, dTN1_, bd, dBIndexOfFace_, dT_,
                     dPerm_, hier_.level(0).b, stream_);
 }
 
@@ -433,8 +459,16 @@ void ThermalModel::advance(int niter, AdvanceReport& rep) {
   CUDA_OK(cudaEventRecord(e1, stream_));
   const long long launches0 = solver_->launches;
   HostMesh& m = *mesh_;
-  dev::BoundaryData bd{(int)boundaryFaces_.size(), dBFace_, dBKind_, dBValue_};
+  const dev::BoundaryData bd = boundaryData();
   for (int it = 0; it < niter; it++) {
+    if (matrixDependsOnT_ && it > 0) {
+      // radiative / mixed conditions: the ghost diagonals follow T, so the
+      // matrix and its AMG levels are rebuilt every outer iteration, as the
+      // reference rebuilds them
+      const auto s2 = std::chrono::steady_clock::now();
+      ensureMatrix();
+      rep.setupSeconds += std::chrono::duration<double>(std::chrono::steady_clock::now() - s2).count();
+    }
     linearize();
     rep.launches += 4;
     if (dSegNorm_) {
@@ -444,7 +478,7 @@ void ThermalModel::advance(int niter, AdvanceReport& rep) {
     SolveReport sr = solver_->solve(stream_);
     const double rNorm = sr.initialNorm;
     if (initialNorm_ < 0) initialNorm_ = rNorm;
-    dev::update_solution(m.nCells, dPerm_, hier_.level(0).x, bd, dFaceCells_, dCoeff_, dBGhost_, dT_,
+    dev::update_solution(m.nCells, dPerm_, hier_.level(0).x, bd, dFaceCells_, dCoeff_, dT_,
                          stream_);
     rep.launches += 2;
     niters_++;
@@ -476,6 +510,39 @@ void ThermalModel::advance(int niter, AdvanceReport& rep) {
   CUDA_OK(cudaGetLastError());
 }
 
+dev::BoundaryData ThermalModel::boundaryData() const {
+  dev::BoundaryData bd;
+  bd.nBFaces = (int)boundaryFaces_.size();
+  bd.bFace = dBFace_;
+  bd.kind = dBKind_;
+  bd.value = dBValue_;
+  bd.param = dBParam_;
+  bd.ghostRhs = dBGhost_;
+  bd.ghostDiag = dBGhostDiag_;
+  bd.hf = dHf_;
+  bd.heatFlux = dHeatFlux_;
+  return bd;
+}
+
+double ThermalModel::heatFluxIntegral(int groupId) {
+  FVM_REQUIRE(initialized_, kBadArgument, "ThermalModel.init() must be called first");
+  const HostMesh& m = *mesh_;
+  int t = 0;
+  for (size_t g = 1; g < m.groups.size(); g++) {
+    const FaceGroup& fg = m.groups[g];
+    if (fg.id == groupId) {
+      std::vector<double> q(fg.size, 0.0);
+      if (deviceReady_ && fg.size > 0)
+        CUDA_OK(cudaMemcpy(q.data(), dHeatFlux_ + t, sizeof(double) * fg.size, cudaMemcpyDeviceToHost));
+      double r = 0.0;
+      for (int f = 0; f < fg.size; f++) r += q[f];
+      return r;
+    }
+    t += fg.size;
+  }
+  throw Error(kBadArgument, "getHeatFluxIntegral: invalid faceGroupID");
+}
+
 void ThermalModel::setLearned(LearnedCorrection* lc) {
   learned_ = lc;
   if (solver_) solver_->setLearned(lc);
@@ -495,6 +562,8 @@ int ThermalModel::harvest(LearnedCorrection& lc, int nOuter, int perSolve, doubl
   FVM_REQUIRE(opt_.linear.solver == kSolverAMG, kUnsupported, "harvest: the model's linear solver must be AMG");
   ensureDevice();
   uploadFields();
+  FVM_REQUIRE(!matrixDependsOnT_, kUnsupported,
+              "harvest: radiative / mixed conditions make the matrix change every iteration");
   ensureMatrix();
   HostMesh& m = *mesh_;
   const int n = m.nCells;
@@ -509,7 +578,7 @@ int ThermalModel::harvest(LearnedCorrection& lc, int nOuter, int perSolve, doubl
     xs[q] = (double*)tmp.alloc(sizeof(double) * (size_t)n);
   }
   e = (double*)tmp.alloc(sizeof(double) * (size_t)n);
-  dev::BoundaryData bd{(int)boundaryFaces_.size(), dBFace_, dBKind_, dBValue_};
+  const dev::BoundaryData bd = boundaryData();
   int pairs = 0;
   for (int it = 0; it < nOuter; it++) {
     linearize();
@@ -522,7 +591,7 @@ int ThermalModel::harvest(LearnedCorrection& lc, int nOuter, int perSolve, doubl
     }
     const double rNorm = sr.initialNorm;
     if (initialNorm_ < 0) initialNorm_ = rNorm;
-    dev::update_solution(n, dPerm_, d0.x, bd, dFaceCells_, dCoeff_, dBGhost_, dT_, stream_);
+    dev::update_solution(n, dPerm_, d0.x, bd, dFaceCells_, dCoeff_, dT_, stream_);
     niters_++;
     history_.push_back(rNorm);
     const double ratio = initialNorm_ > 0 ? rNorm / initialNorm_ : 0.0;

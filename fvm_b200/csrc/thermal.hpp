@@ -103,6 +103,9 @@ class ThermalModel {
   // [9] kernels per cycle, [10] colours of level 0
   void profile(int reps, double* out);
   const std::vector<double>& history() const { return history_; }
+  // ThermalModel::getHeatFluxIntegral (ThermalModel_impl.h:400-422): sum of
+  // the boundary heat flux over a face group, as the last advance() left it
+  double heatFluxIntegral(int groupId);
   cudaStream_t stream() const { return stream_; }
 
   // Independent blocks of self cells (a batch of meshes packed into one
@@ -155,8 +158,12 @@ class ThermalModel {
   double *dGradW_ = nullptr, *dGrad_ = nullptr, *dFlux_ = nullptr, *dCoeff_ = nullptr, *dSec_ = nullptr;
   double *dT_ = nullptr, *dK_ = nullptr, *dSrc_ = nullptr, *dRc_ = nullptr, *dTN1_ = nullptr;
   double *dRhoVdt_ = nullptr, *dBValue_ = nullptr, *dBGhost_ = nullptr, *dDiagOrig_ = nullptr;
+  double *dBParam_ = nullptr, *dBGhostDiag_ = nullptr, *dHf_ = nullptr, *dHeatFlux_ = nullptr;
+  bool matrixDependsOnT_ = false;  // radiative / mixed conditions: the matrix follows T
+  dev::BoundaryData boundaryData() const;
   std::vector<int> boundaryFaces_;       // boundary faces in face order
   std::vector<int> bKindHost_;           // boundary kinds last uploaded
+  std::vector<double> bParamHost_;       // and their h / far-field / emissivity
   std::vector<int> entryFace_;           // interior-only CSR entry -> face
   CSR interiorConn_;                     // cellCells restricted to self rows / self columns
   AmgHierarchy hier_;

@@ -239,6 +239,33 @@ class AMG(LinearSolver):
         return hierarchy_csr(self.options(), row, col, diag, off, finestLocalSize)
 
 
+class JacobiSolver(LinearSolver):
+    """Point Jacobi (fvmbase/JacobiSolver.cpp:27-100): as a solver one
+    sweep per iteration; as the preconditioner of CG / BCGStab two sweeps
+    from zero (JacobiSolver::smooth)."""
+
+    def _fill(self, o: _lib.LinearOptions, solver_kind: int = 0, outer=None) -> None:
+        src = outer if outer is not None else self
+        d = _lib.default_linear_options()
+        ctypes.memmove(ctypes.byref(o), ctypes.byref(d), ctypes.sizeof(o))
+        o.solver = 3 if solver_kind == 0 else solver_kind
+        o.preconditioner = 1
+        o.maxCoarseLevels = 0
+        o.nMaxIterations = int(src.nMaxIterations)
+        o.relativeTolerance = float(src.relativeTolerance)
+        o.absoluteTolerance = float(src.absoluteTolerance)
+        o.verbosity = int(src.verbosity)
+
+    def options(self) -> _lib.LinearOptions:
+        o = _lib.LinearOptions()
+        self._fill(o)
+        return o
+
+    def solve_csr(self, row, col, diag, off, b):
+        """Solves b + A x = 0 from x = 0 with Jacobi sweeps."""
+        return _solve_csr(self.options(), row, col, diag, off, b, self)
+
+
 class _KrylovSolver(LinearSolver):
     _kind = 0
 

@@ -234,8 +234,12 @@ class ThermalModelA:
             for name, v in bc.items():
                 print("   %s %s" % (name, v))
 
-    def getHeatFluxIntegral(self, mesh, faceGroupId: int):
-        raise _lib.FvmError(7, "getHeatFluxIntegral is not available on the GPU path yet")
+    def getHeatFluxIntegral(self, mesh, faceGroupId: int) -> float:
+        """Sum of the boundary heat flux over a face group after the last
+        advance() (ThermalModel::getHeatFluxIntegral)."""
+        out = ctypes.c_double(0)
+        check(_lib.load().fvm_thermal_heat_flux_integral(self._h, 0, int(faceGroupId), ctypes.byref(out)))
+        return out.value
 
     def dumpMatrix(self, fileBase: str) -> None:
         """MatrixMarket dump of the current linearization, in the format of

@@ -74,6 +74,7 @@ typedef struct fvm_linear_options {
   int coarseJacobiRows;     /* levels below the finest with at most this many rows smooth with
                                damped Jacobi instead of multicolour Gauss-Seidel (0: never) */
   double jacobiWeight;      /* damping of that Jacobi smoother (default 2/3) */
+  int preconditioner;       /* of CG / BCGStab: 0 one AMG cycle, 1 two Jacobi sweeps (JacobiSolver) */
 } fvm_linear_options;
 
 /* ThermalModelOptions (fvmbase/ThermalBC.h:33-67) + volume-condition constants */
@@ -150,6 +151,11 @@ int fvm_thermal_get_cell_field(fvm_thermal* t, int mesh, int field, double* out,
 int fvm_thermal_advance(fvm_thermal* t, int niter, fvm_report* rep);
 /* ThermalModel::updateTime (fvmbase/ThermalModel_impl.h:472-495) */
 int fvm_thermal_update_time(fvm_thermal* t);
+/* ThermalModel::getHeatFluxIntegral (fvmbase/ThermalModel_impl.h:400-422):
+ * sum over the boundary face group of the heat flux the last advance()
+ * left (the linearization's boundary flux plus its post-solve update,
+ * LinearSystem::postSolve, fvmbase/LinearSystem.cpp:250-263) */
+int fvm_thermal_heat_flux_integral(fvm_thermal* t, int mesh, int groupId, double* out);
 /* outer L1 norms printed by advance(), one per iteration since init() */
 int fvm_thermal_history(const fvm_thermal* t, double* norms, int cap, int* n);
 /* The linearization advance() solves (ThermalModel::dumpMatrix content,

@@ -251,3 +251,8 @@ class RefThermal:
 
     def update_time(self):
         _check(load().ref_thermal_update_time(self.h))
+
+    def heat_flux_integral(self, group_id: int) -> float:
+        out = ctypes.c_double()
+        _check(load().ref_thermal_heat_flux_integral(self.h, int(group_id), ctypes.byref(out)))
+        return out.value

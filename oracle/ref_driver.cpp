@@ -48,6 +48,7 @@
 #include "GradientModel.h"
 #include "CG.h"
 #include "BCGStab.h"
+#include "JacobiSolver.h"
 #include "LinearSystem.h"
 #include "MultiFieldMatrix.h"
 #include "CRMatrix.h"
@@ -158,6 +159,7 @@ struct RefModel {
   AMG* amg = nullptr;
   CG* cg = nullptr;
   BCGStab* bcg = nullptr;
+  JacobiSolver* jac = nullptr;
   std::vector<double> history;  // outer rNorm per advance iteration
   ~RefModel() {
     // the reference caches least-squares gradient matrices in a static map
@@ -169,6 +171,7 @@ struct RefModel {
     delete amg;
     delete cg;
     delete bcg;
+    delete jac;
     delete mesh;
   }
 };
@@ -422,7 +425,8 @@ int ref_thermal_set_bc(void* h, int groupId, int bcType, const double* vals) {
 }
 
 // Options mirror ThermalModelOptions plus the linear solver.
-// iopts: [solver(0 AMG,1 CG+AMG,2 BCGStab+AMG), maxCoarseLevels, nPreSweeps,
+// iopts: [solver(0 AMG, 1 CG+AMG, 2 BCGStab+AMG, 3 JacobiSolver,
+//         4 CG+JacobiSolver, 5 BCGStab+JacobiSolver), maxCoarseLevels, nPreSweeps,
 //         nPostSweeps, coarseGroupSize, cycleType, smootherType,
 //         nMaxIterations, transient, linearVerbosity]
 // dopts: [outer relTol, outer absTol, linear relTol, linear absTol,
@@ -435,9 +439,11 @@ int ref_thermal_set_options(void* h, const int* iopts, const double* dopts) {
     delete r->amg;
     delete r->cg;
     delete r->bcg;
+    delete r->jac;
     r->amg = new AMG();
     r->cg = nullptr;
     r->bcg = nullptr;
+    r->jac = nullptr;
     AMG& a = *r->amg;
     a.maxCoarseLevels = iopts[1];
     a.nPreSweeps = iopts[2];
@@ -448,13 +454,19 @@ int ref_thermal_set_options(void* h, const int* iopts, const double* dopts) {
     a.weightRatioThreshold = dopts[4];
     a.verbosity = 0;
     LinearSolver* ls = r->amg;
-    if (iopts[0] == 1) {
+    LinearSolver* pre = r->amg;
+    if (iopts[0] >= 3) {
+      r->jac = new JacobiSolver();
+      r->jac->verbosity = 0;
+      pre = ls = r->jac;
+    }
+    if (iopts[0] == 1 || iopts[0] == 4) {
       r->cg = new CG();
-      r->cg->preconditioner = r->amg;
+      r->cg->preconditioner = pre;
       ls = r->cg;
-    } else if (iopts[0] == 2) {
+    } else if (iopts[0] == 2 || iopts[0] == 5) {
       r->bcg = new BCGStab();
-      r->bcg->preconditioner = r->amg;
+      r->bcg->preconditioner = pre;
       ls = r->bcg;
     }
     ls->nMaxIterations = iopts[7];

@@ -287,3 +287,124 @@ def test_csr_residual_matches_reference_order():
         expect[i] = s
     np.testing.assert_array_equal(r, expect)
     assert abs(nrm - np.abs(expect).sum()) <= 1e-13 * np.abs(expect).sum()
+
+
+# ---------------------------------------------------------------------------
+# JacobiSolver (fvmbase/JacobiSolver.cpp:27-100): standalone and as the
+# preconditioner of CG / BCGStab
+
+
+def test_jacobi_solver_outer_history_matches_reference(refo):
+    """One undamped Jacobi sweep per iteration (bit-identical iterates);
+    the outer norms equal the reference's up to the L1 summation order."""
+    mesh, f = _synthetic("quad")
+    bcs = {gid: v for gid, v in f["bc"].items()}
+    fields = {"conductivity": f["k"], "source": f["s"]}
+    js = fvmbaseExt.JacobiSolver()
+    js.relativeTolerance = 1e-1
+    js.nMaxIterations = 20
+    tm, tf, m = gpu_model(mesh, bcs, solver=js, fields=fields)
+    tm.advance(6)
+    hist = tm.getNormHistory()
+    r = ref_model(refo, mesh, bcs, fields=fields, solver=3, lin_rel=1e-1, max_iter=20)
+    norms, _ = r.advance(6)
+    assert len(hist) == len(norms) == 6
+    np.testing.assert_allclose(hist, norms, rtol=1e-11, atol=0)
+    T = tf.temperature[m.getCells()][: mesh["nCells"]]
+    np.testing.assert_allclose(T, r.get_field(0)[: mesh["nCells"]], rtol=1e-12, atol=0)
+
+
+@pytest.mark.parametrize("kind", ["cg", "bcgstab"])
+def test_krylov_with_jacobi_preconditioner_converges_to_reference(refo, kind):
+    mesh, f = _synthetic("quad")
+    bcs = {gid: v for gid, v in f["bc"].items()}
+    fields = {"conductivity": f["k"], "source": f["s"]}
+    s = fvmbaseExt.CG() if kind == "cg" else fvmbaseExt.BCGStab()
+    s.preconditioner = fvmbaseExt.JacobiSolver()
+    s.relativeTolerance = 1e-10
+    s.nMaxIterations = 2000
+    tm, tf, m = gpu_model(mesh, bcs, solver=s, fields=fields, opts={"relativeTolerance": 1e-10})
+    _converge(tm)
+    T = tf.temperature[m.getCells()][: mesh["nCells"]]
+    r = ref_model(refo, mesh, bcs, fields=fields, solver=4 if kind == "cg" else 5, lin_rel=1e-10, max_iter=2000,
+                  rel=1e-10)
+    r.advance(200)
+    assert rel_l2(T, r.get_field(0)[: mesh["nCells"]]) <= TOL_FIELD
+
+
+# ---------------------------------------------------------------------------
+# every boundary-condition type of ThermalModel::linearize
+# (fvmbase/ThermalModel_impl.h:296-398, GenericBCS.h:77-323) and
+# getHeatFluxIntegral (ThermalModel_impl.h:400-422)
+
+_ALL_BCS = {  # group -> (bcType, specifiedTemperature, specifiedHeatFlux, h, farFieldTemperature, emissivity)
+    1: ("SpecifiedTemperature", 300.0, 0.0, 0.0, 300.0, 1.0),
+    2: ("Convective", 0.0, 0.0, 25.0, 350.0, 1.0),
+    3: ("Radiative", 0.0, 0.0, 0.0, 310.0, 0.7),
+    4: ("Mixed", 0.0, 0.0, 8.0, 320.0, 0.5),
+    5: ("SpecifiedHeatFlux", 0.0, 1.5, 0.0, 300.0, 1.0),
+    6: ("Symmetry", 0.0, 0.0, 0.0, 300.0, 1.0),
+}
+_REF_BC = {"SpecifiedTemperature": 0, "SpecifiedHeatFlux": 1, "Symmetry": 2, "Convective": 3, "Radiative": 4,
+           "Mixed": 5}
+
+
+def _all_bc_models(refo, amg, ref_opts):
+    from fvm_b200 import models
+
+    mesh, f = meshgen.config1(m=6, seed=4)
+    fields = {"conductivity": f["k"], "source": f["s"]}
+    tm, tf, m = gpu_model(mesh, {}, solver=amg, fields=None)
+    for gid, (t, T, q, h, Tinf, eps) in _ALL_BCS.items():
+        bc = tm.getBCMap()[gid]
+        bc.bcType = t
+        for name, v in zip(models.BC_VARS, (T, q, h, Tinf, eps)):
+            bc.setVar(name, v)
+    tm.init()
+    for name, vals in fields.items():
+        getattr(tf, name)[m.getCells()] = vals
+    r = ref_model(refo, mesh, {}, fields=None, **ref_opts)
+    for gid, (t, T, q, h, Tinf, eps) in _ALL_BCS.items():
+        r.set_bc(gid, _REF_BC[t], [T, q, h, Tinf, eps])
+    r.init()
+    from fvm_b200.meshgen import extend_to_ghosts
+
+    r.set_field(1, extend_to_ghosts(mesh, f["k"]))
+    r.set_field(2, extend_to_ghosts(mesh, f["s"]))
+    return mesh, tm, tf, m, r
+
+
+def test_all_boundary_conditions_bit_exact(refo):
+    """Matrix, right-hand side, temperatures and boundary heat-flux
+    integrals after each of three outer iterations equal the reference's
+    bit for bit (reference-ordered Gauss-Seidel); the radiative and mixed
+    conditions make the matrix depend on T, so it is rebuilt every
+    iteration."""
+    amg = _amg(smootherOrdering=fvmbaseExt.AMG.SEQUENTIAL, relativeTolerance=1e-1, nMaxIterations=20)
+    mesh, tm, tf, m, r = _all_bc_models(refo, amg, {})
+    n = mesh["nCells"]
+    for it in range(3):
+        diag, off, b = tm.getLinearSystem()
+        d_ref, o_ref, b_ref, _ = r.linearize()
+        np.testing.assert_array_equal(diag, d_ref[:n], err_msg="diag, outer iteration %d" % it)
+        np.testing.assert_array_equal(b, b_ref[:n], err_msg="b, outer iteration %d" % it)
+        tm.advance(1)
+        r.advance(1)
+        np.testing.assert_array_equal(tf.temperature[m.getCells()], r.get_field(0), err_msg="T, iteration %d" % it)
+        for gid in _ALL_BCS:
+            assert tm.getHeatFluxIntegral(m, gid) == r.heat_flux_integral(gid), (it, gid)
+
+
+def test_all_boundary_conditions_converge_to_reference(refo):
+    amg = _amg(nPreSweeps=1, nPostSweeps=1, relativeTolerance=1e-10, nMaxIterations=500)
+    mesh, tm, tf, m, r = _all_bc_models(refo, amg, dict(n_pre=1, n_post=1, lin_rel=1e-10, max_iter=500,
+                                                        rel=1e-10))
+    tm.getOptions().relativeTolerance = 1e-10
+    _converge(tm)
+    r.advance(200)
+    n = mesh["nCells"]
+    T = tf.temperature[m.getCells()][:n]
+    assert rel_l2(T, r.get_field(0)[:n]) <= TOL_FIELD
+    for gid in _ALL_BCS:
+        a, b = tm.getHeatFluxIntegral(m, gid), r.heat_flux_integral(gid)
+        assert abs(a - b) <= 1e-8 * max(1.0, abs(b)), gid

@@ -13,11 +13,11 @@ namespace {
 // Runs f(begin, end) over [0, n) split into contiguous chunks on the host's
 // cores (one chunk when n is small).
 template <class F>
-void parallel_chunks(int n, F f) {
+void parallel_chunks(int n, F f, int minItems = 20000) {
   int nt = (int)std::thread::hardware_concurrency();
   if (nt < 1) nt = 1;
   if (nt > 32) nt = 32;
-  if (n < 20000 || nt == 1) {
+  if (n < minItems || nt == 1) {
     f(0, n);
     return;
   }
@@ -33,14 +33,16 @@ void parallel_chunks(int n, F f) {
 
 }  // namespace
 
-int create_coarsening(const RefLevel& a, int groupSize, double thr, std::vector<int>& ci) {
-  const int n = a.n;
+namespace {
+// The greedy walk over rows [rb, re) with coarse rows numbered from 0; count
+// has re - rb entries. On a level whose rows [rb, re) couple to no row
+// outside the range, this is exactly the walk of the whole level restricted
+// to the range.
+int coarsen_range(const RefLevel& a, int rb, int re, int groupSize, double thr, int* ci, int* count) {
   const std::vector<int>& row = a.conn.row;
   const std::vector<int>& col = a.conn.col;
-  ci.assign(n, -1);
-  std::vector<int> count(n, 0);
   int nCoarse = 0;
-  for (int nr = 0; nr < n; nr++) {
+  for (int nr = rb; nr < re; nr++) {
     if (ci[nr] != -1) continue;
     int current = nr;
     int colMaxGrouped = -1, colMaxUngrouped = -1;
@@ -86,6 +88,43 @@ int create_coarsening(const RefLevel& a, int groupSize, double thr, std::vector<
     }
   }
   return nCoarse;
+}
+}  // namespace
+
+int create_coarsening(const RefLevel& a, int groupSize, double thr, std::vector<int>& ci,
+                      std::vector<int>* coarseSegments) {
+  const int n = a.n;
+  ci.assign(n, -1);
+  const std::vector<int>& seg = a.segments;
+  if (seg.size() < 3) {  // one block: the reference's walk
+    std::vector<int> count(n, 0);
+    const int nc = coarsen_range(a, 0, n, groupSize, thr, ci.data(), count.data());
+    if (coarseSegments) {
+      coarseSegments->clear();
+      if (!seg.empty()) *coarseSegments = {0, nc};
+    }
+    return nc;
+  }
+  // independent blocks (a batch of meshes): the walks run in parallel, then
+  // each block's coarse rows are shifted behind the previous blocks'
+  const int ns = (int)seg.size() - 1;
+  std::vector<int> nc(ns, 0);
+  parallel_chunks(ns, [&](int b, int e) {
+    std::vector<int> count;
+    for (int s = b; s < e; s++) {
+      count.assign(seg[s + 1] - seg[s], 0);
+      nc[s] = coarsen_range(a, seg[s], seg[s + 1], groupSize, thr, ci.data(), count.data());
+    }
+  }, 1);
+  std::vector<int> off(ns + 1, 0);
+  for (int s = 0; s < ns; s++) off[s + 1] = off[s] + nc[s];
+  parallel_chunks(ns, [&](int b, int e) {
+    for (int s = b; s < e; s++)
+      for (int i = seg[s]; i < seg[s + 1]; i++)
+        if (ci[i] >= 0) ci[i] += off[s];
+  }, 1);
+  if (coarseSegments) *coarseSegments = off;
+  return off[ns];
 }
 
 void create_coarse_level(const RefLevel& fine, RefLevel& coarse, CSR& c2f) {
@@ -180,8 +219,8 @@ void build_hierarchy(std::vector<RefLevel>& levels, const HierarchyOptions& opt,
   coarseToFine.clear();
   for (int n = 0; n < opt.maxCoarseLevels; n++) {
     RefLevel& fine = levels.back();
-    std::vector<int> ci;
-    const int nc = create_coarsening(fine, opt.groupSize, opt.weightRatioThreshold, ci);
+    std::vector<int> ci, coarseSeg;
+    const int nc = create_coarsening(fine, opt.groupSize, opt.weightRatioThreshold, ci, &coarseSeg);
     const int fineLocal = (levels.size() == 1 && opt.finestLocalSize > 0) ? opt.finestLocalSize : fine.n;
     if (fineLocal == nc) break;  // AMG.cpp:161-168
     if (nc <= 3) break;          // AMG.cpp:200-204 (serial: level not kept)
@@ -190,6 +229,7 @@ void build_hierarchy(std::vector<RefLevel>& levels, const HierarchyOptions& opt,
     RefLevel coarse;
     CSR c2f;
     create_coarse_level(fine, coarse, c2f);
+    coarse.segments = std::move(coarseSeg);
     levels.push_back(std::move(coarse));
     coarseToFine.push_back(std::move(c2f));
     if (opt.coarsestSize > 0 && nc <= opt.coarsestSize) break;

@@ -30,12 +30,16 @@ struct RefLevel {
   // the Galerkin levels built from a symmetric level); otherwise the
   // colouring uses the pattern of A + A^T
   bool symmetricPattern = false;
+  // optional row offsets of independent diagonal blocks (a batch of
+  // meshes; no entry couples two blocks): the aggregation of each block
+  // runs in parallel, with the same result as the sequential walk
+  std::vector<int> segments;
 };
 
 // Greedy aggregation (reference CRMatrix::createCoarsening). Returns the
 // number of coarse rows.
 int create_coarsening(const RefLevel& a, int groupSize, double weightRatioThreshold,
-                      std::vector<int>& coarseIndex);
+                      std::vector<int>& coarseIndex, std::vector<int>* coarseSegments = nullptr);
 
 // Coarse-to-fine rows (MultiFieldMatrix::createCoarseToFineMapping), coarse
 // connectivity (CRMatrix::createCoarseConnectivity) and Galerkin values

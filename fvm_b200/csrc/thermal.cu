@@ -409,6 +409,7 @@ void ThermalModel::ensureMatrix() {
   l0.n = n;
   l0.conn = interiorConn_;
   l0.symmetricPattern = true;  // cellCells restricted to self rows
+  l0.segments = segOff_;       // a batch: its meshes aggregate in parallel
   l0.diag = std::move(diag);
   l0.off.resize(entryFace_.size());
   for (size_t e = 0; e < entryFace_.size(); e++) l0.off[e] = coeff[entryFace_[e]];

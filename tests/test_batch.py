@@ -98,3 +98,27 @@ def test_batched_solve_matches_reference_per_mesh(refo, variant):
                       lin_rel=1e-10, max_iter=500, rel=1e-10)
         r.advance(300)
         assert rel_l2(T, r.get_field(0)[: m["nCells"]]) <= 1e-8
+
+
+@pytest.mark.gpu
+def test_parallel_block_aggregation_equals_sequential():
+    """With blocks set, each mesh's aggregation runs on its own thread; the
+    hierarchy (every level's coarseIndex) equals the sequential walk's."""
+    from fvm_b200 import fvmbaseExt
+
+    ms = _batch(n=9, lo=6, hi=30, seed=7)
+    hier = []
+    for blocks in (True, False):
+        amg = fvmbaseExt.AMG()
+        bt = batch.BatchedThermal([m for m, _ in ms], ms[0][1]["bc"], amg)
+        if not blocks:
+            bt.model.setSegments(None)
+        cells = bt.mesh.getCells()
+        bt.model.init()
+        bt.fields.conductivity[cells] = np.concatenate([f["k"] for _, f in ms])
+        bt.fields.source[cells] = np.concatenate([f["s"] for _, f in ms])
+        hier.append(bt.model.getHierarchy())
+    (s1, c1), (s2, c2) = hier
+    assert s1 == s2
+    for a, b in zip(c1, c2):
+        np.testing.assert_array_equal(a, b)

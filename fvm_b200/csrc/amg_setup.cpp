@@ -460,9 +460,32 @@ void pack_level(const RefLevel& lv, SmootherOrdering ordering, PackedLevel& out)
     out.maxWidth = std::max(out.maxWidth, out.sliceOff[s + 1]);
     out.sliceOff[s + 1] = out.sliceOff[s] + 32 * out.sliceOff[s + 1];
   }
-  out.cols.resize(out.sliceOff[nSlices]);
-  out.vals.resize(out.sliceOff[nSlices]);
-  parallel_chunks(nSlices, [&](int b, int e) { pack_slices(lv, out, b, e); });
+  // A large level whose rows all have about the same short length (the
+  // finest level of a tet, hex or quad mesh) is stored ELL-32: aligned
+  // 32-row groups of one width, ignoring colour boundaries, so the kernels
+  // compute a slice's position instead of loading it (one dependent load
+  // less per row) at the cost of a little padding.
+  const long long ellEntries = (long long)((n + 31) / 32) * 32 * out.maxWidth;
+  out.ellWidth = 0;
+  if (n >= 32768 && out.maxWidth <= 8 && ellEntries * 100 <= (long long)out.sliceOff[nSlices] * 115) {
+    const int W = out.maxWidth, groups = (n + 31) / 32;
+    out.ellWidth = W;
+    out.sliceRow.resize(groups);
+    out.sliceRows.resize(groups);
+    out.sliceOff.resize(groups + 1);
+    for (int s = 0; s < groups; s++) {
+      out.sliceRow[s] = 32 * s;
+      out.sliceRows[s] = std::min(32, n - 32 * s);
+      out.sliceOff[s] = 32 * W * s;
+    }
+    out.sliceOff[groups] = 32 * W * groups;
+    // colour passes of an ELL-32 level run over colorStart rows
+    out.colorSliceStart = out.colorStart;
+  }
+  const int nPacked = (int)out.sliceRow.size();
+  out.cols.resize(out.sliceOff[nPacked]);
+  out.vals.resize(out.sliceOff[nPacked]);
+  parallel_chunks(nPacked, [&](int b, int e) { pack_slices(lv, out, b, e); });
 }
 
 void pack_slices(const RefLevel& lv, PackedLevel& out, int sBegin, int sEnd) {

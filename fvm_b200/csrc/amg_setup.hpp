@@ -81,6 +81,9 @@ struct PackedLevel {
   std::vector<int> coarseIndex;      // fine row -> coarse row
   std::vector<int> c2fRow, c2fCol;   // coarse row -> fine rows, ascending reference order
   int maxWidth = 0;
+  // > 0: ELL-32 layout (slices = aligned 32-row groups of this width, not
+  // aligned to colours; colour passes use colorStart rows)
+  int ellWidth = 0;
 };
 
 enum SmootherOrdering { kMulticolor = 0, kSequential = 1 };

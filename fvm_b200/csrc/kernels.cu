@@ -99,6 +99,21 @@ __device__ __forceinline__ T row_sum(const SellView<T>& a, const int4 m, int lan
     asm volatile("griddepcontrol.wait;" ::: "memory");             \
   } while (0)
 
+// A slice's {first row, rows, offset, width}: loaded (SELL-32) or computed
+// (ELL-32: aligned 32-row groups of one width)
+template <class T>
+__device__ __forceinline__ int4 slice_meta(const SellView<T>& a, int s) {
+  if (a.ellWidth) {
+    const int r0 = s << 5;
+    return make_int4(r0, min(32, a.n - r0), r0 * a.ellWidth, a.ellWidth);
+  }
+  return a.meta[s];
+}
+template <class T>
+__device__ __forceinline__ int slice_of(const SellView<T>& a, const int* rowSlice, int i) {
+  return a.ellWidth ? (i >> 5) : rowSlice[i];
+}
+
 template <class T>
 __global__ void k_zero(int n, T* x) {
   FVM_PDL();
@@ -110,10 +125,19 @@ __global__ void k_zero(int n, T* x) {
 template <class T>
 __global__ void __launch_bounds__(kBlock, 8) k_gs_color(SellView<T> a, int s0, int s1, T* x, const T* __restrict__ b) {
   FVM_PDL();
-  const int s = s0 + blockIdx.x * kSlicesPerBlock + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
+  if (a.ellWidth) {
+    // rows [s0, s1) of the aligned 32-row groups
+    const int s = (s0 >> 5) + blockIdx.x * kSlicesPerBlock + (threadIdx.x >> 5);
+    const int i = (s << 5) + lane;
+    if (i < s0 || i >= s1) return;
+    const T sum = row_sum(a, slice_meta(a, s), lane, x, b[i]);
+    x[i] = -sum / a.diag[i];
+    return;
+  }
+  const int s = s0 + blockIdx.x * kSlicesPerBlock + (threadIdx.x >> 5);
   if (s >= s1) return;
-  const int4 m = a.meta[s];
+  const int4 m = slice_meta(a, s);
   if (lane >= m.y) return;
   const int i = m.x + lane;
   const T sum = row_sum(a, m, lane, x, b[i]);
@@ -127,7 +151,7 @@ __global__ void k_gs_sequential(SellView<T> a, T* x, const T* __restrict__ b, in
   for (int t = 0; t < a.n; t++) {
     const int i = reverse ? a.n - 1 - t : t;
     const int s = i >> 5, lane = i & 31;  // one colour: slices are consecutive 32-row blocks
-    const T sum = row_sum(a, a.meta[s], lane, x, b[i]);
+    const T sum = row_sum(a, slice_meta(a, s), lane, x, b[i]);
     x[i] = -sum / a.diag[i];
   }
 }
@@ -139,7 +163,7 @@ __global__ void __launch_bounds__(kBlock, 8) k_jacobi(SellView<T> a, int nSlices
   const int s = blockIdx.x * kSlicesPerBlock + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
   if (s >= nSlices) return;
-  const int4 m = a.meta[s];
+  const int4 m = slice_meta(a, s);
   if (lane >= m.y) return;
   const int i = m.x + lane;
   const T sum = row_sum(a, m, lane, xold, b[i]);
@@ -154,7 +178,7 @@ __global__ void __launch_bounds__(kBlock, 8) k_jacobi_damped(SellView<T> a, int 
   const int s = blockIdx.x * kSlicesPerBlock + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
   if (s >= nSlices) return;
-  const int4 m = a.meta[s];
+  const int4 m = slice_meta(a, s);
   if (lane >= m.y) return;
   const int i = m.x + lane;
   const T sum = row_sum(a, m, lane, xold, b[i]);
@@ -170,7 +194,7 @@ __global__ void __launch_bounds__(kBlock, 8) k_residual(SellView<T> a, int nSlic
   const int lane = threadIdx.x & 31;
   double l1 = 0.0;
   if (s < nSlices) {
-    const int4 m = a.meta[s];
+    const int4 m = slice_meta(a, s);
     if (lane < m.y) {
       const int i = m.x + lane;
       // reference order: r = b + d x, then r += a_ij x_j
@@ -206,7 +230,7 @@ __global__ void __launch_bounds__(kBlock, 8) k_spmv(SellView<double> a, int nSli
   const int s = blockIdx.x * kSlicesPerBlock + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
   if (s >= nSlices) return;
-  const int4 m = a.meta[s];
+  const int4 m = slice_meta(a, s);
   if (lane >= m.y) return;
   const int i = m.x + lane;
   y[i] = row_sum(a, m, lane, x, a.diag[i] * x[i]);
@@ -235,7 +259,7 @@ __global__ void __launch_bounds__(kBlock, 4) k_residual_restrict(SellView<T> a, 
   T s = T(0);
   for (int k = c2fRow[I]; k < c2fRow[I + 1]; k++) {
     const int i = c2fCol[k];
-    const int4 m = a.meta[rowSlice[i]];
+    const int4 m = slice_meta(a, slice_of(a, rowSlice, i));
     const int lane = i - m.x;
     const T ri = row_sum(a, m, lane, x, b[i] + a.diag[i] * x[i]);
     s = s + ri;
@@ -749,7 +773,9 @@ void pdl_launch(void (*kernel)(KArgs...), dim3 grid, dim3 block, cudaStream_t st
 template <class T>
 void gs_color(const SellView<T>& a, int s0, int s1, T* x, const T* b, cudaStream_t st) {
   if (s1 <= s0) return;
-  pdl_launch(k_gs_color<T>, ceil_div(s1 - s0, kSlicesPerBlock), kBlock, st, a, s0, s1, x, b);
+  // ELL-32: s0, s1 are rows; the launch covers the 32-row groups they touch
+  const int groups = a.ellWidth ? ((s1 - 1) >> 5) - (s0 >> 5) + 1 : s1 - s0;
+  pdl_launch(k_gs_color<T>, ceil_div(groups, kSlicesPerBlock), kBlock, st, a, s0, s1, x, b);
 }
 template <class T>
 void gs_sequential(const SellView<T>& a, T* x, const T* b, bool reverse, cudaStream_t st) {

@@ -21,10 +21,15 @@ struct SellView {
   // per slice, packed for a single 16-byte load: first row, rows (<= 32),
   // offset of its first entry, width (entries per row, padded)
   const int4* meta;
+  // > 0: ELL-32 layout -- the slices are the aligned 32-row groups, all of
+  // this width, so a slice's metadata and a row's slice are computed, not
+  // loaded (colour passes then take row ranges instead of slice ranges)
+  int ellWidth = 0;
 };
 
 // ---- smoothers -----------------------------------------------------------
-// One Gauss-Seidel pass over the rows of slices [s0, s1) (one colour block):
+// One Gauss-Seidel pass over the rows of slices [s0, s1) (one colour block;
+// on an ELL-32 level s0, s1 are the colour's first and end ROWS):
 // x_i = -(b_i + sum_j a_ij x_j) / a_ii
 template <class T>
 void gs_color(const SellView<T>& a, int s0, int s1, T* x, const T* b, cudaStream_t st);

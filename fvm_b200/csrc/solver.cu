@@ -212,6 +212,7 @@ void AmgHierarchy::uploadMatrix(const PackedLevel& p, DevLevel& d, bool mixed) {
   d.nColors = p.nColors;
   d.nSlices = (int)p.sliceRow.size();
   d.maxWidth = p.maxWidth;
+  d.ellWidth = p.ellWidth;
   d.colorSliceStart = p.colorSliceStart;
   d.entries = p.cols.size();
   d.sliceRow = arena_.upload(p.sliceRow);
@@ -300,8 +301,10 @@ void AmgHierarchy::genCycle(CycleType t, int l, std::vector<dev::Phase>& out) co
 void AmgHierarchy::buildProgram() {
   programReady_ = false;
   tailLevel_ = -1;
-  // the program kernels implement the uniform smoothers only
+  // the program kernels implement the uniform smoothers on SELL-32 levels only
   if ((opt_.ordering == kSequential && opt_.smootherType == kGaussSeidel) || opt_.coarseJacobiRows > 0) return;
+  for (const DevLevel& d : lv_)
+    if (d.ellWidth > 0) return;
   const int L = (int)lv_.size();
   std::vector<dev::ProgLevel<double>> p64(L);
   std::vector<dev::ProgLevel<float>> p32(L);

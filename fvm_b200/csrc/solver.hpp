@@ -83,11 +83,12 @@ struct DevLevel {
   double* partials = nullptr;
   int nPartials = 0;
   int4* meta = nullptr;  // per slice: first row, rows, entry offset, width
+  int ellWidth = 0;  // > 0: ELL-32 layout (colorSliceStart then holds rows)
   dev::SellView<double> view64() const {
-    return {n, sliceRow, sliceRows, sliceOff, cols, vals, diag, meta};
+    return {n, sliceRow, sliceRows, sliceOff, cols, vals, diag, meta, ellWidth};
   }
   dev::SellView<float> view32() const {
-    return {n, sliceRow, sliceRows, sliceOff, cols, valsF, diagF, meta};
+    return {n, sliceRow, sliceRows, sliceOff, cols, valsF, diagF, meta, ellWidth};
   }
   size_t entries = 0;
 };

@@ -408,3 +408,30 @@ def test_all_boundary_conditions_converge_to_reference(refo):
     for gid in _ALL_BCS:
         a, b = tm.getHeatFluxIntegral(m, gid), r.heat_flux_integral(gid)
         assert abs(a - b) <= 1e-8 * max(1.0, abs(b)), gid
+
+
+@pytest.mark.parametrize("ordering", ["sequential", "multicolor"])
+def test_ell_finest_level_matches_reference(refo, ordering):
+    """73k tets: the finest level is stored ELL-32 (aligned 32-row groups of
+    width 4). Sequential GS: temperatures after two outer iterations equal
+    the reference's bit for bit; multicolour: the converged field."""
+    mesh, f = meshgen.config1(m=24, seed=2)
+    assert mesh["nCells"] >= 32768
+    bcs = {gid: v for gid, v in f["bc"].items()}
+    fields = {"conductivity": f["k"], "source": f["s"]}
+    n = mesh["nCells"]
+    if ordering == "sequential":
+        amg = _amg(smootherOrdering=fvmbaseExt.AMG.SEQUENTIAL, relativeTolerance=1e-1, nMaxIterations=20)
+        tm, tf, m = gpu_model(mesh, bcs, solver=amg, fields=fields)
+        r = ref_model(refo, mesh, bcs, fields=fields)
+        for it in range(2):
+            tm.advance(1)
+            r.advance(1)
+            np.testing.assert_array_equal(tf.temperature[m.getCells()][:n], r.get_field(0)[:n])
+    else:
+        amg = _amg(nPreSweeps=1, nPostSweeps=1, relativeTolerance=1e-10, nMaxIterations=500)
+        tm, tf, m = gpu_model(mesh, bcs, solver=amg, fields=fields, opts={"relativeTolerance": 1e-10})
+        _converge(tm)
+        r = ref_model(refo, mesh, bcs, fields=fields, n_pre=1, n_post=1, lin_rel=1e-10, max_iter=500, rel=1e-10)
+        r.advance(200)
+        assert rel_l2(tf.temperature[m.getCells()][:n], r.get_field(0)[:n]) <= TOL_FIELD

@@ -307,6 +307,103 @@ def cpu_reference(mesh, fields, plain_counts, inner_rel, desc, cores_note=True):
     }
 
 
+def bench_batch(args, dist, peaks, peak_kind):
+    """config 2: a batch of independent jittered quad meshes (sides
+    U{32..256}) solved as one system, every mesh to outer relative residual
+    1e-10 on its own norm."""
+    from fvm_b200 import batch, meshgen
+
+    ms = meshgen.config2(n_meshes=args.batch_meshes)
+    meshes = [m for m, _ in ms]
+    ks = [f["k"] for _, f in ms]
+    ss = [f["s"] for _, f in ms]
+    n_cells = int(sum(m["nCells"] for m in meshes))
+    bcs = ms[0][1]["bc"]
+    results = {}
+    for variant in ("plain", "mixed"):
+        bt = batch.BatchedThermal(meshes, bcs, solver_for(variant, args.inner_rel))
+        for _ in range(args.warmup):
+            bt.solve(ks, ss)
+        dist.barrier()
+        sampler = ClockSampler(dist.local)
+        sampler.__enter__()
+        dev_t, wall_t, rep = [], [], None
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            Ts, rep = bt.solve(ks, ss)
+            wall_t.append(time.perf_counter() - t0)
+            dev_t.append(rep.seconds)
+        sampler.__exit__()
+        dist.barrier()
+        first, last, at = bt.status()
+        n_all = bt.mesh.getCells().getCount()
+        results[variant] = {"dev": dist.max(statistics.median(dev_t)), "wall": dist.max(statistics.median(wall_t)),
+                            "outer": rep.iterations, "cycles": rep.linearIterations, "setup": rep.setupSeconds,
+                            "all_converged": bool(np.all(at >= 0)), "max_ratio": float(np.max(last / first)),
+                            "T": np.concatenate(Ts), "launches": rep.launches, "clocks": sampler.summary(),
+                            "h2d": 8 * 3 * n_all, "d2h": 8 * n_all}
+        del bt
+    plain, mixed = results["plain"], results["mixed"]
+    cpu = None
+    if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_reference_batch(ms, args.inner_rel)
+    if dist.rank == 0:
+        rel = float(np.linalg.norm(mixed["T"] - plain["T"]) / np.linalg.norm(plain["T"]))
+        line = {
+            "metric": METRIC, "value": mixed["dev"], "unit": "s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": mixed["dev"] * 1e3, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 V-cycle / f64 refinement", "data": "synthetic",
+            "config": {"workload": "%d independent jittered quad meshes, sides U{32..256}, one batched solve"
+                                   % len(meshes), "cells": n_cells, "meshes": len(meshes), "outer_rel": 1e-10,
+                       "inner_rel": args.inner_rel, "convergence": "every mesh on its own L1 norm",
+                       "l2": "working set > 126 MB L2"},
+            "plain_fp64_s": plain["dev"], "speedup_vs_plain_fp64": plain["dev"] / mixed["dev"],
+            "mixed_vs_plain_rel_l2": rel, "cells_per_s": n_cells / mixed["dev"] * args.gpus,
+            "counts": {k: {"outer": v["outer"], "cycles": v["cycles"], "setup_s": v["setup"],
+                           "all_meshes_converged": v["all_converged"], "max_mesh_ratio": v["max_ratio"]}
+                       for k, v in results.items()},
+            "gpu_launches": int(mixed["launches"]) * args.steps,
+            "cpu_baseline": cpu,
+            "e2e": {"value": mixed["wall"], "unit": "s", "h2d_bytes_per_step": mixed["h2d"],
+                    "d2h_bytes_per_step": mixed["d2h"]},
+            "clocks": mixed["clocks"],
+        }
+        print(json.dumps(line))
+
+
+def cpu_reference_batch(ms, inner_rel, sample=6):
+    """The reference solves each mesh with its own ThermalModel<double>
+    (one core). Bounded sample: full solves (to 1e-10) of `sample` meshes
+    spread over the size range; the batch time is extrapolated by cells."""
+    from oracle import ref
+    from fvm_b200.meshgen import extend_to_ghosts
+
+    if not ref.available():
+        return None
+    order = sorted(range(len(ms)), key=lambda i: ms[i][0]["nCells"])
+    pick = [order[int(q * (len(order) - 1) / (sample - 1))] for q in range(sample)]
+    t_sum, c_sum = 0.0, 0
+    for i in pick:
+        mesh, f = ms[i]
+        r = ref.RefThermal(mesh)
+        r.set_options(n_pre=1, n_post=1, max_iter=200, lin_rel=inner_rel, rel=1e-10)
+        for gid, (kind, val) in f["bc"].items():
+            r.set_bc(gid, 0 if kind == "T" else 1, [val] if kind == "T" else [None, val])
+        r.init()
+        r.set_field(1, extend_to_ghosts(mesh, f["k"]))
+        r.set_field(2, extend_to_ghosts(mesh, f["s"]))
+        _, sec = r.advance(500)
+        t_sum += sec
+        c_sum += mesh["nCells"]
+        del r
+    total_cells = sum(m["nCells"] for m, _ in ms)
+    est = t_sum / c_sum * total_cells
+    return {"value": est, "unit": "s", "cores": 1, "kind": "reference",
+            "sample": ("reference ThermalModel<double>+AMG per mesh (1 pre/1 post GS): full solves to 1e-10 of %d "
+                       "meshes (%d cells, %.2f s), extrapolated by cells to the %d-mesh batch (%d cells)"
+                       % (len(pick), c_sum, t_sum, len(ms), total_cells))}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -321,10 +418,33 @@ def main():
     ap.add_argument("--variants", default="plain,plain-cg,mixed,learned",
                     help="comma list of plain, plain-cg, mixed, learned (mixed + learned correction)")
     ap.add_argument("--train-steps", type=int, default=600)
+    ap.add_argument("--batch-meshes", type=int, default=512, help="config2: number of meshes")
     args = ap.parse_args()
 
     dist = Dist()
     peaks, peak_kind = load_peaks()
+    if args.workload == "config2" and args.impl == "product":
+        bench_batch(args, dist, peaks, peak_kind)
+        dist.close()
+        return
+    if args.workload == "config2":
+        if dist.rank == 0:
+            from fvm_b200 import meshgen
+
+            ms = meshgen.config2(n_meshes=args.batch_meshes)
+            base = cpu_reference_batch(ms, args.inner_rel)
+            if base is None:
+                print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libfvmref.so not built"}))
+            else:
+                v = base["value"]
+                print(json.dumps({"impl": "reference", "metric": METRIC, "value": v, "unit": "s",
+                                  "n_gpus": args.gpus, "steps": 1, "warmup": 0, "ms_per_step": v * 1e3,
+                                  "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                                  "data": "synthetic", "config": {"workload": "config2 batch", "meshes": len(ms)},
+                                  "cpu_baseline": base,
+                                  "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+        dist.close()
+        return
     mesh, fields, desc, gen = make_workload(args.workload)
     n_cells = mesh["nCells"]
 

@@ -23,6 +23,7 @@ namespace {
 
 constexpr int kBlock = 256;           // threads per block for row kernels
 constexpr int kSlicesPerBlock = kBlock / 32;
+constexpr int kRowGridCap = 148 * 8;
 constexpr int kReduceBlocks = 1184;   // 148 SMs x 8: vector reductions
 
 inline int ceil_div(long long a, long long b) { return (int)((a + b - 1) / b); }
@@ -160,14 +161,14 @@ template <class T>
 __global__ void __launch_bounds__(kBlock, 8) k_jacobi(SellView<T> a, int nSlices, const T* __restrict__ xold, T* xnew,
                          const T* __restrict__ b) {
   FVM_PDL();
-  const int s = blockIdx.x * kSlicesPerBlock + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
-  if (s >= nSlices) return;
-  const int4 m = slice_meta(a, s);
-  if (lane >= m.y) return;
-  const int i = m.x + lane;
-  const T sum = row_sum(a, m, lane, xold, b[i]);
-  xnew[i] = -sum / a.diag[i];
+  for (int s = blockIdx.x * kSlicesPerBlock + (threadIdx.x >> 5); s < nSlices; s += gridDim.x * kSlicesPerBlock) {
+    const int4 m = slice_meta(a, s);
+    if (lane >= m.y) continue;
+    const int i = m.x + lane;
+    const T sum = row_sum(a, m, lane, xold, b[i]);
+    xnew[i] = -sum / a.diag[i];
+  }
 }
 
 // damped Jacobi: xnew = xold + w (xJacobi - xold)
@@ -175,32 +176,31 @@ template <class T>
 __global__ void __launch_bounds__(kBlock, 8) k_jacobi_damped(SellView<T> a, int nSlices, const T* __restrict__ xold, T* xnew,
                                 const T* __restrict__ b, T w) {
   FVM_PDL();
-  const int s = blockIdx.x * kSlicesPerBlock + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
-  if (s >= nSlices) return;
-  const int4 m = slice_meta(a, s);
-  if (lane >= m.y) return;
-  const int i = m.x + lane;
-  const T sum = row_sum(a, m, lane, xold, b[i]);
-  const T xo = xold[i];
-  xnew[i] = xo + w * (-sum / a.diag[i] - xo);
+  for (int s = blockIdx.x * kSlicesPerBlock + (threadIdx.x >> 5); s < nSlices; s += gridDim.x * kSlicesPerBlock) {
+    const int4 m = slice_meta(a, s);
+    if (lane >= m.y) continue;
+    const int i = m.x + lane;
+    const T sum = row_sum(a, m, lane, xold, b[i]);
+    const T xo = xold[i];
+    xnew[i] = xo + w * (-sum / a.diag[i] - xo);
+  }
 }
 
 template <class T>
 __global__ void __launch_bounds__(kBlock, 8) k_residual(SellView<T> a, int nSlices, const T* __restrict__ x,
                            const T* __restrict__ b, T* r, double* partials) {
   FVM_PDL();
-  const int s = blockIdx.x * kSlicesPerBlock + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
   double l1 = 0.0;
-  if (s < nSlices) {
+  for (int s = blockIdx.x * kSlicesPerBlock + (threadIdx.x >> 5); s < nSlices; s += gridDim.x * kSlicesPerBlock) {
     const int4 m = slice_meta(a, s);
     if (lane < m.y) {
       const int i = m.x + lane;
       // reference order: r = b + d x, then r += a_ij x_j
       const T ri = row_sum(a, m, lane, x, b[i] + a.diag[i] * x[i]);
       r[i] = ri;
-      l1 = fabs((double)ri);
+      l1 += fabs((double)ri);
     }
   }
   if (partials) {
@@ -227,13 +227,13 @@ __global__ void k_csr_residual(int n, const int* __restrict__ row, const int* __
 
 __global__ void __launch_bounds__(kBlock, 8) k_spmv(SellView<double> a, int nSlices, const double* __restrict__ x, double* y) {
   FVM_PDL();
-  const int s = blockIdx.x * kSlicesPerBlock + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
-  if (s >= nSlices) return;
-  const int4 m = slice_meta(a, s);
-  if (lane >= m.y) return;
-  const int i = m.x + lane;
-  y[i] = row_sum(a, m, lane, x, a.diag[i] * x[i]);
+  for (int s = blockIdx.x * kSlicesPerBlock + (threadIdx.x >> 5); s < nSlices; s += gridDim.x * kSlicesPerBlock) {
+    const int4 m = slice_meta(a, s);
+    if (lane >= m.y) continue;
+    const int i = m.x + lane;
+    y[i] = row_sum(a, m, lane, x, a.diag[i] * x[i]);
+  }
 }
 
 template <class T>
@@ -783,18 +783,24 @@ void gs_sequential(const SellView<T>& a, T* x, const T* b, bool reverse, cudaStr
 }
 template <class T>
 void jacobi(const SellView<T>& a, int nSlices, const T* xold, T* xnew, const T* b, cudaStream_t st) {
-  pdl_launch(k_jacobi<T>, ceil_div(nSlices, kSlicesPerBlock), kBlock, st, a, nSlices, xold, xnew, b);
+  pdl_launch(k_jacobi<T>, reduce_blocks(nSlices), kBlock, st, a, nSlices, xold, xnew, b);
 }
 template <class T>
 void jacobi_damped(const SellView<T>& a, int nSlices, const T* xold, T* xnew, const T* b, T w, cudaStream_t st) {
-  pdl_launch(k_jacobi_damped<T>, ceil_div(nSlices, kSlicesPerBlock), kBlock, st, a, nSlices, xold, xnew, b, w);
+  pdl_launch(k_jacobi_damped<T>, reduce_blocks(nSlices), kBlock, st, a, nSlices, xold, xnew, b, w);
 }
 template <class T>
 void residual(const SellView<T>& a, int nSlices, const T* x, const T* b, T* r, double* partials,
               cudaStream_t st) {
-  pdl_launch(k_residual<T>, ceil_div(nSlices, kSlicesPerBlock), kBlock, st, a, nSlices, x, b, r, partials);
+  pdl_launch(k_residual<T>, reduce_blocks(nSlices), kBlock, st, a, nSlices, x, b, r, partials);
 }
-int reduce_blocks(int nSlices) { return ceil_div(nSlices, kSlicesPerBlock); }
+// Row kernels over a whole level run a grid of at most 8 resident blocks
+// per SM (148 SMs at 32 registers), each striding over slices: no partial
+// last wave, and one L1 partial per block.
+int reduce_blocks(int nSlices) {
+  const int b = ceil_div(nSlices, kSlicesPerBlock);
+  return b < kRowGridCap ? (b < 1 ? 1 : b) : kRowGridCap;
+}
 int csr_residual_blocks(int n) { return ceil_div(n, kBlock); }
 void csr_residual(int n, const int* row, const int* col, const double* diag, const double* off,
                   const double* x, const double* b, double* r, double* partials, cudaStream_t st) {
@@ -804,7 +810,7 @@ void csr_residual_finish(int nPartials, const double* partials, double* l1, cuda
   pdl_launch(k_sum_partials, 1, 1024, st, nPartials, partials, l1);
 }
 void spmv(const SellView<double>& a, int nSlices, const double* x, double* y, cudaStream_t st) {
-  pdl_launch(k_spmv, ceil_div(nSlices, kSlicesPerBlock), kBlock, st, a, nSlices, x, y);
+  pdl_launch(k_spmv, reduce_blocks(nSlices), kBlock, st, a, nSlices, x, y);
 }
 template <class T>
 void restrict_sum(int nc, const int* c2fRow, const int* c2fCol, const T* r, T* bc, cudaStream_t st) {

@@ -139,6 +139,8 @@ _SIGS = {
                                                c_double_p, c_double_p, c_double_p]),
     "fvm_learned_gradient_csr": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, c_int_p, c_int_p, c_double_p,
                                                 c_double_p, c_double_p, c_double_p, c_float_p, c_double_p]),
+    "fvm_learned_set_tensor_cores": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "fvm_learned_tensor_cores": (ctypes.c_int, [ctypes.c_void_p, c_int_p]),
 }
 
 EXPORTED = tuple(_SIGS)

@@ -680,6 +680,7 @@ int fvm_learned_forward_csr(fvm_learned* l, int n, const int* row, const int* co
     l->lc->apply(cg.g, dr, dOut, scal, 0);
     if (cudaMemcpy(out, dOut, sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost) != cudaSuccess)
       throw Error(kDeviceError, "copy of the network output failed");
+    l->lc->checkApplyStatus();
   });
 }
 
@@ -695,10 +696,26 @@ int fvm_learned_gradient_csr(fvm_learned* l, int n, const int* row, const int* c
     double* scal = (double*)tmp.alloc(sizeof(double) * 8);
     nn::Workspace ws;
     ws.allocate(n, true);
+    ws.tensorCores = l->lc->tensorCores();
     nn::forward_backward(cg.g, l->lc->deviceParams(), dr, de, dg, scal + 4, ws, scal, 0);
     if (cudaMemcpy(grad, dg, sizeof(float) * nn::kParams, cudaMemcpyDeviceToHost) != cudaSuccess ||
         cudaMemcpy(loss, scal + 4, sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess)
       throw Error(kDeviceError, "copy of the gradient failed");
+    ws.checkStatus();
+  });
+}
+
+int fvm_learned_set_tensor_cores(fvm_learned* l, int on) {
+  return guarded([&] {
+    FVM_REQUIRE(l, kBadArgument, "null argument");
+    l->lc->setTensorCores(on != 0);
+  });
+}
+
+int fvm_learned_tensor_cores(const fvm_learned* l, int* on) {
+  return guarded([&] {
+    FVM_REQUIRE(l && on, kBadArgument, "null argument");
+    *on = l->lc->tensorCores() ? 1 : 0;
   });
 }
 

@@ -1,5 +1,9 @@
 // Kernels of the learned correction (learned.hpp): forward, backward and
-// Adam, all FP32 with fixed reduction orders (deterministic).
+// Adam with fixed reduction orders (deterministic). Message passing,
+// encoder, decoder and Adam run on the CUDA cores in FP32; the dense 64 ->
+// 32 layer products (forward, and the backward's input and weight
+// gradients) run on the tensor cores (tcgen05, TF32 inputs, FP32 sums), or
+// optionally in FP32 on the CUDA cores.
 //
 // Layout: activations node-major, h[i * 32 + c]; one warp per node, lane =
 // channel, so a neighbour's activations are one coalesced 128-byte load.
@@ -10,6 +14,7 @@
 
 #include "common.hpp"
 #include "learned.hpp"
+#include "umma.cuh"
 
 namespace fvm {
 namespace nn {
@@ -122,6 +127,119 @@ __global__ void __launch_bounds__(kBlock) k_layer(int n, GraphArgs g, const floa
     Hout[(size_t)i * 32 + lane] = relu(z);
     if (Mout) Mout[(size_t)i * 32 + lane] = msg;
   }
+}
+
+// ---- dense layers on the tensor cores (tcgen05, kind tf32) ------------------
+//
+// A tile is 128 nodes (the MMA's M). Operands are staged in shared memory in
+// the no-swizzle K-major layout: element (row r, k) of a K-wide operand at
+// float offset (r/8)*8K + (k/4)*32 + (r%8)*4 + k%4, i.e. 8 x 4 core
+// matrices of 128 bytes, K-adjacent ones 128 B apart (LBO) and 8-row groups
+// 32K bytes apart (SBO). The FP32 accumulator lives in TMEM (lane = row,
+// column = output) and is read back with tcgen05.ld for the epilogue. The
+// MMA reads its operands as TF32 (10-bit mantissa); sums are FP32.
+
+constexpr int kTcRows = 128;
+constexpr int kTcThreads = 256;
+constexpr uint32_t kTcWaitLimit = 1u << 22;  // tries of the completion wait before the kernel gives up
+
+__device__ __forceinline__ int kmajor(int r, int k, int K) {
+  return (r >> 3) * (K << 3) + ((k >> 2) << 5) + ((r & 7) << 2) + (k & 3);
+}
+
+// The same layer as k_layer: the message gather on the CUDA cores (warp per
+// node, FP32, same order), then [h_i, m_i] (128 x 64) times [Ws Wm]^T (64 x
+// 32) as 8 MMAs of K = 8 into TMEM, bias + ReLU in the epilogue. status
+// gets 1 if a completion wait runs out (outputs of that tile not written).
+__global__ void __launch_bounds__(kTcThreads, 4) k_layer_tc(int n, GraphArgs g, const float* __restrict__ P,
+                                                            const float* __restrict__ Hin, float* __restrict__ Hout,
+                                                            float* __restrict__ Mout, int* status) {
+  __shared__ __align__(128) float sA[kTcRows * 64];
+  __shared__ __align__(128) float sB[32 * 64];
+  __shared__ float sBias[32];
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ uint32_t sTmem;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  // B = [Ws Wm]: row = output channel, K = the 64 inputs (h then m)
+  for (int t = threadIdx.x; t < 2048; t += blockDim.x) {
+    const int o = t >> 6, k = t & 63;
+    sB[kmajor(o, k, 64)] = k < 32 ? P[o * 32 + k] : P[1024 + o * 32 + (k - 32)];
+  }
+  if (threadIdx.x < 32) sBias[threadIdx.x] = P[2048 + threadIdx.x];
+  if (warp == 0) umma::tmem_alloc(&sTmem, 32);
+  if (threadIdx.x == 32) umma::mbar_init(&bar, 1);
+  umma::fence_smem_for_mma();
+  umma::fence_before_sync();
+  __syncthreads();
+  umma::fence_after_sync();
+  const uint32_t tmem = sTmem;
+  const uint32_t idesc = umma::idesc_tf32(kTcRows, 32);
+  const uint32_t aBase = umma::smem_addr(sA), bBase = umma::smem_addr(sB);
+  const int nTiles = (n + kTcRows - 1) / kTcRows;
+  uint32_t parity = 0;
+  bool pending = false;
+  for (int tile = blockIdx.x; tile < nTiles; tile += gridDim.x) {
+    const int row0 = tile * kTcRows;
+    for (int r = warp; r < kTcRows; r += kTcThreads / 32) {
+      const int i = row0 + r;
+      float h = 0.f, msg = 0.f;
+      if (i < n) {
+        const int4 m = g.meta[g.rowSlice[i]];
+        const int base = m.z + (i - m.x);
+        const double di = fabs(g.diag[i]);
+        for (int k = 0; k < m.w; k++) {
+          const int e = base + (k << 5);
+          const int j = g.cols[e];
+          const float w = (float)(fabs(g.vals[e]) / di);
+          msg = __fmaf_rn(w, Hin[(size_t)j * 32 + lane], msg);
+        }
+        h = Hin[(size_t)i * 32 + lane];
+        if (Mout) Mout[(size_t)i * 32 + lane] = msg;
+      }
+      sA[kmajor(r, lane, 64)] = h;
+      sA[kmajor(r, 32 + lane, 64)] = msg;
+    }
+    umma::fence_smem_for_mma();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      umma::fence_after_sync();
+#pragma unroll
+      for (int s = 0; s < 8; s++)
+        umma::mma_tf32(tmem, umma::smem_desc(aBase + s * 256, 128, 2048), umma::smem_desc(bBase + s * 256, 128, 2048),
+                       idesc, s > 0);
+      umma::commit(&bar);
+    }
+    pending = true;
+    const bool done = __syncthreads_and(umma::mbar_wait(&bar, parity, kTcWaitLimit));
+    if (!done) {
+      if (threadIdx.x == 0) atomicOr(status, 1);
+      break;
+    }
+    pending = false;
+    parity ^= 1u;
+    umma::fence_after_sync();
+    // warp w reads TMEM lanes 32 (w % 4) .. +31 (its rows), columns 16 (w / 4) .. +15
+    const int q = warp & 3, half = warp >> 2;
+    float z[16];
+    umma::ld16(umma::tmem_at(tmem, 32 * q, 16 * half), z);
+    const int i = row0 + 32 * q + lane;
+    if (i < n) {
+      float4* out = reinterpret_cast<float4*>(Hout + (size_t)i * 32 + 16 * half);
+#pragma unroll
+      for (int c = 0; c < 4; c++) {
+        const float* b = sBias + 16 * half + 4 * c;
+        out[c] = make_float4(relu(z[4 * c] + b[0]), relu(z[4 * c + 1] + b[1]), relu(z[4 * c + 2] + b[2]),
+                             relu(z[4 * c + 3] + b[3]));
+      }
+    }
+    umma::fence_before_sync();
+    __syncthreads();
+  }
+  // after a wait that ran out, give the MMAs in flight one more bounded wait
+  // before their accumulator is released
+  if (pending) __syncthreads_and(umma::mbar_wait(&bar, parity, kTcWaitLimit));
+  umma::fence_after_sync();
+  if (warp == 0) umma::tmem_free(tmem, 32);
 }
 
 __device__ __forceinline__ float warp_sum(float v) {
@@ -250,6 +368,142 @@ __global__ void __launch_bounds__(kBlock) k_layer_bwd_b(int n, GraphArgs g, cons
   }
 }
 
+// k_layer_bwd_a on the tensor cores. Per 128-node tile:
+//   [dS dM] (128 x 64) = dz (128 x 32) [Ws Wm]            4 MMAs, K = 8 channels each
+//   G (128 x 32)      += [h m 1 0]^T (128 x 128 nodes) dz 16 MMAs, K = 8 nodes each
+// G accumulates in TMEM over all tiles of the CTA: row f < 32 is the
+// gradient of Ws[., f], 32 <= f < 64 of Wm[., f - 32], row 64 (the constant
+// 1 feature) of the bias; rows 65..127 multiply zeros. Every operand is
+// staged K-major, so the products that contract over nodes get transposed
+// copies: XT (128 features x 128 nodes), Z (128 nodes x 32 channels), ZT
+// (32 channels x 128 nodes), W^T (64 inputs x 32 channels).
+constexpr int kBwdSmem = (128 * kTcRows + kTcRows * 32 + 32 * kTcRows + 64 * 32) * (int)sizeof(float);
+
+__global__ void __launch_bounds__(kTcThreads, 2) k_layer_bwd_tc(int n, const float* __restrict__ P,
+                                                                const float* __restrict__ Hin,
+                                                                const float* __restrict__ Hout,
+                                                                const float* __restrict__ Min,
+                                                                const float* __restrict__ dHout,
+                                                                float* __restrict__ dS, float* __restrict__ dM,
+                                                                float* gp, int off, int* status) {
+  extern __shared__ __align__(1024) float smem[];
+  float* sXT = smem;                // 128 x 128
+  float* sZ = sXT + 128 * kTcRows;  // 128 x 32
+  float* sZT = sZ + kTcRows * 32;   // 32 x 128
+  float* sW = sZT + 32 * kTcRows;   // 64 x 32
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ uint32_t sTmem;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int t = threadIdx.x; t < 2048; t += blockDim.x) {
+    const int f = t >> 5, c = t & 31;  // W^T[f][c] = Ws[c][f] or Wm[c][f - 32]
+    sW[kmajor(f, c, 32)] = f < 32 ? P[c * 32 + f] : P[1024 + c * 32 + (f - 32)];
+  }
+  for (int t = threadIdx.x; t < 64 * kTcRows; t += blockDim.x) {
+    const int f = 64 + (t >> 7), r = t & 127;
+    sXT[kmajor(f, r, kTcRows)] = f == 64 ? 1.f : 0.f;
+  }
+  if (warp == 0) umma::tmem_alloc(&sTmem, 128);
+  if (threadIdx.x == 32) umma::mbar_init(&bar, 1);
+  umma::fence_smem_for_mma();
+  umma::fence_before_sync();
+  __syncthreads();
+  umma::fence_after_sync();
+  const uint32_t tmem = sTmem;  // columns 0..63: [dS dM]; 64..95: G
+  const uint32_t idescD = umma::idesc_tf32(kTcRows, 64);
+  const uint32_t idescG = umma::idesc_tf32(128, 32);
+  const uint32_t xtBase = umma::smem_addr(sXT), zBase = umma::smem_addr(sZ), ztBase = umma::smem_addr(sZT),
+                 wBase = umma::smem_addr(sW);
+  const int nTiles = (n + kTcRows - 1) / kTcRows;
+  uint32_t parity = 0;
+  bool pending = false, any = false, failed = false;
+  for (int tile = blockIdx.x; tile < nTiles; tile += gridDim.x) {
+    const int row0 = tile * kTcRows;
+    for (int r = warp; r < kTcRows; r += kTcThreads / 32) {
+      const int i = row0 + r;
+      float dz = 0.f, h = 0.f, m = 0.f;
+      if (i < n) {
+        const size_t o = (size_t)i * 32 + lane;
+        dz = Hout[o] > 0.f ? dHout[o] : 0.f;
+        h = Hin[o];
+        m = Min[o];
+      }
+      sZ[kmajor(r, lane, 32)] = dz;
+      sZT[kmajor(lane, r, kTcRows)] = dz;
+      sXT[kmajor(lane, r, kTcRows)] = h;
+      sXT[kmajor(32 + lane, r, kTcRows)] = m;
+    }
+    umma::fence_smem_for_mma();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      umma::fence_after_sync();
+#pragma unroll
+      for (int s = 0; s < 4; s++)
+        umma::mma_tf32(tmem, umma::smem_desc(zBase + s * 256, 128, 1024), umma::smem_desc(wBase + s * 256, 128, 1024),
+                       idescD, s > 0);
+#pragma unroll
+      for (int s = 0; s < 16; s++)
+        umma::mma_tf32(tmem + 64, umma::smem_desc(xtBase + s * 256, 128, 4096),
+                       umma::smem_desc(ztBase + s * 256, 128, 4096), idescG, any || s > 0);
+      umma::commit(&bar);
+    }
+    pending = true;
+    any = true;
+    const bool done = __syncthreads_and(umma::mbar_wait(&bar, parity, kTcWaitLimit));
+    if (!done) {
+      failed = true;
+      break;
+    }
+    pending = false;
+    parity ^= 1u;
+    umma::fence_after_sync();
+    // warp w: rows 32 (w % 4) .., columns 32 (w / 4) ..: dS for w < 4, dM for w >= 4
+    const int q = warp & 3, half = warp >> 2;
+    float v[16];
+    const int i = row0 + 32 * q + lane;
+    float* dst = (half ? dM : dS) + (size_t)i * 32;
+#pragma unroll
+    for (int p = 0; p < 2; p++) {
+      umma::ld16(umma::tmem_at(tmem, 32 * q, 32 * half + 16 * p), v);
+      if (i < n) {
+        float4* o4 = reinterpret_cast<float4*>(dst + 16 * p);
+#pragma unroll
+        for (int c = 0; c < 4; c++) o4[c] = make_float4(v[4 * c], v[4 * c + 1], v[4 * c + 2], v[4 * c + 3]);
+      }
+    }
+    umma::fence_before_sync();
+    __syncthreads();
+  }
+  if (pending) __syncthreads_and(umma::mbar_wait(&bar, parity, kTcWaitLimit));
+  umma::fence_after_sync();
+  // gradient partials of this CTA: warps 0..3 hold features 32 w + lane
+  float* gb = gp + (size_t)blockIdx.x * kParams + off;
+  if (warp < 4) {
+    const int f = 32 * warp + lane;
+    float v[16];
+#pragma unroll
+    for (int p = 0; p < 2; p++) {
+      if (any && !failed) {
+        umma::ld16(umma::tmem_at(tmem, 32 * warp, 64 + 16 * p), v);
+      } else {
+#pragma unroll
+        for (int c = 0; c < 16; c++) v[c] = 0.f;
+      }
+#pragma unroll
+      for (int c = 0; c < 16; c++) {
+        const int ch = 16 * p + c;
+        if (f < 32) gb[ch * 32 + f] = v[c];
+        else if (f < 64) gb[1024 + ch * 32 + (f - 32)] = v[c];
+        else if (f == 64) gb[2048 + ch] = v[c];
+      }
+    }
+  }
+  if (failed && threadIdx.x == 0) atomicOr(status, 1);
+  umma::fence_before_sync();
+  __syncthreads();
+  umma::fence_after_sync();
+  if (warp == 0) umma::tmem_free(tmem, 128);
+}
+
 __global__ void __launch_bounds__(kBlock) k_encode_bwd(int n, const float* __restrict__ u, const float* __restrict__ H0,
                                                        const float* __restrict__ dH0, float* gp) {
   __shared__ float sv[kWarps * 64];
@@ -295,6 +549,12 @@ void check(cudaError_t e, const char* what) {
 
 constexpr int kReduceBlocks = 592;
 
+// persistent grid of the forward tensor-core layer: up to 4 CTAs per SM
+int tc_blocks(int n) {
+  const int t = ceil_div(n, kTcRows);
+  return t < 148 * 4 ? (t < 1 ? 1 : t) : 148 * 4;
+}
+
 void run_forward(const Graph& g, const float* P, const double* r, Workspace& w, double* scal, bool keepMessages,
                  cudaStream_t st) {
   const int n = w.n;
@@ -303,9 +563,14 @@ void run_forward(const Graph& g, const float* P, const double* r, Workspace& w, 
   k_input<<<ceil_div(n, kBlock), kBlock, 0, st>>>(n, r, g.a.diag, scal + 1, w.u, scal);
   k_encode<<<ceil_div((long long)n * 32, kBlock), kBlock, 0, st>>>(n, w.u, P, w.H[0]);
   const GraphArgs ga = args(g);
-  for (int l = 0; l < kLayers; l++)
-    k_layer<<<node_blocks(n), kBlock, 0, st>>>(n, ga, P + kLayer0 + l * kLayerSize, w.H[l], w.H[l + 1],
-                                               keepMessages ? w.M[l] : nullptr);
+  for (int l = 0; l < kLayers; l++) {
+    const float* Pl = P + kLayer0 + l * kLayerSize;
+    float* Ml = keepMessages ? w.M[l] : nullptr;
+    if (w.tensorCores)
+      k_layer_tc<<<tc_blocks(n), kTcThreads, 0, st>>>(n, ga, Pl, w.H[l], w.H[l + 1], Ml, w.status);
+    else
+      k_layer<<<node_blocks(n), kBlock, 0, st>>>(n, ga, Pl, w.H[l], w.H[l + 1], Ml);
+  }
 }
 
 }  // namespace
@@ -321,6 +586,8 @@ void Workspace::allocate(int n_, bool training) {
   check(cudaMalloc(&u, sizeof(float) * (size_t)n), "cudaMalloc");
   for (int l = 0; l <= kLayers; l++) check(cudaMalloc(&H[l], hb), "cudaMalloc");
   check(cudaMalloc(&partials, sizeof(double) * (kReduceBlocks + 8)), "cudaMalloc");
+  check(cudaMalloc(&status, sizeof(int)), "cudaMalloc");
+  check(cudaMemset(status, 0, sizeof(int)), "cudaMemset");
   if (training) {
     for (int l = 0; l < kLayers; l++) check(cudaMalloc(&M[l], hb), "cudaMalloc");
     check(cudaMalloc(&dA, hb), "cudaMalloc");
@@ -340,11 +607,23 @@ void Workspace::release() {
   cudaFree(dS);
   cudaFree(partials);
   cudaFree(gradPartials);
+  cudaFree(status);
   u = dA = dB = dS = gradPartials = nullptr;
   partials = nullptr;
+  status = nullptr;
   for (auto& h : H) h = nullptr;
   for (auto& m : M) m = nullptr;
   n = cap = 0;
+}
+
+void Workspace::checkStatus() {
+  if (!status) return;
+  int h = 0;
+  check(cudaMemcpy(&h, status, sizeof(int), cudaMemcpyDeviceToHost), "status copy");
+  if (h) {
+    check(cudaMemset(status, 0, sizeof(int)), "cudaMemset");
+    throw Error(kDeviceError, "learned correction: a tensor-core completion wait ran out");
+  }
 }
 
 void forward(const Graph& g, const float* params, const double* r, double* out, Workspace& w, double* scal,
@@ -364,11 +643,19 @@ void forward_backward(const Graph& g, const float* P, const double* r, const dou
   dev::sum_partials(kGradBlocks, w.partials, loss, st);
   const GraphArgs ga = args(g);
   const size_t smem = sizeof(float) * kWarps * kLayerSize;
-  cudaFuncSetAttribute(k_layer_bwd_a, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  check(cudaFuncSetAttribute(k_layer_bwd_a, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+        "k_layer_bwd_a shared memory");
+  check(cudaFuncSetAttribute(k_layer_bwd_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kBwdSmem),
+        "k_layer_bwd_tc shared memory");
   for (int l = kLayers - 1; l >= 0; l--) {
     const int off = kLayer0 + l * kLayerSize;
-    k_layer_bwd_a<<<kGradBlocks, kBlock, smem, st>>>(n, P + off, w.H[l], w.H[l + 1], w.M[l], w.dA, w.dS, w.dB,
-                                                     w.gradPartials, off);
+    if (w.tensorCores)
+      k_layer_bwd_tc<<<kGradBlocks, kTcThreads, kBwdSmem, st>>>(n, P + off, w.H[l], w.H[l + 1], w.M[l], w.dA, w.dS,
+                                                                 w.dB, w.gradPartials, off, w.status);
+    else
+      k_layer_bwd_a<<<kGradBlocks, kBlock, smem, st>>>(n, P + off, w.H[l], w.H[l + 1], w.M[l], w.dA, w.dS, w.dB,
+                                                       w.gradPartials, off);
+    check(cudaGetLastError(), "layer backward launch");
     k_layer_bwd_b<<<node_blocks(n), kBlock, 0, st>>>(n, ga, w.dS, w.dB, w.dA);
   }
   k_encode_bwd<<<kGradBlocks, kBlock, 0, st>>>(n, w.u, w.H[0], w.dA, w.gradPartials);
@@ -574,6 +861,7 @@ void LearnedCorrection::train(int steps, float lr, uint64_t seed, double* losses
     for (int q = 0; q < (int)inst_[k].pairs.size(); q++) index.push_back({k, q});
   }
   trainWs_.allocate(maxN, true);
+  trainWs_.tensorCores = tensorCores_;
   double* dLoss = nullptr;
   nn::check(cudaMalloc(&dLoss, sizeof(double) * (size_t)std::max(steps, 1)), "cudaMalloc");
   uint64_t x = seed * 0x9E3779B97F4A7C15ull + 0x51ull;
@@ -595,6 +883,7 @@ void LearnedCorrection::train(int steps, float lr, uint64_t seed, double* losses
     nn::check(cudaMemcpyAsync(losses, dLoss, sizeof(double) * steps, cudaMemcpyDeviceToHost, st), "cudaMemcpy");
   nn::check(cudaStreamSynchronize(st), "training");
   cudaFree(dLoss);
+  trainWs_.checkStatus();
 }
 
 double LearnedCorrection::evaluate(cudaStream_t st) {
@@ -603,6 +892,7 @@ double LearnedCorrection::evaluate(cudaStream_t st) {
   int maxN = 0;
   for (const Instance& k : inst_) maxN = std::max(maxN, k.n);
   trainWs_.allocate(maxN, true);
+  trainWs_.tensorCores = tensorCores_;
   double* dLoss = nullptr;
   nn::check(cudaMalloc(&dLoss, sizeof(double) * (size_t)np), "cudaMalloc");
   int q = 0;
@@ -615,12 +905,21 @@ double LearnedCorrection::evaluate(cudaStream_t st) {
   nn::check(cudaMemcpyAsync(l.data(), dLoss, sizeof(double) * np, cudaMemcpyDeviceToHost, st), "cudaMemcpy");
   nn::check(cudaStreamSynchronize(st), "evaluation");
   cudaFree(dLoss);
+  trainWs_.checkStatus();
   double s = 0.0;
   for (double v : l) s += v;
   return s / np;
 }
 
-void LearnedCorrection::prepare(int n) { applyWs_.allocate(n, false); }
+void LearnedCorrection::prepare(int n) {
+  applyWs_.allocate(n, false);
+  applyWs_.tensorCores = tensorCores_;
+}
+
+void LearnedCorrection::setTensorCores(bool on) {
+  tensorCores_ = on;
+  applyWs_.tensorCores = trainWs_.tensorCores = on;
+}
 
 void LearnedCorrection::apply(const nn::Graph& g, const double* r, double* out, double* scal, cudaStream_t st) {
   FVM_REQUIRE(g.a.n <= applyWs_.cap, kBadArgument, "learned correction: prepare() was not called for this size");

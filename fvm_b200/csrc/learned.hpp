@@ -58,8 +58,12 @@ struct Workspace {
   double* partials = nullptr;    // reductions
   float* gradPartials = nullptr; // blocks x kParams
   int gradBlocks = 0;
+  int* status = nullptr;         // device flag: 1 if a tensor-core completion wait ran out
+  bool tensorCores = true;       // dense layers on tcgen05 (TF32 inputs) instead of FP32 CUDA cores
   void allocate(int n, bool training);
   void release();
+  // throws (and clears the flag) if a tensor-core wait ran out; synchronises
+  void checkStatus();
   ~Workspace() { release(); }
 };
 
@@ -127,6 +131,12 @@ class LearnedCorrection {
   // allocates nothing, so it can run inside a captured graph)
   void prepare(int n);
   void apply(const nn::Graph& g, const double* r, double* out, double* scal, cudaStream_t st);
+  // throws if a tensor-core kernel of apply() gave up waiting (synchronises)
+  void checkApplyStatus() { applyWs_.checkStatus(); }
+
+  // dense layers on the tensor cores (default) or in FP32 on the CUDA cores
+  void setTensorCores(bool on);
+  bool tensorCores() const { return tensorCores_; }
 
  private:
   struct Instance {
@@ -142,6 +152,7 @@ class LearnedCorrection {
   float* dV_ = nullptr;
   double* dScal_ = nullptr;
   int adamT_ = 0;
+  bool tensorCores_ = true;
   nn::Workspace trainWs_;
   nn::Workspace applyWs_;
 };

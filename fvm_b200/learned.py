@@ -70,6 +70,18 @@ class LearnedCorrection:
     def load(self, path: str) -> None:
         self.setParams(np.load(path)["params"])
 
+    @property
+    def tensorCores(self) -> bool:
+        """Dense layers on the tensor cores (tcgen05, TF32 operands, FP32
+        sums; the default) or in FP32 on the CUDA cores."""
+        v = ctypes.c_int(0)
+        check(_lib.load().fvm_learned_tensor_cores(self._h, ctypes.byref(v)))
+        return bool(v.value)
+
+    @tensorCores.setter
+    def tensorCores(self, on: bool) -> None:
+        check(_lib.load().fvm_learned_set_tensor_cores(self._h, 1 if on else 0))
+
     def harvest(self, model, nOuter: int = 20, perSolve: int = 4, relativeTolerance: float = 1e-10,
                 maxCycles: int = 200) -> int:
         """Outer iterations of `model` (a ThermalModelA with a plain AMG

@@ -265,6 +265,14 @@ int fvm_learned_gradient_csr(fvm_learned* l, int n, const int* row, const int* c
                              const double* off, const double* r, const double* e, float* grad,
                              double* loss);
 
+/* Dense layers of the network (the 64 -> 32 products of the forward pass
+ * and of the backward pass) on the tensor cores (on != 0, the default:
+ * tcgen05 MMAs reading TF32 operands, FP32 sums) or in FP32 on the CUDA
+ * cores (on == 0). Applies to training, evaluation, forward/gradient and
+ * the solve. No reference counterpart (the learned correction is new). */
+int fvm_learned_set_tensor_cores(fvm_learned* l, int on);
+int fvm_learned_tensor_cores(const fvm_learned* l, int* on);
+
 const char* fvm_last_error(void);
 
 #ifdef __cplusplus

@@ -25,12 +25,13 @@ N_PARAMS = DEC_W + W + 1
 
 
 def _coupling(row, col, diag, off):
+    """Sparse n x n matrix of the couplings w_ij (duplicates summed)."""
+    from scipy.sparse import csr_matrix
+
     n = len(diag)
     rid = np.repeat(np.arange(n), np.diff(row))
     w = np.abs(off) / np.abs(diag[rid])
-    A = np.zeros((n, n))
-    np.add.at(A, (rid, col), w)
-    return A
+    return csr_matrix((w, (rid, np.asarray(col))), shape=(n, n))
 
 
 def _unpack(P):

@@ -180,10 +180,14 @@ def train_learned(gen, inner_rel, seeds=(101, 102), n_outer=4, per_solve=3, step
         lc.harvest(s.tm, nOuter=n_outer, perSolve=per_solve, relativeTolerance=1e-8, maxCycles=100)
         del s
     before = lc.evaluate()
-    losses = lc.train(steps=steps, lr=lr, seed=0)
+    t1 = time.perf_counter()
+    losses = lc.train(steps=steps, lr=lr, seed=0)  # returns after the device has finished
+    train_s = time.perf_counter() - t1
     info = {"pairs": lc.numPairs(), "instances": len(seeds), "train_steps": steps,
             "loss_before": before, "loss_after": lc.evaluate(),
             "loss_first50": float(np.mean(losses[:50])), "loss_last50": float(np.mean(losses[-50:])),
+            "dense_layers": "tcgen05 tf32" if lc.tensorCores else "fp32 cuda cores",
+            "train_seconds": train_s, "ms_per_train_step": 1e3 * train_s / max(steps, 1),
             "seconds": time.perf_counter() - t0}
     return lc, info
 
@@ -600,6 +604,13 @@ def main():
             "learned_training": learned_info,
             "levels": int(pm["levels"]),
             "kernels_per_cycle": int(pm["kernels_per_cycle"]),
+            "kernel_timings": {
+                v: {"gs_pass_ms": r["profile"]["gs_pass_ms"],
+                    "gs_pass_gbs": r["profile"]["gs_pass_bytes"] / (r["profile"]["gs_pass_ms"] * 1e-3) / 1e9,
+                    "residual_ms": r["profile"]["residual_ms"],
+                    "residual_gbs": r["profile"]["residual_bytes"] / (r["profile"]["residual_ms"] * 1e-3) / 1e9,
+                    "cycle_ms": r["profile"]["cycle_ms"], "kernels_per_cycle": int(r["profile"]["kernels_per_cycle"])}
+                for v, r in results.items()},
             "gpu_launches": int(head["launches"]) * args.steps,
             "roofline": roofline,
             "cpu_baseline": cpu,

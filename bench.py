@@ -155,6 +155,16 @@ def make_workload(name: str):
         gen = lambda seed: meshgen.config0(n=256, seed=seed)  # noqa: E731
         desc = "steady 2D heat conduction, jittered 256^2 quads"
         seed = 0
+    elif name == "config3":
+        gen = lambda seed: meshgen.config3(n=100, seed=seed)  # noqa: E731
+        desc = ("steady 3D heat conduction, 100^3 hexes, two-phase: k = 1e4 in random spheres "
+                "(r 0.02-0.08, 30% volume), 1 outside")
+        seed = 3
+    elif name == "config4":
+        gen = lambda seed: meshgen.config4(n=200, seed=seed)  # noqa: E731
+        desc = ("implicit transient 3D heat conduction, 200^3 hexes, k ~ lognormal(0,1), rho c ~ U[0.5,2]: "
+                "one backward-Euler step (dt = 1e-3) from T0 = 300 with x=1 held at 400")
+        seed = 4
     else:
         raise SystemExit("unknown workload " + name)
     mesh, f = gen(seed)
@@ -177,6 +187,8 @@ def train_learned(gen, inner_rel, seeds=(101, 102), n_outer=4, per_solve=3, step
         s.tm.init()
         s.tf.conductivity[cells] = s.k
         s.tf.source[cells] = s.s
+        if s.rc is not None:
+            s.tf.specificHeat[cells] = s.rc
         lc.harvest(s.tm, nOuter=n_outer, perSolve=per_solve, relativeTolerance=1e-8, maxCycles=100)
         del s
     before = lc.evaluate()
@@ -190,6 +202,32 @@ def train_learned(gen, inner_rel, seeds=(101, 102), n_outer=4, per_solve=3, step
             "train_seconds": train_s, "ms_per_train_step": 1e3 * train_s / max(steps, 1),
             "seconds": time.perf_counter() - t0}
     return lc, info
+
+
+def size_matched_copy_gbs(nbytes: float, reps: int = 7) -> float:
+    """Bandwidth of a plain device-to-device copy that moves the same bytes
+    as a kernel (nbytes/2 read + nbytes/2 written), CUDA events, L2 flushed
+    before each repetition: what streaming reaches at this transfer size,
+    launch and ramp included, beside the large-transfer peak."""
+    import torch
+
+    n = max(1, int(nbytes // 16))
+    src = torch.ones(n, dtype=torch.float64, device="cuda")
+    dst = torch.empty_like(src)
+    flush = torch.empty(64 << 20, dtype=torch.float64, device="cuda")
+    times = []
+    for r in range(reps + 2):
+        flush.fill_(float(r))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        dst.copy_(src)
+        e1.record()
+        e1.synchronize()
+        if r >= 2:
+            times.append(e0.elapsed_time(e1))
+    ms = statistics.median(times)
+    del src, dst, flush
+    return 16.0 * n / (ms * 1e-3) / 1e9
 
 
 def solver_for(variant: str, inner_rel: float):
@@ -241,6 +279,12 @@ class Solve:
         o = self.tm.getOptions()
         o.linearSolver = solver_for(variant, inner_rel)
         o.relativeTolerance = outer_rel
+        self.rc = None
+        if "rc" in fields:  # transient: one backward-Euler step from T0 per bench step
+            o.transient = True
+            o["timeStep"] = 1e-3
+            o["initialTemperature"] = 300.0
+            self.rc = np.ascontiguousarray(fields["rc"])
         self.max_outer = max_outer
         self.k = np.ascontiguousarray(fields["k"])
         self.s = np.ascontiguousarray(fields["s"])
@@ -253,11 +297,13 @@ class Solve:
         self.tm.init()
         self.tf.conductivity[cells] = self.k
         self.tf.source[cells] = self.s
+        if self.rc is not None:
+            self.tf.specificHeat[cells] = self.rc
         rep = self.tm.advance(self.max_outer)
         T = self.tf.temperature[cells]
         t1 = time.perf_counter()
         n_all = cells.getCount()
-        h2d = 8 * 3 * n_all  # T (initial), k, source
+        h2d = 8 * (3 if self.rc is None else 4) * n_all  # T (initial), k, source (, rho c)
         d2h = 8 * n_all
         return rep.seconds, t1 - t0, rep, T, h2d, d2h
 
@@ -280,14 +326,18 @@ def cpu_reference(mesh, fields, plain_counts, inner_rel, desc, cores_note=True):
     r = ref.RefThermal(mesh)
     kk = extend_to_ghosts(mesh, fields["k"])
     ss = extend_to_ghosts(mesh, fields["s"])
+    rc = extend_to_ghosts(mesh, fields["rc"]) if "rc" in fields else None
+    extra = {"transient": True, "dt": 1e-3} if rc is not None else {}
 
     def run(cycles):
-        r.set_options(n_pre=1, n_post=1, max_iter=1 + cycles, lin_rel=1e-30, rel=1e-30)
+        r.set_options(n_pre=1, n_post=1, max_iter=1 + cycles, lin_rel=1e-30, rel=1e-30, **extra)
         for gid, (kind, val) in fields["bc"].items():
             r.set_bc(gid, 0 if kind == "T" else 1, [val] if kind == "T" else [None, val])
         r.init()
         r.set_field(1, kk)
         r.set_field(2, ss)
+        if rc is not None:
+            r.set_field(3, rc)
         _, sec = r.advance(1)
         return sec
 
@@ -553,6 +603,15 @@ def main():
                                  "frac": pp["gs_pass_bytes"] / (pp["gs_pass_ms"] * 1e-3) / 1e9 / peak},
                 "fp64_residual": {"achieved": pp["residual_bytes"] / (pp["residual_ms"] * 1e-3) / 1e9,
                                   "frac": pp["residual_bytes"] / (pp["residual_ms"] * 1e-3) / 1e9 / peak}}
+    try:
+        copy_gbs = dist.max(size_matched_copy_gbs(pp["residual_bytes"])) if dist.world == 1 else None
+    except Exception:  # context only
+        copy_gbs = None
+    if copy_gbs:
+        roofline["size_matched_copy"] = {
+            "bytes": pp["residual_bytes"], "gbs": copy_gbs, "frac_of_peak": copy_gbs / peak,
+            "fp64_residual_vs_copy": roofline["fp64_residual"]["achieved"] / copy_gbs,
+            "fp64_gs_pass_vs_copy": roofline["fp64_gs_pass"]["achieved"] / copy_gbs}
 
     cpu = None
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:

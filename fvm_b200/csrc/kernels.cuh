@@ -52,7 +52,9 @@ void residual(const SellView<T>& a, int nSlices, const T* x, const T* b, T* r, d
               cudaStream_t st);
 // y = D x + O x (FP64 only)
 void spmv(const SellView<double>& a, int nSlices, const double* x, double* y, cudaStream_t st);
-int reduce_blocks(int nSlices);  // number of partials residual() writes
+int reduce_blocks(int nSlices);  // grid of the SELL-32 whole-level row kernels
+// number of L1 partials residual() writes for a level (one per block)
+int residual_partials(int nSlices, int n, int ellWidth);
 
 // r = b + D x + O x on a plain CSR matrix (implicit diagonal, reference
 // column order), one thread per row; block k writes the L1 sum of its 256

@@ -236,7 +236,7 @@ void AmgHierarchy::uploadMatrix(const PackedLevel& p, DevLevel& d, bool mixed) {
   d.tmp = (double*)arena_.alloc(nb);
   CUDA_OK(cudaMemset(d.x, 0, nb));
   CUDA_OK(cudaMemset(d.b, 0, nb));
-  d.nPartials = dev::reduce_blocks(d.nSlices);
+  d.nPartials = dev::residual_partials(d.nSlices, d.n, d.ellWidth);
   d.partials = (double*)arena_.alloc(sizeof(double) * (d.nPartials + 1));
   if (mixed) {
     d.valsF = (float*)arena_.alloc(sizeof(float) * p.vals.size());

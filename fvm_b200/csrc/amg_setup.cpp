@@ -8,30 +8,6 @@
 
 namespace fvm {
 
-namespace {
-
-// Runs f(begin, end) over [0, n) split into contiguous chunks on the host's
-// cores (one chunk when n is small).
-template <class F>
-void parallel_chunks(int n, F f, int minItems = 20000) {
-  int nt = (int)std::thread::hardware_concurrency();
-  if (nt < 1) nt = 1;
-  if (nt > 32) nt = 32;
-  if (n < minItems || nt == 1) {
-    f(0, n);
-    return;
-  }
-  std::vector<std::thread> th;
-  const int chunk = (n + nt - 1) / nt;
-  for (int t = 0; t < nt; t++) {
-    const int b = t * chunk, e = std::min(n, b + chunk);
-    if (b >= e) break;
-    th.emplace_back([=] { f(b, e); });
-  }
-  for (auto& x : th) x.join();
-}
-
-}  // namespace
 
 namespace {
 // The greedy walk over rows [rb, re) with coarse rows numbered from 0; count
@@ -146,75 +122,72 @@ void create_coarse_level(const RefLevel& fine, RefLevel& coarse, CSR& c2f) {
   }
   // Coarse pattern: each coarse row lists the coarse neighbours of its fine
   // rows in first-visit order. Rows are independent, so they are built in
-  // parallel: a count pass, a prefix sum, a fill pass (rows are short, so a
-  // linear search replaces the reference's marker array).
+  // parallel: a count pass, a prefix sum, a fill pass. A per-thread stamp
+  // array (stamp[J] == I: J already listed in row I) replaces the
+  // reference's marker array and needs no clearing between rows.
   coarse.n = nc;
   coarse.symmetricPattern = fine.symmetricPattern;
   coarse.conn.nRows = nc;
   coarse.conn.row.assign(nc + 1, 0);
-  auto visit = [&](int I, int* out) {
+  auto visit = [&](int I, int* out, int* stamp) {
     int cnt = 0;
     for (int k = c2f.row[I]; k < c2f.row[I + 1]; k++) {
       const int i = c2f.col[k];
       for (int nb = row[i]; nb < row[i + 1]; nb++) {
         const int J = ci[col[nb]];
-        if (J < 0 || J == I) continue;
-        bool seen = false;
-        for (int q = 0; q < cnt; q++)
-          if (out[q] == J) {
-            seen = true;
-            break;
-          }
-        if (!seen) out[cnt++] = J;
+        if (J < 0 || J == I || stamp[J] == I) continue;
+        stamp[J] = I;
+        if (out) out[cnt] = J;
+        cnt++;
       }
     }
     return cnt;
   };
-  int maxRow = 0;
-  for (int I = 0; I < nc; I++) {
-    int w = 0;
-    for (int k = c2f.row[I]; k < c2f.row[I + 1]; k++) w += row[c2f.col[k] + 1] - row[c2f.col[k]];
-    maxRow = std::max(maxRow, w);
-  }
+  constexpr int kMinRows = 4096;  // coarse rows per level below which the passes run on one thread
   parallel_chunks(nc, [&](int b, int e) {
-    std::vector<int> buf(maxRow + 1);
-    for (int I = b; I < e; I++) coarse.conn.row[I + 1] = visit(I, buf.data());
-  });
+    std::vector<int> stamp(nc, -1);
+    for (int I = b; I < e; I++) coarse.conn.row[I + 1] = visit(I, nullptr, stamp.data());
+  }, kMinRows);
   for (int I = 0; I < nc; I++) coarse.conn.row[I + 1] += coarse.conn.row[I];
-  coarse.conn.col.assign(coarse.conn.row[nc], 0);
-  parallel_chunks(nc, [&](int b, int e) {
-    for (int I = b; I < e; I++) visit(I, &coarse.conn.col[coarse.conn.row[I]]);
-  });
+  coarse.conn.col.resize(coarse.conn.row[nc]);
+  coarse.diag.resize(nc);
+  coarse.off.resize(coarse.conn.col.size());
   // Galerkin values with piecewise-constant prolongation; every coarse
   // entry receives its fine contributions in the reference's order (fine
   // rows ascending, their entries in stored order), so the sums round
-  // exactly as CRMatrix::createCoarseMatrix's do.
-  coarse.diag.assign(nc, 0.0);
-  coarse.off.assign(coarse.conn.col.size(), 0.0);
+  // exactly as CRMatrix::createCoarseMatrix's do. The fill of row I and its
+  // values share one pass: pos[J] is J's slot in the row being built.
   parallel_chunks(nc, [&](int b, int e) {
+    std::vector<int> stamp(nc, -1), pos(nc, 0);
     for (int I = b; I < e; I++) {
-      const int rb = coarse.conn.row[I], re = coarse.conn.row[I + 1];
+      const int rb = coarse.conn.row[I];
+      int* out = &coarse.conn.col[rb];
+      const int cnt = visit(I, out, stamp.data());
+      for (int q = 0; q < cnt; q++) {
+        pos[out[q]] = rb + q;
+        coarse.off[rb + q] = 0.0;
+      }
+      double d = 0.0;
       for (int k = c2f.row[I]; k < c2f.row[I + 1]; k++) {
         const int i = c2f.col[k];
-        coarse.diag[I] += fine.diag[i];
+        d += fine.diag[i];
         for (int nb = row[i]; nb < row[i + 1]; nb++) {
           const int J = ci[col[nb]];
           if (J < 0) continue;
-          if (J != I) {
-            int p = rb;
-            while (p < re && coarse.conn.col[p] != J) p++;
-            coarse.off[p] += fine.off[nb];
-          } else {
-            coarse.diag[I] += fine.off[nb];
-          }
+          if (J != I)
+            coarse.off[pos[J]] += fine.off[nb];
+          else
+            d += fine.off[nb];
         }
       }
+      coarse.diag[I] = d;
     }
-  });
+  }, kMinRows);
 }
 
 void build_hierarchy(std::vector<RefLevel>& levels, const HierarchyOptions& opt,
-                     std::vector<CSR>& coarseToFine) {
+                     std::vector<CSR>& coarseToFine, std::vector<RefLevel>* spareLevels,
+                     std::vector<CSR>* spareC2f) {
   levels.resize(1);
   coarseToFine.clear();
   for (int n = 0; n < opt.maxCoarseLevels; n++) {
@@ -224,10 +197,15 @@ void build_hierarchy(std::vector<RefLevel>& levels, const HierarchyOptions& opt,
     const int fineLocal = (levels.size() == 1 && opt.finestLocalSize > 0) ? opt.finestLocalSize : fine.n;
     if (fineLocal == nc) break;  // AMG.cpp:161-168
     if (nc <= 3) break;          // AMG.cpp:200-204 (serial: level not kept)
-    fine.coarseIndex = ci;
+    fine.coarseIndex.swap(ci);
     fine.nCoarse = nc;
+    const size_t lc = levels.size();
     RefLevel coarse;
+    if (spareLevels && lc < spareLevels->size()) coarse = std::move((*spareLevels)[lc]);
+    coarse.coarseIndex.clear();
+    coarse.nCoarse = 0;
     CSR c2f;
+    if (spareC2f && lc - 1 < spareC2f->size()) c2f = std::move((*spareC2f)[lc - 1]);
     create_coarse_level(fine, coarse, c2f);
     coarse.segments = std::move(coarseSeg);
     levels.push_back(std::move(coarse));
@@ -412,6 +390,11 @@ int greedy_coloring(const CSR& conn, std::vector<int>& color) {
 void pack_level(const RefLevel& lv, SmootherOrdering ordering, PackedLevel& out) {
   const int n = lv.n;
   out.n = n;
+  // (out may be a reused object: pack_transfer refills these for all but
+  // the coarsest level)
+  out.coarseIndex.clear();
+  out.c2fRow.clear();
+  out.c2fCol.clear();
   std::vector<int> color;
   if (ordering == kSequential) {
     color.assign(n, 0);

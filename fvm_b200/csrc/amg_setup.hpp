@@ -60,8 +60,11 @@ struct HierarchyOptions {
 
 // Builds levels[1..] from levels[0]; levels.size() - 1 coarse levels are
 // kept, following AMG::createCoarseLevels (serial build, AMG.cpp:150-210).
+// spareLevels / spareC2f (optional, indexed by level): objects of an earlier
+// build whose buffers the new levels reuse.
 void build_hierarchy(std::vector<RefLevel>& levels, const HierarchyOptions& opt,
-                     std::vector<CSR>& coarseToFine);
+                     std::vector<CSR>& coarseToFine, std::vector<RefLevel>* spareLevels = nullptr,
+                     std::vector<CSR>* spareC2f = nullptr);
 
 // Packed, colour-permuted form of one level for the GPU.
 struct PackedLevel {

@@ -2,9 +2,11 @@
 // compressed-row (CSR) containers and CUDA call checking.
 #pragma once
 
+#include <algorithm>
 #include <cstdint>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <vector>
 
 namespace fvm {
@@ -47,5 +49,26 @@ struct CSR {
   int count(int i) const { return row[i + 1] - row[i]; }
   int nnz() const { return row.empty() ? 0 : row[nRows]; }
 };
+
+// Runs f(begin, end) over [0, n) split into contiguous chunks on the host's
+// cores (at most 32 threads; one chunk when n < minItems).
+template <class F>
+void parallel_chunks(int n, F f, int minItems = 20000) {
+  int nt = (int)std::thread::hardware_concurrency();
+  if (nt < 1) nt = 1;
+  if (nt > 32) nt = 32;
+  if (n < minItems || nt == 1) {
+    f(0, n);
+    return;
+  }
+  std::vector<std::thread> th;
+  const int chunk = (n + nt - 1) / nt;
+  for (int t = 0; t < nt; t++) {
+    const int b = t * chunk, e = std::min(n, b + chunk);
+    if (b >= e) break;
+    th.emplace_back([=] { f(b, e); });
+  }
+  for (auto& x : th) x.join();
+}
 
 }  // namespace fvm

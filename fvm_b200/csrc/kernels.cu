@@ -990,6 +990,30 @@ const int* gauss_jordan_status(int n, const void* scratch) {
   const char* s = (const char*)scratch;
   return (const int*)(s + gj_align(sizeof(double) * kGjMaxPanel * (size_t)n) + 2 * gj_align(sizeof(int) * (size_t)n));
 }
+namespace {
+// a (n x n, row-major, zeroed) += the SELL-32 level: one thread per row
+__global__ void k_dense_from_sell(SellView<double> m, int nSlices, double* a) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int s = t >> 5, lane = t & 31;
+  if (s >= nSlices) return;
+  const int4 mt = m.meta[s];
+  if (lane >= mt.y) return;
+  const int i = mt.x + lane;
+  double* ai = a + (size_t)i * m.n;
+  ai[i] += m.diag[i];
+  for (int k = 0; k < mt.w; k++) {
+    const int e = mt.z + (k << 5) + lane;
+    const double v = m.vals[e];
+    if (v != 0.0) ai[m.cols[e]] += v;
+  }
+}
+}  // namespace
+
+void dense_from_sell(const SellView<double>& m, int nSlices, double* a, cudaStream_t st) {
+  cudaMemsetAsync(a, 0, sizeof(double) * (size_t)m.n * m.n, st);
+  k_dense_from_sell<<<ceil_div((long long)nSlices * 32, kBlock), kBlock, 0, st>>>(m, nSlices, a);
+}
+
 void gauss_jordan_inverse(int n, double* a, double* inv, void* scratch, cudaStream_t st) {
   char* s = (char*)scratch;
   double* Bt = (double*)s;

@@ -92,6 +92,9 @@ void dense_solve_f32(int n, const float* ainv, const float* b, float* x, cudaStr
 // gauss_jordan_scratch_bytes(n); *status (device int inside scratch, see
 // gauss_jordan_status) becomes 1 if a pivot was exactly zero. Asynchronous
 // on st.
+// a = the dense n x n form (row-major) of a SELL-32 level (not ELL-32):
+// diagonal plus every nonzero stored entry; asynchronous on st.
+void dense_from_sell(const SellView<double>& m, int nSlices, double* a, cudaStream_t st);
 size_t gauss_jordan_scratch_bytes(int n);
 void gauss_jordan_inverse(int n, double* a, double* inv, void* scratch, cudaStream_t st);
 // device address of the status flag inside scratch

@@ -29,6 +29,7 @@ DeviceArena::~DeviceArena() {
 }
 
 void* DeviceArena::alloc(size_t bytes) {
+  std::lock_guard<std::mutex> lock(mu_);
   void* p = nullptr;
   if (bytes == 0) bytes = 16;
   auto it = free_.find(bytes);
@@ -48,19 +49,49 @@ void DeviceArena::copy_h2d(void* d, const void* h, size_t n) {
 }
 
 void DeviceArena::release() {
+  std::lock_guard<std::mutex> lock(mu_);
   for (auto& pb : ptrs_) free_.insert({pb.second, pb.first});
   ptrs_.clear();
   bytes_ = 0;
 }
 
 // ---------------------------------------------------------------------------
+namespace {
+// moves the objects of `from` into the spare slots of the same index
+template <class T>
+void keep_spares(std::vector<T>& from, std::vector<T>& spares) {
+  if (spares.size() < from.size()) spares.resize(from.size());
+  for (size_t l = 0; l < from.size(); l++) spares[l] = std::move(from[l]);
+  from.clear();
+}
+template <class T>
+T take_spare(std::vector<T>& spares, size_t l) {
+  if (l < spares.size()) return std::move(spares[l]);
+  return T();
+}
+}  // namespace
+
 void AmgHierarchy::release() {
   arena_.release();
   lv_.clear();
-  packed_.clear();
-  ref_.clear();
+  keep_spares(packed_, sparePacked_);
+  keep_spares(ref_, spareRef_);
+  keep_spares(c2f_, spareC2f_);
   coarseInv_ = nullptr;
   coarseInvF_ = nullptr;
+}
+
+RefLevel AmgHierarchy::spareLevel(int l) { return take_spare(spareRef_, (size_t)l); }
+
+void* AmgHierarchy::scratch(size_t bytes) { return arena_.alloc(bytes); }
+
+double* AmgHierarchy::pinnedScalars() {
+  if (!pinned_) CUDA_OK(cudaMallocHost(&pinned_, sizeof(double) * 32));
+  return pinned_;
+}
+
+AmgHierarchy::~AmgHierarchy() {
+  if (pinned_) cudaFreeHost(pinned_);
 }
 
 std::vector<int> AmgHierarchy::sizes() const {
@@ -70,7 +101,16 @@ std::vector<int> AmgHierarchy::sizes() const {
 }
 
 void AmgHierarchy::build(std::vector<RefLevel>& levels, int finestLocalSize, const SolverOptions& opt) {
+  const bool trace = getenv("FVM_TRACE") != nullptr;
+  auto t0 = std::chrono::steady_clock::now();
+  auto lap = [&](const char* what) {
+    if (!trace) return;
+    const auto t1 = std::chrono::steady_clock::now();
+    fprintf(stderr, "[fvm setup] %-28s %8.1f ms\n", what, std::chrono::duration<double, std::milli>(t1 - t0).count());
+    t0 = t1;
+  };
   release();
+  lap("previous hierarchy released");
   opt_ = opt;
   ref_ = std::move(levels);
   levels.clear();
@@ -80,20 +120,12 @@ void AmgHierarchy::build(std::vector<RefLevel>& levels, int finestLocalSize, con
   ho.weightRatioThreshold = opt.weightRatioThreshold;
   ho.coarsestSize = opt.coarsestSize;
   ho.finestLocalSize = finestLocalSize;
-  const bool trace = getenv("FVM_TRACE") != nullptr;
-  auto t0 = std::chrono::steady_clock::now();
-  auto lap = [&](const char* what) {
-    if (!trace) return;
-    const auto t1 = std::chrono::steady_clock::now();
-    fprintf(stderr, "[fvm setup] %-28s %8.1f ms\n", what, std::chrono::duration<double, std::milli>(t1 - t0).count());
-    t0 = t1;
-  };
   const bool mixed = opt.precision == kMixed;
   // Level 0 (the largest) is coloured, packed and uploaded on another
   // thread while the coarse levels are aggregated; ref_ has room for every
   // level, so appending coarse levels never moves level 0.
   ref_.reserve((size_t)std::max(1, opt.maxCoarseLevels) + 2);
-  PackedLevel p0;
+  PackedLevel p0 = take_spare(sparePacked_, 0);
   DevLevel d0;
   std::exception_ptr err0;
   std::thread level0([&] {
@@ -104,9 +136,9 @@ void AmgHierarchy::build(std::vector<RefLevel>& levels, int finestLocalSize, con
       err0 = std::current_exception();
     }
   });
-  std::vector<CSR> c2f;
+  std::vector<CSR>& c2f = c2f_;
   try {
-    build_hierarchy(ref_, ho, c2f);
+    build_hierarchy(ref_, ho, c2f, &spareRef_, &spareC2f_);
   } catch (...) {
     level0.join();
     throw;
@@ -114,15 +146,46 @@ void AmgHierarchy::build(std::vector<RefLevel>& levels, int finestLocalSize, con
   lap("aggregation + Galerkin");
   const int L = (int)ref_.size();
   packed_.resize(L);
+  for (int l = 1; l < L; l++) packed_[l] = take_spare(sparePacked_, (size_t)l);
   lv_.resize(L);
+  // Coarsest direct solve: as soon as the coarsest level is packed and
+  // uploaded, its dense form is built on the GPU and inverted on a stream of
+  // its own, overlapping the packing and uploads of the other levels.
+  const bool direct = opt.coarseSolver == kCoarseDirect && !opt.finestOnly();
+  cudaStream_t gjStream = nullptr;
+  void* gjScratch = nullptr;
+  int coarseN = 0;
+  auto startCoarseInverse = [&](int l) {
+    const PackedLevel& c = packed_[l];
+    const size_t nn = (size_t)c.n * c.n;
+    coarseN = c.n;
+    FVM_REQUIRE(c.n <= 4096, kTooLarge,
+                "coarsest level too large for the dense direct solve (max 4096 rows); set coarsestSize");
+    if (c.n <= 128) {
+      std::vector<double> inv;
+      dense_inverse(c, inv);
+      coarseInv_ = arena_.upload(inv);
+      return;
+    }
+    FVM_REQUIRE(lv_[l].ellWidth == 0, kUnsupported, "coarsest level in ELL-32 layout");
+    double* dA = (double*)arena_.alloc(sizeof(double) * nn);
+    gjScratch = arena_.alloc(dev::gauss_jordan_scratch_bytes(c.n));
+    coarseInv_ = (double*)arena_.alloc(sizeof(double) * nn);
+    CUDA_OK(cudaStreamCreateWithFlags(&gjStream, cudaStreamNonBlocking));
+    dev::dense_from_sell(lv_[l].view64(), lv_[l].nSlices, dA, gjStream);
+    dev::gauss_jordan_inverse(c.n, dA, coarseInv_, gjScratch, gjStream);
+  };
   {
     std::vector<std::exception_ptr> errs(L);
     std::vector<std::thread> th;
     for (int l = 1; l < L; l++)
       th.emplace_back([&, l] {
         try {
-          // levels smoothed by damped Jacobi need no colouring
+          // levels smoothed by damped Jacobi need no colouring; each level
+          // uploads as soon as it is packed
           pack_level(ref_[l], dampedLevel(l, ref_[l].n) ? kSequential : opt.ordering, packed_[l]);
+          uploadMatrix(packed_[l], lv_[l], mixed);
+          if (direct && l == L - 1) startCoarseInverse(l);
         } catch (...) {
           errs[l] = std::current_exception();
         }
@@ -135,50 +198,16 @@ void AmgHierarchy::build(std::vector<RefLevel>& levels, int finestLocalSize, con
   }
   packed_[0] = std::move(p0);
   lv_[0] = std::move(d0);
+  if (direct && L == 1) startCoarseInverse(0);
   lap("colouring + packing (+ level 0 upload)");
   for (int l = 0; l + 1 < L; l++) pack_transfer(ref_[l], c2f[l], packed_[l], packed_[l + 1]);
   lap("transfer maps");
-
-  // coarsest direct solve: the inverse runs on its own stream while the
-  // other levels upload
-  cudaStream_t gjStream = nullptr;
-  DeviceArena gjTmp;
-  void* gjScratch = nullptr;
-  const PackedLevel& c = packed_[L - 1];
-  const size_t nn = (size_t)c.n * c.n;
-  if (opt.coarseSolver == kCoarseDirect && !opt.finestOnly()) {
-    FVM_REQUIRE(c.n <= 4096, kTooLarge,
-                "coarsest level too large for the dense direct solve (max 4096 rows); set coarsestSize");
-    if (c.n <= 128) {
-      std::vector<double> inv;
-      dense_inverse(c, inv);
-      coarseInv_ = arena_.upload(inv);
-    } else {
-      // dense copy of the level in its permuted numbering, inverted on the GPU
-      std::vector<double> a(nn, 0.0);
-      for (int p = 0; p < c.n; p++) a[(size_t)p * c.n + p] = c.diag[p];
-      for (size_t s = 0; s + 1 < c.sliceOff.size(); s++) {
-        const int w = (c.sliceOff[s + 1] - c.sliceOff[s]) / 32;
-        for (int l = 0; l < c.sliceRows[s]; l++)
-          for (int k = 0; k < w; k++) {
-            const size_t e = (size_t)c.sliceOff[s] + (size_t)k * 32 + l;
-            if (c.vals[e] != 0.0) a[(size_t)(c.sliceRow[s] + l) * c.n + c.cols[e]] += c.vals[e];
-          }
-      }
-      double* dA = gjTmp.upload(a);
-      gjScratch = gjTmp.alloc(dev::gauss_jordan_scratch_bytes(c.n));
-      coarseInv_ = (double*)arena_.alloc(sizeof(double) * nn);
-      CUDA_OK(cudaStreamCreateWithFlags(&gjStream, cudaStreamNonBlocking));
-      dev::gauss_jordan_inverse(c.n, dA, coarseInv_, gjScratch, gjStream);
-    }
-  }
-  for (int l = 1; l < L; l++) uploadMatrix(packed_[l], lv_[l], mixed);
   for (int l = 0; l + 1 < L; l++) uploadTransfer(packed_[l], lv_[l], packed_[l + 1].n);
-  lap("uploads");
-  if (opt.coarseSolver == kCoarseDirect && !opt.finestOnly()) {
+  lap("transfer uploads");
+  if (direct) {
     if (gjStream) {
       int singular = 0;
-      const cudaError_t e1 = cudaMemcpyAsync(&singular, dev::gauss_jordan_status(c.n, gjScratch), sizeof(int),
+      const cudaError_t e1 = cudaMemcpyAsync(&singular, dev::gauss_jordan_status(coarseN, gjScratch), sizeof(int),
                                              cudaMemcpyDeviceToHost, gjStream);
       const cudaError_t e2 = cudaStreamSynchronize(gjStream);
       cudaStreamDestroy(gjStream);
@@ -187,6 +216,7 @@ void AmgHierarchy::build(std::vector<RefLevel>& levels, int finestLocalSize, con
       FVM_REQUIRE(singular == 0, kBadArgument, "singular coarsest-level matrix");
     }
     if (mixed) {
+      const size_t nn = (size_t)coarseN * coarseN;
       coarseInvF_ = (float*)arena_.alloc(sizeof(float) * nn);
       dev::cast_d2f(nn, coarseInv_, coarseInvF_, 0);
     }
@@ -638,12 +668,15 @@ enum Scal {
 constexpr int kWorkVectors = 9;
 }  // namespace
 
+// Device workspace comes from the hierarchy's arena (recycled by the next
+// build of the same sizes, so a rebuild allocates nothing); the pinned
+// scalars are the hierarchy's too.
 LinearSolve::LinearSolve(AmgHierarchy& h) : h_(h), n_(h.level(0).n) {
-  CUDA_OK(cudaMalloc(&work_, sizeof(double) * (size_t)n_ * kWorkVectors));
-  CUDA_OK(cudaMalloc(&scal_, sizeof(double) * 32));
+  work_ = (double*)h.scratch(sizeof(double) * (size_t)n_ * kWorkVectors);
+  scal_ = (double*)h.scratch(sizeof(double) * 32);
   CUDA_OK(cudaMemset(scal_, 0, sizeof(double) * 32));
-  CUDA_OK(cudaMalloc(&partials_, sizeof(double) * (dev::vec_blocks(n_) + 1)));
-  CUDA_OK(cudaMallocHost(&hostScal_, sizeof(double) * 32));
+  partials_ = (double*)h.scratch(sizeof(double) * (dev::vec_blocks(n_) + 1));
+  hostScal_ = h.pinnedScalars();
 }
 
 LinearSolve::~LinearSolve() {
@@ -652,10 +685,6 @@ LinearSolve::~LinearSolve() {
   if (g3_) cudaGraphExecDestroy(g3_);
   if (g4_) cudaGraphExecDestroy(g4_);
   if (g5_) cudaGraphExecDestroy(g5_);
-  cudaFree(work_);
-  cudaFree(scal_);
-  cudaFree(partials_);
-  cudaFreeHost(hostScal_);
 }
 
 void LinearSolve::norm_into(const double* v, double* scalar, cudaStream_t st) {

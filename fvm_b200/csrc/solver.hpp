@@ -9,6 +9,7 @@
 
 #include <functional>
 #include <map>
+#include <mutex>
 #include <memory>
 #include <vector>
 
@@ -115,6 +116,7 @@ class DeviceArena {
   std::vector<std::pair<void*, size_t>> ptrs_;
   std::multimap<size_t, void*> free_;
   size_t bytes_ = 0;
+  std::mutex mu_;  // levels are uploaded from several setup threads
 };
 
 class AmgHierarchy {
@@ -122,7 +124,20 @@ class AmgHierarchy {
   // levels[0] is the finest matrix in reference order; the hierarchy
   // (reference-exact aggregation) is built, packed and uploaded.
   void build(std::vector<RefLevel>& levels, int finestLocalSize, const SolverOptions& opt);
+  // Drops the device state and keeps the host-side level objects of this
+  // hierarchy as spares: the next build() of a similar hierarchy refills
+  // their buffers instead of allocating (and page-faulting) new ones.
   void release();
+  // a spare host level object for level l (empty when there is none)
+  RefLevel spareLevel(int l);
+  // device memory that lives until the next release() (recycled by size)
+  void* scratch(size_t bytes);
+  // 32 pinned host doubles owned by the hierarchy (one solver at a time)
+  double* pinnedScalars();
+  AmgHierarchy() = default;
+  ~AmgHierarchy();
+  AmgHierarchy(const AmgHierarchy&) = delete;
+  AmgHierarchy& operator=(const AmgHierarchy&) = delete;
 
   int numLevels() const { return (int)lv_.size(); }
   const DevLevel& level(int l) const { return lv_[l]; }
@@ -162,6 +177,12 @@ class AmgHierarchy {
   SolverOptions opt_;
   std::vector<RefLevel> ref_;
   std::vector<PackedLevel> packed_;
+  std::vector<CSR> c2f_;
+  // host objects of the previous build, by level, reused by the next one
+  std::vector<RefLevel> spareRef_;
+  std::vector<PackedLevel> sparePacked_;
+  std::vector<CSR> spareC2f_;
+  double* pinned_ = nullptr;
   std::vector<DevLevel> lv_;
   double* coarseInv_ = nullptr;  // dense inverse of the coarsest level
   float* coarseInvF_ = nullptr;  // its FP32 copy for the FP32 cycle

@@ -404,18 +404,25 @@ void ThermalModel::ensureMatrix() {
   CUDA_OK(cudaMemcpyAsync(diag.data(), dDiagOrig_, sizeof(double) * n, cudaMemcpyDeviceToHost, stream_));
   CUDA_OK(cudaStreamSynchronize(stream_));
   lap("assembly + copy to host");
+  // the previous hierarchy's host buffers are refilled, not reallocated
+  solver_.reset();
+  hier_.release();
+  lap("previous solver released");
   std::vector<RefLevel> levels(1);
+  levels[0] = hier_.spareLevel(0);
   RefLevel& l0 = levels[0];
   l0.n = n;
   l0.conn = interiorConn_;
   l0.symmetricPattern = true;  // cellCells restricted to self rows
   l0.segments = segOff_;       // a batch: its meshes aggregate in parallel
+  l0.coarseIndex.clear();
+  l0.nCoarse = 0;
   l0.diag = std::move(diag);
   l0.off.resize(entryFace_.size());
-  for (size_t e = 0; e < entryFace_.size(); e++) l0.off[e] = coeff[entryFace_[e]];
+  parallel_chunks((int)entryFace_.size(), [&](int b, int e) {
+    for (int k = b; k < e; k++) l0.off[k] = coeff[entryFace_[k]];
+  }, 1 << 18);
   lap("finest level on host");
-  solver_.reset();
-  lap("previous solver released");
   hier_.build(levels, m.nTotalCells(), opt_.linear);
   lap("hierarchy");
   if (dPerm_) cudaFree(dPerm_);

@@ -187,7 +187,7 @@ void create_coarse_level(const RefLevel& fine, RefLevel& coarse, CSR& c2f) {
 
 void build_hierarchy(std::vector<RefLevel>& levels, const HierarchyOptions& opt,
                      std::vector<CSR>& coarseToFine, std::vector<RefLevel>* spareLevels,
-                     std::vector<CSR>* spareC2f) {
+                     std::vector<CSR>* spareC2f, const std::function<void(int)>& onLevel) {
   levels.resize(1);
   coarseToFine.clear();
   for (int n = 0; n < opt.maxCoarseLevels; n++) {
@@ -208,8 +208,11 @@ void build_hierarchy(std::vector<RefLevel>& levels, const HierarchyOptions& opt,
     if (spareC2f && lc - 1 < spareC2f->size()) c2f = std::move((*spareC2f)[lc - 1]);
     create_coarse_level(fine, coarse, c2f);
     coarse.segments = std::move(coarseSeg);
+    FVM_REQUIRE(levels.size() < levels.capacity() || !onLevel, kBadArgument,
+                "build_hierarchy: no room for another level");
     levels.push_back(std::move(coarse));
     coarseToFine.push_back(std::move(c2f));
+    if (onLevel) onLevel((int)levels.size() - 1);
     if (opt.coarsestSize > 0 && nc <= opt.coarsestSize) break;
   }
   levels.back().coarseIndex.clear();

@@ -9,6 +9,7 @@
 // is packed into SELL-32 slices for the GPU smoothers.
 #pragma once
 
+#include <functional>
 #include <vector>
 
 #include "common.hpp"
@@ -61,10 +62,14 @@ struct HierarchyOptions {
 // Builds levels[1..] from levels[0]; levels.size() - 1 coarse levels are
 // kept, following AMG::createCoarseLevels (serial build, AMG.cpp:150-210).
 // spareLevels / spareC2f (optional, indexed by level): objects of an earlier
-// build whose buffers the new levels reuse.
+// build whose buffers the new levels reuse. onLevel (optional) is called
+// with the index of each new coarse level once its matrix is complete (the
+// caller may then read its conn / diag / off from another thread while the
+// next levels are built; levels must have capacity for every level).
 void build_hierarchy(std::vector<RefLevel>& levels, const HierarchyOptions& opt,
                      std::vector<CSR>& coarseToFine, std::vector<RefLevel>* spareLevels = nullptr,
-                     std::vector<CSR>* spareC2f = nullptr);
+                     std::vector<CSR>* spareC2f = nullptr,
+                     const std::function<void(int)>& onLevel = nullptr);
 
 // Packed, colour-permuted form of one level for the GPU.
 struct PackedLevel {

@@ -121,33 +121,47 @@ void AmgHierarchy::build(std::vector<RefLevel>& levels, int finestLocalSize, con
   ho.coarsestSize = opt.coarsestSize;
   ho.finestLocalSize = finestLocalSize;
   const bool mixed = opt.precision == kMixed;
-  // Level 0 (the largest) is coloured, packed and uploaded on another
-  // thread while the coarse levels are aggregated; ref_ has room for every
-  // level, so appending coarse levels never moves level 0.
-  ref_.reserve((size_t)std::max(1, opt.maxCoarseLevels) + 2);
-  PackedLevel p0 = take_spare(sparePacked_, 0);
-  DevLevel d0;
-  std::exception_ptr err0;
-  std::thread level0([&] {
+  // Every level is coloured, packed and uploaded on a thread of its own as
+  // soon as its matrix exists: level 0 while the coarse levels are
+  // aggregated, level l while levels l+1, ... are (the greedy walks are
+  // sequential and leave the other cores free). ref_, packed_ and lv_ have
+  // room for every level, so appending levels never moves one in use.
+  const size_t maxL = (size_t)std::max(1, opt.maxCoarseLevels) + 2;
+  ref_.reserve(maxL);
+  packed_.resize(maxL);
+  lv_.resize(maxL);
+  std::vector<std::thread> th(maxL);
+  std::vector<std::exception_ptr> errs(maxL);
+  auto packAndUpload = [&](int l) {
     try {
-      pack_level(ref_[0], opt.finestOnly() ? kSequential : opt.ordering, p0);
-      uploadMatrix(p0, d0, mixed);
+      // levels smoothed by damped Jacobi need no colouring
+      const SmootherOrdering ord =
+          l == 0 ? (opt.finestOnly() ? kSequential : opt.ordering)
+                 : (dampedLevel(l, ref_[l].n) ? kSequential : opt.ordering);
+      pack_level(ref_[l], ord, packed_[l]);
+      uploadMatrix(packed_[l], lv_[l], mixed);
     } catch (...) {
-      err0 = std::current_exception();
+      errs[l] = std::current_exception();
     }
-  });
+  };
+  auto startLevel = [&](int l) {
+    packed_[l] = take_spare(sparePacked_, (size_t)l);
+    th[l] = std::thread(packAndUpload, l);
+  };
+  auto joinAll = [&] {
+    for (auto& t : th)
+      if (t.joinable()) t.join();
+  };
+  startLevel(0);
   std::vector<CSR>& c2f = c2f_;
   try {
-    build_hierarchy(ref_, ho, c2f, &spareRef_, &spareC2f_);
+    build_hierarchy(ref_, ho, c2f, &spareRef_, &spareC2f_, startLevel);
   } catch (...) {
-    level0.join();
+    joinAll();
     throw;
   }
   lap("aggregation + Galerkin");
   const int L = (int)ref_.size();
-  packed_.resize(L);
-  for (int l = 1; l < L; l++) packed_[l] = take_spare(sparePacked_, (size_t)l);
-  lv_.resize(L);
   // Coarsest direct solve: as soon as the coarsest level is packed and
   // uploaded, its dense form is built on the GPU and inverted on a stream of
   // its own, overlapping the packing and uploads of the other levels.
@@ -175,35 +189,38 @@ void AmgHierarchy::build(std::vector<RefLevel>& levels, int finestLocalSize, con
     dev::dense_from_sell(lv_[l].view64(), lv_[l].nSlices, dA, gjStream);
     dev::gauss_jordan_inverse(c.n, dA, coarseInv_, gjScratch, gjStream);
   };
+  if (th[L - 1].joinable()) th[L - 1].join();
+  try {
+    if (errs[L - 1]) std::rethrow_exception(errs[L - 1]);
+    if (direct) startCoarseInverse(L - 1);
+  } catch (...) {
+    joinAll();
+    throw;
+  }
+  joinAll();
+  for (int l = 0; l < L; l++)
+    if (errs[l]) std::rethrow_exception(errs[l]);
+  packed_.resize(L);
+  lv_.resize(L);
+  lap("colouring + packing (+ level 0 upload)");
   {
-    std::vector<std::exception_ptr> errs(L);
-    std::vector<std::thread> th;
-    for (int l = 1; l < L; l++)
-      th.emplace_back([&, l] {
+    // transfer maps of all levels at once (level l writes only its own)
+    std::vector<std::thread> tt;
+    std::vector<std::exception_ptr> terr(L);
+    for (int l = 0; l + 1 < L; l++)
+      tt.emplace_back([&, l] {
         try {
-          // levels smoothed by damped Jacobi need no colouring; each level
-          // uploads as soon as it is packed
-          pack_level(ref_[l], dampedLevel(l, ref_[l].n) ? kSequential : opt.ordering, packed_[l]);
-          uploadMatrix(packed_[l], lv_[l], mixed);
-          if (direct && l == L - 1) startCoarseInverse(l);
+          pack_transfer(ref_[l], c2f[l], packed_[l], packed_[l + 1]);
+          uploadTransfer(packed_[l], lv_[l], packed_[l + 1].n);
         } catch (...) {
-          errs[l] = std::current_exception();
+          terr[l] = std::current_exception();
         }
       });
-    for (auto& t : th) t.join();
-    level0.join();
-    if (err0) std::rethrow_exception(err0);
-    for (auto& e : errs)
+    for (auto& t : tt) t.join();
+    for (auto& e : terr)
       if (e) std::rethrow_exception(e);
   }
-  packed_[0] = std::move(p0);
-  lv_[0] = std::move(d0);
-  if (direct && L == 1) startCoarseInverse(0);
-  lap("colouring + packing (+ level 0 upload)");
-  for (int l = 0; l + 1 < L; l++) pack_transfer(ref_[l], c2f[l], packed_[l], packed_[l + 1]);
-  lap("transfer maps");
-  for (int l = 0; l + 1 < L; l++) uploadTransfer(packed_[l], lv_[l], packed_[l + 1].n);
-  lap("transfer uploads");
+  lap("transfer maps + uploads");
   if (direct) {
     if (gjStream) {
       int singular = 0;

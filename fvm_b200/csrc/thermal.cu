@@ -37,14 +37,14 @@ ThermalModel::~ThermalModel() {
   solver_.reset();
   hier_.release();
   freeDevice();
+  if (hPinned_) cudaFreeHost(hPinned_);
   if (dSegOff_) cudaFree(dSegOff_);
   if (dSegNorm_) cudaFree(dSegNorm_);
 }
 
 void ThermalModel::freeDevice() {
   arena_.release();
-  if (dPerm_) cudaFree(dPerm_);
-  dPerm_ = nullptr;
+  dPerm_ = nullptr;  // lives in the hierarchy's arena
   if (stream_) cudaStreamDestroy(stream_);
   stream_ = nullptr;
   deviceReady_ = false;
@@ -399,9 +399,20 @@ void ThermalModel::ensureMatrix() {
   dev::CellFaceView cf{dCfRow_, dCfCol_, dBRow_, dBCol_, dBColG_};
   const dev::BoundaryData bd = boundaryData();
   dev::assemble_matrix(n, cf, dFaceCells_, dCoeff_, dAreaMag_, rhoVdt, bd, dBIndexOfFace_, dT_, dDiagOrig_, stream_);
-  std::vector<double> coeff(F), diag(n);
-  CUDA_OK(cudaMemcpyAsync(coeff.data(), dCoeff_, sizeof(double) * F, cudaMemcpyDeviceToHost, stream_));
-  CUDA_OK(cudaMemcpyAsync(diag.data(), dDiagOrig_, sizeof(double) * n, cudaMemcpyDeviceToHost, stream_));
+  // face coefficients and diagonal come back through pinned buffers kept
+  // for the model's lifetime
+  const size_t pinBytes = sizeof(double) * ((size_t)F + (size_t)n);
+  if (pinBytes > hPinnedBytes_) {
+    if (hPinned_) cudaFreeHost(hPinned_);
+    hPinned_ = nullptr;
+    hPinnedBytes_ = 0;
+    CUDA_OK(cudaMallocHost(&hPinned_, pinBytes));
+    hPinnedBytes_ = pinBytes;
+  }
+  const double* coeff = hPinned_;
+  double* hDiag = hPinned_ + F;
+  CUDA_OK(cudaMemcpyAsync(hPinned_, dCoeff_, sizeof(double) * F, cudaMemcpyDeviceToHost, stream_));
+  CUDA_OK(cudaMemcpyAsync(hDiag, dDiagOrig_, sizeof(double) * n, cudaMemcpyDeviceToHost, stream_));
   CUDA_OK(cudaStreamSynchronize(stream_));
   lap("assembly + copy to host");
   // the previous hierarchy's host buffers are refilled, not reallocated
@@ -417,7 +428,7 @@ void ThermalModel::ensureMatrix() {
   l0.segments = segOff_;       // a batch: its meshes aggregate in parallel
   l0.coarseIndex.clear();
   l0.nCoarse = 0;
-  l0.diag = std::move(diag);
+  l0.diag.assign(hDiag, hDiag + n);
   l0.off.resize(entryFace_.size());
   parallel_chunks((int)entryFace_.size(), [&](int b, int e) {
     for (int k = b; k < e; k++) l0.off[k] = coeff[entryFace_[k]];
@@ -425,11 +436,9 @@ void ThermalModel::ensureMatrix() {
   lap("finest level on host");
   hier_.build(levels, m.nTotalCells(), opt_.linear);
   lap("hierarchy");
-  if (dPerm_) cudaFree(dPerm_);
-  dPerm_ = nullptr;
-  CUDA_OK(cudaMalloc(&dPerm_, sizeof(int) * (size_t)n));
-  CUDA_OK(cudaMemcpy(dPerm_, hier_.packed(0).perm.data(), sizeof(int) * (size_t)n,
-                     cudaMemcpyHostToDevice));
+  dPerm_ = (int*)hier_.scratch(sizeof(int) * (size_t)n);
+  CUDA_OK(cudaMemcpyAsync(dPerm_, hier_.packed(0).perm.data(), sizeof(int) * (size_t)n, cudaMemcpyHostToDevice,
+                          stream_));
   solver_.reset(new LinearSolve(hier_));
   solver_->setLearned(learned_);
   lap("solver workspace");

@@ -154,6 +154,8 @@ class ThermalModel {
   int *dFaceCells_ = nullptr, *dCcRow_ = nullptr, *dCcCol_ = nullptr;
   int *dCfRow_ = nullptr, *dCfCol_ = nullptr, *dBRow_ = nullptr, *dBCol_ = nullptr, *dBColG_ = nullptr;
   int *dBFace_ = nullptr, *dBKind_ = nullptr, *dBIndexOfFace_ = nullptr, *dPerm_ = nullptr;
+  double* hPinned_ = nullptr;  // pinned host staging of the face coefficients and diagonal
+  size_t hPinnedBytes_ = 0;
   double *dArea_ = nullptr, *dAreaMag_ = nullptr, *dCentroid_ = nullptr, *dVol_ = nullptr;
   double *dGradW_ = nullptr, *dGrad_ = nullptr, *dFlux_ = nullptr, *dCoeff_ = nullptr, *dSec_ = nullptr;
   double *dT_ = nullptr, *dK_ = nullptr, *dSrc_ = nullptr, *dRc_ = nullptr, *dTN1_ = nullptr;

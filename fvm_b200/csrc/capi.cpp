@@ -572,6 +572,7 @@ struct CsrGraph {
     g.a.meta = arena.upload(meta);
     g.rowSlice = arena.upload(rs);
     g.nSlices = (int)p.sliceRow.size();
+    g.entries = (long long)p.cols.size();
   }
 };
 }  // namespace
@@ -676,7 +677,7 @@ int fvm_learned_forward_csr(fvm_learned* l, int n, const int* row, const int* co
     double* dr = tmp.upload(std::vector<double>(r, r + n));
     double* dOut = (double*)tmp.alloc(sizeof(double) * (size_t)n);
     double* scal = (double*)tmp.alloc(sizeof(double) * 8);
-    l->lc->prepare(n);
+    l->lc->prepare(n, cg.g.entries);
     l->lc->apply(cg.g, dr, dOut, scal, 0);
     if (cudaMemcpy(out, dOut, sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost) != cudaSuccess)
       throw Error(kDeviceError, "copy of the network output failed");
@@ -695,7 +696,7 @@ int fvm_learned_gradient_csr(fvm_learned* l, int n, const int* row, const int* c
     float* dg = (float*)tmp.alloc(sizeof(float) * nn::kParams);
     double* scal = (double*)tmp.alloc(sizeof(double) * 8);
     nn::Workspace ws;
-    ws.allocate(n, true);
+    ws.allocate(n, true, cg.g.entries);
     ws.tensorCores = l->lc->tensorCores();
     nn::forward_backward(cg.g, l->lc->deviceParams(), dr, de, dg, scal + 4, ws, scal, 0);
     if (cudaMemcpy(grad, dg, sizeof(float) * nn::kParams, cudaMemcpyDeviceToHost) != cudaSuccess ||

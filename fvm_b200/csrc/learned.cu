@@ -90,7 +90,53 @@ struct GraphArgs {
   const double* diag;
   const int4* meta;
   const int* rowSlice;
+  const float* wf;  // per stored entry (i, j): |a_ij| / |a_ii| (message weight)
+  const float* wb;  // per stored entry (i, j): |a_ij| / |a_jj| (its transpose's weight)
 };
+
+// The message weights of every stored entry, computed once per pass (the
+// same FP64 quotient rounded to FP32 that the layers used to form inline).
+__global__ void k_edge_weights(int nSlices, const int4* __restrict__ meta, const int* __restrict__ cols,
+                               const double* __restrict__ vals, const double* __restrict__ diag, float* wf,
+                               float* wb) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int s = t >> 5, lane = t & 31;
+  if (s >= nSlices) return;
+  const int4 m = meta[s];
+  if (lane >= m.y) return;
+  const double di = fabs(diag[m.x + lane]);
+  for (int k = 0; k < m.w; k++) {
+    const int e = m.z + (k << 5) + lane;
+    const double a = fabs(vals[e]);
+    wf[e] = (float)(a / di);
+    wb[e] = (float)(a / fabs(diag[cols[e]]));
+  }
+}
+
+// sum_k w[e_k] X[j_k][lane] over the entries e_k = base + 32 k (k < width)
+// of one row, in stored order, with the loads of four entries in flight
+__device__ __forceinline__ float gather_row(const int* __restrict__ cols, const float* __restrict__ w, int base,
+                                            int width, const float* __restrict__ X, int lane, float acc) {
+  int k = 0;
+  for (; k + 4 <= width; k += 4) {
+    int j[4];
+    float wk[4], x[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      j[q] = cols[base + ((k + q) << 5)];
+      wk[q] = w[base + ((k + q) << 5)];
+    }
+#pragma unroll
+    for (int q = 0; q < 4; q++) x[q] = X[(size_t)j[q] * 32 + lane];
+#pragma unroll
+    for (int q = 0; q < 4; q++) acc = __fmaf_rn(wk[q], x[q], acc);
+  }
+  for (; k < width; k++) {
+    const int e = base + (k << 5);
+    acc = __fmaf_rn(w[e], X[(size_t)cols[e] * 32 + lane], acc);
+  }
+  return acc;
+}
 
 // h_out = relu(Ws h + Wm m + b), m_i = sum_j w_ij h_j
 __global__ void __launch_bounds__(kBlock) k_layer(int n, GraphArgs g, const float* __restrict__ P,
@@ -108,15 +154,7 @@ __global__ void __launch_bounds__(kBlock) k_layer(int n, GraphArgs g, const floa
   const int nw = (gridDim.x * blockDim.x) >> 5;
   for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += nw) {
     const int4 m = g.meta[g.rowSlice[i]];
-    const int base = m.z + (i - m.x);
-    const double di = fabs(g.diag[i]);
-    float msg = 0.f;
-    for (int k = 0; k < m.w; k++) {
-      const int e = base + (k << 5);
-      const int j = g.cols[e];
-      const float w = (float)(fabs(g.vals[e]) / di);
-      msg = __fmaf_rn(w, Hin[(size_t)j * 32 + lane], msg);
-    }
+    const float msg = gather_row(g.cols, g.wf, m.z + (i - m.x), m.w, Hin, lane, 0.f);
     const float h = Hin[(size_t)i * 32 + lane];
     float z = sb[lane];
 #pragma unroll
@@ -185,15 +223,8 @@ __global__ void __launch_bounds__(kTcThreads, 4) k_layer_tc(int n, GraphArgs g, 
       float h = 0.f, msg = 0.f;
       if (i < n) {
         const int4 m = g.meta[g.rowSlice[i]];
-        const int base = m.z + (i - m.x);
-        const double di = fabs(g.diag[i]);
-        for (int k = 0; k < m.w; k++) {
-          const int e = base + (k << 5);
-          const int j = g.cols[e];
-          const float w = (float)(fabs(g.vals[e]) / di);
-          msg = __fmaf_rn(w, Hin[(size_t)j * 32 + lane], msg);
-        }
         h = Hin[(size_t)i * 32 + lane];
+        msg = gather_row(g.cols, g.wf, m.z + (i - m.x), m.w, Hin, lane, 0.f);
         if (Mout) Mout[(size_t)i * 32 + lane] = msg;
       }
       sA[kmajor(r, lane, 64)] = h;
@@ -356,14 +387,7 @@ __global__ void __launch_bounds__(kBlock) k_layer_bwd_b(int n, GraphArgs g, cons
   const int nw = (gridDim.x * blockDim.x) >> 5;
   for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += nw) {
     const int4 m = g.meta[g.rowSlice[i]];
-    const int base = m.z + (i - m.x);
-    float acc = dS[(size_t)i * 32 + lane];
-    for (int k = 0; k < m.w; k++) {
-      const int e = base + (k << 5);
-      const int j = g.cols[e];
-      const float w = (float)(fabs(g.vals[e]) / fabs(g.diag[j]));
-      acc = __fmaf_rn(w, dM[(size_t)j * 32 + lane], acc);
-    }
+    const float acc = gather_row(g.cols, g.wb, m.z + (i - m.x), m.w, dM, lane, dS[(size_t)i * 32 + lane]);
     dHin[(size_t)i * 32 + lane] = acc;
   }
 }
@@ -541,7 +565,9 @@ __global__ void k_adam(float* P, const float* __restrict__ g, float* m, float* v
   P[p] -= lr * (mp / c1) / (sqrtf(vp / c2) + eps);
 }
 
-GraphArgs args(const Graph& g) { return {g.a.cols, g.a.vals, g.a.diag, g.a.meta, g.rowSlice}; }
+GraphArgs args(const Graph& g, const Workspace& w) {
+  return {g.a.cols, g.a.vals, g.a.diag, g.a.meta, g.rowSlice, w.wf, w.wb};
+}
 
 void check(cudaError_t e, const char* what) {
   if (e != cudaSuccess) throw Error(kDeviceError, std::string(what) + ": " + cudaGetErrorString(e));
@@ -562,7 +588,11 @@ void run_forward(const Graph& g, const float* P, const double* r, Workspace& w, 
   dev::sum_partials(kReduceBlocks, w.partials, scal + 1, st);
   k_input<<<ceil_div(n, kBlock), kBlock, 0, st>>>(n, r, g.a.diag, scal + 1, w.u, scal);
   k_encode<<<ceil_div((long long)n * 32, kBlock), kBlock, 0, st>>>(n, w.u, P, w.H[0]);
-  const GraphArgs ga = args(g);
+  FVM_REQUIRE(g.entries > 0 && g.entries <= w.wcap, kBadArgument,
+              "learned correction: workspace not prepared for this graph's entries");
+  k_edge_weights<<<ceil_div((long long)g.nSlices * 32, kBlock), kBlock, 0, st>>>(g.nSlices, g.a.meta, g.a.cols,
+                                                                               g.a.vals, g.a.diag, w.wf, w.wb);
+  const GraphArgs ga = args(g, w);
   for (int l = 0; l < kLayers; l++) {
     const float* Pl = P + kLayer0 + l * kLayerSize;
     float* Ml = keepMessages ? w.M[l] : nullptr;
@@ -575,26 +605,34 @@ void run_forward(const Graph& g, const float* P, const double* r, Workspace& w, 
 
 }  // namespace
 
-void Workspace::allocate(int n_, bool training) {
-  if (n_ <= cap && (!training || M[0])) {
-    n = n_;
-    return;
+void Workspace::allocate(int n_, bool training, long long entries) {
+  if (!(n_ <= cap && (!training || M[0]))) {
+    release();
+    n = cap = n_;
+    const size_t hb = sizeof(float) * (size_t)n * 32;
+    check(cudaMalloc(&u, sizeof(float) * (size_t)n), "cudaMalloc");
+    for (int l = 0; l <= kLayers; l++) check(cudaMalloc(&H[l], hb), "cudaMalloc");
+    check(cudaMalloc(&partials, sizeof(double) * (kReduceBlocks + 8)), "cudaMalloc");
+    check(cudaMalloc(&status, sizeof(int)), "cudaMalloc");
+    check(cudaMemset(status, 0, sizeof(int)), "cudaMemset");
+    if (training) {
+      for (int l = 0; l < kLayers; l++) check(cudaMalloc(&M[l], hb), "cudaMalloc");
+      check(cudaMalloc(&dA, hb), "cudaMalloc");
+      check(cudaMalloc(&dB, hb), "cudaMalloc");
+      check(cudaMalloc(&dS, hb), "cudaMalloc");
+      gradBlocks = kGradBlocks;
+      check(cudaMalloc(&gradPartials, sizeof(float) * (size_t)kGradBlocks * kParams), "cudaMalloc");
+    }
   }
-  release();
-  n = cap = n_;
-  const size_t hb = sizeof(float) * (size_t)n * 32;
-  check(cudaMalloc(&u, sizeof(float) * (size_t)n), "cudaMalloc");
-  for (int l = 0; l <= kLayers; l++) check(cudaMalloc(&H[l], hb), "cudaMalloc");
-  check(cudaMalloc(&partials, sizeof(double) * (kReduceBlocks + 8)), "cudaMalloc");
-  check(cudaMalloc(&status, sizeof(int)), "cudaMalloc");
-  check(cudaMemset(status, 0, sizeof(int)), "cudaMemset");
-  if (training) {
-    for (int l = 0; l < kLayers; l++) check(cudaMalloc(&M[l], hb), "cudaMalloc");
-    check(cudaMalloc(&dA, hb), "cudaMalloc");
-    check(cudaMalloc(&dB, hb), "cudaMalloc");
-    check(cudaMalloc(&dS, hb), "cudaMalloc");
-    gradBlocks = kGradBlocks;
-    check(cudaMalloc(&gradPartials, sizeof(float) * (size_t)kGradBlocks * kParams), "cudaMalloc");
+  n = n_;
+  if (entries > wcap) {
+    cudaFree(wf);
+    cudaFree(wb);
+    wf = wb = nullptr;
+    wcap = 0;
+    check(cudaMalloc(&wf, sizeof(float) * (size_t)entries), "cudaMalloc");
+    check(cudaMalloc(&wb, sizeof(float) * (size_t)entries), "cudaMalloc");
+    wcap = entries;
   }
 }
 
@@ -608,6 +646,10 @@ void Workspace::release() {
   cudaFree(partials);
   cudaFree(gradPartials);
   cudaFree(status);
+  cudaFree(wf);
+  cudaFree(wb);
+  wf = wb = nullptr;
+  wcap = 0;
   u = dA = dB = dS = gradPartials = nullptr;
   partials = nullptr;
   status = nullptr;
@@ -641,7 +683,7 @@ void forward_backward(const Graph& g, const float* P, const double* r, const dou
   k_decode_bwd<<<kGradBlocks, kBlock, 0, st>>>(n, P, w.H[kLayers], scal, e, scal + 2, w.dA, w.gradPartials,
                                                w.partials);
   dev::sum_partials(kGradBlocks, w.partials, loss, st);
-  const GraphArgs ga = args(g);
+  const GraphArgs ga = args(g, w);
   const size_t smem = sizeof(float) * kWarps * kLayerSize;
   check(cudaFuncSetAttribute(k_layer_bwd_a, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
         "k_layer_bwd_a shared memory");
@@ -821,6 +863,7 @@ int LearnedCorrection::addInstance(const nn::Graph& g, int nEntries, cudaStream_
   nn::check(cudaMemcpyAsync(meta, g.a.meta, bMeta, cudaMemcpyDeviceToDevice, st), "cudaMemcpy");
   nn::check(cudaMemcpyAsync(rs, g.rowSlice, bRs, cudaMemcpyDeviceToDevice, st), "cudaMemcpy");
   k.g = g;
+  k.g.entries = nEntries;
   k.g.a.cols = cols;
   k.g.a.vals = vals;
   k.g.a.diag = diag;
@@ -860,7 +903,7 @@ void LearnedCorrection::train(int steps, float lr, uint64_t seed, double* losses
     maxN = std::max(maxN, inst_[k].n);
     for (int q = 0; q < (int)inst_[k].pairs.size(); q++) index.push_back({k, q});
   }
-  trainWs_.allocate(maxN, true);
+  trainWs_.allocate(maxN, true, maxEntries());
   trainWs_.tensorCores = tensorCores_;
   double* dLoss = nullptr;
   nn::check(cudaMalloc(&dLoss, sizeof(double) * (size_t)std::max(steps, 1)), "cudaMalloc");
@@ -874,7 +917,7 @@ void LearnedCorrection::train(int steps, float lr, uint64_t seed, double* losses
   for (int t = 0; t < steps; t++) {
     const auto& ix = index[next() % index.size()];
     Instance& in = inst_[ix.first];
-    trainWs_.allocate(in.n, true);
+    trainWs_.allocate(in.n, true, in.g.entries);
     nn::forward_backward(in.g, dParams_, in.pairs[ix.second].first, in.pairs[ix.second].second, dGrad_,
                          dLoss + t, trainWs_, dScal_, st);
     nn::adam_step(dParams_, dGrad_, dM_, dV_, lr, ++adamT_, st);
@@ -891,14 +934,14 @@ double LearnedCorrection::evaluate(cudaStream_t st) {
   FVM_REQUIRE(np > 0, kBadArgument, "learned correction: no pairs to evaluate");
   int maxN = 0;
   for (const Instance& k : inst_) maxN = std::max(maxN, k.n);
-  trainWs_.allocate(maxN, true);
+  trainWs_.allocate(maxN, true, maxEntries());
   trainWs_.tensorCores = tensorCores_;
   double* dLoss = nullptr;
   nn::check(cudaMalloc(&dLoss, sizeof(double) * (size_t)np), "cudaMalloc");
   int q = 0;
   for (Instance& in : inst_)
     for (auto& pr : in.pairs) {
-      trainWs_.allocate(in.n, true);
+      trainWs_.allocate(in.n, true, in.g.entries);
       nn::forward_backward(in.g, dParams_, pr.first, pr.second, dGrad_, dLoss + q++, trainWs_, dScal_, st);
     }
   std::vector<double> l(np);
@@ -911,8 +954,14 @@ double LearnedCorrection::evaluate(cudaStream_t st) {
   return s / np;
 }
 
-void LearnedCorrection::prepare(int n) {
-  applyWs_.allocate(n, false);
+long long LearnedCorrection::maxEntries() const {
+  long long e = 0;
+  for (const Instance& k : inst_) e = std::max(e, k.g.entries);
+  return e;
+}
+
+void LearnedCorrection::prepare(int n, long long entries) {
+  applyWs_.allocate(n, false, entries);
   applyWs_.tensorCores = tensorCores_;
 }
 
@@ -922,7 +971,8 @@ void LearnedCorrection::setTensorCores(bool on) {
 }
 
 void LearnedCorrection::apply(const nn::Graph& g, const double* r, double* out, double* scal, cudaStream_t st) {
-  FVM_REQUIRE(g.a.n <= applyWs_.cap, kBadArgument, "learned correction: prepare() was not called for this size");
+  FVM_REQUIRE(g.a.n <= applyWs_.cap && g.entries <= applyWs_.wcap, kBadArgument,
+              "learned correction: prepare() was not called for this size");
   applyWs_.n = g.a.n;
   nn::forward(g, dParams_, r, out, applyWs_, scal, st);
 }

@@ -43,6 +43,7 @@ struct Graph {
   dev::SellView<double> a;
   const int* rowSlice = nullptr;
   int nSlices = 0;
+  long long entries = 0;  // stored entries (cols / vals length)
 };
 
 // Device workspace for one graph size.
@@ -60,7 +61,10 @@ struct Workspace {
   int gradBlocks = 0;
   int* status = nullptr;         // device flag: 1 if a tensor-core completion wait ran out
   bool tensorCores = true;       // dense layers on tcgen05 (TF32 inputs) instead of FP32 CUDA cores
-  void allocate(int n, bool training);
+  float* wf = nullptr;           // per-entry message weights (forward / transpose)
+  float* wb = nullptr;
+  long long wcap = 0;            // entries the weight buffers hold
+  void allocate(int n, bool training, long long entries);
   void release();
   // throws (and clears the flag) if a tensor-core wait ran out; synchronises
   void checkStatus();
@@ -129,8 +133,10 @@ class LearnedCorrection {
 
   // correction for residual r on graph g (call prepare(n) first: apply
   // allocates nothing, so it can run inside a captured graph)
-  void prepare(int n);
+  void prepare(int n, long long entries);
   void apply(const nn::Graph& g, const double* r, double* out, double* scal, cudaStream_t st);
+  // largest entry count of the training instances' graphs
+  long long maxEntries() const;
   // throws if a tensor-core kernel of apply() gave up waiting (synchronises)
   void checkApplyStatus() { applyWs_.checkStatus(); }
 

@@ -898,7 +898,7 @@ void LinearSolve::setLearned(LearnedCorrection* lc) {
   learned_ = lc;
   learnedActive_ = true;
   lsTries_ = lsKept_ = 0;
-  if (lc) lc->prepare(n_);
+  if (lc) lc->prepare(n_, (long long)h_.level(0).entries);
 }
 
 // Flexible learned step after an AMG refinement iteration: d = N(r),
@@ -910,7 +910,7 @@ void LinearSolve::learnedStep(cudaStream_t st, double* x, double* r) {
   double* D = work_ + 6 * (size_t)n_;
   double* Q = work_ + 7 * (size_t)n_;
   double* RT = work_ + 8 * (size_t)n_;
-  const nn::Graph g{d.view64(), d.rowSlice, d.nSlices};
+  const nn::Graph g{d.view64(), d.rowSlice, d.nSlices, (long long)d.entries};
   learned_->apply(g, r, D, scal_ + kLsScale, st);
   dev::spmv(d.view64(), d.nSlices, D, Q, st);
   dot_into(r, Q, scal_ + kLsRq, st);

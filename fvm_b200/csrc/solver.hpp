@@ -248,8 +248,9 @@ class LinearSolve {
   LearnedCorrection* learned_ = nullptr;
   // the learned step stays on while it pays: after kLsProbe tries it is
   // retired if fewer than a quarter cut the FP64 L1 residual below
-  // kLsUsefulFactor times its value (the step costs several V-cycles)
-  static constexpr int kLsProbe = 8;
+  // kLsUsefulFactor times its value (the step costs about two V-cycles of
+  // the mixed solve: three layers over the finest graph, an SpMV, two dots)
+  static constexpr int kLsProbe = 3;
   static constexpr double kLsUsefulFactor = 0.5;
   bool learnedActive_ = true;
   int lsTries_ = 0, lsKept_ = 0;

@@ -585,7 +585,7 @@ int ThermalModel::harvest(LearnedCorrection& lc, int nOuter, int perSolve, doubl
   HostMesh& m = *mesh_;
   const int n = m.nCells;
   DevLevel& d0 = hier_.level(0);
-  const nn::Graph g{d0.view64(), d0.rowSlice, d0.nSlices};
+  const nn::Graph g{d0.view64(), d0.rowSlice, d0.nSlices, (long long)d0.entries};
   const int inst = lc.addInstance(g, (int)d0.entries, stream_);
   std::vector<double*> rs(perSolve), xs(perSolve);
   double* e = nullptr;

@@ -391,13 +391,30 @@ def bench_batch(args, dist, peaks, peak_kind):
         dist.barrier()
         first, last, at = bt.status()
         n_all = bt.mesh.getCells().getCount()
-        results[variant] = {"dev": dist.max(statistics.median(dev_t)), "wall": dist.max(statistics.median(wall_t)),
+        prof = bt.model.profile(args.profile_reps)
+        plans = bt.model.getLaunchPlans()
+        results[variant] = {"profile": prof, "plans": plans,
+                            "dev": dist.max(statistics.median(dev_t)), "wall": dist.max(statistics.median(wall_t)),
                             "outer": rep.iterations, "cycles": rep.linearIterations, "setup": rep.setupSeconds,
                             "all_converged": bool(np.all(at >= 0)), "max_ratio": float(np.max(last / first)),
                             "T": np.concatenate(Ts), "launches": rep.launches, "clocks": sampler.summary(),
                             "h2d": 8 * 3 * n_all, "d2h": 8 * n_all}
         del bt
     plain, mixed = results["plain"], results["mixed"]
+    peak = float(peaks.get("hbm_gbs", PEAKS_FALLBACK["hbm_gbs"]))
+    pm, pp = mixed["profile"], plain["profile"]
+
+    def gbs(b, ms):
+        return b / (ms * 1e-3) / 1e9
+
+    roofline = {"bound": "hbm", "achieved": gbs(pm["gs_pass_bytes"], pm["gs_pass_ms"]), "peak": peak,
+                "unit": "GB/s", "frac": gbs(pm["gs_pass_bytes"], pm["gs_pass_ms"]) / peak, "traffic": None,
+                "kernel": "k_gs_color_ell<float> (one pass over all colours of the batch's finest level)",
+                "peak_kind": peak_kind,
+                "fp64_gs_pass": {"achieved": gbs(pp["gs_pass_bytes"], pp["gs_pass_ms"]),
+                                 "frac": gbs(pp["gs_pass_bytes"], pp["gs_pass_ms"]) / peak},
+                "fp64_residual": {"achieved": gbs(pp["residual_bytes"], pp["residual_ms"]),
+                                  "frac": gbs(pp["residual_bytes"], pp["residual_ms"]) / peak}}
     cpu = None
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
         cpu = cpu_reference_batch(ms, args.inner_rel)
@@ -417,6 +434,9 @@ def bench_batch(args, dist, peaks, peak_kind):
                            "all_meshes_converged": v["all_converged"], "max_mesh_ratio": v["max_ratio"]}
                        for k, v in results.items()},
             "gpu_launches": int(mixed["launches"]) * args.steps,
+            "launch_plans": {v: ["%d/%d" % p if p[1] else "ell%d" % -p[0] for p in r["plans"]]
+                             for v, r in results.items()},
+            "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": {"value": mixed["wall"], "unit": "s", "h2d_bytes_per_step": mixed["h2d"],
                     "d2h_bytes_per_step": mixed["d2h"]},
@@ -560,6 +580,7 @@ def main():
             sampler.__exit__()
         dist.barrier()
         prof = solve.tm.profile(args.profile_reps)
+        plans = solve.tm.getLaunchPlans()
         results[variant] = {
             "dev": dist.max(statistics.median(dev_t)),
             "wall": dist.max(statistics.median(wall_t)),
@@ -572,6 +593,7 @@ def main():
             "setup": reps[-1].setupSeconds,
             "T": T_last[:n_cells],
             "profile": prof,
+            "plans": plans,
             "clocks": sampler.summary() if sampler else None,
             "h2d": h2d,
             "d2h": d2h,
@@ -663,6 +685,8 @@ def main():
             "learned_training": learned_info,
             "levels": int(pm["levels"]),
             "kernels_per_cycle": int(pm["kernels_per_cycle"]),
+            "launch_plans": {v: ["%d/%d" % p if p[1] else "ell%d" % -p[0] for p in r["plans"]]
+                             for v, r in results.items()},
             "kernel_timings": {
                 v: {"gs_pass_ms": r["profile"]["gs_pass_ms"],
                     "gs_pass_gbs": r["profile"]["gs_pass_bytes"] / (r["profile"]["gs_pass_ms"] * 1e-3) / 1e9,

@@ -41,6 +41,9 @@ class LinearOptions(ctypes.Structure):
         ("coarseJacobiRows", ctypes.c_int),
         ("jacobiWeight", ctypes.c_double),
         ("preconditioner", ctypes.c_int),
+        ("autotune", ctypes.c_int),
+        ("planThreadsPerRow", ctypes.c_int),
+        ("planBlock", ctypes.c_int),
     ]
 
 
@@ -105,6 +108,7 @@ _SIGS = {
     "fvm_thermal_heat_flux_integral": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, c_double_p]),
     "fvm_thermal_history": (ctypes.c_int, [ctypes.c_void_p, c_double_p, ctypes.c_int, c_int_p]),
     "fvm_thermal_linear_system": (ctypes.c_int, [ctypes.c_void_p, c_double_p, c_double_p, c_double_p, c_int_p]),
+    "fvm_thermal_launch_plans": (ctypes.c_int, [ctypes.c_void_p, c_int_p, c_int_p, c_int_p, ctypes.c_int]),
     "fvm_thermal_hierarchy": (ctypes.c_int, [ctypes.c_void_p, c_int_p, c_int_p, ctypes.c_int, c_int_p,
                                              ctypes.c_int]),
     "fvm_thermal_profile": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, c_double_p]),

@@ -91,6 +91,14 @@ SolverOptions to_solver(const fvm_linear_options& o) {
   s.coarseJacobiRows = o.coarseJacobiRows;
   s.jacobiWeight = o.jacobiWeight;
   s.preconditioner = o.preconditioner == 1 ? kPrecJacobi : kPrecAMG;
+  FVM_REQUIRE(o.planThreadsPerRow == 0 || o.planThreadsPerRow == 1 || o.planThreadsPerRow == 2 ||
+                  o.planThreadsPerRow == 4,
+              kBadArgument, "planThreadsPerRow must be 0, 1, 2 or 4");
+  FVM_REQUIRE(o.planBlock == 0 || o.planBlock == 128 || o.planBlock == 256, kBadArgument,
+              "planBlock must be 0, 128 or 256");
+  s.autotune = o.autotune != 0;
+  s.planTpr = o.planThreadsPerRow;
+  s.planBlock = o.planBlock;
   return s;
 }
 
@@ -116,6 +124,9 @@ void from_solver(const SolverOptions& s, fvm_linear_options& o) {
   o.coarseJacobiRows = s.coarseJacobiRows;
   o.jacobiWeight = s.jacobiWeight;
   o.preconditioner = s.preconditioner;
+  o.autotune = s.autotune ? 1 : 0;
+  o.planThreadsPerRow = s.planTpr;
+  o.planBlock = s.planBlock;
 }
 
 RefLevel level_from_csr(int n, const int* row, const int* col, const double* diag, const double* off) {
@@ -411,6 +422,19 @@ int fvm_thermal_hierarchy(fvm_thermal* h, int* nLevels, int* sizes, int sizesCap
     FVM_REQUIRE(h, kBadArgument, "null model");
     const AmgHierarchy& hier = h->model->hierarchy();
     export_hierarchy(hier.refLevels(), nLevels, sizes, sizesCap, coarseIndex, ciCap);
+  });
+}
+
+int fvm_thermal_launch_plans(fvm_thermal* h, int* nLevels, int* threadsPerRow, int* block, int cap) {
+  return guarded([&] {
+    FVM_REQUIRE(h && nLevels, kBadArgument, "null argument");
+    const AmgHierarchy& hier = h->model->hierarchy();
+    *nLevels = hier.numLevels();
+    for (int l = 0; l < hier.numLevels() && l < cap; l++) {
+      const DevLevel& d = hier.level(l);
+      if (threadsPerRow) threadsPerRow[l] = d.ellWidth ? -d.ellWidth : d.plan.tpr;
+      if (block) block[l] = d.ellWidth ? 0 : d.plan.block;
+    }
   });
 }
 

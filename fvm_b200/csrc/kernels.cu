@@ -314,6 +314,94 @@ __global__ void __launch_bounds__(kBlock, 8) k_spmv_ell(SellView<double> a, cons
   y[i] = ell_row<double, W>(a, i, x, a.diag[i] * x[i]);
 }
 
+// ---- SELL-32 smoothers with several threads per row (autotuned plans) ---------
+// A warp covers 32 / TPR rows of one slice; thread `sub` of a row's group
+// takes the entries k = sub, sub + TPR, ... Four entries per thread are in
+// flight per step; the group's products are then added to the row sum in
+// stored order (k ascending), one shuffle per product, so the sum rounds
+// exactly as row_sum's does.
+template <class T, int TPR>
+__device__ __forceinline__ T row_sum_tpr(const SellView<T>& a, const int4 m, int l, const T* __restrict__ x,
+                                         T sum) {
+  constexpr int C = 4;
+  const int lane = threadIdx.x & 31, sub = lane & (TPR - 1), g0 = lane & ~(TPR - 1);
+  const int o = m.z + l, w = m.w;
+  for (int k0 = 0; k0 < w; k0 += TPR * C) {
+    int c[C];
+    T v[C], p[C];
+#pragma unroll
+    for (int q = 0; q < C; q++) {
+      const int k = k0 + q * TPR + sub;
+      c[q] = k < w ? a.cols[o + (k << 5)] : 0;
+      v[q] = k < w ? a.vals[o + (k << 5)] : T(0);
+    }
+#pragma unroll
+    for (int q = 0; q < C; q++) p[q] = v[q] * x[c[q]];
+#pragma unroll
+    for (int q = 0; q < C; q++)
+#pragma unroll
+      for (int s2 = 0; s2 < TPR; s2++) {
+        const T pv = __shfl_sync(0xffffffffu, p[q], g0 + s2);
+        if (k0 + q * TPR + s2 < w) sum = sum + pv;
+      }
+  }
+  return sum;
+}
+
+// global warp gw -> (slice, row within the slice) for TPR threads per row
+template <int TPR>
+__device__ __forceinline__ void tpr_row(int gw, int& sliceOffset, int& l) {
+  sliceOffset = gw / TPR;
+  l = (gw % TPR) * (32 / TPR) + ((threadIdx.x & 31) / TPR);
+}
+
+template <class T, int TPR, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_gs_color_tpr(SellView<T> a, int s0, int s1, T* x,
+                                                        const T* __restrict__ b) {
+  FVM_PDL();
+  int so, l;
+  tpr_row<TPR>(blockIdx.x * (BLOCK / 32) + (threadIdx.x >> 5), so, l);
+  const int s = s0 + so;
+  if (s >= s1) return;  // whole warp
+  const int4 m = a.meta[s];
+  const bool live = l < m.y;
+  const int i = m.x + (live ? l : 0);
+  const T sum = row_sum_tpr<T, TPR>(a, m, l, x, live ? b[i] : T(0));
+  if (live && (threadIdx.x & (TPR - 1)) == 0) x[i] = -sum / a.diag[i];
+}
+
+template <class T, int TPR, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_jacobi_damped_tpr(SellView<T> a, int nSlices, const T* __restrict__ xold,
+                                                             T* xnew, const T* __restrict__ b, T w) {
+  FVM_PDL();
+  int s, l;
+  tpr_row<TPR>(blockIdx.x * (BLOCK / 32) + (threadIdx.x >> 5), s, l);
+  if (s >= nSlices) return;  // whole warp
+  const int4 m = a.meta[s];
+  const bool live = l < m.y;
+  const int i = m.x + (live ? l : 0);
+  const T sum = row_sum_tpr<T, TPR>(a, m, l, xold, live ? b[i] : T(0));
+  if (live && (threadIdx.x & (TPR - 1)) == 0) {
+    const T xo = xold[i];
+    xnew[i] = xo + w * (-sum / a.diag[i] - xo);
+  }
+}
+
+// Calls LAUNCH(TPR, BLOCK) for a supported plan; false otherwise.
+#define FVM_PLAN_SWITCH(plan, LAUNCH)                              \
+  [&]() -> bool {                                                  \
+    const int key_ = (plan).tpr * 1000 + (plan).block;             \
+    switch (key_) {                                                \
+      case 1128: LAUNCH(1, 128); return true;                      \
+      case 1256: LAUNCH(1, 256); return true;                      \
+      case 2128: LAUNCH(2, 128); return true;                      \
+      case 2256: LAUNCH(2, 256); return true;                      \
+      case 4128: LAUNCH(4, 128); return true;                      \
+      case 4256: LAUNCH(4, 256); return true;                      \
+      default: return false;                                       \
+    }                                                              \
+  }()
+
 // Calls LAUNCH(W) with the compile-time width of an ELL level (1..8);
 // false for wider levels (they take the generic kernels).
 #define FVM_ELL_SWITCH(width, LAUNCH) \
@@ -877,7 +965,7 @@ void pdl_launch(void (*kernel)(KArgs...), dim3 grid, dim3 block, cudaStream_t st
 }
 }  // namespace
 template <class T>
-void gs_color(const SellView<T>& a, int s0, int s1, T* x, const T* b, cudaStream_t st) {
+void gs_color(const SellView<T>& a, int s0, int s1, T* x, const T* b, cudaStream_t st, RowPlan plan) {
   if (s1 <= s0) return;
   // ELL-32: s0, s1 are rows; the launch covers the 32-row groups they touch
   const int groups = a.ellWidth ? ((s1 - 1) >> 5) - (s0 >> 5) + 1 : s1 - s0;
@@ -885,6 +973,12 @@ void gs_color(const SellView<T>& a, int s0, int s1, T* x, const T* b, cudaStream
 #define FVM_L(W) pdl_launch(k_gs_color_ell<T, W>, g, kBlock, st, a, s0, s1, x, b)
   if (a.ellWidth && FVM_ELL_SWITCH(a.ellWidth, FVM_L)) return;
 #undef FVM_L
+  if (!a.ellWidth && !plan.isDefault()) {
+#define FVM_P(TPR, BLOCK) \
+  pdl_launch(k_gs_color_tpr<T, TPR, BLOCK>, ceil_div((long long)groups * TPR, BLOCK / 32), BLOCK, st, a, s0, s1, x, b)
+    if (FVM_PLAN_SWITCH(plan, FVM_P)) return;
+#undef FVM_P
+  }
   pdl_launch(k_gs_color<T>, g, kBlock, st, a, s0, s1, x, b);
 }
 template <class T>
@@ -899,10 +993,18 @@ void jacobi(const SellView<T>& a, int nSlices, const T* xold, T* xnew, const T* 
   pdl_launch(k_jacobi<T>, reduce_blocks(nSlices), kBlock, st, a, nSlices, xold, xnew, b);
 }
 template <class T>
-void jacobi_damped(const SellView<T>& a, int nSlices, const T* xold, T* xnew, const T* b, T w, cudaStream_t st) {
+void jacobi_damped(const SellView<T>& a, int nSlices, const T* xold, T* xnew, const T* b, T w, cudaStream_t st,
+                   RowPlan plan) {
 #define FVM_L(W) pdl_launch(k_jacobi_damped_ell<T, W>, ceil_div(a.n, kBlock), kBlock, st, a, xold, xnew, b, w)
   if (a.ellWidth && FVM_ELL_SWITCH(a.ellWidth, FVM_L)) return;
 #undef FVM_L
+  if (!a.ellWidth && !plan.isDefault()) {
+#define FVM_P(TPR, BLOCK)                                                                                          \
+  pdl_launch(k_jacobi_damped_tpr<T, TPR, BLOCK>, ceil_div((long long)nSlices * TPR, BLOCK / 32), BLOCK, st, a, nSlices, \
+             xold, xnew, b, w)
+    if (FVM_PLAN_SWITCH(plan, FVM_P)) return;
+#undef FVM_P
+  }
   pdl_launch(k_jacobi_damped<T>, reduce_blocks(nSlices), kBlock, st, a, nSlices, xold, xnew, b, w);
 }
 template <class T>
@@ -1117,10 +1219,10 @@ void update_solution(int nCells, const int* perm, const double* delta, const Bou
 
 // explicit instantiations
 #define FVM_INST(T)                                                                              \
-  template void gs_color<T>(const SellView<T>&, int, int, T*, const T*, cudaStream_t);           \
+  template void gs_color<T>(const SellView<T>&, int, int, T*, const T*, cudaStream_t, RowPlan);  \
   template void gs_sequential<T>(const SellView<T>&, T*, const T*, bool, cudaStream_t);          \
   template void jacobi<T>(const SellView<T>&, int, const T*, T*, const T*, cudaStream_t);        \
-  template void jacobi_damped<T>(const SellView<T>&, int, const T*, T*, const T*, T, cudaStream_t); \
+  template void jacobi_damped<T>(const SellView<T>&, int, const T*, T*, const T*, T, cudaStream_t, RowPlan); \
   template void residual<T>(const SellView<T>&, int, const T*, const T*, T*, double*, cudaStream_t); \
   template void restrict_sum<T>(int, const int*, const int*, const T*, T*, cudaStream_t);        \
   template void residual_restrict<T>(const SellView<T>&, const int*, int, const int*, const int*,   \

@@ -31,8 +31,19 @@ struct SellView {
 // One Gauss-Seidel pass over the rows of slices [s0, s1) (one colour block;
 // on an ELL-32 level s0, s1 are the colour's first and end ROWS):
 // x_i = -(b_i + sum_j a_ij x_j) / a_ii
+// Launch plan of the SELL-32 smoother kernels, picked per level by the
+// autotuner: threads per row (1, 2 or 4: the entries of a row are split
+// round-robin over the threads, their products are formed in parallel and
+// summed in stored order, so every plan gives bitwise the same result) and
+// threads per block (128 or 256). ELL-32 levels ignore it.
+struct RowPlan {
+  int tpr = 1;
+  int block = 256;
+  bool isDefault() const { return tpr == 1 && block == 256; }
+};
+
 template <class T>
-void gs_color(const SellView<T>& a, int s0, int s1, T* x, const T* b, cudaStream_t st);
+void gs_color(const SellView<T>& a, int s0, int s1, T* x, const T* b, cudaStream_t st, RowPlan plan = RowPlan());
 // Lexicographic Gauss-Seidel by a single thread in row order (reverse when
 // asked): the reference's CRMatrix::forwardGS / reverseGS, for parity runs.
 template <class T>
@@ -42,7 +53,8 @@ template <class T>
 void jacobi(const SellView<T>& a, int nSlices, const T* xold, T* xnew, const T* b, cudaStream_t st);
 // damped Jacobi: xnew = xold + w (Jacobi update - xold)
 template <class T>
-void jacobi_damped(const SellView<T>& a, int nSlices, const T* xold, T* xnew, const T* b, T w, cudaStream_t st);
+void jacobi_damped(const SellView<T>& a, int nSlices, const T* xold, T* xnew, const T* b, T w, cudaStream_t st,
+                   RowPlan plan = RowPlan());
 
 // ---- residual / products ---------------------------------------------------
 // r = b + D x + O x over all rows; when partials != null each block also

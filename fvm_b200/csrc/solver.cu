@@ -11,6 +11,9 @@
 #include <thread>
 #include <limits>
 #include <type_traits>
+#include <map>
+#include <mutex>
+#include <tuple>
 
 namespace fvm {
 
@@ -240,12 +243,130 @@ void AmgHierarchy::build(std::vector<RefLevel>& levels, int finestLocalSize, con
     CUDA_OK(cudaDeviceSynchronize());
     lap("coarsest inverse");
   }
+  tunePlans();
+  lap("launch plans");
   buildProgram();
   lap("cycle program");
   if (trace) {
     fprintf(stderr, "[fvm setup] levels:");
     for (int l = 0; l < L; l++) fprintf(stderr, " %d(%dc)", lv_[l].n, lv_[l].nColors);
     fprintf(stderr, "\n");
+  }
+}
+
+// ---- autotuned launch plans --------------------------------------------------
+namespace {
+struct PlanKey {
+  int n;
+  size_t entries;
+  int width, colors;
+  bool f32, damped;
+  bool operator<(const PlanKey& o) const {
+    return std::tie(n, entries, width, colors, f32, damped) <
+           std::tie(o.n, o.entries, o.width, o.colors, o.f32, o.damped);
+  }
+};
+std::mutex gPlanMu;
+std::map<PlanKey, dev::RowPlan> gPlanCache;  // per process: a shape is timed once
+constexpr int kTuneMinRows = 4096;           // smaller levels are launch-bound: default plan
+const dev::RowPlan kCandidatePlans[] = {{1, 256}, {1, 128}, {2, 256}, {2, 128}, {4, 256}, {4, 128}};
+}  // namespace
+
+void AmgHierarchy::smootherPass(int l, dev::RowPlan plan, cudaStream_t st) {
+  DevLevel& d = lv_[l];
+  const bool f32 = opt_.precision == kMixed;
+  const bool damped = dampedLevel(l, d.n);
+  auto pass = [&](auto a, auto* x, auto* t, const auto* b) {
+    using T = std::remove_pointer_t<decltype(x)>;
+    if (damped || opt_.smootherType != kGaussSeidel) {
+      dev::jacobi_damped<T>(a, d.nSlices, x, t, b, (T)opt_.jacobiWeight, st, plan);
+    } else {
+      for (int c = 0; c < d.nColors; c++)
+        dev::gs_color<T>(a, d.colorSliceStart[c], d.colorSliceStart[c + 1], x, b, st, plan);
+    }
+  };
+  if (f32)
+    pass(d.view32(), d.xF, d.tmpF, (const float*)d.bF);
+  else
+    pass(d.view64(), d.x, d.tmp, (const double*)d.b);
+}
+
+// Each SELL-32 level's smoother runs with the fastest of the candidate
+// plans, timed here with CUDA events (one warm-up and five timed passes,
+// median). All plans give bitwise the same result, so the choice changes
+// speed only. Levels of one shape are timed once per process.
+void AmgHierarchy::tunePlans() {
+  const int L = (int)lv_.size();
+  const bool f32 = opt_.precision == kMixed;
+  const bool direct = opt_.coarseSolver == kCoarseDirect && !opt_.finestOnly();
+  cudaStream_t st = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  bool touched = false;
+  for (int l = 0; l < L; l++) {
+    DevLevel& d = lv_[l];
+    d.plan = dev::RowPlan();
+    if (d.ellWidth) continue;
+    if (opt_.planTpr) {
+      d.plan.tpr = opt_.planTpr;
+      d.plan.block = opt_.planBlock ? opt_.planBlock : 256;
+      continue;
+    }
+    if (!opt_.autotune || d.n < kTuneMinRows || (direct && l == L - 1)) continue;
+    if (opt_.smootherType != kGaussSeidel && !dampedLevel(l, d.n)) continue;  // plain Jacobi: not tuned
+    const PlanKey key{d.n, d.entries, d.maxWidth, d.nColors, f32, dampedLevel(l, d.n)};
+    {
+      std::lock_guard<std::mutex> lock(gPlanMu);
+      auto it = gPlanCache.find(key);
+      if (it != gPlanCache.end()) {
+        d.plan = it->second;
+        continue;
+      }
+    }
+    if (!st) {
+      CUDA_OK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+      CUDA_OK(cudaEventCreate(&e0));
+      CUDA_OK(cudaEventCreate(&e1));
+    }
+    touched = true;
+    float best = std::numeric_limits<float>::max();
+    dev::RowPlan bestPlan;
+    for (const dev::RowPlan& p : kCandidatePlans) {
+      smootherPass(l, p, st);  // warm-up
+      std::vector<float> t;
+      for (int r = 0; r < 5; r++) {
+        CUDA_OK(cudaEventRecord(e0, st));
+        smootherPass(l, p, st);
+        CUDA_OK(cudaEventRecord(e1, st));
+        CUDA_OK(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        CUDA_OK(cudaEventElapsedTime(&ms, e0, e1));
+        t.push_back(ms);
+      }
+      std::sort(t.begin(), t.end());
+      if (t[2] < best) {
+        best = t[2];
+        bestPlan = p;
+      }
+    }
+    d.plan = bestPlan;
+    std::lock_guard<std::mutex> lock(gPlanMu);
+    gPlanCache[key] = bestPlan;
+  }
+  if (st) {
+    CUDA_OK(cudaStreamSynchronize(st));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaStreamDestroy(st);
+  }
+  if (touched) {
+    // the timed passes wrote the level vectors: back to the state after upload
+    for (int l = 0; l < L; l++) {
+      DevLevel& d = lv_[l];
+      CUDA_OK(cudaMemset(d.x, 0, sizeof(double) * d.n));
+      CUDA_OK(cudaMemset(d.tmp, 0, sizeof(double) * d.n));
+      if (d.xF) CUDA_OK(cudaMemset(d.xF, 0, sizeof(float) * d.n));
+      if (d.tmpF) CUDA_OK(cudaMemset(d.tmpF, 0, sizeof(float) * d.n));
+    }
   }
 }
 
@@ -517,8 +638,8 @@ void AmgHierarchy::sweeps(int nSweeps, int l, cudaStream_t st) {
       // launch-bound colour passes
       T* t = vec_tmp<T>(d);
       const T w = (T)opt_.jacobiWeight;
-      dev::jacobi_damped<T>(a, d.nSlices, x, t, b, w, st);
-      dev::jacobi_damped<T>(a, d.nSlices, t, x, b, w, st);
+      dev::jacobi_damped<T>(a, d.nSlices, x, t, b, w, st, d.plan);
+      dev::jacobi_damped<T>(a, d.nSlices, t, x, b, w, st, d.plan);
     } else if (opt_.smootherType == kGaussSeidel) {
       if (opt_.ordering == kSequential) {
         dev::gs_sequential<T>(a, x, b, false, st);
@@ -526,10 +647,10 @@ void AmgHierarchy::sweeps(int nSweeps, int l, cudaStream_t st) {
       } else {
         const int C = d.nColors;
         for (int c = 0; c < C; c++)
-          dev::gs_color<T>(a, d.colorSliceStart[c], d.colorSliceStart[c + 1], x, b, st);
+          dev::gs_color<T>(a, d.colorSliceStart[c], d.colorSliceStart[c + 1], x, b, st, d.plan);
         // reverse pass; its first colour would repeat the last update exactly
         for (int c = C - 2; c >= 0; c--)
-          dev::gs_color<T>(a, d.colorSliceStart[c], d.colorSliceStart[c + 1], x, b, st);
+          dev::gs_color<T>(a, d.colorSliceStart[c], d.colorSliceStart[c + 1], x, b, st, d.plan);
       }
     } else {
       T* t = vec_tmp<T>(d);

@@ -55,6 +55,11 @@ struct SolverOptions {
   // preconditioner of CG / BCGStab: one AMG cycle, or two Jacobi sweeps
   // (JacobiSolver::smooth, fvmbase/JacobiSolver.cpp:27-100)
   PreconditionerKind preconditioner = kPrecAMG;
+  // smoother launch plans of the SELL-32 levels: autotuned at setup, or one
+  // plan forced on every level (planTpr != 0)
+  bool autotune = true;
+  int planTpr = 0;
+  int planBlock = 0;
   // only the finest level is needed (Jacobi solver or preconditioner)
   bool finestOnly() const { return solver == kSolverJacobi || preconditioner == kPrecJacobi; }
 };
@@ -84,6 +89,7 @@ struct DevLevel {
   double* partials = nullptr;
   int nPartials = 0;
   int4* meta = nullptr;  // per slice: first row, rows, entry offset, width
+  dev::RowPlan plan;     // launch plan of this level's smoother (SELL-32 levels)
   int ellWidth = 0;  // > 0: ELL-32 layout (colorSliceStart then holds rows)
   dev::SellView<double> view64() const {
     return {n, sliceRow, sliceRows, sliceOff, cols, vals, diag, meta, ellWidth};
@@ -195,6 +201,10 @@ class AmgHierarchy {
   void uploadTransfer(const PackedLevel& p, DevLevel& d, int nCoarse);
   // persistent cycle program
   void buildProgram();
+  // picks each SELL-32 level's smoother launch plan (autotune or forced)
+  void tunePlans();
+  // one smoother pass of level l with a given plan (what the tuner times)
+  void smootherPass(int l, dev::RowPlan plan, cudaStream_t st);
   void genCycle(CycleType t, int l, std::vector<dev::Phase>& out) const;
   void genSweeps(int n, int l, std::vector<dev::Phase>& out) const;
   bool programReady_ = false;

@@ -189,6 +189,11 @@ class AMG(LinearSolver):
         self.useGraphs = bool(d.useGraphs)
         self.coarseJacobiRows = d.coarseJacobiRows
         self.jacobiWeight = d.jacobiWeight
+        # launch plans of the SELL-32 smoother kernels (speed only, never
+        # the result): autotuned at setup, or one plan forced everywhere
+        self.autotune = bool(d.autotune)
+        self.planThreadsPerRow = d.planThreadsPerRow
+        self.planBlock = d.planBlock
         self._printFile = None
 
     def setMergeLevelSize(self, size: int) -> None:
@@ -223,6 +228,9 @@ class AMG(LinearSolver):
         o.useGraphs = int(bool(self.useGraphs))
         o.coarseJacobiRows = int(self.coarseJacobiRows)
         o.jacobiWeight = float(self.jacobiWeight)
+        o.autotune = int(bool(self.autotune))
+        o.planThreadsPerRow = int(self.planThreadsPerRow)
+        o.planBlock = int(self.planBlock)
 
     def options(self) -> _lib.LinearOptions:
         o = _lib.LinearOptions()

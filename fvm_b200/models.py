@@ -295,6 +295,16 @@ class ThermalModelA:
             p += s[lvl]
         return list(sizes[: nl.value]), out
 
+    def getLaunchPlans(self):
+        """[(threadsPerRow, threadsPerBlock)] of each level's smoother kernels
+        as the autotuner chose them; ELL-32 levels: (-width, 0)."""
+        self._push()
+        tpr = np.zeros(64, np.int32)
+        blk = np.zeros(64, np.int32)
+        nl = ctypes.c_int(0)
+        check(_lib.load().fvm_thermal_launch_plans(self._h, ctypes.byref(nl), iptr(tpr), iptr(blk), 64))
+        return [(int(a), int(b)) for a, b in zip(tpr[: nl.value], blk[: nl.value])]
+
     def profile(self, reps: int = 5) -> dict:
         """CUDA-event timings of the finest-level kernels (see fvm_thermal_profile)."""
         self._push()

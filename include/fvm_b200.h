@@ -75,6 +75,10 @@ typedef struct fvm_linear_options {
                                damped Jacobi instead of multicolour Gauss-Seidel (0: never) */
   double jacobiWeight;      /* damping of that Jacobi smoother (default 2/3) */
   int preconditioner;       /* of CG / BCGStab: 0 one AMG cycle, 1 two Jacobi sweeps (JacobiSolver) */
+  int autotune;             /* time the smoother launch plans of each SELL-32 level at setup and keep
+                               the fastest (plans never change results) */
+  int planThreadsPerRow;    /* != 0: use this plan on every SELL-32 level instead (1, 2 or 4 */
+  int planBlock;            /*   threads per row; 128 or 256 threads per block, 0 = 256) */
 } fvm_linear_options;
 
 /* ThermalModelOptions (fvmbase/ThermalBC.h:33-67) + volume-condition constants */
@@ -168,6 +172,11 @@ int fvm_thermal_linear_system(fvm_thermal* t, double* diag, double* off, double*
  * their sizes, and the coarseIndex of each fine level concatenated. */
 int fvm_thermal_hierarchy(fvm_thermal* t, int* nLevels, int* sizes, int sizesCap,
                           int* coarseIndex, int ciCap);
+/* Launch plans of the smoother kernels, one per level of the current setup
+ * (no reference counterpart): threads per row and threads per block as the
+ * autotuner (or the forced plan) chose them; ELL-32 levels, whose kernels
+ * take no plan, report width, 0 -- threadsPerRow[l] = -(ELL width). */
+int fvm_thermal_launch_plans(fvm_thermal* t, int* nLevels, int* threadsPerRow, int* block, int cap);
 /* Measurement hook (no reference counterpart): CUDA-event timings in ms
  * per launch, each launch preceded by a write of 512 MB to flush L2.
  * out[0] one Gauss-Seidel pass over all colours of the finest level in the

@@ -1,0 +1,58 @@
+"""Autotuned launch plans of the smoother kernels (threads per row, threads
+per block on the SELL-32 levels): the plan changes speed only. Every plan
+forms the products of a row in parallel and adds them in stored order, so
+solves under any plan -- forced or picked by the autotuner -- give bitwise
+the same temperature field."""
+import numpy as np
+import pytest
+
+from fvm_b200 import fvmbaseExt, meshgen
+from helpers import gpu_model
+
+
+def _solve(mixed, autotune, tpr=0, block=0):
+    mesh, f = meshgen.config0(n=96, seed=3)
+    bcs = dict(f["bc"])
+    amg = fvmbaseExt.AMG()
+    amg.nPreSweeps = 1
+    amg.nPostSweeps = 1
+    amg.relativeTolerance = 0.1
+    amg.nMaxIterations = 200
+    if mixed:
+        amg.precision = fvmbaseExt.AMG.MIXED
+        amg.coarseSolver = fvmbaseExt.AMG.COARSE_DIRECT
+        amg.coarsestSize = 1000
+        amg.coarseJacobiRows = 1 << 30  # damped Jacobi below the finest level
+    amg.autotune = autotune
+    amg.planThreadsPerRow = tpr
+    amg.planBlock = block
+    tm, tf, m = gpu_model(mesh, bcs, solver=amg, fields={"conductivity": f["k"], "source": f["s"]},
+                          opts={"relativeTolerance": 1e-10})
+    tm.advance(200)
+    rep = tm.lastReport()
+    assert rep.converged
+    return tf.temperature[m.getCells()][: mesh["nCells"]].copy(), tm.getLaunchPlans(), rep.linearIterations
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mixed", [False, True], ids=["fp64-gs", "mixed-jacobi"])
+def test_plans_give_bitwise_identical_solves(mixed):
+    T0, plans0, c0 = _solve(mixed, autotune=False)
+    # default plan everywhere without the tuner
+    assert all(p in ((1, 256),) or p[1] == 0 for p in plans0)
+    for tpr, block in ((2, 128), (4, 256), (4, 128), (1, 128)):
+        T, plans, c = _solve(mixed, autotune=False, tpr=tpr, block=block)
+        sell = [p for p in plans if p[1] != 0]
+        assert sell and all(p == (tpr, block) for p in sell)
+        assert c == c0
+        np.testing.assert_array_equal(T, T0)
+    T, plans, c = _solve(mixed, autotune=True)
+    assert all((p[0] in (1, 2, 4) and p[1] in (128, 256)) or (p[0] < 0 and p[1] == 0) for p in plans)
+    assert c == c0
+    np.testing.assert_array_equal(T, T0)
+
+
+def test_plan_options_validated():
+    a = fvmbaseExt.AMG()
+    o = a.options()
+    assert o.autotune == 1 and o.planThreadsPerRow == 0 and o.planBlock == 0

@@ -49,6 +49,17 @@ def load_peaks():
 # distributed plumbing (torchrun), kept optional for N=1
 
 
+# Outer iterations and V-cycles of the GPU plain FP64 run (standalone AMG
+# V(1,1), multicolour GS, inner relTol 0.1, outer 1e-10) per workload, as
+# measured on a B200: the reference arm's CPU time is extrapolated with them
+# when no run of the product arm in this checkout has recorded fresher ones.
+PLAIN_COUNTS = {
+    "config1": {"outer": 65, "cycles": 721},
+    "config3": {"outer": 19, "cycles": 3040},
+    "config4": {"outer": 10, "cycles": 45},
+}
+
+
 def Dist():
     from fvm_b200.replicas import Ranks
 
@@ -510,7 +521,10 @@ def main():
         # run the reference itself on one outer iteration to convergence of
         # the inner solve is too long; use the recorded plain-path counts
         counts_path = os.path.join(ROOT, "profiles", "plain_counts_%s.json" % args.workload)
-        counts = json.load(open(counts_path)) if os.path.exists(counts_path) else {"outer": 10, "cycles": 60}
+        if os.path.exists(counts_path):
+            counts = json.load(open(counts_path))
+        else:
+            counts = PLAIN_COUNTS.get(args.workload, {"outer": 10, "cycles": 60})
         vals = []
         base = None
         for _ in range(max(1, args.steps)):

@@ -60,6 +60,11 @@ PLAIN_COUNTS = {
 }
 
 
+# dram__bytes_read.sum + dram__bytes_write.sum of one finest-level FP32 GS
+# pass (sum over its colour launches) from an ncu capture of the workload
+NCU_PASS_TRAFFIC = {"config1": 4 * 24.69e6}
+
+
 def Dist():
     from fvm_b200.replicas import Ranks
 
@@ -613,7 +618,12 @@ def main():
     peak = float(peaks.get("hbm_gbs", PEAKS_FALLBACK["hbm_gbs"]))
     pp = plain["profile"]
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": None, "kernel": "k_gs_color<float> (one pass over all colours, finest level)",
+                "traffic": NCU_PASS_TRAFFIC.get(args.workload),
+                "traffic_note": ("DRAM read+write of the four colour launches of one FP32 pass, ncu, caches cold "
+                                 "before every launch (profiles/k_gs_color_ell_config1.md); per-pass algorithmic "
+                                 "bytes %.1f MB" % (pm["gs_pass_bytes"] / 1e6)) if args.workload in NCU_PASS_TRAFFIC
+                else None,
+                "kernel": "k_gs_color_ell<float, W> (one pass over all colours, finest level)",
                 "peak_kind": peak_kind,
                 "fp64_gs_pass": {"achieved": pp["gs_pass_bytes"] / (pp["gs_pass_ms"] * 1e-3) / 1e9,
                                  "frac": pp["gs_pass_bytes"] / (pp["gs_pass_ms"] * 1e-3) / 1e9 / peak},

@@ -60,9 +60,10 @@ PLAIN_COUNTS = {
 }
 
 
-# dram__bytes_read.sum + dram__bytes_write.sum of one finest-level FP32 GS
-# pass (sum over its colour launches) from an ncu capture of the workload
-NCU_PASS_TRAFFIC = {"config1": 4 * 24.69e6}
+# dram__bytes_read.sum + dram__bytes_write.sum over the algorithmic bytes of
+# the finest-level FP32 GS colour launches in an ncu capture of the workload
+# (24.69 MB for a 502k-row colour of 24.10 MB algorithmic)
+NCU_TRAFFIC_RATIO = {"config1": 24.69 / 24.10}
 
 
 def Dist():
@@ -618,11 +619,12 @@ def main():
     peak = float(peaks.get("hbm_gbs", PEAKS_FALLBACK["hbm_gbs"]))
     pp = plain["profile"]
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": NCU_PASS_TRAFFIC.get(args.workload),
-                "traffic_note": ("DRAM read+write of the four colour launches of one FP32 pass, ncu, caches cold "
-                                 "before every launch (profiles/k_gs_color_ell_config1.md); per-pass algorithmic "
-                                 "bytes %.1f MB" % (pm["gs_pass_bytes"] / 1e6)) if args.workload in NCU_PASS_TRAFFIC
-                else None,
+                "traffic": (NCU_TRAFFIC_RATIO[args.workload] * pm["gs_pass_bytes"]
+                            if args.workload in NCU_TRAFFIC_RATIO else None),
+                "traffic_note": ("ncu DRAM read+write of captured colour launches of this pass (caches cold before "
+                                 "each launch) over their algorithmic bytes, %.3f, times the pass's algorithmic "
+                                 "bytes (profiles/k_gs_color_ell_config1.md)" % NCU_TRAFFIC_RATIO[args.workload])
+                if args.workload in NCU_TRAFFIC_RATIO else None,
                 "kernel": "k_gs_color_ell<float, W> (one pass over all colours, finest level)",
                 "peak_kind": peak_kind,
                 "fp64_gs_pass": {"achieved": pp["gs_pass_bytes"] / (pp["gs_pass_ms"] * 1e-3) / 1e9,

@@ -3,6 +3,8 @@
 #include "amg_setup.hpp"
 
 #include <algorithm>
+#include <limits>
+#include <memory>
 #include <cmath>
 #include <thread>
 
@@ -108,17 +110,38 @@ void create_coarse_level(const RefLevel& fine, RefLevel& coarse, CSR& c2f) {
   const std::vector<int>& ci = fine.coarseIndex;
   const std::vector<int>& row = fine.conn.row;
   const std::vector<int>& col = fine.conn.col;
-  // coarse -> fine rows, fine rows ascending
+  // coarse -> fine rows, fine rows ascending. Independent blocks (a batch
+  // of meshes: fine block s aggregates into coarse rows of block s only)
+  // are counted and filled in parallel.
+  const std::vector<int>& fseg = fine.segments;
+  const bool blocks = fseg.size() >= 3;
+  const int nBlocks = blocks ? (int)fseg.size() - 1 : 1;
+  auto blockRows = [&](int sg, int& b, int& e) {
+    b = blocks ? fseg[sg] : 0;
+    e = blocks ? fseg[sg + 1] : fine.n;
+  };
   c2f.nRows = nc;
   c2f.row.assign(nc + 1, 0);
-  for (int i = 0; i < fine.n; i++)
-    if (ci[i] >= 0) c2f.row[ci[i] + 1]++;
+  parallel_chunks(nBlocks, [&](int b0, int e0) {
+    for (int sg = b0; sg < e0; sg++) {
+      int b, e;
+      blockRows(sg, b, e);
+      for (int i = b; i < e; i++)
+        if (ci[i] >= 0) c2f.row[ci[i] + 1]++;
+    }
+  }, 1);
   for (int I = 0; I < nc; I++) c2f.row[I + 1] += c2f.row[I];
   c2f.col.resize(c2f.row[nc]);
   {
     std::vector<int> cur(c2f.row.begin(), c2f.row.end() - 1);
-    for (int i = 0; i < fine.n; i++)
-      if (ci[i] >= 0) c2f.col[cur[ci[i]]++] = i;
+    parallel_chunks(nBlocks, [&](int b0, int e0) {
+      for (int sg = b0; sg < e0; sg++) {
+        int b, e;
+        blockRows(sg, b, e);
+        for (int i = b; i < e; i++)
+          if (ci[i] >= 0) c2f.col[cur[ci[i]]++] = i;
+      }
+    }, 1);
   }
   // Coarse pattern: each coarse row lists the coarse neighbours of its fine
   // rows in first-visit order. Rows are independent, so they are built in
@@ -129,14 +152,18 @@ void create_coarse_level(const RefLevel& fine, RefLevel& coarse, CSR& c2f) {
   coarse.symmetricPattern = fine.symmetricPattern;
   coarse.conn.nRows = nc;
   coarse.conn.row.assign(nc + 1, 0);
-  auto visit = [&](int I, int* out, int* stamp) {
+  // stamp[J - lo] == tag: J already listed in the row being built. Each
+  // chunk of coarse rows gets stamp / slot arrays spanning only the coarse
+  // columns its rows reach (found by a first pass), so large levels need no
+  // nc-sized array per thread.
+  auto visit = [&](int I, int* out, int* stamp, int lo, int tag) {
     int cnt = 0;
     for (int k = c2f.row[I]; k < c2f.row[I + 1]; k++) {
       const int i = c2f.col[k];
       for (int nb = row[i]; nb < row[i + 1]; nb++) {
         const int J = ci[col[nb]];
-        if (J < 0 || J == I || stamp[J] == I) continue;
-        stamp[J] = I;
+        if (J < 0 || J == I || stamp[J - lo] == tag) continue;
+        stamp[J - lo] = tag;
         if (out) out[cnt] = J;
         cnt++;
       }
@@ -144,9 +171,27 @@ void create_coarse_level(const RefLevel& fine, RefLevel& coarse, CSR& c2f) {
     return cnt;
   };
   constexpr int kMinRows = 4096;  // coarse rows per level below which the passes run on one thread
-  parallel_chunks(nc, [&](int b, int e) {
-    std::vector<int> stamp(nc, -1);
-    for (int I = b; I < e; I++) coarse.conn.row[I + 1] = visit(I, nullptr, stamp.data());
+  const int nChunks = chunk_count(nc, kMinRows);
+  std::vector<int> lo(nChunks, 0), hi(nChunks, -1);
+  std::vector<std::vector<int>> stamps(nChunks);
+  std::vector<std::unique_ptr<int[]>> slots(nChunks);
+  parallel_chunks_indexed(nc, [&](int t, int b, int e) {
+    int l = std::numeric_limits<int>::max(), h = -1;
+    for (int k = c2f.row[b]; k < c2f.row[e]; k++) {
+      const int i = c2f.col[k];
+      for (int nb = row[i]; nb < row[i + 1]; nb++) {
+        const int J = ci[col[nb]];
+        if (J < 0) continue;
+        l = std::min(l, J);
+        h = std::max(h, J);
+      }
+    }
+    if (h < l) l = h = 0;
+    lo[t] = l;
+    hi[t] = h;
+    stamps[t].assign((size_t)(h - l + 1), -1);
+    slots[t].reset(new int[(size_t)(h - l + 1)]);
+    for (int I = b; I < e; I++) coarse.conn.row[I + 1] = visit(I, nullptr, stamps[t].data(), l, I);
   }, kMinRows);
   for (int I = 0; I < nc; I++) coarse.conn.row[I + 1] += coarse.conn.row[I];
   coarse.conn.col.resize(coarse.conn.row[nc]);
@@ -156,15 +201,18 @@ void create_coarse_level(const RefLevel& fine, RefLevel& coarse, CSR& c2f) {
   // entry receives its fine contributions in the reference's order (fine
   // rows ascending, their entries in stored order), so the sums round
   // exactly as CRMatrix::createCoarseMatrix's do. The fill of row I and its
-  // values share one pass: pos[J] is J's slot in the row being built.
-  parallel_chunks(nc, [&](int b, int e) {
-    std::vector<int> stamp(nc, -1), pos(nc, 0);
+  // values share one pass (tag I + nc: the stamps of the count pass need no
+  // clearing): pos[J - lo] is J's slot in the row being built.
+  parallel_chunks_indexed(nc, [&](int t, int b, int e) {
+    int* stamp = stamps[t].data();
+    int* pos = slots[t].get();
+    const int l = lo[t];
     for (int I = b; I < e; I++) {
       const int rb = coarse.conn.row[I];
       int* out = &coarse.conn.col[rb];
-      const int cnt = visit(I, out, stamp.data());
+      const int cnt = visit(I, out, stamp, l, I + nc);
       for (int q = 0; q < cnt; q++) {
-        pos[out[q]] = rb + q;
+        pos[out[q] - l] = rb + q;
         coarse.off[rb + q] = 0.0;
       }
       double d = 0.0;
@@ -175,7 +223,7 @@ void create_coarse_level(const RefLevel& fine, RefLevel& coarse, CSR& c2f) {
           const int J = ci[col[nb]];
           if (J < 0) continue;
           if (J != I)
-            coarse.off[pos[J]] += fine.off[nb];
+            coarse.off[pos[J - l]] += fine.off[nb];
           else
             d += fine.off[nb];
         }
@@ -206,8 +254,8 @@ void build_hierarchy(std::vector<RefLevel>& levels, const HierarchyOptions& opt,
     coarse.nCoarse = 0;
     CSR c2f;
     if (spareC2f && lc - 1 < spareC2f->size()) c2f = std::move((*spareC2f)[lc - 1]);
-    create_coarse_level(fine, coarse, c2f);
     coarse.segments = std::move(coarseSeg);
+    create_coarse_level(fine, coarse, c2f);
     FVM_REQUIRE(levels.size() < levels.capacity() || !onLevel, kBadArgument,
                 "build_hierarchy: no room for another level");
     levels.push_back(std::move(coarse));
@@ -349,11 +397,42 @@ bool symmetrize_pattern(const CSR& a, CSR& out) {
   return extra;
 }
 
-int multicolor(const CSR& connIn, std::vector<int>& color, bool symmetricPattern) {
+int multicolor(const CSR& connIn, std::vector<int>& color, bool symmetricPattern, const std::vector<int>* segments) {
   CSR sym;
   const CSR& conn = (!symmetricPattern && symmetrize_pattern(connIn, sym)) ? sym : connIn;
   constexpr int kFewColors = 5;
   const int n = conn.nRows;
+  if (segments && segments->size() >= 3) {
+    // independent blocks: the row-order greedy colouring of each block is
+    // the global one restricted to it (no edge leaves a block), so the
+    // blocks are coloured in parallel with the same result
+    const std::vector<int>& sg = *segments;
+    const int nb = (int)sg.size() - 1;
+    color.assign(n, -1);
+    std::vector<int> ncol(nb, 0);
+    parallel_chunks(nb, [&](int b0, int e0) {
+      std::vector<int> mark;
+      for (int q = b0; q < e0; q++) {
+        int nc = 0;
+        for (int i = sg[q]; i < sg[q + 1]; i++) {
+          for (int k = conn.row[i]; k < conn.row[i + 1]; k++) {
+            const int c = color[conn.col[k]];
+            if (c >= 0) {
+              if ((int)mark.size() <= c) mark.resize(c + 1, -1);
+              mark[c] = i;
+            }
+          }
+          int c = 0;
+          while (c < (int)mark.size() && mark[c] == i) c++;
+          color[i] = c;
+          nc = std::max(nc, c + 1);
+        }
+        ncol[q] = nc;
+      }
+    }, 1);
+    const int c1 = *std::max_element(ncol.begin(), ncol.end());
+    if (c1 <= kFewColors) return c1;
+  }
   std::vector<int> natural(n);
   for (int i = 0; i < n; i++) natural[i] = i;
   const int c1 = greedy_in_order(conn, natural, color);
@@ -403,24 +482,47 @@ void pack_level(const RefLevel& lv, SmootherOrdering ordering, PackedLevel& out)
     color.assign(n, 0);
     out.nColors = 1;
   } else {
-    out.nColors = multicolor(lv.conn, color, lv.symmetricPattern);
+    out.nColors = multicolor(lv.conn, color, lv.symmetricPattern, &lv.segments);
   }
-  // colour-major permutation, stable in reference order
-  out.colorStart.assign(out.nColors + 1, 0);
-  for (int i = 0; i < n; i++) out.colorStart[color[i] + 1]++;
-  for (int c = 0; c < out.nColors; c++) out.colorStart[c + 1] += out.colorStart[c];
+  // colour-major permutation, stable in reference order: per-chunk colour
+  // counts, then every chunk places its rows behind the earlier chunks'
+  const int C = out.nColors;
+  int nt = (int)std::thread::hardware_concurrency();
+  nt = std::max(1, std::min(nt, 32));
+  if (n < 200000) nt = 1;
+  const int chunk = (n + nt - 1) / nt;
+  std::vector<int> cnt((size_t)nt * C, 0);
+  parallel_chunks(nt, [&](int t0, int t1) {
+    for (int t = t0; t < t1; t++)
+      for (int i = t * chunk; i < std::min(n, (t + 1) * chunk); i++) cnt[(size_t)t * C + color[i]]++;
+  }, 1);
+  out.colorStart.assign(C + 1, 0);
+  std::vector<int> base((size_t)nt * C);
+  {
+    int pos = 0;
+    for (int c = 0; c < C; c++) {
+      out.colorStart[c] = pos;
+      for (int t = 0; t < nt; t++) {
+        base[(size_t)t * C + c] = pos;
+        pos += cnt[(size_t)t * C + c];
+      }
+    }
+    out.colorStart[C] = pos;
+  }
   out.perm.resize(n);
   out.iperm.resize(n);
-  {
-    std::vector<int> cur(out.colorStart.begin(), out.colorStart.end() - 1);
-    for (int i = 0; i < n; i++) {
-      const int p = cur[color[i]]++;
-      out.perm[i] = p;
-      out.iperm[p] = i;
-    }
-  }
   out.diag.resize(n);
-  for (int p = 0; p < n; p++) out.diag[p] = lv.diag[out.iperm[p]];
+  parallel_chunks(nt, [&](int t0, int t1) {
+    for (int t = t0; t < t1; t++) {
+      int* cur = &base[(size_t)t * C];
+      for (int i = t * chunk; i < std::min(n, (t + 1) * chunk); i++) {
+        const int p = cur[color[i]]++;
+        out.perm[i] = p;
+        out.iperm[p] = i;
+        out.diag[p] = lv.diag[i];
+      }
+    }
+  }, 1);
   // SELL-32 slices aligned to colour blocks
   out.colorSliceStart.assign(out.nColors + 1, 0);
   out.sliceRow.clear();
@@ -498,19 +600,24 @@ void pack_slices(const RefLevel& lv, PackedLevel& out, int sBegin, int sEnd) {
 }
 
 void pack_transfer(const RefLevel& fine, const CSR& c2f, PackedLevel& pf, const PackedLevel& pc) {
-  pf.coarseIndex.assign(fine.n, -1);
-  for (int i = 0; i < fine.n; i++)
-    if (fine.coarseIndex[i] >= 0) pf.coarseIndex[pf.perm[i]] = pc.perm[fine.coarseIndex[i]];
+  pf.coarseIndex.resize(fine.n);
+  parallel_chunks(fine.n, [&](int b, int e) {
+    for (int i = b; i < e; i++)
+      pf.coarseIndex[pf.perm[i]] = fine.coarseIndex[i] >= 0 ? pc.perm[fine.coarseIndex[i]] : -1;
+  }, 1 << 17);
   const int nc = pc.n;
   pf.c2fRow.assign(nc + 1, 0);
-  for (int I = 0; I < nc; I++) pf.c2fRow[pc.perm[I] + 1] = c2f.count(I);
+  parallel_chunks(nc, [&](int b, int e) {
+    for (int I = b; I < e; I++) pf.c2fRow[pc.perm[I] + 1] = c2f.count(I);
+  }, 1 << 17);
   for (int P = 0; P < nc; P++) pf.c2fRow[P + 1] += pf.c2fRow[P];
   pf.c2fCol.resize(c2f.nnz());
-  for (int I = 0; I < nc; I++) {
-    const int P = pc.perm[I];
-    int o = pf.c2fRow[P];
-    for (int k = c2f.row[I]; k < c2f.row[I + 1]; k++) pf.c2fCol[o++] = pf.perm[c2f.col[k]];
-  }
+  parallel_chunks(nc, [&](int b, int e) {
+    for (int I = b; I < e; I++) {
+      int o = pf.c2fRow[pc.perm[I]];
+      for (int k = c2f.row[I]; k < c2f.row[I + 1]; k++) pf.c2fCol[o++] = pf.perm[c2f.col[k]];
+    }
+  }, 1 << 17);
 }
 
 void dense_inverse(const PackedLevel& lv, std::vector<double>& inv) {

@@ -102,7 +102,10 @@ int greedy_coloring(const CSR& conn, std::vector<int>& color);
 // The colouring the multicolour smoothers use: row-order greedy, or when
 // that needs more than five colours the better (fewer colours) of it and
 // smallest-last-order greedy; deterministic.
-int multicolor(const CSR& conn, std::vector<int>& color, bool symmetricPattern = true);
+// With segments (row offsets of independent diagonal blocks) the blocks
+// are coloured in parallel, with the same result.
+int multicolor(const CSR& conn, std::vector<int>& color, bool symmetricPattern = true,
+               const std::vector<int>* segments = nullptr);
 // Pattern of A + A^T: each row keeps its stored columns, followed by the
 // columns present only in the transpose, ascending. Returns false (and
 // leaves out untouched) when the pattern is already symmetric.

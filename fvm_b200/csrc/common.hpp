@@ -52,6 +52,36 @@ struct CSR {
 
 // Runs f(begin, end) over [0, n) split into contiguous chunks on the host's
 // cores (at most 32 threads; one chunk when n < minItems).
+// Number of chunks parallel_chunks(n, ..., minItems) splits [0, n) into.
+inline int chunk_count(int n, int minItems = 20000) {
+  int nt = (int)std::thread::hardware_concurrency();
+  if (nt < 1) nt = 1;
+  if (nt > 32) nt = 32;
+  if (n < minItems || nt == 1) return 1;
+  const int chunk = (n + nt - 1) / nt;
+  return (n + chunk - 1) / chunk;
+}
+
+// As parallel_chunks, with f(t, begin, end) also given the chunk index t
+// (0 .. chunk_count(n, minItems) - 1).
+template <class F>
+void parallel_chunks_indexed(int n, F f, int minItems = 20000) {
+  const int nc = chunk_count(n, minItems);
+  if (nc == 1) {
+    f(0, 0, n);
+    return;
+  }
+  int nt = (int)std::thread::hardware_concurrency();
+  if (nt > 32) nt = 32;
+  const int chunk = (n + nt - 1) / nt;
+  std::vector<std::thread> th;
+  for (int t = 0; t < nc; t++) {
+    const int b = t * chunk, e = std::min(n, b + chunk);
+    th.emplace_back([=] { f(t, b, e); });
+  }
+  for (auto& x : th) x.join();
+}
+
 template <class F>
 void parallel_chunks(int n, F f, int minItems = 20000) {
   int nt = (int)std::thread::hardware_concurrency();

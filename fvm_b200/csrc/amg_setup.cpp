@@ -145,9 +145,9 @@ void create_coarse_level(const RefLevel& fine, RefLevel& coarse, CSR& c2f) {
   }
   // Coarse pattern: each coarse row lists the coarse neighbours of its fine
   // rows in first-visit order. Rows are independent, so they are built in
-  // parallel: a count pass, a prefix sum, a fill pass. A per-thread stamp
-  // array (stamp[J] == I: J already listed in row I) replaces the
-  // reference's marker array and needs no clearing between rows.
+  // parallel: a count pass, a prefix sum, then one pass that lists the
+  // columns and sums the values. Stamp arrays replace the reference's marker
+  // array and need no clearing between rows.
   coarse.n = nc;
   coarse.symmetricPattern = fine.symmetricPattern;
   coarse.conn.nRows = nc;
@@ -175,15 +175,24 @@ void create_coarse_level(const RefLevel& fine, RefLevel& coarse, CSR& c2f) {
   std::vector<int> lo(nChunks, 0), hi(nChunks, -1);
   std::vector<std::vector<int>> stamps(nChunks);
   std::vector<std::unique_ptr<int[]>> slots(nChunks);
+  // independent blocks: the columns of coarse rows [b, e) lie in the blocks
+  // of rows b and e - 1 (no pass needed to find them)
+  const std::vector<int>& cseg = coarse.segments;
+  const bool cblocks = cseg.size() >= 3 && cseg.back() == nc;
   parallel_chunks_indexed(nc, [&](int t, int b, int e) {
     int l = std::numeric_limits<int>::max(), h = -1;
-    for (int k = c2f.row[b]; k < c2f.row[e]; k++) {
-      const int i = c2f.col[k];
-      for (int nb = row[i]; nb < row[i + 1]; nb++) {
-        const int J = ci[col[nb]];
-        if (J < 0) continue;
-        l = std::min(l, J);
-        h = std::max(h, J);
+    if (cblocks && e > b) {
+      l = *(std::upper_bound(cseg.begin(), cseg.end(), b) - 1);
+      h = *std::upper_bound(cseg.begin(), cseg.end(), e - 1) - 1;
+    } else {
+      for (int k = c2f.row[b]; k < c2f.row[e]; k++) {
+        const int i = c2f.col[k];
+        for (int nb = row[i]; nb < row[i + 1]; nb++) {
+          const int J = ci[col[nb]];
+          if (J < 0) continue;
+          l = std::min(l, J);
+          h = std::max(h, J);
+        }
       }
     }
     if (h < l) l = h = 0;
@@ -200,21 +209,18 @@ void create_coarse_level(const RefLevel& fine, RefLevel& coarse, CSR& c2f) {
   // Galerkin values with piecewise-constant prolongation; every coarse
   // entry receives its fine contributions in the reference's order (fine
   // rows ascending, their entries in stored order), so the sums round
-  // exactly as CRMatrix::createCoarseMatrix's do. The fill of row I and its
-  // values share one pass (tag I + nc: the stamps of the count pass need no
-  // clearing): pos[J - lo] is J's slot in the row being built.
+  // exactly as CRMatrix::createCoarseMatrix's do. Row I's columns are listed
+  // in the same walk that sums its values: a column gets its slot (pos[J -
+  // lo]) when first met, which is the first-visit order (tag I + nc: the
+  // stamps of the count pass need no clearing).
   parallel_chunks_indexed(nc, [&](int t, int b, int e) {
     int* stamp = stamps[t].data();
     int* pos = slots[t].get();
     const int l = lo[t];
     for (int I = b; I < e; I++) {
       const int rb = coarse.conn.row[I];
-      int* out = &coarse.conn.col[rb];
-      const int cnt = visit(I, out, stamp, l, I + nc);
-      for (int q = 0; q < cnt; q++) {
-        pos[out[q] - l] = rb + q;
-        coarse.off[rb + q] = 0.0;
-      }
+      const int tag = I + nc;
+      int cnt = 0;
       double d = 0.0;
       for (int k = c2f.row[I]; k < c2f.row[I + 1]; k++) {
         const int i = c2f.col[k];
@@ -222,10 +228,18 @@ void create_coarse_level(const RefLevel& fine, RefLevel& coarse, CSR& c2f) {
         for (int nb = row[i]; nb < row[i + 1]; nb++) {
           const int J = ci[col[nb]];
           if (J < 0) continue;
-          if (J != I)
+          if (J != I) {
+            if (stamp[J - l] != tag) {
+              stamp[J - l] = tag;
+              pos[J - l] = rb + cnt;
+              coarse.conn.col[rb + cnt] = J;
+              coarse.off[rb + cnt] = 0.0;
+              cnt++;
+            }
             coarse.off[pos[J - l]] += fine.off[nb];
-          else
+          } else {
             d += fine.off[nb];
+          }
         }
       }
       coarse.diag[I] = d;

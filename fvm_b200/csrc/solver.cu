@@ -147,7 +147,11 @@ void AmgHierarchy::build(std::vector<RefLevel>& levels, int finestLocalSize, con
       errs[l] = std::current_exception();
     }
   };
+  const auto tBuild = std::chrono::steady_clock::now();
   auto startLevel = [&](int l) {
+    if (trace && l > 0)
+      fprintf(stderr, "[fvm setup]   level %d (%d rows) ready at %8.1f ms\n", l, ref_[l].n,
+              std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tBuild).count());
     packed_[l] = take_spare(sparePacked_, (size_t)l);
     th[l] = std::thread(packAndUpload, l);
   };

@@ -423,7 +423,10 @@ void ThermalModel::ensureMatrix() {
   levels[0] = hier_.spareLevel(0);
   RefLevel& l0 = levels[0];
   l0.n = n;
-  l0.conn = interiorConn_;
+  // the spare level 0 of this model's previous build already holds the
+  // (fixed) connectivity of its mesh
+  if (l0.conn.nRows != interiorConn_.nRows || l0.conn.col.size() != interiorConn_.col.size())
+    l0.conn = interiorConn_;
   l0.symmetricPattern = true;  // cellCells restricted to self rows
   l0.segments = segOff_;       // a batch: its meshes aggregate in parallel
   l0.coarseIndex.clear();

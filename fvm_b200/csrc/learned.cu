@@ -762,8 +762,9 @@ __global__ void k_step_trial(int n, const double* __restrict__ r, const double* 
 
 __global__ void k_step_accept(int n, double* __restrict__ x, const double* __restrict__ d, double* __restrict__ r,
                               const double* __restrict__ rt, const double* __restrict__ alpha,
-                              const double* __restrict__ norm, const double* __restrict__ trial) {
-  if (!(trial[0] < norm[0])) return;
+                              const double* __restrict__ norm, const double* __restrict__ trial,
+                              double acceptFactor) {
+  if (!(trial[0] < acceptFactor * norm[0])) return;
   const double a = alpha[0];
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     x[i] += a * d[i];
@@ -772,9 +773,9 @@ __global__ void k_step_accept(int n, double* __restrict__ x, const double* __res
 }
 
 __global__ void k_step_finish(double* norm, const double* trial, double* accepted, double* steps,
-                              double* useful, double usefulFactor) {
+                              double* useful, double usefulFactor, double acceptFactor) {
   if (trial[0] < usefulFactor * norm[0]) useful[0] += 1.0;
-  if (trial[0] < norm[0]) {
+  if (trial[0] < acceptFactor * norm[0]) {
     norm[0] = trial[0];
     accepted[0] += 1.0;
   }
@@ -791,12 +792,12 @@ void step_trial(int n, const double* r, const double* q, const double* alpha, do
   k_step_trial<<<dev::vec_blocks(n), kBlock, 0, st>>>(n, r, q, alpha, rt, partials);
 }
 void step_accept(int n, double* x, const double* d, double* r, const double* rt, const double* alpha,
-                 const double* norm, const double* trialNorm, cudaStream_t st) {
-  k_step_accept<<<dev::vec_blocks(n), kBlock, 0, st>>>(n, x, d, r, rt, alpha, norm, trialNorm);
+                 const double* norm, const double* trialNorm, double acceptFactor, cudaStream_t st) {
+  k_step_accept<<<dev::vec_blocks(n), kBlock, 0, st>>>(n, x, d, r, rt, alpha, norm, trialNorm, acceptFactor);
 }
 void step_finish(double* norm, const double* trialNorm, double* accepted, double* steps, double* useful,
-                 double usefulFactor, cudaStream_t st) {
-  k_step_finish<<<1, 1, 0, st>>>(norm, trialNorm, accepted, steps, useful, usefulFactor);
+                 double usefulFactor, double acceptFactor, cudaStream_t st) {
+  k_step_finish<<<1, 1, 0, st>>>(norm, trialNorm, accepted, steps, useful, usefulFactor, acceptFactor);
 }
 
 }  // namespace nn

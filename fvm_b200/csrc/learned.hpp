@@ -94,13 +94,13 @@ void step_alpha(const double* rq, const double* qq, double* alpha, cudaStream_t 
 // rt = r + alpha q, with per-block L1 partials of rt (vec_blocks(n) of them)
 void step_trial(int n, const double* r, const double* q, const double* alpha, double* rt, double* partials,
                 cudaStream_t st);
-// if trialNorm < norm: x += alpha d, r = rt
+// if trialNorm < acceptFactor * norm: x += alpha d, r = rt
 void step_accept(int n, double* x, const double* d, double* r, const double* rt, const double* alpha,
-                 const double* norm, const double* trialNorm, cudaStream_t st);
-// if trialNorm < norm: norm = trialNorm, accepted += 1; if trialNorm <
-// usefulFactor * norm: useful += 1; steps += 1
+                 const double* norm, const double* trialNorm, double acceptFactor, cudaStream_t st);
+// if trialNorm < acceptFactor * norm: norm = trialNorm, accepted += 1; if
+// trialNorm < usefulFactor * norm: useful += 1; steps += 1
 void step_finish(double* norm, const double* trialNorm, double* accepted, double* steps, double* useful,
-                 double usefulFactor, cudaStream_t st);
+                 double usefulFactor, double acceptFactor, cudaStream_t st);
 }  // namespace nn
 
 // A trained (or training) learned correction: parameters, Adam state and

@@ -264,7 +264,7 @@ class LinearSolve {
   static constexpr double kLsUsefulFactor = 0.5;
   bool learnedActive_ = true;
   int lsTries_ = 0, lsKept_ = 0;
-  void learnedStep(cudaStream_t st, double* x, double* r);
+  void learnedStep(cudaStream_t st, double* x, double* r, double acceptFactor);
   std::map<const void*, long long> nodeCounts_;
   bool graphsFailed_ = false;
 

@@ -1066,7 +1066,9 @@ void dense_solve_f32(int n, const float* ainv, const float* b, float* x, cudaStr
 }
 namespace {
 constexpr int kGjMaxPanel = 8;
-constexpr size_t kGjSmemLimit = 200 * 1024;
+// the panel's shared memory: the 227 KB a CTA may hold, less 2 KB for the
+// kernel's static reduction arrays
+constexpr size_t kGjSmemLimit = 227 * 1024 - 2048;
 size_t gj_align(size_t b) { return (b + 255) & ~size_t(255); }
 template <int B>
 void gj_run(int n, double* a, double* inv, double* Bt, int* piv, int* idx, int* status, cudaStream_t st) {
@@ -1123,9 +1125,17 @@ void gauss_jordan_inverse(int n, double* a, double* inv, void* scratch, cudaStre
   int* idx = piv + gj_align(sizeof(int) * (size_t)n) / sizeof(int);
   int* status = (int*)gauss_jordan_status(n, scratch);
   cudaMemsetAsync(status, 0, sizeof(int), st);
-  if (sizeof(double) * 8 * (size_t)n <= kGjSmemLimit)
+  // the widest panel whose n x B block fits in shared memory: every panel
+  // streams the whole matrix once, so fewer, wider panels cost less (4096
+  // rows: 7 columns, 586 panels instead of 1024 of 4)
+  const size_t col = sizeof(double) * (size_t)n;
+  if (8 * col <= kGjSmemLimit)
     gj_run<8>(n, a, inv, Bt, piv, idx, status, st);
-  else if (sizeof(double) * 4 * (size_t)n <= kGjSmemLimit)
+  else if (7 * col <= kGjSmemLimit)
+    gj_run<7>(n, a, inv, Bt, piv, idx, status, st);
+  else if (6 * col <= kGjSmemLimit)
+    gj_run<6>(n, a, inv, Bt, piv, idx, status, st);
+  else if (4 * col <= kGjSmemLimit)
     gj_run<4>(n, a, inv, Bt, piv, idx, status, st);
   else
     gj_run<2>(n, a, inv, Bt, piv, idx, status, st);

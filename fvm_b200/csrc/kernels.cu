@@ -595,10 +595,12 @@ __global__ void k_gj_swap_rows(int n, int k0, int nb, double* __restrict__ A, co
   for (int t = 0; t < nb; t++) Bt[(size_t)t * n + j] = inPanel ? 0.0 : A[(size_t)(k0 + t) * n + j];
 }
 
-__global__ void k_gj_update(int n, int k0, int nb, double* __restrict__ A, const double* __restrict__ Bt) {
-  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+// columns [jlo, jhi) outside the panel [k0, k0 + nb) and outside [s0, s1)
+__global__ void k_gj_update(int n, int k0, int nb, double* __restrict__ A, const double* __restrict__ Bt, int jlo,
+                            int jhi, int s0, int s1) {
+  const int j = jlo + blockIdx.x * blockDim.x + threadIdx.x;
   const int i = blockIdx.y;
-  if (j >= n || (j >= k0 && j < k0 + nb)) return;
+  if (j >= jhi || (j >= k0 && j < k0 + nb) || (j >= s0 && j < s1)) return;
   const double* Mi = A + (size_t)i * n + k0;
   double s = 0.0;
   for (int t = 0; t < nb; t++) s = s + Mi[t] * Bt[(size_t)t * n + j];
@@ -1070,16 +1072,46 @@ constexpr int kGjMaxPanel = 8;
 // kernel's static reduction arrays
 constexpr size_t kGjSmemLimit = 227 * 1024 - 2048;
 size_t gj_align(size_t b) { return (b + 255) & ~size_t(255); }
+// Look-ahead: after panel p's row swaps, the next panel's columns are
+// updated first and factored on stream st while the rest of the matrix
+// takes panel p's update on a second stream (disjoint columns); panel p+1's
+// row swaps then wait for that update. The single-CTA panel factorization
+// thus overlaps the whole-GPU update instead of following it.
 template <int B>
 void gj_run(int n, double* a, double* inv, double* Bt, int* piv, int* idx, int* status, cudaStream_t st) {
   const size_t smem = sizeof(double) * (size_t)B * n;
   cudaFuncSetAttribute(k_gj_panel<B>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaStream_t us = nullptr;
+  cudaEvent_t swapped = nullptr, updated = nullptr;
+  const bool split = cudaStreamCreateWithFlags(&us, cudaStreamNonBlocking) == cudaSuccess &&
+                     cudaEventCreateWithFlags(&swapped, cudaEventDisableTiming) == cudaSuccess &&
+                     cudaEventCreateWithFlags(&updated, cudaEventDisableTiming) == cudaSuccess;
   const dim3 ug(ceil_div(n, kBlock), n);
+  k_gj_panel<B><<<1, 1024, smem, st>>>(n, 0, n < B ? n : B, a, piv, status);
   for (int k0 = 0; k0 < n; k0 += B) {
     const int nb = n - k0 < B ? n - k0 : B;
-    k_gj_panel<B><<<1, 1024, smem, st>>>(n, k0, nb, a, piv, status);
+    const int k1 = k0 + nb;                          // next panel [k1, k1 + nb1)
+    const int nb1 = n - k1 < B ? n - k1 : B;
+    if (split && k0 > 0) cudaStreamWaitEvent(st, updated, 0);  // previous panel's update done
     k_gj_swap_rows<<<ceil_div(n, kBlock), kBlock, 0, st>>>(n, k0, nb, a, piv, Bt);
-    k_gj_update<<<ug, kBlock, 0, st>>>(n, k0, nb, a, Bt);
+    if (!split || nb1 <= 0) {
+      k_gj_update<<<ug, kBlock, 0, st>>>(n, k0, nb, a, Bt, 0, n, 0, 0);
+      if (nb1 > 0) k_gj_panel<B><<<1, 1024, smem, st>>>(n, k1, nb1, a, piv, status);
+      continue;
+    }
+    cudaEventRecord(swapped, st);
+    const dim3 ul(ceil_div(nb1, kBlock), n);
+    k_gj_update<<<ul, kBlock, 0, st>>>(n, k0, nb, a, Bt, k1, k1 + nb1, 0, 0);
+    k_gj_panel<B><<<1, 1024, smem, st>>>(n, k1, nb1, a, piv, status);
+    cudaStreamWaitEvent(us, swapped, 0);
+    k_gj_update<<<ug, kBlock, 0, us>>>(n, k0, nb, a, Bt, 0, n, k1, k1 + nb1);
+    cudaEventRecord(updated, us);
+  }
+  if (split) {
+    cudaStreamWaitEvent(st, updated, 0);
+    cudaEventDestroy(swapped);
+    cudaEventDestroy(updated);
+    cudaStreamDestroy(us);
   }
   k_gj_colperm<<<1, 1, 0, st>>>(n, piv, idx);
   k_gj_gather<<<ug, kBlock, 0, st>>>(n, a, idx, inv);
@@ -1125,9 +1157,11 @@ void gauss_jordan_inverse(int n, double* a, double* inv, void* scratch, cudaStre
   int* idx = piv + gj_align(sizeof(int) * (size_t)n) / sizeof(int);
   int* status = (int*)gauss_jordan_status(n, scratch);
   cudaMemsetAsync(status, 0, sizeof(int), st);
-  // the widest panel whose n x B block fits in shared memory: every panel
-  // streams the whole matrix once, so fewer, wider panels cost less (4096
-  // rows: 7 columns, 586 panels instead of 1024 of 4)
+  // the widest panel (up to 8 columns) whose n x B block fits in shared
+  // memory: every panel streams the whole matrix once, so fewer, wider panels
+  // stream less (4096 rows: 7 columns, 586 panels instead of 1024 of 4);
+  // wider than 8, the single-CTA panel factorization costs more than the
+  // passes it saves (2294 rows: 20.5 ms with 12 columns, 14.5 ms with 8)
   const size_t col = sizeof(double) * (size_t)n;
   if (8 * col <= kGjSmemLimit)
     gj_run<8>(n, a, inv, Bt, piv, idx, status, st);

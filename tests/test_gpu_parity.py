@@ -438,12 +438,12 @@ def test_ell_finest_level_matches_reference(refo, ordering):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("n", [1000, 3700, 4096])
+@pytest.mark.parametrize("n", [1000, 3000, 3700, 4096])
 def test_gpu_inverse_direct_single_level(n):
     """With no coarse levels and the direct coarse solver, the whole matrix is
     the coarsest level: it is densified on the GPU and inverted by the
-    blocked Gauss-Jordan (panels of 8 columns for 1000 rows, 7 for 3700 and
-    4096), so one cycle is an exact solve. The matrix is not diagonally
+    blocked Gauss-Jordan (panels of 8, 8, 7 and 7 columns for these sizes),
+    so one cycle is an exact solve. The matrix is not diagonally
     dominant (random-sign couplings on a grid pattern), so row pivoting is
     exercised; the solution is compared with numpy's dense solve."""
     rng = np.random.default_rng(n)

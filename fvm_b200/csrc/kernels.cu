@@ -421,13 +421,14 @@ __global__ void __launch_bounds__(BLOCK) k_jacobi_damped_tpr(SellView<T> a, int 
 
 template <class T>
 __global__ void k_restrict(int nc, const int* __restrict__ c2fRow, const int* __restrict__ c2fCol,
-                           const T* __restrict__ r, T* bc) {
+                           const T* __restrict__ r, T* bc, T* xc) {
   FVM_PDL();
   const int I = blockIdx.x * blockDim.x + threadIdx.x;
   if (I >= nc) return;
   T s = T(0);
   for (int k = c2fRow[I]; k < c2fRow[I + 1]; k++) s = s + r[c2fCol[k]];
   bc[I] = s;
+  if (xc) xc[I] = T(0);
 }
 
 // Fine-row residuals computed inside the restriction: rowSlice maps a fine
@@ -1044,11 +1045,16 @@ void spmv(const SellView<double>& a, int nSlices, const double* x, double* y, cu
 }
 template <class T>
 void restrict_sum(int nc, const int* c2fRow, const int* c2fCol, const T* r, T* bc, cudaStream_t st) {
-  pdl_launch(k_restrict<T>, ceil_div(nc, kBlock), kBlock, st, nc, c2fRow, c2fCol, r, bc);
+  pdl_launch(k_restrict<T>, ceil_div(nc, kBlock), kBlock, st, nc, c2fRow, c2fCol, r, bc, (T*)nullptr);
 }
 template <class T>
-void residual_restrict(const SellView<T>& a, const int* rowSlice, int nc, const int* c2fRow,
-                       const int* c2fCol, const T* x, const T* b, T* bc, T* xc, cudaStream_t st) {
+void residual_restrict(const SellView<T>& a, int nSlices, const int* rowSlice, int nc, const int* c2fRow,
+                       const int* c2fCol, const T* x, const T* b, T* bc, T* xc, T* r, cudaStream_t st) {
+  if (r) {
+    residual<T>(a, nSlices, x, b, r, nullptr, st);
+    pdl_launch(k_restrict<T>, ceil_div(nc, kBlock), kBlock, st, nc, c2fRow, c2fCol, (const T*)r, bc, xc);
+    return;
+  }
   pdl_launch(k_residual_restrict<T>, ceil_div(nc, kBlock), kBlock, st, a, rowSlice, nc, c2fRow, c2fCol, x, b, bc, xc);
 }
 template <class T>
@@ -1269,8 +1275,8 @@ void update_solution(int nCells, const int* perm, const double* delta, const Bou
   template void jacobi_damped<T>(const SellView<T>&, int, const T*, T*, const T*, T, cudaStream_t, RowPlan); \
   template void residual<T>(const SellView<T>&, int, const T*, const T*, T*, double*, cudaStream_t); \
   template void restrict_sum<T>(int, const int*, const int*, const T*, T*, cudaStream_t);        \
-  template void residual_restrict<T>(const SellView<T>&, const int*, int, const int*, const int*,   \
-                                     const T*, const T*, T*, T*, cudaStream_t);                  \
+  template void residual_restrict<T>(const SellView<T>&, int, const int*, int, const int*,        \
+                                     const int*, const T*, const T*, T*, T*, T*, cudaStream_t);   \
   template void zero<T>(int, T*, cudaStream_t);                                                  \
   template void prolong<T>(int, const int*, const T*, T*, cudaStream_t);                         \
   template void dense_solve<T>(int, const double*, const T*, T*, cudaStream_t);

@@ -81,11 +81,16 @@ void csr_residual_finish(int nPartials, const double* partials, double* l1, cuda
 // bc[I] = sum over fine rows i of aggregate I (ascending reference order) of r[i]
 template <class T>
 void restrict_sum(int nc, const int* c2fRow, const int* c2fCol, const T* r, T* bc, cudaStream_t st);
-// residual of the fine rows fused into the restriction (r never stored);
-// also zeroes the coarse x (xc may be null)
+// bc = restriction of the fine residual b + A x; also zeroes the coarse x
+// (xc may be null). r == null: one kernel, each coarse row computes its fine
+// rows' residuals itself (r never stored; the fine rows of an aggregate are
+// scattered over the matrix, so its loads are gathers). r != null: the
+// residual pass writes r with coalesced row loads, then a second kernel
+// gathers it per aggregate. Both sum the same products in the same order:
+// bitwise the same bc.
 template <class T>
-void residual_restrict(const SellView<T>& a, const int* rowSlice, int nc, const int* c2fRow,
-                       const int* c2fCol, const T* x, const T* b, T* bc, T* xc, cudaStream_t st);
+void residual_restrict(const SellView<T>& a, int nSlices, const int* rowSlice, int nc, const int* c2fRow,
+                       const int* c2fCol, const T* x, const T* b, T* bc, T* xc, T* r, cudaStream_t st);
 template <class T>
 void zero(int n, T* x, cudaStream_t st);
 // x[i] += xc[ci[i]]

@@ -253,7 +253,8 @@ void AmgHierarchy::build(std::vector<RefLevel>& levels, int finestLocalSize, con
   lap("cycle program");
   if (trace) {
     fprintf(stderr, "[fvm setup] levels:");
-    for (int l = 0; l < L; l++) fprintf(stderr, " %d(%dc)", lv_[l].n, lv_[l].nColors);
+    for (int l = 0; l < L; l++)
+      fprintf(stderr, " %d(%dc%s)", lv_[l].n, lv_[l].nColors, lv_[l].splitRestrict ? ",split" : "");
     fprintf(stderr, "\n");
   }
 }
@@ -274,7 +275,28 @@ std::mutex gPlanMu;
 std::map<PlanKey, dev::RowPlan> gPlanCache;  // per process: a shape is timed once
 constexpr int kTuneMinRows = 4096;           // smaller levels are launch-bound: default plan
 const dev::RowPlan kCandidatePlans[] = {{1, 256}, {1, 128}, {2, 256}, {2, 128}, {4, 256}, {4, 128}};
+struct SplitKey {
+  int n;
+  size_t entries;
+  int nCoarse;
+  bool f32;
+  bool operator<(const SplitKey& o) const {
+    return std::tie(n, entries, nCoarse, f32) < std::tie(o.n, o.entries, o.nCoarse, o.f32);
+  }
+};
+std::map<SplitKey, bool> gSplitCache;
 }  // namespace
+
+void AmgHierarchy::restrictPass(int l, bool split, cudaStream_t st) {
+  DevLevel& d = lv_[l];
+  DevLevel& c = lv_[l + 1];
+  if (opt_.precision == kMixed)
+    dev::residual_restrict<float>(d.view32(), d.nSlices, d.rowSlice, c.n, d.c2fRow, d.c2fCol, d.xF, d.bF, c.bF,
+                                  c.xF, split ? d.rF : nullptr, st);
+  else
+    dev::residual_restrict<double>(d.view64(), d.nSlices, d.rowSlice, c.n, d.c2fRow, d.c2fCol, d.x, d.b, c.b, c.x,
+                                   split ? d.r : nullptr, st);
+}
 
 void AmgHierarchy::smootherPass(int l, dev::RowPlan plan, cudaStream_t st) {
   DevLevel& d = lv_[l];
@@ -306,6 +328,22 @@ void AmgHierarchy::tunePlans() {
   cudaStream_t st = nullptr;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   bool touched = false;
+  // one warm-up and five timed runs, median
+  auto median_ms = [&](auto&& fn) {
+    fn();
+    std::vector<float> t;
+    for (int r = 0; r < 5; r++) {
+      CUDA_OK(cudaEventRecord(e0, st));
+      fn();
+      CUDA_OK(cudaEventRecord(e1, st));
+      CUDA_OK(cudaEventSynchronize(e1));
+      float ms = 0.f;
+      CUDA_OK(cudaEventElapsedTime(&ms, e0, e1));
+      t.push_back(ms);
+    }
+    std::sort(t.begin(), t.end());
+    return t[2];
+  };
   for (int l = 0; l < L; l++) {
     DevLevel& d = lv_[l];
     d.plan = dev::RowPlan();
@@ -335,26 +373,43 @@ void AmgHierarchy::tunePlans() {
     float best = std::numeric_limits<float>::max();
     dev::RowPlan bestPlan;
     for (const dev::RowPlan& p : kCandidatePlans) {
-      smootherPass(l, p, st);  // warm-up
-      std::vector<float> t;
-      for (int r = 0; r < 5; r++) {
-        CUDA_OK(cudaEventRecord(e0, st));
-        smootherPass(l, p, st);
-        CUDA_OK(cudaEventRecord(e1, st));
-        CUDA_OK(cudaEventSynchronize(e1));
-        float ms = 0.f;
-        CUDA_OK(cudaEventElapsedTime(&ms, e0, e1));
-        t.push_back(ms);
-      }
-      std::sort(t.begin(), t.end());
-      if (t[2] < best) {
-        best = t[2];
+      const float t = median_ms([&] { smootherPass(l, p, st); });
+      if (t < best) {
+        best = t;
         bestPlan = p;
       }
     }
     d.plan = bestPlan;
     std::lock_guard<std::mutex> lock(gPlanMu);
     gPlanCache[key] = bestPlan;
+  }
+  // residual + restriction of each level above the coarsest: the fused
+  // kernel (gathers of scattered fine rows) or the coalesced residual pass
+  // followed by the gather of r, whichever is faster (same result bits)
+  for (int l = 0; l + 1 < L; l++) {
+    DevLevel& d = lv_[l];
+    d.splitRestrict = false;
+    if (!opt_.autotune || d.n < kTuneMinRows) continue;
+    const SplitKey key{d.n, d.entries, lv_[l + 1].n, f32};
+    {
+      std::lock_guard<std::mutex> lock(gPlanMu);
+      auto it = gSplitCache.find(key);
+      if (it != gSplitCache.end()) {
+        d.splitRestrict = it->second;
+        continue;
+      }
+    }
+    if (!st) {
+      CUDA_OK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+      CUDA_OK(cudaEventCreate(&e0));
+      CUDA_OK(cudaEventCreate(&e1));
+    }
+    touched = true;
+    const float fused = median_ms([&] { restrictPass(l, false, st); });
+    const float split = median_ms([&] { restrictPass(l, true, st); });
+    d.splitRestrict = split < fused;
+    std::lock_guard<std::mutex> lock(gPlanMu);
+    gSplitCache[key] = d.splitRestrict;
   }
   if (st) {
     CUDA_OK(cudaStreamSynchronize(st));
@@ -691,8 +746,8 @@ void AmgHierarchy::cycle(CycleType t, int l, cudaStream_t st) {
   sweeps<T>(opt_.nPreSweeps, l, st);
   if (!coarsest) {
     DevLevel& c = lv_[l + 1];
-    dev::residual_restrict<T>(view<T>(d), d.rowSlice, c.n, d.c2fRow, d.c2fCol, vec_x<T>(d),
-                              vec_b<T>(d), vec_b<T>(c), vec_x<T>(c), st);
+    dev::residual_restrict<T>(view<T>(d), d.nSlices, d.rowSlice, c.n, d.c2fRow, d.c2fCol, vec_x<T>(d),
+                              vec_b<T>(d), vec_b<T>(c), vec_x<T>(c), d.splitRestrict ? vec_r<T>(d) : nullptr, st);
     cycle<T>(t, l + 1, st);
     if (t == kWCycle)
       cycle<T>(kWCycle, l + 1, st);

@@ -90,6 +90,7 @@ struct DevLevel {
   int nPartials = 0;
   int4* meta = nullptr;  // per slice: first row, rows, entry offset, width
   dev::RowPlan plan;     // launch plan of this level's smoother (SELL-32 levels)
+  bool splitRestrict = false;  // residual pass + gather instead of the fused restriction
   int ellWidth = 0;  // > 0: ELL-32 layout (colorSliceStart then holds rows)
   dev::SellView<double> view64() const {
     return {n, sliceRow, sliceRows, sliceOff, cols, vals, diag, meta, ellWidth};
@@ -205,6 +206,8 @@ class AmgHierarchy {
   void tunePlans();
   // one smoother pass of level l with a given plan (what the tuner times)
   void smootherPass(int l, dev::RowPlan plan, cudaStream_t st);
+  // level l's residual restricted to level l + 1, fused or split
+  void restrictPass(int l, bool split, cudaStream_t st);
   void genCycle(CycleType t, int l, std::vector<dev::Phase>& out) const;
   void genSweeps(int n, int l, std::vector<dev::Phase>& out) const;
   bool programReady_ = false;

@@ -1078,6 +1078,128 @@ constexpr int kGjMaxPanel = 8;
 // kernel's static reduction arrays
 constexpr size_t kGjSmemLimit = 227 * 1024 - 2048;
 size_t gj_align(size_t b) { return (b + 255) & ~size_t(255); }
+
+// ---- Gauss-Jordan without pivoting (diagonally dominant matrices) ----------
+// The in-place sweep over a panel K = [k0, k0 + nb) of pivots, with
+// D = A[K][K]:
+//   A[K][K] <- D^-1          A[K][j] <- D^-1 A[K][j]                 (j not in K)
+//   A[i][K] <- -A[i][K] D^-1 A[i][j] <- A[i][j] - A[i][K] D^-1 A[K][j] (i, j not in K)
+// After all panels A holds its inverse. Without pivot searches each panel
+// is ONE kernel over the whole matrix: every CTA inverts the small D itself
+// (from a copy of the panel's rows) and updates a 32 x 128 tile. The
+// panel's old rows A[K][:] and columns A[:][K] are read from side buffers
+// (R, C) that the previous panel's kernel filled while writing them, so no
+// CTA reads a value another CTA of the same launch writes. Diagonal
+// dominance keeps every pivot away from zero and the growth bounded, which
+// is why the caller takes this path only for diagonally dominant levels.
+constexpr int kNpB = 16;    // panel width
+constexpr int kNpTJ = 128;  // columns per CTA, one per thread in x
+constexpr int kNpTI = 32;   // rows per CTA, 16 per thread
+
+// C[i * kNpB + t] = A[i][k0 + t], R[t * n + j] = A[k0 + t][j] (t < nb; 0 beyond)
+__global__ void k_gjnp_extract(int n, int k0, int nb, const double* __restrict__ A, double* __restrict__ C,
+                               double* __restrict__ R) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  for (int t = 0; t < kNpB; t++) {
+    R[(size_t)t * n + j] = t < nb ? A[(size_t)(k0 + t) * n + j] : 0.0;
+    C[(size_t)j * kNpB + t] = t < nb ? A[(size_t)j * n + k0 + t] : 0.0;
+  }
+}
+
+// One panel [k0, k0 + nb) over the whole matrix; also fills Cn / Rn with the
+// next panel's [k1, k1 + nb1) new columns / rows. Launch: grid
+// (ceil(n / kNpTJ), ceil(n / kNpTI)), 256 threads.
+__global__ void __launch_bounds__(256) k_gjnp_update(int n, int k0, int nb, double* __restrict__ A,
+                                                     const double* __restrict__ C, const double* __restrict__ R,
+                                                     double* __restrict__ Cn, double* __restrict__ Rn, int k1,
+                                                     int nb1, int* __restrict__ status) {
+  __shared__ double D[kNpB][kNpB + 1];
+  __shared__ double Ct[kNpTI][kNpB];
+  const int tid = threadIdx.x;
+  const int i0 = blockIdx.y * kNpTI;
+  {
+    const int r = tid / kNpB, c = tid % kNpB;  // 256 threads: one entry of D each
+    D[r][c] = (r < nb && c < nb) ? R[(size_t)r * n + k0 + c] : (r == c ? 1.0 : 0.0);
+  }
+  for (int e = tid; e < kNpTI * kNpB; e += blockDim.x) {
+    const int r = e / kNpB, t = e % kNpB;
+    Ct[r][t] = (i0 + r < n && t < nb) ? C[(size_t)(i0 + r) * kNpB + t] : 0.0;
+  }
+  __syncthreads();
+  {
+    // D <- D^-1 by the scalar sweep over its pivots (identity padding
+    // beyond nb leaves those rows and columns unchanged)
+    const int r = tid / kNpB, c = tid % kNpB;
+    for (int t = 0; t < kNpB; t++) {
+      const double p = D[t][t];
+      const double drt = D[r][t], dtc = D[t][c], drc = D[r][c];
+      __syncthreads();
+      double v;
+      if (r == t && c == t)
+        v = 1.0 / p;
+      else if (r == t)
+        v = dtc / p;
+      else if (c == t)
+        v = -drt / p;
+      else
+        v = drc - drt * (dtc / p);
+      D[r][c] = v;
+      if (p == 0.0 && tid == 0 && blockIdx.x == 0 && blockIdx.y == 0) atomicExch(status, 1);
+      __syncthreads();
+    }
+  }
+  const int tx = tid & (kNpTJ - 1), ty = tid / kNpTJ;
+  const int j = blockIdx.x * kNpTJ + tx;
+  if (j >= n) return;
+  const bool jK = j >= k0 && j < k0 + nb;
+  // this column's new pivot-row values rj[t] = (D^-1 A[K][j])[t]
+  double rj[kNpB];
+  {
+    double rs[kNpB];
+#pragma unroll
+    for (int t = 0; t < kNpB; t++) rs[t] = t < nb ? R[(size_t)t * n + j] : 0.0;
+#pragma unroll
+    for (int t = 0; t < kNpB; t++) {
+      double acc = 0.0;
+#pragma unroll
+      for (int u = 0; u < kNpB; u++) acc = acc + D[t][u] * rs[u];
+      rj[t] = acc;
+    }
+  }
+  const bool jNext = j >= k1 && j < k1 + nb1;
+#pragma unroll 4
+  for (int q = 0; q < kNpTI / 2; q++) {
+    const int r = ty + 2 * q;
+    const int i = i0 + r;
+    if (i >= n) break;
+    const size_t e = (size_t)i * n + j;
+    double v;
+    if (i >= k0 && i < k0 + nb) {
+      const int t = i - k0;
+      if (jK) {
+        v = D[t][j - k0];
+      } else {
+        v = 0.0;
+#pragma unroll
+        for (int u = 0; u < kNpB; u++) v = u == t ? rj[u] : v;  // registers, no local-memory index
+      }
+    } else if (jK) {
+      double acc = 0.0;
+#pragma unroll
+      for (int u = 0; u < kNpB; u++) acc = acc + Ct[r][u] * D[u][j - k0];
+      v = -acc;
+    } else {
+      double acc = 0.0;
+#pragma unroll
+      for (int t = 0; t < kNpB; t++) acc = acc + Ct[r][t] * rj[t];
+      v = A[e] - acc;
+    }
+    A[e] = v;
+    if (jNext) Cn[(size_t)i * kNpB + (j - k1)] = v;
+    if (i >= k1 && i < k1 + nb1) Rn[(size_t)(i - k1) * n + j] = v;
+  }
+}
 // Look-ahead: after panel p's row swaps, the next panel's columns are
 // updated first and factored on stream st while the rest of the matrix
 // takes panel p's update on a second stream (disjoint columns); panel p+1's
@@ -1124,13 +1246,38 @@ void gj_run(int n, double* a, double* inv, double* Bt, int* piv, int* idx, int* 
 }
 }  // namespace
 
+// scratch: [panel doubles][piv: n ints][idx: n ints][status]; the panel
+// doubles hold the pivoted path's Bt (kGjMaxPanel x n) or the unpivoted
+// path's two pairs of side buffers (4 x kNpB x n)
+constexpr int kGjScratchPanels = 4 * kNpB > kGjMaxPanel ? 4 * kNpB : kGjMaxPanel;
 size_t gauss_jordan_scratch_bytes(int n) {
-  return gj_align(sizeof(double) * kGjMaxPanel * (size_t)n) + 2 * gj_align(sizeof(int) * (size_t)n) +
+  return gj_align(sizeof(double) * kGjScratchPanels * (size_t)n) + 2 * gj_align(sizeof(int) * (size_t)n) +
          gj_align(sizeof(int));
 }
 const int* gauss_jordan_status(int n, const void* scratch) {
   const char* s = (const char*)scratch;
-  return (const int*)(s + gj_align(sizeof(double) * kGjMaxPanel * (size_t)n) + 2 * gj_align(sizeof(int) * (size_t)n));
+  return (const int*)(s + gj_align(sizeof(double) * kGjScratchPanels * (size_t)n) +
+                      2 * gj_align(sizeof(int) * (size_t)n));
+}
+void gauss_jordan_inverse_dominant(int n, double* a, void* scratch, cudaStream_t st) {
+  double* sb = (double*)scratch;
+  const size_t pn = (size_t)kNpB * n;
+  double* C[2] = {sb, sb + pn};
+  double* R[2] = {sb + 2 * pn, sb + 3 * pn};
+  int* status = (int*)gauss_jordan_status(n, scratch);
+  cudaMemsetAsync(status, 0, sizeof(int), st);
+  if (n <= 0) return;
+  k_gjnp_extract<<<ceil_div(n, kBlock), kBlock, 0, st>>>(n, 0, n < kNpB ? n : kNpB, a, C[0], R[0]);
+  const dim3 grid(ceil_div(n, kNpTJ), ceil_div(n, kNpTI));
+  int cur = 0;
+  for (int k0 = 0; k0 < n; k0 += kNpB) {
+    const int nb = n - k0 < kNpB ? n - k0 : kNpB;
+    const int k1 = k0 + nb;
+    const int nb1 = n - k1 < kNpB ? n - k1 : kNpB;
+    k_gjnp_update<<<grid, 256, 0, st>>>(n, k0, nb, a, C[cur], R[cur], C[cur ^ 1], R[cur ^ 1], k1, nb1 > 0 ? nb1 : 0,
+                                        status);
+    cur ^= 1;
+  }
 }
 namespace {
 // a (n x n, row-major, zeroed) += the SELL-32 level: one thread per row
@@ -1159,7 +1306,7 @@ void dense_from_sell(const SellView<double>& m, int nSlices, double* a, cudaStre
 void gauss_jordan_inverse(int n, double* a, double* inv, void* scratch, cudaStream_t st) {
   char* s = (char*)scratch;
   double* Bt = (double*)s;
-  int* piv = (int*)(s + gj_align(sizeof(double) * kGjMaxPanel * (size_t)n));
+  int* piv = (int*)(s + gj_align(sizeof(double) * kGjScratchPanels * (size_t)n));
   int* idx = piv + gj_align(sizeof(int) * (size_t)n) / sizeof(int);
   int* status = (int*)gauss_jordan_status(n, scratch);
   cudaMemsetAsync(status, 0, sizeof(int), st);

@@ -116,6 +116,10 @@ size_t gauss_jordan_scratch_bytes(int n);
 void gauss_jordan_inverse(int n, double* a, double* inv, void* scratch, cudaStream_t st);
 // device address of the status flag inside scratch
 const int* gauss_jordan_status(int n, const void* scratch);
+// In-place inverse of a diagonally dominant (by rows or by columns) dense
+// matrix `a` by blocked Gauss-Jordan without pivoting: one kernel per panel
+// of 16 pivots. Same scratch and status as gauss_jordan_inverse.
+void gauss_jordan_inverse_dominant(int n, double* a, void* scratch, cudaStream_t st);
 void cast_d2f(size_t n, const double* a, float* b, cudaStream_t st);
 
 // ---- vector ops ------------------------------------------------------------

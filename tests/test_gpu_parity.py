@@ -475,3 +475,42 @@ def test_gpu_inverse_direct_single_level(n):
     assert list(info["levelSizes"]) == []
     assert info["iterations"] == 1
     assert rel_l2(x, xref) <= 1e-11
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n", [1000, 2294, 3000, 4096])
+def test_gpu_inverse_dominant_single_level(n):
+    """A diagonally dominant single level (the shape of every diffusion
+    coarsest level) takes the unpivoted blocked Gauss-Jordan: panels of 16
+    pivots, the last one partial for all sizes here but 4096. One cycle is an
+    exact solve; the solution is compared with numpy's dense solve."""
+    rng = np.random.default_rng(7 * n)
+    nx = int(np.ceil(np.sqrt(n)))
+    rows = [[] for _ in range(n)]
+    for i in range(n):
+        for j in (i + 1, i + nx, i + 3 * nx + 5):
+            if j < n and (j != i + 1 or (i + 1) % nx):
+                rows[i].append((j, rng.uniform(-1.0, 1.0)))
+                rows[j].append((i, rng.uniform(-1.0, 1.0)))
+    row = np.zeros(n + 1, np.int32)
+    row[1:] = np.cumsum([len(r) for r in rows])
+    col = np.array([j for r in rows for j, _ in r], np.int32)
+    off = np.array([v for r in rows for _, v in r])
+    # weakly dominant rows with a few strict ones, signs of both kinds
+    absum = np.array([sum(abs(v) for _, v in r) for r in rows])
+    diag = -(absum + np.where(rng.uniform(size=n) < 0.05, rng.uniform(0.01, 0.5, n), 0.0))
+    diag[rng.uniform(size=n) < 0.3] *= -1.0
+    diag[absum == 0] = -1.0
+    b = rng.normal(size=n)
+    A = np.diag(diag)
+    for i in range(n):
+        for k in range(row[i], row[i + 1]):
+            A[i, col[k]] += off[k]
+    xref = np.linalg.solve(A, -b)
+    amg = _amg(maxCoarseLevels=0, relativeTolerance=1e-10, nMaxIterations=5)
+    amg.coarseSolver = fvmbaseExt.AMG.COARSE_DIRECT
+    amg.coarsestSize = 4096
+    x, info = amg.solve_csr(row, col, diag, off, b)
+    assert list(info["levelSizes"]) == []
+    assert info["iterations"] == 1
+    assert rel_l2(x, xref) <= 1e-10

@@ -1085,16 +1085,19 @@ size_t gj_align(size_t b) { return (b + 255) & ~size_t(255); }
 //   A[K][K] <- D^-1          A[K][j] <- D^-1 A[K][j]                 (j not in K)
 //   A[i][K] <- -A[i][K] D^-1 A[i][j] <- A[i][j] - A[i][K] D^-1 A[K][j] (i, j not in K)
 // After all panels A holds its inverse. Without pivot searches each panel
-// is ONE kernel over the whole matrix: every CTA inverts the small D itself
-// (from a copy of the panel's rows) and updates a 32 x 128 tile. The
+// is ONE kernel over the whole matrix, each CTA a 64 x 128 tile. The
 // panel's old rows A[K][:] and columns A[:][K] are read from side buffers
 // (R, C) that the previous panel's kernel filled while writing them, so no
-// CTA reads a value another CTA of the same launch writes. Diagonal
+// CTA reads a value another CTA of the same launch writes; D^-1 comes
+// ready-made: the last CTA of the previous launch to finish (a fence and
+// a ticket counter, no waiting) inverts the next panel's block. Diagonal
 // dominance keeps every pivot away from zero and the growth bounded, which
 // is why the caller takes this path only for diagonally dominant levels.
+// This is not a reference computation, so the products use fused
+// multiply-adds (__fma_rn) although the file is built without contraction.
 constexpr int kNpB = 16;    // panel width
 constexpr int kNpTJ = 128;  // columns per CTA, one per thread in x
-constexpr int kNpTI = 32;   // rows per CTA, 16 per thread
+constexpr int kNpTI = 64;   // rows per CTA, 32 per thread
 
 // C[i * kNpB + t] = A[i][k0 + t], R[t * n + j] = A[k0 + t][j] (t < nb; 0 beyond)
 __global__ void k_gjnp_extract(int n, int k0, int nb, const double* __restrict__ A, double* __restrict__ C,
@@ -1107,98 +1110,127 @@ __global__ void k_gjnp_extract(int n, int k0, int nb, const double* __restrict__
   }
 }
 
-// One panel [k0, k0 + nb) over the whole matrix; also fills Cn / Rn with the
-// next panel's [k1, k1 + nb1) new columns / rows. Launch: grid
-// (ceil(n / kNpTJ), ceil(n / kNpTI)), 256 threads.
+// Dout = inverse of the panel's pivot block R[t][k0 + c] (t, c < nb; the
+// identity beyond), by the scalar sweep over its pivots; 256 threads, one
+// entry each. *status = 1 on a zero pivot.
+__device__ void gjnp_invert_block(int n, int k0, int nb, const double* R, double* Dout, int* status) {
+  __shared__ double D[2][kNpB][kNpB + 1];
+  const int tid = threadIdx.x, r = tid / kNpB, c = tid % kNpB;
+  D[0][r][c] = (r < nb && c < nb) ? __ldcg(R + (size_t)r * n + k0 + c) : (r == c ? 1.0 : 0.0);
+  __syncthreads();
+  int cur = 0;
+  for (int t = 0; t < kNpB; t++) {
+    const double p = D[cur][t][t];
+    const double ip = 1.0 / p;
+    const double drt = D[cur][r][t], dtc = D[cur][t][c], drc = D[cur][r][c];
+    double v;
+    if (r == t && c == t)
+      v = ip;
+    else if (r == t)
+      v = dtc * ip;
+    else if (c == t)
+      v = -drt * ip;
+    else
+      v = __fma_rn(-drt, dtc * ip, drc);
+    D[cur ^ 1][r][c] = v;
+    if (p == 0.0 && tid == 0) atomicExch(status, 1);
+    cur ^= 1;
+    __syncthreads();
+  }
+  Dout[r * kNpB + c] = D[cur][r][c];
+}
+
+__global__ void __launch_bounds__(256) k_gjnp_first(int n, int nb, const double* __restrict__ R, double* Dout,
+                                                    int* status) {
+  gjnp_invert_block(n, 0, nb, R, Dout, status);
+}
+
+// One panel [k0, k0 + nb) over the whole matrix (Dinv = its pivot block's
+// inverse); also fills Cn / Rn with the next panel's [k1, k1 + nb1) new
+// columns / rows and, in the launch's last CTA, Dnext. Launch: grid
+// (ceil(n / kNpTJ), ceil(n / kNpTI)), 256 threads; *ticket is 0 on entry
+// and left 0.
 __global__ void __launch_bounds__(256) k_gjnp_update(int n, int k0, int nb, double* __restrict__ A,
                                                      const double* __restrict__ C, const double* __restrict__ R,
-                                                     double* __restrict__ Cn, double* __restrict__ Rn, int k1,
-                                                     int nb1, int* __restrict__ status) {
+                                                     const double* __restrict__ Dinv, double* __restrict__ Cn,
+                                                     double* __restrict__ Rn, double* __restrict__ Dnext, int k1,
+                                                     int nb1, unsigned* ticket, int* status) {
   __shared__ double D[kNpB][kNpB + 1];
   __shared__ double Ct[kNpTI][kNpB];
+  __shared__ bool last;
   const int tid = threadIdx.x;
   const int i0 = blockIdx.y * kNpTI;
-  {
-    const int r = tid / kNpB, c = tid % kNpB;  // 256 threads: one entry of D each
-    D[r][c] = (r < nb && c < nb) ? R[(size_t)r * n + k0 + c] : (r == c ? 1.0 : 0.0);
-  }
+  D[tid / kNpB][tid % kNpB] = Dinv[tid];
   for (int e = tid; e < kNpTI * kNpB; e += blockDim.x) {
     const int r = e / kNpB, t = e % kNpB;
     Ct[r][t] = (i0 + r < n && t < nb) ? C[(size_t)(i0 + r) * kNpB + t] : 0.0;
   }
   __syncthreads();
-  {
-    // D <- D^-1 by the scalar sweep over its pivots (identity padding
-    // beyond nb leaves those rows and columns unchanged)
-    const int r = tid / kNpB, c = tid % kNpB;
-    for (int t = 0; t < kNpB; t++) {
-      const double p = D[t][t];
-      const double drt = D[r][t], dtc = D[t][c], drc = D[r][c];
-      __syncthreads();
-      double v;
-      if (r == t && c == t)
-        v = 1.0 / p;
-      else if (r == t)
-        v = dtc / p;
-      else if (c == t)
-        v = -drt / p;
-      else
-        v = drc - drt * (dtc / p);
-      D[r][c] = v;
-      if (p == 0.0 && tid == 0 && blockIdx.x == 0 && blockIdx.y == 0) atomicExch(status, 1);
-      __syncthreads();
-    }
-  }
   const int tx = tid & (kNpTJ - 1), ty = tid / kNpTJ;
   const int j = blockIdx.x * kNpTJ + tx;
-  if (j >= n) return;
-  const bool jK = j >= k0 && j < k0 + nb;
-  // this column's new pivot-row values rj[t] = (D^-1 A[K][j])[t]
-  double rj[kNpB];
-  {
-    double rs[kNpB];
+  if (j < n) {
+    const bool jK = j >= k0 && j < k0 + nb;
+    // this column's new pivot-row values rj[t] = (D^-1 A[K][j])[t]
+    double rj[kNpB];
+    {
+      double rs[kNpB];
 #pragma unroll
-    for (int t = 0; t < kNpB; t++) rs[t] = t < nb ? R[(size_t)t * n + j] : 0.0;
+      for (int t = 0; t < kNpB; t++) rs[t] = t < nb ? R[(size_t)t * n + j] : 0.0;
 #pragma unroll
-    for (int t = 0; t < kNpB; t++) {
-      double acc = 0.0;
+      for (int t = 0; t < kNpB; t++) {
+        double acc = 0.0;
 #pragma unroll
-      for (int u = 0; u < kNpB; u++) acc = acc + D[t][u] * rs[u];
-      rj[t] = acc;
-    }
-  }
-  const bool jNext = j >= k1 && j < k1 + nb1;
-#pragma unroll 4
-  for (int q = 0; q < kNpTI / 2; q++) {
-    const int r = ty + 2 * q;
-    const int i = i0 + r;
-    if (i >= n) break;
-    const size_t e = (size_t)i * n + j;
-    double v;
-    if (i >= k0 && i < k0 + nb) {
-      const int t = i - k0;
-      if (jK) {
-        v = D[t][j - k0];
-      } else {
-        v = 0.0;
-#pragma unroll
-        for (int u = 0; u < kNpB; u++) v = u == t ? rj[u] : v;  // registers, no local-memory index
+        for (int u = 0; u < kNpB; u++) acc = __fma_rn(D[t][u], rs[u], acc);
+        rj[t] = acc;
       }
-    } else if (jK) {
-      double acc = 0.0;
-#pragma unroll
-      for (int u = 0; u < kNpB; u++) acc = acc + Ct[r][u] * D[u][j - k0];
-      v = -acc;
-    } else {
-      double acc = 0.0;
-#pragma unroll
-      for (int t = 0; t < kNpB; t++) acc = acc + Ct[r][t] * rj[t];
-      v = A[e] - acc;
     }
-    A[e] = v;
-    if (jNext) Cn[(size_t)i * kNpB + (j - k1)] = v;
-    if (i >= k1 && i < k1 + nb1) Rn[(size_t)(i - k1) * n + j] = v;
+    const bool jNext = j >= k1 && j < k1 + nb1;
+#pragma unroll 4
+    for (int q = 0; q < kNpTI / 2; q++) {
+      const int r = ty + 2 * q;
+      const int i = i0 + r;
+      if (i >= n) break;
+      const size_t e = (size_t)i * n + j;
+      double v;
+      if (i >= k0 && i < k0 + nb) {
+        const int t = i - k0;
+        if (jK) {
+          v = D[t][j - k0];
+        } else {
+          v = 0.0;
+#pragma unroll
+          for (int u = 0; u < kNpB; u++) v = u == t ? rj[u] : v;  // registers, no local-memory index
+        }
+      } else if (jK) {
+        double acc = 0.0;
+#pragma unroll
+        for (int u = 0; u < kNpB; u++) acc = __fma_rn(Ct[r][u], D[u][j - k0], acc);
+        v = -acc;
+      } else {
+        double acc = A[e];
+#pragma unroll
+        for (int t = 0; t < kNpB; t++) acc = __fma_rn(-Ct[r][t], rj[t], acc);
+        v = acc;
+      }
+      A[e] = v;
+      if (jNext) Cn[(size_t)i * kNpB + (j - k1)] = v;
+      if (i >= k1 && i < k1 + nb1) Rn[(size_t)(i - k1) * n + j] = v;
+    }
   }
+  if (nb1 <= 0) return;  // the last panel: no next block to invert
+  // the last CTA to finish inverts the next panel's pivot block: every
+  // other CTA's writes of Rn are visible to it after their fence and its own
+  __syncthreads();
+  if (tid == 0) {
+    __threadfence();
+    const unsigned done = atomicAdd(ticket, 1u);
+    last = done == gridDim.x * gridDim.y - 1;
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  gjnp_invert_block(n, k1, nb1, Rn, Dnext, status);
+  if (tid == 0) *ticket = 0u;
 }
 // Look-ahead: after panel p's row swaps, the next panel's columns are
 // updated first and factored on stream st while the rest of the matrix
@@ -1250,32 +1282,40 @@ void gj_run(int n, double* a, double* inv, double* Bt, int* piv, int* idx, int* 
 // doubles hold the pivoted path's Bt (kGjMaxPanel x n) or the unpivoted
 // path's two pairs of side buffers (4 x kNpB x n)
 constexpr int kGjScratchPanels = 4 * kNpB > kGjMaxPanel ? 4 * kNpB : kGjMaxPanel;
+// the panel doubles, plus the unpivoted path's two inverted pivot blocks
+// and its ticket counter
+size_t gj_panel_bytes(int n) {
+  return gj_align(sizeof(double) * ((size_t)kGjScratchPanels * n + 2 * kNpB * kNpB + 1));
+}
 size_t gauss_jordan_scratch_bytes(int n) {
-  return gj_align(sizeof(double) * kGjScratchPanels * (size_t)n) + 2 * gj_align(sizeof(int) * (size_t)n) +
-         gj_align(sizeof(int));
+  return gj_panel_bytes(n) + 2 * gj_align(sizeof(int) * (size_t)n) + gj_align(sizeof(int));
 }
 const int* gauss_jordan_status(int n, const void* scratch) {
   const char* s = (const char*)scratch;
-  return (const int*)(s + gj_align(sizeof(double) * kGjScratchPanels * (size_t)n) +
-                      2 * gj_align(sizeof(int) * (size_t)n));
+  return (const int*)(s + gj_panel_bytes(n) + 2 * gj_align(sizeof(int) * (size_t)n));
 }
 void gauss_jordan_inverse_dominant(int n, double* a, void* scratch, cudaStream_t st) {
   double* sb = (double*)scratch;
   const size_t pn = (size_t)kNpB * n;
   double* C[2] = {sb, sb + pn};
   double* R[2] = {sb + 2 * pn, sb + 3 * pn};
+  double* Dv[2] = {sb + 4 * pn, sb + 4 * pn + kNpB * kNpB};
+  unsigned* ticket = (unsigned*)(sb + 4 * pn + 2 * kNpB * kNpB);
   int* status = (int*)gauss_jordan_status(n, scratch);
   cudaMemsetAsync(status, 0, sizeof(int), st);
+  cudaMemsetAsync(ticket, 0, sizeof(unsigned), st);
   if (n <= 0) return;
-  k_gjnp_extract<<<ceil_div(n, kBlock), kBlock, 0, st>>>(n, 0, n < kNpB ? n : kNpB, a, C[0], R[0]);
+  const int nb0 = n < kNpB ? n : kNpB;
+  k_gjnp_extract<<<ceil_div(n, kBlock), kBlock, 0, st>>>(n, 0, nb0, a, C[0], R[0]);
+  k_gjnp_first<<<1, 256, 0, st>>>(n, nb0, R[0], Dv[0], status);
   const dim3 grid(ceil_div(n, kNpTJ), ceil_div(n, kNpTI));
   int cur = 0;
   for (int k0 = 0; k0 < n; k0 += kNpB) {
     const int nb = n - k0 < kNpB ? n - k0 : kNpB;
     const int k1 = k0 + nb;
     const int nb1 = n - k1 < kNpB ? n - k1 : kNpB;
-    k_gjnp_update<<<grid, 256, 0, st>>>(n, k0, nb, a, C[cur], R[cur], C[cur ^ 1], R[cur ^ 1], k1, nb1 > 0 ? nb1 : 0,
-                                        status);
+    k_gjnp_update<<<grid, 256, 0, st>>>(n, k0, nb, a, C[cur], R[cur], Dv[cur], C[cur ^ 1], R[cur ^ 1], Dv[cur ^ 1],
+                                        k1, nb1 > 0 ? nb1 : 0, ticket, status);
     cur ^= 1;
   }
 }
@@ -1306,7 +1346,7 @@ void dense_from_sell(const SellView<double>& m, int nSlices, double* a, cudaStre
 void gauss_jordan_inverse(int n, double* a, double* inv, void* scratch, cudaStream_t st) {
   char* s = (char*)scratch;
   double* Bt = (double*)s;
-  int* piv = (int*)(s + gj_align(sizeof(double) * kGjScratchPanels * (size_t)n));
+  int* piv = (int*)(s + gj_panel_bytes(n));
   int* idx = piv + gj_align(sizeof(int) * (size_t)n) / sizeof(int);
   int* status = (int*)gauss_jordan_status(n, scratch);
   cudaMemsetAsync(status, 0, sizeof(int), st);

@@ -1098,6 +1098,7 @@ size_t gj_align(size_t b) { return (b + 255) & ~size_t(255); }
 constexpr int kNpB = 16;    // panel width
 constexpr int kNpTJ = 128;  // columns per CTA, one per thread in x
 constexpr int kNpTI = 64;   // rows per CTA, 32 per thread
+constexpr int kNpGroup = 4; // rows whose loads are issued together
 
 // C[i * kNpB + t] = A[i][k0 + t], R[t * n + j] = A[k0 + t][j] (t < nb; 0 beyond)
 __global__ void k_gjnp_extract(int n, int k0, int nb, const double* __restrict__ A, double* __restrict__ C,
@@ -1150,7 +1151,7 @@ __global__ void __launch_bounds__(256) k_gjnp_first(int n, int nb, const double*
 // columns / rows and, in the launch's last CTA, Dnext. Launch: grid
 // (ceil(n / kNpTJ), ceil(n / kNpTI)), 256 threads; *ticket is 0 on entry
 // and left 0.
-__global__ void __launch_bounds__(256) k_gjnp_update(int n, int k0, int nb, double* __restrict__ A,
+__global__ void __launch_bounds__(256, 3) k_gjnp_update(int n, int k0, int nb, double* __restrict__ A,
                                                      const double* __restrict__ C, const double* __restrict__ R,
                                                      const double* __restrict__ Dinv, double* __restrict__ Cn,
                                                      double* __restrict__ Rn, double* __restrict__ Dnext, int k1,
@@ -1185,11 +1186,22 @@ __global__ void __launch_bounds__(256) k_gjnp_update(int n, int k0, int nb, doub
       }
     }
     const bool jNext = j >= k1 && j < k1 + nb1;
-#pragma unroll 4
-    for (int q = 0; q < kNpTI / 2; q++) {
-      const int r = ty + 2 * q;
+    const bool full = i0 + kNpTI <= n;
+    // rows in groups of kNpGroup: a group's loads are all issued before its
+    // updates (a bound check per row would keep each load behind the
+    // previous row's 16-deep FMA chain)
+    for (int q0 = 0; q0 < kNpTI / 2; q0 += kNpGroup) {
+      double a[kNpGroup];
+#pragma unroll
+      for (int u = 0; u < kNpGroup; u++) {
+        const int i = i0 + ty + 2 * (q0 + u);
+        a[u] = (full || i < n) ? A[(size_t)i * n + j] : 0.0;
+      }
+#pragma unroll
+      for (int u = 0; u < kNpGroup; u++) {
+      const int r = ty + 2 * (q0 + u);
       const int i = i0 + r;
-      if (i >= n) break;
+      if (!full && i >= n) break;
       const size_t e = (size_t)i * n + j;
       double v;
       if (i >= k0 && i < k0 + nb) {
@@ -1207,7 +1219,7 @@ __global__ void __launch_bounds__(256) k_gjnp_update(int n, int k0, int nb, doub
         for (int u = 0; u < kNpB; u++) acc = __fma_rn(Ct[r][u], D[u][j - k0], acc);
         v = -acc;
       } else {
-        double acc = A[e];
+        double acc = a[u];
 #pragma unroll
         for (int t = 0; t < kNpB; t++) acc = __fma_rn(-Ct[r][t], rj[t], acc);
         v = acc;
@@ -1215,6 +1227,7 @@ __global__ void __launch_bounds__(256) k_gjnp_update(int n, int k0, int nb, doub
       A[e] = v;
       if (jNext) Cn[(size_t)i * kNpB + (j - k1)] = v;
       if (i >= k1 && i < k1 + nb1) Rn[(size_t)(i - k1) * n + j] = v;
+      }
     }
   }
   if (nb1 <= 0) return;  // the last panel: no next block to invert

@@ -1199,34 +1199,34 @@ __global__ void __launch_bounds__(256, 3) k_gjnp_update(int n, int k0, int nb, d
       }
 #pragma unroll
       for (int u = 0; u < kNpGroup; u++) {
-      const int r = ty + 2 * (q0 + u);
-      const int i = i0 + r;
-      if (!full && i >= n) break;
-      const size_t e = (size_t)i * n + j;
-      double v;
-      if (i >= k0 && i < k0 + nb) {
-        const int t = i - k0;
-        if (jK) {
-          v = D[t][j - k0];
+        const int r = ty + 2 * (q0 + u);
+        const int i = i0 + r;
+        if (!full && i >= n) break;
+        const size_t e = (size_t)i * n + j;
+        double v;
+        if (i >= k0 && i < k0 + nb) {
+          const int t = i - k0;
+          if (jK) {
+            v = D[t][j - k0];
+          } else {
+            v = 0.0;
+#pragma unroll
+            for (int s = 0; s < kNpB; s++) v = s == t ? rj[s] : v;  // registers, no local-memory index
+          }
+        } else if (jK) {
+          double acc = 0.0;
+#pragma unroll
+          for (int s = 0; s < kNpB; s++) acc = __fma_rn(Ct[r][s], D[s][j - k0], acc);
+          v = -acc;
         } else {
-          v = 0.0;
+          double acc = a[u];
 #pragma unroll
-          for (int u = 0; u < kNpB; u++) v = u == t ? rj[u] : v;  // registers, no local-memory index
+          for (int t = 0; t < kNpB; t++) acc = __fma_rn(-Ct[r][t], rj[t], acc);
+          v = acc;
         }
-      } else if (jK) {
-        double acc = 0.0;
-#pragma unroll
-        for (int u = 0; u < kNpB; u++) acc = __fma_rn(Ct[r][u], D[u][j - k0], acc);
-        v = -acc;
-      } else {
-        double acc = a[u];
-#pragma unroll
-        for (int t = 0; t < kNpB; t++) acc = __fma_rn(-Ct[r][t], rj[t], acc);
-        v = acc;
-      }
-      A[e] = v;
-      if (jNext) Cn[(size_t)i * kNpB + (j - k1)] = v;
-      if (i >= k1 && i < k1 + nb1) Rn[(size_t)(i - k1) * n + j] = v;
+        A[e] = v;
+        if (jNext) Cn[(size_t)i * kNpB + (j - k1)] = v;
+        if (i >= k1 && i < k1 + nb1) Rn[(size_t)(i - k1) * n + j] = v;
       }
     }
   }

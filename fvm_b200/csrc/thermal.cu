@@ -310,10 +310,14 @@ void ThermalModel::uploadFields() {
   if (tDirty_) CUDA_OK(cudaMemcpyAsync(dT_, T_.data(), cb, cudaMemcpyHostToDevice, stream_));
   if (kDirty_) CUDA_OK(cudaMemcpyAsync(dK_, k_.data(), cb, cudaMemcpyHostToDevice, stream_));
   if (srcDirty_) CUDA_OK(cudaMemcpyAsync(dSrc_, src_.data(), cb, cudaMemcpyHostToDevice, stream_));
-  if (rcDirty_) CUDA_OK(cudaMemcpyAsync(dRc_, rc_.data(), cb, cudaMemcpyHostToDevice, stream_));
-  if (tn1Dirty_) CUDA_OK(cudaMemcpyAsync(dTN1_, TN1_.data(), cb, cudaMemcpyHostToDevice, stream_));
+  // rho c and the previous step's T enter only the transient term: a steady
+  // model leaves them on the host (still dirty) until it becomes transient
+  const bool transient = opt_.transient;
+  if (rcDirty_ && transient) CUDA_OK(cudaMemcpyAsync(dRc_, rc_.data(), cb, cudaMemcpyHostToDevice, stream_));
+  if (tn1Dirty_ && transient) CUDA_OK(cudaMemcpyAsync(dTN1_, TN1_.data(), cb, cudaMemcpyHostToDevice, stream_));
   CUDA_OK(cudaStreamSynchronize(stream_));
-  tDirty_ = kDirty_ = srcDirty_ = rcDirty_ = tn1Dirty_ = false;
+  tDirty_ = kDirty_ = srcDirty_ = false;
+  if (transient) rcDirty_ = tn1Dirty_ = false;
   // boundary kinds and values (cheap; a change of kind or of a value the
   // matrix depends on changes the matrix)
   const int nB = (int)boundaryFaces_.size();

@@ -49,17 +49,6 @@ def load_peaks():
 # distributed plumbing (torchrun), kept optional for N=1
 
 
-# Outer iterations and V-cycles of the GPU plain FP64 run (standalone AMG
-# V(1,1), multicolour GS, inner relTol 0.1, outer 1e-10) per workload, as
-# measured on a B200: the reference arm's CPU time is extrapolated with them
-# when no run of the product arm in this checkout has recorded fresher ones.
-PLAIN_COUNTS = {
-    "config1": {"outer": 65, "cycles": 721},
-    "config3": {"outer": 19, "cycles": 3040},
-    "config4": {"outer": 10, "cycles": 45},
-}
-
-
 # dram__bytes_read.sum + dram__bytes_write.sum over the algorithmic bytes of
 # the finest-level FP32 GS colour launches in an ncu capture of the workload
 # (24.69 MB for a 502k-row colour of 24.10 MB algorithmic)
@@ -158,7 +147,7 @@ def make_workload(name: str):
     else:
         raise SystemExit("unknown workload " + name)
     mesh, f = gen(seed)
-    return mesh, f, desc, gen
+    return mesh, f, desc, gen, seed
 
 
 def train_learned(gen, inner_rel, seeds=(101, 102), n_outer=4, per_solve=3, steps=600, lr=1e-3):
@@ -220,6 +209,9 @@ def size_matched_copy_gbs(nbytes: float, reps: int = 7) -> float:
     return 16.0 * n / (ms * 1e-3) / 1e9
 
 
+HOST_SETUP = False  # --host-setup: the mixed path on the reference's host aggregation
+
+
 def solver_for(variant: str, inner_rel: float):
     """plain: the reference's default solver on the GPU -- standalone FP64
     AMG, V(1,1), multicolour Gauss-Seidel, coarsest level <= 100 rows
@@ -237,6 +229,7 @@ def solver_for(variant: str, inner_rel: float):
     amg.relativeTolerance = inner_rel
     amg.nMaxIterations = 200
     if variant in ("mixed", "learned"):
+        amg.setupOnDevice = not HOST_SETUP
         amg.precision = fvmbaseExt.AMG.MIXED
         amg.coarseSolver = fvmbaseExt.AMG.COARSE_DIRECT
         amg.coarsestSize = 4096
@@ -303,54 +296,73 @@ class Solve:
 # ---------------------------------------------------------------------------
 
 
-def cpu_reference(mesh, fields, plain_counts, inner_rel, desc, cores_note=True):
-    """Reference ThermalModel<double> + AMG (oracle/_ref, the reference's own
-    sources, -O3, one thread) on the same mesh. Bounded sample: one outer
-    iteration with 0 and with 3 V-cycles gives the per-outer cost (AMG setup,
-    linearization, residuals) and the per-cycle cost; time-to-solution is
-    extrapolated with the outer-iteration and cycle counts of the GPU plain
-    FP64 run (same aggregation, same outer loop)."""
+REF_CACHE = os.path.join(ROOT, ".ref_cache")
+
+
+def _host_cpu():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def reference_solve(workload, seed, mesh, fields, inner_rel, use_cache=True):
+    """One complete solve by the reference itself (oracle/_ref: its own
+    ThermalModel<double> + AMG sources, -O3, one thread -- the reference is
+    single-threaded) on the same mesh and fields: init, fields, advance()
+    until the outer L1 ratio is below 1e-10, with the reference's default
+    solver (AMG, 1 pre + 1 post Gauss-Seidel sweep, lexicographic order,
+    inner relTol `inner_rel`). Returns the measured wall time of advance(),
+    the reference's own outer-iteration count and the converged field.
+
+    The result is cached (.ref_cache/, not part of the source tree) keyed by
+    workload, seed and cell count, so that the product arm of the same run
+    states its fields' error against this solve without solving again."""
     from oracle import ref
     from fvm_b200.meshgen import extend_to_ghosts
 
+    n = mesh["nCells"]
+    path = os.path.join(REF_CACHE, "%s_seed%d_n%d_rel%g.npz" % (workload, seed, n, inner_rel))
+    if use_cache and os.path.exists(path):
+        z = np.load(path, allow_pickle=False)
+        return {"T": z["T"], "seconds": float(z["seconds"]), "outer": int(z["outer"]), "ratio": float(z["ratio"]),
+                "cpu": str(z["cpu"]), "cached": True}
     if not ref.available():
         return None
     r = ref.RefThermal(mesh)
-    kk = extend_to_ghosts(mesh, fields["k"])
-    ss = extend_to_ghosts(mesh, fields["s"])
-    rc = extend_to_ghosts(mesh, fields["rc"]) if "rc" in fields else None
-    extra = {"transient": True, "dt": 1e-3} if rc is not None else {}
+    extra = {"transient": True, "dt": 1e-3} if "rc" in fields else {}
+    r.set_options(n_pre=1, n_post=1, max_iter=200, lin_rel=inner_rel, rel=1e-10, **extra)
+    for gid, (kind, val) in fields["bc"].items():
+        r.set_bc(gid, 0 if kind == "T" else 1, [val] if kind == "T" else [None, val])
+    r.init()
+    r.set_field(1, extend_to_ghosts(mesh, fields["k"]))
+    r.set_field(2, extend_to_ghosts(mesh, fields["s"]))
+    if "rc" in fields:
+        r.set_field(3, extend_to_ghosts(mesh, fields["rc"]))
+    norms, sec = r.advance(500)
+    T = r.get_field(0)[:n].copy()
+    out = {"T": T, "seconds": sec, "outer": int(len(norms)), "ratio": float(norms[-1] / norms[0]),
+           "cpu": _host_cpu(), "cached": False}
+    del r
+    try:
+        os.makedirs(REF_CACHE, exist_ok=True)
+        np.savez(path, T=T, seconds=sec, outer=out["outer"], ratio=out["ratio"], cpu=out["cpu"])
+    except OSError:
+        pass
+    return out
 
-    def run(cycles):
-        r.set_options(n_pre=1, n_post=1, max_iter=1 + cycles, lin_rel=1e-30, rel=1e-30, **extra)
-        for gid, (kind, val) in fields["bc"].items():
-            r.set_bc(gid, 0 if kind == "T" else 1, [val] if kind == "T" else [None, val])
-        r.init()
-        r.set_field(1, kk)
-        r.set_field(2, ss)
-        if rc is not None:
-            r.set_field(3, rc)
-        _, sec = r.advance(1)
-        return sec
 
-    run(0)  # first linearization builds the reference's cached connectivity and gradient matrix
-    t_outer0 = run(0)
-    t_outer3 = run(3)
-    per_cycle = max(t_outer3 - t_outer0, 0.0) / 3.0
-    outer, cycles = plain_counts
-    est = outer * t_outer0 + cycles * per_cycle
-    return {
-        "value": est,
-        "unit": "s",
-        "cores": 1,
-        "kind": "reference",
-        "sample": ("reference ThermalModel<double>+AMG (1 pre/1 post GS sweep) on the full %d-cell mesh: one outer "
-                   "iteration with 0 and 3 V-cycles measured (%.3f s, %.3f s); time-to-solution = %d outer x %.3f s "
-                   "+ %d cycles x %.3f s (counts of the GPU FP64 run)" % (mesh["nCells"], t_outer0, t_outer3, outer,
-                                                                          t_outer0, cycles, per_cycle)),
-        "seconds_per_cycle": per_cycle,
-        "seconds_per_outer_setup": t_outer0,
-    }
+def reference_baseline(res, n_cells):
+    """cpu_baseline entry of a measured reference solve."""
+    return {"value": res["seconds"], "unit": "s", "cores": 1, "kind": "reference",
+            "sample": ("one complete solve of the same %d-cell workload by the compiled reference "
+                       "(ThermalModel<double> + AMG V(1,1), lexicographic Gauss-Seidel, one thread, host %s): "
+                       "%d outer iterations to outer L1 ratio %.2e, wall time of advance() measured%s"
+                       % (n_cells, res["cpu"], res["outer"], res["ratio"],
+                          " by the reference arm of this run" if res.get("cached") else ""))}
 
 
 def bench_batch(args, dist, peaks, peak_kind):
@@ -492,7 +504,12 @@ def main():
                     help="comma list of plain, plain-cg, mixed, learned (mixed + learned correction)")
     ap.add_argument("--train-steps", type=int, default=600)
     ap.add_argument("--batch-meshes", type=int, default=512, help="config2: number of meshes")
+    ap.add_argument("--host-setup", action="store_true",
+                    help="mixed path: AMG levels by the reference's greedy aggregation on the host instead of the "
+                         "GPU-built hierarchy")
     args = ap.parse_args()
+    global HOST_SETUP
+    HOST_SETUP = args.host_setup
 
     dist = Dist()
     peaks, peak_kind = load_peaks()
@@ -518,36 +535,29 @@ def main():
                                   "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
         dist.close()
         return
-    mesh, fields, desc, gen = make_workload(args.workload)
+    mesh, fields, desc, gen, seed = make_workload(args.workload)
     n_cells = mesh["nCells"]
 
     if args.impl == "reference":
         if dist.rank != 0:
             dist.close()
             return
-        # counts for the extrapolation come from a short GPU-free estimate:
-        # run the reference itself on one outer iteration to convergence of
-        # the inner solve is too long; use the recorded plain-path counts
-        counts_path = os.path.join(ROOT, "profiles", "plain_counts_%s.json" % args.workload)
-        if os.path.exists(counts_path):
-            counts = json.load(open(counts_path))
-        else:
-            counts = PLAIN_COUNTS.get(args.workload, {"outer": 10, "cycles": 60})
-        vals = []
-        base = None
-        for _ in range(max(1, args.steps)):
-            base = cpu_reference(mesh, fields, (counts["outer"], counts["cycles"]), args.inner_rel, desc)
-            if base is None:
-                print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libfvmref.so not built"}))
-                return
-            vals.append(base["value"])
-        v = statistics.median(vals)
+        # One complete reference solve, measured (a full solve of the 1.5M-cell
+        # workload takes about two minutes on one core, so the requested
+        # --steps / --warmup are not repeated: `steps` reports the solves run).
+        res = reference_solve(args.workload, seed, mesh, fields, args.inner_rel, use_cache=False)
+        if res is None:
+            print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libfvmref.so not built"}))
+            return
+        v = res["seconds"]
         line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "s", "n_gpus": args.gpus,
-                "steps": args.steps, "warmup": args.warmup, "ms_per_step": v * 1e3, "higher_is_better": False,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "steps": 1, "warmup": 0, "requested_steps": args.steps, "requested_warmup": args.warmup,
+                "ms_per_step": v * 1e3, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f64", "data": "synthetic",
                 "config": {"workload": desc, "cells": n_cells, "solver": "AMG, 1 pre + 1 post GS sweep",
-                           "inner_rel": args.inner_rel, "outer_rel": 1e-10, "counts_from": counts},
-                "cpu_baseline": {k: base[k] for k in ("value", "unit", "cores", "kind", "sample")},
+                           "inner_rel": args.inner_rel, "outer_rel": 1e-10},
+                "outer_iterations": res["outer"], "final_outer_ratio": res["ratio"],
+                "cpu_baseline": reference_baseline(res, n_cells),
                 "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
         return
@@ -612,7 +622,6 @@ def main():
     plain, mixed = results["plain"], results["mixed"]
     head = results.get("learned", mixed)  # the metric's mixed+learned solve
     rel_err = float(np.linalg.norm(head["T"] - plain["T"]) / np.linalg.norm(plain["T"]))
-    os.makedirs(os.path.join(ROOT, "profiles"), exist_ok=True)
 
     # dominant kernel of the product path: the finest-level FP32 GS pass
     pm = mixed["profile"]
@@ -625,7 +634,7 @@ def main():
                             if args.workload in NCU_TRAFFIC_RATIO else None),
                 "traffic_note": ("ncu DRAM read+write of captured colour launches of this pass (caches cold before "
                                  "each launch) over their algorithmic bytes, %.3f, times the pass's algorithmic "
-                                 "bytes (profiles/k_gs_color_ell_config1.md)" % NCU_TRAFFIC_RATIO[args.workload])
+                                 "bytes" % NCU_TRAFFIC_RATIO[args.workload])
                 if args.workload in NCU_TRAFFIC_RATIO else None,
                 "kernel": "k_gs_color_ell<float, W> (one pass over all colours, finest level)",
                 "peak_kind": peak_kind,
@@ -643,16 +652,21 @@ def main():
             "fp64_residual_vs_copy": roofline["fp64_residual"]["achieved"] / copy_gbs,
             "fp64_gs_pass_vs_copy": roofline["fp64_gs_pass"]["achieved"] / copy_gbs}
 
-    cpu = None
+    # the reference's own FP64 solve of the same workload: the CPU baseline
+    # and the oracle every field here is stated against (measured once per
+    # run: cached by the reference arm, or solved now, after the timed work)
+    cpu, vs_ref = None, {}
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
-        with open(os.path.join(ROOT, "profiles", "plain_counts_%s.json" % args.workload), "w") as f:
-            json.dump({"outer": plain["outer"], "cycles": plain["cycles"]}, f)
         try:
-            cpu = cpu_reference(mesh, fields, (plain["outer"], plain["cycles"]), args.inner_rel, desc)
-            if cpu:
-                cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
+            res = reference_solve(args.workload, seed, mesh, fields, args.inner_rel)
         except Exception as e:  # the baseline is reported, never required
+            res = None
             cpu = {"value": None, "unit": "s", "cores": 1, "kind": "reference", "sample": "failed: %s" % e}
+        if res is not None:
+            cpu = reference_baseline(res, n_cells)
+            Tr = res["T"]
+            vs_ref = {"%s_vs_reference_rel_l2" % ("mixed_learned" if v == "learned" else v.replace("-", "_")):
+                      float(np.linalg.norm(r["T"] - Tr) / np.linalg.norm(Tr)) for v, r in results.items()}
 
     if dist.rank == 0:
         line = {
@@ -686,6 +700,7 @@ def main():
             "mixed_without_learned_s": mixed["dev"],
             "speedup_vs_plain_fp64": plain["dev"] / head["dev"],
             "mixed_vs_plain_rel_l2": rel_err,
+            "error_vs_reference": vs_ref or None,
             "cells_per_s": n_cells * head["outer"] / head["dev"] * args.gpus,
             "counts": {k: {"outer": v["outer"], "cycles": v["cycles"], "setup_s": v["setup"],
                            "learned_steps": v["learned_steps"], "learned_kept": v["learned_kept"]}

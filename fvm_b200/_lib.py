@@ -44,6 +44,9 @@ class LinearOptions(ctypes.Structure):
         ("autotune", ctypes.c_int),
         ("planThreadsPerRow", ctypes.c_int),
         ("planBlock", ctypes.c_int),
+        ("setupOnDevice", ctypes.c_int),
+        ("matchRounds", ctypes.c_int),
+        ("matchBeta", ctypes.c_double),
     ]
 
 
@@ -109,6 +112,9 @@ _SIGS = {
     "fvm_thermal_history": (ctypes.c_int, [ctypes.c_void_p, c_double_p, ctypes.c_int, c_int_p]),
     "fvm_thermal_linear_system": (ctypes.c_int, [ctypes.c_void_p, c_double_p, c_double_p, c_double_p, c_int_p]),
     "fvm_thermal_launch_plans": (ctypes.c_int, [ctypes.c_void_p, c_int_p, c_int_p, c_int_p, ctypes.c_int]),
+    "fvm_thermal_level_matrix": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, c_int_p, c_int_p, c_int_p, c_int_p,
+                                                 c_double_p, c_double_p, ctypes.c_int]),
+    "fvm_thermal_profile_levels": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, c_int_p, c_double_p, ctypes.c_int]),
     "fvm_thermal_hierarchy": (ctypes.c_int, [ctypes.c_void_p, c_int_p, c_int_p, ctypes.c_int, c_int_p,
                                              ctypes.c_int]),
     "fvm_thermal_profile": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, c_double_p]),

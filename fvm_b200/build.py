@@ -7,6 +7,9 @@ that it travels with the source tree. Host code is compiled with
 -ffp-contract=off and device code with -fmad=false: the mesh geometry,
 matrix coefficients and AMG setup must round exactly like the reference's
 scalar C++ for the integer setup (aggregation) to match it bit for bit.
+Files whose results need no bitwise match with the reference (the learned
+network, the GPU-built hierarchy of the mixed-precision path) are compiled
+with fused multiply-adds (FMA_SOURCES).
 """
 from __future__ import annotations
 
@@ -24,11 +27,13 @@ LIB = os.path.join(HERE, "libfvm_b200.so")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CXX_FLAGS = ["-O3", "-std=c++17", "-fPIC", "-ffp-contract=off", "-Wall", "-Wno-unused-function"]
-NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-fmad=false", "--expt-relaxed-constexpr",
+NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--expt-relaxed-constexpr",
               "-Xcompiler", "-fPIC,-ffp-contract=off"] + ARCH
 
 HOST_SOURCES = ["mesh.cpp", "amg_setup.cpp", "capi.cpp"]
-CUDA_SOURCES = ["kernels.cu", "solver.cu", "thermal.cu", "residual_noalloc.cu", "cycle_program.cu", "learned.cu"]
+CUDA_SOURCES = ["kernels.cu", "solver.cu", "thermal.cu", "residual_noalloc.cu", "learned.cu", "amg_device.cu"]
+# device code free to contract a * b + c into one rounding
+FMA_SOURCES = {"learned.cu", "amg_device.cu"}
 
 
 def _nvcc() -> str:
@@ -80,7 +85,8 @@ def build(verbose: bool = False, force: bool = False) -> str:
         obj = os.path.join(OBJ, f + ".o")
         objs.append(obj)
         if force or _newer([src] + headers, obj):
-            jobs.append([nvcc] + NVCC_FLAGS + inc + ["-c", src, "-o", obj])
+            fmad = ["-fmad=true"] if f in FMA_SOURCES else ["-fmad=false"]
+            jobs.append([nvcc] + NVCC_FLAGS + fmad + inc + ["-c", src, "-o", obj])
     with ThreadPoolExecutor(max_workers=min(8, max(1, len(jobs)))) as ex:
         for out in ex.map(_run, jobs):
             if verbose and out.strip():

@@ -1,0 +1,821 @@
+// Device-built AMG hierarchy: aggregation, coarse-to-fine lists, Galerkin
+// products and SELL-32 packing as sm_100a kernels (amg_device.cuh), and the
+// host orchestration AmgHierarchy::buildDevice.
+//
+// Every result is deterministic: each output element is written by one
+// thread (or one warp) that reads its inputs in a fixed order; the only
+// atomics place fine rows into coarse-row lists, which are then sorted.
+#include "amg_device.cuh"
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+
+#include "common.hpp"
+#include "solver.hpp"
+
+namespace fvm {
+namespace dev {
+
+namespace {
+
+constexpr int kT = 256;
+constexpr int kScanTile = 1024;  // 256 threads x 4 elements
+constexpr unsigned kFull = 0xffffffffu;
+
+inline int cdiv(long long a, long long b) { return (int)((a + b - 1) / b); }
+
+__device__ __forceinline__ void row_range(const LevelRows& a, int i, int& base, int& w) {
+  if (a.ellWidth) {
+    base = ((i >> 5) << 5) * a.ellWidth + (i & 31);
+    w = a.ellWidth;
+  } else {
+    const int4 m = a.meta[a.rowSlice[i]];
+    base = m.z + (i - m.x);
+    w = m.w;
+  }
+}
+
+// exclusive scan of one int per thread over a 256-thread block
+__device__ __forceinline__ int block_exclusive_scan(int v, int& total) {
+  __shared__ int wsum[kT / 32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  int x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(kFull, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) wsum[wid] = x;
+  __syncthreads();
+  if (wid == 0) {
+    int s = lane < kT / 32 ? wsum[lane] : 0;
+#pragma unroll
+    for (int o = 1; o < kT / 32; o <<= 1) {
+      const int y = __shfl_up_sync(kFull, s, o);
+      if (lane >= o) s += y;
+    }
+    if (lane < kT / 32) wsum[lane] = s;
+  }
+  __syncthreads();
+  const int off = wid > 0 ? wsum[wid - 1] : 0;
+  total = wsum[kT / 32 - 1];
+  __syncthreads();
+  return off + x - v;
+}
+
+__global__ void k_scan_tiles(const int* __restrict__ in, int* out, int n, int* tileSum) {
+  const int base = blockIdx.x * kScanTile + threadIdx.x * 4;
+  int v[4];
+  int s = 0;
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    v[q] = base + q < n ? in[base + q] : 0;
+    s += v[q];
+  }
+  int total;
+  int e = block_exclusive_scan(s, total);
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    if (base + q < n) out[base + q] = e;
+    e += v[q];
+  }
+  if (threadIdx.x == 0) tileSum[blockIdx.x] = total;
+}
+
+// one block: exclusive scan of the tile sums in place, total at [nTiles]
+__global__ void k_scan_tile_sums(int* tileSum, int nTiles) {
+  const int per = (nTiles + kT - 1) / kT;
+  const int b = threadIdx.x * per;
+  int s = 0;
+  for (int q = 0; q < per; q++)
+    if (b + q < nTiles) s += tileSum[b + q];
+  int total;
+  int e = block_exclusive_scan(s, total);
+  for (int q = 0; q < per; q++)
+    if (b + q < nTiles) {
+      const int t = tileSum[b + q];
+      tileSum[b + q] = e;
+      e += t;
+    }
+  if (threadIdx.x == 0) tileSum[nTiles] = total;
+}
+
+__global__ void k_scan_add(int* out, int n, const int* tileSum, int nTiles) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] += tileSum[i / kScanTile];
+  if (i == 0) out[n] = tileSum[nTiles];
+}
+
+__global__ void k_fill_finest_vals(long long entries, const int* __restrict__ posSrc, const double* __restrict__ src,
+                                   double* vals, float* valsF) {
+  const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= entries) return;
+  const int s = posSrc[p];
+  const double v = s >= 0 ? src[s] : 0.0;
+  vals[p] = v;
+  if (valsF) valsF[p] = (float)v;
+}
+
+__global__ void k_fill_finest_diag(int n, const int* __restrict__ iperm, const double* __restrict__ diagSrc,
+                                   double* diag, float* diagF) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  const double d = diagSrc[iperm[p]];
+  diag[p] = d;
+  if (diagF) diagF[p] = (float)d;
+}
+
+// ---- aggregation -------------------------------------------------------------
+
+__device__ __forceinline__ double strength(double v, double di, double dj) { return fabs(v) / fmax(di, dj); }
+
+__global__ void k_agg_init(LevelRows a, double* maxw, int* partner) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.n) return;
+  int base, w;
+  row_range(a, i, base, w);
+  const double di = fabs(a.diag[i]);
+  double m = 0.0;
+  for (int k = 0; k < w; k++) {
+    const int j = a.cols[base + 32 * k];
+    const double v = a.vals[base + 32 * k];
+    if (j == i || v == 0.0) continue;
+    m = fmax(m, strength(v, di, fabs(a.diag[j])));
+  }
+  maxw[i] = m;
+  partner[i] = -1;
+}
+
+// strongest unpaired candidate of every unpaired row (ties: smaller index)
+__global__ void k_agg_best(LevelRows a, const double* __restrict__ maxw, double beta, const int* __restrict__ partner,
+                           int* best) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.n) return;
+  if (partner[i] != -1) {
+    best[i] = -1;
+    return;
+  }
+  int base, w;
+  row_range(a, i, base, w);
+  const double di = fabs(a.diag[i]);
+  const double thr = beta * maxw[i];
+  int bj = -1;
+  double bw = 0.0;
+  for (int k = 0; k < w; k++) {
+    const int j = a.cols[base + 32 * k];
+    const double v = a.vals[base + 32 * k];
+    if (j == i || v == 0.0 || partner[j] != -1) continue;
+    const double s = strength(v, di, fabs(a.diag[j]));
+    if (!(s > 0.0) || s < thr) continue;
+    if (s > bw || (s == bw && j < bj)) {
+      bw = s;
+      bj = j;
+    }
+  }
+  best[i] = bj;
+}
+
+// handshake: i and j pair when each is the other's strongest candidate
+__global__ void k_agg_match(int n, const int* __restrict__ best, int* partner) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n || partner[i] != -1) return;
+  const int j = best[i];
+  if (j >= 0 && best[j] == i) partner[i] = j;
+}
+
+// an unpaired row joins the pair of its strongest paired candidate
+__global__ void k_agg_join(LevelRows a, const double* __restrict__ maxw, double beta, const int* __restrict__ partner,
+                           int* join) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.n) return;
+  if (partner[i] != -1) {
+    join[i] = -1;
+    return;
+  }
+  int base, w;
+  row_range(a, i, base, w);
+  const double di = fabs(a.diag[i]);
+  const double thr = beta * maxw[i];
+  int bj = -1;
+  double bw = 0.0;
+  for (int k = 0; k < w; k++) {
+    const int j = a.cols[base + 32 * k];
+    const double v = a.vals[base + 32 * k];
+    if (j == i || v == 0.0 || partner[j] < 0) continue;
+    const double s = strength(v, di, fabs(a.diag[j]));
+    if (!(s > 0.0) || s < thr) continue;
+    if (s > bw || (s == bw && j < bj)) {
+      bw = s;
+      bj = j;
+    }
+  }
+  join[i] = bj;
+}
+
+__device__ __forceinline__ bool is_leader(int i, const int* partner, const int* join) {
+  const int p = partner[i];
+  return p >= 0 ? i < p : join[i] < 0;
+}
+
+__global__ void k_agg_flags(int n, const int* __restrict__ partner, const int* __restrict__ join,
+                            const int* __restrict__ order, int* flag) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  flag[order ? order[i] : i] = is_leader(i, partner, join) ? 1 : 0;
+}
+
+__global__ void k_agg_ci_leaders(int n, const int* __restrict__ partner, const int* __restrict__ join,
+                                 const int* __restrict__ order, const int* __restrict__ pos, int* ci) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n || !is_leader(i, partner, join)) return;
+  ci[i] = pos[order ? order[i] : i];
+}
+
+__global__ void k_agg_ci_rest(int n, const int* __restrict__ partner, const int* __restrict__ join, int* ci) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n || is_leader(i, partner, join)) return;
+  const int p = partner[i];
+  if (p >= 0) {
+    ci[i] = ci[p];  // the pair's leader is its smaller row
+  } else {
+    const int j = join[i];
+    const int q = partner[j];
+    ci[i] = ci[j < q ? j : q];
+  }
+}
+
+// ---- coarse-to-fine lists ------------------------------------------------------
+
+__global__ void k_c2f_count(int n, const int* __restrict__ ci, int* cnt) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) atomicAdd(&cnt[ci[i]], 1);
+}
+
+__global__ void k_c2f_place(int n, const int* __restrict__ ci, const int* __restrict__ c2fRow, int* cursor,
+                            int* c2fCol) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int c = ci[i];
+  c2fCol[c2fRow[c] + atomicAdd(&cursor[c], 1)] = i;
+}
+
+__global__ void k_c2f_sort(int nc, const int* __restrict__ c2fRow, int* c2fCol) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nc) return;
+  const int b = c2fRow[c], e = c2fRow[c + 1];
+  for (int q = b + 1; q < e; q++) {
+    const int v = c2fCol[q];
+    int r = q - 1;
+    while (r >= b && c2fCol[r] > v) {
+      c2fCol[r + 1] = c2fCol[r];
+      r--;
+    }
+    c2fCol[r + 1] = v;
+  }
+}
+
+// ---- Galerkin ----------------------------------------------------------------------
+
+constexpr int kGalWarps = 4;
+
+template <bool kFill>
+__global__ void __launch_bounds__(32 * kGalWarps) k_galerkin(LevelRows a, int nc, const int* __restrict__ ci,
+                                                             const int* __restrict__ c2fRow,
+                                                             const int* __restrict__ c2fCol, int* count,
+                                                             int* overflow, const int* __restrict__ sliceOff,
+                                                             int* ccols, double* cvals, float* cvalsF,
+                                                             double* cdiag, float* cdiagF) {
+  __shared__ int sJ[kGalWarps][kGalerkinCap];
+  __shared__ double sV[kGalWarps][kGalerkinCap];
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int I = blockIdx.x * kGalWarps + wid;
+  if (I >= nc) return;  // the whole warp leaves together
+  int* J = sJ[wid];
+  double* V = sV[wid];
+  const int f0 = c2fRow[I], f1 = c2fRow[I + 1];
+  // every entry of the aggregate's fine rows, fine rows ascending, entries
+  // in stored order; J = coarse column (-1: padding)
+  int L = 0;
+  bool over = false;
+  for (int q = f0; q < f1; q++) {
+    const int f = c2fCol[q];
+    int base, w;
+    row_range(a, f, base, w);
+    if (L + w > kGalerkinCap) {
+      over = true;
+      break;
+    }
+    for (int k = lane; k < w; k += 32) {
+      const int j = a.cols[base + 32 * k];
+      const double v = a.vals[base + 32 * k];
+      J[L + k] = (j == f || v == 0.0) ? -1 : ci[j];
+      V[L + k] = v;
+    }
+    L += w;
+  }
+  __syncwarp();
+  if (over) {
+    if (lane == 0) {
+      atomicExch(overflow, 1);
+      if (!kFill) count[I] = 0;
+    }
+    return;
+  }
+  int cbase = 0, cw = 0;
+  if (kFill) {
+    const int s = I >> 5;
+    cbase = sliceOff[s] + (I & 31);
+    cw = (sliceOff[s + 1] - sliceOff[s]) >> 5;
+  }
+  // off-diagonal coarse columns in first-visit order; each first visit sums
+  // every later entry of its column in stored order
+  int nUnique = 0;
+  for (int e0 = 0; e0 < L; e0 += 32) {
+    const int e = e0 + lane;
+    bool first = false;
+    int Je = -1;
+    if (e < L) {
+      Je = J[e];
+      if (Je >= 0 && Je != I) {
+        first = true;
+        for (int e2 = 0; e2 < e; e2++)
+          if (J[e2] == Je) {
+            first = false;
+            break;
+          }
+      }
+    }
+    const unsigned m = __ballot_sync(kFull, first);
+    if (kFill && first) {
+      const int slot = nUnique + __popc(m & ((1u << lane) - 1u));
+      double s = 0.0;
+      for (int e2 = e; e2 < L; e2++)
+        if (J[e2] == Je) s += V[e2];
+      const size_t o = (size_t)cbase + 32 * (size_t)slot;
+      ccols[o] = Je;
+      cvals[o] = s;
+      cvalsF[o] = (float)s;
+    }
+    nUnique += __popc(m);
+  }
+  if constexpr (!kFill) {
+    if (lane == 0) count[I] = nUnique;
+    return;
+  } else {
+    for (int slot = nUnique + lane; slot < cw; slot += 32) {
+      const size_t o = (size_t)cbase + 32 * (size_t)slot;
+      ccols[o] = I;
+      cvals[o] = 0.0;
+      cvalsF[o] = 0.f;
+    }
+  }
+  if (lane == 0) {
+    // diagonal: fine diagonals plus the entries inside the aggregate
+    double d = 0.0;
+    int e = 0;
+    for (int q = f0; q < f1; q++) {
+      const int f = c2fCol[q];
+      int base, w;
+      row_range(a, f, base, w);
+      d += a.diag[f];
+      for (int k = 0; k < w; k++, e++)
+        if (J[e] == I) d += V[e];
+    }
+    cdiag[I] = d;
+    cdiagF[I] = (float)d;
+  }
+}
+
+__global__ void k_slice_widths(int n, const int* __restrict__ count, int* width32) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  const int ns = (n + 31) >> 5;
+  if (s >= ns) return;
+  int w = 0;
+  for (int r = s << 5; r < min(n, (s + 1) << 5); r++) w = max(w, count[r]);
+  width32[s] = 32 * w;
+}
+
+__global__ void k_slice_meta(int n, const int* __restrict__ sliceOff, int4* meta, int* sliceRow, int* sliceRows,
+                             int* rowSlice, int* maxWidth) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  const int ns = (n + 31) >> 5;
+  if (s >= ns) return;
+  const int r0 = s << 5, rows = min(32, n - r0);
+  const int w = (sliceOff[s + 1] - sliceOff[s]) >> 5;
+  meta[s] = make_int4(r0, rows, sliceOff[s], w);
+  sliceRow[s] = r0;
+  sliceRows[s] = rows;
+  for (int r = 0; r < rows; r++) rowSlice[r0 + r] = s;
+  atomicMax(maxWidth, w);
+}
+
+__global__ void k_dominance(LevelRows a, int* flag) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.n) return;
+  int base, w;
+  row_range(a, i, base, w);
+  double s = 0.0;
+  for (int k = 0; k < w; k++) {
+    const int j = a.cols[base + 32 * k];
+    if (j != i) s += fabs(a.vals[base + 32 * k]);
+  }
+  const double d = a.diag[i];
+  if (!(d != 0.0 && s <= fabs(d) * (1.0 + 1e-8))) atomicOr(flag, 1);
+}
+
+}  // namespace
+
+int scan_scratch_ints(int n) { return cdiv(n, kScanTile) + 1; }
+
+void scan_exclusive(const int* in, int* out, int n, int* scratch, cudaStream_t st) {
+  const int tiles = std::max(1, cdiv(n, kScanTile));
+  k_scan_tiles<<<tiles, kT, 0, st>>>(in, out, n, scratch);
+  k_scan_tile_sums<<<1, kT, 0, st>>>(scratch, tiles);
+  k_scan_add<<<std::max(1, cdiv(n, kT)), kT, 0, st>>>(out, n, scratch, tiles);
+}
+
+void fill_finest(long long entries, const int* posSrc, const double* src, double* vals, float* valsF, int n,
+                 const int* iperm, const double* diagSrc, double* diag, float* diagF, cudaStream_t st) {
+  if (entries > 0) k_fill_finest_vals<<<cdiv(entries, kT), kT, 0, st>>>(entries, posSrc, src, vals, valsF);
+  if (n > 0) k_fill_finest_diag<<<cdiv(n, kT), kT, 0, st>>>(n, iperm, diagSrc, diag, diagF);
+}
+
+void aggregate_pairs(const LevelRows& a, double beta, int rounds, const int* order, const AggWork& w, int* ci,
+                     cudaStream_t st) {
+  const int n = a.n, g = cdiv(n, kT);
+  k_agg_init<<<g, kT, 0, st>>>(a, w.maxw, w.partner);
+  for (int r = 0; r < rounds; r++) {
+    k_agg_best<<<g, kT, 0, st>>>(a, w.maxw, beta, w.partner, w.best);
+    k_agg_match<<<g, kT, 0, st>>>(n, w.best, w.partner);
+  }
+  k_agg_join<<<g, kT, 0, st>>>(a, w.maxw, beta, w.partner, w.join);
+  k_agg_flags<<<g, kT, 0, st>>>(n, w.partner, w.join, order, w.flag);
+  scan_exclusive(w.flag, w.pos, n, w.scan, st);
+  k_agg_ci_leaders<<<g, kT, 0, st>>>(n, w.partner, w.join, order, w.pos, ci);
+  k_agg_ci_rest<<<g, kT, 0, st>>>(n, w.partner, w.join, ci);
+}
+
+void coarse_to_fine(int n, int nc, const int* ci, int* cnt, int* c2fRow, int* c2fCol, int* scanScratch,
+                    cudaStream_t st) {
+  cudaMemsetAsync(cnt, 0, sizeof(int) * (size_t)nc, st);
+  k_c2f_count<<<cdiv(n, kT), kT, 0, st>>>(n, ci, cnt);
+  scan_exclusive(cnt, c2fRow, nc, scanScratch, st);
+  cudaMemsetAsync(cnt, 0, sizeof(int) * (size_t)nc, st);
+  k_c2f_place<<<cdiv(n, kT), kT, 0, st>>>(n, ci, c2fRow, cnt, c2fCol);
+  k_c2f_sort<<<cdiv(nc, kT), kT, 0, st>>>(nc, c2fRow, c2fCol);
+}
+
+void galerkin_count(const LevelRows& a, int nc, const int* ci, const int* c2fRow, const int* c2fCol, int* count,
+                    int* overflow, cudaStream_t st) {
+  k_galerkin<false><<<cdiv(nc, kGalWarps), 32 * kGalWarps, 0, st>>>(a, nc, ci, c2fRow, c2fCol, count, overflow,
+                                                                      nullptr, nullptr, nullptr, nullptr, nullptr,
+                                                                      nullptr);
+}
+
+void galerkin_fill(const LevelRows& a, int nc, const int* ci, const int* c2fRow, const int* c2fCol,
+                   const int* sliceOff, int* cols, double* vals, float* valsF, double* diag, float* diagF,
+                   cudaStream_t st) {
+  k_galerkin<true><<<cdiv(nc, kGalWarps), 32 * kGalWarps, 0, st>>>(a, nc, ci, c2fRow, c2fCol, nullptr, nullptr,
+                                                                     sliceOff, cols, vals, valsF, diag, diagF);
+}
+
+void slice_widths(int n, const int* count, int* width32, cudaStream_t st) {
+  const int ns = cdiv(n, 32);
+  k_slice_widths<<<cdiv(ns, kT), kT, 0, st>>>(n, count, width32);
+}
+
+void slice_meta_fill(int n, const int* sliceOff, int4* meta, int* sliceRow, int* sliceRows, int* rowSlice,
+                     int* maxWidth, cudaStream_t st) {
+  const int ns = cdiv(n, 32);
+  k_slice_meta<<<cdiv(ns, kT), kT, 0, st>>>(n, sliceOff, meta, sliceRow, sliceRows, rowSlice, maxWidth);
+}
+
+void dominance_check(const LevelRows& a, int* flag, cudaStream_t st) {
+  k_dominance<<<cdiv(a.n, kT), kT, 0, st>>>(a, flag);
+}
+
+}  // namespace dev
+}  // namespace fvm
+
+// ===========================================================================
+// Host orchestration
+namespace fvm {
+
+#define CUDA_OK(call)                                                                            \
+  do {                                                                                           \
+    cudaError_t e_ = (call);                                                                     \
+    if (e_ != cudaSuccess)                                                                       \
+      throw ::fvm::Error(::fvm::kDeviceError, std::string(#call ": ") + cudaGetErrorString(e_)); \
+  } while (0)
+
+namespace {
+// Device blocks of a rebuilt hierarchy are recycled by exact size; sizes
+// rounded up to 1/8 of their power of two let a rebuild whose level sizes
+// moved a little (another conductivity field) reuse them too.
+size_t size_class(size_t bytes) {
+  if (bytes <= 4096) return 4096;
+  size_t p = 1;
+  while (p < bytes) p <<= 1;
+  const size_t g = p >> 3;
+  return (bytes + g - 1) / g * g;
+}
+}  // namespace
+
+void AmgHierarchy::prepareFinestPattern(const FinestDevice& in, int ordering) {
+  if (finest_ && in.key != 0 && finest_->key == in.key && finest_->ordering == ordering) return;
+  finest_.reset(new FinestPattern());
+  FinestPattern& fp = *finest_;
+  fp.key = in.key;
+  fp.ordering = ordering;
+  const CSR& c = *in.conn;
+  const int n = c.nRows;
+  RefLevel tmp;
+  tmp.n = n;
+  tmp.conn = c;
+  tmp.symmetricPattern = in.symmetricPattern;
+  tmp.segments = in.segments;
+  tmp.diag.assign(n, 1.0);
+  // values = entry index + 1, so the packing tells where every entry went
+  tmp.off.resize(c.nnz());
+  for (int k = 0; k < c.nnz(); k++) tmp.off[k] = (double)(k + 1);
+  pack_level(tmp, (SmootherOrdering)ordering, fp.packed);
+  PackedLevel& p = fp.packed;
+  const size_t E = p.cols.size();
+  std::vector<int> posSrc(E);
+  parallel_chunks((int)E, [&](int b, int e) {
+    for (int q = b; q < e; q++) {
+      const double v = p.vals[q];
+      if (v == 0.0) {
+        posSrc[q] = -1;
+      } else {
+        const int k = (int)v - 1;
+        posSrc[q] = in.entrySrc ? (*in.entrySrc)[k] : k;
+      }
+    }
+  }, 1 << 18);
+  p.vals.clear();
+  p.vals.shrink_to_fit();
+  const int nSlices = (int)p.sliceRow.size();
+  std::vector<int> rs(n);
+  std::vector<int4> meta(nSlices);
+  for (int s = 0; s < nSlices; s++) {
+    for (int k = 0; k < p.sliceRows[s]; k++) rs[p.sliceRow[s] + k] = s;
+    meta[s] = make_int4(p.sliceRow[s], p.sliceRows[s], p.sliceOff[s], (p.sliceOff[s + 1] - p.sliceOff[s]) / 32);
+  }
+  fp.sliceRow = fp.arena.upload(p.sliceRow);
+  fp.sliceRows = fp.arena.upload(p.sliceRows);
+  fp.sliceOff = fp.arena.upload(p.sliceOff);
+  fp.cols = fp.arena.upload(p.cols);
+  fp.rowSlice = fp.arena.upload(rs);
+  fp.meta = fp.arena.upload(meta);
+  fp.posSrc = fp.arena.upload(posSrc);
+  fp.iperm = fp.arena.upload(p.iperm);
+  fp.perm = fp.arena.upload(p.perm);
+}
+
+void AmgHierarchy::allocVectors(DevLevel& d, bool mixed) {
+  const size_t nb = (size_t)d.n * sizeof(double);
+  d.x = (double*)arena_.alloc(size_class(nb));
+  d.b = (double*)arena_.alloc(size_class(nb));
+  d.r = (double*)arena_.alloc(size_class(nb));
+  d.tmp = (double*)arena_.alloc(size_class(nb));
+  CUDA_OK(cudaMemsetAsync(d.x, 0, nb, setupStream_));
+  CUDA_OK(cudaMemsetAsync(d.b, 0, nb, setupStream_));
+  CUDA_OK(cudaMemsetAsync(d.tmp, 0, nb, setupStream_));
+  d.nPartials = dev::residual_partials(d.nSlices, d.n, d.ellWidth);
+  d.partials = (double*)arena_.alloc(size_class(sizeof(double) * (d.nPartials + 1)));
+  if (mixed) {
+    const size_t fb = (size_t)d.n * sizeof(float);
+    d.xF = (float*)arena_.alloc(size_class(fb));
+    d.bF = (float*)arena_.alloc(size_class(fb));
+    d.rF = (float*)arena_.alloc(size_class(fb));
+    d.tmpF = (float*)arena_.alloc(size_class(fb));
+    CUDA_OK(cudaMemsetAsync(d.xF, 0, fb, setupStream_));
+    CUDA_OK(cudaMemsetAsync(d.tmpF, 0, fb, setupStream_));
+  }
+}
+
+void AmgHierarchy::buildDevice(const FinestDevice& in, const SolverOptions& opt) {
+  const bool trace = getenv("FVM_TRACE") != nullptr;
+  auto t0 = std::chrono::steady_clock::now();
+  auto lap = [&](const char* what) {
+    if (!trace) return;
+    CUDA_OK(cudaStreamSynchronize(setupStream_));
+    const auto t1 = std::chrono::steady_clock::now();
+    fprintf(stderr, "[fvm device setup] %-30s %8.2f ms\n", what,
+            std::chrono::duration<double, std::milli>(t1 - t0).count());
+    t0 = t1;
+  };
+  FVM_REQUIRE(in.conn && in.offSrc && in.diag, kBadArgument, "device-built hierarchy: missing level-0 input");
+  FVM_REQUIRE(!opt.finestOnly(), kUnsupported, "device-built hierarchy: not for the Jacobi solver or preconditioner");
+  release();
+  opt_ = opt;
+  if (!setupStream_) CUDA_OK(cudaStreamCreateWithFlags(&setupStream_, cudaStreamNonBlocking));
+  cudaStream_t st = setupStream_;
+  const bool mixed = opt.precision == kMixed;
+  prepareFinestPattern(in, (int)opt.ordering);
+  deviceBuilt_ = true;
+  lap("level-0 pattern");
+  const FinestPattern& fp = *finest_;
+  const PackedLevel& p0 = fp.packed;
+  const int n0 = p0.n;
+  const size_t maxL = (size_t)std::max(1, opt.maxCoarseLevels) + 2;
+  lv_.clear();
+  lv_.reserve(maxL);
+  lv_.emplace_back();
+  {
+    DevLevel& d = lv_[0];
+    d.n = n0;
+    d.nColors = p0.nColors;
+    d.nSlices = (int)p0.sliceRow.size();
+    d.maxWidth = p0.maxWidth;
+    d.ellWidth = p0.ellWidth;
+    d.colorSliceStart = p0.colorSliceStart;
+    d.entries = p0.cols.size();
+    d.sliceRow = fp.sliceRow;
+    d.sliceRows = fp.sliceRows;
+    d.sliceOff = fp.sliceOff;
+    d.cols = fp.cols;
+    d.rowSlice = fp.rowSlice;
+    d.meta = fp.meta;
+    d.vals = (double*)arena_.alloc(size_class(sizeof(double) * d.entries));
+    d.diag = (double*)arena_.alloc(size_class(sizeof(double) * n0));
+    if (mixed) {
+      d.valsF = (float*)arena_.alloc(size_class(sizeof(float) * d.entries));
+      d.diagF = (float*)arena_.alloc(size_class(sizeof(float) * n0));
+    }
+    dev::fill_finest((long long)d.entries, fp.posSrc, in.offSrc, d.vals, d.valsF, n0, fp.iperm, in.diag, d.diag,
+                     d.diagF, st);
+    allocVectors(d, mixed);
+  }
+  // work arrays sized by level 0, shared by every level
+  dev::AggWork w;
+  w.maxw = (double*)arena_.alloc(size_class(sizeof(double) * n0));
+  w.best = (int*)arena_.alloc(size_class(sizeof(int) * n0));
+  w.partner = (int*)arena_.alloc(size_class(sizeof(int) * n0));
+  w.join = (int*)arena_.alloc(size_class(sizeof(int) * n0));
+  w.flag = (int*)arena_.alloc(size_class(sizeof(int) * n0));
+  w.pos = (int*)arena_.alloc(size_class(sizeof(int) * (n0 + 1)));
+  w.scan = (int*)arena_.alloc(size_class(sizeof(int) * (dev::scan_scratch_ints(n0 + 1) + 1)));
+  int* flags = (int*)arena_.alloc(4096);  // [0] overflow, [1] max width, [2] not dominant
+  int* hflags = reinterpret_cast<int*>(pinnedScalars());
+  lap("level 0 values");
+
+  for (int l = 0;; l++) {
+    DevLevel& f = lv_[l];
+    if (l >= opt.maxCoarseLevels || lv_.size() + 1 > maxL) break;
+    if (opt.coarsestSize > 0 ? f.n <= opt.coarsestSize : f.n <= 3) break;
+    const dev::LevelRows a{f.n, f.cols, f.vals, f.diag, f.meta, f.rowSlice, f.ellWidth};
+    int* ci = (int*)arena_.alloc(size_class(sizeof(int) * f.n));
+    dev::aggregate_pairs(a, opt.matchBeta, opt.matchRounds, l == 0 ? fp.iperm : nullptr, w, ci, st);
+    CUDA_OK(cudaMemcpyAsync(hflags, w.pos + f.n, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CUDA_OK(cudaStreamSynchronize(st));
+    const int nc = hflags[0];
+    // a level that no longer shrinks is the coarsest
+    if (nc <= 0 || nc >= f.n || (double)nc > 0.9 * f.n) break;
+    f.ci = ci;
+    f.nCoarse = nc;
+    f.c2fRow = (int*)arena_.alloc(size_class(sizeof(int) * (nc + 1)));
+    f.c2fCol = (int*)arena_.alloc(size_class(sizeof(int) * f.n));
+    dev::coarse_to_fine(f.n, nc, ci, w.flag, f.c2fRow, f.c2fCol, w.scan, st);
+    // coarse level: counts, slice widths and offsets, then the entries
+    const int nSlices = (nc + 31) / 32;
+    int* sliceOff = (int*)arena_.alloc(size_class(sizeof(int) * (nSlices + 1)));
+    CUDA_OK(cudaMemsetAsync(flags, 0, 3 * sizeof(int), st));
+    dev::galerkin_count(a, nc, ci, f.c2fRow, f.c2fCol, w.best, flags, st);
+    dev::slice_widths(nc, w.best, w.join, st);
+    dev::scan_exclusive(w.join, sliceOff, nSlices, w.scan, st);
+    CUDA_OK(cudaMemcpyAsync(hflags, sliceOff + nSlices, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CUDA_OK(cudaMemcpyAsync(hflags + 1, flags, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CUDA_OK(cudaStreamSynchronize(st));
+    const long long E = hflags[0];
+    FVM_REQUIRE(hflags[1] == 0, kUnsupported,
+                "device-built hierarchy: an aggregate's entries exceed the Galerkin kernel's capacity");
+    lv_.emplace_back();
+    DevLevel& c = lv_.back();
+    DevLevel& fine = lv_[l];
+    c.n = nc;
+    c.nColors = 1;
+    c.nSlices = nSlices;
+    c.colorSliceStart = {0, nSlices};
+    c.entries = (size_t)E;
+    c.ellWidth = 0;
+    c.sliceOff = sliceOff;
+    c.cols = (int*)arena_.alloc(size_class(sizeof(int) * (size_t)std::max<long long>(E, 1)));
+    c.vals = (double*)arena_.alloc(size_class(sizeof(double) * (size_t)std::max<long long>(E, 1)));
+    c.valsF = (float*)arena_.alloc(size_class(sizeof(float) * (size_t)std::max<long long>(E, 1)));
+    c.diag = (double*)arena_.alloc(size_class(sizeof(double) * nc));
+    c.diagF = (float*)arena_.alloc(size_class(sizeof(float) * nc));
+    c.meta = (int4*)arena_.alloc(size_class(sizeof(int4) * nSlices));
+    c.sliceRow = (int*)arena_.alloc(size_class(sizeof(int) * nSlices));
+    c.sliceRows = (int*)arena_.alloc(size_class(sizeof(int) * nSlices));
+    c.rowSlice = (int*)arena_.alloc(size_class(sizeof(int) * nc));
+    const dev::LevelRows af{fine.n, fine.cols, fine.vals, fine.diag, fine.meta, fine.rowSlice, fine.ellWidth};
+    dev::galerkin_fill(af, nc, fine.ci, fine.c2fRow, fine.c2fCol, sliceOff, c.cols, c.vals, c.valsF, c.diag, c.diagF,
+                       st);
+    dev::slice_meta_fill(nc, sliceOff, c.meta, c.sliceRow, c.sliceRows, c.rowSlice, flags + 1, st);
+    CUDA_OK(cudaMemcpyAsync(hflags, flags + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
+    allocVectors(c, mixed);
+    CUDA_OK(cudaStreamSynchronize(st));
+    c.maxWidth = hflags[0];
+    if (trace) {
+      char msg[96];
+      snprintf(msg, sizeof msg, "level %d: %d rows, %lld entries", l + 1, nc, E);
+      lap(msg);
+    }
+  }
+  const int L = (int)lv_.size();
+  // coarsest direct solve: dense inverse built on the GPU (no pivoting when
+  // the level is diagonally dominant), FP32 copy for the FP32 cycle
+  if (opt.coarseSolver == kCoarseDirect) {
+    DevLevel& c = lv_[L - 1];
+    FVM_REQUIRE(c.n <= 4096, kTooLarge,
+                "coarsest level too large for the dense direct solve (max 4096 rows); set coarsestSize");
+    const size_t nn = (size_t)c.n * c.n;
+    if (c.n <= 128) {
+      // small: inverted on the host (a launch sequence costs more)
+      PackedLevel h;
+      h.n = c.n;
+      const int ns = c.nSlices;
+      std::vector<int4> meta(ns);
+      if (c.ellWidth == 0) {
+        CUDA_OK(cudaMemcpyAsync(meta.data(), c.meta, sizeof(int4) * ns, cudaMemcpyDeviceToHost, st));
+      } else {
+        for (int s = 0; s < ns; s++)
+          meta[s] = make_int4(32 * s, std::min(32, c.n - 32 * s), 32 * s * c.ellWidth, c.ellWidth);
+      }
+      h.cols.resize(c.entries);
+      h.vals.resize(c.entries);
+      h.diag.resize(c.n);
+      CUDA_OK(cudaMemcpyAsync(h.cols.data(), c.cols, sizeof(int) * c.entries, cudaMemcpyDeviceToHost, st));
+      CUDA_OK(cudaMemcpyAsync(h.vals.data(), c.vals, sizeof(double) * c.entries, cudaMemcpyDeviceToHost, st));
+      CUDA_OK(cudaMemcpyAsync(h.diag.data(), c.diag, sizeof(double) * c.n, cudaMemcpyDeviceToHost, st));
+      CUDA_OK(cudaStreamSynchronize(st));
+      h.sliceRow.resize(ns);
+      h.sliceRows.resize(ns);
+      h.sliceOff.resize(ns + 1);
+      for (int s = 0; s < ns; s++) {
+        h.sliceRow[s] = meta[s].x;
+        h.sliceRows[s] = meta[s].y;
+        h.sliceOff[s] = meta[s].z;
+      }
+      h.sliceOff[ns] = (int)c.entries;
+      std::vector<double> inv;
+      dense_inverse(h, inv);
+      coarseInv_ = arena_.upload(inv);
+    } else {
+      FVM_REQUIRE(c.ellWidth == 0, kUnsupported, "coarsest level in ELL-32 layout");
+      const dev::LevelRows a{c.n, c.cols, c.vals, c.diag, c.meta, c.rowSlice, c.ellWidth};
+      CUDA_OK(cudaMemsetAsync(flags + 2, 0, sizeof(int), st));
+      dev::dominance_check(a, flags + 2, st);
+      CUDA_OK(cudaMemcpyAsync(hflags, flags + 2, sizeof(int), cudaMemcpyDeviceToHost, st));
+      CUDA_OK(cudaStreamSynchronize(st));
+      const bool dominant = hflags[0] == 0;
+      void* gjScratch = arena_.alloc(size_class(dev::gauss_jordan_scratch_bytes(c.n)));
+      coarseInv_ = (double*)arena_.alloc(size_class(sizeof(double) * nn));
+      if (dominant) {
+        dev::dense_from_sell(c.view64(), c.nSlices, coarseInv_, st);
+        dev::gauss_jordan_inverse_dominant(c.n, coarseInv_, gjScratch, st);
+      } else {
+        double* dA = (double*)arena_.alloc(size_class(sizeof(double) * nn));
+        dev::dense_from_sell(c.view64(), c.nSlices, dA, st);
+        dev::gauss_jordan_inverse(c.n, dA, coarseInv_, gjScratch, st);
+      }
+      CUDA_OK(cudaMemcpyAsync(hflags, dev::gauss_jordan_status(c.n, gjScratch), sizeof(int), cudaMemcpyDeviceToHost,
+                              st));
+      CUDA_OK(cudaStreamSynchronize(st));
+      FVM_REQUIRE(hflags[0] == 0, kBadArgument, "singular coarsest-level matrix");
+    }
+    if (mixed) {
+      coarseInvF_ = (float*)arena_.alloc(size_class(sizeof(float) * nn));
+      dev::cast_d2f(nn, coarseInv_, coarseInvF_, st);
+    }
+    lap("coarsest inverse");
+  }
+  CUDA_OK(cudaStreamSynchronize(st));
+  tunePlans();
+  lap("launch plans");
+  if (trace) {
+    fprintf(stderr, "[fvm device setup] levels:");
+    for (int l = 0; l < L; l++) fprintf(stderr, " %d", lv_[l].n);
+    fprintf(stderr, "\n");
+  }
+}
+
+std::vector<int> AmgHierarchy::coarseIndexHost(int l) const {
+  FVM_REQUIRE(l >= 0 && l + 1 < (int)lv_.size(), kBadArgument, "no coarser level");
+  if (!deviceBuilt_) return ref_[l].coarseIndex;
+  const DevLevel& d = lv_[l];
+  std::vector<int> ci(d.n);
+  CUDA_OK(cudaMemcpy(ci.data(), d.ci, sizeof(int) * d.n, cudaMemcpyDeviceToHost));
+  if (l > 0) return ci;
+  std::vector<int> ref(d.n);
+  const PackedLevel& p = finest_->packed;
+  for (int i = 0; i < d.n; i++) ref[i] = ci[p.perm[i]];
+  return ref;
+}
+
+}  // namespace fvm

@@ -99,6 +99,11 @@ SolverOptions to_solver(const fvm_linear_options& o) {
   s.autotune = o.autotune != 0;
   s.planTpr = o.planThreadsPerRow;
   s.planBlock = o.planBlock;
+  FVM_REQUIRE(o.matchRounds >= 1 && o.matchRounds <= 64, kBadArgument, "matchRounds must be in [1, 64]");
+  FVM_REQUIRE(o.matchBeta >= 0.0 && o.matchBeta <= 1.0, kBadArgument, "matchBeta must be in [0, 1]");
+  s.setupOnDevice = o.setupOnDevice != 0;
+  s.matchRounds = o.matchRounds;
+  s.matchBeta = o.matchBeta;
   return s;
 }
 
@@ -127,6 +132,9 @@ void from_solver(const SolverOptions& s, fvm_linear_options& o) {
   o.autotune = s.autotune ? 1 : 0;
   o.planThreadsPerRow = s.planTpr;
   o.planBlock = s.planBlock;
+  o.setupOnDevice = s.setupOnDevice ? 1 : 0;
+  o.matchRounds = s.matchRounds;
+  o.matchBeta = s.matchBeta;
 }
 
 RefLevel level_from_csr(int n, const int* row, const int* col, const double* diag, const double* off) {
@@ -421,7 +429,38 @@ int fvm_thermal_hierarchy(fvm_thermal* h, int* nLevels, int* sizes, int sizesCap
   return guarded([&] {
     FVM_REQUIRE(h, kBadArgument, "null model");
     const AmgHierarchy& hier = h->model->hierarchy();
-    export_hierarchy(hier.refLevels(), nLevels, sizes, sizesCap, coarseIndex, ciCap);
+    if (!hier.deviceBuilt()) {
+      export_hierarchy(hier.refLevels(), nLevels, sizes, sizesCap, coarseIndex, ciCap);
+      return;
+    }
+    const int L = hier.numLevels();
+    if (nLevels) *nLevels = L - 1;
+    int pos = 0;
+    for (int l = 1; l < L; l++) {
+      if (sizes && l - 1 < sizesCap) sizes[l - 1] = hier.level(l).n;
+      if (!coarseIndex) continue;
+      const std::vector<int> ci = hier.coarseIndexHost(l - 1);
+      for (size_t i = 0; i < ci.size(); i++, pos++)
+        if (pos < ciCap) coarseIndex[pos] = ci[i];
+    }
+  });
+}
+
+int fvm_thermal_level_matrix(fvm_thermal* h, int level, int* n, int* nnz, int* row, int* col, double* val,
+                             double* diag, int cap) {
+  return guarded([&] {
+    FVM_REQUIRE(h && n && nnz, kBadArgument, "null argument");
+    const AmgHierarchy& hier = h->model->hierarchy();
+    FVM_REQUIRE(level >= 0 && level < hier.numLevels(), kBadArgument, "no such level");
+    std::vector<int> r, c;
+    std::vector<double> v, d;
+    hier.levelCsr(level, r, c, v, d);
+    *n = (int)d.size();
+    *nnz = (int)c.size();
+    if (row && (int)r.size() <= cap + 1) std::copy(r.begin(), r.end(), row);
+    if (col && (int)c.size() <= cap) std::copy(c.begin(), c.end(), col);
+    if (val && (int)v.size() <= cap) std::copy(v.begin(), v.end(), val);
+    if (diag && (int)d.size() <= cap) std::copy(d.begin(), d.end(), diag);
   });
 }
 
@@ -442,6 +481,16 @@ int fvm_thermal_profile(fvm_thermal* h, int reps, double* out) {
   return guarded([&] {
     FVM_REQUIRE(h && out, kBadArgument, "null argument");
     h->model->profile(reps, out);
+  });
+}
+
+int fvm_thermal_profile_levels(fvm_thermal* h, int reps, int* nLevels, double* out, int cap) {
+  return guarded([&] {
+    FVM_REQUIRE(h && nLevels, kBadArgument, "null argument");
+    std::vector<double> v;
+    h->model->profileLevels(reps, v);
+    *nLevels = (int)(v.size() / AmgHierarchy::kLevelProfile);
+    if (out && (int)v.size() <= cap) std::copy(v.begin(), v.end(), out);
   });
 }
 

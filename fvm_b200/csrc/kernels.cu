@@ -680,6 +680,11 @@ __global__ void k_scalar_div(const double* num, const double* den, double* out) 
   FVM_PDL();
   out[0] = num[0] / den[0];
 }
+// flexible (Polak-Ribiere) CG: beta = (r_k+1, z_k+1 - z_k) / (r_k, z_k)
+__global__ void k_scalar_flex_beta(const double* rho, const double* rzPrev, const double* rhoPrev, double* out) {
+  FVM_PDL();
+  out[0] = (rho[0] - rzPrev[0]) / rhoPrev[0];
+}
 __global__ void k_scalar_ratio_product(const double* a, const double* b, const double* c,
                                        const double* d, double* out) {
   FVM_PDL();
@@ -1048,6 +1053,10 @@ void restrict_sum(int nc, const int* c2fRow, const int* c2fCol, const T* r, T* b
   pdl_launch(k_restrict<T>, ceil_div(nc, kBlock), kBlock, st, nc, c2fRow, c2fCol, r, bc, (T*)nullptr);
 }
 template <class T>
+void restrict_rhs(int nc, const int* c2fRow, const int* c2fCol, const T* b, T* bc, T* xc, cudaStream_t st) {
+  pdl_launch(k_restrict<T>, ceil_div(nc, kBlock), kBlock, st, nc, c2fRow, c2fCol, b, bc, xc);
+}
+template <class T>
 void residual_restrict(const SellView<T>& a, int nSlices, const int* rowSlice, int nc, const int* c2fRow,
                        const int* c2fCol, const T* x, const T* b, T* bc, T* xc, T* r, cudaStream_t st) {
   if (r) {
@@ -1232,10 +1241,11 @@ __global__ void __launch_bounds__(256, 3) k_gjnp_update(int n, int k0, int nb, d
   }
   if (nb1 <= 0) return;  // the last panel: no next block to invert
   // the last CTA to finish inverts the next panel's pivot block: every
-  // other CTA's writes of Rn are visible to it after their fence and its own
+  // thread that wrote Rn / Cn / A fences its own writes before the barrier,
+  // so they are visible device-wide before the ticket is taken
+  __threadfence();
   __syncthreads();
   if (tid == 0) {
-    __threadfence();
     const unsigned done = atomicAdd(ticket, 1u);
     last = done == gridDim.x * gridDim.y - 1;
   }
@@ -1405,6 +1415,9 @@ void sum_partials(int np, const double* partials, double* out, cudaStream_t st) 
 void scalar_div(const double* num, const double* den, double* out, cudaStream_t st) {
   pdl_launch(k_scalar_div, 1, 1, st, num, den, out);
 }
+void scalar_flex_beta(const double* rho, const double* rzPrev, const double* rhoPrev, double* out, cudaStream_t st) {
+  pdl_launch(k_scalar_flex_beta, 1, 1, st, rho, rzPrev, rhoPrev, out);
+}
 void scalar_ratio_product(const double* a, const double* b, const double* c, const double* d,
                           double* out, cudaStream_t st) {
   pdl_launch(k_scalar_ratio_product, 1, 1, st, a, b, c, d, out);
@@ -1475,6 +1488,7 @@ void update_solution(int nCells, const int* perm, const double* delta, const Bou
   template void jacobi_damped<T>(const SellView<T>&, int, const T*, T*, const T*, T, cudaStream_t, RowPlan); \
   template void residual<T>(const SellView<T>&, int, const T*, const T*, T*, double*, cudaStream_t); \
   template void restrict_sum<T>(int, const int*, const int*, const T*, T*, cudaStream_t);        \
+  template void restrict_rhs<T>(int, const int*, const int*, const T*, T*, T*, cudaStream_t);    \
   template void residual_restrict<T>(const SellView<T>&, int, const int*, int, const int*,        \
                                      const int*, const T*, const T*, T*, T*, T*, cudaStream_t);   \
   template void zero<T>(int, T*, cudaStream_t);                                                  \

@@ -91,6 +91,10 @@ void restrict_sum(int nc, const int* c2fRow, const int* c2fCol, const T* r, T* b
 template <class T>
 void residual_restrict(const SellView<T>& a, int nSlices, const int* rowSlice, int nc, const int* c2fRow,
                        const int* c2fCol, const T* x, const T* b, T* bc, T* xc, T* r, cudaStream_t st);
+// bc[I] = sum of b over the fine rows of aggregate I (ascending order) and
+// xc = 0: the restricted residual of a level whose x is zero (r = b)
+template <class T>
+void restrict_rhs(int nc, const int* c2fRow, const int* c2fCol, const T* b, T* bc, T* xc, cudaStream_t st);
 template <class T>
 void zero(int n, T* x, cudaStream_t st);
 // x[i] += xc[ci[i]]
@@ -134,6 +138,8 @@ void sum_partials(int np, const double* partials, double* out, cudaStream_t st);
 // scalar recurrences for the Krylov solvers, all on the device:
 // out = num / den (out, num, den are device scalars)
 void scalar_div(const double* num, const double* den, double* out, cudaStream_t st);
+// out = (rho - rzPrev) / rhoPrev (flexible CG's beta)
+void scalar_flex_beta(const double* rho, const double* rzPrev, const double* rhoPrev, double* out, cudaStream_t st);
 // out = (a / b) * (c / d)
 void scalar_ratio_product(const double* a, const double* b, const double* c, const double* d,
                           double* out, cudaStream_t st);

@@ -8,6 +8,7 @@
 #include <cstring>
 #include <cstdlib>
 #include <exception>
+#include <functional>
 #include <thread>
 #include <limits>
 #include <type_traits>
@@ -75,6 +76,7 @@ T take_spare(std::vector<T>& spares, size_t l) {
 }  // namespace
 
 void AmgHierarchy::release() {
+  deviceBuilt_ = false;
   arena_.release();
   lv_.clear();
   keep_spares(packed_, sparePacked_);
@@ -95,6 +97,7 @@ double* AmgHierarchy::pinnedScalars() {
 
 AmgHierarchy::~AmgHierarchy() {
   if (pinned_) cudaFreeHost(pinned_);
+  if (setupStream_) cudaStreamDestroy(setupStream_);
 }
 
 std::vector<int> AmgHierarchy::sizes() const {
@@ -269,8 +272,6 @@ void AmgHierarchy::build(std::vector<RefLevel>& levels, int finestLocalSize, con
   }
   tunePlans();
   lap("launch plans");
-  buildProgram();
-  lap("cycle program");
   if (trace) {
     fprintf(stderr, "[fvm setup] levels:");
     for (int l = 0; l < L; l++)
@@ -450,6 +451,8 @@ void AmgHierarchy::tunePlans() {
 }
 
 bool AmgHierarchy::dampedLevel(int l, int n) const {
+  // device-built coarse levels carry no colouring
+  if (deviceBuilt_ && l > 0 && opt_.smootherType == kGaussSeidel) return true;
   return l > 0 && opt_.coarseJacobiRows > 0 && n <= opt_.coarseJacobiRows && opt_.smootherType == kGaussSeidel &&
          opt_.ordering == kMulticolor;
 }
@@ -506,171 +509,14 @@ void AmgHierarchy::uploadTransfer(const PackedLevel& p, DevLevel& d, int nCoarse
   d.c2fCol = arena_.upload(p.c2fCol);
 }
 
-void AmgHierarchy::genSweeps(int n, int l, std::vector<dev::Phase>& out) const {
-  const DevLevel& d = lv_[l];
-  for (int s = 0; s < n; s++) {
-    if (opt_.smootherType == kGaussSeidel) {
-      const int C = d.nColors;
-      for (int c = 0; c < C; c++)
-        if (d.colorSliceStart[c + 1] > d.colorSliceStart[c])
-          out.push_back({dev::kPhaseGS, l, d.colorSliceStart[c], d.colorSliceStart[c + 1]});
-      for (int c = C - 2; c >= 0; c--)
-        if (d.colorSliceStart[c + 1] > d.colorSliceStart[c])
-          out.push_back({dev::kPhaseGS, l, d.colorSliceStart[c], d.colorSliceStart[c + 1]});
-    } else {
-      out.push_back({dev::kPhaseJacobi, l, 0, 0});
-      out.push_back({dev::kPhaseJacobi, l, 1, 0});
-    }
-  }
-}
-
-// Flattens AmgHierarchy::cycle into phases (same order of operations).
-void AmgHierarchy::genCycle(CycleType t, int l, std::vector<dev::Phase>& out) const {
-  const int L = (int)lv_.size();
-  const bool coarsest = (l == L - 1);
-  if (coarsest && coarseInv_) {
-    out.push_back({dev::kPhaseDense, l, 0, 0});
-    return;
-  }
-  genSweeps(opt_.nPreSweeps, l, out);
-  if (!coarsest) {
-    out.push_back({dev::kPhaseRestrict, l, 0, 0});
-    genCycle(t, l + 1, out);
-    if (t == kWCycle)
-      genCycle(kWCycle, l + 1, out);
-    else if (t == kFCycle)
-      genCycle(kVCycle, l + 1, out);
-    out.push_back({dev::kPhaseProlong, l, 0, 0});
-  }
-  genSweeps(opt_.nPostSweeps, l, out);
-}
-
-void AmgHierarchy::buildProgram() {
-  programReady_ = false;
-  tailLevel_ = -1;
-  // the program kernels implement the uniform smoothers on SELL-32 levels only
-  if ((opt_.ordering == kSequential && opt_.smootherType == kGaussSeidel) || opt_.coarseJacobiRows > 0) return;
-  for (const DevLevel& d : lv_)
-    if (d.ellWidth > 0) return;
-  const int L = (int)lv_.size();
-  std::vector<dev::ProgLevel<double>> p64(L);
-  std::vector<dev::ProgLevel<float>> p32(L);
-  for (int l = 0; l < L; l++) {
-    const DevLevel& d = lv_[l];
-    dev::ProgLevel<double>& a = p64[l];
-    a.n = d.n;
-    a.nSlices = d.nSlices;
-    a.nCoarse = d.nCoarse;
-    a.sliceRow = d.sliceRow;
-    a.sliceRows = d.sliceRows;
-    a.sliceOff = d.sliceOff;
-    a.cols = d.cols;
-    a.rowSlice = d.rowSlice;
-    a.vals = d.vals;
-    a.diag = d.diag;
-    a.x = d.x;
-    a.b = d.b;
-    a.tmp = d.tmp;
-    a.ci = d.ci;
-    a.c2fRow = d.c2fRow;
-    a.c2fCol = d.c2fCol;
-    dev::ProgLevel<float>& f = p32[l];
-    f.n = d.n;
-    f.nSlices = d.nSlices;
-    f.nCoarse = d.nCoarse;
-    f.sliceRow = d.sliceRow;
-    f.sliceRows = d.sliceRows;
-    f.sliceOff = d.sliceOff;
-    f.cols = d.cols;
-    f.rowSlice = d.rowSlice;
-    f.vals = d.valsF;
-    f.diag = d.diagF;
-    f.x = d.xF;
-    f.b = d.bF;
-    f.tmp = d.tmpF;
-    f.ci = d.ci;
-    f.c2fRow = d.c2fRow;
-    f.c2fCol = d.c2fCol;
-  }
-  dProg64_ = arena_.upload(p64);
-  if (opt_.precision == kMixed) dProg32_ = arena_.upload(p32);
-
-  // Coarse tail: from the first level (below the finest) with at most
-  // kTailRows rows down to the coarsest, a V-cycle is one cluster kernel.
-  // Those levels fit in L2 and their phases are latency bound; the
-  // cluster barrier between phases is far cheaper than a kernel launch.
-  // Off by default (FVM_TAIL_ROWS=<rows> enables): measured slower than one
-  // launch per phase at 1.5M cells (2.26 vs 1.37 ms per FP32 V-cycle).
-  int tailRows = 0;
-  if (const char* tr = getenv("FVM_TAIL_ROWS")) tailRows = atoi(tr);
-  if (opt_.cycleType == kVCycle && tailRows > 0) {
-    int lt = -1;
-    for (int l = 1; l < L; l++)
-      if (lv_[l].n <= tailRows) {
-        lt = l;
-        break;
-      }
-    const int cs = lt >= 0 ? (opt_.precision == kMixed ? dev::cluster_program_size<float>()
-                                                        : dev::cluster_program_size<double>())
-                           : 0;
-    if (lt >= 0 && cs > 0) {
-      tailPhases_.clear();
-      genCycle(kVCycle, lt, tailPhases_);
-      dTailPhases_ = arena_.upload(tailPhases_);
-      clusterSize_ = cs;
-      tailLevel_ = lt;
-    }
-  }
-
-  // Opt-in (FVM_PERSISTENT_CYCLE=1): the whole cycle as one cooperative
-  // kernel with grid barriers. Measured on B200 at 1.5M cells, a 296-block
-  // grid barrier per phase costs more than a kernel launch per phase (3.8 vs
-  // 2.5 ms per FP32 V-cycle), so it is not the default.
-  const char* env = getenv("FVM_PERSISTENT_CYCLE");
-  if (!env || env[0] != '1') return;
-  phases_.clear();
-  genCycle(opt_.cycleType, 0, phases_);
-  if (phases_.empty()) return;
-  dPhases_ = arena_.upload(phases_);
-  dBarrier_ = (dev::BarrierState*)arena_.alloc(sizeof(dev::BarrierState));
-  CUDA_OK(cudaMemset(dBarrier_, 0, sizeof(dev::BarrierState)));
-  grid64_ = dev::cycle_program_max_grid<double>();
-  grid32_ = dev::cycle_program_max_grid<float>();
-  FVM_REQUIRE(grid64_ > 0 && grid32_ > 0, kDeviceError, "cycle program cannot be made co-resident");
-  programReady_ = true;
+template <>
+void AmgHierarchy::runCycle<double>(cudaStream_t st, bool xZero) {
+  cycle<double>(opt_.cycleType, 0, st, xZero);
 }
 
 template <>
-void AmgHierarchy::runCycle<double>(cudaStream_t st) {
-  if (!programReady_) {
-    cycle<double>(opt_.cycleType, 0, st);
-    return;
-  }
-  const int L = (int)lv_.size();
-  CUDA_OK(dev::run_cycle_program<double>(dPhases_, (int)phases_.size(), dProg64_, coarseInv_, lv_[L - 1].n,
-                                         dBarrier_, grid64_, st));
-}
-
-template <>
-void AmgHierarchy::runCycle<float>(cudaStream_t st) {
-  if (!programReady_) {
-    cycle<float>(opt_.cycleType, 0, st);
-    return;
-  }
-  const int L = (int)lv_.size();
-  CUDA_OK(dev::run_cycle_program<float>(dPhases_, (int)phases_.size(), dProg32_, coarseInv_, lv_[L - 1].n,
-                                        dBarrier_, grid32_, st));
-}
-
-void AmgHierarchy::checkProgram(cudaStream_t st) {
-  if (!programReady_) return;
-  dev::BarrierState bs;
-  CUDA_OK(cudaMemcpyAsync(&bs, dBarrier_, sizeof(bs), cudaMemcpyDeviceToHost, st));
-  CUDA_OK(cudaStreamSynchronize(st));
-  if (bs.error) {
-    CUDA_OK(cudaMemset(dBarrier_, 0, sizeof(dev::BarrierState)));
-    throw Error(kDeviceError, "a grid barrier of the cycle program exceeded its wait limit");
-  }
+void AmgHierarchy::runCycle<float>(cudaStream_t st, bool xZero) {
+  cycle<float>(opt_.cycleType, 0, st, xZero);
 }
 
 template <class T>
@@ -740,19 +586,10 @@ void AmgHierarchy::sweeps(int nSweeps, int l, cudaStream_t st) {
 }
 
 template <class T>
-void AmgHierarchy::cycle(CycleType t, int l, cudaStream_t st) {
+void AmgHierarchy::cycle(CycleType t, int l, cudaStream_t st, bool xZero) {
   const int L = (int)lv_.size();
   DevLevel& d = lv_[l];
   const bool coarsest = (l == L - 1);
-  if (l == tailLevel_ && t == kVCycle) {
-    if constexpr (std::is_same<T, float>::value)
-      CUDA_OK(dev::run_cluster_program<float>(dTailPhases_, (int)tailPhases_.size(), dProg32_, coarseInv_,
-                                              coarseInvF_, lv_[L - 1].n, clusterSize_, st));
-    else
-      CUDA_OK(dev::run_cluster_program<double>(dTailPhases_, (int)tailPhases_.size(), dProg64_, coarseInv_,
-                                               nullptr, lv_[L - 1].n, clusterSize_, st));
-    return;
-  }
   if (coarsest && coarseInv_) {
     if constexpr (std::is_same<T, float>::value) {
       if (coarseInvF_) {
@@ -766,9 +603,12 @@ void AmgHierarchy::cycle(CycleType t, int l, cudaStream_t st) {
   sweeps<T>(opt_.nPreSweeps, l, st);
   if (!coarsest) {
     DevLevel& c = lv_[l + 1];
-    dev::residual_restrict<T>(view<T>(d), d.nSlices, d.rowSlice, c.n, d.c2fRow, d.c2fCol, vec_x<T>(d),
-                              vec_b<T>(d), vec_b<T>(c), vec_x<T>(c), d.splitRestrict ? vec_r<T>(d) : nullptr, st);
-    cycle<T>(t, l + 1, st);
+    if (xZero && opt_.nPreSweeps == 0)
+      dev::restrict_rhs<T>(c.n, d.c2fRow, d.c2fCol, vec_b<T>(d), vec_b<T>(c), vec_x<T>(c), st);
+    else
+      dev::residual_restrict<T>(view<T>(d), d.nSlices, d.rowSlice, c.n, d.c2fRow, d.c2fCol, vec_x<T>(d),
+                                vec_b<T>(d), vec_b<T>(c), vec_x<T>(c), d.splitRestrict ? vec_r<T>(d) : nullptr, st);
+    cycle<T>(t, l + 1, st, true);
     if (t == kWCycle)
       cycle<T>(kWCycle, l + 1, st);
     else if (t == kFCycle)
@@ -790,13 +630,13 @@ void AmgHierarchy::apply(const double* r, double* z, cudaStream_t st) {
   if (opt_.precision == kMixed) {
     dev::convert_d2f(d.n, r, d.bF, st);
     dev::zero<float>(d.n, d.xF, st);
-    runCycle<float>(st);
+    runCycle<float>(st, true);
     dev::zero<double>(d.n, z, st);
     dev::add_f2d(d.n, d.xF, z, st);
   } else {
     dev::copy_d(d.n, r, d.b, st);
     dev::zero<double>(d.n, d.x, st);
-    runCycle<double>(st);
+    runCycle<double>(st, true);
     dev::copy_d(d.n, d.x, z, st);
   }
 }
@@ -853,8 +693,142 @@ int AmgHierarchy::kernelsPerCycle() const {
   return k;
 }
 
-template void AmgHierarchy::cycle<double>(CycleType, int, cudaStream_t);
-template void AmgHierarchy::cycle<float>(CycleType, int, cudaStream_t);
+void AmgHierarchy::profileLevels(int reps, void* flush, size_t flushBytes, cudaStream_t st,
+                                 std::vector<double>& out) {
+  const int L = (int)lv_.size();
+  const bool f32 = opt_.precision == kMixed;
+  const double vb = f32 ? 4.0 : 8.0;
+  cudaEvent_t a, b;
+  CUDA_OK(cudaEventCreate(&a));
+  CUDA_OK(cudaEventCreate(&b));
+  auto timed = [&](const std::function<void()>& body) {
+    double total = 0;
+    for (int r = 0; r < reps; r++) {
+      CUDA_OK(cudaMemsetAsync(flush, r & 0xff, flushBytes, st));
+      CUDA_OK(cudaEventRecord(a, st));
+      body();
+      CUDA_OK(cudaEventRecord(b, st));
+      CUDA_OK(cudaEventSynchronize(b));
+      float ms = 0;
+      CUDA_OK(cudaEventElapsedTime(&ms, a, b));
+      total += ms;
+    }
+    return total / reps;
+  };
+  out.assign((size_t)kLevelProfile * L, 0.0);
+  for (int l = 0; l < L; l++) {
+    DevLevel& d = lv_[l];
+    double* o = &out[(size_t)kLevelProfile * l];
+    o[0] = d.n;
+    o[1] = (double)d.entries;
+    const double pass = d.n * 4.0 * vb + d.entries * (4.0 + vb);
+    if (l == L - 1 && coarseInv_) {
+      o[2] = timed([&] {
+        if (f32 && coarseInvF_)
+          dev::dense_solve_f32(d.n, coarseInvF_, d.bF, d.xF, st);
+        else if (f32)
+          dev::dense_solve<float>(d.n, coarseInv_, d.bF, d.xF, st);
+        else
+          dev::dense_solve<double>(d.n, coarseInv_, d.b, d.x, st);
+      });
+      o[3] = (double)d.n * d.n * ((f32 && coarseInvF_) ? 4.0 : 8.0) + 2.0 * vb * d.n;
+      continue;
+    }
+    o[2] = timed([&] { smootherPass(l, d.plan, st); });
+    o[3] = pass;
+    if (l + 1 < L) {
+      DevLevel& c = lv_[l + 1];
+      const bool rhsOnly = opt_.nPreSweeps == 0 && (f32 || l > 0);  // x = 0 on entry
+      o[4] = timed([&] {
+        if (rhsOnly) {
+          if (f32)
+            dev::restrict_rhs<float>(c.n, d.c2fRow, d.c2fCol, d.bF, c.bF, c.xF, st);
+          else
+            dev::restrict_rhs<double>(c.n, d.c2fRow, d.c2fCol, d.b, c.b, c.x, st);
+        } else {
+          restrictPass(l, d.splitRestrict, st);
+        }
+      });
+      if (rhsOnly)
+        o[5] = (vb + 4.0) * d.n + (4.0 + 2.0 * vb) * c.n;
+      else if (d.splitRestrict)
+        o[5] = pass + (vb + 4.0) * d.n + (4.0 + 2.0 * vb) * c.n;
+      else
+        o[5] = 3.0 * vb * d.n + (4.0 + vb) * d.entries + (4.0 + 2.0 * vb) * c.n;
+      o[6] = timed([&] {
+        if (f32)
+          dev::prolong<float>(d.n, d.ci, c.xF, d.xF, st);
+        else
+          dev::prolong<double>(d.n, d.ci, c.x, d.x, st);
+      });
+      o[7] = (2.0 * vb + 4.0) * d.n + vb * c.n;
+    }
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  // the timed passes wrote the level vectors
+  for (int l = 0; l < L; l++) {
+    DevLevel& d = lv_[l];
+    CUDA_OK(cudaMemsetAsync(d.x, 0, sizeof(double) * d.n, st));
+    if (d.xF) CUDA_OK(cudaMemsetAsync(d.xF, 0, sizeof(float) * d.n, st));
+    if (d.tmpF) CUDA_OK(cudaMemsetAsync(d.tmpF, 0, sizeof(float) * d.n, st));
+  }
+  CUDA_OK(cudaStreamSynchronize(st));
+}
+
+void AmgHierarchy::levelCsr(int l, std::vector<int>& row, std::vector<int>& col, std::vector<double>& val,
+                            std::vector<double>& diag) const {
+  FVM_REQUIRE(l >= 0 && l < (int)lv_.size(), kBadArgument, "no such level");
+  const DevLevel& d = lv_[l];
+  const int n = d.n;
+  std::vector<int> cols(d.entries);
+  std::vector<double> vals(d.entries), dg(n);
+  std::vector<int4> meta(d.nSlices);
+  CUDA_OK(cudaMemcpy(cols.data(), d.cols, sizeof(int) * d.entries, cudaMemcpyDeviceToHost));
+  CUDA_OK(cudaMemcpy(vals.data(), d.vals, sizeof(double) * d.entries, cudaMemcpyDeviceToHost));
+  CUDA_OK(cudaMemcpy(dg.data(), d.diag, sizeof(double) * n, cudaMemcpyDeviceToHost));
+  if (d.ellWidth) {
+    for (int s = 0; s < d.nSlices; s++)
+      meta[s] = make_int4(32 * s, std::min(32, n - 32 * s), 32 * s * d.ellWidth, d.ellWidth);
+  } else {
+    CUDA_OK(cudaMemcpy(meta.data(), d.meta, sizeof(int4) * d.nSlices, cudaMemcpyDeviceToHost));
+  }
+  // storage row -> row of the exported numbering
+  const std::vector<int>* iperm = nullptr;
+  if (deviceBuilt_) {
+    if (l == 0) iperm = &finest_->packed.iperm;
+  } else if (!packed_[l].iperm.empty()) {
+    iperm = &packed_[l].iperm;
+  }
+  auto out = [&](int p) { return iperm ? (*iperm)[p] : p; };
+  std::vector<std::vector<std::pair<int, double>>> rows(n);
+  diag.assign(n, 0.0);
+  for (int s = 0; s < d.nSlices; s++) {
+    const int4 m = meta[s];
+    for (int q = 0; q < m.y; q++) {
+      const int p = m.x + q;
+      const int i = out(p);
+      diag[i] = dg[p];
+      for (int k = 0; k < m.w; k++) {
+        const size_t e = (size_t)m.z + 32 * (size_t)k + q;
+        if (vals[e] != 0.0 && cols[e] != p) rows[i].push_back({out(cols[e]), vals[e]});
+      }
+    }
+  }
+  row.assign(n + 1, 0);
+  col.clear();
+  val.clear();
+  for (int i = 0; i < n; i++) {
+    for (const auto& cv : rows[i]) {
+      col.push_back(cv.first);
+      val.push_back(cv.second);
+    }
+    row[i + 1] = (int)col.size();
+  }
+}
+
+template void AmgHierarchy::cycle<double>(CycleType, int, cudaStream_t, bool);
+template void AmgHierarchy::cycle<float>(CycleType, int, cudaStream_t, bool);
 
 // ---------------------------------------------------------------------------
 namespace {
@@ -871,6 +845,7 @@ enum Scal {
   kTdott,
   kOmegaPrev,
   kAlphaPrev,
+  kRzPrev,
   // learned step
   kLsScale = 20,  // and kLsScale + 1 (input sum)
   kLsRq = 22,
@@ -970,7 +945,6 @@ SolveReport LinearSolve::solve(cudaStream_t st) {
     default:
       r = solveAMG(st);
   }
-  h_.checkProgram(st);
   return r;
 }
 
@@ -1007,7 +981,7 @@ SolveReport LinearSolve::solveAMG(cudaStream_t st) {
       if (o.precision == kMixed) {
         dev::convert_d2f(n_, d.r, d.bF, st);
         dev::zero<float>(n_, d.xF, st);
-        h_.runCycle<float>(st);
+        h_.runCycle<float>(st, true);
         dev::add_f2d(n_, d.xF, d.x, st);
       } else {
         h_.runCycle<double>(st);
@@ -1151,7 +1125,7 @@ int LinearSolve::solveRecording(cudaStream_t st, double relTol, int maxIter, int
     if (o.precision == kMixed) {
       dev::convert_d2f(n_, d.r, d.bF, st);
       dev::zero<float>(n_, d.xF, st);
-      h_.runCycle<float>(st);
+      h_.runCycle<float>(st, true);
       dev::add_f2d(n_, d.xF, d.x, st);
     } else {
       h_.runCycle<double>(st);
@@ -1172,7 +1146,11 @@ int LinearSolve::solveRecording(cudaStream_t st, double relTol, int maxIter, int
   return recorded;
 }
 
-// CG::solve (CG.cpp:26-139) with the AMG cycle as preconditioner.
+// CG::solve (CG.cpp:26-139) with the AMG cycle as preconditioner. The
+// reference's beta = rho_k+1 / rho_k assumes a symmetric preconditioner;
+// the FP32 cycle and cycles with nPreSweeps != nPostSweeps are not, so
+// those use the flexible (Polak-Ribiere) beta (r_k+1, z_k+1 - z_k) / rho_k,
+// equal to the reference's in exact arithmetic for a symmetric one.
 SolveReport LinearSolve::solveCG(cudaStream_t st) {
   const SolverOptions& o = h_.options();
   DevLevel& d = h_.level(0);
@@ -1182,9 +1160,12 @@ SolveReport LinearSolve::solveCG(cudaStream_t st) {
   double* P = work_ + 3 * (size_t)n_;
   double* Q = work_ + 4 * (size_t)n_;
   double* B = work_ + 5 * (size_t)n_;
+  const bool flexible = o.preconditioner == kPrecAMG &&
+                        (o.precision == kMixed || o.nPreSweeps != o.nPostSweeps || o.cycleType != kVCycle);
   SolveReport rep;
   CUDA_OK(cudaMemsetAsync(X, 0, sizeof(double) * (size_t)n_, st));
   CUDA_OK(cudaMemsetAsync(P, 0, sizeof(double) * (size_t)n_, st));
+  CUDA_OK(cudaMemsetAsync(Z, 0, sizeof(double) * (size_t)n_, st));  // z_0 enters the first flexible beta
   dev::copy_d(n_, d.b, B, st);
   dev::residual<double>(d.view64(), d.nSlices, X, B, R, nullptr, st);
   norm_into(R, scal_ + kNorm, st);
@@ -1216,10 +1197,14 @@ SolveReport LinearSolve::solveCG(cudaStream_t st) {
   }
   for (int i = 0; i < o.nMaxIterations; i++) {
     run(g1_, st, [&] {
+      if (flexible) dot_into(R, Z, scal_ + kRzPrev, st);  // (r_k+1, z_k) before z is replaced
       h_.apply(R, Z, st);
       dev::copy_d(1, scal_ + kRho, scal_ + kRhoPrev, st);
       dot_into(R, Z, scal_ + kRho, st);
-      dev::scalar_div(scal_ + kRho, scal_ + kRhoPrev, scal_ + kBeta, st);  // 0 on the first pass
+      if (flexible)
+        dev::scalar_flex_beta(scal_ + kRho, scal_ + kRzPrev, scal_ + kRhoPrev, scal_ + kBeta, st);
+      else
+        dev::scalar_div(scal_ + kRho, scal_ + kRhoPrev, scal_ + kBeta, st);  // 0 on the first pass
       dev::xpby_dev(n_, Z, scal_ + kBeta, P, st);
       dev::spmv(d.view64(), d.nSlices, P, Q, st);
       dot_into(P, Q, scal_ + kPtq, st);
@@ -1240,6 +1225,14 @@ SolveReport LinearSolve::solveCG(cudaStream_t st) {
       rep.converged = true;
       break;
     }
+  }
+  // the recursively updated R can drift from b + A x: the reported final
+  // norm is that of the true residual
+  if (rep.iterations > 0) {
+    dev::residual<double>(d.view64(), d.nSlices, X, B, R, nullptr, st);
+    norm_into(R, scal_ + kNorm, st);
+    rep.finalNorm = fetch(scal_ + kNorm, st);
+    rep.history.back() = rep.finalNorm;
   }
   // restore the system: delta = X, b = original
   dev::copy_d(n_, X, d.x, st);
@@ -1329,6 +1322,12 @@ SolveReport LinearSolve::solveBCGStab(cudaStream_t st) {
       rep.converged = true;
       break;
     }
+  }
+  if (rep.iterations > 0) {
+    dev::residual<double>(d.view64(), d.nSlices, X, B, R, nullptr, st);
+    norm_into(R, scal_ + kNorm, st);
+    rep.finalNorm = fetch(scal_ + kNorm, st);
+    if (!rep.history.empty()) rep.history.back() = rep.finalNorm;
   }
   dev::copy_d(n_, X, d.x, st);
   dev::copy_d(n_, B, d.b, st);

@@ -14,7 +14,6 @@
 #include <vector>
 
 #include "amg_setup.hpp"
-#include "cycle_program.cuh"
 #include "kernels.cuh"
 #include "learned.hpp"
 
@@ -60,6 +59,14 @@ struct SolverOptions {
   bool autotune = true;
   int planTpr = 0;
   int planBlock = 0;
+  // Build the coarse levels on the GPU (parallel pairwise matching and
+  // Galerkin kernels) instead of the reference's sequential greedy walk on
+  // the host; coarse levels then smooth with damped Jacobi. The hierarchy is
+  // not the reference's: for the mixed-precision path, whose result is
+  // judged by the converged field only.
+  bool setupOnDevice = false;
+  int matchRounds = 4;          // handshake rounds per level
+  double matchBeta = 0.25;      // candidate when strength >= beta * the row's strongest
   // only the finest level is needed (Jacobi solver or preconditioner)
   bool finestOnly() const { return solver == kSolverJacobi || preconditioner == kPrecJacobi; }
 };
@@ -126,11 +133,53 @@ class DeviceArena {
   std::mutex mu_;  // levels are uploaded from several setup threads
 };
 
+// Level-0 input of a hierarchy built on the device: the pattern on the host
+// (reference row order, self rows, implicit diagonal) and its values on the
+// device.
+struct FinestDevice {
+  const CSR* conn = nullptr;
+  // CSR entry k -> index of its value in offSrc (null: k itself)
+  const std::vector<int>* entrySrc = nullptr;
+  const double* offSrc = nullptr;  // device
+  const double* diag = nullptr;    // device, reference order
+  // equal non-zero keys promise the same pattern and entrySrc: the packed
+  // level-0 structure (colouring, permutation, slices) is reused
+  unsigned long long key = 0;
+  bool symmetricPattern = true;
+  std::vector<int> segments;  // independent diagonal blocks (a batch)
+};
+
+// Cached level-0 structure of device-built hierarchies (pattern only).
+struct FinestPattern {
+  unsigned long long key = 0;
+  int ordering = 0;
+  PackedLevel packed;  // colours, permutation, slices (values unused)
+  DeviceArena arena;
+  int *sliceRow = nullptr, *sliceRows = nullptr, *sliceOff = nullptr, *cols = nullptr, *rowSlice = nullptr;
+  int *posSrc = nullptr, *iperm = nullptr, *perm = nullptr;
+  int4* meta = nullptr;
+};
+
 class AmgHierarchy {
  public:
   // levels[0] is the finest matrix in reference order; the hierarchy
   // (reference-exact aggregation) is built, packed and uploaded.
   void build(std::vector<RefLevel>& levels, int finestLocalSize, const SolverOptions& opt);
+  // The same hierarchy built on the GPU from a level 0 resident there
+  // (opt.setupOnDevice): pairwise matching, Galerkin products and SELL-32
+  // packing as kernels; only level 0's colouring is host work, once per
+  // pattern. refLevels() is then empty and packed(l) exists for l = 0 only.
+  void buildDevice(const FinestDevice& in, const SolverOptions& opt);
+  bool deviceBuilt() const { return deviceBuilt_; }
+  // device-built: reference row -> level-0 row, on the device
+  const int* finestPermDevice() const { return deviceBuilt_ && finest_ ? finest_->perm : nullptr; }
+  // fine -> coarse index of level l on the host (device-built hierarchies:
+  // downloaded; level 0 in reference row order, coarse levels in their own)
+  std::vector<int> coarseIndexHost(int l) const;
+  // level l's matrix as CSR (diagonal apart, stored zeros left out), rows
+  // numbered as coarseIndexHost numbers them
+  void levelCsr(int l, std::vector<int>& row, std::vector<int>& col, std::vector<double>& val,
+                std::vector<double>& diag) const;
   // Drops the device state and keeps the host-side level objects of this
   // hierarchy as spares: the next build() of a similar hierarchy refills
   // their buffers instead of allocating (and page-faulting) new ones.
@@ -149,24 +198,22 @@ class AmgHierarchy {
   int numLevels() const { return (int)lv_.size(); }
   const DevLevel& level(int l) const { return lv_[l]; }
   DevLevel& level(int l) { return lv_[l]; }
-  const PackedLevel& packed(int l) const { return packed_[l]; }
+  const PackedLevel& packed(int l) const { return deviceBuilt_ && l == 0 ? finest_->packed : packed_[l]; }
   const std::vector<RefLevel>& refLevels() const { return ref_; }
   std::vector<int> sizes() const;
 
-  // one cycle on level l of precision T (x, b of each level as stored)
+  // one cycle on level l of precision T (x, b of each level as stored);
+  // xZero: level l's x is zero on entry, so without pre-smoothing its
+  // residual is b and the restriction needs no pass over the matrix
   template <class T>
-  void cycle(CycleType t, int l, cudaStream_t st);
+  void cycle(CycleType t, int l, cudaStream_t st, bool xZero = false);
   template <class T>
   void sweeps(int nSweeps, int l, cudaStream_t st);
 
-  // one cycle from the finest level: the persistent program kernel when
-  // available (multicolour or Jacobi smoothing), else one launch per phase
+  // one cycle of the configured type from the finest level (xZero: level
+  // 0's x is zero on entry)
   template <class T>
-  void runCycle(cudaStream_t st);
-  bool usesProgram() const { return programReady_; }
-  int programPhases() const { return (int)phases_.size(); }
-  // raises if a program barrier ever exceeded its wait limit
-  void checkProgram(cudaStream_t st);
+  void runCycle(cudaStream_t st, bool xZero = false);
 
   // x = z <- M^-1 applied to r (FP64 in/out; runs the cycle in the
   // configured precision): b0 <- r, x0 <- 0, cycle, z <- x0
@@ -175,6 +222,16 @@ class AmgHierarchy {
   const SolverOptions& options() const { return opt_; }
 
   size_t deviceBytes() const { return arena_.bytes(); }
+  // Per level, CUDA-event times (ms, mean of reps, L2 flushed by a write of
+  // `flush` before each timed launch) of the cycle's kernels in the
+  // configured precision, with their algorithmic bytes; kLevelProfile
+  // doubles per level: rows, stored entries, smoother pass (one damped
+  // Jacobi launch, or one Gauss-Seidel pass over all colours; the coarsest
+  // level with a direct solve: the dense solve) ms and bytes, restriction
+  // (as the cycle runs it) ms and bytes, prolongation ms and bytes (0 on
+  // the coarsest level).
+  static constexpr int kLevelProfile = 8;
+  void profileLevels(int reps, void* flush, size_t flushBytes, cudaStream_t st, std::vector<double>& out);
   // algorithmic bytes moved by one cycle (for roofline reporting)
   double cycleBytes() const;
   double fineSweepBytes() const;  // one GS pass over all colours of level 0
@@ -200,28 +257,18 @@ class AmgHierarchy {
   // of its transfer to the next coarser level
   void uploadMatrix(const PackedLevel& p, DevLevel& d, bool mixed);
   void uploadTransfer(const PackedLevel& p, DevLevel& d, int nCoarse);
-  // persistent cycle program
-  void buildProgram();
+  // device-built hierarchies
+  bool deviceBuilt_ = false;
+  std::unique_ptr<FinestPattern> finest_;
+  cudaStream_t setupStream_ = nullptr;
+  void prepareFinestPattern(const FinestDevice& in, int ordering);
+  void allocVectors(DevLevel& d, bool mixed);
   // picks each SELL-32 level's smoother launch plan (autotune or forced)
   void tunePlans();
   // one smoother pass of level l with a given plan (what the tuner times)
   void smootherPass(int l, dev::RowPlan plan, cudaStream_t st);
   // level l's residual restricted to level l + 1, fused or split
   void restrictPass(int l, bool split, cudaStream_t st);
-  void genCycle(CycleType t, int l, std::vector<dev::Phase>& out) const;
-  void genSweeps(int n, int l, std::vector<dev::Phase>& out) const;
-  bool programReady_ = false;
-  // coarse tail: levels >= tailLevel_ run as one cluster kernel per cycle
-  int tailLevel_ = -1;
-  int clusterSize_ = 0;
-  std::vector<dev::Phase> tailPhases_;
-  dev::Phase* dTailPhases_ = nullptr;
-  std::vector<dev::Phase> phases_;
-  dev::Phase* dPhases_ = nullptr;
-  dev::ProgLevel<double>* dProg64_ = nullptr;
-  dev::ProgLevel<float>* dProg32_ = nullptr;
-  dev::BarrierState* dBarrier_ = nullptr;
-  int grid64_ = 0, grid32_ = 0;
 };
 
 // Linear solve of the finest system held by the hierarchy: level 0's b is

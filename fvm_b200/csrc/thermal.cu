@@ -1,6 +1,8 @@
 // ThermalModel on the GPU.
 #include "thermal.hpp"
 
+#include <atomic>
+
 #include <algorithm>
 #include <chrono>
 #include <functional>
@@ -300,6 +302,11 @@ void ThermalModel::ensureDevice() {
   dCoeff_ = (double*)arena_.alloc(sizeof(double) * (size_t)F);
   dSec_ = (double*)arena_.alloc(3 * sizeof(double) * (size_t)F);
   CUDA_OK(cudaMemset(dGrad_, 0, 3 * cb));
+  {
+    // identifies this model's level-0 pattern (interiorConn_, entryFace_)
+    static std::atomic<unsigned long long> nextKey{1};
+    patternKey_ = nextKey++;
+  }
   deviceReady_ = true;
   tDirty_ = kDirty_ = srcDirty_ = rcDirty_ = tn1Dirty_ = true;
   matrixDirty_ = true;
@@ -403,6 +410,30 @@ void ThermalModel::ensureMatrix() {
   dev::CellFaceView cf{dCfRow_, dCfCol_, dBRow_, dBCol_, dBColG_};
   const dev::BoundaryData bd = boundaryData();
   dev::assemble_matrix(n, cf, dFaceCells_, dCoeff_, dAreaMag_, rhoVdt, bd, dBIndexOfFace_, dT_, dDiagOrig_, stream_);
+  if (opt_.linear.setupOnDevice && !opt_.linear.finestOnly()) {
+    // the whole hierarchy is built on the GPU from the assembled face
+    // coefficients and diagonal: nothing comes back to the host
+    lap("assembly");
+    solver_.reset();
+    hier_.release();
+    FinestDevice in;
+    in.conn = &interiorConn_;
+    in.entrySrc = &entryFace_;
+    in.offSrc = dCoeff_;
+    in.diag = dDiagOrig_;
+    in.key = patternKey_;
+    in.symmetricPattern = true;
+    in.segments = segOff_;
+    CUDA_OK(cudaStreamSynchronize(stream_));
+    hier_.buildDevice(in, opt_.linear);
+    lap("hierarchy on the device");
+    dPerm_ = const_cast<int*>(hier_.finestPermDevice());
+    solver_.reset(new LinearSolve(hier_));
+    solver_->setLearned(learned_);
+    lap("solver workspace");
+    matrixDirty_ = hierarchyDirty_ = false;
+    return;
+  }
   // face coefficients and diagonal come back through pinned buffers kept
   // for the model's lifetime
   const size_t pinBytes = sizeof(double) * ((size_t)F + (size_t)n);
@@ -474,8 +505,10 @@ void ThermalModel::advance(int niter, AdvanceReport& rep) {
   CUDA_OK(cudaEventCreate(&e0));
   CUDA_OK(cudaEventCreate(&e1));
   CUDA_OK(cudaEventCreate(&e2));
-  CUDA_OK(cudaEventRecord(e0, stream_));
+  // the cell fields set on the host since the last call go to the device
+  // first; the timed region (rep.seconds) starts with them resident
   uploadFields();
+  CUDA_OK(cudaEventRecord(e0, stream_));
   const auto s0 = std::chrono::steady_clock::now();
   ensureMatrix();
   const auto s1 = std::chrono::steady_clock::now();
@@ -701,10 +734,14 @@ void ThermalModel::profile(int reps, double* out) {
   out[2] = timed([&] { dev::residual<double>(d.view64(), d.nSlices, d.x, d.b, d.r, d.partials, stream_); });
   out[3] = d.n * 32.0 + d.entries * 12.0;
   out[4] = timed([&] {
-    if (mixed)
-      hier_.cycle<float>(opt_.linear.cycleType, 0, stream_);
-    else
+    // as the solvers run it: the FP32 preconditioner cycle starts from
+    // x = 0; the FP64 AMG iteration from the current iterate
+    if (mixed) {
+      dev::zero<float>(d.n, d.xF, stream_);
+      hier_.cycle<float>(opt_.linear.cycleType, 0, stream_, true);
+    } else {
       hier_.cycle<double>(opt_.linear.cycleType, 0, stream_);
+    }
   });
   out[5] = hier_.cycleBytes();
   out[6] = hier_.numLevels();
@@ -718,6 +755,27 @@ void ThermalModel::profile(int reps, double* out) {
   CUDA_OK(cudaMemsetAsync(d.x, 0, sizeof(double) * d.n, stream_));
   if (d.xF) CUDA_OK(cudaMemsetAsync(d.xF, 0, sizeof(float) * d.n, stream_));
   CUDA_OK(cudaStreamSynchronize(stream_));
+}
+
+void ThermalModel::profileLevels(int reps, std::vector<double>& out) {
+  FVM_REQUIRE(initialized_, kBadArgument, "ThermalModel.init() must be called first");
+  FVM_REQUIRE(reps > 0, kBadArgument, "reps must be positive");
+  ensureDevice();
+  uploadFields();
+  ensureMatrix();
+  linearize();
+  DevLevel& d = hier_.level(0);
+  if (opt_.linear.precision == kMixed) dev::convert_d2f(d.n, d.b, d.bF, stream_);
+  const size_t flushBytes = 512u << 20;  // > 126 MB L2
+  void* flush = nullptr;
+  CUDA_OK(cudaMalloc(&flush, flushBytes));
+  try {
+    hier_.profileLevels(reps, flush, flushBytes, stream_, out);
+  } catch (...) {
+    cudaFree(flush);
+    throw;
+  }
+  cudaFree(flush);
 }
 
 const AmgHierarchy& ThermalModel::hierarchy() {

@@ -65,7 +65,7 @@ struct AdvanceReport {
   double initialNorm = 0;  // of the model's first linear system
   double lastNorm = 0;
   bool converged = false;
-  double seconds = 0;      // device time (CUDA events) of the advance call
+  double seconds = 0;      // device time (CUDA events) of the advance call, after the field uploads
   double setupSeconds = 0; // part spent rebuilding matrix + hierarchy
   long long launches = 0;
   int learnedSteps = 0;    // learned corrections tried / kept (all outer iterations)
@@ -102,6 +102,8 @@ class ThermalModel {
   // [6] levels, [7] rows of level 0, [8] stored entries of level 0,
   // [9] kernels per cycle, [10] colours of level 0
   void profile(int reps, double* out);
+  // per-level kernel timings of the cycle (AmgHierarchy::profileLevels)
+  void profileLevels(int reps, std::vector<double>& out);
   const std::vector<double>& history() const { return history_; }
   // ThermalModel::getHeatFluxIntegral (ThermalModel_impl.h:400-422): sum of
   // the boundary heat flux over a face group, as the last advance() left it
@@ -168,6 +170,7 @@ class ThermalModel {
   std::vector<double> bParamHost_;       // and their h / far-field / emissivity
   std::vector<int> entryFace_;           // interior-only CSR entry -> face
   CSR interiorConn_;                     // cellCells restricted to self rows / self columns
+  unsigned long long patternKey_ = 0;    // names interiorConn_ for the device-built hierarchy
   AmgHierarchy hier_;
   LearnedCorrection* learned_ = nullptr;
   // blocks of cells with their own convergence test

@@ -194,6 +194,9 @@ class AMG(LinearSolver):
         self.autotune = bool(d.autotune)
         self.planThreadsPerRow = d.planThreadsPerRow
         self.planBlock = d.planBlock
+        self.setupOnDevice = bool(d.setupOnDevice)
+        self.matchRounds = d.matchRounds
+        self.matchBeta = d.matchBeta
         self._printFile = None
 
     def setMergeLevelSize(self, size: int) -> None:
@@ -231,6 +234,9 @@ class AMG(LinearSolver):
         o.autotune = int(bool(self.autotune))
         o.planThreadsPerRow = int(self.planThreadsPerRow)
         o.planBlock = int(self.planBlock)
+        o.setupOnDevice = int(bool(self.setupOnDevice))
+        o.matchRounds = int(self.matchRounds)
+        o.matchBeta = float(self.matchBeta)
 
     def options(self) -> _lib.LinearOptions:
         o = _lib.LinearOptions()

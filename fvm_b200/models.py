@@ -295,6 +295,25 @@ class ThermalModelA:
             p += s[lvl]
         return list(sizes[: nl.value]), out
 
+    def getLevelMatrix(self, level: int) -> dict:
+        """Level `level` of the AMG hierarchy as CSR {row, col, val, diag},
+        numbered as getHierarchy()'s coarseIndex numbers it (level 0 in
+        reference cell order); stored zeros left out."""
+        self._push()
+        lib = _lib.load()
+        n = ctypes.c_int(0)
+        nnz = ctypes.c_int(0)
+        check(lib.fvm_thermal_level_matrix(self._h, int(level), ctypes.byref(n), ctypes.byref(nnz), None, None, None,
+                                           None, 0))
+        row = np.zeros(n.value + 1, np.int32)
+        col = np.zeros(max(nnz.value, 1), np.int32)
+        val = np.zeros(max(nnz.value, 1))
+        diag = np.zeros(max(n.value, 1))
+        cap = max(nnz.value, n.value, 1)
+        check(lib.fvm_thermal_level_matrix(self._h, int(level), ctypes.byref(n), ctypes.byref(nnz), iptr(row),
+                                           iptr(col), dptr(val), dptr(diag), cap))
+        return {"row": row, "col": col[: nnz.value], "val": val[: nnz.value], "diag": diag[: n.value]}
+
     def getLaunchPlans(self):
         """[(threadsPerRow, threadsPerBlock)] of each level's smoother kernels
         as the autotuner chose them; ELL-32 levels: (-width, 0)."""
@@ -313,6 +332,17 @@ class ThermalModelA:
         keys = ["gs_pass_ms", "gs_pass_bytes", "residual_ms", "residual_bytes", "cycle_ms", "cycle_bytes", "levels",
                 "rows", "entries", "kernels_per_cycle", "colors"]
         return dict(zip(keys, out.tolist()))
+
+    def profileLevels(self, reps: int = 5) -> list:
+        """Per AMG level: CUDA-event timings and algorithmic bytes of the
+        cycle's kernels (see fvm_thermal_profile_levels)."""
+        self._push()
+        out = np.zeros(8 * 64)
+        nl = ctypes.c_int(0)
+        check(_lib.load().fvm_thermal_profile_levels(self._h, int(reps), ctypes.byref(nl), dptr(out), len(out)))
+        keys = ["rows", "entries", "smoother_ms", "smoother_bytes", "restrict_ms", "restrict_bytes", "prolong_ms",
+                "prolong_bytes"]
+        return [dict(zip(keys, out[8 * lvl: 8 * lvl + 8].tolist())) for lvl in range(nl.value)]
 
     def lastReport(self):
         return self._lastReport

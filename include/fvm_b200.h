@@ -79,6 +79,13 @@ typedef struct fvm_linear_options {
                                the fastest (plans never change results) */
   int planThreadsPerRow;    /* != 0: use this plan on every SELL-32 level instead (1, 2 or 4 */
   int planBlock;            /*   threads per row; 128 or 256 threads per block, 0 = 256) */
+  int setupOnDevice;        /* build the coarse levels on the GPU (parallel pairwise matching and
+                               Galerkin kernels) instead of the reference's sequential greedy
+                               aggregation; coarse levels then smooth with damped Jacobi. Not the
+                               reference's hierarchy: meant for precision = 1 */
+  int matchRounds;          /* handshake rounds per level of that matching (default 4) */
+  double matchBeta;         /* a neighbour is a matching candidate when its strength is at least
+                               this fraction of the row's strongest (default 0.25) */
 } fvm_linear_options;
 
 /* ThermalModelOptions (fvmbase/ThermalBC.h:33-67) + volume-condition constants */
@@ -101,7 +108,8 @@ typedef struct fvm_report {
   double initialNorm;      /* L1 norm of the first linear system */
   double lastNorm;         /* L1 norm of the last linear system / final residual */
   int converged;
-  double seconds;          /* device time, CUDA events around the call */
+  double seconds;          /* device time, CUDA events from after the upload of the
+                              changed cell fields to the end of the call */
   double setupSeconds;     /* host+device time rebuilding matrix and AMG levels */
   long long launches;      /* kernels and copies issued (graph nodes counted per replay) */
   int learnedSteps;        /* learned corrections tried (0 without a learned correction) */
@@ -172,6 +180,14 @@ int fvm_thermal_linear_system(fvm_thermal* t, double* diag, double* off, double*
  * their sizes, and the coarseIndex of each fine level concatenated. */
 int fvm_thermal_hierarchy(fvm_thermal* t, int* nLevels, int* sizes, int sizesCap,
                           int* coarseIndex, int ciCap);
+/* One level of the AMG hierarchy of the current linearization (no reference
+ * counterpart; for tests of the Galerkin products): its matrix as CSR with
+ * the diagonal apart, rows numbered as fvm_thermal_hierarchy's coarseIndex
+ * numbers them (level 0: reference cell order). Stored zeros are left out.
+ * *n and *nnz are always written; the arrays (row: n + 1, the others: cap
+ * entries) only when they fit. */
+int fvm_thermal_level_matrix(fvm_thermal* t, int level, int* n, int* nnz, int* row, int* col, double* val,
+                             double* diag, int cap);
 /* Launch plans of the smoother kernels, one per level of the current setup
  * (no reference counterpart): threads per row and threads per block as the
  * autotuner (or the forced plan) chose them; ELL-32 levels, whose kernels
@@ -185,6 +201,15 @@ int fvm_thermal_launch_plans(fvm_thermal* t, int* nLevels, int* threadsPerRow, i
  * out[6] levels, out[7] finest rows, out[8] finest stored entries,
  * out[9] kernels per cycle, out[10] colours of the finest level. */
 int fvm_thermal_profile(fvm_thermal* t, int reps, double* out11);
+/* Measurement hook (no reference counterpart): per AMG level, CUDA-event
+ * times in ms (mean of reps, each launch preceded by a 512 MB write that
+ * flushes L2) of the kernels one cycle runs there, in the cycle's
+ * precision, with their algorithmic bytes -- 8 doubles per level: rows,
+ * stored entries, smoother pass ms, bytes (one damped-Jacobi launch, or one
+ * Gauss-Seidel pass over all colours; on a coarsest level with the direct
+ * solve, the dense solve), restriction ms, bytes (as the cycle runs it),
+ * prolongation ms, bytes. out receives 8 * nLevels doubles when cap allows. */
+int fvm_thermal_profile_levels(fvm_thermal* t, int reps, int* nLevels, double* out, int cap);
 int fvm_thermal_destroy(fvm_thermal* t);
 
 /* Raw system path (testLinearSolver / MMReader + AMG::solve,
@@ -210,8 +235,10 @@ int fvm_csr_residual(int n, const int* row, const int* col, const double* diag, 
  * enqueued on `stream` (a cudaStream_t; null = default stream) and nothing
  * is allocated: the reduction's block sums live in a fixed 512 KB device
  * array inside the library, so n is limited to 16,777,216 rows (larger n
- * returns FVM_ERR_TOO_LARGE). The first call on each device looks up that
- * array's device address; make it outside any stream capture. Calls share
+ * returns FVM_ERR_TOO_LARGE). The first call in each CUDA context (the
+ * device's primary context, or a context the caller made current) looks up
+ * that array's device address; make it outside any stream capture. After
+ * cudaDeviceReset the next call looks the address up again. Calls share
  * the array: calls that overlap on one device race, so serialise them. */
 int fvm_csr_residual_device_noalloc(int n, const int* row, const int* col, const double* diag,
                                     const double* off, const double* x, const double* b, double* r,

@@ -52,6 +52,67 @@ def test_mm226_jacobi_matches_reference_history(refo):
     np.testing.assert_allclose(info["history"], rh, rtol=1e-12, atol=0)
 
 
+@pytest.mark.parametrize("cycle", ["W", "F"])
+def test_mm226_w_and_f_cycles_match_reference_history(refo, cycle):
+    """W and F cycles (AMG::cycle, fvmbase/AMG.cpp:105-110) with the
+    reference-ordered Gauss-Seidel: residual history equal to the reference's
+    own W / F cycle history to 1e-12 relative."""
+    z = load_fixture("mm226.npz")
+    ct = {"W": fvmbaseExt.AMG.W_CYCLE, "F": fvmbaseExt.AMG.F_CYCLE}[cycle]
+    _, _, rh, _ = refo.amg_csr(z["row"], z["col"], z["diag"], z["off"], z["b"], max_iter=25, rel_tol=1e-30,
+                               n_pre=1, n_post=1, cycle=ct)
+    a = _amg(nMaxIterations=25, relativeTolerance=1e-30, absoluteTolerance=0.0, nPreSweeps=1, nPostSweeps=1,
+             cycleType=ct, smootherOrdering=fvmbaseExt.AMG.SEQUENTIAL)
+    _, info = a.solve_csr(z["row"], z["col"], z["diag"], z["off"], z["b"])
+    assert len(info["history"]) == len(rh)
+    np.testing.assert_allclose(info["history"], rh, rtol=1e-12, atol=0)
+
+
+@pytest.mark.parametrize("cycle", ["W", "F"])
+@pytest.mark.parametrize("precision", [0, 1])
+def test_w_and_f_cycles_converge_to_reference_field(refo, cycle, precision):
+    """Multicolour W / F cycles (FP64, and FP32 under FP64 refinement) inside
+    the thermal outer loop: converged field within 1e-8 of the reference's
+    own W / F cycle solve on the jittered tets."""
+    mesh, f = _synthetic("tet")
+    bcs = {gid: v for gid, v in f["bc"].items()}
+    fields = {"conductivity": f["k"], "source": f["s"]}
+    ct = {"W": fvmbaseExt.AMG.W_CYCLE, "F": fvmbaseExt.AMG.F_CYCLE}[cycle]
+    amg = _amg(nPreSweeps=1, nPostSweeps=1, relativeTolerance=1e-10, nMaxIterations=500, cycleType=ct,
+               precision=precision)
+    tm, tf, m = gpu_model(mesh, bcs, solver=amg, fields=fields, opts={"relativeTolerance": 1e-10})
+    _converge(tm)
+    T = tf.temperature[m.getCells()][: mesh["nCells"]]
+    r = ref_model(refo, mesh, bcs, fields=fields, n_pre=1, n_post=1, lin_rel=1e-10, max_iter=500, rel=1e-10,
+                  cycle=ct)
+    norms, _ = r.advance(200)
+    assert norms[-1] / norms[0] < 1e-10
+    assert rel_l2(T, r.get_field(0)[: mesh["nCells"]]) <= TOL_FIELD
+
+
+def test_nan_conductivity_returns_nan_status():
+    """A NaN conductivity (a host-made failure) reaches the residual norm of
+    the first linear system: advance() raises the NaN status (FVM_ERR_NAN),
+    with no GPU fault, and the model stays usable with good data."""
+    mesh, f = _synthetic("quad")
+    bcs = {gid: v for gid, v in f["bc"].items()}
+    k = np.array(f["k"], dtype=np.float64)
+    k[len(k) // 2] = np.nan
+    amg = _amg(nPreSweeps=1, nPostSweeps=1, relativeTolerance=1e-10, nMaxIterations=100)
+    tm, tf, m = gpu_model(mesh, bcs, solver=amg, fields={"conductivity": k, "source": f["s"]},
+                          opts={"relativeTolerance": 1e-10})
+    from fvm_b200._lib import FvmError
+
+    with pytest.raises(FvmError) as err:
+        tm.advance(20)
+    assert err.value.status == 4  # FVM_ERR_NAN
+    assert "finite" in str(err.value)
+    tm.init()
+    tf.conductivity[m.getCells()] = f["k"]
+    tf.source[m.getCells()] = f["s"]
+    _converge(tm)
+
+
 @pytest.mark.parametrize("precision", [0, 1])
 @pytest.mark.parametrize("solver", ["AMG", "CG", "BCGStab"])
 def test_mm226_multicolor_converges_to_reference_solution(refo, solver, precision):
@@ -514,3 +575,45 @@ def test_gpu_inverse_dominant_single_level(n):
     assert list(info["levelSizes"]) == []
     assert info["iterations"] == 1
     assert rel_l2(x, xref) <= 1e-10
+
+
+# ---------------------------------------------------------------------------
+# config 0 at its stated size: 256 x 256 jittered quads, 65,536 cells
+
+
+@pytest.fixture(scope="module")
+def config0_reference(refo):
+    """The reference's own FP64 CPU solve of config 0 (ThermalModel<double>
+    + AMG V(1,1), inner relTol 0.1, outer 1e-10), computed once."""
+    mesh, f = meshgen.config0(n=256, seed=0)
+    bcs = {gid: v for gid, v in f["bc"].items()}
+    fields = {"conductivity": f["k"], "source": f["s"]}
+    r = ref_model(refo, mesh, bcs, fields=fields, n_pre=1, n_post=1, lin_rel=0.1, max_iter=200, rel=1e-10)
+    norms, _ = r.advance(500)
+    assert norms[-1] / norms[0] < 1e-10
+    return mesh, bcs, fields, r.get_field(0)[: mesh["nCells"]]
+
+
+@pytest.mark.parametrize("variant", ["plain", "mixed-cg"])
+def test_config0_full_size_matches_reference(config0_reference, variant):
+    """Config 0 as stated (65,536 cells, AMG V(1,1), coarsening to at most
+    100 rows, outer relative residual 1e-10): the plain FP64 GPU AMG and the
+    mixed-precision CG + FP32 V(0,2) against the reference's FP64 solve,
+    relative L2 <= 1e-8."""
+    mesh, bcs, fields, Tr = config0_reference
+    amg = _amg(nPreSweeps=1, nPostSweeps=1, relativeTolerance=0.1, nMaxIterations=200, coarsestSize=100)
+    solver = amg
+    if variant == "mixed-cg":
+        amg.precision = fvmbaseExt.AMG.MIXED
+        amg.coarseSolver = fvmbaseExt.AMG.COARSE_DIRECT
+        amg.coarsestSize = 4096
+        amg.coarseJacobiRows = 1 << 30
+        amg.nPreSweeps, amg.nPostSweeps = 0, 2
+        solver = fvmbaseExt.CG()
+        solver.preconditioner = amg
+        solver.relativeTolerance = 0.1
+        solver.nMaxIterations = 200
+    tm, tf, m = gpu_model(mesh, bcs, solver=solver, fields=fields, opts={"relativeTolerance": 1e-10})
+    _converge(tm, n_outer=500)
+    T = tf.temperature[m.getCells()][: mesh["nCells"]]
+    assert rel_l2(T, Tr) <= TOL_FIELD

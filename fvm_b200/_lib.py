@@ -115,6 +115,15 @@ _SIGS = {
     "fvm_thermal_level_matrix": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, c_int_p, c_int_p, c_int_p, c_int_p,
                                                  c_double_p, c_double_p, ctypes.c_int]),
     "fvm_thermal_profile_levels": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, c_int_p, c_double_p, ctypes.c_int]),
+    "fvm_fluent_read": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_void_p)]),
+    "fvm_fluent_cell_zones": (ctypes.c_int, [ctypes.c_void_p, c_int_p]),
+    "fvm_fluent_mesh_sizes": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, c_int_p]),
+    "fvm_fluent_mesh_arrays": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, c_double_p, c_int_p, c_int_p, c_int_p,
+                                               c_int_p, c_int_p]),
+    "fvm_fluent_group_type": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_char_p,
+                                              ctypes.c_int]),
+    "fvm_fluent_mesh_create": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
+    "fvm_fluent_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "fvm_thermal_hierarchy": (ctypes.c_int, [ctypes.c_void_p, c_int_p, c_int_p, ctypes.c_int, c_int_p,
                                              ctypes.c_int]),
     "fvm_thermal_profile": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, c_double_p]),

@@ -30,7 +30,7 @@ CXX_FLAGS = ["-O3", "-std=c++17", "-fPIC", "-ffp-contract=off", "-Wall", "-Wno-u
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--expt-relaxed-constexpr",
               "-Xcompiler", "-fPIC,-ffp-contract=off"] + ARCH
 
-HOST_SOURCES = ["mesh.cpp", "amg_setup.cpp", "capi.cpp"]
+HOST_SOURCES = ["mesh.cpp", "amg_setup.cpp", "capi.cpp", "fluent.cpp"]
 CUDA_SOURCES = ["kernels.cu", "solver.cu", "thermal.cu", "residual_noalloc.cu", "learned.cu", "amg_device.cu"]
 # device code free to contract a * b + c into one rounding
 FMA_SOURCES = {"learned.cu", "amg_device.cu"}

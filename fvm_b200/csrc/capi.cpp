@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <cstring>
+#include <map>
 #include <memory>
 #include <string>
 
@@ -12,6 +13,7 @@
 #include "mesh.hpp"
 #include "learned.hpp"
 #include "solver.hpp"
+#include "fluent.hpp"
 #include "thermal.hpp"
 
 using namespace fvm;
@@ -203,6 +205,95 @@ int fvm_mesh_create(int dim, int nCells, int nNodes, const double* xyz, int nFac
                                           faceNodeCount, nGroups, groupSize));
     *out = new fvm_mesh{m};
   });
+}
+
+struct fvm_fluent {
+  std::unique_ptr<FluentCase> file;
+  std::map<int, FluentMeshArrays> meshes;
+  const FluentMeshArrays& mesh(int zone) {
+    auto it = meshes.find(zone);
+    if (it == meshes.end()) it = meshes.emplace(zone, file->mesh(zone)).first;
+    return it->second;
+  }
+};
+
+int fvm_fluent_read(const char* path, fvm_fluent** out) {
+  return guarded([&] {
+    FVM_REQUIRE(path && out, kBadArgument, "null argument");
+    *out = nullptr;
+    std::unique_ptr<fvm_fluent> r(new fvm_fluent);
+    r->file.reset(new FluentCase(path));
+    *out = r.release();
+  });
+}
+
+int fvm_fluent_cell_zones(const fvm_fluent* r, int* n) {
+  return guarded([&] {
+    FVM_REQUIRE(r && n, kBadArgument, "null argument");
+    *n = r->file->numCellZones();
+  });
+}
+
+int fvm_fluent_mesh_sizes(fvm_fluent* r, int zone, int* out) {
+  return guarded([&] {
+    FVM_REQUIRE(r && out, kBadArgument, "null argument");
+    const FluentMeshArrays& m = r->mesh(zone);
+    out[0] = m.dim;
+    out[1] = m.nCells;
+    out[2] = (int)(m.xyz.size() / 3);
+    out[3] = (int)m.faceNodeCount.size();
+    out[4] = (int)m.faceNodes.size();
+    out[5] = (int)m.groupSize.size();
+  });
+}
+
+int fvm_fluent_mesh_arrays(fvm_fluent* r, int zone, double* xyz, int* faceCells, int* faceNodes,
+                           int* faceNodeCount, int* groupSize, int* groupId) {
+  return guarded([&] {
+    FVM_REQUIRE(r, kBadArgument, "null argument");
+    const FluentMeshArrays& m = r->mesh(zone);
+    if (xyz) std::copy(m.xyz.begin(), m.xyz.end(), xyz);
+    if (faceCells) std::copy(m.faceCells.begin(), m.faceCells.end(), faceCells);
+    if (faceNodes) std::copy(m.faceNodes.begin(), m.faceNodes.end(), faceNodes);
+    if (faceNodeCount) std::copy(m.faceNodeCount.begin(), m.faceNodeCount.end(), faceNodeCount);
+    if (groupSize) std::copy(m.groupSize.begin(), m.groupSize.end(), groupSize);
+    if (groupId) std::copy(m.groupId.begin(), m.groupId.end(), groupId);
+  });
+}
+
+int fvm_fluent_group_type(fvm_fluent* r, int zone, int group, char* buf, int cap) {
+  return guarded([&] {
+    FVM_REQUIRE(r && buf && cap > 0, kBadArgument, "null argument");
+    const FluentMeshArrays& m = r->mesh(zone);
+    FVM_REQUIRE(group >= 0 && group < (int)m.groupType.size(), kBadArgument, "no such face group");
+    const std::string& t = m.groupType[group];
+    FVM_REQUIRE((int)t.size() < cap, kBadArgument, "buffer too small for the group type");
+    std::memcpy(buf, t.c_str(), t.size() + 1);
+  });
+}
+
+int fvm_fluent_mesh_create(fvm_fluent* r, int zone, fvm_mesh** out) {
+  return guarded([&] {
+    FVM_REQUIRE(r && out, kBadArgument, "null argument");
+    *out = nullptr;
+    const FluentMeshArrays& m = r->mesh(zone);
+    std::shared_ptr<HostMesh> hm(make_mesh(m.dim, m.nCells, (int)(m.xyz.size() / 3), m.xyz.data(),
+                                           (int)m.faceNodeCount.size(), m.faceCells.data(), m.faceNodes.data(),
+                                           m.faceNodeCount.data(), (int)m.groupSize.size(), m.groupSize.data()));
+    bool symmetry = false;
+    for (size_t g = 1; g < m.groupSize.size(); g++) {
+      hm->groups[g].id = m.groupId[g];
+      hm->groups[g].type = m.groupType[g];
+      symmetry = symmetry || m.groupType[g] == "symmetry";
+    }
+    if (symmetry) hm->build();  // ghost centroids depend on the group type
+    *out = new fvm_mesh{hm};
+  });
+}
+
+int fvm_fluent_destroy(fvm_fluent* r) {
+  delete r;
+  return FVM_OK;
 }
 
 int fvm_mesh_set_group(fvm_mesh* h, int group, int id, const char* type) {

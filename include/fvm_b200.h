@@ -133,6 +133,34 @@ int fvm_mesh_create(int dim, int nCells, int nNodes, const double* xyz, int nFac
 /* FaceGroup id/type of group g (g >= 1), as imported meshes carry them
  * (fvmbase/Mesh.h FaceGroup). */
 int fvm_mesh_set_group(fvm_mesh* m, int group, int id, const char* type);
+
+/* Fluent case-file import (importers.FluentReader, the reference's
+ * src/modules/importers/FluentReader.cpp: readMesh() :572-611 reads the
+ * file, getMeshList() :954-1040 and createMesh :696-952 turn each cell zone
+ * into a Mesh). ASCII and binary (single / double precision) sections.
+ * Not covered, with FVM_ERR_UNSUPPORTED: periodic face pairs and faces
+ * between two cell zones (interfaces). */
+typedef struct fvm_fluent fvm_fluent;
+int fvm_fluent_read(const char* path, fvm_fluent** out);
+/* number of cell zones = length of getMeshList() */
+int fvm_fluent_cell_zones(const fvm_fluent* r, int* n);
+/* sizes of the mesh of cell zone `zone` (ascending zone id): dim, nCells,
+ * nNodes, nFaces, faceNodes entries, face groups (interior + boundary zones) */
+int fvm_fluent_mesh_sizes(fvm_fluent* r, int zone, int* out6);
+/* its arrays, as fvm_mesh_create takes them: xyz (3 per node), faceCells
+ * (2 per face; boundary faces (cell, nCells + k)), faceNodes, faceNodeCount,
+ * groupSize, and groupId (Fluent zone id per group, 0 for the interior).
+ * Faces: interior zones, then boundary zones, ascending zone id; nodes in
+ * first-visit order over the zone's cells and their faces. Null arrays are
+ * skipped. */
+int fvm_fluent_mesh_arrays(fvm_fluent* r, int zone, double* xyz, int* faceCells, int* faceNodes,
+                           int* faceNodeCount, int* groupSize, int* groupId);
+/* type name of face group `group` ("interior", then the zones' Fluent types
+ * such as "wall" or "velocity-inlet"), NUL-terminated into buf */
+int fvm_fluent_group_type(fvm_fluent* r, int zone, int group, char* buf, int cap);
+/* getMeshList()[zone]: the mesh, with its boundary groups' ids and types */
+int fvm_fluent_mesh_create(fvm_fluent* r, int zone, fvm_mesh** out);
+int fvm_fluent_destroy(fvm_fluent* r);
 /* out: dim, nCells, nGhost, nNodes, nFaces, nnz(cellCells), nGroups */
 int fvm_mesh_sizes(const fvm_mesh* m, int* out7);
 /* Mesh::getCellCells + CRConnectivity::getPairToColMapping

@@ -14,6 +14,9 @@ Fixtures (all inputs are the reference's, converted to plain arrays):
   cav32_matrix.npz  src/fvm/test/cav32.cas as read by FluentReader, and the
                   golden linear system of src/fvm/test/THERMAL_MATRIX/GOLDEN
                   (matrix_mesh0.mat, matrix.rhs).
+  <mesh>.cas.gz   the Fluent case files of those tests (src/fvm/test/cav32.cas,
+                  cav32_thermal.cas, tri_894.cas, cav_hexa.cas, cav_tetra.cas),
+                  gzip-compressed, as inputs of the product's own importer.
   ptest_<case>.npz  the meshes of src/fvm/test/PARALLEL_TESTS *_THERMALSOLVER
                   np=1 cases and their golden cell temperatures
                   (SOLVER_AMG/ThermalSolver/<CASE>/proc1/GOLDEN/temp_proc0.dat),
@@ -109,8 +112,19 @@ def ptest(test_dir: str, case: str, cas: str) -> None:
                         T_gold=T_gold[idx])
 
 
+def fluent_cases(test_dir: str) -> None:
+    import gzip
+    import shutil
+
+    for cas in ("cav32.cas", "cav32_thermal.cas", "tri_894.cas", "cav_hexa.cas", "cav_tetra.cas"):
+        with open(os.path.join(test_dir, cas), "rb") as src, \
+                gzip.GzipFile(os.path.join(HERE, cas + ".gz"), "wb", mtime=0) as dst:
+            shutil.copyfileobj(src, dst)
+
+
 def main(reference_root: str = "/root/reference") -> None:
     test_dir = os.path.join(reference_root, "src", "fvm", "test")
+    fluent_cases(test_dir)
     mm226(test_dir)
     cav32_matrix(test_dir)
     for case, cas in (("QUAD_1024", "cav32_thermal.cas"), ("TRI_894", "tri_894.cas"),

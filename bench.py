@@ -152,13 +152,16 @@ def make_workload(name: str):
 
 def train_learned(gen, inner_rel, seeds=(101, 102), n_outer=4, per_solve=3, steps=600, lr=1e-3):
     """Learned correction trained on the GPU (the library's own forward /
-    backward kernels and Adam) on pairs harvested from plain-solver runs of
-    other draws of the workload (other mesh jitter and conductivity seeds).
-    Not timed: it is the offline training stage."""
+    backward kernels and Adam) on residuals harvested from plain-solver runs
+    of other draws of the workload (other mesh jitter and conductivity
+    seeds), with the residual objective |r + A d|^2 / |r|^2. Not timed: it
+    is the offline training stage. The solve uses the network only when the
+    residual reduction it reaches on its pairs pays for its cost."""
     from fvm_b200.learned import LearnedCorrection
 
     t0 = time.perf_counter()
     lc = LearnedCorrection(seed=0)
+    lc.setObjective(LearnedCorrection.RESIDUAL)
     for seed in seeds:
         mesh, f = gen(seed)
         s = Solve(mesh, f, "plain", inner_rel)
@@ -174,8 +177,12 @@ def train_learned(gen, inner_rel, seeds=(101, 102), n_outer=4, per_solve=3, step
     t1 = time.perf_counter()
     losses = lc.train(steps=steps, lr=lr, seed=0)  # returns after the device has finished
     train_s = time.perf_counter() - t1
-    info = {"pairs": lc.numPairs(), "instances": len(seeds), "train_steps": steps,
-            "loss_before": before, "loss_after": lc.evaluate(),
+    after = lc.evaluate()
+    factor = lc.residualFactor()
+    info = {"objective": "residual |r + A d|^2 / |r|^2", "pairs": lc.numPairs(), "instances": len(seeds),
+            "train_steps": steps, "loss_before": before, "loss_after": after,
+            "residual_factor": factor, "useful_factor": 0.5,
+            "used_in_solve": bool(factor <= 0.5),
             "loss_first50": float(np.mean(losses[:50])), "loss_last50": float(np.mean(losses[-50:])),
             "dense_layers": "tcgen05 tf32" if lc.tensorCores else "fp32 cuda cores",
             "train_seconds": train_s, "ms_per_train_step": 1e3 * train_s / max(steps, 1),
@@ -237,6 +244,11 @@ def solver_for(variant: str, inner_rel: float):
         amg.jacobiWeight = 2.0 / 3.0
         amg.nPreSweeps = 0
         amg.nPostSweeps = 2
+        if not HOST_SETUP:
+            # GPU-built levels: pairs of pairs (aggregates of about 4 rows),
+            # one damped-Jacobi sweep on each level below the finest
+            amg.matchPasses = 2
+            amg.coarsePostSweeps = 1
     if variant in ("plain-cg", "mixed", "learned"):
         cg = fvmbaseExt.CG()
         cg.preconditioner = amg
@@ -456,6 +468,131 @@ def bench_batch(args, dist, peaks, peak_kind):
         print(json.dumps(line))
 
 
+def bench_transient(args, dist, peaks, peak_kind):
+    """config 4 as stated: 200^3 hexes (8M cells), 50 backward-Euler steps
+    (dt = 1e-3, updateTime between steps), every step solved to outer
+    relative residual 1e-10. Arms, each a full 50-step run from T0 = 300:
+    plain FP64 AMG (the reference's default solver on the GPU), mixed
+    (CG + FP32 V-cycle), and mixed + learned, whose network is retrained on
+    pairs harvested from the first 5 plain steps (an untimed stage). The
+    AMG hierarchy is built on the first step and kept (the matrix does not
+    change between steps). Times are device times of advance() per step."""
+    from fvm_b200.learned import LearnedCorrection
+
+    mesh, fields, desc, gen, seed = make_workload("config4")
+    n_cells = mesh["nCells"]
+    n_steps = args.time_steps
+
+    def run(variant, lc=None, harvest=None):
+        s = Solve(mesh, fields, variant, args.inner_rel)
+        if lc is not None:
+            s.tm.setLearnedCorrection(lc)
+        cells = s.m.getCells()
+        s.tm.init()
+        s.tf.conductivity[cells] = s.k
+        s.tf.source[cells] = s.s
+        s.tf.specificHeat[cells] = s.rc
+        per, outer, cycles, kept, tried = [], [], [], 0, 0
+        t0 = time.perf_counter()
+        for step in range(n_steps if harvest is None else harvest[1]):
+            if harvest is not None:
+                harvest[0].harvest(s.tm, nOuter=200, perSolve=3, relativeTolerance=1e-8, maxCycles=100)
+            else:
+                rep = s.tm.advance(200)
+                rep = s.tm.lastReport()
+                if not rep.converged:
+                    raise RuntimeError("%s: step %d did not converge" % (variant, step))
+                per.append(rep.seconds)
+                outer.append(rep.iterations)
+                cycles.append(rep.linearIterations)
+                kept += rep.learnedAccepted
+                tried += rep.learnedSteps
+            s.tm.updateTime()
+        wall = time.perf_counter() - t0
+        T = s.tf.temperature[cells][:n_cells].copy()
+        del s
+        return {"per_step_s": per, "total_s": float(sum(per)), "outer": outer, "cycles": cycles,
+                "learned_tried": tried, "learned_kept": kept, "wall_s": wall, "T": T}
+
+    dist.barrier()
+    sampler = ClockSampler(dist.local)
+    sampler.__enter__()
+    plain = run("plain")
+    mixed = run("mixed")
+    lc = LearnedCorrection(seed=0)
+    t_train = time.perf_counter()
+    run("plain", harvest=(lc, 5))
+    pairs = lc.numPairs()
+    losses = lc.train(steps=args.train_steps, lr=1e-3, seed=0)
+    train_s = time.perf_counter() - t_train
+    learned = run("learned", lc=lc)
+    sampler.__exit__()
+    dist.barrier()
+    if dist.rank != 0:
+        return
+    rel = {k: float(np.linalg.norm(v["T"] - plain["T"]) / np.linalg.norm(plain["T"]))
+           for k, v in (("mixed", mixed), ("mixed_learned", learned))}
+
+    def summary(r):
+        return {"total_s": r["total_s"], "first_step_s": r["per_step_s"][0],
+                "mean_later_step_s": float(np.mean(r["per_step_s"][1:])) if len(r["per_step_s"]) > 1 else None,
+                "outer_per_step": r["outer"], "cycles_per_step": r["cycles"],
+                "learned_tried": r["learned_tried"], "learned_kept": r["learned_kept"]}
+
+    cpu = None
+    if dist.world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_reference_transient(mesh, fields, args.inner_rel, args.ref_time_steps)
+    head = learned
+    line = {
+        "metric": METRIC, "value": head["total_s"], "unit": "s", "n_gpus": args.gpus, "steps": 1, "warmup": 0,
+        "ms_per_step": head["total_s"] * 1e3 / max(n_steps, 1), "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 V-cycle / f64 refinement", "data": "synthetic",
+        "config": {"workload": desc.replace("one backward-Euler step (dt = 1e-3) from T0 = 300",
+                                            "%d backward-Euler steps (dt = 1e-3) from T0 = 300" % n_steps),
+                   "cells": n_cells, "time_steps": n_steps, "outer_rel": 1e-10, "inner_rel": args.inner_rel,
+                   "value": "device time of all %d steps of the mixed + learned run" % n_steps},
+        "plain_fp64_s": plain["total_s"], "mixed_without_learned_s": mixed["total_s"],
+        "speedup_vs_plain_fp64": plain["total_s"] / head["total_s"],
+        "field_rel_l2_vs_plain_after_last_step": rel,
+        "arms": {"plain": summary(plain), "mixed": summary(mixed), "mixed_learned": summary(learned)},
+        "learned_training": {"pairs": pairs, "from": "first 5 plain steps", "train_steps": args.train_steps,
+                             "loss_first50": float(np.mean(losses[:50])), "loss_last50": float(np.mean(losses[-50:])),
+                             "seconds": train_s},
+        "cpu_baseline": cpu,
+        "clocks": sampler.summary(),
+    }
+    print(json.dumps(line))
+
+
+def cpu_reference_transient(mesh, fields, inner_rel, n_steps):
+    """The compiled reference (one thread) on the first n_steps backward-Euler
+    steps of the same 8M-cell problem, each to outer 1e-10: a bounded sample
+    of the 50-step run, stated as such."""
+    from oracle import ref
+    from fvm_b200.meshgen import extend_to_ghosts
+
+    if not ref.available() or n_steps <= 0:
+        return None
+    r = ref.RefThermal(mesh)
+    r.set_options(n_pre=1, n_post=1, max_iter=200, lin_rel=inner_rel, rel=1e-10, transient=True, dt=1e-3)
+    for gid, (kind, val) in fields["bc"].items():
+        r.set_bc(gid, 0 if kind == "T" else 1, [val] if kind == "T" else [None, val])
+    r.init()
+    r.set_field(1, extend_to_ghosts(mesh, fields["k"]))
+    r.set_field(2, extend_to_ghosts(mesh, fields["s"]))
+    r.set_field(3, extend_to_ghosts(mesh, fields["rc"]))
+    secs = []
+    for _ in range(n_steps):
+        _, sec = r.advance(200)
+        secs.append(sec)
+        r.update_time()
+    del r
+    return {"value": float(sum(secs)), "unit": "s", "cores": 1, "kind": "reference",
+            "sample": ("the compiled reference (ThermalModel<double> + AMG V(1,1), one thread, host %s) on the first "
+                       "%d of the backward-Euler steps, each to outer 1e-10: %s s per step (a bounded sample of the "
+                       "run)" % (_host_cpu(), n_steps, ", ".join("%.1f" % x for x in secs)))}
+
+
 def cpu_reference_batch(ms, inner_rel, sample=6):
     """The reference solves each mesh with its own ThermalModel<double>
     (one core). Bounded sample: full solves (to 1e-10) of `sample` meshes
@@ -504,6 +641,9 @@ def main():
                     help="comma list of plain, plain-cg, mixed, learned (mixed + learned correction)")
     ap.add_argument("--train-steps", type=int, default=600)
     ap.add_argument("--batch-meshes", type=int, default=512, help="config2: number of meshes")
+    ap.add_argument("--time-steps", type=int, default=50, help="config4: backward-Euler steps")
+    ap.add_argument("--ref-time-steps", type=int, default=1,
+                    help="config4: steps of the CPU reference sample")
     ap.add_argument("--host-setup", action="store_true",
                     help="mixed path: AMG levels by the reference's greedy aggregation on the host instead of the "
                          "GPU-built hierarchy")
@@ -515,6 +655,10 @@ def main():
     peaks, peak_kind = load_peaks()
     if args.workload == "config2" and args.impl == "product":
         bench_batch(args, dist, peaks, peak_kind)
+        dist.close()
+        return
+    if args.workload == "config4" and args.impl == "product":
+        bench_transient(args, dist, peaks, peak_kind)
         dist.close()
         return
     if args.workload == "config2":

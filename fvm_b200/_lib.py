@@ -47,6 +47,8 @@ class LinearOptions(ctypes.Structure):
         ("setupOnDevice", ctypes.c_int),
         ("matchRounds", ctypes.c_int),
         ("matchBeta", ctypes.c_double),
+        ("matchPasses", ctypes.c_int),
+        ("coarsePostSweeps", ctypes.c_int),
     ]
 
 
@@ -124,6 +126,10 @@ _SIGS = {
                                               ctypes.c_int]),
     "fvm_fluent_mesh_create": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
     "fvm_fluent_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "fvm_learned_wait_probe": (ctypes.c_int, [ctypes.c_uint, c_int_p]),
+    "fvm_learned_set_objective": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "fvm_learned_set_useful_factor": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double]),
+    "fvm_learned_residual_factor": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]),
     "fvm_thermal_hierarchy": (ctypes.c_int, [ctypes.c_void_p, c_int_p, c_int_p, ctypes.c_int, c_int_p,
                                              ctypes.c_int]),
     "fvm_thermal_profile": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, c_double_p]),

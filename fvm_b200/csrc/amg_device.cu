@@ -357,7 +357,7 @@ __global__ void __launch_bounds__(32 * kGalWarps) k_galerkin(LevelRows a, int nc
       const size_t o = (size_t)cbase + 32 * (size_t)slot;
       ccols[o] = Je;
       cvals[o] = s;
-      cvalsF[o] = (float)s;
+      if (cvalsF) cvalsF[o] = (float)s;
     }
     nUnique += __popc(m);
   }
@@ -369,7 +369,7 @@ __global__ void __launch_bounds__(32 * kGalWarps) k_galerkin(LevelRows a, int nc
       const size_t o = (size_t)cbase + 32 * (size_t)slot;
       ccols[o] = I;
       cvals[o] = 0.0;
-      cvalsF[o] = 0.f;
+      if (cvalsF) cvalsF[o] = 0.f;
     }
   }
   if (lane == 0) {
@@ -385,7 +385,7 @@ __global__ void __launch_bounds__(32 * kGalWarps) k_galerkin(LevelRows a, int nc
         if (J[e] == I) d += V[e];
     }
     cdiag[I] = d;
-    cdiagF[I] = (float)d;
+    if (cdiagF) cdiagF[I] = (float)d;
   }
 }
 
@@ -410,6 +410,11 @@ __global__ void k_slice_meta(int n, const int* __restrict__ sliceOff, int4* meta
   sliceRows[s] = rows;
   for (int r = 0; r < rows; r++) rowSlice[r0 + r] = s;
   atomicMax(maxWidth, w);
+}
+
+__global__ void k_compose(int n, int* ci, const int* __restrict__ ci2) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) ci[i] = ci2[ci[i]];
 }
 
 __global__ void k_dominance(LevelRows a, int* flag) {
@@ -491,6 +496,10 @@ void slice_meta_fill(int n, const int* sliceOff, int4* meta, int* sliceRow, int*
                      int* maxWidth, cudaStream_t st) {
   const int ns = cdiv(n, 32);
   k_slice_meta<<<cdiv(ns, kT), kT, 0, st>>>(n, sliceOff, meta, sliceRow, sliceRows, rowSlice, maxWidth);
+}
+
+void compose_index(int n, int* ci, const int* ci2, cudaStream_t st) {
+  if (n > 0) k_compose<<<cdiv(n, kT), kT, 0, st>>>(n, ci, ci2);
 }
 
 void dominance_check(const LevelRows& a, int* flag, cudaStream_t st) {
@@ -664,28 +673,20 @@ void AmgHierarchy::buildDevice(const FinestDevice& in, const SolverOptions& opt)
   int* hflags = reinterpret_cast<int*>(pinnedScalars());
   lap("level 0 values");
 
-  for (int l = 0;; l++) {
-    DevLevel& f = lv_[l];
-    if (l >= opt.maxCoarseLevels || lv_.size() + 1 > maxL) break;
-    if (opt.coarsestSize > 0 ? f.n <= opt.coarsestSize : f.n <= 3) break;
-    const dev::LevelRows a{f.n, f.cols, f.vals, f.diag, f.meta, f.rowSlice, f.ellWidth};
-    int* ci = (int*)arena_.alloc(size_class(sizeof(int) * f.n));
-    dev::aggregate_pairs(a, opt.matchBeta, opt.matchRounds, l == 0 ? fp.iperm : nullptr, w, ci, st);
-    CUDA_OK(cudaMemcpyAsync(hflags, w.pos + f.n, sizeof(int), cudaMemcpyDeviceToHost, st));
-    CUDA_OK(cudaStreamSynchronize(st));
-    const int nc = hflags[0];
-    // a level that no longer shrinks is the coarsest
-    if (nc <= 0 || nc >= f.n || (double)nc > 0.9 * f.n) break;
-    f.ci = ci;
-    f.nCoarse = nc;
-    f.c2fRow = (int*)arena_.alloc(size_class(sizeof(int) * (nc + 1)));
-    f.c2fCol = (int*)arena_.alloc(size_class(sizeof(int) * f.n));
-    dev::coarse_to_fine(f.n, nc, ci, w.flag, f.c2fRow, f.c2fCol, w.scan, st);
-    // coarse level: counts, slice widths and offsets, then the entries
+  // Coarse level of `fine` under the aggregation ci (nc rows): coarse-to-fine
+  // lists into fine's c2fRow / c2fCol, then counts, slice widths and
+  // offsets, then the Galerkin entries into c (FP32 copies when f32).
+  auto galerkin = [&](DevLevel& fine, int* ci, int nc, DevLevel& c, bool f32) -> long long {
+    fine.ci = ci;
+    fine.nCoarse = nc;
+    fine.c2fRow = (int*)arena_.alloc(size_class(sizeof(int) * (nc + 1)));
+    fine.c2fCol = (int*)arena_.alloc(size_class(sizeof(int) * fine.n));
+    dev::coarse_to_fine(fine.n, nc, ci, w.flag, fine.c2fRow, fine.c2fCol, w.scan, st);
+    const dev::LevelRows af{fine.n, fine.cols, fine.vals, fine.diag, fine.meta, fine.rowSlice, fine.ellWidth};
     const int nSlices = (nc + 31) / 32;
     int* sliceOff = (int*)arena_.alloc(size_class(sizeof(int) * (nSlices + 1)));
     CUDA_OK(cudaMemsetAsync(flags, 0, 3 * sizeof(int), st));
-    dev::galerkin_count(a, nc, ci, f.c2fRow, f.c2fCol, w.best, flags, st);
+    dev::galerkin_count(af, nc, ci, fine.c2fRow, fine.c2fCol, w.best, flags, st);
     dev::slice_widths(nc, w.best, w.join, st);
     dev::scan_exclusive(w.join, sliceOff, nSlices, w.scan, st);
     CUDA_OK(cudaMemcpyAsync(hflags, sliceOff + nSlices, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -694,9 +695,7 @@ void AmgHierarchy::buildDevice(const FinestDevice& in, const SolverOptions& opt)
     const long long E = hflags[0];
     FVM_REQUIRE(hflags[1] == 0, kUnsupported,
                 "device-built hierarchy: an aggregate's entries exceed the Galerkin kernel's capacity");
-    lv_.emplace_back();
-    DevLevel& c = lv_.back();
-    DevLevel& fine = lv_[l];
+    const size_t e1 = (size_t)std::max<long long>(E, 1);
     c.n = nc;
     c.nColors = 1;
     c.nSlices = nSlices;
@@ -704,23 +703,58 @@ void AmgHierarchy::buildDevice(const FinestDevice& in, const SolverOptions& opt)
     c.entries = (size_t)E;
     c.ellWidth = 0;
     c.sliceOff = sliceOff;
-    c.cols = (int*)arena_.alloc(size_class(sizeof(int) * (size_t)std::max<long long>(E, 1)));
-    c.vals = (double*)arena_.alloc(size_class(sizeof(double) * (size_t)std::max<long long>(E, 1)));
-    c.valsF = (float*)arena_.alloc(size_class(sizeof(float) * (size_t)std::max<long long>(E, 1)));
+    c.cols = (int*)arena_.alloc(size_class(sizeof(int) * e1));
+    c.vals = (double*)arena_.alloc(size_class(sizeof(double) * e1));
     c.diag = (double*)arena_.alloc(size_class(sizeof(double) * nc));
-    c.diagF = (float*)arena_.alloc(size_class(sizeof(float) * nc));
+    c.valsF = f32 ? (float*)arena_.alloc(size_class(sizeof(float) * e1)) : nullptr;
+    c.diagF = f32 ? (float*)arena_.alloc(size_class(sizeof(float) * nc)) : nullptr;
     c.meta = (int4*)arena_.alloc(size_class(sizeof(int4) * nSlices));
     c.sliceRow = (int*)arena_.alloc(size_class(sizeof(int) * nSlices));
     c.sliceRows = (int*)arena_.alloc(size_class(sizeof(int) * nSlices));
     c.rowSlice = (int*)arena_.alloc(size_class(sizeof(int) * nc));
-    const dev::LevelRows af{fine.n, fine.cols, fine.vals, fine.diag, fine.meta, fine.rowSlice, fine.ellWidth};
-    dev::galerkin_fill(af, nc, fine.ci, fine.c2fRow, fine.c2fCol, sliceOff, c.cols, c.vals, c.valsF, c.diag, c.diagF,
+    dev::galerkin_fill(af, nc, ci, fine.c2fRow, fine.c2fCol, sliceOff, c.cols, c.vals, c.valsF, c.diag, c.diagF,
                        st);
     dev::slice_meta_fill(nc, sliceOff, c.meta, c.sliceRow, c.sliceRows, c.rowSlice, flags + 1, st);
     CUDA_OK(cudaMemcpyAsync(hflags, flags + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
-    allocVectors(c, mixed);
     CUDA_OK(cudaStreamSynchronize(st));
     c.maxWidth = hflags[0];
+    return E;
+  };
+  // one matching: coarse size of `a`'s pairs (ci written)
+  auto match = [&](const dev::LevelRows& a, const int* order, int* ci) {
+    dev::aggregate_pairs(a, opt.matchBeta, opt.matchRounds, order, w, ci, st);
+    CUDA_OK(cudaMemcpyAsync(hflags, w.pos + a.n, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CUDA_OK(cudaStreamSynchronize(st));
+    return hflags[0];
+  };
+  for (int l = 0;; l++) {
+    if (l >= opt.maxCoarseLevels || lv_.size() + 1 > maxL) break;
+    {
+      const DevLevel& f = lv_[l];
+      if (opt.coarsestSize > 0 ? f.n <= opt.coarsestSize : f.n <= 3) break;
+    }
+    DevLevel& f = lv_[l];
+    const dev::LevelRows a{f.n, f.cols, f.vals, f.diag, f.meta, f.rowSlice, f.ellWidth};
+    int* ci = (int*)arena_.alloc(size_class(sizeof(int) * f.n));
+    int nc = match(a, l == 0 ? fp.iperm : nullptr, ci);
+    // a level that no longer shrinks is the coarsest
+    if (nc <= 0 || nc >= f.n || (double)nc > 0.9 * f.n) break;
+    if (opt.matchPasses == 2 && (opt.coarsestSize <= 0 || nc > opt.coarsestSize)) {
+      // pairs of pairs: the pairs' Galerkin matrix (not kept) is matched
+      // again and the two aggregations composed
+      DevLevel t;
+      galerkin(f, ci, nc, t, false);
+      const dev::LevelRows at{t.n, t.cols, t.vals, t.diag, t.meta, t.rowSlice, t.ellWidth};
+      int* ci2 = (int*)arena_.alloc(size_class(sizeof(int) * t.n));
+      const int nc2 = match(at, nullptr, ci2);
+      if (nc2 > 0 && nc2 < nc) {
+        dev::compose_index(f.n, ci, ci2, st);
+        nc = nc2;
+      }
+    }
+    lv_.emplace_back();
+    const long long E = galerkin(lv_[l], ci, nc, lv_.back(), mixed);
+    allocVectors(lv_.back(), mixed);
     if (trace) {
       char msg[96];
       snprintf(msg, sizeof msg, "level %d: %d rows, %lld entries", l + 1, nc, E);

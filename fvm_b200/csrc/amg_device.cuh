@@ -62,8 +62,9 @@ void coarse_to_fine(int n, int nc, const int* ci, int* cnt, int* c2fRow, int* c2
 // its fine rows ascending, entries in stored order) and sums into the
 // coarse SELL-32 level (natural row order, 32-row slices described by
 // sliceOff), padding (own row, 0); diagonal = sum of the fine diagonals and
-// of the entries inside the aggregate. FP64 and FP32 values. *overflow is
-// set when an aggregate's entries exceed the per-warp capacity.
+// of the entries inside the aggregate. FP64 values, and FP32 copies where
+// valsF / diagF are not null. *overflow is set when an aggregate's entries
+// exceed the per-warp capacity.
 constexpr int kGalerkinCap = 512;
 void galerkin_count(const LevelRows& a, int nc, const int* ci, const int* c2fRow, const int* c2fCol, int* count,
                     int* overflow, cudaStream_t st);
@@ -77,6 +78,9 @@ void galerkin_fill(const LevelRows& a, int nc, const int* ci, const int* c2fRow,
 void slice_widths(int n, const int* count, int* width32, cudaStream_t st);
 void slice_meta_fill(int n, const int* sliceOff, int4* meta, int* sliceRow, int* sliceRows, int* rowSlice,
                      int* maxWidth, cudaStream_t st);
+
+// ci[i] = ci2[ci[i]]: two aggregations composed
+void compose_index(int n, int* ci, const int* ci2, cudaStream_t st);
 
 // *flag = 1 unless every row is diagonally dominant (|a_ii| >= sum |a_ij|
 // up to a relative slack of 1e-8); *flag must be 0 on entry

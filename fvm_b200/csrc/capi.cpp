@@ -106,6 +106,11 @@ SolverOptions to_solver(const fvm_linear_options& o) {
   s.setupOnDevice = o.setupOnDevice != 0;
   s.matchRounds = o.matchRounds;
   s.matchBeta = o.matchBeta;
+  FVM_REQUIRE(o.matchPasses == 1 || o.matchPasses == 2, kBadArgument, "matchPasses must be 1 or 2");
+  FVM_REQUIRE(o.coarsePostSweeps >= -1 && o.coarsePostSweeps <= 16, kBadArgument,
+              "coarsePostSweeps must be in [-1, 16]");
+  s.matchPasses = o.matchPasses;
+  s.coarsePostSweeps = o.coarsePostSweeps;
   return s;
 }
 
@@ -137,6 +142,8 @@ void from_solver(const SolverOptions& s, fvm_linear_options& o) {
   o.setupOnDevice = s.setupOnDevice ? 1 : 0;
   o.matchRounds = s.matchRounds;
   o.matchBeta = s.matchBeta;
+  o.matchPasses = s.matchPasses;
+  o.coarsePostSweeps = s.coarsePostSweeps;
 }
 
 RefLevel level_from_csr(int n, const int* row, const int* col, const double* diag, const double* off) {
@@ -874,6 +881,35 @@ int fvm_learned_set_tensor_cores(fvm_learned* l, int on) {
   return guarded([&] {
     FVM_REQUIRE(l, kBadArgument, "null argument");
     l->lc->setTensorCores(on != 0);
+  });
+}
+
+int fvm_learned_set_useful_factor(fvm_learned* l, double f) {
+  return guarded([&] {
+    FVM_REQUIRE(l, kBadArgument, "null argument");
+    l->lc->setUsefulFactor(f);
+  });
+}
+
+int fvm_learned_residual_factor(const fvm_learned* l, double* factor) {
+  return guarded([&] {
+    FVM_REQUIRE(l && factor, kBadArgument, "null argument");
+    *factor = l->lc->residualFactor();
+  });
+}
+
+int fvm_learned_set_objective(fvm_learned* l, int objective) {
+  return guarded([&] {
+    FVM_REQUIRE(l, kBadArgument, "null argument");
+    l->lc->setObjective(objective);
+  });
+}
+
+int fvm_learned_wait_probe(unsigned limit, int* status) {
+  return guarded([&] {
+    FVM_REQUIRE(status, kBadArgument, "null argument");
+    FVM_REQUIRE(limit >= 1 && limit <= (1u << 22), kBadArgument, "limit must be in [1, 2^22]");
+    *status = nn::tc_wait_probe(limit);
   });
 }
 

@@ -314,6 +314,128 @@ __global__ void __launch_bounds__(kBlock, 8) k_spmv_ell(SellView<double> a, cons
   y[i] = ell_row<double, W>(a, i, x, a.diag[i] * x[i]);
 }
 
+// ---- fused Krylov vector steps ---------------------------------------------
+
+// Block-wide sums of two doubles per thread; results valid in thread 0.
+__device__ __forceinline__ void block_sum2(double& a, double& b) {
+  __shared__ double sh[2][32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  a = warp_sum(a);
+  b = warp_sum(b);
+  if (lane == 0) {
+    sh[0][wid] = a;
+    sh[1][wid] = b;
+  }
+  __syncthreads();
+  const int nw = (blockDim.x + 31) >> 5;
+  a = (threadIdx.x < nw) ? sh[0][threadIdx.x] : 0.0;
+  b = (threadIdx.x < nw) ? sh[1][threadIdx.x] : 0.0;
+  if (wid == 0) {
+    a = warp_sum(a);
+    b = warp_sum(b);
+  }
+}
+
+// y = A x over an ELL-32 level, with one partial of x.y per block
+template <int W>
+__global__ void __launch_bounds__(kBlock, 8) k_spmv_dot_ell(SellView<double> a, const double* __restrict__ x, double* y,
+                                                            double* partials) {
+  FVM_PDL();
+  const int i = blockIdx.x * kBlock + threadIdx.x;
+  double d = 0.0;
+  if (i < a.n) {
+    const double xi = x[i];
+    const double yi = ell_row<double, W>(a, i, x, a.diag[i] * xi);
+    y[i] = yi;
+    d = xi * yi;
+  }
+  d = block_sum(d);
+  if (threadIdx.x == 0) partials[blockIdx.x] = d;
+}
+
+// the same over a SELL-32 level (grid-stride over slices)
+__global__ void __launch_bounds__(kBlock, 8) k_spmv_dot(SellView<double> a, int nSlices, const double* __restrict__ x,
+                                                        double* y, double* partials) {
+  FVM_PDL();
+  const int lane = threadIdx.x & 31;
+  double d = 0.0;
+  for (int s = blockIdx.x * kSlicesPerBlock + (threadIdx.x >> 5); s < nSlices; s += gridDim.x * kSlicesPerBlock) {
+    const int4 m = slice_meta(a, s);
+    if (lane >= m.y) continue;
+    const int i = m.x + lane;
+    const double xi = x[i];
+    const double yi = row_sum(a, m, lane, x, a.diag[i] * xi);
+    y[i] = yi;
+    d += xi * yi;
+  }
+  d = block_sum(d);
+  if (threadIdx.x == 0) partials[blockIdx.x] = d;
+}
+
+// z <- src (as FP64), with block partials of r.z_old and r.z_new
+template <class S>
+__global__ void k_cg_take_z(int n, const S* __restrict__ src, const double* __restrict__ r, double* z,
+                            double* partials) {
+  FVM_PDL();
+  double a = 0.0, b = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double ri = r[i];
+    const double zo = z[i];
+    const double zn = (double)src[i];
+    z[i] = zn;
+    a += ri * zo;
+    b += ri * zn;
+  }
+  block_sum2(a, b);
+  if (threadIdx.x == 0) {
+    partials[2 * blockIdx.x] = a;
+    partials[2 * blockIdx.x + 1] = b;
+  }
+}
+
+// rho_prev <- rho, rho <- (r, z_new), beta (flexible: (rho - (r, z_old)) / rho_prev)
+__global__ void k_cg_beta(int np, const double* __restrict__ p, double* rho, double* rhoPrev, double* beta,
+                          int flexible) {
+  FVM_PDL();
+  double a = 0.0, b = 0.0;
+  for (int i = threadIdx.x; i < np; i += blockDim.x) {
+    a += p[2 * i];
+    b += p[2 * i + 1];
+  }
+  block_sum2(a, b);
+  if (threadIdx.x == 0) {
+    const double prev = rho[0];
+    rhoPrev[0] = prev;
+    rho[0] = b;
+    beta[0] = flexible ? (b - a) / prev : b / prev;
+  }
+}
+
+// alpha = rho / sum of the partials (p.Ap)
+__global__ void k_cg_alpha(int np, const double* __restrict__ p, const double* rho, double* alpha) {
+  FVM_PDL();
+  double s = 0.0;
+  for (int i = threadIdx.x; i < np; i += blockDim.x) s += p[i];
+  s = block_sum(s);
+  if (threadIdx.x == 0) alpha[0] = rho[0] / s;
+}
+
+// x += -alpha p; r += -alpha q; block partials of |r|
+__global__ void k_cg_update(int n, const double* alpha, const double* __restrict__ p, const double* __restrict__ q,
+                            double* x, double* r, double* partials) {
+  FVM_PDL();
+  const double am = -1.0 * alpha[0];
+  double l1 = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    x[i] = x[i] + am * p[i];
+    const double ri = r[i] + am * q[i];
+    r[i] = ri;
+    l1 += fabs(ri);
+  }
+  l1 = block_sum(l1);
+  if (threadIdx.x == 0) partials[blockIdx.x] = l1;
+}
+
 // ---- SELL-32 smoothers with several threads per row (autotuned plans) ---------
 // A warp covers 32 / TPR rows of one slice; thread `sub` of a row's group
 // takes the entries k = sub, sub + TPR, ... Four entries per thread are in
@@ -453,12 +575,15 @@ __global__ void __launch_bounds__(kBlock, 4) k_residual_restrict(SellView<T> a, 
 }
 
 template <class T>
-__global__ void k_prolong(int n, const int* __restrict__ ci, const T* __restrict__ xc, T* x) {
+__global__ void k_prolong(int n, const int* __restrict__ ci, const T* __restrict__ xc, T* x, int assign) {
   FVM_PDL();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const int c = ci[i];
-  if (c >= 0) x[i] = x[i] + xc[c];
+  if (assign)
+    x[i] = c >= 0 ? xc[c] : T(0);
+  else if (c >= 0)
+    x[i] = x[i] + xc[c];
 }
 
 template <class T>
@@ -1048,6 +1173,32 @@ void spmv(const SellView<double>& a, int nSlices, const double* x, double* y, cu
 #undef FVM_L
   pdl_launch(k_spmv, reduce_blocks(nSlices), kBlock, st, a, nSlices, x, y);
 }
+int spmv_dot_blocks(const SellView<double>& a, int nSlices) {
+  return (a.ellWidth >= 1 && a.ellWidth <= 8) ? ceil_div(a.n, kBlock) : reduce_blocks(nSlices);
+}
+void spmv_dot(const SellView<double>& a, int nSlices, const double* x, double* y, double* partials, cudaStream_t st) {
+#define FVM_L(W) pdl_launch(k_spmv_dot_ell<W>, ceil_div(a.n, kBlock), kBlock, st, a, x, y, partials)
+  if (a.ellWidth && FVM_ELL_SWITCH(a.ellWidth, FVM_L)) return;
+#undef FVM_L
+  pdl_launch(k_spmv_dot, reduce_blocks(nSlices), kBlock, st, a, nSlices, x, y, partials);
+}
+template <class S>
+void cg_take_z(int n, const S* src, const double* r, double* z, double* partials, cudaStream_t st) {
+  pdl_launch(k_cg_take_z<S>, vec_blocks(n), kBlock, st, n, src, r, z, partials);
+}
+template void cg_take_z<float>(int, const float*, const double*, double*, double*, cudaStream_t);
+template void cg_take_z<double>(int, const double*, const double*, double*, double*, cudaStream_t);
+void cg_beta(int np, const double* partials, double* rho, double* rhoPrev, double* beta, bool flexible,
+             cudaStream_t st) {
+  pdl_launch(k_cg_beta, 1, 1024, st, np, partials, rho, rhoPrev, beta, flexible ? 1 : 0);
+}
+void cg_alpha(int np, const double* partials, const double* rho, double* alpha, cudaStream_t st) {
+  pdl_launch(k_cg_alpha, 1, 1024, st, np, partials, rho, alpha);
+}
+void cg_update(int n, const double* alpha, const double* p, const double* q, double* x, double* r, double* partials,
+               cudaStream_t st) {
+  pdl_launch(k_cg_update, vec_blocks(n), kBlock, st, n, alpha, p, q, x, r, partials);
+}
 template <class T>
 void restrict_sum(int nc, const int* c2fRow, const int* c2fCol, const T* r, T* bc, cudaStream_t st) {
   pdl_launch(k_restrict<T>, ceil_div(nc, kBlock), kBlock, st, nc, c2fRow, c2fCol, r, bc, (T*)nullptr);
@@ -1071,8 +1222,8 @@ void zero(int n, T* x, cudaStream_t st) {
   pdl_launch(k_zero<T>, ceil_div(n, kBlock), kBlock, st, n, x);
 }
 template <class T>
-void prolong(int n, const int* ci, const T* xc, T* x, cudaStream_t st) {
-  pdl_launch(k_prolong<T>, ceil_div(n, kBlock), kBlock, st, n, ci, xc, x);
+void prolong(int n, const int* ci, const T* xc, T* x, cudaStream_t st, bool assign) {
+  pdl_launch(k_prolong<T>, ceil_div(n, kBlock), kBlock, st, n, ci, xc, x, assign ? 1 : 0);
 }
 template <class T>
 void dense_solve(int n, const double* ainv, const T* b, T* x, cudaStream_t st) {
@@ -1094,155 +1245,178 @@ size_t gj_align(size_t b) { return (b + 255) & ~size_t(255); }
 //   A[K][K] <- D^-1          A[K][j] <- D^-1 A[K][j]                 (j not in K)
 //   A[i][K] <- -A[i][K] D^-1 A[i][j] <- A[i][j] - A[i][K] D^-1 A[K][j] (i, j not in K)
 // After all panels A holds its inverse. Without pivot searches each panel
-// is ONE kernel over the whole matrix, each CTA a 64 x 128 tile. The
-// panel's old rows A[K][:] and columns A[:][K] are read from side buffers
-// (R, C) that the previous panel's kernel filled while writing them, so no
-// CTA reads a value another CTA of the same launch writes; D^-1 comes
-// ready-made: the last CTA of the previous launch to finish (a fence and
-// a ticket counter, no waiting) inverts the next panel's block. Diagonal
-// dominance keeps every pivot away from zero and the growth bounded, which
-// is why the caller takes this path only for diagonally dominant levels.
-// This is not a reference computation, so the products use fused
-// multiply-adds (__fma_rn) although the file is built without contraction.
-constexpr int kNpB = 16;    // panel width
-constexpr int kNpTJ = 128;  // columns per CTA, one per thread in x
-constexpr int kNpTI = 64;   // rows per CTA, 32 per thread
-constexpr int kNpGroup = 4; // rows whose loads are issued together
+// is two kernels over the matrix: k_gjd_rows forms the panel's new pivot
+// rows Rp = D^-1 A[K][:] once, then k_gjd_update sweeps 64 x 64 tiles,
+// each thread 4 x 4 entries, with the tile's 64 x 32 panel columns and
+// 32 x 64 pivot rows staged in shared memory (16 fused multiply-adds per 8
+// shared loads). The panel's old rows and columns are read from side
+// buffers (R, C) that the previous panel's update filled while writing
+// them, so no CTA reads a value another CTA of the same launch writes;
+// D^-1 comes ready-made: the last CTA of the previous launch to finish (a
+// fence and a ticket counter, no waiting) inverts the next panel's block.
+// Diagonal dominance keeps every pivot away from zero and the growth
+// bounded, which is why the caller takes this path only for diagonally
+// dominant levels. This is not a reference computation, so the products use
+// fused multiply-adds (__fma_rn) although the file is built without
+// contraction.
+constexpr int kGdB = 32;   // panel width
+constexpr int kGdT = 64;   // tile rows / columns
 
-// C[i * kNpB + t] = A[i][k0 + t], R[t * n + j] = A[k0 + t][j] (t < nb; 0 beyond)
-__global__ void k_gjnp_extract(int n, int k0, int nb, const double* __restrict__ A, double* __restrict__ C,
-                               double* __restrict__ R) {
-  const int j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= n) return;
-  for (int t = 0; t < kNpB; t++) {
-    R[(size_t)t * n + j] = t < nb ? A[(size_t)(k0 + t) * n + j] : 0.0;
-    C[(size_t)j * kNpB + t] = t < nb ? A[(size_t)j * n + k0 + t] : 0.0;
+// D: shared memory of 2 x kGdB x (kGdB + 1) doubles (double-buffered block)
+__device__ void gjd_invert_block(int n, int k0, int nb, const double* R, double* Dout, int* status,
+                                 double (*D)[kGdB][kGdB + 1]) {
+  const int tid = threadIdx.x, nt = blockDim.x;
+  for (int e = tid; e < kGdB * kGdB; e += nt) {
+    const int r = e / kGdB, c = e % kGdB;
+    D[0][r][c] = (r < nb && c < nb) ? __ldcg(R + (size_t)r * n + k0 + c) : (r == c ? 1.0 : 0.0);
   }
-}
-
-// Dout = inverse of the panel's pivot block R[t][k0 + c] (t, c < nb; the
-// identity beyond), by the scalar sweep over its pivots; 256 threads, one
-// entry each. *status = 1 on a zero pivot.
-__device__ void gjnp_invert_block(int n, int k0, int nb, const double* R, double* Dout, int* status) {
-  __shared__ double D[2][kNpB][kNpB + 1];
-  const int tid = threadIdx.x, r = tid / kNpB, c = tid % kNpB;
-  D[0][r][c] = (r < nb && c < nb) ? __ldcg(R + (size_t)r * n + k0 + c) : (r == c ? 1.0 : 0.0);
   __syncthreads();
   int cur = 0;
-  for (int t = 0; t < kNpB; t++) {
-    const double p = D[cur][t][t];
-    const double ip = 1.0 / p;
-    const double drt = D[cur][r][t], dtc = D[cur][t][c], drc = D[cur][r][c];
-    double v;
-    if (r == t && c == t)
-      v = ip;
-    else if (r == t)
-      v = dtc * ip;
-    else if (c == t)
-      v = -drt * ip;
-    else
-      v = __fma_rn(-drt, dtc * ip, drc);
-    D[cur ^ 1][r][c] = v;
-    if (p == 0.0 && tid == 0) atomicExch(status, 1);
+  for (int t = 0; t < kGdB; t++) {
+    const double pv = D[cur][t][t];
+    const double ip = 1.0 / pv;
+    for (int e = tid; e < kGdB * kGdB; e += nt) {
+      const int r = e / kGdB, c = e % kGdB;
+      const double drt = D[cur][r][t], dtc = D[cur][t][c], drc = D[cur][r][c];
+      double v;
+      if (r == t && c == t)
+        v = ip;
+      else if (r == t)
+        v = dtc * ip;
+      else if (c == t)
+        v = -drt * ip;
+      else
+        v = __fma_rn(-drt, dtc * ip, drc);
+      D[cur ^ 1][r][c] = v;
+    }
+    if (pv == 0.0 && tid == 0) atomicExch(status, 1);
     cur ^= 1;
     __syncthreads();
   }
-  Dout[r * kNpB + c] = D[cur][r][c];
+  for (int e = tid; e < kGdB * kGdB; e += nt) Dout[e] = D[cur][e / kGdB][e % kGdB];
 }
 
-__global__ void __launch_bounds__(256) k_gjnp_first(int n, int nb, const double* __restrict__ R, double* Dout,
-                                                    int* status) {
-  gjnp_invert_block(n, 0, nb, R, Dout, status);
+// C[i * kGdB + t] = A[i][k0 + t], R[t * n + j] = A[k0 + t][j] (t < nb; 0 beyond)
+__global__ void k_gjd_extract(int n, int k0, int nb, const double* __restrict__ A, double* __restrict__ C,
+                              double* __restrict__ R) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  for (int t = 0; t < kGdB; t++) {
+    R[(size_t)t * n + j] = t < nb ? A[(size_t)(k0 + t) * n + j] : 0.0;
+    C[(size_t)j * kGdB + t] = t < nb ? A[(size_t)j * n + k0 + t] : 0.0;
+  }
 }
 
-// One panel [k0, k0 + nb) over the whole matrix (Dinv = its pivot block's
-// inverse); also fills Cn / Rn with the next panel's [k1, k1 + nb1) new
-// columns / rows and, in the launch's last CTA, Dnext. Launch: grid
-// (ceil(n / kNpTJ), ceil(n / kNpTI)), 256 threads; *ticket is 0 on entry
-// and left 0.
-__global__ void __launch_bounds__(256, 3) k_gjnp_update(int n, int k0, int nb, double* __restrict__ A,
-                                                     const double* __restrict__ C, const double* __restrict__ R,
-                                                     const double* __restrict__ Dinv, double* __restrict__ Cn,
-                                                     double* __restrict__ Rn, double* __restrict__ Dnext, int k1,
-                                                     int nb1, unsigned* ticket, int* status) {
-  __shared__ double D[kNpB][kNpB + 1];
-  __shared__ double Ct[kNpTI][kNpB];
+__global__ void __launch_bounds__(256) k_gjd_first(int n, int nb, const double* __restrict__ R, double* Dout,
+                                                   int* status) {
+  __shared__ double D[2][kGdB][kGdB + 1];
+  gjd_invert_block(n, 0, nb, R, Dout, status, D);
+}
+
+// Rp[t][j] = sum_u D[t][u] R[u][j]: the panel's new pivot rows
+__global__ void __launch_bounds__(256) k_gjd_rows(int n, int nb, const double* __restrict__ R,
+                                                  const double* __restrict__ Dinv, double* __restrict__ Rp) {
+  __shared__ double D[kGdB][kGdB + 1];
+  for (int e = threadIdx.x; e < kGdB * kGdB; e += blockDim.x) D[e / kGdB][e % kGdB] = Dinv[e];
+  __syncthreads();
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  double r[kGdB];
+#pragma unroll
+  for (int u = 0; u < kGdB; u++) r[u] = u < nb ? R[(size_t)u * n + j] : 0.0;
+#pragma unroll 4
+  for (int t = 0; t < kGdB; t++) {
+    double acc = 0.0;
+#pragma unroll
+    for (int u = 0; u < kGdB; u++) acc = __fma_rn(D[t][u], r[u], acc);
+    Rp[(size_t)t * n + j] = t < nb ? acc : 0.0;
+  }
+}
+
+// One panel [k0, k0 + nb) over the whole matrix in 64 x 64 tiles; grid
+// (ceil(n / 64), ceil(n / 64)), 256 threads. Also fills Cn / Rn with the
+// next panel's [k1, k1 + nb1) columns / rows and, in the launch's last CTA,
+// Dnext. *ticket is 0 on entry and left 0.
+__global__ void __launch_bounds__(256, 2) k_gjd_update(int n, int k0, int nb, double* __restrict__ A,
+                                                    const double* __restrict__ C, const double* __restrict__ Rp,
+                                                    const double* __restrict__ Dinv, double* __restrict__ Cn,
+                                                    double* __restrict__ Rn, double* __restrict__ Dnext, int k1,
+                                                    int nb1, unsigned* ticket, int* status) {
+  // Cs doubles as the last CTA's pivot-block workspace (2 x 32 x 33 doubles)
+  static_assert(kGdT * (kGdB + 1) >= 2 * kGdB * (kGdB + 1), "block inverse workspace");
+  __shared__ double Cs[kGdT][kGdB + 1];
+  __shared__ double Rs[kGdB][kGdT + 2];
+  __shared__ double Ds[kGdB][kGdB + 1];
   __shared__ bool last;
   const int tid = threadIdx.x;
-  const int i0 = blockIdx.y * kNpTI;
-  D[tid / kNpB][tid % kNpB] = Dinv[tid];
-  for (int e = tid; e < kNpTI * kNpB; e += blockDim.x) {
-    const int r = e / kNpB, t = e % kNpB;
-    Ct[r][t] = (i0 + r < n && t < nb) ? C[(size_t)(i0 + r) * kNpB + t] : 0.0;
+  const int i0 = blockIdx.y * kGdT, j0 = blockIdx.x * kGdT;
+  const int ty = tid >> 4, tx = tid & 15;
+  // does the tile meet the panel's rows / columns?
+  const bool rowsK = i0 < k0 + nb && i0 + kGdT > k0;
+  const bool colsK = j0 < k0 + nb && j0 + kGdT > k0;
+  for (int e = tid; e < kGdT * kGdB; e += 256) {
+    const int r = e / kGdB, t = e % kGdB;
+    Cs[r][t] = i0 + r < n ? C[(size_t)(i0 + r) * kGdB + t] : 0.0;
   }
+  for (int e = tid; e < kGdB * kGdT; e += 256) {
+    const int t = e / kGdT, c = e % kGdT;
+    Rs[t][c] = j0 + c < n ? Rp[(size_t)t * n + j0 + c] : 0.0;
+  }
+  if (colsK || rowsK)
+    for (int e = tid; e < kGdB * kGdB; e += 256) Ds[e / kGdB][e % kGdB] = Dinv[e];
   __syncthreads();
-  const int tx = tid & (kNpTJ - 1), ty = tid / kNpTJ;
-  const int j = blockIdx.x * kNpTJ + tx;
-  if (j < n) {
-    const bool jK = j >= k0 && j < k0 + nb;
-    // this column's new pivot-row values rj[t] = (D^-1 A[K][j])[t]
-    double rj[kNpB];
-    {
-      double rs[kNpB];
+  double acc[4][4];
 #pragma unroll
-      for (int t = 0; t < kNpB; t++) rs[t] = t < nb ? R[(size_t)t * n + j] : 0.0;
+  for (int a = 0; a < 4; a++) {
+    const int i = i0 + ty + 16 * a;
 #pragma unroll
-      for (int t = 0; t < kNpB; t++) {
-        double acc = 0.0;
-#pragma unroll
-        for (int u = 0; u < kNpB; u++) acc = __fma_rn(D[t][u], rs[u], acc);
-        rj[t] = acc;
-      }
+    for (int b = 0; b < 4; b++) {
+      const int j = j0 + tx + 16 * b;
+      acc[a][b] = (i < n && j < n) ? A[(size_t)i * n + j] : 0.0;
     }
-    const bool jNext = j >= k1 && j < k1 + nb1;
-    const bool full = i0 + kNpTI <= n;
-    // rows in groups of kNpGroup: a group's loads are all issued before its
-    // updates (a bound check per row would keep each load behind the
-    // previous row's 16-deep FMA chain)
-    for (int q0 = 0; q0 < kNpTI / 2; q0 += kNpGroup) {
-      double a[kNpGroup];
+  }
+#pragma unroll 4
+  for (int t = 0; t < kGdB; t++) {
+    double c[4], r[4];
 #pragma unroll
-      for (int u = 0; u < kNpGroup; u++) {
-        const int i = i0 + ty + 2 * (q0 + u);
-        a[u] = (full || i < n) ? A[(size_t)i * n + j] : 0.0;
+    for (int a = 0; a < 4; a++) c[a] = Cs[ty + 16 * a][t];
+#pragma unroll
+    for (int b = 0; b < 4; b++) r[b] = Rs[t][tx + 16 * b];
+#pragma unroll
+    for (int a = 0; a < 4; a++)
+#pragma unroll
+      for (int b = 0; b < 4; b++) acc[a][b] = __fma_rn(-c[a], r[b], acc[a][b]);
+  }
+#pragma unroll
+  for (int a = 0; a < 4; a++) {
+    const int r = ty + 16 * a;
+    const int i = i0 + r;
+    if (i >= n) continue;
+    const bool iK = i >= k0 && i < k0 + nb;
+#pragma unroll
+    for (int b = 0; b < 4; b++) {
+      const int cix = tx + 16 * b;
+      const int j = j0 + cix;
+      if (j >= n) continue;
+      const bool jK = j >= k0 && j < k0 + nb;
+      double v = acc[a][b];
+      if (iK && jK) {
+        v = Ds[i - k0][j - k0];
+      } else if (iK) {
+        v = Rs[i - k0][cix];
+      } else if (jK) {
+        double s = 0.0;
+        for (int t = 0; t < kGdB; t++) s = __fma_rn(Cs[r][t], Ds[t][j - k0], s);
+        v = -s;
       }
-#pragma unroll
-      for (int u = 0; u < kNpGroup; u++) {
-        const int r = ty + 2 * (q0 + u);
-        const int i = i0 + r;
-        if (!full && i >= n) break;
-        const size_t e = (size_t)i * n + j;
-        double v;
-        if (i >= k0 && i < k0 + nb) {
-          const int t = i - k0;
-          if (jK) {
-            v = D[t][j - k0];
-          } else {
-            v = 0.0;
-#pragma unroll
-            for (int s = 0; s < kNpB; s++) v = s == t ? rj[s] : v;  // registers, no local-memory index
-          }
-        } else if (jK) {
-          double acc = 0.0;
-#pragma unroll
-          for (int s = 0; s < kNpB; s++) acc = __fma_rn(Ct[r][s], D[s][j - k0], acc);
-          v = -acc;
-        } else {
-          double acc = a[u];
-#pragma unroll
-          for (int t = 0; t < kNpB; t++) acc = __fma_rn(-Ct[r][t], rj[t], acc);
-          v = acc;
-        }
-        A[e] = v;
-        if (jNext) Cn[(size_t)i * kNpB + (j - k1)] = v;
-        if (i >= k1 && i < k1 + nb1) Rn[(size_t)(i - k1) * n + j] = v;
-      }
+      A[(size_t)i * n + j] = v;
+      if (j >= k1 && j < k1 + nb1) Cn[(size_t)i * kGdB + (j - k1)] = v;
+      if (i >= k1 && i < k1 + nb1) Rn[(size_t)(i - k1) * n + j] = v;
     }
   }
   if (nb1 <= 0) return;  // the last panel: no next block to invert
-  // the last CTA to finish inverts the next panel's pivot block: every
-  // thread that wrote Rn / Cn / A fences its own writes before the barrier,
-  // so they are visible device-wide before the ticket is taken
+  // the last CTA to finish inverts the next panel's pivot block (every
+  // thread fences its own writes before the barrier)
   __threadfence();
   __syncthreads();
   if (tid == 0) {
@@ -1252,9 +1426,10 @@ __global__ void __launch_bounds__(256, 3) k_gjnp_update(int n, int k0, int nb, d
   __syncthreads();
   if (!last) return;
   __threadfence();
-  gjnp_invert_block(n, k1, nb1, Rn, Dnext, status);
+  gjd_invert_block(n, k1, nb1, Rn, Dnext, status, reinterpret_cast<double(*)[kGdB][kGdB + 1]>(&Cs[0][0]));
   if (tid == 0) *ticket = 0u;
 }
+
 // Look-ahead: after panel p's row swaps, the next panel's columns are
 // updated first and factored on stream st while the rest of the matrix
 // takes panel p's update on a second stream (disjoint columns); panel p+1's
@@ -1303,12 +1478,13 @@ void gj_run(int n, double* a, double* inv, double* Bt, int* piv, int* idx, int* 
 
 // scratch: [panel doubles][piv: n ints][idx: n ints][status]; the panel
 // doubles hold the pivoted path's Bt (kGjMaxPanel x n) or the unpivoted
-// path's two pairs of side buffers (4 x kNpB x n)
-constexpr int kGjScratchPanels = 4 * kNpB > kGjMaxPanel ? 4 * kNpB : kGjMaxPanel;
+// path's side buffers
+// (the unpivoted path: C, R of two panels and Rp, 5 x kGdB x n)
+constexpr int kGjScratchPanels = 5 * kGdB > kGjMaxPanel ? 5 * kGdB : kGjMaxPanel;
 // the panel doubles, plus the unpivoted path's two inverted pivot blocks
 // and its ticket counter
 size_t gj_panel_bytes(int n) {
-  return gj_align(sizeof(double) * ((size_t)kGjScratchPanels * n + 2 * kNpB * kNpB + 1));
+  return gj_align(sizeof(double) * ((size_t)kGjScratchPanels * n + 2 * kGdB * kGdB + 1));
 }
 size_t gauss_jordan_scratch_bytes(int n) {
   return gj_panel_bytes(n) + 2 * gj_align(sizeof(int) * (size_t)n) + gj_align(sizeof(int));
@@ -1319,26 +1495,28 @@ const int* gauss_jordan_status(int n, const void* scratch) {
 }
 void gauss_jordan_inverse_dominant(int n, double* a, void* scratch, cudaStream_t st) {
   double* sb = (double*)scratch;
-  const size_t pn = (size_t)kNpB * n;
+  const size_t pn = (size_t)kGdB * n;
   double* C[2] = {sb, sb + pn};
   double* R[2] = {sb + 2 * pn, sb + 3 * pn};
-  double* Dv[2] = {sb + 4 * pn, sb + 4 * pn + kNpB * kNpB};
-  unsigned* ticket = (unsigned*)(sb + 4 * pn + 2 * kNpB * kNpB);
+  double* Rp = sb + 4 * pn;
+  double* Dv[2] = {sb + 5 * pn, sb + 5 * pn + kGdB * kGdB};
+  unsigned* ticket = (unsigned*)(sb + 5 * pn + 2 * kGdB * kGdB);
   int* status = (int*)gauss_jordan_status(n, scratch);
   cudaMemsetAsync(status, 0, sizeof(int), st);
   cudaMemsetAsync(ticket, 0, sizeof(unsigned), st);
   if (n <= 0) return;
-  const int nb0 = n < kNpB ? n : kNpB;
-  k_gjnp_extract<<<ceil_div(n, kBlock), kBlock, 0, st>>>(n, 0, nb0, a, C[0], R[0]);
-  k_gjnp_first<<<1, 256, 0, st>>>(n, nb0, R[0], Dv[0], status);
-  const dim3 grid(ceil_div(n, kNpTJ), ceil_div(n, kNpTI));
+  const int nb0 = n < kGdB ? n : kGdB;
+  k_gjd_extract<<<ceil_div(n, kBlock), kBlock, 0, st>>>(n, 0, nb0, a, C[0], R[0]);
+  k_gjd_first<<<1, 256, 0, st>>>(n, nb0, R[0], Dv[0], status);
+  const dim3 grid(ceil_div(n, kGdT), ceil_div(n, kGdT));
   int cur = 0;
-  for (int k0 = 0; k0 < n; k0 += kNpB) {
-    const int nb = n - k0 < kNpB ? n - k0 : kNpB;
+  for (int k0 = 0; k0 < n; k0 += kGdB) {
+    const int nb = n - k0 < kGdB ? n - k0 : kGdB;
     const int k1 = k0 + nb;
-    const int nb1 = n - k1 < kNpB ? n - k1 : kNpB;
-    k_gjnp_update<<<grid, 256, 0, st>>>(n, k0, nb, a, C[cur], R[cur], Dv[cur], C[cur ^ 1], R[cur ^ 1], Dv[cur ^ 1],
-                                        k1, nb1 > 0 ? nb1 : 0, ticket, status);
+    const int nb1 = n - k1 < kGdB ? n - k1 : kGdB;
+    k_gjd_rows<<<ceil_div(n, kBlock), kBlock, 0, st>>>(n, nb, R[cur], Dv[cur], Rp);
+    k_gjd_update<<<grid, 256, 0, st>>>(n, k0, nb, a, C[cur], Rp, Dv[cur], C[cur ^ 1], R[cur ^ 1], Dv[cur ^ 1], k1,
+                                       nb1 > 0 ? nb1 : 0, ticket, status);
     cur ^= 1;
   }
 }
@@ -1492,7 +1670,7 @@ void update_solution(int nCells, const int* perm, const double* delta, const Bou
   template void residual_restrict<T>(const SellView<T>&, int, const int*, int, const int*,        \
                                      const int*, const T*, const T*, T*, T*, T*, cudaStream_t);   \
   template void zero<T>(int, T*, cudaStream_t);                                                  \
-  template void prolong<T>(int, const int*, const T*, T*, cudaStream_t);                         \
+  template void prolong<T>(int, const int*, const T*, T*, cudaStream_t, bool);                         \
   template void dense_solve<T>(int, const double*, const T*, T*, cudaStream_t);
 FVM_INST(double)
 FVM_INST(float)

@@ -65,6 +65,25 @@ void residual(const SellView<T>& a, int nSlices, const T* x, const T* b, T* r, d
 // y = D x + O x (FP64 only)
 void spmv(const SellView<double>& a, int nSlices, const double* x, double* y, cudaStream_t st);
 int reduce_blocks(int nSlices);  // grid of the SELL-32 whole-level row kernels
+
+// ---- fused Krylov vector steps (CG) -------------------------------------------
+// y = A x with one partial of x.y per block (spmv_dot_blocks of them)
+int spmv_dot_blocks(const SellView<double>& a, int nSlices);
+void spmv_dot(const SellView<double>& a, int nSlices, const double* x, double* y, double* partials, cudaStream_t st);
+// z <- src (converted to FP64) with per-block partials of r.z_old and
+// r.z_new (interleaved, vec_blocks(n) pairs)
+template <class S>
+void cg_take_z(int n, const S* src, const double* r, double* z, double* partials, cudaStream_t st);
+// from those pairs: *rhoPrev <- *rho, *rho <- (r, z_new), *beta <- *rho /
+// *rhoPrev, or with flexible (Polak-Ribiere) (*rho - (r, z_old)) / *rhoPrev
+void cg_beta(int np, const double* partials, double* rho, double* rhoPrev, double* beta, bool flexible,
+             cudaStream_t st);
+// *alpha = *rho / (sum of np partials)
+void cg_alpha(int np, const double* partials, const double* rho, double* alpha, cudaStream_t st);
+// x += -alpha p, r += -alpha q, and per-block L1 partials of the new r
+// (vec_blocks(n) of them)
+void cg_update(int n, const double* alpha, const double* p, const double* q, double* x, double* r, double* partials,
+               cudaStream_t st);
 // number of L1 partials residual() writes for a level (one per block)
 int residual_partials(int nSlices, int n, int ellWidth);
 
@@ -97,9 +116,9 @@ template <class T>
 void restrict_rhs(int nc, const int* c2fRow, const int* c2fCol, const T* b, T* bc, T* xc, cudaStream_t st);
 template <class T>
 void zero(int n, T* x, cudaStream_t st);
-// x[i] += xc[ci[i]]
+// x[i] += xc[ci[i]] (assign: x[i] = xc[ci[i]], for an x that is zero)
 template <class T>
-void prolong(int n, const int* ci, const T* xc, T* x, cudaStream_t st);
+void prolong(int n, const int* ci, const T* xc, T* x, cudaStream_t st, bool assign = false);
 
 // ---- coarsest level --------------------------------------------------------
 // x = -Ainv b with a dense FP64 inverse (n x n, row-major)

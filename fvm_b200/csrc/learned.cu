@@ -273,6 +273,25 @@ __global__ void __launch_bounds__(kTcThreads, 4) k_layer_tc(int n, GraphArgs g, 
   if (warp == 0) umma::tmem_free(tmem, 32);
 }
 
+// Failure path of the bounded completion wait of the tensor-core layers:
+// TMEM is allocated as the layers allocate it and an mbarrier is armed, but
+// no MMA commits to it, so the wait runs out after `limit` tries; the
+// kernel then sets *status, releases TMEM and returns, as the layers do.
+__global__ void k_tc_wait_probe(uint32_t limit, int* status) {
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ uint32_t sTmem;
+  const int warp = threadIdx.x >> 5;
+  if (warp == 0) umma::tmem_alloc(&sTmem, 32);
+  if (threadIdx.x == 32) umma::mbar_init(&bar, 1);
+  umma::fence_before_sync();
+  __syncthreads();
+  umma::fence_after_sync();
+  const bool done = __syncthreads_and(umma::mbar_wait(&bar, 0u, limit));
+  if (!done && threadIdx.x == 0) atomicOr(status, 1);
+  umma::fence_after_sync();
+  if (warp == 0) umma::tmem_free(sTmem, 32);
+}
+
 __device__ __forceinline__ float warp_sum(float v) {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(kFull, v, o);
   return __shfl_sync(kFull, v, 0);
@@ -330,6 +349,66 @@ __global__ void __launch_bounds__(kBlock) k_decode_bwd(int n, const float* __res
   block_grad_store(sv, 33, gp, kDecW);
   loss = block_sum(loss);
   if (threadIdx.x == 0) lossPartials[blockIdx.x] = loss;
+}
+
+// Decoder backward from a given gradient of the loss with respect to the
+// FP64 output d = s y: gd[i] * gdScale[0] (dL/dy = s dL/dd).
+__global__ void __launch_bounds__(kBlock) k_decode_bwd_grad(int n, const float* __restrict__ P,
+                                                            const float* __restrict__ H3,
+                                                            const double* __restrict__ scale,
+                                                            const double* __restrict__ gd,
+                                                            const double* __restrict__ gdScale,
+                                                            float* __restrict__ dH3, float* gp) {
+  __shared__ float sv[kWarps * 33];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  const float wd = P[kDecW + lane];
+  const double s = scale[0] * gdScale[0];
+  float gwd = 0.f, gbd = 0.f;
+  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += nw) {
+    const float h = H3[(size_t)i * 32 + lane];
+    const float gy = (float)(s * gd[i]);
+    dH3[(size_t)i * 32 + lane] = gy * wd;
+    gwd = __fmaf_rn(gy, h, gwd);
+    gbd += gy;
+  }
+  sv[w * 33 + lane] = gwd;
+  if (lane == 0) sv[w * 33 + 32] = gbd;
+  block_grad_store(sv, 33, gp, kDecW);
+}
+
+// t = r + q in place of q, with block partials of t.t and r.r
+__global__ void k_residual_loss(int n, const double* __restrict__ r, double* q, double* partials) {
+  double a = 0.0, b = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double ri = r[i];
+    const double t = ri + q[i];
+    q[i] = t;
+    a += t * t;
+    b += ri * ri;
+  }
+  a = block_sum(a);
+  b = block_sum(b);
+  if (threadIdx.x == 0) {
+    partials[2 * blockIdx.x] = a;
+    partials[2 * blockIdx.x + 1] = b;
+  }
+}
+
+// loss = sum t.t / sum r.r; gscale = 2 / sum r.r
+__global__ void k_residual_loss_finish(int np, const double* __restrict__ partials, double* loss, double* gscale) {
+  double a = 0.0, b = 0.0;
+  for (int k = threadIdx.x; k < np; k += blockDim.x) {
+    a += partials[2 * k];
+    b += partials[2 * k + 1];
+  }
+  a = block_sum(a);
+  b = block_sum(b);
+  if (threadIdx.x == 0) {
+    const double r2 = b > 0.0 ? b : 1.0;
+    loss[0] = a / r2;
+    gscale[0] = 2.0 / r2;
+  }
 }
 
 // dz = dHout * [Hout > 0]; dS = Ws^T dz; dM = Wm^T dz; gradients of Ws, Wm, b
@@ -622,6 +701,7 @@ void Workspace::allocate(int n_, bool training, long long entries) {
       check(cudaMalloc(&dS, hb), "cudaMalloc");
       gradBlocks = kGradBlocks;
       check(cudaMalloc(&gradPartials, sizeof(float) * (size_t)kGradBlocks * kParams), "cudaMalloc");
+      check(cudaMalloc(&dv, 2 * sizeof(double) * (size_t)n), "cudaMalloc");
     }
   }
   n = n_;
@@ -656,6 +736,8 @@ void Workspace::release() {
   for (auto& h : H) h = nullptr;
   for (auto& m : M) m = nullptr;
   n = cap = 0;
+  cudaFree(dv);
+  dv = nullptr;
 }
 
 void Workspace::checkStatus() {
@@ -702,6 +784,54 @@ void forward_backward(const Graph& g, const float* P, const double* r, const dou
   }
   k_encode_bwd<<<kGradBlocks, kBlock, 0, st>>>(n, w.u, w.H[0], w.dA, w.gradPartials);
   k_grad_reduce<<<ceil_div(kParams, kBlock), kBlock, 0, st>>>(kGradBlocks, w.gradPartials, grad);
+}
+
+void forward_backward_residual(const Graph& g, const float* P, const double* r, float* grad, double* loss,
+                               Workspace& w, double* scal, cudaStream_t st) {
+  const int n = w.n;
+  double* d = w.dv;
+  double* t = w.dv + n;
+  run_forward(g, P, r, w, scal, true, st);
+  k_decode<<<node_blocks(n), kBlock, 0, st>>>(n, P, w.H[kLayers], scal, d);
+  dev::spmv(g.a, g.nSlices, d, t, st);  // t = A d
+  k_residual_loss<<<kReduceBlocks, kBlock, 0, st>>>(n, r, t, w.partials);  // t = r + A d
+  k_residual_loss_finish<<<1, kBlock, 0, st>>>(kReduceBlocks, w.partials, loss, scal + 3);
+  dev::spmv(g.a, g.nSlices, t, d, st);  // d = A (r + A d): dL/dd / (2 / |r|^2)
+  k_decode_bwd_grad<<<kGradBlocks, kBlock, 0, st>>>(n, P, w.H[kLayers], scal, d, scal + 3, w.dA, w.gradPartials);
+  const GraphArgs ga = args(g, w);
+  const size_t smem = sizeof(float) * kWarps * kLayerSize;
+  check(cudaFuncSetAttribute(k_layer_bwd_a, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+        "k_layer_bwd_a shared memory");
+  check(cudaFuncSetAttribute(k_layer_bwd_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kBwdSmem),
+        "k_layer_bwd_tc shared memory");
+  for (int l = kLayers - 1; l >= 0; l--) {
+    const int off = kLayer0 + l * kLayerSize;
+    if (w.tensorCores)
+      k_layer_bwd_tc<<<kGradBlocks, kTcThreads, kBwdSmem, st>>>(n, P + off, w.H[l], w.H[l + 1], w.M[l], w.dA, w.dS,
+                                                                 w.dB, w.gradPartials, off, w.status);
+    else
+      k_layer_bwd_a<<<kGradBlocks, kBlock, smem, st>>>(n, P + off, w.H[l], w.H[l + 1], w.M[l], w.dA, w.dS, w.dB,
+                                                       w.gradPartials, off);
+    check(cudaGetLastError(), "layer backward launch");
+    k_layer_bwd_b<<<node_blocks(n), kBlock, 0, st>>>(n, ga, w.dS, w.dB, w.dA);
+  }
+  k_encode_bwd<<<kGradBlocks, kBlock, 0, st>>>(n, w.u, w.H[0], w.dA, w.gradPartials);
+  k_grad_reduce<<<ceil_div(kParams, kBlock), kBlock, 0, st>>>(kGradBlocks, w.gradPartials, grad);
+}
+
+int tc_wait_probe(unsigned limit) {
+  int* status = nullptr;
+  check(cudaMalloc(&status, sizeof(int)), "cudaMalloc");
+  int h = 0;
+  cudaError_t e = cudaMemset(status, 0, sizeof(int));
+  if (e == cudaSuccess) {
+    k_tc_wait_probe<<<1, 64>>>(limit, status);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpy(&h, status, sizeof(int), cudaMemcpyDeviceToHost);
+  cudaFree(status);
+  check(e, "tensor-core wait probe");
+  return h;
 }
 
 void adam_step(float* params, const float* grad, float* m, float* v, float lr, int t, cudaStream_t st) {
@@ -895,6 +1025,7 @@ int LearnedCorrection::numPairs() const {
 }
 
 void LearnedCorrection::train(int steps, float lr, uint64_t seed, double* losses, cudaStream_t st) {
+  residualFactor_ = -1.0;
   const int np = numPairs();
   FVM_REQUIRE(np > 0, kBadArgument, "learned correction: no training pairs (harvest first)");
   FVM_REQUIRE(steps >= 0 && lr > 0.f, kBadArgument, "learned correction: bad training settings");
@@ -919,8 +1050,12 @@ void LearnedCorrection::train(int steps, float lr, uint64_t seed, double* losses
     const auto& ix = index[next() % index.size()];
     Instance& in = inst_[ix.first];
     trainWs_.allocate(in.n, true, in.g.entries);
-    nn::forward_backward(in.g, dParams_, in.pairs[ix.second].first, in.pairs[ix.second].second, dGrad_,
-                         dLoss + t, trainWs_, dScal_, st);
+    if (objective_ == 1)
+      nn::forward_backward_residual(in.g, dParams_, in.pairs[ix.second].first, dGrad_, dLoss + t, trainWs_, dScal_,
+                                    st);
+    else
+      nn::forward_backward(in.g, dParams_, in.pairs[ix.second].first, in.pairs[ix.second].second, dGrad_,
+                           dLoss + t, trainWs_, dScal_, st);
     nn::adam_step(dParams_, dGrad_, dM_, dV_, lr, ++adamT_, st);
   }
   if (losses && steps > 0)
@@ -943,7 +1078,10 @@ double LearnedCorrection::evaluate(cudaStream_t st) {
   for (Instance& in : inst_)
     for (auto& pr : in.pairs) {
       trainWs_.allocate(in.n, true, in.g.entries);
-      nn::forward_backward(in.g, dParams_, pr.first, pr.second, dGrad_, dLoss + q++, trainWs_, dScal_, st);
+      if (objective_ == 1)
+        nn::forward_backward_residual(in.g, dParams_, pr.first, dGrad_, dLoss + q++, trainWs_, dScal_, st);
+      else
+        nn::forward_backward(in.g, dParams_, pr.first, pr.second, dGrad_, dLoss + q++, trainWs_, dScal_, st);
     }
   std::vector<double> l(np);
   nn::check(cudaMemcpyAsync(l.data(), dLoss, sizeof(double) * np, cudaMemcpyDeviceToHost, st), "cudaMemcpy");
@@ -952,6 +1090,7 @@ double LearnedCorrection::evaluate(cudaStream_t st) {
   trainWs_.checkStatus();
   double s = 0.0;
   for (double v : l) s += v;
+  if (objective_ == 1) residualFactor_ = std::sqrt(s / np);
   return s / np;
 }
 
@@ -964,6 +1103,17 @@ long long LearnedCorrection::maxEntries() const {
 void LearnedCorrection::prepare(int n, long long entries) {
   applyWs_.allocate(n, false, entries);
   applyWs_.tensorCores = tensorCores_;
+}
+
+void LearnedCorrection::setUsefulFactor(double f) {
+  FVM_REQUIRE(f > 0.0 && f <= 1.0, kBadArgument, "learned correction: useful factor must be in (0, 1]");
+  usefulFactor_ = f;
+}
+
+void LearnedCorrection::setObjective(int o) {
+  FVM_REQUIRE(o == 0 || o == 1, kBadArgument, "learned correction: objective must be 0 or 1");
+  if (o != objective_) residualFactor_ = -1.0;
+  objective_ = o;
 }
 
 void LearnedCorrection::setTensorCores(bool on) {

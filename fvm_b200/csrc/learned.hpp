@@ -61,6 +61,7 @@ struct Workspace {
   int gradBlocks = 0;
   int* status = nullptr;         // device flag: 1 if a tensor-core completion wait ran out
   bool tensorCores = true;       // dense layers on tcgen05 (TF32 inputs) instead of FP32 CUDA cores
+  double* dv = nullptr;          // n x 2 (training with the residual objective: d, then r + A d / A(r + A d))
   float* wf = nullptr;           // per-entry message weights (forward / transpose)
   float* wb = nullptr;
   long long wcap = 0;            // entries the weight buffers hold
@@ -70,6 +71,11 @@ struct Workspace {
   void checkStatus();
   ~Workspace() { release(); }
 };
+
+// Runs the tensor-core layers' bounded completion wait on an mbarrier that
+// no MMA signals, with `limit` tries; returns the status flag the kernel
+// set (1: the wait ran out, TMEM released, the kernel returned).
+int tc_wait_probe(unsigned limit);
 
 // Forward pass: out_i = d_i (FP64, may alias nothing). sOut (device) gets
 // the input scale s.
@@ -81,6 +87,13 @@ void forward(const Graph& g, const float* params, const double* r, double* out, 
 // double) = relative squared error of the pair.
 void forward_backward(const Graph& g, const float* params, const double* r, const double* e, float* grad,
                       double* loss, Workspace& w, double* scal, cudaStream_t st);
+
+// The same with the residual objective: loss = |r + A d|^2 / |r|^2 for the
+// network's correction d of residual r on graph g (A = g's matrix,
+// symmetric), gradient 2 A (r + A d) / |r|^2 through the network. Needs
+// only the residual of each pair.
+void forward_backward_residual(const Graph& g, const float* params, const double* r, float* grad, double* loss,
+                               Workspace& w, double* scal, cudaStream_t st);
 
 // Adam step on the parameters (t = step number from 1).
 void adam_step(float* params, const float* grad, float* m, float* v, float lr, int t, cudaStream_t st);
@@ -140,6 +153,23 @@ class LearnedCorrection {
   // throws if a tensor-core kernel of apply() gave up waiting (synchronises)
   void checkApplyStatus() { applyWs_.checkStatus(); }
 
+  // training objective: 0 = relative squared error of the predicted error
+  // (default), 1 = residual left by the correction, |r + A d|^2 / |r|^2
+  void setObjective(int o);
+  int objective() const { return objective_; }
+  // In the solve the step is retired after a few tries if fewer than a
+  // quarter of them cut the residual below this fraction of its value
+  // (default 0.5: what pays for the step's cost); 1 keeps every step that
+  // lowers the residual at all.
+  void setUsefulFactor(double f);
+  double usefulFactor() const { return usefulFactor_; }
+  // With the residual objective, evaluate() also records the residual
+  // reduction the network achieves on the training pairs, sqrt(mean
+  // |r + A d|^2 / |r|^2) (-1 before that). A solve does not use a network
+  // whose recorded reduction is above its useful factor: the step could
+  // not pay for itself.
+  double residualFactor() const { return residualFactor_; }
+
   // dense layers on the tensor cores (default) or in FP32 on the CUDA cores
   void setTensorCores(bool on);
   bool tensorCores() const { return tensorCores_; }
@@ -159,6 +189,9 @@ class LearnedCorrection {
   double* dScal_ = nullptr;
   int adamT_ = 0;
   bool tensorCores_ = true;
+  int objective_ = 0;
+  double usefulFactor_ = 0.5;
+  double residualFactor_ = -1.0;
   nn::Workspace trainWs_;
   nn::Workspace applyWs_;
 };

@@ -1,6 +1,8 @@
 // GPU AMG hierarchy and the linear solvers built on it.
 #include "solver.hpp"
 
+#include <math_constants.h>
+
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -600,11 +602,16 @@ void AmgHierarchy::cycle(CycleType t, int l, cudaStream_t st, bool xZero) {
     dev::dense_solve<T>(d.n, coarseInv_, vec_b<T>(d), vec_x<T>(d), st);
     return;
   }
+  // xZero: x is taken as zero. Without pre-smoothing its memory is not read
+  // before the prolongation assigns it; pre-smoothing, and the smoothing of
+  // a coarsest level, need it zeroed first.
+  const bool rhsOnly = xZero && opt_.nPreSweeps == 0 && !coarsest;
+  if (xZero && !rhsOnly) dev::zero<T>(d.n, vec_x<T>(d), st);
   sweeps<T>(opt_.nPreSweeps, l, st);
   if (!coarsest) {
     DevLevel& c = lv_[l + 1];
-    if (xZero && opt_.nPreSweeps == 0)
-      dev::restrict_rhs<T>(c.n, d.c2fRow, d.c2fCol, vec_b<T>(d), vec_b<T>(c), vec_x<T>(c), st);
+    if (rhsOnly)
+      dev::restrict_rhs<T>(c.n, d.c2fRow, d.c2fCol, vec_b<T>(d), vec_b<T>(c), (T*)nullptr, st);
     else
       dev::residual_restrict<T>(view<T>(d), d.nSlices, d.rowSlice, c.n, d.c2fRow, d.c2fCol, vec_x<T>(d),
                                 vec_b<T>(d), vec_b<T>(c), vec_x<T>(c), d.splitRestrict ? vec_r<T>(d) : nullptr, st);
@@ -613,9 +620,20 @@ void AmgHierarchy::cycle(CycleType t, int l, cudaStream_t st, bool xZero) {
       cycle<T>(kWCycle, l + 1, st);
     else if (t == kFCycle)
       cycle<T>(kVCycle, l + 1, st);
-    dev::prolong<T>(d.n, d.ci, vec_x<T>(c), vec_x<T>(d), st);
+    dev::prolong<T>(d.n, d.ci, vec_x<T>(c), vec_x<T>(d), st, rhsOnly);
   }
-  sweeps<T>(opt_.nPostSweeps, l, st);
+  sweeps<T>(opt_.postSweeps(l), l, st);
+}
+
+void AmgHierarchy::applyCycle(const double* r, cudaStream_t st) {
+  DevLevel& d = lv_[0];
+  if (opt_.precision == kMixed) {
+    dev::convert_d2f(d.n, r, d.bF, st);
+    runCycle<float>(st, true);
+  } else {
+    dev::copy_d(d.n, r, d.b, st);
+    runCycle<double>(st, true);
+  }
 }
 
 void AmgHierarchy::apply(const double* r, double* z, cudaStream_t st) {
@@ -629,13 +647,11 @@ void AmgHierarchy::apply(const double* r, double* z, cudaStream_t st) {
   }
   if (opt_.precision == kMixed) {
     dev::convert_d2f(d.n, r, d.bF, st);
-    dev::zero<float>(d.n, d.xF, st);
     runCycle<float>(st, true);
     dev::zero<double>(d.n, z, st);
     dev::add_f2d(d.n, d.xF, z, st);
   } else {
     dev::copy_d(d.n, r, d.b, st);
-    dev::zero<double>(d.n, d.x, st);
     runCycle<double>(st, true);
     dev::copy_d(d.n, d.x, z, st);
   }
@@ -657,8 +673,7 @@ double AmgHierarchy::cycleBytes() const {
   for (int l = 0; l < L; l++) {
     const DevLevel& d = lv_[l];
     const double pass = d.n * (4.0 * vb) + d.entries * (4.0 + vb);
-    const int sweeps = (l == L - 1) ? opt_.nPreSweeps + opt_.nPostSweeps
-                                    : opt_.nPreSweeps + opt_.nPostSweeps;
+    const int sweeps = opt_.nPreSweeps + opt_.postSweeps(l);
     if (l == L - 1 && coarseInv_) {
       total += (double)d.n * d.n * 8.0;
       continue;
@@ -687,7 +702,7 @@ int AmgHierarchy::kernelsPerCycle() const {
     const int perSweep = (opt_.smootherType == kGaussSeidel && !dampedLevel(l, d.n))
                              ? (opt_.ordering == kSequential ? 2 : 2 * d.nColors - 1)
                              : 2;
-    k += perSweep * (opt_.nPreSweeps + opt_.nPostSweeps);
+    k += perSweep * (opt_.nPreSweeps + opt_.postSweeps(l));
     if (l + 1 < L) k += 2;  // fused residual + restriction, prolongation
   }
   return k;
@@ -855,9 +870,60 @@ enum Scal {
   kLsAccepted,
   kLsSteps,
   kLsUseful,
+  kLsBefore,  // |r + A z1|_1 before the CG post-correction
   kNumScal
 };
-constexpr int kWorkVectors = 9;
+static_assert(kNumScal <= 32, "device scalars");
+constexpr int kWorkVectors = 11;
+
+// z = d1 + alpha d (the learned post-correction added to the cycle's z)
+__global__ void k_combine(int n, const double* __restrict__ d1, const double* alpha, const double* __restrict__ d,
+                          double* z) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) z[i] = d1[i] + alpha[0] * d[i];
+}
+// y = (double) x
+__global__ void k_f2d(int n, const float* __restrict__ x, double* y) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) y[i] = (double)x[i];
+}
+// y = a + b
+__global__ void k_add_vec(int n, const double* __restrict__ a, const double* __restrict__ b, double* y) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) y[i] = a[i] + b[i];
+}
+
+// Device-side loop control of the CG graph. Status: 0 running, 1
+// converged, 2 non-finite residual, 3 iteration limit.
+__global__ void k_cg_loop_init(double* scal, int* loopInt, double* history, double absTol, int maxIt,
+                               cudaGraphConditionalHandle h) {
+  const double r0 = scal[kNorm];
+  history[0] = r0;
+  loopInt[0] = 0;
+  const bool finite = isfinite(r0);
+  const bool done = !finite || r0 < absTol || maxIt <= 0;
+  loopInt[1] = !finite ? 2 : (r0 < absTol ? 1 : (maxIt <= 0 ? 3 : 0));
+  scal[kRho] = CUDART_INF;  // first beta = 0
+  cudaGraphSetConditional(h, done ? 0u : 1u);
+}
+
+__global__ void k_cg_loop_check(const double* scal, int* loopInt, double* history, double relTol, double absTol,
+                                int maxIt, cudaGraphConditionalHandle h) {
+  const double rn = scal[kNorm];
+  const int i = loopInt[0] + 1;
+  loopInt[0] = i;
+  history[i] = rn;
+  const double r0 = history[0];
+  int status = 0;
+  if (!isfinite(rn))
+    status = 2;
+  else if (rn < absTol || rn / r0 < relTol)
+    status = 1;
+  else if (i >= maxIt)
+    status = 3;
+  loopInt[1] = status;
+  cudaGraphSetConditional(h, status == 0 ? 1u : 0u);
+}
 }  // namespace
 
 // Device workspace comes from the hierarchy's arena (recycled by the next
@@ -868,10 +934,16 @@ LinearSolve::LinearSolve(AmgHierarchy& h) : h_(h), n_(h.level(0).n) {
   scal_ = (double*)h.scratch(sizeof(double) * 32);
   CUDA_OK(cudaMemset(scal_, 0, sizeof(double) * 32));
   partials_ = (double*)h.scratch(sizeof(double) * (dev::vec_blocks(n_) + 1));
+  {
+    const DevLevel& d = h.level(0);
+    const int np = std::max(2 * dev::vec_blocks(n_), dev::spmv_dot_blocks(d.view64(), d.nSlices));
+    partials2_ = (double*)h.scratch(sizeof(double) * (np + 2));
+  }
   hostScal_ = h.pinnedScalars();
 }
 
 LinearSolve::~LinearSolve() {
+  if (gLoop_) cudaGraphExecDestroy(gLoop_);
   if (g1_) cudaGraphExecDestroy(g1_);
   if (g2_) cudaGraphExecDestroy(g2_);
   if (g3_) cudaGraphExecDestroy(g3_);
@@ -980,7 +1052,6 @@ SolveReport LinearSolve::solveAMG(cudaStream_t st) {
     run(useLs ? g4_ : g1_, st, [&] {
       if (o.precision == kMixed) {
         dev::convert_d2f(n_, d.r, d.bF, st);
-        dev::zero<float>(n_, d.xF, st);
         h_.runCycle<float>(st, true);
         dev::add_f2d(n_, d.xF, d.x, st);
       } else {
@@ -1001,7 +1072,7 @@ SolveReport LinearSolve::solveAMG(cudaStream_t st) {
       // Any step that lowers the residual is kept. The step is retired for
       // good once it has been tried kLsProbe times and fewer than a quarter
       // of the tries cut the residual by the factor that pays for its cost
-      // (kLsUsefulFactor).
+      // (the correction's useful factor).
       const int kept = (int)hostScal_[1], useful = (int)hostScal_[2];
       rep.learnedSteps++;
       lsTries_++;
@@ -1070,7 +1141,8 @@ void LinearSolve::setLearned(LearnedCorrection* lc) {
     g4_ = nullptr;
   }
   learned_ = lc;
-  learnedActive_ = true;
+  // a network whose measured residual reduction cannot pay is not tried
+  learnedActive_ = !(lc && lc->residualFactor() >= 0.0 && lc->residualFactor() > lc->usefulFactor());
   lsTries_ = lsKept_ = 0;
   if (lc) lc->prepare(n_, (long long)h_.level(0).entries);
 }
@@ -1095,7 +1167,7 @@ void LinearSolve::learnedStep(cudaStream_t st, double* x, double* r, double acce
   dev::sum_partials(dev::vec_blocks(n_), partials_, scal_ + kLsTrial, st);
   nn::step_accept(n_, x, D, r, RT, scal_ + kLsAlpha, scal_ + kNorm, scal_ + kLsTrial, acceptFactor, st);
   nn::step_finish(scal_ + kNorm, scal_ + kLsTrial, scal_ + kLsAccepted, scal_ + kLsSteps, scal_ + kLsUseful,
-                  kLsUsefulFactor, acceptFactor, st);
+                  learned_->usefulFactor(), acceptFactor, st);
   launches += 19;
 }
 
@@ -1124,7 +1196,6 @@ int LinearSolve::solveRecording(cudaStream_t st, double relTol, int maxIter, int
   for (int i = 1; i < maxIter; i++) {
     if (o.precision == kMixed) {
       dev::convert_d2f(n_, d.r, d.bF, st);
-      dev::zero<float>(n_, d.xF, st);
       h_.runCycle<float>(st, true);
       dev::add_f2d(n_, d.xF, d.x, st);
     } else {
@@ -1163,6 +1234,11 @@ SolveReport LinearSolve::solveCG(cudaStream_t st) {
   const bool flexible = o.preconditioner == kPrecAMG &&
                         (o.precision == kMixed || o.nPreSweeps != o.nPostSweeps || o.cycleType != kVCycle);
   SolveReport rep;
+  // the whole solve on the device when nothing needs the host between
+  // iterations (no learned step, no printing)
+  if (o.preconditioner == kPrecAMG && o.useGraphs && o.verbosity <= 0 && !(learned_ && learnedActive_) &&
+      !graphsFailed_ && solveCGLoop(st, flexible, rep))
+    return rep;
   CUDA_OK(cudaMemsetAsync(X, 0, sizeof(double) * (size_t)n_, st));
   CUDA_OK(cudaMemsetAsync(P, 0, sizeof(double) * (size_t)n_, st));
   CUDA_OK(cudaMemsetAsync(Z, 0, sizeof(double) * (size_t)n_, st));  // z_0 enters the first flexible beta
@@ -1179,43 +1255,102 @@ SolveReport LinearSolve::solveCG(cudaStream_t st) {
   rep.history.push_back(r0);
   if (o.verbosity > 0) printf("0: %g\n", r0);
   if (!std::isfinite(r0)) throw Error(kNaN, "initial residual is not finite");
-  if (learned_ && learnedActive_ && r0 > 0.0) {
-    // learned initial correction of the delta; CG then starts from it. It is
-    // kept only if it at least halves the FP64 residual: a smaller cut does
-    // not pay for the new Krylov start (measured: +16 of 86 iterations on the
-    // 1.5M-cell tets when every lowering step was kept)
-    CUDA_OK(cudaMemsetAsync(scal_ + kLsAccepted, 0, 3 * sizeof(double), st));
-    learnedStep(st, X, R, kLsUsefulFactor);
-    CUDA_OK(cudaMemcpyAsync(hostScal_, scal_ + kLsAccepted, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
-    CUDA_OK(cudaStreamSynchronize(st));
-    rep.learnedSteps = 1;
-    rep.learnedAccepted = (int)hostScal_[0];
-    rep.learnedUseful = (int)hostScal_[2];
-    lsTries_++;
-    lsKept_ += rep.learnedUseful;
-    if (lsTries_ >= kLsProbe && 4 * lsKept_ < lsTries_) learnedActive_ = false;
-  }
+  // With the AMG preconditioner the vector work of an iteration is fused:
+  // z taken from the cycle with both dots, beta; p update; q = A p with
+  // p.q; alpha; the x and r updates with |r|.
+  const bool fused = o.preconditioner == kPrecAMG;
+  const bool mixedCycle = o.precision == kMixed;
   for (int i = 0; i < o.nMaxIterations; i++) {
-    run(g1_, st, [&] {
-      if (flexible) dot_into(R, Z, scal_ + kRzPrev, st);  // (r_k+1, z_k) before z is replaced
-      h_.apply(R, Z, st);
-      dev::copy_d(1, scal_ + kRho, scal_ + kRhoPrev, st);
-      dot_into(R, Z, scal_ + kRho, st);
-      if (flexible)
-        dev::scalar_flex_beta(scal_ + kRho, scal_ + kRzPrev, scal_ + kRhoPrev, scal_ + kBeta, st);
-      else
-        dev::scalar_div(scal_ + kRho, scal_ + kRhoPrev, scal_ + kBeta, st);  // 0 on the first pass
-      dev::xpby_dev(n_, Z, scal_ + kBeta, P, st);
-      dev::spmv(d.view64(), d.nSlices, P, Q, st);
-      dot_into(P, Q, scal_ + kPtq, st);
-      dev::scalar_div(scal_ + kRho, scal_ + kPtq, scal_ + kAlpha, st);
-      dev::axpy_dev(n_, scal_ + kAlpha, -1.0, P, X, st);
-      dev::axpy_dev(n_, scal_ + kAlpha, -1.0, Q, R, st);
-      norm_into(R, scal_ + kNorm, st);
-      CUDA_OK(cudaMemcpyAsync(hostScal_, scal_ + kNorm, sizeof(double), cudaMemcpyDeviceToHost, st));
-    });
+    // learned post-correction of the preconditioner (flexible CG): after the
+    // cycle's z1, the network corrects the residual r + A z1 that z1 leaves,
+    // with the step length alpha that minimises |r + A z1 + alpha A d|_2
+    const bool useLs = fused && learned_ && learnedActive_;
+    if (useLs) {
+      double* D1 = work_ + 6 * (size_t)n_;
+      double* R1 = work_ + 7 * (size_t)n_;
+      double* DN = work_ + 8 * (size_t)n_;
+      double* Q2 = work_ + 9 * (size_t)n_;
+      double* RT = work_ + 10 * (size_t)n_;
+      run(g4_, st, [&] {
+        h_.applyCycle(R, st);
+        const int gb = (n_ + 255) / 256;
+        if (mixedCycle)
+          k_f2d<<<gb, 256, 0, st>>>(n_, d.xF, D1);
+        else
+          dev::copy_d(n_, d.x, D1, st);
+        dev::spmv(d.view64(), d.nSlices, D1, R1, st);
+        k_add_vec<<<gb, 256, 0, st>>>(n_, R, R1, R1);
+        const nn::Graph g{d.view64(), d.rowSlice, d.nSlices, (long long)d.entries};
+        learned_->apply(g, R1, DN, scal_ + kLsScale, st);
+        dev::spmv(d.view64(), d.nSlices, DN, Q2, st);
+        dot_into(R1, Q2, scal_ + kLsRq, st);
+        dot_into(Q2, Q2, scal_ + kLsQq, st);
+        nn::step_alpha(scal_ + kLsRq, scal_ + kLsQq, scal_ + kLsAlpha, st);
+        norm_into(R1, scal_ + kLsBefore, st);
+        nn::step_trial(n_, R1, Q2, scal_ + kLsAlpha, RT, partials_, st);
+        dev::sum_partials(dev::vec_blocks(n_), partials_, scal_ + kLsTrial, st);
+        k_combine<<<gb, 256, 0, st>>>(n_, D1, scal_ + kLsAlpha, DN, D1);
+        dev::cg_take_z<double>(n_, D1, R, Z, partials2_, st);
+        dev::cg_beta(dev::vec_blocks(n_), partials2_, scal_ + kRho, scal_ + kRhoPrev, scal_ + kBeta, flexible, st);
+        dev::xpby_dev(n_, Z, scal_ + kBeta, P, st);
+        dev::spmv_dot(d.view64(), d.nSlices, P, Q, partials2_, st);
+        dev::cg_alpha(dev::spmv_dot_blocks(d.view64(), d.nSlices), partials2_, scal_ + kRho, scal_ + kAlpha, st);
+        dev::cg_update(n_, scal_ + kAlpha, P, Q, X, R, partials_, st);
+        dev::sum_partials(dev::vec_blocks(n_), partials_, scal_ + kNorm, st);
+        CUDA_OK(cudaMemcpyAsync(hostScal_, scal_ + kNorm, sizeof(double), cudaMemcpyDeviceToHost, st));
+        CUDA_OK(cudaMemcpyAsync(hostScal_ + 1, scal_ + kLsBefore, sizeof(double), cudaMemcpyDeviceToHost, st));
+        CUDA_OK(cudaMemcpyAsync(hostScal_ + 2, scal_ + kLsTrial, sizeof(double), cudaMemcpyDeviceToHost, st));
+      });
+      launches += 6;
+    } else if (fused) {
+      run(g1_, st, [&] {
+        h_.applyCycle(R, st);
+        if (mixedCycle)
+          dev::cg_take_z<float>(n_, d.xF, R, Z, partials2_, st);
+        else
+          dev::cg_take_z<double>(n_, d.x, R, Z, partials2_, st);
+        dev::cg_beta(dev::vec_blocks(n_), partials2_, scal_ + kRho, scal_ + kRhoPrev, scal_ + kBeta, flexible, st);
+        dev::xpby_dev(n_, Z, scal_ + kBeta, P, st);
+        dev::spmv_dot(d.view64(), d.nSlices, P, Q, partials2_, st);
+        dev::cg_alpha(dev::spmv_dot_blocks(d.view64(), d.nSlices), partials2_, scal_ + kRho, scal_ + kAlpha, st);
+        dev::cg_update(n_, scal_ + kAlpha, P, Q, X, R, partials_, st);
+        dev::sum_partials(dev::vec_blocks(n_), partials_, scal_ + kNorm, st);
+        CUDA_OK(cudaMemcpyAsync(hostScal_, scal_ + kNorm, sizeof(double), cudaMemcpyDeviceToHost, st));
+      });
+    } else {
+      run(g1_, st, [&] {
+        if (flexible) dot_into(R, Z, scal_ + kRzPrev, st);  // (r_k+1, z_k) before z is replaced
+        h_.apply(R, Z, st);
+        dev::copy_d(1, scal_ + kRho, scal_ + kRhoPrev, st);
+        dot_into(R, Z, scal_ + kRho, st);
+        if (flexible)
+          dev::scalar_flex_beta(scal_ + kRho, scal_ + kRzPrev, scal_ + kRhoPrev, scal_ + kBeta, st);
+        else
+          dev::scalar_div(scal_ + kRho, scal_ + kRhoPrev, scal_ + kBeta, st);  // 0 on the first pass
+        dev::xpby_dev(n_, Z, scal_ + kBeta, P, st);
+        dev::spmv(d.view64(), d.nSlices, P, Q, st);
+        dot_into(P, Q, scal_ + kPtq, st);
+        dev::scalar_div(scal_ + kRho, scal_ + kPtq, scal_ + kAlpha, st);
+        dev::axpy_dev(n_, scal_ + kAlpha, -1.0, P, X, st);
+        dev::axpy_dev(n_, scal_ + kAlpha, -1.0, Q, R, st);
+        norm_into(R, scal_ + kNorm, st);
+        CUDA_OK(cudaMemcpyAsync(hostScal_, scal_ + kNorm, sizeof(double), cudaMemcpyDeviceToHost, st));
+      });
+    }
     CUDA_OK(cudaStreamSynchronize(st));
     const double rn = hostScal_[0];
+    if (useLs) {
+      // the step pays when it cuts the residual z1 leaves by the useful factor;
+      // after kLsProbe tries it is retired if fewer than a quarter did
+      const double before = hostScal_[1], after = hostScal_[2];
+      const bool useful = std::isfinite(after) && after < learned_->usefulFactor() * before;
+      rep.learnedSteps++;
+      rep.learnedAccepted += useful ? 1 : 0;
+      rep.learnedUseful += useful ? 1 : 0;
+      lsTries_++;
+      lsKept_ += useful ? 1 : 0;
+      if (lsTries_ >= kLsProbe && 4 * lsKept_ < lsTries_) learnedActive_ = false;
+    }
     rep.iterations = i + 1;
     rep.finalNorm = rn;
     rep.history.push_back(rn);
@@ -1239,6 +1374,161 @@ SolveReport LinearSolve::solveCG(cudaStream_t st) {
   dev::copy_d(n_, B, d.b, st);
   CUDA_OK(cudaStreamSynchronize(st));
   return rep;
+}
+
+bool LinearSolve::buildCGLoop(cudaStream_t st, bool flexible) {
+  const SolverOptions& o = h_.options();
+  DevLevel& d = h_.level(0);
+  double* X = work_;
+  double* R = work_ + (size_t)n_;
+  double* Z = work_ + 2 * (size_t)n_;
+  double* P = work_ + 3 * (size_t)n_;
+  double* Q = work_ + 4 * (size_t)n_;
+  double* B = work_ + 5 * (size_t)n_;
+  if (gLoop_) cudaGraphExecDestroy(gLoop_);
+  gLoop_ = nullptr;
+  if (!loopInt_) loopInt_ = (int*)h_.scratch(4 * sizeof(int));
+  history_ = (double*)h_.scratch(sizeof(double) * (size_t)(o.nMaxIterations + 2));
+  const bool mixedCycle = o.precision == kMixed;
+  const cudaStreamCaptureMode mode = cudaStreamCaptureModeThreadLocal;
+  cudaGraph_t g = nullptr;
+  cudaGraphConditionalHandle h = 0;
+  bool ok = cudaGraphCreate(&g, 0) == cudaSuccess &&
+            cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault) == cudaSuccess;
+  // prologue: x = 0, p = 0, z = 0, r = b, |r| (host copies of b kept in B)
+  ok = ok && cudaStreamBeginCaptureToGraph(st, g, nullptr, nullptr, 0, mode) == cudaSuccess;
+  if (ok) {
+    try {
+      CUDA_OK(cudaMemsetAsync(X, 0, sizeof(double) * (size_t)n_, st));
+      CUDA_OK(cudaMemsetAsync(P, 0, sizeof(double) * (size_t)n_, st));
+      CUDA_OK(cudaMemsetAsync(Z, 0, sizeof(double) * (size_t)n_, st));
+      dev::copy_d(n_, d.b, B, st);
+      dev::residual<double>(d.view64(), d.nSlices, X, B, R, nullptr, st);
+      norm_into(R, scal_ + kNorm, st);
+      k_cg_loop_init<<<1, 1, 0, st>>>(scal_, loopInt_, history_, o.absoluteTolerance, o.nMaxIterations, h);
+    } catch (const Error&) {
+      ok = false;
+    }
+    cudaGraph_t gg = nullptr;
+    ok = cudaStreamEndCapture(st, &gg) == cudaSuccess && ok;
+  }
+  // the while node after the prologue's last node
+  cudaGraphNode_t cnode = nullptr;
+  cudaGraph_t body = nullptr;
+  if (ok) {
+    size_t nn = 0;
+    ok = cudaGraphGetNodes(g, nullptr, &nn) == cudaSuccess && nn > 0;
+    std::vector<cudaGraphNode_t> nodes(nn), leaves;
+    ok = ok && cudaGraphGetNodes(g, nodes.data(), &nn) == cudaSuccess;
+    for (size_t k = 0; ok && k < nn; k++) {
+      size_t nd = 0;
+      ok = cudaGraphNodeGetDependentNodes(nodes[k], nullptr, &nd) == cudaSuccess;
+      if (ok && nd == 0) leaves.push_back(nodes[k]);
+    }
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    ok = ok && !leaves.empty() && cudaGraphAddNode(&cnode, g, leaves.data(), leaves.size(), &cp) == cudaSuccess;
+    if (ok) body = cp.conditional.phGraph_out[0];
+  }
+  // body: one fused iteration and the convergence check
+  ok = ok && cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0, mode) == cudaSuccess;
+  if (ok) {
+    try {
+      h_.applyCycle(R, st);
+      if (mixedCycle)
+        dev::cg_take_z<float>(n_, d.xF, R, Z, partials2_, st);
+      else
+        dev::cg_take_z<double>(n_, d.x, R, Z, partials2_, st);
+      dev::cg_beta(dev::vec_blocks(n_), partials2_, scal_ + kRho, scal_ + kRhoPrev, scal_ + kBeta, flexible, st);
+      dev::xpby_dev(n_, Z, scal_ + kBeta, P, st);
+      dev::spmv_dot(d.view64(), d.nSlices, P, Q, partials2_, st);
+      dev::cg_alpha(dev::spmv_dot_blocks(d.view64(), d.nSlices), partials2_, scal_ + kRho, scal_ + kAlpha, st);
+      dev::cg_update(n_, scal_ + kAlpha, P, Q, X, R, partials_, st);
+      dev::sum_partials(dev::vec_blocks(n_), partials_, scal_ + kNorm, st);
+      k_cg_loop_check<<<1, 1, 0, st>>>(scal_, loopInt_, history_, o.relativeTolerance, o.absoluteTolerance,
+                                       o.nMaxIterations, h);
+    } catch (const Error&) {
+      ok = false;
+    }
+    cudaGraph_t bb = nullptr;
+    ok = cudaStreamEndCapture(st, &bb) == cudaSuccess && ok;
+    size_t nb = 0;
+    if (ok) cudaGraphGetNodes(body, nullptr, &nb);
+    loopBodyNodes_ = (long long)nb;
+  }
+  // epilogue: the true residual's norm, the system restored, the results to
+  // the pinned host scalars
+  ok = ok && cudaStreamBeginCaptureToGraph(st, g, &cnode, nullptr, 1, mode) == cudaSuccess;
+  if (ok) {
+    try {
+      dev::residual<double>(d.view64(), d.nSlices, X, B, R, nullptr, st);
+      norm_into(R, scal_ + kNorm, st);
+      dev::copy_d(n_, X, d.x, st);
+      dev::copy_d(n_, B, d.b, st);
+      CUDA_OK(cudaMemcpyAsync(hostScal_, scal_ + kNorm, sizeof(double), cudaMemcpyDeviceToHost, st));
+      CUDA_OK(cudaMemcpyAsync(hostScal_ + 1, history_, sizeof(double), cudaMemcpyDeviceToHost, st));
+      CUDA_OK(cudaMemcpyAsync(hostScal_ + 2, loopInt_, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
+    } catch (const Error&) {
+      ok = false;
+    }
+    cudaGraph_t ee = nullptr;
+    ok = cudaStreamEndCapture(st, &ee) == cudaSuccess && ok;
+  }
+  if (ok) {
+    size_t nn = 0;
+    cudaGraphGetNodes(g, nullptr, &nn);
+    loopOtherNodes_ = (long long)nn - 1;  // all but the while node
+  }
+  ok = ok && cudaGraphInstantiate(&gLoop_, g, 0) == cudaSuccess;
+  if (g) cudaGraphDestroy(g);
+  if (!ok) {
+    if (gLoop_) cudaGraphExecDestroy(gLoop_);
+    gLoop_ = nullptr;
+    cudaGetLastError();
+    return false;
+  }
+  loopFlexible_ = flexible;
+  loopMaxIt_ = o.nMaxIterations;
+  loopRel_ = o.relativeTolerance;
+  loopAbs_ = o.absoluteTolerance;
+  return true;
+}
+
+bool LinearSolve::solveCGLoop(cudaStream_t st, bool flexible, SolveReport& rep) {
+  const SolverOptions& o = h_.options();
+  if (loopFailed_) return false;
+  if (!gLoop_ || loopFlexible_ != flexible || loopMaxIt_ != o.nMaxIterations || loopRel_ != o.relativeTolerance ||
+      loopAbs_ != o.absoluteTolerance) {
+    if (!buildCGLoop(st, flexible)) {
+      loopFailed_ = true;
+      return false;
+    }
+  }
+  CUDA_OK(cudaGraphLaunch(gLoop_, st));
+  CUDA_OK(cudaStreamSynchronize(st));
+  const double finalNorm = hostScal_[0];
+  const double r0 = hostScal_[1];
+  int loop[2];
+  std::memcpy(loop, hostScal_ + 2, sizeof(loop));
+  const int iters = loop[0], status = loop[1];
+  launches += loopOtherNodes_ + (long long)iters * loopBodyNodes_;
+  rep = SolveReport();
+  rep.initialNorm = r0;
+  rep.iterations = iters;
+  rep.history.assign((size_t)iters + 1, 0.0);
+  if (iters > 0)
+    CUDA_OK(cudaMemcpy(rep.history.data(), history_, sizeof(double) * (iters + 1), cudaMemcpyDeviceToHost));
+  else
+    rep.history[0] = r0;
+  if (!std::isfinite(r0)) throw Error(kNaN, "initial residual is not finite");
+  if (status == 2) throw Error(kNaN, "residual became non-finite");
+  rep.converged = status == 1;
+  rep.finalNorm = iters > 0 ? finalNorm : r0;
+  if (iters > 0) rep.history.back() = rep.finalNorm;
+  return true;
 }
 
 // BCGStab::solve (BCGStab.cpp:27-170) with the AMG cycle as preconditioner.

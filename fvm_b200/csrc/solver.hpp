@@ -67,6 +67,10 @@ struct SolverOptions {
   bool setupOnDevice = false;
   int matchRounds = 4;          // handshake rounds per level
   double matchBeta = 0.25;      // candidate when strength >= beta * the row's strongest
+  int matchPasses = 1;          // matchings per level: 2 pairs the pairs (aggregates of about 4 rows)
+  // post-smoothing sweeps on the levels below the finest (-1: nPostSweeps)
+  int coarsePostSweeps = -1;
+  int postSweeps(int l) const { return l > 0 && coarsePostSweeps >= 0 ? coarsePostSweeps : nPostSweeps; }
   // only the finest level is needed (Jacobi solver or preconditioner)
   bool finestOnly() const { return solver == kSolverJacobi || preconditioner == kPrecJacobi; }
 };
@@ -218,6 +222,9 @@ class AmgHierarchy {
   // x = z <- M^-1 applied to r (FP64 in/out; runs the cycle in the
   // configured precision): b0 <- r, x0 <- 0, cycle, z <- x0
   void apply(const double* r, double* z, cudaStream_t st);
+  // the same cycle, its result left in level 0's x (FP64) or xF (mixed)
+  // instead of being copied to z; AMG preconditioner only
+  void applyCycle(const double* r, cudaStream_t st);
 
   const SolverOptions& options() const { return opt_; }
 
@@ -290,6 +297,20 @@ class LinearSolve {
  private:
   SolveReport solveAMG(cudaStream_t st);
   SolveReport solveCG(cudaStream_t st);
+  // CG with the fused iteration, every iteration of one solve inside one
+  // CUDA graph (a conditional while node whose condition a device kernel
+  // sets from the residual norm): one host synchronisation per solve.
+  // Returns false (and is not used again) when the graph cannot be built.
+  bool solveCGLoop(cudaStream_t st, bool flexible, SolveReport& rep);
+  bool buildCGLoop(cudaStream_t st, bool flexible);
+  cudaGraphExec_t gLoop_ = nullptr;
+  bool loopFailed_ = false;
+  bool loopFlexible_ = false;
+  int loopMaxIt_ = -1;
+  double loopRel_ = 0.0, loopAbs_ = 0.0;
+  int* loopInt_ = nullptr;       // device: iterations, status
+  long long loopBodyNodes_ = 0, loopOtherNodes_ = 0;  // kernels and copies per iteration / per solve
+  double* history_ = nullptr;    // device: norms of iterations 0..nMaxIterations
   SolveReport solveBCGStab(cudaStream_t st);
   SolveReport solveJacobi(cudaStream_t st);
   void norm_into(const double* v, double* scalar, cudaStream_t st);
@@ -303,15 +324,16 @@ class LinearSolve {
   double* work_ = nullptr;    // vectors
   double* scal_ = nullptr;    // device scalars
   double* partials_ = nullptr;
+  double* partials2_ = nullptr;  // the fused CG steps' partial sums
   double* hostScal_ = nullptr;  // pinned
   cudaGraphExec_t g1_ = nullptr, g2_ = nullptr, g3_ = nullptr, g4_ = nullptr, g5_ = nullptr;
   LearnedCorrection* learned_ = nullptr;
   // the learned step stays on while it pays: after kLsProbe tries it is
-  // retired if fewer than a quarter cut the FP64 L1 residual below
-  // kLsUsefulFactor times its value (the step costs about two V-cycles of
-  // the mixed solve: three layers over the finest graph, an SpMV, two dots)
+  // retired if fewer than a quarter cut the FP64 L1 residual below the
+  // correction's useful factor times its value (default 0.5: the step costs
+  // about two V-cycles of the mixed solve: three layers over the finest
+  // graph, an SpMV, two dots)
   static constexpr int kLsProbe = 3;
-  static constexpr double kLsUsefulFactor = 0.5;
   bool learnedActive_ = true;
   int lsTries_ = 0, lsKept_ = 0;
   void learnedStep(cudaStream_t st, double* x, double* r, double acceptFactor);

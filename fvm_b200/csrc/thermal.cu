@@ -58,13 +58,24 @@ GroupBC& ThermalModel::bc(int groupId) {
   throw Error(kBadArgument, "no boundary face group with id " + std::to_string(groupId));
 }
 
+namespace {
+__global__ void k_fill_value(int n, double* x, double v) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) x[i] = v;
+}
+}  // namespace
+
 void ThermalModel::init() {
   const int nAll = mesh_->nTotalCells();
-  T_.assign(nAll, opt_.initialTemperature);
-  k_.assign(nAll, opt_.thermalConductivity);
-  src_.assign(nAll, 0.0);
-  rc_.assign(nAll, opt_.density * opt_.specificHeat);
-  TN1_ = T_;
+  for (HostField* f : {&T_, &k_, &src_, &rc_, &TN1_})
+    if ((int)f->size() != nAll) f->resize(nAll);
+  // every field starts uniform: nothing is written on the host here
+  uniform_.fill(true);
+  uniformValue_[kFieldTemperature] = opt_.initialTemperature;
+  uniformValue_[kFieldConductivity] = opt_.thermalConductivity;
+  uniformValue_[kFieldSource] = 0.0;
+  uniformValue_[kFieldSpecificHeat] = opt_.density * opt_.specificHeat;
+  uniformValue_[kFieldTemperatureN1] = opt_.initialTemperature;
   tDirty_ = kDirty_ = srcDirty_ = rcDirty_ = tn1Dirty_ = true;
   matrixDirty_ = hierarchyDirty_ = true;
   initialNorm_ = -1;
@@ -142,22 +153,26 @@ bool ThermalModel::segmentsConverged() {
   return all;
 }
 
-static std::vector<double>& field_ref(int field, std::vector<double>& T, std::vector<double>& k,
-                                      std::vector<double>& s, std::vector<double>& rc,
-                                      std::vector<double>& tn1) {
-  switch (field) {
+HostField& ThermalModel::field(int f) {
+  switch (f) {
     case kFieldTemperature:
-      return T;
+      return T_;
     case kFieldConductivity:
-      return k;
+      return k_;
     case kFieldSource:
-      return s;
+      return src_;
     case kFieldSpecificHeat:
-      return rc;
+      return rc_;
     case kFieldTemperatureN1:
-      return tn1;
+      return TN1_;
   }
   throw Error(kBadArgument, "unknown cell field");
+}
+
+void ThermalModel::materialize(int f) {
+  HostField& v = field(f);
+  if (uniform_[f]) std::fill(v.begin(), v.end(), uniformValue_[f]);
+  uniform_[f] = false;
 }
 
 void ThermalModel::setCellField(int field, const double* values, int count) {
@@ -165,12 +180,19 @@ void ThermalModel::setCellField(int field, const double* values, int count) {
   const int n = mesh_->nCells, nAll = mesh_->nTotalCells();
   FVM_REQUIRE(count == nAll || count == n, kBadArgument,
               "cell field length must be nCells or nCells + ghost cells");
-  if (field == kFieldTemperature && deviceReady_ && !tDirty_) {
-    // keep ghost values the device already holds when only self cells are given
-    CUDA_OK(cudaMemcpy(T_.data(), dT_, sizeof(double) * nAll, cudaMemcpyDeviceToHost));
+  if (field == kFieldTemperature && count == n) {
+    // keep the ghost values the device (or the uniform start) holds when
+    // only self cells are given
+    if (deviceReady_ && !tDirty_) {
+      CUDA_OK(cudaMemcpy(T_.data(), dT_, sizeof(double) * nAll, cudaMemcpyDeviceToHost));
+      uniform_[kFieldTemperature] = false;
+    } else {
+      materialize(kFieldTemperature);
+    }
   }
-  std::vector<double>& f = field_ref(field, T_, k_, src_, rc_, TN1_);
+  HostField& f = this->field(field);
   std::copy(values, values + count, f.begin());
+  uniform_[field] = false;
   if (count == n && field != kFieldTemperature) {
     // ghost cells take the value of their interior neighbour
     const HostMesh& m = *mesh_;
@@ -209,7 +231,14 @@ void ThermalModel::getCellField(int field, double* out, int count) {
     if (field == kFieldTemperatureN1 && !tn1Dirty_)
       CUDA_OK(cudaMemcpy(TN1_.data(), dTN1_, sizeof(double) * nAll, cudaMemcpyDeviceToHost));
   }
-  std::vector<double>& f = field_ref(field, T_, k_, src_, rc_, TN1_);
+  if ((field == kFieldTemperature && deviceReady_ && !tDirty_) ||
+      (field == kFieldTemperatureN1 && deviceReady_ && !tn1Dirty_))
+    uniform_[field] = false;  // the device copy just came back
+  if (uniform_[field]) {
+    std::fill(out, out + count, uniformValue_[field]);
+    return;
+  }
+  HostField& f = this->field(field);
   std::copy(f.begin(), f.begin() + count, out);
 }
 
@@ -314,14 +343,23 @@ void ThermalModel::ensureDevice() {
 
 void ThermalModel::uploadFields() {
   const size_t cb = sizeof(double) * (size_t)mesh_->nTotalCells();
-  if (tDirty_) CUDA_OK(cudaMemcpyAsync(dT_, T_.data(), cb, cudaMemcpyHostToDevice, stream_));
-  if (kDirty_) CUDA_OK(cudaMemcpyAsync(dK_, k_.data(), cb, cudaMemcpyHostToDevice, stream_));
-  if (srcDirty_) CUDA_OK(cudaMemcpyAsync(dSrc_, src_.data(), cb, cudaMemcpyHostToDevice, stream_));
+  const int nAll = mesh_->nTotalCells();
+  // a uniform field is filled on the device; the others are copied from
+  // the pinned host arrays
+  auto up = [&](int f, double* d) {
+    if (uniform_[f])
+      k_fill_value<<<(nAll + 255) / 256, 256, 0, stream_>>>(nAll, d, uniformValue_[f]);
+    else
+      CUDA_OK(cudaMemcpyAsync(d, field(f).data(), cb, cudaMemcpyHostToDevice, stream_));
+  };
+  if (tDirty_) up(kFieldTemperature, dT_);
+  if (kDirty_) up(kFieldConductivity, dK_);
+  if (srcDirty_) up(kFieldSource, dSrc_);
   // rho c and the previous step's T enter only the transient term: a steady
   // model leaves them on the host (still dirty) until it becomes transient
   const bool transient = opt_.transient;
-  if (rcDirty_ && transient) CUDA_OK(cudaMemcpyAsync(dRc_, rc_.data(), cb, cudaMemcpyHostToDevice, stream_));
-  if (tn1Dirty_ && transient) CUDA_OK(cudaMemcpyAsync(dTN1_, TN1_.data(), cb, cudaMemcpyHostToDevice, stream_));
+  if (rcDirty_ && transient) up(kFieldSpecificHeat, dRc_);
+  if (tn1Dirty_ && transient) up(kFieldTemperatureN1, dTN1_);
   CUDA_OK(cudaStreamSynchronize(stream_));
   tDirty_ = kDirty_ = srcDirty_ = false;
   if (transient) rcDirty_ = tn1Dirty_ = false;
@@ -662,7 +700,13 @@ int ThermalModel::harvest(LearnedCorrection& lc, int nOuter, int perSolve, doubl
 void ThermalModel::updateTime() {
   FVM_REQUIRE(initialized_, kBadArgument, "ThermalModel.init() must be called first");
   if (!deviceReady_ || tDirty_) {
-    TN1_ = T_;
+    if (uniform_[kFieldTemperature]) {
+      uniform_[kFieldTemperatureN1] = true;
+      uniformValue_[kFieldTemperatureN1] = uniformValue_[kFieldTemperature];
+    } else {
+      TN1_ = T_;
+      uniform_[kFieldTemperatureN1] = false;
+    }
     tn1Dirty_ = true;
     return;
   }

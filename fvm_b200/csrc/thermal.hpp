@@ -6,6 +6,8 @@
 #include <cuda_runtime.h>
 
 #include <array>
+#include <cstdlib>
+#include <new>
 #include <memory>
 #include <string>
 #include <vector>
@@ -14,6 +16,40 @@
 #include "solver.hpp"
 
 namespace fvm {
+
+// Page-locked host memory for the cell fields that cross to the device on
+// every solve, so their copies run at the link's full rate; plain heap
+// memory where no device is present (the host-only tests).
+template <class T>
+struct PinnedAllocator {
+  using value_type = T;
+  PinnedAllocator() = default;
+  template <class U>
+  PinnedAllocator(const PinnedAllocator<U>&) {}
+  T* allocate(size_t n) {
+    void* p = nullptr;
+    if (n == 0) n = 1;
+    if (cudaMallocHost(&p, n * sizeof(T)) == cudaSuccess) return static_cast<T*>(p);
+    cudaGetLastError();
+    p = std::malloc(n * sizeof(T));
+    if (!p) throw std::bad_alloc();
+    return static_cast<T*>(p);
+  }
+  void deallocate(T* p, size_t) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) == cudaSuccess && a.type == cudaMemoryTypeHost) {
+      cudaFreeHost(p);
+    } else {
+      cudaGetLastError();
+      std::free(p);
+    }
+  }
+  template <class U>
+  bool operator==(const PinnedAllocator<U>&) const { return true; }
+  template <class U>
+  bool operator!=(const PinnedAllocator<U>&) const { return false; }
+};
+using HostField = std::vector<double, PinnedAllocator<double>>;
 
 enum BcType {
   kBcSpecifiedTemperature = 0,
@@ -142,7 +178,14 @@ class ThermalModel {
   ThermalOptions opt_;
   bool initialized_ = false;
   // host fields, self + ghost cells
-  std::vector<double> T_, k_, src_, rc_, TN1_;
+  HostField T_, k_, src_, rc_, TN1_;
+  // a field still holding the uniform value init() gave it is not written
+  // on the host: it is filled where it is needed (on the device by a
+  // kernel, on the host when only part of it is set or it is read back)
+  std::array<bool, 5> uniform_{};
+  std::array<double, 5> uniformValue_{};
+  HostField& field(int f);
+  void materialize(int f);
   bool tDirty_ = true, kDirty_ = true, srcDirty_ = true, rcDirty_ = true, tn1Dirty_ = true;
   bool matrixDirty_ = true, hierarchyDirty_ = true;
   double initialNorm_ = -1;

@@ -197,6 +197,8 @@ class AMG(LinearSolver):
         self.setupOnDevice = bool(d.setupOnDevice)
         self.matchRounds = d.matchRounds
         self.matchBeta = d.matchBeta
+        self.matchPasses = d.matchPasses
+        self.coarsePostSweeps = d.coarsePostSweeps
         self._printFile = None
 
     def setMergeLevelSize(self, size: int) -> None:
@@ -237,6 +239,8 @@ class AMG(LinearSolver):
         o.setupOnDevice = int(bool(self.setupOnDevice))
         o.matchRounds = int(self.matchRounds)
         o.matchBeta = float(self.matchBeta)
+        o.matchPasses = int(self.matchPasses)
+        o.coarsePostSweeps = int(self.coarsePostSweeps)
 
     def options(self) -> _lib.LinearOptions:
         o = _lib.LinearOptions()

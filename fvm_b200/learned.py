@@ -82,6 +82,27 @@ class LearnedCorrection:
     def tensorCores(self, on: bool) -> None:
         check(_lib.load().fvm_learned_set_tensor_cores(self._h, 1 if on else 0))
 
+    ERROR, RESIDUAL = 0, 1
+
+    def setObjective(self, objective: int) -> None:
+        """Training objective: ERROR (relative squared error of the
+        predicted error, the default) or RESIDUAL (|r + A d|^2 / |r|^2, the
+        residual the correction leaves)."""
+        check(_lib.load().fvm_learned_set_objective(self._h, int(objective)))
+
+    def setUsefulFactor(self, f: float) -> None:
+        """The solve retires the step after three tries if fewer than a
+        quarter cut the residual below f times its value (default 0.5)."""
+        check(_lib.load().fvm_learned_set_useful_factor(self._h, float(f)))
+
+    def residualFactor(self) -> float:
+        """sqrt(mean |r + A d|^2 / |r|^2) on the pairs at the last
+        evaluate() with the RESIDUAL objective (-1 if none since training);
+        a solve skips the network when it is above the useful factor."""
+        v = ctypes.c_double(0)
+        check(_lib.load().fvm_learned_residual_factor(self._h, ctypes.byref(v)))
+        return v.value
+
     def harvest(self, model, nOuter: int = 20, perSolve: int = 4, relativeTolerance: float = 1e-10,
                 maxCycles: int = 200) -> int:
         """Outer iterations of `model` (a ThermalModelA with a plain AMG

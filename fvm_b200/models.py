@@ -395,6 +395,6 @@ class ThermalModelA:
 
     def _get_field(self, name, site) -> np.ndarray:
         n = site.getCount()
-        out = np.zeros(n)
+        out = np.empty(n)
         check(_lib.load().fvm_thermal_get_cell_field(self._h, 0, FIELD_IDS[name], dptr(out), n))
         return out

@@ -86,6 +86,9 @@ typedef struct fvm_linear_options {
   int matchRounds;          /* handshake rounds per level of that matching (default 4) */
   double matchBeta;         /* a neighbour is a matching candidate when its strength is at least
                                this fraction of the row's strongest (default 0.25) */
+  int matchPasses;          /* matchings per level: 1 pairs rows, 2 pairs the pairs (aggregates of
+                               about 4 rows, half as many levels) */
+  int coarsePostSweeps;     /* post-smoothing sweeps on the levels below the finest (-1: nPostSweeps) */
 } fvm_linear_options;
 
 /* ThermalModelOptions (fvmbase/ThermalBC.h:33-67) + volume-condition constants */
@@ -335,7 +338,27 @@ int fvm_learned_gradient_csr(fvm_learned* l, int n, const int* row, const int* c
  * cores (on == 0). Applies to training, evaluation, forward/gradient and
  * the solve. No reference counterpart (the learned correction is new). */
 int fvm_learned_set_tensor_cores(fvm_learned* l, int on);
+/* Training objective (no reference counterpart): 0 = relative squared
+ * error of the predicted error against the pair's error (default), 1 =
+ * the residual the correction leaves, |r + A d|^2 / |r|^2 (needs only the
+ * pair's residual; A is the instance's matrix). */
+int fvm_learned_set_objective(fvm_learned* l, int objective);
+/* In the solve the learned step is retired after three tries if fewer than
+ * a quarter cut the FP64 residual below f times its value (default 0.5,
+ * what pays for the step; 1 keeps any step that lowers it). */
+int fvm_learned_set_useful_factor(fvm_learned* l, double f);
+/* With the residual objective, the reduction sqrt(mean |r + A d|^2 /
+ * |r|^2) the network reached on its pairs at the last evaluation (-1 when
+ * not evaluated since training). A solve does not use a network whose
+ * reduction is above its useful factor. */
+int fvm_learned_residual_factor(const fvm_learned* l, double* factor);
 int fvm_learned_tensor_cores(const fvm_learned* l, int* on);
+/* Failure-path check of the tensor-core layers' bounded completion wait (no
+ * reference counterpart): one CTA allocates TMEM and waits `limit` tries on
+ * an mbarrier that nothing signals; *status = 1 when the wait ran out and
+ * the kernel set its error flag, released TMEM and returned (the layers'
+ * own path on a stuck MMA). The context stays usable. */
+int fvm_learned_wait_probe(unsigned limit, int* status);
 
 const char* fvm_last_error(void);
 

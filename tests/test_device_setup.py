@@ -4,8 +4,9 @@ SELL-32 packing as kernels.
 
 Bars:
   * aggregation: every fine row in exactly one aggregate, every coarse row
-    non-empty, aggregates of at most 16 rows, every level smaller than the
-    one above it;
+    non-empty, every level smaller than the one above it; aggregates of at
+    most 16 rows for one matching per level, 64 for pairs of pairs (rows
+    left unpaired join a pair, so a few aggregates grow past 2 or 4);
   * Galerkin: each coarse matrix equals P^T A P of the level above it
     (piecewise-constant P from the aggregation), computed here in numpy from
     the exported levels, to 1e-12 relative (the device sums in another
@@ -32,8 +33,9 @@ def _mesh(kind):
     return meshgen.config3(n=16, seed=3)
 
 
-def _amg(device=True, coarsest=100):
+def _amg(device=True, coarsest=100, passes=1):
     a = fvmbaseExt.AMG()
+    a.matchPasses = passes
     a.precision = fvmbaseExt.AMG.MIXED
     a.coarseSolver = fvmbaseExt.AMG.COARSE_DIRECT
     a.coarsestSize = coarsest
@@ -80,10 +82,11 @@ def _as_dict(A):
     return {(int(a), int(b)): float(v) for a, b, v in zip(rows, A["col"], A["val"])}
 
 
-@pytest.mark.parametrize("device", [True, False])
+@pytest.mark.parametrize("mode", ["device", "device-pairs-of-pairs", "host"])
 @pytest.mark.parametrize("kind", ["quad", "tet", "hex"])
-def test_hierarchy_partition_and_galerkin(kind, device):
-    _, _, _, _, tm, _, _ = _model(kind, _cg(_amg(device)))
+def test_hierarchy_partition_and_galerkin(kind, mode):
+    amg = _amg(mode != "host", passes=2 if mode == "device-pairs-of-pairs" else 1)
+    _, _, _, _, tm, _, _ = _model(kind, _cg(amg))
     sizes, cis = tm.getHierarchy()
     assert len(sizes) >= 2
     A = tm.getLevelMatrix(0)
@@ -94,7 +97,7 @@ def test_hierarchy_partition_and_galerkin(kind, device):
         assert ci.min() >= 0 and ci.max() < nc
         counts = np.bincount(ci, minlength=nc)
         assert counts.min() >= 1
-        assert counts.max() <= 16
+        assert counts.max() <= (64 if mode == "device-pairs-of-pairs" else 16)
         Ac = tm.getLevelMatrix(lvl + 1)
         cd, off = _galerkin(A, ci, nc)
         scale = np.abs(cd).max()
@@ -127,9 +130,12 @@ def test_device_hierarchy_is_deterministic():
 
 
 @pytest.mark.parametrize("kind", ["quad", "tet", "hex"])
-@pytest.mark.parametrize("variant", ["cg", "amg", "cg-large-coarsest"])
+@pytest.mark.parametrize("variant", ["cg", "amg", "cg-large-coarsest", "cg-pairs-of-pairs"])
 def test_device_hierarchy_converged_field_matches_reference(refo, kind, variant):
-    amg = _amg(coarsest=4096 if variant == "cg-large-coarsest" else 100)
+    amg = _amg(coarsest=4096 if variant == "cg-large-coarsest" else 100,
+               passes=2 if variant == "cg-pairs-of-pairs" else 1)
+    if variant == "cg-pairs-of-pairs":
+        amg.coarsePostSweeps = 1
     amg.relativeTolerance = 1e-10
     amg.nMaxIterations = 500
     solver = amg if variant == "amg" else _cg(amg)

@@ -191,7 +191,8 @@ void ThermalModel::setCellField(int field, const double* values, int count) {
     }
   }
   HostField& f = this->field(field);
-  std::copy(values, values + count, f.begin());
+  // large fields are copied by all host cores (one core moves ~5-10 GB/s)
+  parallel_chunks(count, [&](int b, int e) { std::copy(values + b, values + e, f.begin() + b); }, 1 << 20);
   uniform_[field] = false;
   if (count == n && field != kFieldTemperature) {
     // ghost cells take the value of their interior neighbour
@@ -239,7 +240,7 @@ void ThermalModel::getCellField(int field, double* out, int count) {
     return;
   }
   HostField& f = this->field(field);
-  std::copy(f.begin(), f.begin() + count, out);
+  parallel_chunks(count, [&](int b, int e) { std::copy(f.begin() + b, f.begin() + e, out + b); }, 1 << 20);
 }
 
 void ThermalModel::ensureDevice() {

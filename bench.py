@@ -217,6 +217,7 @@ def size_matched_copy_gbs(nbytes: float, reps: int = 7) -> float:
 
 
 HOST_SETUP = False  # --host-setup: the mixed path on the reference's host aggregation
+USE_GRAPHS = True   # --no-graphs: kernels launched one by one (for ncu launch lists)
 
 
 def solver_for(variant: str, inner_rel: float):
@@ -235,6 +236,7 @@ def solver_for(variant: str, inner_rel: float):
     amg.coarsestSize = 100
     amg.relativeTolerance = inner_rel
     amg.nMaxIterations = 200
+    amg.useGraphs = USE_GRAPHS
     if variant in ("mixed", "learned"):
         amg.setupOnDevice = not HOST_SETUP
         amg.precision = fvmbaseExt.AMG.MIXED
@@ -644,12 +646,16 @@ def main():
     ap.add_argument("--time-steps", type=int, default=50, help="config4: backward-Euler steps")
     ap.add_argument("--ref-time-steps", type=int, default=1,
                     help="config4: steps of the CPU reference sample")
+    ap.add_argument("--no-graphs", action="store_true",
+                    help="launch every kernel on its own instead of replaying CUDA graphs (ncu does not profile the "
+                         "kernels of a graph with conditional nodes, which the CG solves use)")
     ap.add_argument("--host-setup", action="store_true",
                     help="mixed path: AMG levels by the reference's greedy aggregation on the host instead of the "
                          "GPU-built hierarchy")
     args = ap.parse_args()
-    global HOST_SETUP
+    global HOST_SETUP, USE_GRAPHS
     HOST_SETUP = args.host_setup
+    USE_GRAPHS = not args.no_graphs
 
     dist = Dist()
     peaks, peak_kind = load_peaks()
@@ -785,7 +791,12 @@ def main():
                 "fp64_gs_pass": {"achieved": pp["gs_pass_bytes"] / (pp["gs_pass_ms"] * 1e-3) / 1e9,
                                  "frac": pp["gs_pass_bytes"] / (pp["gs_pass_ms"] * 1e-3) / 1e9 / peak},
                 "fp64_residual": {"achieved": pp["residual_bytes"] / (pp["residual_ms"] * 1e-3) / 1e9,
-                                  "frac": pp["residual_bytes"] / (pp["residual_ms"] * 1e-3) / 1e9 / peak}}
+                                  "frac": pp["residual_bytes"] / (pp["residual_ms"] * 1e-3) / 1e9 / peak},
+                "whole_cycle": {"bytes": pm["cycle_bytes"], "ms": pm["cycle_ms"],
+                                "achieved": pm["cycle_bytes"] / (pm["cycle_ms"] * 1e-3) / 1e9,
+                                "frac": pm["cycle_bytes"] / (pm["cycle_ms"] * 1e-3) / 1e9 / peak,
+                                "note": "algorithmic bytes of one FP32 cycle from a zero guess over its CUDA-event "
+                                        "time after an L2 flush (coarse levels L2-resident within the cycle)"}}
     try:
         copy_gbs = dist.max(size_matched_copy_gbs(pp["residual_bytes"])) if dist.world == 1 else None
     except Exception:  # context only
@@ -829,11 +840,13 @@ def main():
             "config": {
                 "workload": desc,
                 "cells": n_cells,
-                "solver": ("mixed+learned: CG (FP64) preconditioned by an FP32 AMG V(0,2) -- multicolour GS on the "
-                           "finest level, damped Jacobi (w=2/3) below, dense FP64 inverse on the coarsest level "
-                           "(<= 4096 rows) -- with the learned initial correction (kept only when it lowers the FP64 "
-                           "residual, retired when it does not pay); plain: standalone FP64 AMG V(1,1), multicolour "
-                           "GS on every level, coarsest <= 100 rows smoothed (the reference's default solver)"),
+                "solver": ("mixed+learned: flexible CG (FP64, fused iteration, each linear solve one CUDA graph) "
+                           "preconditioned by an FP32 AMG V(0,2) on a hierarchy built on the GPU (pairs of pairs) -- "
+                           "two multicolour GS sweeps on the finest level, one damped-Jacobi sweep (w=2/3) below, "
+                           "dense FP64 inverse (FP32 copy) on the coarsest level (<= 4096 rows) -- with the learned "
+                           "post-correction of each preconditioner application when its measured residual reduction "
+                           "pays; plain: standalone FP64 AMG V(1,1) on the reference's aggregation, multicolour GS on "
+                           "every level, coarsest <= 100 rows smoothed (the reference's default solver)"),
                 "outer_rel": 1e-10,
                 "inner_rel": args.inner_rel,
                 "l2": "working set > 126 MB L2 (kernel timings flush L2 with a 512 MB write)",

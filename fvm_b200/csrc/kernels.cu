@@ -1313,19 +1313,22 @@ __global__ void __launch_bounds__(256) k_gjd_first(int n, int nb, const double* 
   gjd_invert_block(n, 0, nb, R, Dout, status, D);
 }
 
-// Rp[t][j] = sum_u D[t][u] R[u][j]: the panel's new pivot rows
+// Rp[t][j] = sum_u D[t][u] R[u][j]: the panel's new pivot rows; four
+// threads per column, eight output rows each (grid ceil(4 n / 256))
 __global__ void __launch_bounds__(256) k_gjd_rows(int n, int nb, const double* __restrict__ R,
                                                   const double* __restrict__ Dinv, double* __restrict__ Rp) {
   __shared__ double D[kGdB][kGdB + 1];
   for (int e = threadIdx.x; e < kGdB * kGdB; e += blockDim.x) D[e / kGdB][e % kGdB] = Dinv[e];
   __syncthreads();
-  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = g >> 2, t0 = (g & 3) * 8;
   if (j >= n) return;
   double r[kGdB];
 #pragma unroll
   for (int u = 0; u < kGdB; u++) r[u] = u < nb ? R[(size_t)u * n + j] : 0.0;
-#pragma unroll 4
-  for (int t = 0; t < kGdB; t++) {
+#pragma unroll
+  for (int q = 0; q < 8; q++) {
+    const int t = t0 + q;
     double acc = 0.0;
 #pragma unroll
     for (int u = 0; u < kGdB; u++) acc = __fma_rn(D[t][u], r[u], acc);
@@ -1354,6 +1357,18 @@ __global__ void __launch_bounds__(256, 2) k_gjd_update(int n, int k0, int nb, do
   // does the tile meet the panel's rows / columns?
   const bool rowsK = i0 < k0 + nb && i0 + kGdT > k0;
   const bool colsK = j0 < k0 + nb && j0 + kGdT > k0;
+  // the tile's own entries are loaded first, so their latency overlaps the
+  // staging of the panel columns and pivot rows (they do not depend on it)
+  double acc[4][4];
+#pragma unroll
+  for (int a = 0; a < 4; a++) {
+    const int i = i0 + ty + 16 * a;
+#pragma unroll
+    for (int b = 0; b < 4; b++) {
+      const int j = j0 + tx + 16 * b;
+      acc[a][b] = (i < n && j < n) ? A[(size_t)i * n + j] : 0.0;
+    }
+  }
   for (int e = tid; e < kGdT * kGdB; e += 256) {
     const int r = e / kGdB, t = e % kGdB;
     Cs[r][t] = i0 + r < n ? C[(size_t)(i0 + r) * kGdB + t] : 0.0;
@@ -1365,16 +1380,6 @@ __global__ void __launch_bounds__(256, 2) k_gjd_update(int n, int k0, int nb, do
   if (colsK || rowsK)
     for (int e = tid; e < kGdB * kGdB; e += 256) Ds[e / kGdB][e % kGdB] = Dinv[e];
   __syncthreads();
-  double acc[4][4];
-#pragma unroll
-  for (int a = 0; a < 4; a++) {
-    const int i = i0 + ty + 16 * a;
-#pragma unroll
-    for (int b = 0; b < 4; b++) {
-      const int j = j0 + tx + 16 * b;
-      acc[a][b] = (i < n && j < n) ? A[(size_t)i * n + j] : 0.0;
-    }
-  }
 #pragma unroll 4
   for (int t = 0; t < kGdB; t++) {
     double c[4], r[4];
@@ -1514,7 +1519,7 @@ void gauss_jordan_inverse_dominant(int n, double* a, void* scratch, cudaStream_t
     const int nb = n - k0 < kGdB ? n - k0 : kGdB;
     const int k1 = k0 + nb;
     const int nb1 = n - k1 < kGdB ? n - k1 : kGdB;
-    k_gjd_rows<<<ceil_div(n, kBlock), kBlock, 0, st>>>(n, nb, R[cur], Dv[cur], Rp);
+    k_gjd_rows<<<ceil_div(4LL * n, kBlock), kBlock, 0, st>>>(n, nb, R[cur], Dv[cur], Rp);
     k_gjd_update<<<grid, 256, 0, st>>>(n, k0, nb, a, C[cur], Rp, Dv[cur], C[cur ^ 1], R[cur ^ 1], Dv[cur ^ 1], k1,
                                        nb1 > 0 ? nb1 : 0, ticket, status);
     cur ^= 1;

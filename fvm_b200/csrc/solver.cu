@@ -665,26 +665,34 @@ double AmgHierarchy::fineSweepBytes() const {
   return d.n * (4.0 * vb) + d.entries * (4.0 + vb);
 }
 
+// Algorithmic bytes of one cycle from a zero guess (the preconditioner's
+// use; the FP64 standalone iteration adds a residual pass on level 0), in
+// the configured precision, following AmgHierarchy::cycle: per level its
+// smoothing passes, the restriction (of b alone from a zero guess without
+// pre-smoothing) and the prolongation; the coarsest level's dense solve.
 double AmgHierarchy::cycleBytes() const {
   const double vb = opt_.precision == kMixed ? 4.0 : 8.0;
   double total = 0;
   const int L = (int)lv_.size();
-  const int passesPerSweep = opt_.smootherType == kGaussSeidel ? 2 : 2;
   for (int l = 0; l < L; l++) {
     const DevLevel& d = lv_[l];
     const double pass = d.n * (4.0 * vb) + d.entries * (4.0 + vb);
-    const int sweeps = opt_.nPreSweeps + opt_.postSweeps(l);
     if (l == L - 1 && coarseInv_) {
-      total += (double)d.n * d.n * 8.0;
+      total += (double)d.n * d.n * (opt_.precision == kMixed && coarseInvF_ ? 4.0 : 8.0) + 2.0 * vb * d.n;
       continue;
     }
-    total += sweeps * passesPerSweep * pass;
+    // a sweep: two damped-Jacobi passes, or forward + reverse over the
+    // colours (2C - 1 colour passes, C of which make one pass)
+    const bool gsPasses = opt_.smootherType == kGaussSeidel && !dampedLevel(l, d.n) && d.nColors > 0;
+    const double perSweep = gsPasses ? (2.0 * d.nColors - 1.0) / d.nColors : 2.0;
+    total += (opt_.nPreSweeps + opt_.postSweeps(l)) * perSweep * pass;
     if (l + 1 < L) {
       const DevLevel& c = lv_[l + 1];
-      // fused residual+restriction reads the matrix once, writes coarse b
-      total += d.n * (3.0 * vb + 8.0) + d.entries * (4.0 + vb) + c.n * (vb + 4.0);
-      // zero coarse x, prolongation
-      total += c.n * vb + d.n * (2.0 * vb + 4.0);
+      if (opt_.nPreSweeps == 0)
+        total += (vb + 4.0) * d.n + (4.0 + vb) * c.n;  // b restricted; x assigned below
+      else
+        total += 3.0 * vb * d.n + (4.0 + vb) * d.entries + (4.0 + 2.0 * vb) * c.n;
+      total += (2.0 * vb + 4.0) * d.n + vb * c.n;
     }
   }
   return total;

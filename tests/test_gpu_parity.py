@@ -542,7 +542,7 @@ def test_gpu_inverse_direct_single_level(n):
 @pytest.mark.parametrize("n", [1000, 2294, 3000, 4096])
 def test_gpu_inverse_dominant_single_level(n):
     """A diagonally dominant single level (the shape of every diffusion
-    coarsest level) takes the unpivoted blocked Gauss-Jordan: panels of 16
+    coarsest level) takes the unpivoted blocked Gauss-Jordan: panels of 32
     pivots, the last one partial for all sizes here but 4096. One cycle is an
     exact solve; the solution is compared with numpy's dense solve."""
     rng = np.random.default_rng(7 * n)

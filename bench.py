@@ -37,6 +37,14 @@ METRIC = "time to 1e-10 rel. residual: mixed+learned vs plain FP64 AMG, same B20
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0}
 
 
+
+def plan_name(p):
+    """A level's smoother launch plan: "tpr/block" on SELL-32 levels, "ellW"
+    (and "x2" with two rows per thread) on ELL-32 levels."""
+    if p[0] < 0:
+        return "ell%d" % -p[0] + ("x%d" % -p[1] if p[1] < -1 else "")
+    return "%d/%d" % p
+
 def load_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -459,7 +467,7 @@ def bench_batch(args, dist, peaks, peak_kind):
                            "all_meshes_converged": v["all_converged"], "max_mesh_ratio": v["max_ratio"]}
                        for k, v in results.items()},
             "gpu_launches": int(mixed["launches"]) * args.steps,
-            "launch_plans": {v: ["%d/%d" % p if p[1] else "ell%d" % -p[0] for p in r["plans"]]
+            "launch_plans": {v: [plan_name(p) for p in r["plans"]]
                              for v, r in results.items()},
             "roofline": roofline,
             "cpu_baseline": cpu,
@@ -566,6 +574,137 @@ def bench_transient(args, dist, peaks, peak_kind):
     print(json.dumps(line))
 
 
+def bench_learned_protocol(args, dist, peaks, peak_kind):
+    """Config 3's learned-correction protocol: 100^3 hexes, two-phase
+    conductivity (k = 1e4 in random spheres of radius 0.02-0.08 filling 30 %
+    of the volume, 1 outside), source U[0,1]. The network is trained on the
+    GPU on (residual, error) pairs harvested from plain FP64 AMG runs of
+    `--train-instances` seeded instances (seeds 1000, 1001, ...), with the
+    residual objective, then evaluated on `--held-out` other seeds (5000,
+    5001, ...) against plain FP64 AMG and against the mixed method without
+    it. All instances share the mesh; each draws its own spheres and source.
+    Arms per held-out seed, each one full solve to outer 1e-10: plain (the
+    reference's default solver on the GPU), mixed (CG + FP32 V-cycle),
+    mixed+learned as the product runs it (the network is used only when its
+    measured residual reduction pays for its cost), and mixed+learned with
+    the network forced on (every step that lowers the residual is kept),
+    which shows what the network itself gains or costs."""
+    from fvm_b200 import meshgen
+    from fvm_b200.learned import LearnedCorrection
+
+    mesh = meshgen.hex_mesh(100)
+    n = mesh["nCells"]
+    pts = meshgen.cell_centers(mesh)
+    bc = {1: ("T", 300.0), 2: ("T", 400.0)}
+
+    def draw(seed):
+        return meshgen.sphere_inclusions(pts, seed + 100), meshgen.uniform_field(n, 0.0, 1.0, seed + 200)
+
+    def set_fields(s, k, src):
+        s.k, s.s = np.ascontiguousarray(k), np.ascontiguousarray(src)
+
+    t0 = time.perf_counter()
+    k0, s0 = draw(1000)
+    lc = LearnedCorrection(seed=0)
+    lc.setObjective(LearnedCorrection.RESIDUAL)
+    harvester = Solve(mesh, {"k": k0, "s": s0, "bc": bc}, "plain", args.inner_rel)
+    cells = harvester.m.getCells()
+    per_solve = max(1, args.pairs_per_instance // 2)
+    for i in range(args.train_instances):
+        k, src = draw(1000 + i) if i else (k0, s0)
+        set_fields(harvester, k, src)
+        harvester.tm.init()
+        harvester.tf.conductivity[cells] = harvester.k
+        harvester.tf.source[cells] = harvester.s
+        lc.harvest(harvester.tm, nOuter=2, perSolve=per_solve, relativeTolerance=1e-8, maxCycles=100)
+    del harvester
+    harvest_s = time.perf_counter() - t0
+    before = lc.evaluate()
+    t1 = time.perf_counter()
+    losses = lc.train(steps=args.train_steps, lr=1e-3, seed=0)
+    train_s = time.perf_counter() - t1
+    after = lc.evaluate()
+    factor = lc.residualFactor()
+    forced = LearnedCorrection(seed=0)
+    forced.setParams(lc.getParams())
+    forced.setUsefulFactor(1.0)
+
+    arms = {"plain": Solve(mesh, {"k": k0, "s": s0, "bc": bc}, "plain", args.inner_rel),
+            "mixed": Solve(mesh, {"k": k0, "s": s0, "bc": bc}, "mixed", args.inner_rel),
+            "mixed_learned": Solve(mesh, {"k": k0, "s": s0, "bc": bc}, "learned", args.inner_rel),
+            "mixed_learned_forced": Solve(mesh, {"k": k0, "s": s0, "bc": bc}, "learned", args.inner_rel)}
+    arms["mixed_learned"].tm.setLearnedCorrection(lc)
+    arms["mixed_learned_forced"].tm.setLearnedCorrection(forced)
+    # warm-up on a training instance (setup caches, launch plans)
+    for a in arms.values():
+        if a is not arms["plain"]:
+            a.step()
+    res = {k: {"dev_s": [], "cycles": [], "outer": [], "learned_tried": 0, "learned_kept": 0} for k in arms}
+    err = {k: [] for k in arms if k != "plain"}
+    dist.barrier()
+    sampler = ClockSampler(dist.local)
+    if sampler:
+        sampler.__enter__()
+    for j in range(args.held_out):
+        k, src = draw(5000 + j)
+        T = {}
+        for name, a in arms.items():
+            set_fields(a, k, src)
+            d, w, rep, Tn, _, _ = a.step()
+            if not rep.converged:
+                raise RuntimeError("%s: held-out seed %d did not converge" % (name, 5000 + j))
+            r = res[name]
+            r["dev_s"].append(d)
+            r["cycles"].append(rep.linearIterations)
+            r["outer"].append(rep.iterations)
+            r["learned_tried"] += rep.learnedSteps
+            r["learned_kept"] += rep.learnedAccepted
+            T[name] = Tn[:n]
+        for name in err:
+            err[name].append(float(np.linalg.norm(T[name] - T["plain"]) / np.linalg.norm(T["plain"])))
+    if sampler:
+        sampler.__exit__()
+    dist.barrier()
+    if dist.rank != 0:
+        return
+
+    def mean(v):
+        return float(np.mean(v))
+
+    summary = {k: {"mean_dev_s": mean(r["dev_s"]), "mean_cycles": mean(r["cycles"]), "mean_outer": mean(r["outer"]),
+                   "dev_s": r["dev_s"], "cycles": r["cycles"], "learned_tried": r["learned_tried"],
+                   "learned_kept": r["learned_kept"]} for k, r in res.items()}
+    head = summary["mixed_learned"]
+    line = {
+        "metric": METRIC, "value": head["mean_dev_s"], "unit": "s", "n_gpus": args.gpus, "steps": args.held_out,
+        "warmup": 1, "ms_per_step": head["mean_dev_s"] * 1e3, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 V-cycle / f64 refinement", "data": "synthetic",
+        "config": {"workload": "config3 learned protocol: steady 3D heat conduction, 100^3 hexes, two-phase k = 1e4 "
+                               "in random spheres (r 0.02-0.08, 30% volume), 1 outside",
+                   "cells": n, "train_instances": args.train_instances,
+                   "pairs_per_instance": 2 * per_solve, "held_out_seeds": args.held_out, "outer_rel": 1e-10,
+                   "inner_rel": args.inner_rel,
+                   "value": "mean device time of advance() over the held-out seeds, mixed + learned as the product "
+                            "runs it",
+                   "subsample": "the stated protocol is 200 instances, 20k pairs and 50 held-out seeds; 20k pairs of "
+                                "1M-cell FP64 residual/error vectors are 320 GB, more than the GPU holds, so the pairs "
+                                "and seeds here are a stated subsample"},
+        "plain_fp64_s": summary["plain"]["mean_dev_s"], "mixed_without_learned_s": summary["mixed"]["mean_dev_s"],
+        "speedup_vs_plain_fp64": summary["plain"]["mean_dev_s"] / head["mean_dev_s"],
+        "forced_learned_vs_mixed": summary["mixed_learned_forced"]["mean_dev_s"] / summary["mixed"]["mean_dev_s"],
+        "arms": summary,
+        "field_rel_l2_vs_plain": {k: max(v) for k, v in err.items()},
+        "learned_training": {"objective": "residual |r + A d|^2 / |r|^2", "pairs": lc.numPairs(),
+                             "instances": args.train_instances, "train_steps": args.train_steps,
+                             "loss_before": before, "loss_after": after, "residual_factor": factor,
+                             "useful_factor": 0.5, "used_in_solve": bool(0 <= factor <= 0.5),
+                             "loss_first50": mean(losses[:50]), "loss_last50": mean(losses[-50:]),
+                             "harvest_seconds": harvest_s, "train_seconds": train_s},
+        "clocks": sampler.summary() if sampler else None,
+    }
+    print(json.dumps(line))
+
+
 def cpu_reference_transient(mesh, fields, inner_rel, n_steps):
     """The compiled reference (one thread) on the first n_steps backward-Euler
     steps of the same 8M-cell problem, each to outer 1e-10: a bounded sample
@@ -646,6 +785,12 @@ def main():
     ap.add_argument("--time-steps", type=int, default=50, help="config4: backward-Euler steps")
     ap.add_argument("--ref-time-steps", type=int, default=1,
                     help="config4: steps of the CPU reference sample")
+    ap.add_argument("--learned-protocol", action="store_true",
+                    help="config3: train the learned correction on --train-instances seeded instances and evaluate "
+                         "it on --held-out other seeds")
+    ap.add_argument("--train-instances", type=int, default=100)
+    ap.add_argument("--pairs-per-instance", type=int, default=10)
+    ap.add_argument("--held-out", type=int, default=10)
     ap.add_argument("--no-graphs", action="store_true",
                     help="launch every kernel on its own instead of replaying CUDA graphs (ncu does not profile the "
                          "kernels of a graph with conditional nodes, which the CG solves use)")
@@ -665,6 +810,10 @@ def main():
         return
     if args.workload == "config4" and args.impl == "product":
         bench_transient(args, dist, peaks, peak_kind)
+        dist.close()
+        return
+    if args.workload == "config3" and args.learned_protocol and args.impl == "product":
+        bench_learned_protocol(args, dist, peaks, peak_kind)
         dist.close()
         return
     if args.workload == "config2":
@@ -796,7 +945,11 @@ def main():
                                 "achieved": pm["cycle_bytes"] / (pm["cycle_ms"] * 1e-3) / 1e9,
                                 "frac": pm["cycle_bytes"] / (pm["cycle_ms"] * 1e-3) / 1e9 / peak,
                                 "note": "algorithmic bytes of one FP32 cycle from a zero guess over its CUDA-event "
-                                        "time after an L2 flush (coarse levels L2-resident within the cycle)"}}
+                                        "time after an L2 flush (coarse levels L2-resident within the cycle)"},
+                "face_flux": {"bytes": pm["face_flux_bytes"], "ms": pm["face_flux_ms"],
+                              "achieved": pm["face_flux_bytes"] / (pm["face_flux_ms"] * 1e-3) / 1e9,
+                              "frac": pm["face_flux_bytes"] / (pm["face_flux_ms"] * 1e-3) / 1e9 / peak,
+                              "note": "face loop of the linearization (k_face_flux), once per outer iteration"}}
     try:
         copy_gbs = dist.max(size_matched_copy_gbs(pp["residual_bytes"])) if dist.world == 1 else None
     except Exception:  # context only
@@ -865,7 +1018,7 @@ def main():
             "learned_training": learned_info,
             "levels": int(pm["levels"]),
             "kernels_per_cycle": int(pm["kernels_per_cycle"]),
-            "launch_plans": {v: ["%d/%d" % p if p[1] else "ell%d" % -p[0] for p in r["plans"]]
+            "launch_plans": {v: [plan_name(p) for p in r["plans"]]
                              for v, r in results.items()},
             "kernel_timings": {
                 v: {"gs_pass_ms": r["profile"]["gs_pass_ms"],

@@ -49,6 +49,9 @@ class LinearOptions(ctypes.Structure):
         ("matchBeta", ctypes.c_double),
         ("matchPasses", ctypes.c_int),
         ("coarsePostSweeps", ctypes.c_int),
+        ("planEllRows", ctypes.c_int),
+        ("chebyshevDegree", ctypes.c_int),
+        ("chebyshevFraction", ctypes.c_double),
     ]
 
 

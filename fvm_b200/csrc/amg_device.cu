@@ -830,6 +830,7 @@ void AmgHierarchy::buildDevice(const FinestDevice& in, const SolverOptions& opt)
     lap("coarsest inverse");
   }
   CUDA_OK(cudaStreamSynchronize(st));
+  prepareChebyshev();
   tunePlans();
   lap("launch plans");
   if (trace) {

@@ -101,6 +101,14 @@ SolverOptions to_solver(const fvm_linear_options& o) {
   s.autotune = o.autotune != 0;
   s.planTpr = o.planThreadsPerRow;
   s.planBlock = o.planBlock;
+  FVM_REQUIRE(o.planEllRows >= 0 && o.planEllRows <= 2, kBadArgument, "planEllRows must be 0, 1 or 2");
+  s.planEllRows = o.planEllRows;
+  FVM_REQUIRE(o.chebyshevDegree >= 0 && o.chebyshevDegree <= 16, kBadArgument,
+              "chebyshevDegree must be in [0, 16]");
+  FVM_REQUIRE(o.chebyshevFraction > 0.0 && o.chebyshevFraction < 1.0, kBadArgument,
+              "chebyshevFraction must be in (0, 1)");
+  s.chebyshevDegree = o.chebyshevDegree;
+  s.chebyshevFraction = o.chebyshevFraction;
   FVM_REQUIRE(o.matchRounds >= 1 && o.matchRounds <= 64, kBadArgument, "matchRounds must be in [1, 64]");
   FVM_REQUIRE(o.matchBeta >= 0.0 && o.matchBeta <= 1.0, kBadArgument, "matchBeta must be in [0, 1]");
   s.setupOnDevice = o.setupOnDevice != 0;
@@ -144,6 +152,9 @@ void from_solver(const SolverOptions& s, fvm_linear_options& o) {
   o.matchBeta = s.matchBeta;
   o.matchPasses = s.matchPasses;
   o.coarsePostSweeps = s.coarsePostSweeps;
+  o.planEllRows = s.planEllRows;
+  o.chebyshevDegree = s.chebyshevDegree;
+  o.chebyshevFraction = s.chebyshevFraction;
 }
 
 RefLevel level_from_csr(int n, const int* row, const int* col, const double* diag, const double* off) {
@@ -570,7 +581,7 @@ int fvm_thermal_launch_plans(fvm_thermal* h, int* nLevels, int* threadsPerRow, i
     for (int l = 0; l < hier.numLevels() && l < cap; l++) {
       const DevLevel& d = hier.level(l);
       if (threadsPerRow) threadsPerRow[l] = d.ellWidth ? -d.ellWidth : d.plan.tpr;
-      if (block) block[l] = d.ellWidth ? 0 : d.plan.block;
+      if (block) block[l] = d.ellWidth ? -d.plan.ellRows : d.plan.block;
     }
   });
 }

@@ -187,6 +187,45 @@ __global__ void __launch_bounds__(kBlock, 8) k_jacobi_damped(SellView<T> a, int 
   }
 }
 
+// One step of a Chebyshev polynomial smoother on D^-1 A: with the row's
+// residual res = b + A x, dv = c1 dv + c2 (-res / a_ii) (First: dv is
+// written, not read) and xnew = x + dv. dv is indexed by row only, so it
+// is updated in place; x and xnew are distinct.
+template <class T, bool First>
+__global__ void __launch_bounds__(kBlock, 8) k_cheb(SellView<T> a, int nSlices, const T* __restrict__ x, T* xnew,
+                                                    T* dv, const T* __restrict__ b, T c1, T c2) {
+  FVM_PDL();
+  const int lane = threadIdx.x & 31;
+  for (int s = blockIdx.x * kSlicesPerBlock + (threadIdx.x >> 5); s < nSlices; s += gridDim.x * kSlicesPerBlock) {
+    const int4 m = slice_meta(a, s);
+    if (lane >= m.y) continue;
+    const int i = m.x + lane;
+    const T xi = x[i];
+    const T res = row_sum(a, m, lane, x, b[i] + a.diag[i] * xi);
+    const T z = -res / a.diag[i];
+    const T d = First ? c2 * z : c1 * dv[i] + c2 * z;
+    dv[i] = d;
+    xnew[i] = xi + d;
+  }
+}
+
+// Gershgorin bound of the spectrum of D^-1 A: max over rows of
+// 1 + sum_j |a_ij / a_ii|, by atomicMax on the bits of a non-negative double
+__global__ void __launch_bounds__(kBlock) k_gershgorin(SellView<double> a, int nSlices, unsigned long long* out) {
+  const int lane = threadIdx.x & 31;
+  double best = 0.0;
+  for (int s = blockIdx.x * kSlicesPerBlock + (threadIdx.x >> 5); s < nSlices; s += gridDim.x * kSlicesPerBlock) {
+    const int4 m = slice_meta(a, s);
+    if (lane >= m.y) continue;
+    const int i = m.x + lane;
+    double sum = 0.0;
+    for (int k = 0; k < m.w; k++) sum += fabs(a.vals[m.z + (k << 5) + lane]);
+    best = fmax(best, 1.0 + sum / fabs(a.diag[i]));
+  }
+  for (int o = 16; o > 0; o >>= 1) best = fmax(best, __shfl_xor_sync(0xffffffffu, best, o));
+  if (lane == 0 && best > 0.0) atomicMax(out, (unsigned long long)__double_as_longlong(best));
+}
+
 template <class T>
 __global__ void __launch_bounds__(kBlock, 8) k_residual(SellView<T> a, int nSlices, const T* __restrict__ x,
                            const T* __restrict__ b, T* r, double* partials) {
@@ -267,6 +306,26 @@ __global__ void __launch_bounds__(kBlock, 8) k_gs_color_ell(SellView<T> a, int r
   x[i] = -sum / a.diag[i];
 }
 
+// The same pass with two rows per thread (32-row groups g and g + 8 of a
+// block's 16): both rows' loads are issued before either row is written, so
+// a thread keeps twice the loads in flight and a colour of a few hundred
+// thousand rows fits in one wave. Rows of one colour never read each other,
+// so the result is bitwise that of k_gs_color_ell.
+template <class T, int W>
+__global__ void __launch_bounds__(kBlock, 4) k_gs_color_ell2(SellView<T> a, int r0, int r1, T* x,
+                                                             const T* __restrict__ b) {
+  FVM_PDL();
+  const int g0 = (r0 >> 5) + blockIdx.x * (2 * kSlicesPerBlock) + (threadIdx.x >> 5);
+  const int i0 = (g0 << 5) + (threadIdx.x & 31);
+  const int i1 = i0 + (kSlicesPerBlock << 5);
+  const bool v0 = i0 >= r0 && i0 < r1, v1 = i1 >= r0 && i1 < r1;
+  T s0 = T(0), s1 = T(0);
+  if (v0) s0 = ell_row<T, W>(a, i0, x, b[i0]);
+  if (v1) s1 = ell_row<T, W>(a, i1, x, b[i1]);
+  if (v0) x[i0] = -s0 / a.diag[i0];
+  if (v1) x[i1] = -s1 / a.diag[i1];
+}
+
 template <class T, int W>
 __global__ void __launch_bounds__(kBlock, 8) k_jacobi_ell(SellView<T> a, const T* __restrict__ xold, T* xnew,
                                                           const T* __restrict__ b) {
@@ -286,6 +345,20 @@ __global__ void __launch_bounds__(kBlock, 8) k_jacobi_damped_ell(SellView<T> a, 
   const T sum = ell_row<T, W>(a, i, xold, b[i]);
   const T xo = xold[i];
   xnew[i] = xo + w * (-sum / a.diag[i] - xo);
+}
+
+template <class T, int W, bool First>
+__global__ void __launch_bounds__(kBlock, 8) k_cheb_ell(SellView<T> a, const T* __restrict__ x, T* xnew, T* dv,
+                                                        const T* __restrict__ b, T c1, T c2) {
+  FVM_PDL();
+  const int i = blockIdx.x * kBlock + threadIdx.x;
+  if (i >= a.n) return;
+  const T xi = x[i];
+  const T res = ell_row<T, W>(a, i, x, b[i] + a.diag[i] * xi);
+  const T z = -res / a.diag[i];
+  const T d = First ? c2 * z : c1 * dv[i] + c2 * z;
+  dv[i] = d;
+  xnew[i] = xi + d;
 }
 
 // residual with one L1 partial per block (256 rows)
@@ -864,7 +937,9 @@ __global__ void k_face_coefficients(FaceGeom g, const double* __restrict__ k, do
   const double am = g.faceAreaMag[f];
   const double dm = am * am / (A[0] * ds[0] + A[1] * ds[1] + A[2] * ds[2]);
   coeff[f] = kf * dm;
-  for (int d = 0; d < 3; d++) secCoeff[3 * f + d] = kf * (A[d] - ds[d] * dm);
+  // one 32-byte record per face (the fourth entry pads)
+  reinterpret_cast<double4*>(secCoeff)[f] =
+      make_double4(kf * (A[0] - ds[0] * dm), kf * (A[1] - ds[1] * dm), kf * (A[2] - ds[2] * dm), 0.0);
 }
 
 __global__ void k_gradient(int nCells, const int* __restrict__ row, const int* __restrict__ col,
@@ -880,9 +955,8 @@ __global__ void k_gradient(int nCells, const int* __restrict__ row, const int* _
     g1 += w[3 * k + 1] * dx;
     g2 += w[3 * k + 2] * dx;
   }
-  grad[3 * i] = g0;
-  grad[3 * i + 1] = g1;
-  grad[3 * i + 2] = g2;
+  // one 32-byte record per cell (the fourth entry pads)
+  reinterpret_cast<double4*>(grad)[i] = make_double4(g0, g1, g2, 0.0);
 }
 
 __global__ void k_ghost_gradient(int nB, const int* __restrict__ bFaces, const int* __restrict__ fc,
@@ -892,7 +966,8 @@ __global__ void k_ghost_gradient(int nB, const int* __restrict__ bFaces, const i
   if (t >= nB) return;
   const int f = bFaces[t];
   const int c0 = fc[2 * f], c1 = fc[2 * f + 1];
-  for (int d = 0; d < 3; d++) grad[3 * c1 + d] = grad[3 * c0 + d];
+  double4* g4 = reinterpret_cast<double4*>(grad);
+  g4[c1] = g4[c0];
 }
 
 __global__ void k_face_flux(FaceGeom g, const double* __restrict__ coeff,
@@ -901,14 +976,19 @@ __global__ void k_face_flux(FaceGeom g, const double* __restrict__ coeff,
   FVM_PDL();
   const int f = blockIdx.x * blockDim.x + threadIdx.x;
   if (f >= g.nFaces) return;
-  const int c0 = g.faceCells[2 * f], c1 = g.faceCells[2 * f + 1];
+  // faceCells as one 8-byte load, the two gradients and the secondary
+  // coefficient as 32-byte records (vector loads); same arithmetic order
+  const int2 cc = reinterpret_cast<const int2*>(g.faceCells)[f];
+  const int c0 = cc.x, c1 = cc.y;
   const double vol0 = g.cellVolume[c0], vol1 = g.cellVolume[c1];
+  const double4 ga = reinterpret_cast<const double4*>(grad)[c0];
+  const double4 gb = reinterpret_cast<const double4*>(grad)[c1];
+  const double4 sc = reinterpret_cast<const double4*>(sec)[f];
   const double vs = vol0 + vol1;
   double s = 0.0;
-  for (int d = 0; d < 3; d++) {
-    const double gF = (grad[3 * c0 + d] * vol0 + grad[3 * c1 + d] * vol1) / vs;
-    s += gF * sec[3 * f + d];
-  }
+  s += ((ga.x * vol0 + gb.x * vol1) / vs) * sc.x;
+  s += ((ga.y * vol0 + gb.y * vol1) / vs) * sc.y;
+  s += ((ga.z * vol0 + gb.z * vol1) / vs) * sc.z;
   flux[f] = coeff[f] * (x[c1] - x[c0]) + s;
 }
 
@@ -1103,6 +1183,11 @@ void gs_color(const SellView<T>& a, int s0, int s1, T* x, const T* b, cudaStream
   // ELL-32: s0, s1 are rows; the launch covers the 32-row groups they touch
   const int groups = a.ellWidth ? ((s1 - 1) >> 5) - (s0 >> 5) + 1 : s1 - s0;
   const int g = ceil_div(groups, kSlicesPerBlock);
+  if (a.ellWidth && plan.ellRows == 2) {
+#define FVM_L(W) pdl_launch(k_gs_color_ell2<T, W>, ceil_div(groups, 2 * kSlicesPerBlock), kBlock, st, a, s0, s1, x, b)
+    if (FVM_ELL_SWITCH(a.ellWidth, FVM_L)) return;
+#undef FVM_L
+  }
 #define FVM_L(W) pdl_launch(k_gs_color_ell<T, W>, g, kBlock, st, a, s0, s1, x, b)
   if (a.ellWidth && FVM_ELL_SWITCH(a.ellWidth, FVM_L)) return;
 #undef FVM_L
@@ -1140,6 +1225,27 @@ void jacobi_damped(const SellView<T>& a, int nSlices, const T* xold, T* xnew, co
   }
   pdl_launch(k_jacobi_damped<T>, reduce_blocks(nSlices), kBlock, st, a, nSlices, xold, xnew, b, w);
 }
+template <class T>
+void chebyshev_step(const SellView<T>& a, int nSlices, const T* x, T* xnew, T* dv, const T* b, T c1, T c2,
+                    bool first, cudaStream_t st) {
+  if (a.ellWidth) {
+#define FVM_L(W)                                                                                          \
+  (first ? pdl_launch(k_cheb_ell<T, W, true>, ceil_div(a.n, kBlock), kBlock, st, a, x, xnew, dv, b, c1, c2) \
+         : pdl_launch(k_cheb_ell<T, W, false>, ceil_div(a.n, kBlock), kBlock, st, a, x, xnew, dv, b, c1, c2))
+    if (FVM_ELL_SWITCH(a.ellWidth, FVM_L)) return;
+#undef FVM_L
+  }
+  if (first)
+    pdl_launch(k_cheb<T, true>, reduce_blocks(nSlices), kBlock, st, a, nSlices, x, xnew, dv, b, c1, c2);
+  else
+    pdl_launch(k_cheb<T, false>, reduce_blocks(nSlices), kBlock, st, a, nSlices, x, xnew, dv, b, c1, c2);
+}
+
+void gershgorin_bound(const SellView<double>& a, int nSlices, double* out, cudaStream_t st) {
+  cudaMemsetAsync(out, 0, sizeof(double), st);
+  k_gershgorin<<<reduce_blocks(nSlices), kBlock, 0, st>>>(a, nSlices, reinterpret_cast<unsigned long long*>(out));
+}
+
 template <class T>
 void residual(const SellView<T>& a, int nSlices, const T* x, const T* b, T* r, double* partials,
               cudaStream_t st) {
@@ -1248,27 +1354,41 @@ size_t gj_align(size_t b) { return (b + 255) & ~size_t(255); }
 // is two kernels over the matrix: k_gjd_rows forms the panel's new pivot
 // rows Rp = D^-1 A[K][:] once, then k_gjd_update sweeps 64 x 64 tiles,
 // each thread 4 x 4 entries, with the tile's 64 x 32 panel columns and
-// 32 x 64 pivot rows staged in shared memory (16 fused multiply-adds per 8
-// shared loads). The panel's old rows and columns are read from side
+// 32 x 64 pivot rows staged in shared memory by asynchronous copies
+// (cp.async, issued after the tile's own loads, so the latencies of both
+// overlap and no register holds a staged value; 16 fused multiply-adds per
+// 8 shared loads). The panel's old rows and columns are read from side
 // buffers (R, C) that the previous panel's update filled while writing
 // them, so no CTA reads a value another CTA of the same launch writes;
 // D^-1 comes ready-made: the last CTA of the previous launch to finish (a
 // fence and a ticket counter, no waiting) inverts the next panel's block.
-// Diagonal dominance keeps every pivot away from zero and the growth
-// bounded, which is why the caller takes this path only for diagonally
-// dominant levels. This is not a reference computation, so the products use
-// fused multiply-adds (__fma_rn) although the file is built without
-// contraction.
+// Side buffers use padded strides: rows of R and Rp hold ld = n rounded up
+// to 64 doubles, C holds ld rows of 32, and their padding stays zero (the
+// buffers are cleared once), so every staged copy is 16-byte aligned and in
+// bounds. Diagonal dominance keeps every pivot away from zero and the
+// growth bounded, which is why the caller takes this path only for
+// diagonally dominant levels. This is not a reference computation, so the
+// products use fused multiply-adds (__fma_rn) although the file is built
+// without contraction.
 constexpr int kGdB = 32;   // panel width
 constexpr int kGdT = 64;   // tile rows / columns
+constexpr int kGdPad = 2;  // shared row padding (keeps 16-byte row alignment)
+
+int gjd_ld(int n) { return (n + kGdT - 1) / kGdT * kGdT; }
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
 // D: shared memory of 2 x kGdB x (kGdB + 1) doubles (double-buffered block)
-__device__ void gjd_invert_block(int n, int k0, int nb, const double* R, double* Dout, int* status,
+__device__ void gjd_invert_block(int ld, int k0, int nb, const double* R, double* Dout, int* status,
                                  double (*D)[kGdB][kGdB + 1]) {
   const int tid = threadIdx.x, nt = blockDim.x;
   for (int e = tid; e < kGdB * kGdB; e += nt) {
     const int r = e / kGdB, c = e % kGdB;
-    D[0][r][c] = (r < nb && c < nb) ? __ldcg(R + (size_t)r * n + k0 + c) : (r == c ? 1.0 : 0.0);
+    D[0][r][c] = (r < nb && c < nb) ? __ldcg(R + (size_t)r * ld + k0 + c) : (r == c ? 1.0 : 0.0);
   }
   __syncthreads();
   int cur = 0;
@@ -1296,43 +1416,46 @@ __device__ void gjd_invert_block(int n, int k0, int nb, const double* R, double*
   for (int e = tid; e < kGdB * kGdB; e += nt) Dout[e] = D[cur][e / kGdB][e % kGdB];
 }
 
-// C[i * kGdB + t] = A[i][k0 + t], R[t * n + j] = A[k0 + t][j] (t < nb; 0 beyond)
-__global__ void k_gjd_extract(int n, int k0, int nb, const double* __restrict__ A, double* __restrict__ C,
+// C[i * kGdB + t] = A[i][k0 + t], R[t * ld + j] = A[k0 + t][j] (t < nb; 0 beyond)
+__global__ void k_gjd_extract(int n, int ld, int k0, int nb, const double* __restrict__ A, double* __restrict__ C,
                               double* __restrict__ R) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= n) return;
   for (int t = 0; t < kGdB; t++) {
-    R[(size_t)t * n + j] = t < nb ? A[(size_t)(k0 + t) * n + j] : 0.0;
+    R[(size_t)t * ld + j] = t < nb ? A[(size_t)(k0 + t) * n + j] : 0.0;
     C[(size_t)j * kGdB + t] = t < nb ? A[(size_t)j * n + k0 + t] : 0.0;
   }
 }
 
-__global__ void __launch_bounds__(256) k_gjd_first(int n, int nb, const double* __restrict__ R, double* Dout,
+__global__ void __launch_bounds__(256) k_gjd_first(int ld, int nb, const double* __restrict__ R, double* Dout,
                                                    int* status) {
   __shared__ double D[2][kGdB][kGdB + 1];
-  gjd_invert_block(n, 0, nb, R, Dout, status, D);
+  gjd_invert_block(ld, 0, nb, R, Dout, status, D);
 }
 
-// Rp[t][j] = sum_u D[t][u] R[u][j]: the panel's new pivot rows; four
-// threads per column, eight output rows each (grid ceil(4 n / 256))
-__global__ void __launch_bounds__(256) k_gjd_rows(int n, int nb, const double* __restrict__ R,
+// Rp[t][j] = sum_u D[t][u] R[u][j]: the panel's new pivot rows; one CTA
+// (256 threads) per 32 columns stages R's 32 x 32 block, each thread forms
+// four outputs (grid ceil(n / 32); the padding columns come out zero)
+__global__ void __launch_bounds__(256) k_gjd_rows(int ld, int nb, const double* __restrict__ R,
                                                   const double* __restrict__ Dinv, double* __restrict__ Rp) {
   __shared__ double D[kGdB][kGdB + 1];
-  for (int e = threadIdx.x; e < kGdB * kGdB; e += blockDim.x) D[e / kGdB][e % kGdB] = Dinv[e];
+  __shared__ double Rs[kGdB][kGdB + 1];
+  const int tid = threadIdx.x, c = tid & 31, w = tid >> 5;
+  const int j = blockIdx.x * kGdB + c;
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    const int u = w + 8 * q;
+    Rs[u][c] = u < nb ? R[(size_t)u * ld + j] : 0.0;
+    D[u][c] = Dinv[u * kGdB + c];
+  }
   __syncthreads();
-  const int g = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = g >> 2, t0 = (g & 3) * 8;
-  if (j >= n) return;
-  double r[kGdB];
 #pragma unroll
-  for (int u = 0; u < kGdB; u++) r[u] = u < nb ? R[(size_t)u * n + j] : 0.0;
-#pragma unroll
-  for (int q = 0; q < 8; q++) {
-    const int t = t0 + q;
+  for (int q = 0; q < 4; q++) {
+    const int t = w + 8 * q;
     double acc = 0.0;
 #pragma unroll
-    for (int u = 0; u < kGdB; u++) acc = __fma_rn(D[t][u], r[u], acc);
-    Rp[(size_t)t * n + j] = t < nb ? acc : 0.0;
+    for (int u = 0; u < kGdB; u++) acc = __fma_rn(D[t][u], Rs[u][c], acc);
+    Rp[(size_t)t * ld + j] = t < nb ? acc : 0.0;
   }
 }
 
@@ -1340,16 +1463,16 @@ __global__ void __launch_bounds__(256) k_gjd_rows(int n, int nb, const double* _
 // (ceil(n / 64), ceil(n / 64)), 256 threads. Also fills Cn / Rn with the
 // next panel's [k1, k1 + nb1) columns / rows and, in the launch's last CTA,
 // Dnext. *ticket is 0 on entry and left 0.
-__global__ void __launch_bounds__(256, 2) k_gjd_update(int n, int k0, int nb, double* __restrict__ A,
+__global__ void __launch_bounds__(256, 3) k_gjd_update(int n, int ld, int k0, int nb, double* __restrict__ A,
                                                     const double* __restrict__ C, const double* __restrict__ Rp,
                                                     const double* __restrict__ Dinv, double* __restrict__ Cn,
                                                     double* __restrict__ Rn, double* __restrict__ Dnext, int k1,
                                                     int nb1, unsigned* ticket, int* status) {
   // Cs doubles as the last CTA's pivot-block workspace (2 x 32 x 33 doubles)
-  static_assert(kGdT * (kGdB + 1) >= 2 * kGdB * (kGdB + 1), "block inverse workspace");
-  __shared__ double Cs[kGdT][kGdB + 1];
-  __shared__ double Rs[kGdB][kGdT + 2];
-  __shared__ double Ds[kGdB][kGdB + 1];
+  static_assert(kGdT * (kGdB + kGdPad) >= 2 * kGdB * (kGdB + 1), "block inverse workspace");
+  __shared__ __align__(16) double Cs[kGdT][kGdB + kGdPad];
+  __shared__ __align__(16) double Rs[kGdB][kGdT + kGdPad];
+  __shared__ __align__(16) double Ds[kGdB][kGdB + kGdPad];
   __shared__ bool last;
   const int tid = threadIdx.x;
   const int i0 = blockIdx.y * kGdT, j0 = blockIdx.x * kGdT;
@@ -1369,16 +1492,29 @@ __global__ void __launch_bounds__(256, 2) k_gjd_update(int n, int k0, int nb, do
       acc[a][b] = (i < n && j < n) ? A[(size_t)i * n + j] : 0.0;
     }
   }
-  for (int e = tid; e < kGdT * kGdB; e += 256) {
-    const int r = e / kGdB, t = e % kGdB;
-    Cs[r][t] = i0 + r < n ? C[(size_t)(i0 + r) * kGdB + t] : 0.0;
+  // 16-byte copies: Cs 64 rows x 16, Rs 32 rows x 32, Ds 32 rows x 16;
+  // i0 + 64 <= ld and j0 + 64 <= ld keep every source inside the buffers
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    const int e = tid + 256 * q;
+    const int r = e >> 4, k = (e & 15) * 2;
+    cp_async16(&Cs[r][k], C + (size_t)(i0 + r) * kGdB + k);
   }
-  for (int e = tid; e < kGdB * kGdT; e += 256) {
-    const int t = e / kGdT, c = e % kGdT;
-    Rs[t][c] = j0 + c < n ? Rp[(size_t)t * n + j0 + c] : 0.0;
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    const int e = tid + 256 * q;
+    const int t = e >> 5, k = (e & 31) * 2;
+    cp_async16(&Rs[t][k], Rp + (size_t)t * ld + j0 + k);
   }
-  if (colsK || rowsK)
-    for (int e = tid; e < kGdB * kGdB; e += 256) Ds[e / kGdB][e % kGdB] = Dinv[e];
+  if (colsK || rowsK) {
+#pragma unroll
+    for (int q = 0; q < 2; q++) {
+      const int e = tid + 256 * q;
+      const int r = e >> 4, k = (e & 15) * 2;
+      cp_async16(&Ds[r][k], Dinv + r * kGdB + k);
+    }
+  }
+  cp_async_wait_all();
   __syncthreads();
 #pragma unroll 4
   for (int t = 0; t < kGdB; t++) {
@@ -1416,22 +1552,23 @@ __global__ void __launch_bounds__(256, 2) k_gjd_update(int n, int k0, int nb, do
       }
       A[(size_t)i * n + j] = v;
       if (j >= k1 && j < k1 + nb1) Cn[(size_t)i * kGdB + (j - k1)] = v;
-      if (i >= k1 && i < k1 + nb1) Rn[(size_t)(i - k1) * n + j] = v;
+      if (i >= k1 && i < k1 + nb1) Rn[(size_t)(i - k1) * ld + j] = v;
     }
   }
   if (nb1 <= 0) return;  // the last panel: no next block to invert
-  // the last CTA to finish inverts the next panel's pivot block (every
-  // thread fences its own writes before the barrier)
-  __threadfence();
+  // the last CTA to finish inverts the next panel's pivot block: the
+  // barrier orders the CTA's writes before thread 0's fence, which makes
+  // them visible device-wide before its ticket increment
   __syncthreads();
   if (tid == 0) {
+    __threadfence();
     const unsigned done = atomicAdd(ticket, 1u);
     last = done == gridDim.x * gridDim.y - 1;
   }
   __syncthreads();
   if (!last) return;
   __threadfence();
-  gjd_invert_block(n, k1, nb1, Rn, Dnext, status, reinterpret_cast<double(*)[kGdB][kGdB + 1]>(&Cs[0][0]));
+  gjd_invert_block(ld, k1, nb1, Rn, Dnext, status, reinterpret_cast<double(*)[kGdB][kGdB + 1]>(&Cs[0][0]));
   if (tid == 0) *ticket = 0u;
 }
 
@@ -1483,13 +1620,14 @@ void gj_run(int n, double* a, double* inv, double* Bt, int* piv, int* idx, int* 
 
 // scratch: [panel doubles][piv: n ints][idx: n ints][status]; the panel
 // doubles hold the pivoted path's Bt (kGjMaxPanel x n) or the unpivoted
-// path's side buffers
-// (the unpivoted path: C, R of two panels and Rp, 5 x kGdB x n)
-constexpr int kGjScratchPanels = 5 * kGdB > kGjMaxPanel ? 5 * kGdB : kGjMaxPanel;
-// the panel doubles, plus the unpivoted path's two inverted pivot blocks
-// and its ticket counter
+// path's side buffers (C, R of two panels and Rp, 5 x kGdB x ld, ld = n
+// rounded up to 64), plus its two inverted pivot blocks and its ticket
+// counter
 size_t gj_panel_bytes(int n) {
-  return gj_align(sizeof(double) * ((size_t)kGjScratchPanels * n + 2 * kGdB * kGdB + 1));
+  const size_t ld = (size_t)gjd_ld(n);
+  const size_t unpiv = 5 * (size_t)kGdB * ld + 2 * kGdB * kGdB + 2;
+  const size_t piv = (size_t)kGjMaxPanel * n;
+  return gj_align(sizeof(double) * (unpiv > piv ? unpiv : piv));
 }
 size_t gauss_jordan_scratch_bytes(int n) {
   return gj_panel_bytes(n) + 2 * gj_align(sizeof(int) * (size_t)n) + gj_align(sizeof(int));
@@ -1500,7 +1638,8 @@ const int* gauss_jordan_status(int n, const void* scratch) {
 }
 void gauss_jordan_inverse_dominant(int n, double* a, void* scratch, cudaStream_t st) {
   double* sb = (double*)scratch;
-  const size_t pn = (size_t)kGdB * n;
+  const int ld = gjd_ld(n);
+  const size_t pn = (size_t)kGdB * ld;
   double* C[2] = {sb, sb + pn};
   double* R[2] = {sb + 2 * pn, sb + 3 * pn};
   double* Rp = sb + 4 * pn;
@@ -1508,20 +1647,21 @@ void gauss_jordan_inverse_dominant(int n, double* a, void* scratch, cudaStream_t
   unsigned* ticket = (unsigned*)(sb + 5 * pn + 2 * kGdB * kGdB);
   int* status = (int*)gauss_jordan_status(n, scratch);
   cudaMemsetAsync(status, 0, sizeof(int), st);
-  cudaMemsetAsync(ticket, 0, sizeof(unsigned), st);
+  // side buffers, blocks and ticket: the padding must read as zero
+  cudaMemsetAsync(sb, 0, sizeof(double) * (5 * pn + 2 * kGdB * kGdB + 2), st);
   if (n <= 0) return;
   const int nb0 = n < kGdB ? n : kGdB;
-  k_gjd_extract<<<ceil_div(n, kBlock), kBlock, 0, st>>>(n, 0, nb0, a, C[0], R[0]);
-  k_gjd_first<<<1, 256, 0, st>>>(n, nb0, R[0], Dv[0], status);
+  k_gjd_extract<<<ceil_div(n, kBlock), kBlock, 0, st>>>(n, ld, 0, nb0, a, C[0], R[0]);
+  k_gjd_first<<<1, 256, 0, st>>>(ld, nb0, R[0], Dv[0], status);
   const dim3 grid(ceil_div(n, kGdT), ceil_div(n, kGdT));
   int cur = 0;
   for (int k0 = 0; k0 < n; k0 += kGdB) {
     const int nb = n - k0 < kGdB ? n - k0 : kGdB;
     const int k1 = k0 + nb;
     const int nb1 = n - k1 < kGdB ? n - k1 : kGdB;
-    k_gjd_rows<<<ceil_div(4LL * n, kBlock), kBlock, 0, st>>>(n, nb, R[cur], Dv[cur], Rp);
-    k_gjd_update<<<grid, 256, 0, st>>>(n, k0, nb, a, C[cur], Rp, Dv[cur], C[cur ^ 1], R[cur ^ 1], Dv[cur ^ 1], k1,
-                                       nb1 > 0 ? nb1 : 0, ticket, status);
+    k_gjd_rows<<<ceil_div(n, kGdB), 256, 0, st>>>(ld, nb, R[cur], Dv[cur], Rp);
+    k_gjd_update<<<grid, 256, 0, st>>>(n, ld, k0, nb, a, C[cur], Rp, Dv[cur], C[cur ^ 1], R[cur ^ 1], Dv[cur ^ 1],
+                                       k1, nb1 > 0 ? nb1 : 0, ticket, status);
     cur ^= 1;
   }
 }
@@ -1669,6 +1809,7 @@ void update_solution(int nCells, const int* perm, const double* delta, const Bou
   template void gs_sequential<T>(const SellView<T>&, T*, const T*, bool, cudaStream_t);          \
   template void jacobi<T>(const SellView<T>&, int, const T*, T*, const T*, cudaStream_t);        \
   template void jacobi_damped<T>(const SellView<T>&, int, const T*, T*, const T*, T, cudaStream_t, RowPlan); \
+  template void chebyshev_step<T>(const SellView<T>&, int, const T*, T*, T*, const T*, T, T, bool, cudaStream_t); \
   template void residual<T>(const SellView<T>&, int, const T*, const T*, T*, double*, cudaStream_t); \
   template void restrict_sum<T>(int, const int*, const int*, const T*, T*, cudaStream_t);        \
   template void restrict_rhs<T>(int, const int*, const int*, const T*, T*, T*, cudaStream_t);    \

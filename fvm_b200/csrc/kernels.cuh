@@ -39,7 +39,8 @@ struct SellView {
 struct RowPlan {
   int tpr = 1;
   int block = 256;
-  bool isDefault() const { return tpr == 1 && block == 256; }
+  int ellRows = 1;  // ELL-32 levels: rows per thread of the Gauss-Seidel pass (1 or 2)
+  bool isDefault() const { return tpr == 1 && block == 256 && ellRows == 1; }
 };
 
 template <class T>
@@ -55,6 +56,15 @@ void jacobi(const SellView<T>& a, int nSlices, const T* xold, T* xnew, const T* 
 template <class T>
 void jacobi_damped(const SellView<T>& a, int nSlices, const T* xold, T* xnew, const T* b, T w, cudaStream_t st,
                    RowPlan plan = RowPlan());
+// one step of a Chebyshev smoother on D^-1 A over all rows: res = b + A x,
+// dv = c1 dv + c2 (-res / a_ii) (first: dv = c2 (-res / a_ii), dv not read),
+// xnew = x + dv; x and xnew distinct
+template <class T>
+void chebyshev_step(const SellView<T>& a, int nSlices, const T* x, T* xnew, T* dv, const T* b, T c1, T c2,
+                    bool first, cudaStream_t st);
+// Gershgorin bound of the spectrum of D^-1 A, max_i 1 + sum_j |a_ij / a_ii|,
+// into *out (device; asynchronous)
+void gershgorin_bound(const SellView<double>& a, int nSlices, double* out, cudaStream_t st);
 
 // ---- residual / products ---------------------------------------------------
 // r = b + D x + O x over all rows; when partials != null each block also
@@ -181,10 +191,12 @@ struct FaceGeom {
   const double* cellCentroid; // 3 per cell (self + ghost)
   const double* cellVolume;   // per cell (self + ghost)
 };
-// c_f and the secondary (non-orthogonal) coefficient per face
+// c_f and the secondary (non-orthogonal) coefficient per face; secCoeff
+// holds one 32-byte record per face (x, y, z, pad), 32-byte aligned
 void face_coefficients(const FaceGeom& g, const double* k, double* coeff, double* secCoeff,
                        cudaStream_t st);
-// least-squares gradient of x on self rows, then boundary ghosts copy c0
+// least-squares gradient of x on self rows, then boundary ghosts copy c0;
+// grad holds one 32-byte record per cell (x, y, z, pad), 32-byte aligned
 void gradient(int nCells, const int* ccRow, const int* ccCol, const double* w, const double* x,
               double* grad, cudaStream_t st);
 void ghost_gradient(int nBFaces, const int* bFaces, const int* faceCells, double* grad,

@@ -272,6 +272,7 @@ void AmgHierarchy::build(std::vector<RefLevel>& levels, int finestLocalSize, con
     CUDA_OK(cudaDeviceSynchronize());
     lap(gjUnpivoted ? "coarsest inverse (unpivoted)" : "coarsest inverse");
   }
+  prepareChebyshev();
   tunePlans();
   lap("launch plans");
   if (trace) {
@@ -370,7 +371,39 @@ void AmgHierarchy::tunePlans() {
   for (int l = 0; l < L; l++) {
     DevLevel& d = lv_[l];
     d.plan = dev::RowPlan();
-    if (d.ellWidth) continue;
+    if (d.ellWidth) {
+      // ELL-32 Gauss-Seidel levels: one or two rows per thread
+      if (opt_.planEllRows) {
+        d.plan.ellRows = opt_.planEllRows;
+        continue;
+      }
+      if (!opt_.autotune || d.n < kTuneMinRows || opt_.smootherType != kGaussSeidel || dampedLevel(l, d.n) ||
+          opt_.ordering != kMulticolor || chebyshevLevel(l))
+        continue;
+      const PlanKey key{d.n, d.entries, -d.ellWidth, d.nColors, f32, false};
+      {
+        std::lock_guard<std::mutex> lock(gPlanMu);
+        auto it = gPlanCache.find(key);
+        if (it != gPlanCache.end()) {
+          d.plan = it->second;
+          continue;
+        }
+      }
+      if (!st) {
+        CUDA_OK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        CUDA_OK(cudaEventCreate(&e0));
+        CUDA_OK(cudaEventCreate(&e1));
+      }
+      touched = true;
+      dev::RowPlan two;
+      two.ellRows = 2;
+      const float t1 = median_ms([&] { smootherPass(l, dev::RowPlan(), st); });
+      const float t2 = median_ms([&] { smootherPass(l, two, st); });
+      if (t2 < t1) d.plan = two;
+      std::lock_guard<std::mutex> lock(gPlanMu);
+      gPlanCache[key] = d.plan;
+      continue;
+    }
     if (opt_.planTpr) {
       d.plan.tpr = opt_.planTpr;
       d.plan.block = opt_.planBlock ? opt_.planBlock : 256;
@@ -449,6 +482,38 @@ void AmgHierarchy::tunePlans() {
       if (d.xF) CUDA_OK(cudaMemset(d.xF, 0, sizeof(float) * d.n));
       if (d.tmpF) CUDA_OK(cudaMemset(d.tmpF, 0, sizeof(float) * d.n));
     }
+  }
+}
+
+// Chebyshev iteration (Saad, Iterative Methods for Sparse Linear Systems,
+// 2nd ed., Alg. 12.1) on D^-1 A with eigenvalues taken in [alpha, beta]:
+// theta = (beta + alpha) / 2, delta = (beta - alpha) / 2, sigma = theta /
+// delta; step 0: d = z / theta; step k: rho_k = 1 / (2 sigma - rho_{k-1}),
+// d = rho_k rho_{k-1} d + (2 rho_k / delta) z, with z = -D^-1 (b + A x) the
+// scaled residual and rho_0 = 1 / sigma. beta is the Gershgorin bound of
+// level 0 (never below the spectrum), alpha = chebyshevFraction * beta: the
+// polynomial damps the upper part of the spectrum, what a smoother must.
+void AmgHierarchy::prepareChebyshev() {
+  chebC1_.clear();
+  chebC2_.clear();
+  chebBound_ = 0.0;
+  if (opt_.chebyshevDegree <= 0 || lv_.empty() || opt_.finestOnly()) return;
+  DevLevel& d = lv_[0];
+  double* dv = (double*)scratch(sizeof(double));
+  dev::gershgorin_bound(d.view64(), d.nSlices, dv, nullptr);
+  CUDA_OK(cudaMemcpy(&chebBound_, dv, sizeof(double), cudaMemcpyDeviceToHost));
+  FVM_REQUIRE(std::isfinite(chebBound_) && chebBound_ > 0.0, kBadArgument,
+              "Chebyshev smoother: no finite spectrum bound (zero diagonal?)");
+  const double beta = chebBound_, alpha = opt_.chebyshevFraction * beta;
+  const double theta = 0.5 * (beta + alpha), delta = 0.5 * (beta - alpha), sigma = theta / delta;
+  double rho = 1.0 / sigma;
+  chebC1_.push_back(0.0);
+  chebC2_.push_back(1.0 / theta);
+  for (int k = 1; k < opt_.chebyshevDegree; k++) {
+    const double rn = 1.0 / (2.0 * sigma - rho);
+    chebC1_.push_back(rn * rho);
+    chebC2_.push_back(2.0 * rn / delta);
+    rho = rn;
   }
 }
 
@@ -559,6 +624,21 @@ void AmgHierarchy::sweeps(int nSweeps, int l, cudaStream_t st) {
   T* x = vec_x<T>(d);
   const T* b = vec_b<T>(d);
   const bool damped = dampedLevel(l, d.n);
+  if (chebyshevLevel(l) && nSweeps > 0) {
+    // x and tmp alternate as the step's input and output; the level's r
+    // holds the step direction (every use of r recomputes it afterwards)
+    T* bufs[2] = {x, vec_tmp<T>(d)};
+    T* dv = vec_r<T>(d);
+    int cur = 0;
+    for (int s = 0; s < nSweeps; s++)
+      for (size_t k = 0; k < chebC1_.size(); k++) {
+        dev::chebyshev_step<T>(a, d.nSlices, bufs[cur], bufs[cur ^ 1], dv, b, (T)chebC1_[k], (T)chebC2_[k], k == 0,
+                               st);
+        cur ^= 1;
+      }
+    if (cur) CUDA_OK(cudaMemcpyAsync(x, bufs[1], sizeof(T) * (size_t)d.n, cudaMemcpyDeviceToDevice, st));
+    return;
+  }
   for (int s = 0; s < nSweeps; s++) {
     if (damped) {
       // small coarse levels: two damped Jacobi passes instead of 2C-1
@@ -681,11 +761,20 @@ double AmgHierarchy::cycleBytes() const {
       total += (double)d.n * d.n * (opt_.precision == kMixed && coarseInvF_ ? 4.0 : 8.0) + 2.0 * vb * d.n;
       continue;
     }
-    // a sweep: two damped-Jacobi passes, or forward + reverse over the
-    // colours (2C - 1 colour passes, C of which make one pass)
-    const bool gsPasses = opt_.smootherType == kGaussSeidel && !dampedLevel(l, d.n) && d.nColors > 0;
-    const double perSweep = gsPasses ? (2.0 * d.nColors - 1.0) / d.nColors : 2.0;
-    total += (opt_.nPreSweeps + opt_.postSweeps(l)) * perSweep * pass;
+    const int sweeps = opt_.nPreSweeps + opt_.postSweeps(l);
+    if (chebyshevLevel(l)) {
+      // a Chebyshev step: x, b, diag, the direction (read but in the first
+      // step, written) and the new x per row, col + val per entry
+      const int steps = sweeps * (int)chebC1_.size();
+      total += steps * (d.n * 6.0 * vb + d.entries * (4.0 + vb)) - sweeps * d.n * vb;
+      if (steps & 1) total += 2.0 * vb * d.n;
+    } else {
+      // a sweep: two damped-Jacobi passes, or forward + reverse over the
+      // colours (2C - 1 colour passes, C of which make one pass)
+      const bool gsPasses = opt_.smootherType == kGaussSeidel && !dampedLevel(l, d.n) && d.nColors > 0;
+      const double perSweep = gsPasses ? (2.0 * d.nColors - 1.0) / d.nColors : 2.0;
+      total += sweeps * perSweep * pass;
+    }
     if (l + 1 < L) {
       const DevLevel& c = lv_[l + 1];
       if (opt_.nPreSweeps == 0)
@@ -707,7 +796,8 @@ int AmgHierarchy::kernelsPerCycle() const {
       k += 1;
       continue;
     }
-    const int perSweep = (opt_.smootherType == kGaussSeidel && !dampedLevel(l, d.n))
+    const int perSweep = chebyshevLevel(l) ? (int)chebC1_.size()
+                         : (opt_.smootherType == kGaussSeidel && !dampedLevel(l, d.n))
                              ? (opt_.ordering == kSequential ? 2 : 2 * d.nColors - 1)
                              : 2;
     k += perSweep * (opt_.nPreSweeps + opt_.postSweeps(l));

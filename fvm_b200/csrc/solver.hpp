@@ -59,6 +59,15 @@ struct SolverOptions {
   bool autotune = true;
   int planTpr = 0;
   int planBlock = 0;
+  // rows per thread of the Gauss-Seidel pass on ELL-32 levels (1 or 2;
+  // 0: autotuned)
+  int planEllRows = 0;
+  // > 0: the finest level smooths with a Chebyshev polynomial of this
+  // degree in D^-1 A per sweep (one launch per degree) instead of
+  // multicolour Gauss-Seidel; its interval is [fraction * b, b], b the
+  // Gershgorin bound of the spectrum
+  int chebyshevDegree = 0;
+  double chebyshevFraction = 0.3;
   // Build the coarse levels on the GPU (parallel pairwise matching and
   // Galerkin kernels) instead of the reference's sequential greedy walk on
   // the host; coarse levels then smooth with damped Jacobi. The hierarchy is
@@ -272,6 +281,12 @@ class AmgHierarchy {
   void allocVectors(DevLevel& d, bool mixed);
   // picks each SELL-32 level's smoother launch plan (autotune or forced)
   void tunePlans();
+  // Chebyshev smoother of level 0: coefficients (c1, c2) of each step of
+  // one sweep, from the Gershgorin bound of level 0's D^-1 A
+  std::vector<double> chebC1_, chebC2_;
+  double chebBound_ = 0.0;
+  void prepareChebyshev();
+  bool chebyshevLevel(int l) const { return l == 0 && !chebC1_.empty(); }
   // one smoother pass of level l with a given plan (what the tuner times)
   void smootherPass(int l, dev::RowPlan plan, cudaStream_t st);
   // level l's residual restricted to level l + 1, fused or split

@@ -326,12 +326,12 @@ void ThermalModel::ensureDevice() {
   dRc_ = (double*)arena_.alloc(cb);
   dTN1_ = (double*)arena_.alloc(cb);
   dRhoVdt_ = (double*)arena_.alloc(cb);
-  dGrad_ = (double*)arena_.alloc(3 * cb);
+  dGrad_ = (double*)arena_.alloc(4 * cb);  // 32-byte record per cell
   dDiagOrig_ = (double*)arena_.alloc(cb);
   dFlux_ = (double*)arena_.alloc(sizeof(double) * (size_t)F);
   dCoeff_ = (double*)arena_.alloc(sizeof(double) * (size_t)F);
-  dSec_ = (double*)arena_.alloc(3 * sizeof(double) * (size_t)F);
-  CUDA_OK(cudaMemset(dGrad_, 0, 3 * cb));
+  dSec_ = (double*)arena_.alloc(4 * sizeof(double) * (size_t)F);  // 32-byte record per face
+  CUDA_OK(cudaMemset(dGrad_, 0, 4 * cb));
   {
     // identifies this model's level-0 pattern (interiorConn_, entryFace_)
     static std::atomic<unsigned long long> nextKey{1};
@@ -769,10 +769,12 @@ void ThermalModel::profile(int reps, double* out) {
   out[0] = timed([&] {
     if (mixed) {
       for (int c = 0; c < d.nColors; c++)
-        dev::gs_color<float>(d.view32(), d.colorSliceStart[c], d.colorSliceStart[c + 1], d.xF, d.bF, stream_);
+        dev::gs_color<float>(d.view32(), d.colorSliceStart[c], d.colorSliceStart[c + 1], d.xF, d.bF, stream_,
+                             d.plan);
     } else {
       for (int c = 0; c < d.nColors; c++)
-        dev::gs_color<double>(d.view64(), d.colorSliceStart[c], d.colorSliceStart[c + 1], d.x, d.b, stream_);
+        dev::gs_color<double>(d.view64(), d.colorSliceStart[c], d.colorSliceStart[c + 1], d.x, d.b, stream_,
+                              d.plan);
     }
   });
   out[1] = hier_.fineSweepBytes();
@@ -794,6 +796,16 @@ void ThermalModel::profile(int reps, double* out) {
   out[8] = (double)d.entries;
   out[9] = hier_.kernelsPerCycle();
   out[10] = d.nColors;
+  {
+    // the face loop of the linearization (k_face_flux), compulsory bytes:
+    // per face cells (int2), c_f, the secondary coefficient (3 doubles) and
+    // the flux written; per cell (self + ghost) its volume, gradient (3
+    // doubles) and value
+    HostMesh& m = *mesh_;
+    dev::FaceGeom g{m.nFaces, m.nCells, dFaceCells_, dArea_, dAreaMag_, dCentroid_, dVol_};
+    out[11] = timed([&] { dev::face_flux(g, dCoeff_, dSec_, dGrad_, dT_, dFlux_, stream_); });
+    out[12] = 48.0 * m.nFaces + 40.0 * m.nTotalCells();
+  }
   cudaEventDestroy(a);
   cudaEventDestroy(b);
   cudaFree(flush);

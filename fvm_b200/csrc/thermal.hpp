@@ -136,7 +136,8 @@ class ThermalModel {
   // configured V-cycle precision, [1] its algorithmic bytes, [2] FP64
   // residual of level 0, [3] its bytes, [4] one full cycle, [5] its bytes,
   // [6] levels, [7] rows of level 0, [8] stored entries of level 0,
-  // [9] kernels per cycle, [10] colours of level 0
+  // [9] kernels per cycle, [10] colours of level 0, [11] the face loop of
+  // the linearization (k_face_flux), [12] its bytes
   void profile(int reps, double* out);
   // per-level kernel timings of the cycle (AmgHierarchy::profileLevels)
   void profileLevels(int reps, std::vector<double>& out);

@@ -194,6 +194,10 @@ class AMG(LinearSolver):
         self.autotune = bool(d.autotune)
         self.planThreadsPerRow = d.planThreadsPerRow
         self.planBlock = d.planBlock
+        self.planEllRows = d.planEllRows  # rows per thread of the ELL-32 Gauss-Seidel pass
+        # finest-level Chebyshev smoother (0: multicolour Gauss-Seidel)
+        self.chebyshevDegree = d.chebyshevDegree
+        self.chebyshevFraction = d.chebyshevFraction
         self.setupOnDevice = bool(d.setupOnDevice)
         self.matchRounds = d.matchRounds
         self.matchBeta = d.matchBeta
@@ -236,6 +240,9 @@ class AMG(LinearSolver):
         o.autotune = int(bool(self.autotune))
         o.planThreadsPerRow = int(self.planThreadsPerRow)
         o.planBlock = int(self.planBlock)
+        o.planEllRows = int(self.planEllRows)
+        o.chebyshevDegree = int(self.chebyshevDegree)
+        o.chebyshevFraction = float(self.chebyshevFraction)
         o.setupOnDevice = int(bool(self.setupOnDevice))
         o.matchRounds = int(self.matchRounds)
         o.matchBeta = float(self.matchBeta)

@@ -327,10 +327,10 @@ class ThermalModelA:
     def profile(self, reps: int = 5) -> dict:
         """CUDA-event timings of the finest-level kernels (see fvm_thermal_profile)."""
         self._push()
-        out = np.zeros(11)
+        out = np.zeros(13)
         check(_lib.load().fvm_thermal_profile(self._h, int(reps), dptr(out)))
         keys = ["gs_pass_ms", "gs_pass_bytes", "residual_ms", "residual_bytes", "cycle_ms", "cycle_bytes", "levels",
-                "rows", "entries", "kernels_per_cycle", "colors"]
+                "rows", "entries", "kernels_per_cycle", "colors", "face_flux_ms", "face_flux_bytes"]
         return dict(zip(keys, out.tolist()))
 
     def profileLevels(self, reps: int = 5) -> list:

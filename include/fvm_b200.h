@@ -89,6 +89,12 @@ typedef struct fvm_linear_options {
   int matchPasses;          /* matchings per level: 1 pairs rows, 2 pairs the pairs (aggregates of
                                about 4 rows, half as many levels) */
   int coarsePostSweeps;     /* post-smoothing sweeps on the levels below the finest (-1: nPostSweeps) */
+  int planEllRows;          /* != 0: rows per thread (1 or 2) of the Gauss-Seidel pass on ELL-32
+                               levels instead of the autotuner's choice (results never change) */
+  int chebyshevDegree;      /* > 0: the finest level smooths with a Chebyshev polynomial of this
+                               degree in D^-1 A per sweep (one launch per degree) instead of
+                               multicolour Gauss-Seidel (0: Gauss-Seidel, the reference's smoother) */
+  double chebyshevFraction; /* its interval [fraction * b, b], b the Gershgorin bound (default 0.3) */
 } fvm_linear_options;
 
 /* ThermalModelOptions (fvmbase/ThermalBC.h:33-67) + volume-condition constants */
@@ -221,8 +227,9 @@ int fvm_thermal_level_matrix(fvm_thermal* t, int level, int* n, int* nnz, int* r
                              double* diag, int cap);
 /* Launch plans of the smoother kernels, one per level of the current setup
  * (no reference counterpart): threads per row and threads per block as the
- * autotuner (or the forced plan) chose them; ELL-32 levels, whose kernels
- * take no plan, report width, 0 -- threadsPerRow[l] = -(ELL width). */
+ * autotuner (or the forced plan) chose them; ELL-32 levels report
+ * threadsPerRow[l] = -(ELL width) and block[l] = -(rows per thread of
+ * their Gauss-Seidel pass). */
 int fvm_thermal_launch_plans(fvm_thermal* t, int* nLevels, int* threadsPerRow, int* block, int cap);
 /* Measurement hook (no reference counterpart): CUDA-event timings in ms
  * per launch, each launch preceded by a write of 512 MB to flush L2.
@@ -231,7 +238,7 @@ int fvm_thermal_launch_plans(fvm_thermal* t, int* nLevels, int* threadsPerRow, i
  * residual, out[3] its bytes, out[4] one full cycle, out[5] its bytes,
  * out[6] levels, out[7] finest rows, out[8] finest stored entries,
  * out[9] kernels per cycle, out[10] colours of the finest level. */
-int fvm_thermal_profile(fvm_thermal* t, int reps, double* out11);
+int fvm_thermal_profile(fvm_thermal* t, int reps, double* out13);
 /* Measurement hook (no reference counterpart): per AMG level, CUDA-event
  * times in ms (mean of reps, each launch preceded by a 512 MB write that
  * flushes L2) of the kernels one cycle runs there, in the cycle's

@@ -213,7 +213,8 @@ def _converge(tm, n_outer=200):
 
 @pytest.mark.parametrize("kind", ["quad", "tet", "hex"])
 @pytest.mark.parametrize("variant", ["fp64-gs", "fp64-sequential", "mixed-direct", "mixed-direct-gpu-inverse",
-                                     "mixed-coarse-jacobi", "cg-mixed", "bcgstab", "jacobi"])
+                                     "mixed-coarse-jacobi", "cg-mixed", "bcgstab", "jacobi", "fp64-chebyshev",
+                                     "cg-mixed-chebyshev"])
 def test_converged_field_matches_reference(refo, kind, variant):
     mesh, f = _synthetic(kind)
     bcs = {gid: v for gid, v in f["bc"].items()}
@@ -252,6 +253,21 @@ def test_converged_field_matches_reference(refo, kind, variant):
         solver.nMaxIterations = 500
     elif variant == "jacobi":
         amg.smootherType = fvmbaseExt.AMG.JACOBI
+    elif variant == "fp64-chebyshev":
+        # finest level: Chebyshev polynomial of degree 3 per sweep
+        amg.chebyshevDegree = 3
+    elif variant == "cg-mixed-chebyshev":
+        amg.precision = fvmbaseExt.AMG.MIXED
+        amg.coarseSolver = fvmbaseExt.AMG.COARSE_DIRECT
+        amg.coarsestSize = 100
+        amg.coarseJacobiRows = 1 << 30
+        amg.chebyshevDegree = 2
+        amg.nPreSweeps = 0
+        amg.nPostSweeps = 2
+        solver = fvmbaseExt.CG()
+        solver.preconditioner = amg
+        solver.relativeTolerance = 1e-10
+        solver.nMaxIterations = 500
     tm, tf, m = gpu_model(mesh, bcs, solver=solver, fields=fields, opts={"relativeTolerance": 1e-10})
     _converge(tm)
     T = tf.temperature[m.getCells()][: mesh["nCells"]]

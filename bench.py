@@ -198,15 +198,17 @@ def train_learned(gen, inner_rel, seeds=(101, 102), n_outer=4, per_solve=3, step
     return lc, info
 
 
-def size_matched_copy_gbs(nbytes: float, reps: int = 7) -> float:
-    """Bandwidth of a plain device-to-device copy that moves the same bytes
+def size_matched_copy_gbs(nbytes: float, reps: int = 7, launches: int = 1) -> float:
+    """Bandwidth of plain device-to-device copies that move the same bytes
     as a kernel (nbytes/2 read + nbytes/2 written), CUDA events, L2 flushed
     before each repetition: what streaming reaches at this transfer size,
-    launch and ramp included, beside the large-transfer peak."""
+    launch and ramp included, beside the large-transfer peak. With
+    launches > 1 the bytes are split into that many copies in a row, as a
+    multicolour pass splits its rows into one launch per colour."""
     import torch
 
-    n = max(1, int(nbytes // 16))
-    src = torch.ones(n, dtype=torch.float64, device="cuda")
+    n = max(1, int(nbytes // (16 * launches)))
+    src = torch.ones(n * launches, dtype=torch.float64, device="cuda")
     dst = torch.empty_like(src)
     flush = torch.empty(64 << 20, dtype=torch.float64, device="cuda")
     times = []
@@ -214,14 +216,15 @@ def size_matched_copy_gbs(nbytes: float, reps: int = 7) -> float:
         flush.fill_(float(r))
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        dst.copy_(src)
+        for q in range(launches):
+            dst[q * n:(q + 1) * n].copy_(src[q * n:(q + 1) * n])
         e1.record()
         e1.synchronize()
         if r >= 2:
             times.append(e0.elapsed_time(e1))
     ms = statistics.median(times)
     del src, dst, flush
-    return 16.0 * n / (ms * 1e-3) / 1e9
+    return 16.0 * n * launches / (ms * 1e-3) / 1e9
 
 
 HOST_SETUP = False  # --host-setup: the mixed path on the reference's host aggregation
@@ -959,6 +962,17 @@ def main():
             "bytes": pp["residual_bytes"], "gbs": copy_gbs, "frac_of_peak": copy_gbs / peak,
             "fp64_residual_vs_copy": roofline["fp64_residual"]["achieved"] / copy_gbs,
             "fp64_gs_pass_vs_copy": roofline["fp64_gs_pass"]["achieved"] / copy_gbs}
+        # the Gauss-Seidel pass is one launch per colour: copies of the same
+        # bytes split into as many launches
+        colors = int(pp.get("colors", 0))
+        try:
+            split_gbs = dist.max(size_matched_copy_gbs(pp["gs_pass_bytes"], launches=colors)) if colors > 1 else None
+        except Exception:  # context only
+            split_gbs = None
+        if split_gbs:
+            roofline["size_matched_copy"]["per_colour_copies"] = {
+                "launches": colors, "bytes": pp["gs_pass_bytes"], "gbs": split_gbs,
+                "fp64_gs_pass_vs_copies": roofline["fp64_gs_pass"]["achieved"] / split_gbs}
 
     # the reference's own FP64 solve of the same workload: the CPU baseline
     # and the oracle every field here is stated against (measured once per

@@ -812,7 +812,16 @@ void AmgHierarchy::buildDevice(const FinestDevice& in, const SolverOptions& opt)
       coarseInv_ = (double*)arena_.alloc(size_class(sizeof(double) * nn));
       if (dominant) {
         dev::dense_from_sell(c.view64(), c.nSlices, coarseInv_, st);
-        dev::gauss_jordan_inverse_dominant(c.n, coarseInv_, gjScratch, st);
+        // a symmetric level (a diffusion operator's Galerkin level) takes
+        // the symmetric sweep: half the products
+        CUDA_OK(cudaMemsetAsync(flags + 2, 0, sizeof(int), st));
+        dev::dense_symmetry_check(c.n, coarseInv_, flags + 2, st);
+        CUDA_OK(cudaMemcpyAsync(hflags, flags + 2, sizeof(int), cudaMemcpyDeviceToHost, st));
+        CUDA_OK(cudaStreamSynchronize(st));
+        if (hflags[0] == 0)
+          dev::gauss_jordan_inverse_symmetric(c.n, coarseInv_, gjScratch, st);
+        else
+          dev::gauss_jordan_inverse_dominant(c.n, coarseInv_, gjScratch, st);
       } else {
         double* dA = (double*)arena_.alloc(size_class(sizeof(double) * nn));
         dev::dense_from_sell(c.view64(), c.nSlices, dA, st);

@@ -1382,13 +1382,15 @@ __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
-// D: shared memory of 2 x kGdB x (kGdB + 1) doubles (double-buffered block)
-__device__ void gjd_invert_block(int ld, int k0, int nb, const double* R, double* Dout, int* status,
+// The inverse of the nb x nb block src[r * stride + c] (padded to kGdB with
+// the identity) into Dout; D: shared memory of 2 x kGdB x (kGdB + 1)
+// doubles (double-buffered block)
+__device__ void gjd_invert_block(const double* src, size_t stride, int nb, double* Dout, int* status,
                                  double (*D)[kGdB][kGdB + 1]) {
   const int tid = threadIdx.x, nt = blockDim.x;
   for (int e = tid; e < kGdB * kGdB; e += nt) {
     const int r = e / kGdB, c = e % kGdB;
-    D[0][r][c] = (r < nb && c < nb) ? __ldcg(R + (size_t)r * ld + k0 + c) : (r == c ? 1.0 : 0.0);
+    D[0][r][c] = (r < nb && c < nb) ? __ldcg(src + (size_t)r * stride + c) : (r == c ? 1.0 : 0.0);
   }
   __syncthreads();
   int cur = 0;
@@ -1427,10 +1429,10 @@ __global__ void k_gjd_extract(int n, int ld, int k0, int nb, const double* __res
   }
 }
 
-__global__ void __launch_bounds__(256) k_gjd_first(int ld, int nb, const double* __restrict__ R, double* Dout,
-                                                   int* status) {
+__global__ void __launch_bounds__(256) k_gjd_first(const double* __restrict__ src, size_t stride, int nb,
+                                                   double* Dout, int* status) {
   __shared__ double D[2][kGdB][kGdB + 1];
-  gjd_invert_block(ld, 0, nb, R, Dout, status, D);
+  gjd_invert_block(src, stride, nb, Dout, status, D);
 }
 
 // Rp[t][j] = sum_u D[t][u] R[u][j]: the panel's new pivot rows; one CTA
@@ -1459,10 +1461,17 @@ __global__ void __launch_bounds__(256) k_gjd_rows(int ld, int nb, const double* 
   }
 }
 
-// One panel [k0, k0 + nb) over the whole matrix in 64 x 64 tiles; grid
-// (ceil(n / 64), ceil(n / 64)), 256 threads. Also fills Cn / Rn with the
-// next panel's [k1, k1 + nb1) columns / rows and, in the launch's last CTA,
+// One panel [k0, k0 + nb) over the whole matrix in 64 x 64 tiles, 256
+// threads. Unsymmetric (Sym = false): grid (ceil(n / 64), ceil(n / 64)),
+// the Gauss-Jordan sweep; fills Cn / Rn with the next panel's [k1, k1 +
+// nb1) columns / rows. Symmetric (Sym = true): one CTA per tile on or above
+// the diagonal (grid T (T + 1) / 2, T = ceil(n / 64)), the sweep operator
+// (pivot block -D^-1, panel columns C D^-1 unnegated), which keeps the
+// matrix symmetric; Cn gets the next panel's columns from the column strip
+// and, transposed, from the row strip of the off-diagonal tiles (Rn is not
+// used). In both the launch's last CTA inverts the next pivot block into
 // Dnext. *ticket is 0 on entry and left 0.
+template <bool Sym>
 __global__ void __launch_bounds__(256, 3) k_gjd_update(int n, int ld, int k0, int nb, double* __restrict__ A,
                                                     const double* __restrict__ C, const double* __restrict__ Rp,
                                                     const double* __restrict__ Dinv, double* __restrict__ Cn,
@@ -1475,7 +1484,19 @@ __global__ void __launch_bounds__(256, 3) k_gjd_update(int n, int ld, int k0, in
   __shared__ __align__(16) double Ds[kGdB][kGdB + kGdPad];
   __shared__ bool last;
   const int tid = threadIdx.x;
-  const int i0 = blockIdx.y * kGdT, j0 = blockIdx.x * kGdT;
+  int bi = blockIdx.y, bj = blockIdx.x;
+  if (Sym) {
+    // the p-th tile of the upper triangle, row by row
+    const int T = (n + kGdT - 1) / kGdT;
+    int p = blockIdx.x;
+    bi = 0;
+    while (p >= T - bi) {
+      p -= T - bi;
+      bi++;
+    }
+    bj = bi + p;
+  }
+  const int i0 = bi * kGdT, j0 = bj * kGdT;
   const int ty = tid >> 4, tx = tid & 15;
   // does the tile meet the panel's rows / columns?
   const bool rowsK = i0 < k0 + nb && i0 + kGdT > k0;
@@ -1542,17 +1563,22 @@ __global__ void __launch_bounds__(256, 3) k_gjd_update(int n, int ld, int k0, in
       const bool jK = j >= k0 && j < k0 + nb;
       double v = acc[a][b];
       if (iK && jK) {
-        v = Ds[i - k0][j - k0];
+        v = Sym ? -Ds[i - k0][j - k0] : Ds[i - k0][j - k0];
       } else if (iK) {
         v = Rs[i - k0][cix];
       } else if (jK) {
         double s = 0.0;
         for (int t = 0; t < kGdB; t++) s = __fma_rn(Cs[r][t], Ds[t][j - k0], s);
-        v = -s;
+        v = Sym ? s : -s;
       }
       A[(size_t)i * n + j] = v;
       if (j >= k1 && j < k1 + nb1) Cn[(size_t)i * kGdB + (j - k1)] = v;
-      if (i >= k1 && i < k1 + nb1) Rn[(size_t)(i - k1) * ld + j] = v;
+      if (i >= k1 && i < k1 + nb1) {
+        if (!Sym)
+          Rn[(size_t)(i - k1) * ld + j] = v;
+        else if (bi != bj)  // the diagonal tile's own column strip covers it
+          Cn[(size_t)j * kGdB + (i - k1)] = v;
+      }
     }
   }
   if (nb1 <= 0) return;  // the last panel: no next block to invert
@@ -1568,8 +1594,86 @@ __global__ void __launch_bounds__(256, 3) k_gjd_update(int n, int ld, int k0, in
   __syncthreads();
   if (!last) return;
   __threadfence();
-  gjd_invert_block(ld, k1, nb1, Rn, Dnext, status, reinterpret_cast<double(*)[kGdB][kGdB + 1]>(&Cs[0][0]));
+  double(*ws)[kGdB][kGdB + 1] = reinterpret_cast<double(*)[kGdB][kGdB + 1]>(&Cs[0][0]);
+  if (Sym)
+    gjd_invert_block(Cn + (size_t)k1 * kGdB, kGdB, nb1, Dnext, status, ws);
+  else
+    gjd_invert_block(Rn + k1, (size_t)ld, nb1, Dnext, status, ws);
   if (tid == 0) *ticket = 0u;
+}
+
+// Symmetric sweep: C[j * kGdB + t] = A[j][t] (t < nb; 0 beyond)
+__global__ void k_gjs_extract(int n, int nb, const double* __restrict__ A, double* __restrict__ C) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  for (int t = 0; t < kGdB; t++) C[(size_t)j * kGdB + t] = t < nb ? A[(size_t)j * n + t] : 0.0;
+}
+
+// Symmetric sweep: the pivot rows Rp[t][j] = sum_u D[t][u] A[K + u][j], with
+// A[K + u][j] = C[j][u] by symmetry; one CTA (256 threads) per 32 columns
+__global__ void __launch_bounds__(256) k_gjs_rows(int ld, int nb, const double* __restrict__ C,
+                                                  const double* __restrict__ Dinv, double* __restrict__ Rp) {
+  __shared__ double D[kGdB][kGdB + 1];
+  __shared__ double Ct[kGdB][kGdB + 1];  // Ct[c][u] = C[j0 + c][u]
+  const int tid = threadIdx.x, c = tid & 31, w = tid >> 5;
+  const int j0 = blockIdx.x * kGdB;
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    const int rr = w + 8 * q;
+    Ct[rr][c] = C[(size_t)(j0 + rr) * kGdB + c];
+    D[rr][c] = Dinv[rr * kGdB + c];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    const int t = w + 8 * q;
+    double acc = 0.0;
+#pragma unroll
+    for (int u = 0; u < kGdB; u++) acc = __fma_rn(D[t][u], u < nb ? Ct[c][u] : 0.0, acc);
+    Rp[(size_t)t * ld + j0 + c] = t < nb ? acc : 0.0;
+  }
+}
+
+// Symmetric sweep, last step: the upper triangle holds -A^-1; negate it and
+// mirror it to the lower triangle (32 x 32 tiles on and above the diagonal,
+// grid T (T + 1) / 2 with T = ceil(n / 32), block 32 x 8). Each CTA reads
+// only its own upper tile and writes it and its mirror, so no two CTAs
+// touch the same entry.
+__global__ void __launch_bounds__(256) k_gjs_finish(int n, double* A) {
+  __shared__ double S[32][33];
+  const int T = (n + 31) / 32;
+  int p = blockIdx.x, bi = 0;
+  while (p >= T - bi) {
+    p -= T - bi;
+    bi++;
+  }
+  const int bj = bi + p;
+  const int i0 = bi * 32, j0 = bj * 32;
+  const int c = threadIdx.x;
+  for (int r = threadIdx.y; r < 32; r += 8) {
+    const int i = i0 + r, j = j0 + c;
+    S[r][c] = (i < n && j < n) ? A[(size_t)i * n + j] : 0.0;
+  }
+  __syncthreads();
+  for (int r = threadIdx.y; r < 32; r += 8) {
+    const int i = i0 + r, j = j0 + c;
+    if (i < n && j < n) A[(size_t)i * n + j] = -(bi == bj && r > c ? S[c][r] : S[r][c]);
+    if (bi != bj) {
+      const int i2 = j0 + r, j2 = i0 + c;  // mirror tile: A[j0 + r][i0 + c] = -S[c][r]
+      if (i2 < n && j2 < n) A[(size_t)i2 * n + j2] = -S[c][r];
+    }
+  }
+}
+
+// *flag = 1 unless |a_ij - a_ji| <= 1e-12 max(|a_ij|, |a_ji|) everywhere
+// (one thread per entry above the diagonal; *flag must be 0 on entry)
+__global__ void k_dense_symmetry(int n, const double* __restrict__ A, int* flag) {
+  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= (long long)n * n) return;
+  const int i = (int)(e / n), j = (int)(e % n);
+  if (j <= i) return;
+  const double a = A[(size_t)i * n + j], b = A[(size_t)j * n + i];
+  if (!(fabs(a - b) <= 1e-12 * fmax(fabs(a), fabs(b)))) atomicExch(flag, 1);
 }
 
 // Look-ahead: after panel p's row swaps, the next panel's columns are
@@ -1652,7 +1756,7 @@ void gauss_jordan_inverse_dominant(int n, double* a, void* scratch, cudaStream_t
   if (n <= 0) return;
   const int nb0 = n < kGdB ? n : kGdB;
   k_gjd_extract<<<ceil_div(n, kBlock), kBlock, 0, st>>>(n, ld, 0, nb0, a, C[0], R[0]);
-  k_gjd_first<<<1, 256, 0, st>>>(ld, nb0, R[0], Dv[0], status);
+  k_gjd_first<<<1, 256, 0, st>>>(R[0], (size_t)ld, nb0, Dv[0], status);
   const dim3 grid(ceil_div(n, kGdT), ceil_div(n, kGdT));
   int cur = 0;
   for (int k0 = 0; k0 < n; k0 += kGdB) {
@@ -1660,10 +1764,42 @@ void gauss_jordan_inverse_dominant(int n, double* a, void* scratch, cudaStream_t
     const int k1 = k0 + nb;
     const int nb1 = n - k1 < kGdB ? n - k1 : kGdB;
     k_gjd_rows<<<ceil_div(n, kGdB), 256, 0, st>>>(ld, nb, R[cur], Dv[cur], Rp);
-    k_gjd_update<<<grid, 256, 0, st>>>(n, ld, k0, nb, a, C[cur], Rp, Dv[cur], C[cur ^ 1], R[cur ^ 1], Dv[cur ^ 1],
-                                       k1, nb1 > 0 ? nb1 : 0, ticket, status);
+    k_gjd_update<false><<<grid, 256, 0, st>>>(n, ld, k0, nb, a, C[cur], Rp, Dv[cur], C[cur ^ 1], R[cur ^ 1],
+                                              Dv[cur ^ 1], k1, nb1 > 0 ? nb1 : 0, ticket, status);
     cur ^= 1;
   }
+}
+void gauss_jordan_inverse_symmetric(int n, double* a, void* scratch, cudaStream_t st) {
+  double* sb = (double*)scratch;
+  const int ld = gjd_ld(n);
+  const size_t pn = (size_t)kGdB * ld;
+  double* C[2] = {sb, sb + pn};
+  double* Rp = sb + 4 * pn;
+  double* Dv[2] = {sb + 5 * pn, sb + 5 * pn + kGdB * kGdB};
+  unsigned* ticket = (unsigned*)(sb + 5 * pn + 2 * kGdB * kGdB);
+  int* status = (int*)gauss_jordan_status(n, scratch);
+  cudaMemsetAsync(status, 0, sizeof(int), st);
+  cudaMemsetAsync(sb, 0, sizeof(double) * (5 * pn + 2 * kGdB * kGdB + 2), st);
+  if (n <= 0) return;
+  const int nb0 = n < kGdB ? n : kGdB;
+  k_gjs_extract<<<ceil_div(n, kBlock), kBlock, 0, st>>>(n, nb0, a, C[0]);
+  k_gjd_first<<<1, 256, 0, st>>>(C[0], (size_t)kGdB, nb0, Dv[0], status);
+  const int T = ceil_div(n, kGdT);
+  int cur = 0;
+  for (int k0 = 0; k0 < n; k0 += kGdB) {
+    const int nb = n - k0 < kGdB ? n - k0 : kGdB;
+    const int k1 = k0 + nb;
+    const int nb1 = n - k1 < kGdB ? n - k1 : kGdB;
+    k_gjs_rows<<<ceil_div(n, kGdB), 256, 0, st>>>(ld, nb, C[cur], Dv[cur], Rp);
+    k_gjd_update<true><<<T * (T + 1) / 2, 256, 0, st>>>(n, ld, k0, nb, a, C[cur], Rp, Dv[cur], C[cur ^ 1], nullptr,
+                                                         Dv[cur ^ 1], k1, nb1 > 0 ? nb1 : 0, ticket, status);
+    cur ^= 1;
+  }
+  const int T32 = ceil_div(n, 32);
+  k_gjs_finish<<<T32 * (T32 + 1) / 2, dim3(32, 8), 0, st>>>(n, a);
+}
+void dense_symmetry_check(int n, const double* a, int* flag, cudaStream_t st) {
+  if (n > 0) k_dense_symmetry<<<ceil_div((long long)n * n, kBlock), kBlock, 0, st>>>(n, a, flag);
 }
 namespace {
 // a (n x n, row-major, zeroed) += the SELL-32 level: one thread per row

@@ -153,6 +153,14 @@ const int* gauss_jordan_status(int n, const void* scratch);
 // matrix `a` by blocked Gauss-Jordan without pivoting: one kernel per panel
 // of 16 pivots. Same scratch and status as gauss_jordan_inverse.
 void gauss_jordan_inverse_dominant(int n, double* a, void* scratch, cudaStream_t st);
+// The same for a symmetric diagonally dominant matrix: the sweep operator,
+// which keeps the matrix symmetric, on the tiles on and above the diagonal
+// only (half the products), then the lower triangle mirrored. Same scratch
+// and status.
+void gauss_jordan_inverse_symmetric(int n, double* a, void* scratch, cudaStream_t st);
+// *flag = 1 unless the dense n x n matrix is symmetric to a relative 1e-12
+// entry by entry (*flag must be 0 on entry)
+void dense_symmetry_check(int n, const double* a, int* flag, cudaStream_t st);
 void cast_d2f(size_t n, const double* a, float* b, cudaStream_t st);
 
 // ---- vector ops ------------------------------------------------------------

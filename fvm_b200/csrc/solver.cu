@@ -208,13 +208,30 @@ void AmgHierarchy::build(std::vector<RefLevel>& levels, int finestLocalSize, con
       for (int k = rl.conn.row[i]; k < rl.conn.row[i + 1]; k++) s += std::fabs(rl.off[k]);
       dominant = rl.diag[i] != 0.0 && s <= std::fabs(rl.diag[i]) * (1.0 + 1e-8);
     }
+    // symmetric to a relative 1e-12 entry by entry (a diffusion operator
+    // and its Galerkin levels): the symmetric sweep, half the products
+    bool symmetric = dominant;
+    for (int i = 0; i < rl.n && symmetric; i++)
+      for (int k = rl.conn.row[i]; k < rl.conn.row[i + 1] && symmetric; k++) {
+        const int j = rl.conn.col[k];
+        bool found = false;
+        for (int q = rl.conn.row[j]; q < rl.conn.row[j + 1]; q++)
+          if (rl.conn.col[q] == i) {
+            found = std::fabs(rl.off[k] - rl.off[q]) <= 1e-12 * std::max(std::fabs(rl.off[k]), std::fabs(rl.off[q]));
+            break;
+          }
+        symmetric = found;
+      }
     gjScratch = arena_.alloc(dev::gauss_jordan_scratch_bytes(c.n));
     coarseInv_ = (double*)arena_.alloc(sizeof(double) * nn);
     CUDA_OK(cudaStreamCreateWithFlags(&gjStream, cudaStreamNonBlocking));
     gjUnpivoted = dominant;
     if (dominant) {
       dev::dense_from_sell(lv_[l].view64(), lv_[l].nSlices, coarseInv_, gjStream);
-      dev::gauss_jordan_inverse_dominant(c.n, coarseInv_, gjScratch, gjStream);
+      if (symmetric)
+        dev::gauss_jordan_inverse_symmetric(c.n, coarseInv_, gjScratch, gjStream);
+      else
+        dev::gauss_jordan_inverse_dominant(c.n, coarseInv_, gjScratch, gjStream);
       return;
     }
     double* dA = (double*)arena_.alloc(sizeof(double) * nn);

@@ -555,20 +555,24 @@ def test_gpu_inverse_direct_single_level(n):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("symmetric", [False, True], ids=["unsymmetric", "symmetric"])
 @pytest.mark.parametrize("n", [1000, 2294, 3000, 4096])
-def test_gpu_inverse_dominant_single_level(n):
+def test_gpu_inverse_dominant_single_level(n, symmetric):
     """A diagonally dominant single level (the shape of every diffusion
     coarsest level) takes the unpivoted blocked Gauss-Jordan: panels of 32
-    pivots, the last one partial for all sizes here but 4096. One cycle is an
-    exact solve; the solution is compared with numpy's dense solve."""
+    pivots, the last one partial for all sizes here but 4096; a symmetric
+    one the symmetric sweep over the tiles on and above the diagonal. One
+    cycle is an exact solve; the solution is compared with numpy's dense
+    solve."""
     rng = np.random.default_rng(7 * n)
     nx = int(np.ceil(np.sqrt(n)))
     rows = [[] for _ in range(n)]
     for i in range(n):
         for j in (i + 1, i + nx, i + 3 * nx + 5):
             if j < n and (j != i + 1 or (i + 1) % nx):
-                rows[i].append((j, rng.uniform(-1.0, 1.0)))
-                rows[j].append((i, rng.uniform(-1.0, 1.0)))
+                v = rng.uniform(-1.0, 1.0)
+                rows[i].append((j, v))
+                rows[j].append((i, v if symmetric else rng.uniform(-1.0, 1.0)))
     row = np.zeros(n + 1, np.int32)
     row[1:] = np.cumsum([len(r) for r in rows])
     col = np.array([j for r in rows for j, _ in r], np.int32)

@@ -52,6 +52,7 @@ class LinearOptions(ctypes.Structure):
         ("planEllRows", ctypes.c_int),
         ("chebyshevDegree", ctypes.c_int),
         ("chebyshevFraction", ctypes.c_double),
+        ("gsReverse", ctypes.c_int),
     ]
 
 

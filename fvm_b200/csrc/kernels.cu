@@ -495,7 +495,7 @@ __global__ void k_cg_alpha(int np, const double* __restrict__ p, const double* r
 
 // x += -alpha p; r += -alpha q; block partials of |r|
 __global__ void k_cg_update(int n, const double* alpha, const double* __restrict__ p, const double* __restrict__ q,
-                            double* x, double* r, double* partials) {
+                            double* x, double* r, double* partials, float* rF) {
   FVM_PDL();
   const double am = -1.0 * alpha[0];
   double l1 = 0.0;
@@ -503,6 +503,7 @@ __global__ void k_cg_update(int n, const double* alpha, const double* __restrict
     x[i] = x[i] + am * p[i];
     const double ri = r[i] + am * q[i];
     r[i] = ri;
+    if (rF) rF[i] = (float)ri;
     l1 += fabs(ri);
   }
   l1 = block_sum(l1);
@@ -1302,8 +1303,8 @@ void cg_alpha(int np, const double* partials, const double* rho, double* alpha, 
   pdl_launch(k_cg_alpha, 1, 1024, st, np, partials, rho, alpha);
 }
 void cg_update(int n, const double* alpha, const double* p, const double* q, double* x, double* r, double* partials,
-               cudaStream_t st) {
-  pdl_launch(k_cg_update, vec_blocks(n), kBlock, st, n, alpha, p, q, x, r, partials);
+               cudaStream_t st, float* rF) {
+  pdl_launch(k_cg_update, vec_blocks(n), kBlock, st, n, alpha, p, q, x, r, partials, rF);
 }
 template <class T>
 void restrict_sum(int nc, const int* c2fRow, const int* c2fCol, const T* r, T* bc, cudaStream_t st) {

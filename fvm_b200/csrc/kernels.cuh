@@ -91,9 +91,10 @@ void cg_beta(int np, const double* partials, double* rho, double* rhoPrev, doubl
 // *alpha = *rho / (sum of np partials)
 void cg_alpha(int np, const double* partials, const double* rho, double* alpha, cudaStream_t st);
 // x += -alpha p, r += -alpha q, and per-block L1 partials of the new r
-// (vec_blocks(n) of them)
+// (vec_blocks(n) of them); rF (optional) gets the new r in FP32, the
+// right-hand side of the next FP32 cycle
 void cg_update(int n, const double* alpha, const double* p, const double* q, double* x, double* r, double* partials,
-               cudaStream_t st);
+               cudaStream_t st, float* rF = nullptr);
 // number of L1 partials residual() writes for a level (one per block)
 int residual_partials(int nSlices, int n, int ellWidth);
 

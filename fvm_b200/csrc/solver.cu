@@ -673,8 +673,9 @@ void AmgHierarchy::sweeps(int nSweeps, int l, cudaStream_t st) {
         for (int c = 0; c < C; c++)
           dev::gs_color<T>(a, d.colorSliceStart[c], d.colorSliceStart[c + 1], x, b, st, d.plan);
         // reverse pass; its first colour would repeat the last update exactly
-        for (int c = C - 2; c >= 0; c--)
-          dev::gs_color<T>(a, d.colorSliceStart[c], d.colorSliceStart[c + 1], x, b, st, d.plan);
+        if (opt_.gsReverse)
+          for (int c = C - 2; c >= 0; c--)
+            dev::gs_color<T>(a, d.colorSliceStart[c], d.colorSliceStart[c + 1], x, b, st, d.plan);
       }
     } else {
       T* t = vec_tmp<T>(d);
@@ -789,7 +790,8 @@ double AmgHierarchy::cycleBytes() const {
       // a sweep: two damped-Jacobi passes, or forward + reverse over the
       // colours (2C - 1 colour passes, C of which make one pass)
       const bool gsPasses = opt_.smootherType == kGaussSeidel && !dampedLevel(l, d.n) && d.nColors > 0;
-      const double perSweep = gsPasses ? (2.0 * d.nColors - 1.0) / d.nColors : 2.0;
+      const double perSweep =
+          gsPasses ? (opt_.gsReverse ? (2.0 * d.nColors - 1.0) / d.nColors : 1.0) : 2.0;
       total += sweeps * perSweep * pass;
     }
     if (l + 1 < L) {
@@ -815,7 +817,7 @@ int AmgHierarchy::kernelsPerCycle() const {
     }
     const int perSweep = chebyshevLevel(l) ? (int)chebC1_.size()
                          : (opt_.smootherType == kGaussSeidel && !dampedLevel(l, d.n))
-                             ? (opt_.ordering == kSequential ? 2 : 2 * d.nColors - 1)
+                             ? (opt_.ordering == kSequential ? 2 : opt_.gsReverse ? 2 * d.nColors - 1 : d.nColors)
                              : 2;
     k += perSweep * (opt_.nPreSweeps + opt_.postSweeps(l));
     if (l + 1 < L) k += 2;  // fused residual + restriction, prolongation
@@ -1347,7 +1349,8 @@ SolveReport LinearSolve::solveCG(cudaStream_t st) {
   double* Q = work_ + 4 * (size_t)n_;
   double* B = work_ + 5 * (size_t)n_;
   const bool flexible = o.preconditioner == kPrecAMG &&
-                        (o.precision == kMixed || o.nPreSweeps != o.nPostSweeps || o.cycleType != kVCycle);
+                        (o.precision == kMixed || o.nPreSweeps != o.nPostSweeps || o.cycleType != kVCycle ||
+                         !o.gsReverse || o.chebyshevDegree > 0);
   SolveReport rep;
   // the whole solve on the device when nothing needs the host between
   // iterations (no learned step, no printing)
@@ -1375,6 +1378,12 @@ SolveReport LinearSolve::solveCG(cudaStream_t st) {
   // p.q; alpha; the x and r updates with |r|.
   const bool fused = o.preconditioner == kPrecAMG;
   const bool mixedCycle = o.precision == kMixed;
+  // the FP32 cycle's right-hand side: r in FP32, written by each update
+  float* rF = fused && mixedCycle ? d.bF : nullptr;
+  if (rF) {
+    dev::convert_d2f(n_, R, rF, st);
+    launches += 1;
+  }
   for (int i = 0; i < o.nMaxIterations; i++) {
     // learned post-correction of the preconditioner (flexible CG): after the
     // cycle's z1, the network corrects the residual r + A z1 that z1 leaves,
@@ -1410,7 +1419,7 @@ SolveReport LinearSolve::solveCG(cudaStream_t st) {
         dev::xpby_dev(n_, Z, scal_ + kBeta, P, st);
         dev::spmv_dot(d.view64(), d.nSlices, P, Q, partials2_, st);
         dev::cg_alpha(dev::spmv_dot_blocks(d.view64(), d.nSlices), partials2_, scal_ + kRho, scal_ + kAlpha, st);
-        dev::cg_update(n_, scal_ + kAlpha, P, Q, X, R, partials_, st);
+        dev::cg_update(n_, scal_ + kAlpha, P, Q, X, R, partials_, st, rF);
         dev::sum_partials(dev::vec_blocks(n_), partials_, scal_ + kNorm, st);
         CUDA_OK(cudaMemcpyAsync(hostScal_, scal_ + kNorm, sizeof(double), cudaMemcpyDeviceToHost, st));
         CUDA_OK(cudaMemcpyAsync(hostScal_ + 1, scal_ + kLsBefore, sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -1419,7 +1428,10 @@ SolveReport LinearSolve::solveCG(cudaStream_t st) {
       launches += 6;
     } else if (fused) {
       run(g1_, st, [&] {
-        h_.applyCycle(R, st);
+        if (mixedCycle)
+          h_.runCycle<float>(st, true);  // on rF, level 0's FP32 right-hand side
+        else
+          h_.applyCycle(R, st);
         if (mixedCycle)
           dev::cg_take_z<float>(n_, d.xF, R, Z, partials2_, st);
         else
@@ -1428,7 +1440,7 @@ SolveReport LinearSolve::solveCG(cudaStream_t st) {
         dev::xpby_dev(n_, Z, scal_ + kBeta, P, st);
         dev::spmv_dot(d.view64(), d.nSlices, P, Q, partials2_, st);
         dev::cg_alpha(dev::spmv_dot_blocks(d.view64(), d.nSlices), partials2_, scal_ + kRho, scal_ + kAlpha, st);
-        dev::cg_update(n_, scal_ + kAlpha, P, Q, X, R, partials_, st);
+        dev::cg_update(n_, scal_ + kAlpha, P, Q, X, R, partials_, st, rF);
         dev::sum_partials(dev::vec_blocks(n_), partials_, scal_ + kNorm, st);
         CUDA_OK(cudaMemcpyAsync(hostScal_, scal_ + kNorm, sizeof(double), cudaMemcpyDeviceToHost, st));
       });
@@ -1520,6 +1532,7 @@ bool LinearSolve::buildCGLoop(cudaStream_t st, bool flexible) {
       dev::copy_d(n_, d.b, B, st);
       dev::residual<double>(d.view64(), d.nSlices, X, B, R, nullptr, st);
       norm_into(R, scal_ + kNorm, st);
+      if (mixedCycle) dev::convert_d2f(n_, R, d.bF, st);  // the FP32 cycle's right-hand side
       k_cg_loop_init<<<1, 1, 0, st>>>(scal_, loopInt_, history_, o.absoluteTolerance, o.nMaxIterations, h);
     } catch (const Error&) {
       ok = false;
@@ -1552,7 +1565,12 @@ bool LinearSolve::buildCGLoop(cudaStream_t st, bool flexible) {
   ok = ok && cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0, mode) == cudaSuccess;
   if (ok) {
     try {
-      h_.applyCycle(R, st);
+      // the FP32 cycle runs on level 0's bF, which the prologue and each
+      // update write (r in FP32)
+      if (mixedCycle)
+        h_.runCycle<float>(st, true);
+      else
+        h_.applyCycle(R, st);
       if (mixedCycle)
         dev::cg_take_z<float>(n_, d.xF, R, Z, partials2_, st);
       else
@@ -1561,7 +1579,7 @@ bool LinearSolve::buildCGLoop(cudaStream_t st, bool flexible) {
       dev::xpby_dev(n_, Z, scal_ + kBeta, P, st);
       dev::spmv_dot(d.view64(), d.nSlices, P, Q, partials2_, st);
       dev::cg_alpha(dev::spmv_dot_blocks(d.view64(), d.nSlices), partials2_, scal_ + kRho, scal_ + kAlpha, st);
-      dev::cg_update(n_, scal_ + kAlpha, P, Q, X, R, partials_, st);
+      dev::cg_update(n_, scal_ + kAlpha, P, Q, X, R, partials_, st, mixedCycle ? d.bF : nullptr);
       dev::sum_partials(dev::vec_blocks(n_), partials_, scal_ + kNorm, st);
       k_cg_loop_check<<<1, 1, 0, st>>>(scal_, loopInt_, history_, o.relativeTolerance, o.absoluteTolerance,
                                        o.nMaxIterations, h);

@@ -68,6 +68,10 @@ struct SolverOptions {
   // Gershgorin bound of the spectrum
   int chebyshevDegree = 0;
   double chebyshevFraction = 0.3;
+  // a multicolour Gauss-Seidel sweep is forward + reverse over the colours
+  // (the reference's sweep, AMG.cpp:57-61); false: forward only (C colour
+  // passes instead of 2C - 1; a nonsymmetric preconditioner, for flexible CG)
+  bool gsReverse = true;
   // Build the coarse levels on the GPU (parallel pairwise matching and
   // Galerkin kernels) instead of the reference's sequential greedy walk on
   // the host; coarse levels then smooth with damped Jacobi. The hierarchy is

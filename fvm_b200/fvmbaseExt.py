@@ -198,6 +198,7 @@ class AMG(LinearSolver):
         # finest-level Chebyshev smoother (0: multicolour Gauss-Seidel)
         self.chebyshevDegree = d.chebyshevDegree
         self.chebyshevFraction = d.chebyshevFraction
+        self.gsReverse = bool(d.gsReverse)  # Gauss-Seidel sweep: forward + reverse (reference) or forward only
         self.setupOnDevice = bool(d.setupOnDevice)
         self.matchRounds = d.matchRounds
         self.matchBeta = d.matchBeta
@@ -243,6 +244,7 @@ class AMG(LinearSolver):
         o.planEllRows = int(self.planEllRows)
         o.chebyshevDegree = int(self.chebyshevDegree)
         o.chebyshevFraction = float(self.chebyshevFraction)
+        o.gsReverse = int(bool(self.gsReverse))
         o.setupOnDevice = int(bool(self.setupOnDevice))
         o.matchRounds = int(self.matchRounds)
         o.matchBeta = float(self.matchBeta)

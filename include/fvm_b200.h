@@ -95,6 +95,9 @@ typedef struct fvm_linear_options {
                                degree in D^-1 A per sweep (one launch per degree) instead of
                                multicolour Gauss-Seidel (0: Gauss-Seidel, the reference's smoother) */
   double chebyshevFraction; /* its interval [fraction * b, b], b the Gershgorin bound (default 0.3) */
+  int gsReverse;            /* 1: a multicolour Gauss-Seidel sweep is forward + reverse over the
+                               colours (the reference's sweep); 0: forward only (a nonsymmetric
+                               preconditioner: for flexible CG or standalone AMG) */
 } fvm_linear_options;
 
 /* ThermalModelOptions (fvmbase/ThermalBC.h:33-67) + volume-condition constants */

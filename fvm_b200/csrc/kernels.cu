@@ -1585,7 +1585,11 @@ __global__ void __launch_bounds__(256, 3) k_gjd_update(int n, int ld, int k0, in
   if (nb1 <= 0) return;  // the last panel: no next block to invert
   // the last CTA to finish inverts the next panel's pivot block: the
   // barrier orders the CTA's writes before thread 0's fence, which makes
-  // them visible device-wide before its ticket increment
+  // them visible device-wide before its ticket increment (fences are
+  // cumulative in the PTX memory model; the CUDA cooperative-groups grid
+  // barrier relies on the same CTA barrier + one-thread fence pattern).
+  // A fence in every thread measured one membar stall per issued
+  // instruction here.
   __syncthreads();
   if (tid == 0) {
     __threadfence();

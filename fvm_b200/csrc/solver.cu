@@ -670,7 +670,11 @@ void AmgHierarchy::sweeps(int nSweeps, int l, cudaStream_t st) {
         dev::gs_sequential<T>(a, x, b, true, st);
       } else {
         const int C = d.nColors;
-        for (int c = 0; c < C; c++)
+        // a symmetric sweep ends with colour 0, whose rows then agree with
+        // their (unchanged) neighbours: the next sweep's colour-0 pass would
+        // write bitwise the same values, so it starts at colour 1
+        const int c0 = (s > 0 && opt_.gsReverse) ? 1 : 0;
+        for (int c = c0; c < C; c++)
           dev::gs_color<T>(a, d.colorSliceStart[c], d.colorSliceStart[c + 1], x, b, st, d.plan);
         // reverse pass; its first colour would repeat the last update exactly
         if (opt_.gsReverse)
@@ -755,6 +759,13 @@ void AmgHierarchy::apply(const double* r, double* z, cudaStream_t st) {
   }
 }
 
+int AmgHierarchy::colourPasses(int colors, int nSweeps) const {
+  if (nSweeps <= 0) return 0;
+  if (!opt_.gsReverse) return nSweeps * colors;
+  // forward + reverse (2C - 1 passes), later sweeps without their first pass
+  return nSweeps * (2 * colors - 1) - (nSweeps - 1);
+}
+
 double AmgHierarchy::fineSweepBytes() const {
   // one pass over every row of level 0: b, diag, x (read+write) per row,
   // col + val per stored entry
@@ -786,13 +797,13 @@ double AmgHierarchy::cycleBytes() const {
       const int steps = sweeps * (int)chebC1_.size();
       total += steps * (d.n * 6.0 * vb + d.entries * (4.0 + vb)) - sweeps * d.n * vb;
       if (steps & 1) total += 2.0 * vb * d.n;
+    } else if (opt_.smootherType == kGaussSeidel && !dampedLevel(l, d.n) && d.nColors > 0) {
+      // colour passes of the pre- and post-smoothing (C of which make one
+      // pass over the level)
+      total += (double)(colourPasses(d.nColors, opt_.nPreSweeps) + colourPasses(d.nColors, opt_.postSweeps(l))) /
+               d.nColors * pass;
     } else {
-      // a sweep: two damped-Jacobi passes, or forward + reverse over the
-      // colours (2C - 1 colour passes, C of which make one pass)
-      const bool gsPasses = opt_.smootherType == kGaussSeidel && !dampedLevel(l, d.n) && d.nColors > 0;
-      const double perSweep =
-          gsPasses ? (opt_.gsReverse ? (2.0 * d.nColors - 1.0) / d.nColors : 1.0) : 2.0;
-      total += sweeps * perSweep * pass;
+      total += sweeps * 2.0 * pass;  // a sweep: two (damped) Jacobi passes
     }
     if (l + 1 < L) {
       const DevLevel& c = lv_[l + 1];
@@ -815,11 +826,13 @@ int AmgHierarchy::kernelsPerCycle() const {
       k += 1;
       continue;
     }
-    const int perSweep = chebyshevLevel(l) ? (int)chebC1_.size()
-                         : (opt_.smootherType == kGaussSeidel && !dampedLevel(l, d.n))
-                             ? (opt_.ordering == kSequential ? 2 : opt_.gsReverse ? 2 * d.nColors - 1 : d.nColors)
-                             : 2;
-    k += perSweep * (opt_.nPreSweeps + opt_.postSweeps(l));
+    const int sw = opt_.nPreSweeps + opt_.postSweeps(l);
+    if (chebyshevLevel(l))
+      k += (int)chebC1_.size() * sw;
+    else if (opt_.smootherType == kGaussSeidel && !dampedLevel(l, d.n) && opt_.ordering != kSequential)
+      k += colourPasses(d.nColors, opt_.nPreSweeps) + colourPasses(d.nColors, opt_.postSweeps(l));
+    else
+      k += 2 * sw;
     if (l + 1 < L) k += 2;  // fused residual + restriction, prolongation
   }
   return k;

@@ -255,6 +255,8 @@ class AmgHierarchy {
   // algorithmic bytes moved by one cycle (for roofline reporting)
   double cycleBytes() const;
   double fineSweepBytes() const;  // one GS pass over all colours of level 0
+  // colour launches of nSweeps multicolour Gauss-Seidel sweeps in a row
+  int colourPasses(int colors, int nSweeps) const;
   int kernelsPerCycle() const;
 
  private:

@@ -258,9 +258,11 @@ def solver_for(variant: str, inner_rel: float):
         amg.nPreSweeps = 0
         amg.nPostSweeps = 2
         if not HOST_SETUP:
-            # GPU-built levels: pairs of pairs (aggregates of about 4 rows),
+            # GPU-built levels: pairs of pairs (aggregates of about 4 rows)
+            # of neighbours at least half as strong as a row's strongest,
             # one damped-Jacobi sweep on each level below the finest
             amg.matchPasses = 2
+            amg.matchBeta = 0.5
             amg.coarsePostSweeps = 1
     if variant in ("plain-cg", "mixed", "learned"):
         cg = fvmbaseExt.CG()
@@ -1008,8 +1010,9 @@ def main():
                 "workload": desc,
                 "cells": n_cells,
                 "solver": ("mixed+learned: flexible CG (FP64, fused iteration, each linear solve one CUDA graph) "
-                           "preconditioned by an FP32 AMG V(0,2) on a hierarchy built on the GPU (pairs of pairs) -- "
-                           "two multicolour GS sweeps on the finest level, one damped-Jacobi sweep (w=2/3) below, "
+                           "preconditioned by an FP32 AMG V(0,2) on a hierarchy built on the GPU (pairs of pairs, "
+                           "matchBeta 0.5) -- two multicolour GS sweeps on the finest level, one damped-Jacobi sweep "
+                           "(w=2/3) below, "
                            "dense FP64 inverse (FP32 copy) on the coarsest level (<= 4096 rows) -- with the learned "
                            "post-correction of each preconditioner application when its measured residual reduction "
                            "pays; plain: standalone FP64 AMG V(1,1) on the reference's aggregation, multicolour GS on "

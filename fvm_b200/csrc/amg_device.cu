@@ -290,6 +290,7 @@ __global__ void __launch_bounds__(32 * kGalWarps) k_galerkin(LevelRows a, int nc
                                                              double* cdiag, float* cdiagF) {
   __shared__ int sJ[kGalWarps][kGalerkinCap];
   __shared__ double sV[kGalWarps][kGalerkinCap];
+  __shared__ int sOff[kGalWarps][32], sBase[kGalWarps][32], sRow[kGalWarps][32];
   const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int I = blockIdx.x * kGalWarps + wid;
   if (I >= nc) return;  // the whole warp leaves together
@@ -297,24 +298,50 @@ __global__ void __launch_bounds__(32 * kGalWarps) k_galerkin(LevelRows a, int nc
   double* V = sV[wid];
   const int f0 = c2fRow[I], f1 = c2fRow[I + 1];
   // every entry of the aggregate's fine rows, fine rows ascending, entries
-  // in stored order; J = coarse column (-1: padding)
+  // in stored order; J = coarse column (-1: padding). Up to 32 fine rows at
+  // a time: each lane looks up one row's range, a warp scan places the rows,
+  // and the lanes then gather all their entries at once.
   int L = 0;
   bool over = false;
-  for (int q = f0; q < f1; q++) {
-    const int f = c2fCol[q];
-    int base, w;
-    row_range(a, f, base, w);
-    if (L + w > kGalerkinCap) {
+  for (int q0 = f0; q0 < f1; q0 += 32) {
+    const int nq = min(32, f1 - q0);
+    int base = 0, w = 0, f = -1;
+    if (lane < nq) {
+      f = c2fCol[q0 + lane];
+      row_range(a, f, base, w);
+    }
+    int incl = w;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(kFull, incl, o);
+      if (lane >= o) incl += t;
+    }
+    const int tot = __shfl_sync(kFull, incl, 31);
+    if (L + tot > kGalerkinCap) {
       over = true;
       break;
     }
-    for (int k = lane; k < w; k += 32) {
-      const int j = a.cols[base + 32 * k];
-      const double v = a.vals[base + 32 * k];
-      J[L + k] = (j == f || v == 0.0) ? -1 : ci[j];
-      V[L + k] = v;
+    sOff[wid][lane] = incl - w;
+    sBase[wid][lane] = base;
+    sRow[wid][lane] = f;
+    __syncwarp();
+    for (int e = lane; e < tot; e += 32) {
+      // the last row q < nq whose range starts at or before e
+      int lo = 0, hi = nq - 1;
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (sOff[wid][mid] <= e)
+          lo = mid;
+        else
+          hi = mid - 1;
+      }
+      const int idx = sBase[wid][lo] + 32 * (e - sOff[wid][lo]);
+      const int j = a.cols[idx];
+      const double v = a.vals[idx];
+      J[L + e] = (j == sRow[wid][lo] || v == 0.0) ? -1 : ci[j];
+      V[L + e] = v;
     }
-    L += w;
+    __syncwarp();
+    L += tot;
   }
   __syncwarp();
   if (over) {
@@ -712,6 +739,10 @@ void AmgHierarchy::buildDevice(const FinestDevice& in, const SolverOptions& opt)
     c.sliceRow = (int*)arena_.alloc(size_class(sizeof(int) * nSlices));
     c.sliceRows = (int*)arena_.alloc(size_class(sizeof(int) * nSlices));
     c.rowSlice = (int*)arena_.alloc(size_class(sizeof(int) * nc));
+    // the fill writes every row's entries and padding; the lanes of the last
+    // slice past the last row keep these (column 0) so that no index in the
+    // level is undefined
+    CUDA_OK(cudaMemsetAsync(c.cols, 0, sizeof(int) * e1, st));
     dev::galerkin_fill(af, nc, ci, fine.c2fRow, fine.c2fCol, sliceOff, c.cols, c.vals, c.valsF, c.diag, c.diagF,
                        st);
     dev::slice_meta_fill(nc, sliceOff, c.meta, c.sliceRow, c.sliceRows, c.rowSlice, flags + 1, st);

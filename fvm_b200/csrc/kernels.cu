@@ -516,9 +516,11 @@ __global__ void k_cg_update(int n, const double* alpha, const double* __restrict
 // flight per step; the group's products are then added to the row sum in
 // stored order (k ascending), one shuffle per product, so the sum rounds
 // exactly as row_sum's does.
+// Lanes of rows past the slice's last row (live = false) take part in the
+// shuffles but load nothing: their slots of the slice hold no entries.
 template <class T, int TPR>
-__device__ __forceinline__ T row_sum_tpr(const SellView<T>& a, const int4 m, int l, const T* __restrict__ x,
-                                         T sum) {
+__device__ __forceinline__ T row_sum_tpr(const SellView<T>& a, const int4 m, int l, bool live,
+                                         const T* __restrict__ x, T sum) {
   constexpr int C = 4;
   const int lane = threadIdx.x & 31, sub = lane & (TPR - 1), g0 = lane & ~(TPR - 1);
   const int o = m.z + l, w = m.w;
@@ -528,8 +530,9 @@ __device__ __forceinline__ T row_sum_tpr(const SellView<T>& a, const int4 m, int
 #pragma unroll
     for (int q = 0; q < C; q++) {
       const int k = k0 + q * TPR + sub;
-      c[q] = k < w ? a.cols[o + (k << 5)] : 0;
-      v[q] = k < w ? a.vals[o + (k << 5)] : T(0);
+      const bool ok = live && k < w;
+      c[q] = ok ? a.cols[o + (k << 5)] : 0;
+      v[q] = ok ? a.vals[o + (k << 5)] : T(0);
     }
 #pragma unroll
     for (int q = 0; q < C; q++) p[q] = v[q] * x[c[q]];
@@ -562,7 +565,7 @@ __global__ void __launch_bounds__(BLOCK) k_gs_color_tpr(SellView<T> a, int s0, i
   const int4 m = a.meta[s];
   const bool live = l < m.y;
   const int i = m.x + (live ? l : 0);
-  const T sum = row_sum_tpr<T, TPR>(a, m, l, x, live ? b[i] : T(0));
+  const T sum = row_sum_tpr<T, TPR>(a, m, l, live, x, live ? b[i] : T(0));
   if (live && (threadIdx.x & (TPR - 1)) == 0) x[i] = -sum / a.diag[i];
 }
 
@@ -576,7 +579,7 @@ __global__ void __launch_bounds__(BLOCK) k_jacobi_damped_tpr(SellView<T> a, int 
   const int4 m = a.meta[s];
   const bool live = l < m.y;
   const int i = m.x + (live ? l : 0);
-  const T sum = row_sum_tpr<T, TPR>(a, m, l, xold, live ? b[i] : T(0));
+  const T sum = row_sum_tpr<T, TPR>(a, m, l, live, xold, live ? b[i] : T(0));
   if (live && (threadIdx.x & (TPR - 1)) == 0) {
     const T xo = xold[i];
     xnew[i] = xo + w * (-sum / a.diag[i] - xo);

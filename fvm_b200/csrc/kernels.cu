@@ -307,23 +307,44 @@ __global__ void __launch_bounds__(kBlock, 8) k_gs_color_ell(SellView<T> a, int r
 }
 
 // The same pass with two rows per thread (32-row groups g and g + 8 of a
-// block's 16): both rows' loads are issued before either row is written, so
-// a thread keeps twice the loads in flight and a colour of a few hundred
-// thousand rows fits in one wave. Rows of one colour never read each other,
-// so the result is bitwise that of k_gs_color_ell.
+// block's 16): both rows' column, value, b and diagonal loads are issued
+// first, then both rows' x gathers, then the two sums, so a thread keeps
+// twice the loads in flight and a colour of a few hundred thousand rows
+// fits in one wave. Each row sums b then its products in stored order, as
+// ell_row does, and rows of one colour never read each other, so the
+// result is bitwise that of k_gs_color_ell.
 template <class T, int W>
-__global__ void __launch_bounds__(kBlock, 4) k_gs_color_ell2(SellView<T> a, int r0, int r1, T* x,
-                                                             const T* __restrict__ b) {
+__global__ void __launch_bounds__(kBlock) k_gs_color_ell2(SellView<T> a, int r0, int r1, T* x,
+                                                          const T* __restrict__ b) {
   FVM_PDL();
   const int g0 = (r0 >> 5) + blockIdx.x * (2 * kSlicesPerBlock) + (threadIdx.x >> 5);
   const int i0 = (g0 << 5) + (threadIdx.x & 31);
   const int i1 = i0 + (kSlicesPerBlock << 5);
   const bool v0 = i0 >= r0 && i0 < r1, v1 = i1 >= r0 && i1 < r1;
-  T s0 = T(0), s1 = T(0);
-  if (v0) s0 = ell_row<T, W>(a, i0, x, b[i0]);
-  if (v1) s1 = ell_row<T, W>(a, i1, x, b[i1]);
-  if (v0) x[i0] = -s0 / a.diag[i0];
-  if (v1) x[i1] = -s1 / a.diag[i1];
+  const int o0 = (i0 >> 5) * (32 * W) + (i0 & 31), o1 = (i1 >> 5) * (32 * W) + (i1 & 31);
+  int c0[W], c1[W];
+  T a0[W], a1[W], x0[W], x1[W];
+#pragma unroll
+  for (int k = 0; k < W; k++) {
+    c0[k] = v0 ? a.cols[o0 + (k << 5)] : 0;
+    a0[k] = v0 ? a.vals[o0 + (k << 5)] : T(0);
+    c1[k] = v1 ? a.cols[o1 + (k << 5)] : 0;
+    a1[k] = v1 ? a.vals[o1 + (k << 5)] : T(0);
+  }
+  T s0 = v0 ? b[i0] : T(0), s1 = v1 ? b[i1] : T(0);
+  const T d0 = v0 ? a.diag[i0] : T(1), d1 = v1 ? a.diag[i1] : T(1);
+#pragma unroll
+  for (int k = 0; k < W; k++) {
+    x0[k] = v0 ? x[c0[k]] : T(0);
+    x1[k] = v1 ? x[c1[k]] : T(0);
+  }
+#pragma unroll
+  for (int k = 0; k < W; k++) {
+    s0 = s0 + a0[k] * x0[k];
+    s1 = s1 + a1[k] * x1[k];
+  }
+  if (v0) x[i0] = -s0 / d0;
+  if (v1) x[i1] = -s1 / d1;
 }
 
 template <class T, int W>

@@ -1519,17 +1519,20 @@ SolveReport LinearSolve::solveCG(cudaStream_t st) {
 bool LinearSolve::buildCGLoop(cudaStream_t st, bool flexible) {
   const SolverOptions& o = h_.options();
   DevLevel& d = h_.level(0);
-  double* X = work_;
+  const bool mixedCycle = o.precision == kMixed;
+  // The FP32 cycle works on level 0's FP32 vectors only, so the iterate and
+  // the right-hand side can be level 0's own FP64 x and b: no copy in, no
+  // restore. The FP64 cycle overwrites them, so it keeps copies.
+  double* X = mixedCycle ? d.x : work_;
   double* R = work_ + (size_t)n_;
   double* Z = work_ + 2 * (size_t)n_;
   double* P = work_ + 3 * (size_t)n_;
   double* Q = work_ + 4 * (size_t)n_;
-  double* B = work_ + 5 * (size_t)n_;
+  double* B = mixedCycle ? d.b : work_ + 5 * (size_t)n_;
   if (gLoop_) cudaGraphExecDestroy(gLoop_);
   gLoop_ = nullptr;
   if (!loopInt_) loopInt_ = (int*)h_.scratch(4 * sizeof(int));
   history_ = (double*)h_.scratch(sizeof(double) * (size_t)(o.nMaxIterations + 2));
-  const bool mixedCycle = o.precision == kMixed;
   const cudaStreamCaptureMode mode = cudaStreamCaptureModeThreadLocal;
   cudaGraph_t g = nullptr;
   cudaGraphConditionalHandle h = 0;
@@ -1542,7 +1545,7 @@ bool LinearSolve::buildCGLoop(cudaStream_t st, bool flexible) {
       CUDA_OK(cudaMemsetAsync(X, 0, sizeof(double) * (size_t)n_, st));
       CUDA_OK(cudaMemsetAsync(P, 0, sizeof(double) * (size_t)n_, st));
       CUDA_OK(cudaMemsetAsync(Z, 0, sizeof(double) * (size_t)n_, st));
-      dev::copy_d(n_, d.b, B, st);
+      if (B != d.b) dev::copy_d(n_, d.b, B, st);
       dev::residual<double>(d.view64(), d.nSlices, X, B, R, nullptr, st);
       norm_into(R, scal_ + kNorm, st);
       if (mixedCycle) dev::convert_d2f(n_, R, d.bF, st);  // the FP32 cycle's right-hand side
@@ -1612,8 +1615,8 @@ bool LinearSolve::buildCGLoop(cudaStream_t st, bool flexible) {
     try {
       dev::residual<double>(d.view64(), d.nSlices, X, B, R, nullptr, st);
       norm_into(R, scal_ + kNorm, st);
-      dev::copy_d(n_, X, d.x, st);
-      dev::copy_d(n_, B, d.b, st);
+      if (X != d.x) dev::copy_d(n_, X, d.x, st);
+      if (B != d.b) dev::copy_d(n_, B, d.b, st);
       CUDA_OK(cudaMemcpyAsync(hostScal_, scal_ + kNorm, sizeof(double), cudaMemcpyDeviceToHost, st));
       CUDA_OK(cudaMemcpyAsync(hostScal_ + 1, history_, sizeof(double), cudaMemcpyDeviceToHost, st));
       CUDA_OK(cudaMemcpyAsync(hostScal_ + 2, loopInt_, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));

@@ -10,7 +10,7 @@ from fvm_b200 import fvmbaseExt, meshgen
 from helpers import gpu_model
 
 
-def _solve(mixed, autotune, tpr=0, block=0, ell_rows=0, n=96):
+def _solve(mixed, autotune, tpr=0, block=0, ell_rows=0, n=96, device=False):
     mesh, f = meshgen.config0(n=n, seed=3)
     bcs = dict(f["bc"])
     amg = fvmbaseExt.AMG()
@@ -23,6 +23,7 @@ def _solve(mixed, autotune, tpr=0, block=0, ell_rows=0, n=96):
         amg.coarseSolver = fvmbaseExt.AMG.COARSE_DIRECT
         amg.coarsestSize = 1000
         amg.coarseJacobiRows = 1 << 30  # damped Jacobi below the finest level
+        amg.setupOnDevice = device
     amg.autotune = autotune
     amg.planThreadsPerRow = tpr
     amg.planBlock = block
@@ -51,6 +52,20 @@ def test_plans_give_bitwise_identical_solves(mixed):
     assert all((p[0] in (1, 2, 4) and p[1] in (128, 256)) or (p[0] < 0 and p[1] in (-1, -2)) for p in plans)
     assert c == c0
     np.testing.assert_array_equal(T, T0)
+
+
+@pytest.mark.gpu
+def test_plans_on_gpu_built_levels_bitwise_identical():
+    """Every threads-per-row plan forced on the GPU-built coarse levels
+    (natural row order, the last slice of each level partly empty): the
+    same iterations and bitwise the same field as the default plan."""
+    T0, _, c0 = _solve(True, autotune=False, device=True)
+    for tpr, block in ((2, 128), (2, 256), (4, 128), (4, 256), (1, 128)):
+        T, plans, c = _solve(True, autotune=False, tpr=tpr, block=block, device=True)
+        sell = [p for p in plans if p[0] > 0]
+        assert sell and all(p == (tpr, block) for p in sell)
+        assert c == c0
+        np.testing.assert_array_equal(T, T0)
 
 
 @pytest.mark.gpu

@@ -211,18 +211,19 @@ def size_matched_copy_gbs(nbytes: float, reps: int = 7, launches: int = 1) -> fl
     src = torch.ones(n * launches, dtype=torch.float64, device="cuda")
     dst = torch.empty_like(src)
     flush = torch.empty(64 << 20, dtype=torch.float64, device="cuda")
-    # the copies replay as one CUDA graph, so no host launch gap sits
-    # between them (as the solver's own launches replay)
+    # the copies are elementwise kernels (dst = src * 1) replayed as one
+    # CUDA graph, so no host launch gap sits between them (as the solver's
+    # own launches replay); a captured memcpy would run on a copy engine
     s = torch.cuda.Stream()
     s.wait_stream(torch.cuda.current_stream())
     with torch.cuda.stream(s):
         for q in range(launches):  # warm-up outside the capture
-            dst[q * n:(q + 1) * n].copy_(src[q * n:(q + 1) * n])
+            torch.mul(src[q * n:(q + 1) * n], 1.0, out=dst[q * n:(q + 1) * n])
     torch.cuda.current_stream().wait_stream(s)
     graph = torch.cuda.CUDAGraph()
     with torch.cuda.graph(graph):
         for q in range(launches):
-            dst[q * n:(q + 1) * n].copy_(src[q * n:(q + 1) * n])
+            torch.mul(src[q * n:(q + 1) * n], 1.0, out=dst[q * n:(q + 1) * n])
     times = []
     for r in range(reps + 2):
         flush.fill_(float(r))

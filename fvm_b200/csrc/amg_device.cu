@@ -568,32 +568,21 @@ void AmgHierarchy::prepareFinestPattern(const FinestDevice& in, int ordering) {
   fp.ordering = ordering;
   const CSR& c = *in.conn;
   const int n = c.nRows;
-  RefLevel tmp;
-  tmp.n = n;
-  tmp.conn = c;
-  tmp.symmetricPattern = in.symmetricPattern;
-  tmp.segments = in.segments;
-  tmp.diag.assign(n, 1.0);
-  // values = entry index + 1, so the packing tells where every entry went
-  tmp.off.resize(c.nnz());
-  for (int k = 0; k < c.nnz(); k++) tmp.off[k] = (double)(k + 1);
-  pack_level(tmp, (SmootherOrdering)ordering, fp.packed);
+  // colours, permutation and slices of the pattern, with the CSR entry
+  // stored in every packed slot
+  std::unique_ptr<int[]> cols, posSrc;
+  size_t E = 0;
+  pack_pattern(c, in.symmetricPattern, in.segments, (SmootherOrdering)ordering, fp.packed, cols, posSrc, E);
   PackedLevel& p = fp.packed;
-  const size_t E = p.cols.size();
-  std::vector<int> posSrc(E);
-  parallel_chunks((int)E, [&](int b, int e) {
-    for (int q = b; q < e; q++) {
-      const double v = p.vals[q];
-      if (v == 0.0) {
-        posSrc[q] = -1;
-      } else {
-        const int k = (int)v - 1;
-        posSrc[q] = in.entrySrc ? (*in.entrySrc)[k] : k;
-      }
-    }
-  }, 1 << 18);
-  p.vals.clear();
-  p.vals.shrink_to_fit();
+  fp.entries = E;
+  if (in.entrySrc) {
+    const std::vector<int>& src = *in.entrySrc;
+    int* ps = posSrc.get();
+    parallel_chunks((int)E, [&](int b, int e) {
+      for (int q = b; q < e; q++)
+        if (ps[q] >= 0) ps[q] = src[ps[q]];
+    }, 1 << 18);
+  }
   const int nSlices = (int)p.sliceRow.size();
   std::vector<int> rs(n);
   std::vector<int4> meta(nSlices);
@@ -604,10 +593,10 @@ void AmgHierarchy::prepareFinestPattern(const FinestDevice& in, int ordering) {
   fp.sliceRow = fp.arena.upload(p.sliceRow);
   fp.sliceRows = fp.arena.upload(p.sliceRows);
   fp.sliceOff = fp.arena.upload(p.sliceOff);
-  fp.cols = fp.arena.upload(p.cols);
+  fp.cols = fp.arena.upload(cols.get(), E);
   fp.rowSlice = fp.arena.upload(rs);
   fp.meta = fp.arena.upload(meta);
-  fp.posSrc = fp.arena.upload(posSrc);
+  fp.posSrc = fp.arena.upload(posSrc.get(), E);
   fp.iperm = fp.arena.upload(p.iperm);
   fp.perm = fp.arena.upload(p.perm);
 }
@@ -670,7 +659,7 @@ void AmgHierarchy::buildDevice(const FinestDevice& in, const SolverOptions& opt)
     d.maxWidth = p0.maxWidth;
     d.ellWidth = p0.ellWidth;
     d.colorSliceStart = p0.colorSliceStart;
-    d.entries = p0.cols.size();
+    d.entries = fp.entries;
     d.sliceRow = fp.sliceRow;
     d.sliceRows = fp.sliceRows;
     d.sliceOff = fp.sliceOff;
@@ -683,8 +672,10 @@ void AmgHierarchy::buildDevice(const FinestDevice& in, const SolverOptions& opt)
       d.valsF = (float*)arena_.alloc(size_class(sizeof(float) * d.entries));
       d.diagF = (float*)arena_.alloc(size_class(sizeof(float) * n0));
     }
+    lap("level 0 allocations");
     dev::fill_finest((long long)d.entries, fp.posSrc, in.offSrc, d.vals, d.valsF, n0, fp.iperm, in.diag, d.diag,
                      d.diagF, st);
+    lap("level 0 values filled");
     allocVectors(d, mixed);
   }
   // work arrays sized by level 0, shared by every level

@@ -483,8 +483,15 @@ int greedy_coloring(const CSR& conn, std::vector<int>& color) {
   return nColors;
 }
 
-void pack_level(const RefLevel& lv, SmootherOrdering ordering, PackedLevel& out) {
-  const int n = lv.n;
+namespace {
+// The colouring, colour-major permutation, slices and packed slots of a
+// level. With values, diag and off give the diagonal and the stored
+// entries; without, the pattern alone is packed. pos (optional) gets the
+// CSR entry index of every packed slot (-1: padding).
+void pack_core(const CSR& conn, bool symmetricPattern, const std::vector<int>& segments, bool values,
+               const double* diag, const double* off, SmootherOrdering ordering, PackedLevel& out,
+               std::unique_ptr<int[]>* colsOut, std::unique_ptr<int[]>* pos, size_t* slotsOut) {
+  const int n = conn.nRows;
   out.n = n;
   // (out may be a reused object: pack_transfer refills these for all but
   // the coarsest level)
@@ -496,7 +503,7 @@ void pack_level(const RefLevel& lv, SmootherOrdering ordering, PackedLevel& out)
     color.assign(n, 0);
     out.nColors = 1;
   } else {
-    out.nColors = multicolor(lv.conn, color, lv.symmetricPattern, &lv.segments);
+    out.nColors = multicolor(conn, color, symmetricPattern, &segments);
   }
   // colour-major permutation, stable in reference order: per-chunk colour
   // counts, then every chunk places its rows behind the earlier chunks'
@@ -525,7 +532,10 @@ void pack_level(const RefLevel& lv, SmootherOrdering ordering, PackedLevel& out)
   }
   out.perm.resize(n);
   out.iperm.resize(n);
-  out.diag.resize(n);
+  if (values)
+    out.diag.resize(n);
+  else
+    out.diag.clear();
   parallel_chunks(nt, [&](int t0, int t1) {
     for (int t = t0; t < t1; t++) {
       int* cur = &base[(size_t)t * C];
@@ -533,7 +543,7 @@ void pack_level(const RefLevel& lv, SmootherOrdering ordering, PackedLevel& out)
         const int p = cur[color[i]]++;
         out.perm[i] = p;
         out.iperm[p] = i;
-        out.diag[p] = lv.diag[i];
+        if (values) out.diag[p] = diag[i];
       }
     }
   }, 1);
@@ -554,7 +564,7 @@ void pack_level(const RefLevel& lv, SmootherOrdering ordering, PackedLevel& out)
   parallel_chunks(nSlices, [&](int b, int e) {
     for (int s = b; s < e; s++) {
       int w = 0;
-      for (int l = 0; l < out.sliceRows[s]; l++) w = std::max(w, lv.conn.count(out.iperm[out.sliceRow[s] + l]));
+      for (int l = 0; l < out.sliceRows[s]; l++) w = std::max(w, conn.count(out.iperm[out.sliceRow[s] + l]));
       out.sliceOff[s + 1] = w;
     }
   });
@@ -585,32 +595,64 @@ void pack_level(const RefLevel& lv, SmootherOrdering ordering, PackedLevel& out)
     out.colorSliceStart = out.colorStart;
   }
   const int nPacked = (int)out.sliceRow.size();
-  out.cols.resize(out.sliceOff[nPacked]);
-  out.vals.resize(out.sliceOff[nPacked]);
-  parallel_chunks(nPacked, [&](int b, int e) { pack_slices(lv, out, b, e); });
-}
-
-void pack_slices(const RefLevel& lv, PackedLevel& out, int sBegin, int sEnd) {
-  for (int s = sBegin; s < sEnd; s++) {
-    const int w = (out.sliceOff[s + 1] - out.sliceOff[s]) / 32;
-    for (int l = 0; l < 32; l++) {
-      const int p = out.sliceRow[s] + l;
-      const bool live = l < out.sliceRows[s];
-      const int i = live ? out.iperm[p] : -1;
-      const int cnt = live ? lv.conn.count(i) : 0;
-      for (int k = 0; k < w; k++) {
-        const size_t e = (size_t)out.sliceOff[s] + (size_t)k * 32 + l;
-        if (k < cnt) {
-          const int nb = lv.conn.row[i] + k;
-          out.cols[e] = out.perm[lv.conn.col[nb]];
-          out.vals[e] = lv.off[nb];
-        } else {
-          out.cols[e] = live ? p : out.sliceRow[s];
-          out.vals[e] = 0.0;
+  const size_t slots = (size_t)out.sliceOff[nPacked];
+  // the pattern's arrays are not zero-filled first: the parallel fill below
+  // writes every slot (and first-touches the pages on many threads)
+  int* cols = nullptr;
+  if (colsOut) {
+    colsOut->reset(new int[slots > 0 ? slots : 1]);
+    cols = colsOut->get();
+    out.cols.clear();
+  } else {
+    out.cols.resize(slots);
+    cols = out.cols.data();
+  }
+  if (values)
+    out.vals.resize(slots);
+  else
+    out.vals.clear();
+  int* posp = nullptr;
+  if (pos) {
+    pos->reset(new int[slots > 0 ? slots : 1]);
+    posp = pos->get();
+  }
+  if (slotsOut) *slotsOut = slots;
+  parallel_chunks(nPacked, [&](int sBegin, int sEnd) {
+    for (int s = sBegin; s < sEnd; s++) {
+      const int w = (out.sliceOff[s + 1] - out.sliceOff[s]) / 32;
+      for (int l = 0; l < 32; l++) {
+        const int p = out.sliceRow[s] + l;
+        const bool live = l < out.sliceRows[s];
+        const int i = live ? out.iperm[p] : -1;
+        const int cnt = live ? conn.count(i) : 0;
+        for (int k = 0; k < w; k++) {
+          const size_t e = (size_t)out.sliceOff[s] + (size_t)k * 32 + l;
+          if (k < cnt) {
+            const int nb = conn.row[i] + k;
+            cols[e] = out.perm[conn.col[nb]];
+            if (values) out.vals[e] = off[nb];
+            if (posp) posp[e] = nb;
+          } else {
+            cols[e] = live ? p : out.sliceRow[s];
+            if (values) out.vals[e] = 0.0;
+            if (posp) posp[e] = -1;
+          }
         }
       }
     }
-  }
+  });
+}
+}  // namespace
+
+void pack_level(const RefLevel& lv, SmootherOrdering ordering, PackedLevel& out) {
+  pack_core(lv.conn, lv.symmetricPattern, lv.segments, true, lv.diag.data(), lv.off.data(), ordering, out,
+            nullptr, nullptr, nullptr);
+}
+
+void pack_pattern(const CSR& conn, bool symmetricPattern, const std::vector<int>& segments,
+                  SmootherOrdering ordering, PackedLevel& out, std::unique_ptr<int[]>& cols,
+                  std::unique_ptr<int[]>& pos, size_t& slots) {
+  pack_core(conn, symmetricPattern, segments, false, nullptr, nullptr, ordering, out, &cols, &pos, &slots);
 }
 
 void pack_transfer(const RefLevel& fine, const CSR& c2f, PackedLevel& pf, const PackedLevel& pc) {

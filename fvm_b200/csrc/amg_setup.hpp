@@ -10,6 +10,7 @@
 #pragma once
 
 #include <functional>
+#include <memory>
 #include <vector>
 
 #include "common.hpp"
@@ -114,8 +115,13 @@ bool symmetrize_pattern(const CSR& a, CSR& out);
 bool pattern_is_symmetric(const CSR& a);
 
 void pack_level(const RefLevel& lv, SmootherOrdering ordering, PackedLevel& out);
-// fills cols/vals of slices [sBegin, sEnd) (pack_level runs it in parallel)
-void pack_slices(const RefLevel& lv, PackedLevel& out, int sBegin, int sEnd);
+// The same colouring, permutation and slices for a pattern alone: out gets
+// everything but cols, vals and diag; cols (the packed columns) and pos
+// (the CSR entry index of every packed slot, -1 for padding) are filled in
+// parallel into fresh arrays of `slots` ints, never zero-initialised.
+void pack_pattern(const CSR& conn, bool symmetricPattern, const std::vector<int>& segments,
+                  SmootherOrdering ordering, PackedLevel& out, std::unique_ptr<int[]>& cols,
+                  std::unique_ptr<int[]>& pos, size_t& slots);
 void pack_transfer(const RefLevel& fine, const CSR& coarseToFine, PackedLevel& pf,
                    const PackedLevel& pc);
 

@@ -135,8 +135,12 @@ class DeviceArena {
   void* alloc(size_t bytes);
   template <class T>
   T* upload(const std::vector<T>& v) {
-    T* p = (T*)alloc(v.size() * sizeof(T));
-    if (!v.empty()) copy_h2d(p, v.data(), v.size() * sizeof(T));
+    return upload(v.data(), v.size());
+  }
+  template <class T>
+  T* upload(const T* v, size_t count) {
+    T* p = (T*)alloc(count * sizeof(T));
+    if (count) copy_h2d(p, v, count * sizeof(T));
     return p;
   }
   void release();
@@ -170,7 +174,8 @@ struct FinestDevice {
 struct FinestPattern {
   unsigned long long key = 0;
   int ordering = 0;
-  PackedLevel packed;  // colours, permutation, slices (values unused)
+  PackedLevel packed;  // colours, permutation, slices (no columns or values on the host)
+  size_t entries = 0;  // packed slots
   DeviceArena arena;
   int *sliceRow = nullptr, *sliceRows = nullptr, *sliceOff = nullptr, *cols = nullptr, *rowSlice = nullptr;
   int *posSrc = nullptr, *iperm = nullptr, *perm = nullptr;

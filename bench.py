@@ -563,6 +563,7 @@ def bench_transient(args, dist, peaks, peak_kind):
     def summary(r):
         return {"total_s": r["total_s"], "first_step_s": r["per_step_s"][0],
                 "mean_later_step_s": float(np.mean(r["per_step_s"][1:])) if len(r["per_step_s"]) > 1 else None,
+                "step_ms": [round(1e3 * t, 2) for t in r["per_step_s"]],
                 "outer_per_step": r["outer"], "cycles_per_step": r["cycles"],
                 "learned_tried": r["learned_tried"], "learned_kept": r["learned_kept"]}
 

@@ -1111,9 +1111,10 @@ void LinearSolve::run(cudaGraphExec_t& exec, cudaStream_t st, const std::functio
     CUDA_OK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
     try {
       body();
-    } catch (const Error&) {
+    } catch (const Error& e) {
       // a launch that cannot be captured (e.g. cooperative launch on an
       // older driver): drop graphs for this solver and run eagerly
+      if (getenv("FVM_TRACE")) fprintf(stderr, "[fvm solve] graph capture failed, running eagerly: %s\n", e.what());
       cudaStreamEndCapture(st, &g);
       if (g) cudaGraphDestroy(g);
       cudaGetLastError();
@@ -1370,6 +1371,10 @@ SolveReport LinearSolve::solveCG(cudaStream_t st) {
   if (o.preconditioner == kPrecAMG && o.useGraphs && o.verbosity <= 0 && !(learned_ && learnedActive_) &&
       !graphsFailed_ && solveCGLoop(st, flexible, rep))
     return rep;
+  if (getenv("FVM_TRACE"))
+    fprintf(stderr, "[fvm solve] CG on the host loop (learned step %s, graphs %s, loop graph %s)\n",
+            learned_ && learnedActive_ ? "active" : "inactive", graphsFailed_ ? "failed" : "ok",
+            loopFailed_ ? "failed" : "ok");
   CUDA_OK(cudaMemsetAsync(X, 0, sizeof(double) * (size_t)n_, st));
   CUDA_OK(cudaMemsetAsync(P, 0, sizeof(double) * (size_t)n_, st));
   CUDA_OK(cudaMemsetAsync(Z, 0, sizeof(double) * (size_t)n_, st));  // z_0 enters the first flexible beta

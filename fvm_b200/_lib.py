@@ -53,6 +53,7 @@ class LinearOptions(ctypes.Structure):
         ("chebyshevDegree", ctypes.c_int),
         ("chebyshevFraction", ctypes.c_double),
         ("gsReverse", ctypes.c_int),
+        ("patternOnDevice", ctypes.c_int),
     ]
 
 

@@ -458,6 +458,156 @@ __global__ void k_dominance(LevelRows a, int* flag) {
   if (!(d != 0.0 && s <= fabs(d) * (1.0 + 1e-8))) atomicOr(flag, 1);
 }
 
+// ---- level-0 pattern of a mesh on the device -------------------------------
+// Self-column entries per self row of cellCells.
+__global__ void k_ip_count(int n, const int* __restrict__ ccRow, const int* __restrict__ ccCol, int* cnt) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int c = 0;
+  for (int k = ccRow[i]; k < ccRow[i + 1]; k++) c += ccCol[k] < n ? 1 : 0;
+  cnt[i] = c;
+}
+
+// The self-column entries in cellCells order, with the face behind each:
+// the last of the row's faces (ascending) joining the two cells, as the
+// face -> entry map of cellCells assigns it. *bad is set when no face joins
+// an entry's cells.
+__global__ void k_ip_fill(int n, const int* __restrict__ ccRow, const int* __restrict__ ccCol,
+                          const int* __restrict__ cfRow, const int* __restrict__ cfCol,
+                          const int* __restrict__ fc, const int* __restrict__ rowOff, int* col, int* face,
+                          int* bad) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int q = rowOff[i];
+  for (int k = ccRow[i]; k < ccRow[i + 1]; k++) {
+    const int j = ccCol[k];
+    if (j >= n) continue;
+    int f = -1;
+    for (int t = cfRow[i]; t < cfRow[i + 1]; t++) {
+      const int g = cfCol[t];
+      const int a = fc[2 * g], b = fc[2 * g + 1];
+      if ((a == i && b == j) || (a == j && b == i)) f = g;
+    }
+    if (f < 0) atomicOr(bad, 1);
+    col[q] = j;
+    face[q] = f;
+    q++;
+  }
+}
+
+// One in-place sweep towards the row-order greedy colouring: color[i] =
+// the smallest colour no neighbour j < i holds. That colouring is the
+// unique fixed point of the update (row i's value depends only on rows
+// below it), and a sweep in which no row changes has read only settled
+// values, so it is the fixed point. *changed is set when a row changes;
+// *overflow when a row would need colour 32 or more.
+__global__ void k_greedy_sweep(int n, const int* __restrict__ rowOff, const int* __restrict__ col, int* color,
+                               int* changed, int* overflow) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  unsigned used = 0u;
+  for (int q = rowOff[i]; q < rowOff[i + 1]; q++) {
+    const int j = col[q];
+    if (j < i) {
+      const int c = __ldcg(color + j);
+      if (c < 32) used |= 1u << c;
+    }
+  }
+  if (used == 0xffffffffu) {
+    atomicOr(overflow, 1);
+    return;
+  }
+  const int c = __ffs(~used) - 1;
+  if (c != __ldcg(color + i)) {
+    __stcg(color + i, c);
+    atomicOr(changed, 1);
+  }
+}
+
+// per-colour row counts (colours < 32), one atomic per block and colour
+__global__ void k_color_hist(int n, const int* __restrict__ color, int* hist) {
+  __shared__ int h[32];
+  if (threadIdx.x < 32) h[threadIdx.x] = 0;
+  __syncthreads();
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) atomicAdd(&h[color[i] & 31], 1);
+  __syncthreads();
+  if (threadIdx.x < 32 && h[threadIdx.x]) atomicAdd(&hist[threadIdx.x], h[threadIdx.x]);
+}
+
+__global__ void k_color_flags(int n, const int* __restrict__ color, int c, int* flag) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) flag[i] = color[i] == c ? 1 : 0;
+}
+
+// rows of colour c in ascending order after those of the colours below it
+__global__ void k_color_place(int n, const int* __restrict__ color, int c, const int* __restrict__ pos, int start,
+                              int* perm, int* iperm) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n || color[i] != c) return;
+  const int p = start + pos[i];
+  perm[i] = p;
+  iperm[p] = i;
+}
+
+// largest row length (atomicMax) and the SELL-32 size of colour-aligned
+// slices (one warp per slice; slice s of colour c starts at row
+// colorStart[c] + 32 (s - sliceStart[c]))
+__global__ void k_row_max(int n, const int* __restrict__ rowOff, int* maxLen) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  int w = i < n ? rowOff[i + 1] - rowOff[i] : 0;
+  for (int o = 16; o > 0; o >>= 1) w = max(w, __shfl_xor_sync(kFull, w, o));
+  if ((threadIdx.x & 31) == 0 && w > 0) atomicMax(maxLen, w);
+}
+
+__global__ void k_sell_size(int nSlices, int nColors, const int* __restrict__ colorStart,
+                            const int* __restrict__ sliceStart, const int* __restrict__ iperm,
+                            const int* __restrict__ rowOff, unsigned long long* total) {
+  const int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (s >= nSlices) return;  // whole warp
+  int c = 0;
+  while (c + 1 < nColors && sliceStart[c + 1] <= s) c++;
+  const int r0 = colorStart[c] + 32 * (s - sliceStart[c]);
+  const int rows = min(32, colorStart[c + 1] - r0);
+  int w = 0;
+  if (lane < rows) {
+    const int i = iperm[r0 + lane];
+    w = rowOff[i + 1] - rowOff[i];
+  }
+  for (int o = 16; o > 0; o >>= 1) w = max(w, __shfl_xor_sync(kFull, w, o));
+  if (lane == 0) atomicAdd(total, 32ull * (unsigned long long)w);
+}
+
+// ELL-32 slots of every packed row p (groups x 32 rows, rows past n are
+// padding): the permuted column and the face of each entry, padding (own
+// row, no face); rowSlice of every row
+__global__ void k_ell_fill(int n, int rowsPadded, int W, const int* __restrict__ iperm,
+                           const int* __restrict__ rowOff, const int* __restrict__ col, const int* __restrict__ face,
+                           const int* __restrict__ perm, int* cols, int* posSrc, int* rowSlice) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= rowsPadded) return;
+  const bool live = p < n;
+  const int g = p >> 5;
+  const size_t base = (size_t)g * 32 * W + (p & 31);
+  int i = 0, q0 = 0, cnt = 0;
+  if (live) {
+    i = iperm[p];
+    q0 = rowOff[i];
+    cnt = rowOff[i + 1] - q0;
+    rowSlice[p] = g;
+  }
+  for (int k = 0; k < W; k++) {
+    const size_t e = base + 32 * (size_t)k;
+    if (k < cnt) {
+      cols[e] = perm[col[q0 + k]];
+      posSrc[e] = face[q0 + k];
+    } else {
+      cols[e] = live ? p : 32 * g;
+      posSrc[e] = -1;
+    }
+  }
+}
+
 }  // namespace
 
 int scan_scratch_ints(int n) { return cdiv(n, kScanTile) + 1; }
@@ -560,6 +710,146 @@ size_t size_class(size_t bytes) {
 }
 }  // namespace
 
+bool AmgHierarchy::prepareFinestPatternDevice(const FinestDevice& in) {
+  const int n = in.conn->nRows;
+  if (n <= 0 || !in.ccRow || !in.ccCol || !in.cfRow || !in.cfCol || !in.faceCells || !in.symmetricPattern)
+    return false;
+  constexpr int kFewColors = 5;
+  cudaStream_t st = setupStream_;
+  const bool trace = getenv("FVM_TRACE") != nullptr;
+  auto t0 = std::chrono::steady_clock::now();
+  auto lap = [&](const char* what) {
+    if (!trace) return;
+    CUDA_OK(cudaStreamSynchronize(st));
+    const auto t1 = std::chrono::steady_clock::now();
+    fprintf(stderr, "[fvm device pattern] %-28s %8.2f ms\n", what,
+            std::chrono::duration<double, std::milli>(t1 - t0).count());
+    t0 = t1;
+  };
+  std::unique_ptr<FinestPattern> fpp(new FinestPattern());
+  FinestPattern& fp = *fpp;
+  DeviceArena tmp;  // work arrays of this build only
+  int* flags = (int*)tmp.alloc(64 * sizeof(int));  // [0] bad face, [1] changed, [2] overflow, [3] max len, [8..39] hist
+  unsigned long long* sellTotal = (unsigned long long*)tmp.alloc(sizeof(unsigned long long));
+  CUDA_OK(cudaMemsetAsync(flags, 0, 64 * sizeof(int), st));
+  CUDA_OK(cudaMemsetAsync(sellTotal, 0, sizeof(unsigned long long), st));
+  int* h = reinterpret_cast<int*>(pinnedScalars());
+  // self-column entries of cellCells with the face behind each
+  int* cnt = (int*)tmp.alloc(sizeof(int) * ((size_t)n + 1));
+  int* rowOff = (int*)tmp.alloc(sizeof(int) * ((size_t)n + 1));
+  int* scan = (int*)tmp.alloc(sizeof(int) * (dev::scan_scratch_ints(n + 1) + 1));
+  dev::k_ip_count<<<dev::cdiv(n, dev::kT), dev::kT, 0, st>>>(n, in.ccRow, in.ccCol, cnt);
+  dev::scan_exclusive(cnt, rowOff, n, scan, st);
+  CUDA_OK(cudaMemcpyAsync(h, rowOff + n, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CUDA_OK(cudaStreamSynchronize(st));
+  const int nnz = h[0];
+  if (nnz != in.conn->nnz()) return false;
+  int* col = (int*)tmp.alloc(sizeof(int) * (size_t)std::max(nnz, 1));
+  int* face = (int*)tmp.alloc(sizeof(int) * (size_t)std::max(nnz, 1));
+  dev::k_ip_fill<<<dev::cdiv(n, dev::kT), dev::kT, 0, st>>>(n, in.ccRow, in.ccCol, in.cfRow, in.cfCol, in.faceCells,
+                                                           rowOff, col, face, flags);
+  // row-order greedy colouring: sweeps until one changes nothing, read back
+  // every 32 sweeps (the flag is cleared before the last sweep of a batch)
+  lap("entries and faces");
+  int* color = cnt;  // the counts are no longer needed
+  CUDA_OK(cudaMemsetAsync(color, 0, sizeof(int) * (size_t)n, st));
+  constexpr int kBatch = 32, kMaxBatches = 128;
+  bool settled = false;
+  int batches = 0;
+  for (int b = 0; b < kMaxBatches && !settled; b++, batches++) {
+    for (int k = 0; k < kBatch; k++) {
+      if (k == kBatch - 1) CUDA_OK(cudaMemsetAsync(flags + 1, 0, sizeof(int), st));
+      dev::k_greedy_sweep<<<dev::cdiv(n, dev::kT), dev::kT, 0, st>>>(n, rowOff, col, color, flags + 1, flags + 2);
+    }
+    CUDA_OK(cudaMemcpyAsync(h, flags, 3 * sizeof(int), cudaMemcpyDeviceToHost, st));
+    CUDA_OK(cudaStreamSynchronize(st));
+    if (h[0] || h[2]) return false;  // an entry without a face, or a colour >= 32
+    settled = h[1] == 0;
+  }
+  if (trace) fprintf(stderr, "[fvm device pattern] colouring settled within %d sweeps\n", 32 * batches);
+  lap("colouring");
+  if (!settled) return false;
+  dev::k_color_hist<<<dev::cdiv(n, dev::kT), dev::kT, 0, st>>>(n, color, flags + 8);
+  dev::k_row_max<<<dev::cdiv(n, dev::kT), dev::kT, 0, st>>>(n, rowOff, flags + 3);
+  CUDA_OK(cudaMemcpyAsync(h, flags, 40 * sizeof(int), cudaMemcpyDeviceToHost, st));
+  CUDA_OK(cudaStreamSynchronize(st));
+  int C = 0;
+  for (int c = 0; c < 32; c++)
+    if (h[8 + c] > 0) C = c + 1;
+  const int maxWidth = h[3];
+  if (C < 1 || C > kFewColors || maxWidth > 8 || n < 32768) return false;
+  PackedLevel& pk = fp.packed;
+  pk.n = n;
+  pk.nColors = C;
+  pk.colorStart.assign(C + 1, 0);
+  for (int c = 0; c < C; c++) pk.colorStart[c + 1] = pk.colorStart[c] + h[8 + c];
+  // colour-major permutation, ascending rows within a colour
+  fp.perm = (int*)fp.arena.alloc(sizeof(int) * (size_t)n);
+  fp.iperm = (int*)fp.arena.alloc(sizeof(int) * (size_t)n);
+  int* flag = (int*)tmp.alloc(sizeof(int) * (size_t)n);
+  int* pos = (int*)tmp.alloc(sizeof(int) * ((size_t)n + 1));
+  for (int c = 0; c < C; c++) {
+    dev::k_color_flags<<<dev::cdiv(n, dev::kT), dev::kT, 0, st>>>(n, color, c, flag);
+    dev::scan_exclusive(flag, pos, n, scan, st);
+    dev::k_color_place<<<dev::cdiv(n, dev::kT), dev::kT, 0, st>>>(n, color, c, pos, pk.colorStart[c], fp.perm,
+                                                                 fp.iperm);
+  }
+  lap("permutation");
+  // ELL-32 when the colour-aligned SELL-32 slices would not save more than
+  // 15 % (the host packing's rule)
+  std::vector<int> sliceStart(C + 1, 0);
+  for (int c = 0; c < C; c++) sliceStart[c + 1] = sliceStart[c] + dev::cdiv(pk.colorStart[c + 1] - pk.colorStart[c], 32);
+  const int nSellSlices = sliceStart[C];
+  int* dStarts = (int*)tmp.alloc(sizeof(int) * 2 * (C + 1));
+  std::vector<int> starts(pk.colorStart);
+  starts.insert(starts.end(), sliceStart.begin(), sliceStart.end());
+  CUDA_OK(cudaMemcpyAsync(dStarts, starts.data(), sizeof(int) * starts.size(), cudaMemcpyHostToDevice, st));
+  dev::k_sell_size<<<dev::cdiv((long long)nSellSlices * 32, dev::kT), dev::kT, 0, st>>>(
+      nSellSlices, C, dStarts, dStarts + C + 1, fp.iperm, rowOff, sellTotal);
+  unsigned long long sellEntries = 0;
+  CUDA_OK(cudaMemcpyAsync(&sellEntries, sellTotal, sizeof(sellEntries), cudaMemcpyDeviceToHost, st));
+  CUDA_OK(cudaStreamSynchronize(st));
+  const int groups = dev::cdiv(n, 32), W = maxWidth;
+  const long long ellEntries = (long long)groups * 32 * W;
+  if (W < 1 || ellEntries * 100 > (long long)sellEntries * 115) return false;
+  pk.maxWidth = W;
+  pk.ellWidth = W;
+  pk.colorSliceStart = pk.colorStart;
+  pk.sliceRow.resize(groups);
+  pk.sliceRows.resize(groups);
+  pk.sliceOff.resize(groups + 1);
+  std::vector<int4> meta(groups);
+  for (int g = 0; g < groups; g++) {
+    pk.sliceRow[g] = 32 * g;
+    pk.sliceRows[g] = std::min(32, n - 32 * g);
+    pk.sliceOff[g] = 32 * W * g;
+    meta[g] = make_int4(32 * g, pk.sliceRows[g], 32 * W * g, W);
+  }
+  pk.sliceOff[groups] = 32 * W * groups;
+  fp.entries = (size_t)ellEntries;
+  fp.cols = (int*)fp.arena.alloc(sizeof(int) * fp.entries);
+  fp.posSrc = (int*)fp.arena.alloc(sizeof(int) * fp.entries);
+  fp.rowSlice = (int*)fp.arena.alloc(sizeof(int) * (size_t)n);
+  dev::k_ell_fill<<<dev::cdiv((long long)groups * 32, dev::kT), dev::kT, 0, st>>>(
+      n, groups * 32, W, fp.iperm, rowOff, col, face, fp.perm, fp.cols, fp.posSrc, fp.rowSlice);
+  lap("ELL-32 slots");
+  fp.sliceRow = fp.arena.upload(pk.sliceRow);
+  fp.sliceRows = fp.arena.upload(pk.sliceRows);
+  fp.sliceOff = fp.arena.upload(pk.sliceOff);
+  fp.meta = fp.arena.upload(meta);
+  // the permutation on the host too (exports of level 0 use it)
+  pk.perm.resize(n);
+  pk.iperm.resize(n);
+  CUDA_OK(cudaMemcpyAsync(pk.perm.data(), fp.perm, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost, st));
+  CUDA_OK(cudaMemcpyAsync(pk.iperm.data(), fp.iperm, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost, st));
+  CUDA_OK(cudaStreamSynchronize(st));
+  lap("slices and host permutation");
+  fp.key = in.key;
+  fp.ordering = (int)kMulticolor;
+  finest_ = std::move(fpp);
+  return true;
+}
+
 void AmgHierarchy::prepareFinestPattern(const FinestDevice& in, int ordering) {
   if (finest_ && in.key != 0 && finest_->key == in.key && finest_->ordering == ordering) return;
   finest_.reset(new FinestPattern());
@@ -641,7 +931,11 @@ void AmgHierarchy::buildDevice(const FinestDevice& in, const SolverOptions& opt)
   if (!setupStream_) CUDA_OK(cudaStreamCreateWithFlags(&setupStream_, cudaStreamNonBlocking));
   cudaStream_t st = setupStream_;
   const bool mixed = opt.precision == kMixed;
-  prepareFinestPattern(in, (int)opt.ordering);
+  {
+    const bool cached = finest_ && in.key != 0 && finest_->key == in.key && finest_->ordering == (int)opt.ordering;
+    if (!cached && !(opt.patternOnDevice && opt.ordering == kMulticolor && prepareFinestPatternDevice(in)))
+      prepareFinestPattern(in, (int)opt.ordering);
+  }
   deviceBuilt_ = true;
   lap("level-0 pattern");
   const FinestPattern& fp = *finest_;

@@ -83,6 +83,9 @@ struct SolverOptions {
   int matchPasses = 1;          // matchings per level: 2 pairs the pairs (aggregates of about 4 rows)
   // post-smoothing sweeps on the levels below the finest (-1: nPostSweeps)
   int coarsePostSweeps = -1;
+  // GPU-built hierarchies: colour and pack level 0 on the device when the
+  // pattern is there (the same colouring and packing as on the host)
+  bool patternOnDevice = true;
   int postSweeps(int l) const { return l > 0 && coarsePostSweeps >= 0 ? coarsePostSweeps : nPostSweeps; }
   // only the finest level is needed (Jacobi solver or preconditioner)
   bool finestOnly() const { return solver == kSolverJacobi || preconditioner == kPrecJacobi; }
@@ -168,6 +171,12 @@ struct FinestDevice {
   unsigned long long key = 0;
   bool symmetricPattern = true;
   std::vector<int> segments;  // independent diagonal blocks (a batch)
+  // The same pattern on the device, so that it can be coloured and packed
+  // there (all null: on the host): cellCells of the self rows (ccRow n + 1
+  // offsets, ccCol with ghost columns >= n), each self cell's faces
+  // ascending (cfRow, cfCol) and faceCells (2 per face). conn is then the
+  // self-column part of cellCells and entrySrc the face behind each entry.
+  const int *ccRow = nullptr, *ccCol = nullptr, *cfRow = nullptr, *cfCol = nullptr, *faceCells = nullptr;
 };
 
 // Cached level-0 structure of device-built hierarchies (pattern only).
@@ -289,6 +298,11 @@ class AmgHierarchy {
   std::unique_ptr<FinestPattern> finest_;
   cudaStream_t setupStream_ = nullptr;
   void prepareFinestPattern(const FinestDevice& in, int ordering);
+  // the same on the device (row-order greedy colouring by fixed-point
+  // sweeps, ELL-32 packing); false (nothing kept) when the level needs the
+  // host path: more than five colours, no ELL-32 layout, or a mesh whose
+  // entries it cannot match to faces
+  bool prepareFinestPatternDevice(const FinestDevice& in);
   void allocVectors(DevLevel& d, bool mixed);
   // picks each SELL-32 level's smoother launch plan (autotune or forced)
   void tunePlans();

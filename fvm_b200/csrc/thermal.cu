@@ -463,6 +463,11 @@ void ThermalModel::ensureMatrix() {
     in.key = patternKey_;
     in.symmetricPattern = true;
     in.segments = segOff_;
+    in.ccRow = dCcRow_;
+    in.ccCol = dCcCol_;
+    in.cfRow = dCfRow_;
+    in.cfCol = dCfCol_;
+    in.faceCells = dFaceCells_;
     CUDA_OK(cudaStreamSynchronize(stream_));
     hier_.buildDevice(in, opt_.linear);
     lap("hierarchy on the device");

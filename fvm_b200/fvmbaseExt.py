@@ -199,6 +199,7 @@ class AMG(LinearSolver):
         self.chebyshevDegree = d.chebyshevDegree
         self.chebyshevFraction = d.chebyshevFraction
         self.gsReverse = bool(d.gsReverse)  # Gauss-Seidel sweep: forward + reverse (reference) or forward only
+        self.patternOnDevice = bool(d.patternOnDevice)  # finest level of a GPU-built hierarchy packed on the GPU
         self.setupOnDevice = bool(d.setupOnDevice)
         self.matchRounds = d.matchRounds
         self.matchBeta = d.matchBeta
@@ -245,6 +246,7 @@ class AMG(LinearSolver):
         o.chebyshevDegree = int(self.chebyshevDegree)
         o.chebyshevFraction = float(self.chebyshevFraction)
         o.gsReverse = int(bool(self.gsReverse))
+        o.patternOnDevice = int(bool(self.patternOnDevice))
         o.setupOnDevice = int(bool(self.setupOnDevice))
         o.matchRounds = int(self.matchRounds)
         o.matchBeta = float(self.matchBeta)

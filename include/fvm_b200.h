@@ -98,6 +98,8 @@ typedef struct fvm_linear_options {
   int gsReverse;            /* 1: a multicolour Gauss-Seidel sweep is forward + reverse over the
                                colours (the reference's sweep); 0: forward only (a nonsymmetric
                                preconditioner: for flexible CG or standalone AMG) */
+  int patternOnDevice;      /* setupOnDevice: 1 colours and packs a new mesh's finest level on the
+                               GPU (the same colouring and packing as the host's), 0 on the host */
 } fvm_linear_options;
 
 /* ThermalModelOptions (fvmbase/ThermalBC.h:33-67) + volume-condition constants */

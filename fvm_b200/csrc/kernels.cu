@@ -49,8 +49,23 @@ __device__ __forceinline__ double block_sum(double v) {
 // Up to K entries of a row: every column and value load is issued, then
 // every x gather, then the products are accumulated in stored order -- two
 // dependent round trips to memory for the whole chunk.
-template <class T, int K>
-__device__ __forceinline__ T row_chunk(const SellView<T>& a, int e0, int cnt, const T* __restrict__ x, T sum) {
+// The value of column j a row sum gathers: x[j], or, for a pass that
+// starts right after a prolongation that assigned x = xc[ci], xc[ci[j]]
+// (the same value, without the prolongation's launch and x round trip)
+template <class T>
+struct XDirect {
+  const T* __restrict__ x;
+  __device__ __forceinline__ T operator()(int j) const { return x[j]; }
+};
+template <class T>
+struct XProlonged {
+  const T* __restrict__ xc;
+  const int* __restrict__ ci;
+  __device__ __forceinline__ T operator()(int j) const { return xc[ci[j]]; }
+};
+
+template <class T, int K, class X>
+__device__ __forceinline__ T row_chunk_g(const SellView<T>& a, int e0, int cnt, const X& xg, T sum) {
   int c[K];
   T v[K];
   T xv[K];
@@ -62,29 +77,36 @@ __device__ __forceinline__ T row_chunk(const SellView<T>& a, int e0, int cnt, co
     }
 #pragma unroll
   for (int k = 0; k < K; k++)
-    if (k < cnt) xv[k] = x[c[k]];
+    if (k < cnt) xv[k] = xg(c[k]);
 #pragma unroll
   for (int k = 0; k < K; k++)
     if (k < cnt) sum = sum + v[k] * xv[k];
   return sum;
 }
+template <class T, int K>
+__device__ __forceinline__ T row_chunk(const SellView<T>& a, int e0, int cnt, const T* __restrict__ x, T sum) {
+  return row_chunk_g<T, K>(a, e0, cnt, XDirect<T>{x}, sum);
+}
 
 // Sum over one row of a slice (m = the slice's packed metadata) in stored
-// order. Coarse-level rows hold 10-20 entries and their passes are latency
-// bound, so the row is processed in chunks of 16 with all loads of a chunk
-// in flight together; the summation order is the stored order.
-template <class T>
-__device__ __forceinline__ T row_sum(const SellView<T>& a, const int4 m, int lane, const T* __restrict__ x,
-                                     T sum) {
+// order, in chunks of four entries with all loads of a chunk in flight
+// together; the summation order is the stored order.
+template <class T, class X>
+__device__ __forceinline__ T row_sum_g(const SellView<T>& a, const int4 m, int lane, const X& xg, T sum) {
   // four entries in flight per chunk: wider chunks (8 or 16) raised the
   // register count to 63 and halved the occupancy of the finest-level
   // passes (ncu: 42 % warps active, 22 % of DRAM peak)
   const int o = m.z + lane;
   const int w = m.w;
   int k = 0;
-  for (; k + 4 <= w; k += 4) sum = row_chunk<T, 4>(a, o + (k << 5), 4, x, sum);
-  if (k < w) sum = row_chunk<T, 4>(a, o + (k << 5), w - k, x, sum);
+  for (; k + 4 <= w; k += 4) sum = row_chunk_g<T, 4>(a, o + (k << 5), 4, xg, sum);
+  if (k < w) sum = row_chunk_g<T, 4>(a, o + (k << 5), w - k, xg, sum);
   return sum;
+}
+template <class T>
+__device__ __forceinline__ T row_sum(const SellView<T>& a, const int4 m, int lane, const T* __restrict__ x,
+                                     T sum) {
+  return row_sum_g(a, m, lane, XDirect<T>{x}, sum);
 }
 
 
@@ -171,18 +193,26 @@ __global__ void __launch_bounds__(kBlock, 8) k_jacobi(SellView<T> a, int nSlices
   }
 }
 
-// damped Jacobi: xnew = xold + w (xJacobi - xold)
-template <class T>
-__global__ void __launch_bounds__(kBlock, 8) k_jacobi_damped(SellView<T> a, int nSlices, const T* __restrict__ xold, T* xnew,
-                                const T* __restrict__ b, T w) {
+// damped Jacobi: xnew = xold + w (xJacobi - xold); Pro: xold is the
+// prolongation xc[ci] a pass would otherwise have assigned first
+template <class T, bool Pro>
+__global__ void __launch_bounds__(kBlock, 8) k_jacobi_damped(SellView<T> a, int nSlices, const T* __restrict__ xold,
+                                                             T* xnew, const T* __restrict__ b, T w,
+                                                             const T* __restrict__ xc, const int* __restrict__ ci) {
   FVM_PDL();
   const int lane = threadIdx.x & 31;
   for (int s = blockIdx.x * kSlicesPerBlock + (threadIdx.x >> 5); s < nSlices; s += gridDim.x * kSlicesPerBlock) {
     const int4 m = slice_meta(a, s);
     if (lane >= m.y) continue;
     const int i = m.x + lane;
-    const T sum = row_sum(a, m, lane, xold, b[i]);
-    const T xo = xold[i];
+    T sum, xo;
+    if constexpr (Pro) {
+      sum = row_sum_g(a, m, lane, XProlonged<T>{xc, ci}, b[i]);
+      xo = xc[ci[i]];
+    } else {
+      sum = row_sum(a, m, lane, xold, b[i]);
+      xo = xold[i];
+    }
     xnew[i] = xo + w * (-sum / a.diag[i] - xo);
   }
 }
@@ -284,16 +314,33 @@ __global__ void __launch_bounds__(kBlock, 8) k_spmv(SellView<double> a, int nSli
 // beat a resident-sized striding grid by 7-45 % (8M-row width-6 pass:
 // 5.8 vs 4.4 TB/s, 1M rows: 3.9 vs 2.7 TB/s). Summation in stored order,
 // as row_sum.
-template <class T, int W>
-__device__ __forceinline__ T ell_row(const SellView<T>& a, int i, const T* __restrict__ x, T sum) {
+template <class T, int W, class X>
+__device__ __forceinline__ T ell_row_g(const SellView<T>& a, int i, const X& xg, T sum) {
   const int o = (i >> 5) * (32 * W) + (i & 31);
   if constexpr (W <= 6) {
-    return row_chunk<T, W>(a, o, W, x, sum);
+    return row_chunk_g<T, W>(a, o, W, xg, sum);
   } else {
-    sum = row_chunk<T, 4>(a, o, 4, x, sum);
-    return row_chunk<T, W - 4>(a, o + 128, W - 4, x, sum);
+    sum = row_chunk_g<T, 4>(a, o, 4, xg, sum);
+    return row_chunk_g<T, W - 4>(a, o + 128, W - 4, xg, sum);
   }
 }
+template <class T, int W>
+__device__ __forceinline__ T ell_row(const SellView<T>& a, int i, const T* __restrict__ x, T sum) {
+  return ell_row_g<T, W>(a, i, XDirect<T>{x}, sum);
+}
+
+// The first forward Gauss-Seidel sweep after a prolongation that would
+// assign x = xc[ci]: rows of earlier colours (below r0 in the colour-major
+// order) already hold their new values, rows of later colours still the
+// prolonged ones, read from xc
+template <class T>
+struct XSweepProlonged {
+  const T* x;
+  const T* __restrict__ xc;
+  const int* __restrict__ ci;
+  int r0;
+  __device__ __forceinline__ T operator()(int j) const { return j < r0 ? x[j] : xc[ci[j]]; }
+};
 
 // rows [r0, r1) of one colour
 template <class T, int W>
@@ -303,6 +350,19 @@ __global__ void __launch_bounds__(kBlock, 8) k_gs_color_ell(SellView<T> a, int r
   const int i = (((r0 >> 5) + blockIdx.x * kSlicesPerBlock) << 5) + threadIdx.x;
   if (i < r0 || i >= r1) return;
   const T sum = ell_row<T, W>(a, i, x, b[i]);
+  x[i] = -sum / a.diag[i];
+}
+
+// the same colour pass in the first forward sweep after a fused
+// prolongation (XSweepProlonged): bitwise the values of prolongation + pass
+template <class T, int W>
+__global__ void __launch_bounds__(kBlock, 8) k_gs_color_ell_pro(SellView<T> a, int r0, int r1, T* x,
+                                                                const T* __restrict__ b, const T* __restrict__ xc,
+                                                                const int* __restrict__ ci) {
+  FVM_PDL();
+  const int i = (((r0 >> 5) + blockIdx.x * kSlicesPerBlock) << 5) + threadIdx.x;
+  if (i < r0 || i >= r1) return;
+  const T sum = ell_row_g<T, W>(a, i, XSweepProlonged<T>{x, xc, ci, r0}, b[i]);
   x[i] = -sum / a.diag[i];
 }
 
@@ -539,9 +599,9 @@ __global__ void k_cg_update(int n, const double* alpha, const double* __restrict
 // exactly as row_sum's does.
 // Lanes of rows past the slice's last row (live = false) take part in the
 // shuffles but load nothing: their slots of the slice hold no entries.
-template <class T, int TPR>
-__device__ __forceinline__ T row_sum_tpr(const SellView<T>& a, const int4 m, int l, bool live,
-                                         const T* __restrict__ x, T sum) {
+template <class T, int TPR, class X>
+__device__ __forceinline__ T row_sum_tpr(const SellView<T>& a, const int4 m, int l, bool live, const X& xg,
+                                         T sum) {
   constexpr int C = 4;
   const int lane = threadIdx.x & 31, sub = lane & (TPR - 1), g0 = lane & ~(TPR - 1);
   const int o = m.z + l, w = m.w;
@@ -556,7 +616,7 @@ __device__ __forceinline__ T row_sum_tpr(const SellView<T>& a, const int4 m, int
       v[q] = ok ? a.vals[o + (k << 5)] : T(0);
     }
 #pragma unroll
-    for (int q = 0; q < C; q++) p[q] = v[q] * x[c[q]];
+    for (int q = 0; q < C; q++) p[q] = v[q] * xg(c[q]);
 #pragma unroll
     for (int q = 0; q < C; q++)
 #pragma unroll
@@ -586,13 +646,16 @@ __global__ void __launch_bounds__(BLOCK) k_gs_color_tpr(SellView<T> a, int s0, i
   const int4 m = a.meta[s];
   const bool live = l < m.y;
   const int i = m.x + (live ? l : 0);
-  const T sum = row_sum_tpr<T, TPR>(a, m, l, live, x, live ? b[i] : T(0));
+  const T sum = row_sum_tpr<T, TPR>(a, m, l, live, XDirect<T>{x}, live ? b[i] : T(0));
   if (live && (threadIdx.x & (TPR - 1)) == 0) x[i] = -sum / a.diag[i];
 }
 
-template <class T, int TPR, int BLOCK>
+// Pro: the pass right after a prolongation that would assign x = xc[ci]
+// reads those values from xc directly (xold unused)
+template <class T, int TPR, int BLOCK, bool Pro>
 __global__ void __launch_bounds__(BLOCK) k_jacobi_damped_tpr(SellView<T> a, int nSlices, const T* __restrict__ xold,
-                                                             T* xnew, const T* __restrict__ b, T w) {
+                                                             T* xnew, const T* __restrict__ b, T w,
+                                                             const T* __restrict__ xc, const int* __restrict__ ci) {
   FVM_PDL();
   int s, l;
   tpr_row<TPR>(blockIdx.x * (BLOCK / 32) + (threadIdx.x >> 5), s, l);
@@ -600,9 +663,13 @@ __global__ void __launch_bounds__(BLOCK) k_jacobi_damped_tpr(SellView<T> a, int 
   const int4 m = a.meta[s];
   const bool live = l < m.y;
   const int i = m.x + (live ? l : 0);
-  const T sum = row_sum_tpr<T, TPR>(a, m, l, live, xold, live ? b[i] : T(0));
+  T sum;
+  if constexpr (Pro)
+    sum = row_sum_tpr<T, TPR>(a, m, l, live, XProlonged<T>{xc, ci}, live ? b[i] : T(0));
+  else
+    sum = row_sum_tpr<T, TPR>(a, m, l, live, XDirect<T>{xold}, live ? b[i] : T(0));
   if (live && (threadIdx.x & (TPR - 1)) == 0) {
-    const T xo = xold[i];
+    const T xo = Pro ? xc[ci[i]] : xold[i];
     xnew[i] = xo + w * (-sum / a.diag[i] - xo);
   }
 }
@@ -1203,11 +1270,17 @@ void pdl_launch(void (*kernel)(KArgs...), dim3 grid, dim3 block, cudaStream_t st
 }
 }  // namespace
 template <class T>
-void gs_color(const SellView<T>& a, int s0, int s1, T* x, const T* b, cudaStream_t st, RowPlan plan) {
+void gs_color(const SellView<T>& a, int s0, int s1, T* x, const T* b, cudaStream_t st, RowPlan plan, const T* xc,
+              const int* ci) {
   if (s1 <= s0) return;
   // ELL-32: s0, s1 are rows; the launch covers the 32-row groups they touch
   const int groups = a.ellWidth ? ((s1 - 1) >> 5) - (s0 >> 5) + 1 : s1 - s0;
   const int g = ceil_div(groups, kSlicesPerBlock);
+  if (xc) {
+#define FVM_L(W) pdl_launch(k_gs_color_ell_pro<T, W>, g, kBlock, st, a, s0, s1, x, b, xc, ci)
+    if (a.ellWidth && FVM_ELL_SWITCH(a.ellWidth, FVM_L)) return;
+#undef FVM_L
+  }
   if (a.ellWidth && plan.ellRows == 2) {
 #define FVM_L(W) pdl_launch(k_gs_color_ell2<T, W>, ceil_div(groups, 2 * kSlicesPerBlock), kBlock, st, a, s0, s1, x, b)
     if (FVM_ELL_SWITCH(a.ellWidth, FVM_L)) return;
@@ -1237,18 +1310,26 @@ void jacobi(const SellView<T>& a, int nSlices, const T* xold, T* xnew, const T* 
 }
 template <class T>
 void jacobi_damped(const SellView<T>& a, int nSlices, const T* xold, T* xnew, const T* b, T w, cudaStream_t st,
-                   RowPlan plan) {
+                   RowPlan plan, const T* xc, const int* ci) {
+  const bool pro = xc != nullptr;
+  if (a.ellWidth && !pro) {
 #define FVM_L(W) pdl_launch(k_jacobi_damped_ell<T, W>, ceil_div(a.n, kBlock), kBlock, st, a, xold, xnew, b, w)
-  if (a.ellWidth && FVM_ELL_SWITCH(a.ellWidth, FVM_L)) return;
+    if (FVM_ELL_SWITCH(a.ellWidth, FVM_L)) return;
 #undef FVM_L
+  }
   if (!a.ellWidth && !plan.isDefault()) {
 #define FVM_P(TPR, BLOCK)                                                                                          \
-  pdl_launch(k_jacobi_damped_tpr<T, TPR, BLOCK>, ceil_div((long long)nSlices * TPR, BLOCK / 32), BLOCK, st, a, nSlices, \
-             xold, xnew, b, w)
+  (pro ? pdl_launch(k_jacobi_damped_tpr<T, TPR, BLOCK, true>, ceil_div((long long)nSlices * TPR, BLOCK / 32), BLOCK, \
+                    st, a, nSlices, xold, xnew, b, w, xc, ci)                                                        \
+       : pdl_launch(k_jacobi_damped_tpr<T, TPR, BLOCK, false>, ceil_div((long long)nSlices * TPR, BLOCK / 32), BLOCK, \
+                    st, a, nSlices, xold, xnew, b, w, xc, ci))
     if (FVM_PLAN_SWITCH(plan, FVM_P)) return;
 #undef FVM_P
   }
-  pdl_launch(k_jacobi_damped<T>, reduce_blocks(nSlices), kBlock, st, a, nSlices, xold, xnew, b, w);
+  if (pro)
+    pdl_launch(k_jacobi_damped<T, true>, reduce_blocks(nSlices), kBlock, st, a, nSlices, xold, xnew, b, w, xc, ci);
+  else
+    pdl_launch(k_jacobi_damped<T, false>, reduce_blocks(nSlices), kBlock, st, a, nSlices, xold, xnew, b, w, xc, ci);
 }
 template <class T>
 void chebyshev_step(const SellView<T>& a, int nSlices, const T* x, T* xnew, T* dv, const T* b, T c1, T c2,
@@ -1970,10 +2051,12 @@ void update_solution(int nCells, const int* perm, const double* delta, const Bou
 
 // explicit instantiations
 #define FVM_INST(T)                                                                              \
-  template void gs_color<T>(const SellView<T>&, int, int, T*, const T*, cudaStream_t, RowPlan);  \
+  template void gs_color<T>(const SellView<T>&, int, int, T*, const T*, cudaStream_t, RowPlan, const T*,  \
+                            const int*);                                                                \
   template void gs_sequential<T>(const SellView<T>&, T*, const T*, bool, cudaStream_t);          \
   template void jacobi<T>(const SellView<T>&, int, const T*, T*, const T*, cudaStream_t);        \
-  template void jacobi_damped<T>(const SellView<T>&, int, const T*, T*, const T*, T, cudaStream_t, RowPlan); \
+  template void jacobi_damped<T>(const SellView<T>&, int, const T*, T*, const T*, T, cudaStream_t, RowPlan,     \
+                                 const T*, const int*);                                                          \
   template void chebyshev_step<T>(const SellView<T>&, int, const T*, T*, T*, const T*, T, T, bool, cudaStream_t); \
   template void residual<T>(const SellView<T>&, int, const T*, const T*, T*, double*, cudaStream_t); \
   template void restrict_sum<T>(int, const int*, const int*, const T*, T*, cudaStream_t);        \

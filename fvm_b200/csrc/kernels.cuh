@@ -43,8 +43,12 @@ struct RowPlan {
   bool isDefault() const { return tpr == 1 && block == 256 && ellRows == 1; }
 };
 
+// With xc (ELL-32 levels only): the pass is part of the first forward
+// sweep after a prolongation that would have assigned x = xc[ci]; rows of
+// later colours are read from xc (bitwise that prolongation + the pass)
 template <class T>
-void gs_color(const SellView<T>& a, int s0, int s1, T* x, const T* b, cudaStream_t st, RowPlan plan = RowPlan());
+void gs_color(const SellView<T>& a, int s0, int s1, T* x, const T* b, cudaStream_t st, RowPlan plan = RowPlan(),
+              const T* xc = nullptr, const int* ci = nullptr);
 // Lexicographic Gauss-Seidel by a single thread in row order (reverse when
 // asked): the reference's CRMatrix::forwardGS / reverseGS, for parity runs.
 template <class T>
@@ -52,10 +56,13 @@ void gs_sequential(const SellView<T>& a, T* x, const T* b, bool reverse, cudaStr
 // Jacobi: xnew_i = -(b_i + sum_j a_ij xold_j) / a_ii over all rows
 template <class T>
 void jacobi(const SellView<T>& a, int nSlices, const T* xold, T* xnew, const T* b, cudaStream_t st);
-// damped Jacobi: xnew = xold + w (Jacobi update - xold)
+// damped Jacobi: xnew = xold + w (Jacobi update - xold). With xc (and ci),
+// xold is taken as the prolongation xc[ci] (the values a prolongation that
+// assigns would have written; xold unused): bitwise the result of that
+// prolongation followed by this pass, one launch and one x round trip less.
 template <class T>
 void jacobi_damped(const SellView<T>& a, int nSlices, const T* xold, T* xnew, const T* b, T w, cudaStream_t st,
-                   RowPlan plan = RowPlan());
+                   RowPlan plan = RowPlan(), const T* xc = nullptr, const int* ci = nullptr);
 // one step of a Chebyshev smoother on D^-1 A over all rows: res = b + A x,
 // dv = c1 dv + c2 (-res / a_ii) (first: dv = c2 (-res / a_ii), dv not read),
 // xnew = x + dv; x and xnew distinct

@@ -635,7 +635,7 @@ template <>
 dev::SellView<float> view<float>(const DevLevel& d) { return d.view32(); }
 
 template <class T>
-void AmgHierarchy::sweeps(int nSweeps, int l, cudaStream_t st) {
+void AmgHierarchy::sweeps(int nSweeps, int l, cudaStream_t st, const T* xc, const int* ci) {
   DevLevel& d = lv_[l];
   const dev::SellView<T> a = view<T>(d);
   T* x = vec_x<T>(d);
@@ -662,7 +662,11 @@ void AmgHierarchy::sweeps(int nSweeps, int l, cudaStream_t st) {
       // launch-bound colour passes
       T* t = vec_tmp<T>(d);
       const T w = (T)opt_.jacobiWeight;
-      dev::jacobi_damped<T>(a, d.nSlices, x, t, b, w, st, d.plan);
+      // the first pass after a fused prolongation reads xc[ci] for x
+      if (s == 0 && xc)
+        dev::jacobi_damped<T>(a, d.nSlices, x, t, b, w, st, d.plan, xc, ci);
+      else
+        dev::jacobi_damped<T>(a, d.nSlices, x, t, b, w, st, d.plan);
       dev::jacobi_damped<T>(a, d.nSlices, t, x, b, w, st, d.plan);
     } else if (opt_.smootherType == kGaussSeidel) {
       if (opt_.ordering == kSequential) {
@@ -674,8 +678,12 @@ void AmgHierarchy::sweeps(int nSweeps, int l, cudaStream_t st) {
         // their (unchanged) neighbours: the next sweep's colour-0 pass would
         // write bitwise the same values, so it starts at colour 1
         const int c0 = (s > 0 && opt_.gsReverse) ? 1 : 0;
+        // after a fused prolongation the first forward pass reads the rows
+        // of colours not yet visited from xc[ci]
+        const bool pro = s == 0 && xc;
         for (int c = c0; c < C; c++)
-          dev::gs_color<T>(a, d.colorSliceStart[c], d.colorSliceStart[c + 1], x, b, st, d.plan);
+          dev::gs_color<T>(a, d.colorSliceStart[c], d.colorSliceStart[c + 1], x, b, st, d.plan, pro ? xc : nullptr,
+                           pro ? ci : nullptr);
         // reverse pass; its first colour would repeat the last update exactly
         if (opt_.gsReverse)
           for (int c = C - 2; c >= 0; c--)
@@ -722,9 +730,24 @@ void AmgHierarchy::cycle(CycleType t, int l, cudaStream_t st, bool xZero) {
       cycle<T>(kWCycle, l + 1, st);
     else if (t == kFCycle)
       cycle<T>(kVCycle, l + 1, st);
+    if (rhsOnly && fusedProlong(l)) {
+      // x = xc[ci] is read straight from the coarse level by the first
+      // damped-Jacobi pass (bitwise the same values)
+      sweeps<T>(opt_.postSweeps(l), l, st, vec_x<T>(c), d.ci);
+      return;
+    }
     dev::prolong<T>(d.n, d.ci, vec_x<T>(c), vec_x<T>(d), st, rhsOnly);
   }
   sweeps<T>(opt_.postSweeps(l), l, st);
+}
+
+bool AmgHierarchy::fusedProlong(int l) const {
+  const int L = (int)lv_.size();
+  if (l + 1 >= L || opt_.nPreSweeps != 0 || opt_.postSweeps(l) <= 0 || chebyshevLevel(l)) return false;
+  const DevLevel& d = lv_[l];
+  if (dampedLevel(l, d.n)) return true;
+  // multicolour Gauss-Seidel on an ELL-32 level (the fused colour kernel)
+  return opt_.smootherType == kGaussSeidel && opt_.ordering == kMulticolor && d.ellWidth > 0 && d.nColors > 0;
 }
 
 void AmgHierarchy::applyCycle(const double* r, cudaStream_t st) {
@@ -811,7 +834,12 @@ double AmgHierarchy::cycleBytes() const {
         total += (vb + 4.0) * d.n + (4.0 + vb) * c.n;  // b restricted; x assigned below
       else
         total += 3.0 * vb * d.n + (4.0 + vb) * d.entries + (4.0 + 2.0 * vb) * c.n;
-      total += (2.0 * vb + 4.0) * d.n + vb * c.n;
+      if (fusedProlong(l))
+        // the first Jacobi pass reads ci and xc instead of x: no x write
+        // and read of the prolongation
+        total += 4.0 * d.n + vb * c.n - vb * d.n;
+      else
+        total += (2.0 * vb + 4.0) * d.n + vb * c.n;
     }
   }
   return total;
@@ -833,7 +861,7 @@ int AmgHierarchy::kernelsPerCycle() const {
       k += colourPasses(d.nColors, opt_.nPreSweeps) + colourPasses(d.nColors, opt_.postSweeps(l));
     else
       k += 2 * sw;
-    if (l + 1 < L) k += 2;  // fused residual + restriction, prolongation
+    if (l + 1 < L) k += fusedProlong(l) ? 1 : 2;  // restriction, prolongation (unless fused)
   }
   return k;
 }

@@ -238,8 +238,13 @@ class AmgHierarchy {
   // residual is b and the restriction needs no pass over the matrix
   template <class T>
   void cycle(CycleType t, int l, cudaStream_t st, bool xZero = false);
+  // xc, ci: the first damped-Jacobi pass takes x = xc[ci] (a prolongation
+  // fused into it); x itself is not read
   template <class T>
-  void sweeps(int nSweeps, int l, cudaStream_t st);
+  void sweeps(int nSweeps, int l, cudaStream_t st, const T* xc = nullptr, const int* ci = nullptr);
+  // level l's prolongation (after a zero-guess visit) is fused into its
+  // first post-smoothing pass: damped Jacobi, no pre-smoothing
+  bool fusedProlong(int l) const;
 
   // one cycle of the configured type from the finest level (xZero: level
   // 0's x is zero on entry)

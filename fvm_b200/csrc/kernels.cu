@@ -46,9 +46,6 @@ __device__ __forceinline__ double block_sum(double v) {
   return v;
 }
 
-// Up to K entries of a row: every column and value load is issued, then
-// every x gather, then the products are accumulated in stored order -- two
-// dependent round trips to memory for the whole chunk.
 // The value of column j a row sum gathers: x[j], or, for a pass that
 // starts right after a prolongation that assigned x = xc[ci], xc[ci[j]]
 // (the same value, without the prolongation's launch and x round trip)
@@ -64,6 +61,9 @@ struct XProlonged {
   __device__ __forceinline__ T operator()(int j) const { return xc[ci[j]]; }
 };
 
+// Up to K entries of a row: every column and value load is issued, then
+// every x gather, then the products are accumulated in stored order -- two
+// dependent round trips to memory for the whole chunk.
 template <class T, int K, class X>
 __device__ __forceinline__ T row_chunk_g(const SellView<T>& a, int e0, int cnt, const X& xg, T sum) {
   int c[K];

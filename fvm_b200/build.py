@@ -92,7 +92,7 @@ def build(verbose: bool = False, force: bool = False) -> str:
             if verbose and out.strip():
                 print(out)
     if force or _newer(objs, LIB):
-        _run([nvcc] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart"])
+        _run([nvcc] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart", "-ldl"])
     return LIB
 
 

@@ -711,6 +711,7 @@ size_t size_class(size_t bytes) {
 }  // namespace
 
 bool AmgHierarchy::prepareFinestPatternDevice(const FinestDevice& in) {
+  TraceRange traceRange("level-0 pattern on the device");
   const int n = in.conn->nRows;
   if (n <= 0 || !in.ccRow || !in.ccCol || !in.cfRow || !in.cfCol || !in.faceCells || !in.symmetricPattern)
     return false;
@@ -914,6 +915,7 @@ void AmgHierarchy::allocVectors(DevLevel& d, bool mixed) {
 }
 
 void AmgHierarchy::buildDevice(const FinestDevice& in, const SolverOptions& opt) {
+  TraceRange traceRange("AMG hierarchy on the device");
   const bool trace = getenv("FVM_TRACE") != nullptr;
   auto t0 = std::chrono::steady_clock::now();
   auto lap = [&](const char* what) {

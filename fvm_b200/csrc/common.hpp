@@ -2,6 +2,8 @@
 // compressed-row (CSR) containers and CUDA call checking.
 #pragma once
 
+#include <nvtx3/nvToolsExt.h>
+
 #include <algorithm>
 #include <cstdint>
 #include <stdexcept>
@@ -10,6 +12,15 @@
 #include <vector>
 
 namespace fvm {
+
+// An NVTX range over a scope (setup phases, outer iterations, linear
+// solves): visible on a profiler's timeline, no cost without one.
+struct TraceRange {
+  explicit TraceRange(const char* name) { nvtxRangePushA(name); }
+  ~TraceRange() { nvtxRangePop(); }
+  TraceRange(const TraceRange&) = delete;
+  TraceRange& operator=(const TraceRange&) = delete;
+};
 
 // Status codes returned through the C ABI (mirrored in include/fvm_b200.h).
 enum Status {

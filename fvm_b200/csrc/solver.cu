@@ -109,6 +109,7 @@ std::vector<int> AmgHierarchy::sizes() const {
 }
 
 void AmgHierarchy::build(std::vector<RefLevel>& levels, int finestLocalSize, const SolverOptions& opt) {
+  TraceRange traceRange("AMG hierarchy (reference aggregation)");
   const bool trace = getenv("FVM_TRACE") != nullptr;
   auto t0 = std::chrono::steady_clock::now();
   auto lap = [&](const char* what) {

@@ -543,6 +543,7 @@ void ThermalModel::linearize() {
 
 void ThermalModel::advance(int niter, AdvanceReport& rep) {
   FVM_REQUIRE(initialized_, kBadArgument, "ThermalModel.init() must be called before advance()");
+  TraceRange traceAdvance("ThermalModel::advance");
   rep = AdvanceReport();
   ensureDevice();
   cudaEvent_t e0, e1, e2;
@@ -554,7 +555,10 @@ void ThermalModel::advance(int niter, AdvanceReport& rep) {
   uploadFields();
   CUDA_OK(cudaEventRecord(e0, stream_));
   const auto s0 = std::chrono::steady_clock::now();
-  ensureMatrix();
+  {
+    TraceRange traceSetup("setup (matrix, AMG hierarchy)");
+    ensureMatrix();
+  }
   const auto s1 = std::chrono::steady_clock::now();
   rep.setupSeconds = std::chrono::duration<double>(s1 - s0).count();
   CUDA_OK(cudaEventRecord(e1, stream_));
@@ -570,13 +574,20 @@ void ThermalModel::advance(int niter, AdvanceReport& rep) {
       ensureMatrix();
       rep.setupSeconds += std::chrono::duration<double>(std::chrono::steady_clock::now() - s2).count();
     }
-    linearize();
+    {
+      TraceRange traceLin("linearize");
+      linearize();
+    }
     rep.launches += 4;
     if (dSegNorm_) {
       k_segment_l1<<<numSegments(), 256, 0, stream_>>>(dSegOff_, dPerm_, hier_.level(0).b, dSegNorm_);
       rep.launches += 1;
     }
-    SolveReport sr = solver_->solve(stream_);
+    SolveReport sr;
+    {
+      TraceRange traceSolve("linear solve");
+      sr = solver_->solve(stream_);
+    }
     const double rNorm = sr.initialNorm;
     if (initialNorm_ < 0) initialNorm_ = rNorm;
     dev::update_solution(m.nCells, dPerm_, hier_.level(0).x, bd, dFaceCells_, dCoeff_, dT_,

@@ -713,7 +713,9 @@ size_t size_class(size_t bytes) {
 bool AmgHierarchy::prepareFinestPatternDevice(const FinestDevice& in) {
   TraceRange traceRange("level-0 pattern on the device");
   const int n = in.conn->nRows;
-  if (n <= 0 || !in.ccRow || !in.ccCol || !in.cfRow || !in.cfCol || !in.faceCells || !in.symmetricPattern)
+  // ELL-32 needs at least 32768 rows (the host packing's rule); smaller
+  // levels are packed on the host, where they take a few milliseconds
+  if (n < 32768 || !in.ccRow || !in.ccCol || !in.cfRow || !in.cfCol || !in.faceCells || !in.symmetricPattern)
     return false;
   constexpr int kFewColors = 5;
   cudaStream_t st = setupStream_;
@@ -778,7 +780,7 @@ bool AmgHierarchy::prepareFinestPatternDevice(const FinestDevice& in) {
   for (int c = 0; c < 32; c++)
     if (h[8 + c] > 0) C = c + 1;
   const int maxWidth = h[3];
-  if (C < 1 || C > kFewColors || maxWidth > 8 || n < 32768) return false;
+  if (C < 1 || C > kFewColors || maxWidth > 8) return false;
   PackedLevel& pk = fp.packed;
   pk.n = n;
   pk.nColors = C;

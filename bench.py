@@ -953,7 +953,9 @@ def main():
                                  "each launch) over their algorithmic bytes, %.3f, times the pass's algorithmic "
                                  "bytes" % NCU_TRAFFIC_RATIO[args.workload])
                 if args.workload in NCU_TRAFFIC_RATIO else None,
-                "kernel": "k_gs_color_ell<float, W> (one pass over all colours, finest level)",
+                "kernel": "k_gs_color_ell%s<float, W> (one pass over all colours of the finest level, the autotuned "
+                          "plan: %s)" % ("2" if mixed["plans"][0][1] == -2 else "",
+                                         plan_name(mixed["plans"][0])),
                 "peak_kind": peak_kind,
                 "fp64_gs_pass": {"achieved": pp["gs_pass_bytes"] / (pp["gs_pass_ms"] * 1e-3) / 1e9,
                                  "frac": pp["gs_pass_bytes"] / (pp["gs_pass_ms"] * 1e-3) / 1e9 / peak},

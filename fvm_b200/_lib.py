@@ -54,6 +54,7 @@ class LinearOptions(ctypes.Structure):
         ("chebyshevFraction", ctypes.c_double),
         ("gsReverse", ctypes.c_int),
         ("patternOnDevice", ctypes.c_int),
+        ("fuseProlongation", ctypes.c_int),
     ]
 
 

@@ -111,6 +111,7 @@ SolverOptions to_solver(const fvm_linear_options& o) {
   s.chebyshevFraction = o.chebyshevFraction;
   s.gsReverse = o.gsReverse != 0;
   s.patternOnDevice = o.patternOnDevice != 0;
+  s.fuseProlongation = o.fuseProlongation != 0;
   FVM_REQUIRE(o.matchRounds >= 1 && o.matchRounds <= 64, kBadArgument, "matchRounds must be in [1, 64]");
   FVM_REQUIRE(o.matchBeta >= 0.0 && o.matchBeta <= 1.0, kBadArgument, "matchBeta must be in [0, 1]");
   s.setupOnDevice = o.setupOnDevice != 0;
@@ -159,6 +160,7 @@ void from_solver(const SolverOptions& s, fvm_linear_options& o) {
   o.chebyshevFraction = s.chebyshevFraction;
   o.gsReverse = s.gsReverse ? 1 : 0;
   o.patternOnDevice = s.patternOnDevice ? 1 : 0;
+  o.fuseProlongation = s.fuseProlongation ? 1 : 0;
 }
 
 RefLevel level_from_csr(int n, const int* row, const int* col, const double* diag, const double* off) {

@@ -744,7 +744,8 @@ void AmgHierarchy::cycle(CycleType t, int l, cudaStream_t st, bool xZero) {
 
 bool AmgHierarchy::fusedProlong(int l) const {
   const int L = (int)lv_.size();
-  if (l + 1 >= L || opt_.nPreSweeps != 0 || opt_.postSweeps(l) <= 0 || chebyshevLevel(l)) return false;
+  if (!opt_.fuseProlongation || l + 1 >= L || opt_.nPreSweeps != 0 || opt_.postSweeps(l) <= 0 || chebyshevLevel(l))
+    return false;
   const DevLevel& d = lv_[l];
   if (dampedLevel(l, d.n)) return true;
   // multicolour Gauss-Seidel on an ELL-32 level (the fused colour kernel)

@@ -86,6 +86,9 @@ struct SolverOptions {
   // GPU-built hierarchies: colour and pack level 0 on the device when the
   // pattern is there (the same colouring and packing as on the host)
   bool patternOnDevice = true;
+  // a zero-guess cycle without pre-smoothing folds each prolongation into
+  // the level's first post-smoothing pass (bitwise the same result)
+  bool fuseProlongation = true;
   int postSweeps(int l) const { return l > 0 && coarsePostSweeps >= 0 ? coarsePostSweeps : nPostSweeps; }
   // only the finest level is needed (Jacobi solver or preconditioner)
   bool finestOnly() const { return solver == kSolverJacobi || preconditioner == kPrecJacobi; }

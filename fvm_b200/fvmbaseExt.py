@@ -200,6 +200,7 @@ class AMG(LinearSolver):
         self.chebyshevFraction = d.chebyshevFraction
         self.gsReverse = bool(d.gsReverse)  # Gauss-Seidel sweep: forward + reverse (reference) or forward only
         self.patternOnDevice = bool(d.patternOnDevice)  # finest level of a GPU-built hierarchy packed on the GPU
+        self.fuseProlongation = bool(d.fuseProlongation)  # prolongation folded into the first smoothing pass
         self.setupOnDevice = bool(d.setupOnDevice)
         self.matchRounds = d.matchRounds
         self.matchBeta = d.matchBeta
@@ -247,6 +248,7 @@ class AMG(LinearSolver):
         o.chebyshevFraction = float(self.chebyshevFraction)
         o.gsReverse = int(bool(self.gsReverse))
         o.patternOnDevice = int(bool(self.patternOnDevice))
+        o.fuseProlongation = int(bool(self.fuseProlongation))
         o.setupOnDevice = int(bool(self.setupOnDevice))
         o.matchRounds = int(self.matchRounds)
         o.matchBeta = float(self.matchBeta)

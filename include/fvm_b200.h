@@ -100,6 +100,9 @@ typedef struct fvm_linear_options {
                                preconditioner: for flexible CG or standalone AMG) */
   int patternOnDevice;      /* setupOnDevice: 1 colours and packs a new mesh's finest level on the
                                GPU (the same colouring and packing as the host's), 0 on the host */
+  int fuseProlongation;     /* 1: a zero-guess cycle without pre-smoothing folds each prolongation
+                               into the level's first post-smoothing pass (bitwise the same result),
+                               0: separate prolongation launches */
 } fvm_linear_options;
 
 /* ThermalModelOptions (fvmbase/ThermalBC.h:33-67) + volume-condition constants */

@@ -55,6 +55,7 @@ class LinearOptions(ctypes.Structure):
         ("gsReverse", ctypes.c_int),
         ("patternOnDevice", ctypes.c_int),
         ("fuseProlongation", ctypes.c_int),
+        ("outerOnDevice", ctypes.c_int),
     ]
 
 
@@ -85,6 +86,7 @@ class Report(ctypes.Structure):
         ("launches", ctypes.c_longlong),
         ("learnedSteps", ctypes.c_int),
         ("learnedAccepted", ctypes.c_int),
+        ("outerOnDevice", ctypes.c_int),
     ]
 
 

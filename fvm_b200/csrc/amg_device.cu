@@ -916,7 +916,17 @@ void AmgHierarchy::allocVectors(DevLevel& d, bool mixed) {
   }
 }
 
-void AmgHierarchy::buildDevice(const FinestDevice& in, const SolverOptions& opt) {
+int* AmgHierarchy::pendingStatus() { return reinterpret_cast<int*>(pinnedScalars() + 31); }
+
+void AmgHierarchy::finishBuild() {
+  if (!setupStream_) return;
+  CUDA_OK(cudaStreamSynchronize(setupStream_));
+  if (!inversePending_) return;
+  inversePending_ = false;
+  FVM_REQUIRE(*pendingStatus() == 0, kBadArgument, "singular coarsest-level matrix");
+}
+
+void AmgHierarchy::buildDevice(const FinestDevice& in, const SolverOptions& opt, bool deferCheck) {
   TraceRange traceRange("AMG hierarchy on the device");
   const bool trace = getenv("FVM_TRACE") != nullptr;
   auto t0 = std::chrono::steady_clock::now();
@@ -1082,6 +1092,13 @@ void AmgHierarchy::buildDevice(const FinestDevice& in, const SolverOptions& opt)
     }
   }
   const int L = (int)lv_.size();
+  // launch plans before the coarsest inverse (the tuning does not run the
+  // coarsest level): the inverse is the last GPU work of the build, and the
+  // host may queue or prepare other work while it runs
+  CUDA_OK(cudaStreamSynchronize(st));
+  prepareChebyshev();
+  tunePlans();
+  lap("launch plans");
   // coarsest direct solve: dense inverse built on the GPU (no pivoting when
   // the level is diagonally dominant), FP32 copy for the FP32 cycle
   if (opt.coarseSolver == kCoarseDirect) {
@@ -1147,21 +1164,21 @@ void AmgHierarchy::buildDevice(const FinestDevice& in, const SolverOptions& opt)
         dev::dense_from_sell(c.view64(), c.nSlices, dA, st);
         dev::gauss_jordan_inverse(c.n, dA, coarseInv_, gjScratch, st);
       }
-      CUDA_OK(cudaMemcpyAsync(hflags, dev::gauss_jordan_status(c.n, gjScratch), sizeof(int), cudaMemcpyDeviceToHost,
-                              st));
-      CUDA_OK(cudaStreamSynchronize(st));
-      FVM_REQUIRE(hflags[0] == 0, kBadArgument, "singular coarsest-level matrix");
+      // the status is read by finishBuild
+      CUDA_OK(cudaMemcpyAsync(pendingStatus(), dev::gauss_jordan_status(c.n, gjScratch), sizeof(int),
+                              cudaMemcpyDeviceToHost, st));
+      inversePending_ = true;
     }
     if (mixed) {
       coarseInvF_ = (float*)arena_.alloc(size_class(sizeof(float) * nn));
       dev::cast_d2f(nn, coarseInv_, coarseInvF_, st);
     }
-    lap("coarsest inverse");
+    if (trace) {
+      finishBuild();
+      lap("coarsest inverse");
+    }
   }
-  CUDA_OK(cudaStreamSynchronize(st));
-  prepareChebyshev();
-  tunePlans();
-  lap("launch plans");
+  if (!deferCheck) finishBuild();
   if (trace) {
     fprintf(stderr, "[fvm device setup] levels:");
     for (int l = 0; l < L; l++) fprintf(stderr, " %d", lv_[l].n);

@@ -112,6 +112,7 @@ SolverOptions to_solver(const fvm_linear_options& o) {
   s.gsReverse = o.gsReverse != 0;
   s.patternOnDevice = o.patternOnDevice != 0;
   s.fuseProlongation = o.fuseProlongation != 0;
+  s.outerOnDevice = o.outerOnDevice != 0;
   FVM_REQUIRE(o.matchRounds >= 1 && o.matchRounds <= 64, kBadArgument, "matchRounds must be in [1, 64]");
   FVM_REQUIRE(o.matchBeta >= 0.0 && o.matchBeta <= 1.0, kBadArgument, "matchBeta must be in [0, 1]");
   s.setupOnDevice = o.setupOnDevice != 0;
@@ -161,6 +162,7 @@ void from_solver(const SolverOptions& s, fvm_linear_options& o) {
   o.gsReverse = s.gsReverse ? 1 : 0;
   o.patternOnDevice = s.patternOnDevice ? 1 : 0;
   o.fuseProlongation = s.fuseProlongation ? 1 : 0;
+  o.outerOnDevice = s.outerOnDevice ? 1 : 0;
 }
 
 RefLevel level_from_csr(int n, const int* row, const int* col, const double* diag, const double* off) {
@@ -493,6 +495,7 @@ int fvm_thermal_advance(fvm_thermal* h, int niter, fvm_report* rep) {
       rep->launches = r.launches;
       rep->learnedSteps = r.learnedSteps;
       rep->learnedAccepted = r.learnedAccepted;
+      rep->outerOnDevice = r.outerOnDevice ? 1 : 0;
     }
   });
 }

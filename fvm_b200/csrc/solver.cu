@@ -78,6 +78,9 @@ T take_spare(std::vector<T>& spares, size_t l) {
 }  // namespace
 
 void AmgHierarchy::release() {
+  // nothing of the arena may still be in use by the setup stream
+  if (setupStream_) cudaStreamSynchronize(setupStream_);
+  inversePending_ = false;
   deviceBuilt_ = false;
   arena_.release();
   lv_.clear();
@@ -98,6 +101,7 @@ double* AmgHierarchy::pinnedScalars() {
 }
 
 AmgHierarchy::~AmgHierarchy() {
+  if (setupStream_) cudaStreamSynchronize(setupStream_);
   if (pinned_) cudaFreeHost(pinned_);
   if (setupStream_) cudaStreamDestroy(setupStream_);
 }
@@ -1392,9 +1396,7 @@ SolveReport LinearSolve::solveCG(cudaStream_t st) {
   double* P = work_ + 3 * (size_t)n_;
   double* Q = work_ + 4 * (size_t)n_;
   double* B = work_ + 5 * (size_t)n_;
-  const bool flexible = o.preconditioner == kPrecAMG &&
-                        (o.precision == kMixed || o.nPreSweeps != o.nPostSweeps || o.cycleType != kVCycle ||
-                         !o.gsReverse || o.chebyshevDegree > 0);
+  const bool flexible = cgFlexible();
   SolveReport rep;
   // the whole solve on the device when nothing needs the host between
   // iterations (no learned step, no printing)
@@ -1551,7 +1553,21 @@ SolveReport LinearSolve::solveCG(cudaStream_t st) {
   return rep;
 }
 
-bool LinearSolve::buildCGLoop(cudaStream_t st, bool flexible) {
+bool graph_leaves(cudaGraph_t g, std::vector<cudaGraphNode_t>& leaves) {
+  leaves.clear();
+  size_t nn = 0;
+  if (cudaGraphGetNodes(g, nullptr, &nn) != cudaSuccess) return false;
+  std::vector<cudaGraphNode_t> nodes(nn);
+  if (nn && cudaGraphGetNodes(g, nodes.data(), &nn) != cudaSuccess) return false;
+  for (size_t k = 0; k < nn; k++) {
+    size_t nd = 0;
+    if (cudaGraphNodeGetDependentNodes(nodes[k], nullptr, &nd) != cudaSuccess) return false;
+    if (nd == 0) leaves.push_back(nodes[k]);
+  }
+  return true;
+}
+
+bool LinearSolve::addCGLoop(cudaGraph_t g, cudaStream_t st, bool flexible, bool hostCopies) {
   const SolverOptions& o = h_.options();
   DevLevel& d = h_.level(0);
   const bool mixedCycle = o.precision == kMixed;
@@ -1564,17 +1580,20 @@ bool LinearSolve::buildCGLoop(cudaStream_t st, bool flexible) {
   double* P = work_ + 3 * (size_t)n_;
   double* Q = work_ + 4 * (size_t)n_;
   double* B = mixedCycle ? d.b : work_ + 5 * (size_t)n_;
-  if (gLoop_) cudaGraphExecDestroy(gLoop_);
-  gLoop_ = nullptr;
   if (!loopInt_) loopInt_ = (int*)h_.scratch(4 * sizeof(int));
-  history_ = (double*)h_.scratch(sizeof(double) * (size_t)(o.nMaxIterations + 2));
+  if (!history_ || historyCap_ < o.nMaxIterations + 2) {
+    history_ = (double*)h_.scratch(sizeof(double) * (size_t)(o.nMaxIterations + 2));
+    historyCap_ = o.nMaxIterations + 2;
+  }
   const cudaStreamCaptureMode mode = cudaStreamCaptureModeThreadLocal;
-  cudaGraph_t g = nullptr;
   cudaGraphConditionalHandle h = 0;
-  bool ok = cudaGraphCreate(&g, 0) == cudaSuccess &&
+  // the loop goes after whatever g already holds
+  std::vector<cudaGraphNode_t> before;
+  bool ok = graph_leaves(g, before) &&
             cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault) == cudaSuccess;
   // prologue: x = 0, p = 0, z = 0, r = b, |r| (host copies of b kept in B)
-  ok = ok && cudaStreamBeginCaptureToGraph(st, g, nullptr, nullptr, 0, mode) == cudaSuccess;
+  ok = ok && cudaStreamBeginCaptureToGraph(st, g, before.empty() ? nullptr : before.data(), nullptr, before.size(),
+                                           mode) == cudaSuccess;
   if (ok) {
     try {
       CUDA_OK(cudaMemsetAsync(X, 0, sizeof(double) * (size_t)n_, st));
@@ -1595,15 +1614,8 @@ bool LinearSolve::buildCGLoop(cudaStream_t st, bool flexible) {
   cudaGraphNode_t cnode = nullptr;
   cudaGraph_t body = nullptr;
   if (ok) {
-    size_t nn = 0;
-    ok = cudaGraphGetNodes(g, nullptr, &nn) == cudaSuccess && nn > 0;
-    std::vector<cudaGraphNode_t> nodes(nn), leaves;
-    ok = ok && cudaGraphGetNodes(g, nodes.data(), &nn) == cudaSuccess;
-    for (size_t k = 0; ok && k < nn; k++) {
-      size_t nd = 0;
-      ok = cudaGraphNodeGetDependentNodes(nodes[k], nullptr, &nd) == cudaSuccess;
-      if (ok && nd == 0) leaves.push_back(nodes[k]);
-    }
+    std::vector<cudaGraphNode_t> leaves;
+    ok = graph_leaves(g, leaves);
     cudaGraphNodeParams cp = {};
     cp.type = cudaGraphNodeTypeConditional;
     cp.conditional.handle = h;
@@ -1652,15 +1664,57 @@ bool LinearSolve::buildCGLoop(cudaStream_t st, bool flexible) {
       norm_into(R, scal_ + kNorm, st);
       if (X != d.x) dev::copy_d(n_, X, d.x, st);
       if (B != d.b) dev::copy_d(n_, B, d.b, st);
-      CUDA_OK(cudaMemcpyAsync(hostScal_, scal_ + kNorm, sizeof(double), cudaMemcpyDeviceToHost, st));
-      CUDA_OK(cudaMemcpyAsync(hostScal_ + 1, history_, sizeof(double), cudaMemcpyDeviceToHost, st));
-      CUDA_OK(cudaMemcpyAsync(hostScal_ + 2, loopInt_, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
+      if (hostCopies) {
+        CUDA_OK(cudaMemcpyAsync(hostScal_, scal_ + kNorm, sizeof(double), cudaMemcpyDeviceToHost, st));
+        CUDA_OK(cudaMemcpyAsync(hostScal_ + 1, history_, sizeof(double), cudaMemcpyDeviceToHost, st));
+        CUDA_OK(cudaMemcpyAsync(hostScal_ + 2, loopInt_, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
+      }
     } catch (const Error&) {
       ok = false;
     }
     cudaGraph_t ee = nullptr;
     ok = cudaStreamEndCapture(st, &ee) == cudaSuccess && ok;
   }
+  if (!ok) cudaGetLastError();
+  return ok;
+}
+
+// The FP32 cycle, unequal sweeps, W cycles, one-directional or Chebyshev
+// smoothing make the preconditioner non-symmetric or variable: CG then takes
+// the flexible (Polak-Ribiere) beta.
+bool LinearSolve::cgFlexible() const {
+  const SolverOptions& o = h_.options();
+  return o.preconditioner == kPrecAMG &&
+         (o.precision == kMixed || o.nPreSweeps != o.nPostSweeps || o.cycleType != kVCycle || !o.gsReverse ||
+          o.chebyshevDegree > 0);
+}
+
+bool LinearSolve::deviceSolvable() const {
+  const SolverOptions& o = h_.options();
+  return o.solver == kSolverCG && o.preconditioner == kPrecAMG && o.useGraphs && o.verbosity <= 0 &&
+         !(learned_ && learnedActive_) && !graphsFailed_ && !loopFailed_;
+}
+
+LinearSolve::LoopKey LinearSolve::loopKey() const {
+  const SolverOptions& o = h_.options();
+  return LoopKey{cgFlexible(), o.nMaxIterations, o.relativeTolerance, o.absoluteTolerance};
+}
+
+void LinearSolve::prebuild(cudaStream_t st) {
+  if (!deviceSolvable() || gLoop_) return;
+  if (!buildCGLoop(st, cgFlexible())) loopFailed_ = true;
+}
+
+bool LinearSolve::appendDeviceSolve(cudaGraph_t g, cudaStream_t st) {
+  return deviceSolvable() && addCGLoop(g, st, cgFlexible(), false);
+}
+
+bool LinearSolve::buildCGLoop(cudaStream_t st, bool flexible) {
+  const SolverOptions& o = h_.options();
+  if (gLoop_) cudaGraphExecDestroy(gLoop_);
+  gLoop_ = nullptr;
+  cudaGraph_t g = nullptr;
+  bool ok = cudaGraphCreate(&g, 0) == cudaSuccess && addCGLoop(g, st, flexible, true);
   if (ok) {
     size_t nn = 0;
     cudaGraphGetNodes(g, nullptr, &nn);

@@ -89,6 +89,9 @@ struct SolverOptions {
   // a zero-guess cycle without pre-smoothing folds each prolongation into
   // the level's first post-smoothing pass (bitwise the same result)
   bool fuseProlongation = true;
+  // a thermal model's advance() runs all its outer iterations as one CUDA
+  // graph when the solve needs no host step (deviceSolvable)
+  bool outerOnDevice = true;
   int postSweeps(int l) const { return l > 0 && coarsePostSweeps >= 0 ? coarsePostSweeps : nPostSweeps; }
   // only the finest level is needed (Jacobi solver or preconditioner)
   bool finestOnly() const { return solver == kSolverJacobi || preconditioner == kPrecJacobi; }
@@ -203,7 +206,11 @@ class AmgHierarchy {
   // (opt.setupOnDevice): pairwise matching, Galerkin products and SELL-32
   // packing as kernels; only level 0's colouring is host work, once per
   // pattern. refLevels() is then empty and packed(l) exists for l = 0 only.
-  void buildDevice(const FinestDevice& in, const SolverOptions& opt);
+  // The coarsest inverse is the build's last GPU work; with deferCheck the
+  // call returns while it runs (the host may build graphs meanwhile) and
+  // finishBuild() waits for it and checks it, before any solve.
+  void buildDevice(const FinestDevice& in, const SolverOptions& opt, bool deferCheck = false);
+  void finishBuild();
   bool deviceBuilt() const { return deviceBuilt_; }
   // device-built: reference row -> level-0 row, on the device
   const int* finestPermDevice() const { return deviceBuilt_ && finest_ ? finest_->perm : nullptr; }
@@ -291,6 +298,10 @@ class AmgHierarchy {
   std::vector<PackedLevel> sparePacked_;
   std::vector<CSR> spareC2f_;
   double* pinned_ = nullptr;
+  // the coarsest inverse's status, read back into the last pinned scalar,
+  // not yet checked
+  bool inversePending_ = false;
+  int* pendingStatus();
   std::vector<DevLevel> lv_;
   double* coarseInv_ = nullptr;  // dense inverse of the coarsest level
   float* coarseInvF_ = nullptr;  // its FP32 copy for the FP32 cycle
@@ -326,6 +337,9 @@ class AmgHierarchy {
   void restrictPass(int l, bool split, cudaStream_t st);
 };
 
+// nodes of g that no node depends on
+bool graph_leaves(cudaGraph_t g, std::vector<cudaGraphNode_t>& leaves);
+
 // Linear solve of the finest system held by the hierarchy: level 0's b is
 // the right-hand side, level 0's x the delta (zeroed on entry).
 class LinearSolve {
@@ -342,7 +356,34 @@ class LinearSolve {
   int solveRecording(cudaStream_t st, double relTol, int maxIter, int record, const std::vector<double*>& rs,
                      const std::vector<double*>& xs, SolveReport& rep);
 
+  // The whole solve can run inside a graph with no host step: CG under the
+  // AMG cycle, graphs on, no printing, no active learned step.
+  bool deviceSolvable() const;
+  // Appends that solve to g after its current leaves (no host copies):
+  // afterwards deviceLoopState() holds {iterations, status} (status 1
+  // converged, 2 non-finite, 3 iteration limit) and deviceInitialNorm()
+  // the L1 norm of the right-hand side. False when a graph call failed (g
+  // is then unusable).
+  bool appendDeviceSolve(cudaGraph_t g, cudaStream_t st);
+  // builds the graph of solveCG's device loop now (when it will be used)
+  // rather than in the first solve
+  void prebuild(cudaStream_t st);
+  const int* deviceLoopState() const { return loopInt_; }
+  const double* deviceInitialNorm() const { return history_; }
+  long long loopBodyNodes() const { return loopBodyNodes_; }
+  // the CG settings a graph from appendDeviceSolve bakes in
+  struct LoopKey {
+    bool flexible;
+    int maxIt;
+    double rel, abs;
+    bool operator==(const LoopKey& o) const {
+      return flexible == o.flexible && maxIt == o.maxIt && rel == o.rel && abs == o.abs;
+    }
+  };
+  LoopKey loopKey() const;
+
  private:
+  bool cgFlexible() const;
   SolveReport solveAMG(cudaStream_t st);
   SolveReport solveCG(cudaStream_t st);
   // CG with the fused iteration, every iteration of one solve inside one
@@ -351,6 +392,11 @@ class LinearSolve {
   // Returns false (and is not used again) when the graph cannot be built.
   bool solveCGLoop(cudaStream_t st, bool flexible, SolveReport& rep);
   bool buildCGLoop(cudaStream_t st, bool flexible);
+  // appends the CG loop (prologue, while node, epilogue) to g after its
+  // current leaves; hostCopies: the epilogue also copies the final norm,
+  // the initial norm and the loop state to the pinned host scalars
+  bool addCGLoop(cudaGraph_t g, cudaStream_t st, bool flexible, bool hostCopies);
+  int historyCap_ = 0;
   cudaGraphExec_t gLoop_ = nullptr;
   bool loopFailed_ = false;
   bool loopFlexible_ = false;

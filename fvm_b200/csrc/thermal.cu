@@ -36,6 +36,9 @@ ThermalModel::ThermalModel(std::shared_ptr<HostMesh> mesh) : mesh_(std::move(mes
 }
 
 ThermalModel::~ThermalModel() {
+  releaseAdvanceGraph();
+  if (dOuter_) cudaFree(dOuter_);
+  if (hOuter_) cudaFreeHost(hOuter_);
   solver_.reset();
   hier_.release();
   freeDevice();
@@ -45,6 +48,7 @@ ThermalModel::~ThermalModel() {
 }
 
 void ThermalModel::freeDevice() {
+  releaseAdvanceGraph();
   arena_.release();
   dPerm_ = nullptr;  // lives in the hierarchy's arena
   if (stream_) cudaStreamDestroy(stream_);
@@ -132,7 +136,200 @@ __global__ void k_segment_l1(const int* __restrict__ off, const int* __restrict_
   }
   if (threadIdx.x == 0) out[s] = red[0];
 }
+
+// Outer-loop state of advance() on the device; the outer norms follow it at
+// kOuterHead bytes.
+struct OuterState {
+  double initialNorm;    // in: the model's first outer norm (< 0: none yet); out: as updated
+  double absTol, relTol; // in: the outer tolerances
+  int niter;             // in: outer iterations allowed
+  int iterations;        // out: outer iterations completed
+  int linearIterations;  // out: CG iterations over them
+  int status;            // out: 0 running, 1 converged, 3 niter reached, 2 initial residual
+                         // non-finite, 4 residual became non-finite
+};
+constexpr size_t kOuterHead = 64;
+constexpr int kOuterHistory = 4096;  // outer norms a graph records before a longer call rebuilds it
+static_assert(sizeof(OuterState) <= kOuterHead, "outer state header");
+
+__global__ void k_outer_init(OuterState* s, cudaGraphConditionalHandle hOuter) {
+  s->iterations = 0;
+  s->linearIterations = 0;
+  s->status = 0;
+  cudaGraphSetConditional(hOuter, s->niter > 0 ? 1u : 0u);
+}
+
+// The test of the host loop of advance() on this outer iteration's linear
+// system: rNorm is the L1 norm of its right-hand side (the CG's initial
+// norm). A non-finite solve ends the loop before the update, as the host
+// loop's exception does.
+__global__ void k_outer_check(OuterState* s, double* hist, const double* cgInitialNorm, const int* cgLoop,
+                              cudaGraphConditionalHandle hOuter, cudaGraphConditionalHandle hUpdate) {
+  const double rNorm = cgInitialNorm[0];
+  int status = 0;
+  if (!isfinite(rNorm)) {
+    status = 2;
+  } else if (cgLoop[1] == 2) {
+    status = 4;
+  } else {
+    const int it = s->iterations;
+    hist[it] = rNorm;
+    s->iterations = it + 1;
+    s->linearIterations += cgLoop[0];
+    if (s->initialNorm < 0) s->initialNorm = rNorm;
+    const double ratio = s->initialNorm > 0 ? rNorm / s->initialNorm : 0.0;
+    if (rNorm < s->absTol || ratio < s->relTol)
+      status = 1;
+    else if (it + 1 >= s->niter)
+      status = 3;
+  }
+  s->status = status;
+  cudaGraphSetConditional(hUpdate, status == 2 || status == 4 ? 0u : 1u);
+  cudaGraphSetConditional(hOuter, status == 0 ? 1u : 0u);
+}
 }  // namespace
+
+void ThermalModel::releaseAdvanceGraph() {
+  if (gAdvance_) cudaGraphExecDestroy(gAdvance_);
+  gAdvance_ = nullptr;
+}
+
+bool ThermalModel::buildAdvanceGraph(int historyCap) {
+  const auto t0 = std::chrono::steady_clock::now();
+  releaseAdvanceGraph();
+  if (historyCap > advHistoryCap_) {
+    if (dOuter_) cudaFree(dOuter_);
+    if (hOuter_) cudaFreeHost(hOuter_);
+    dOuter_ = hOuter_ = nullptr;
+    advHistoryCap_ = 0;
+    const size_t bytes = kOuterHead + sizeof(double) * (size_t)historyCap;
+    CUDA_OK(cudaMalloc(&dOuter_, bytes));
+    CUDA_OK(cudaMallocHost(&hOuter_, bytes));
+    advHistoryCap_ = historyCap;
+  }
+  OuterState* state = (OuterState*)dOuter_;
+  double* hist = (double*)((char*)dOuter_ + kOuterHead);
+  const dev::BoundaryData bd = boundaryData();
+  const int nCells = mesh_->nCells;
+  const cudaStreamCaptureMode mode = cudaStreamCaptureModeThreadLocal;
+  // fn's launches on stream_ go into gr after its current leaves
+  auto capture = [&](cudaGraph_t gr, const std::function<void()>& fn) {
+    std::vector<cudaGraphNode_t> leaves;
+    if (!graph_leaves(gr, leaves)) return false;
+    if (cudaStreamBeginCaptureToGraph(stream_, gr, leaves.empty() ? nullptr : leaves.data(), nullptr, leaves.size(),
+                                      mode) != cudaSuccess)
+      return false;
+    bool ok = true;
+    try {
+      fn();
+    } catch (const Error&) {
+      ok = false;
+    }
+    cudaGraph_t out = nullptr;
+    return cudaStreamEndCapture(stream_, &out) == cudaSuccess && ok;
+  };
+  // a conditional node after gr's leaves; its body graph in *bodyOut
+  auto conditional = [&](cudaGraph_t gr, cudaGraphConditionalHandle h, cudaGraphConditionalNodeType type,
+                         cudaGraph_t* bodyOut) {
+    std::vector<cudaGraphNode_t> leaves;
+    if (!graph_leaves(gr, leaves) || leaves.empty()) return false;
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h;
+    cp.conditional.type = type;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node = nullptr;
+    if (cudaGraphAddNode(&node, gr, leaves.data(), leaves.size(), &cp) != cudaSuccess) return false;
+    *bodyOut = cp.conditional.phGraph_out[0];
+    return true;
+  };
+  cudaGraph_t g = nullptr, body = nullptr, upd = nullptr;
+  cudaGraphConditionalHandle hOuter = 0, hUpdate = 0;
+  bool ok = cudaGraphCreate(&g, 0) == cudaSuccess &&
+            cudaGraphConditionalHandleCreate(&hOuter, g, 0, cudaGraphCondAssignDefault) == cudaSuccess;
+  ok = ok && capture(g, [&] {
+    k_outer_init<<<1, 1, 0, stream_>>>(state, hOuter);
+    CUDA_OK(cudaGetLastError());
+  });
+  ok = ok && conditional(g, hOuter, cudaGraphCondTypeWhile, &body);
+  ok = ok && cudaGraphConditionalHandleCreate(&hUpdate, body, 0, cudaGraphCondAssignDefault) == cudaSuccess;
+  ok = ok && capture(body, [&] { linearize(); });
+  ok = ok && solver_->appendDeviceSolve(body, stream_);
+  ok = ok && capture(body, [&] {
+    k_outer_check<<<1, 1, 0, stream_>>>(state, hist, solver_->deviceInitialNorm(), solver_->deviceLoopState(),
+                                        hOuter, hUpdate);
+    CUDA_OK(cudaGetLastError());
+  });
+  ok = ok && conditional(body, hUpdate, cudaGraphCondTypeIf, &upd);
+  ok = ok && capture(upd, [&] {
+    dev::update_solution(nCells, dPerm_, hier_.level(0).x, bd, dFaceCells_, dCoeff_, dT_, stream_);
+  });
+  if (ok) {
+    size_t nb = 0, nu = 0;
+    cudaGraphGetNodes(body, nullptr, &nb);
+    cudaGraphGetNodes(upd, nullptr, &nu);
+    advOuterNodes_ = (long long)nb - 2 + (long long)nu;  // the while and if nodes launch nothing themselves
+  }
+  const auto t1 = std::chrono::steady_clock::now();
+  ok = ok && cudaGraphInstantiate(&gAdvance_, g, 0) == cudaSuccess;
+  if (getenv("FVM_TRACE")) {
+    const auto t2 = std::chrono::steady_clock::now();
+    fprintf(stderr, "[fvm advance] outer-loop graph: captured in %.2f ms, instantiated in %.2f ms (%s)\n",
+            std::chrono::duration<double, std::milli>(t1 - t0).count(),
+            std::chrono::duration<double, std::milli>(t2 - t1).count(), ok ? "ok" : "failed");
+  }
+  if (g) cudaGraphDestroy(g);
+  if (!ok) {
+    releaseAdvanceGraph();
+    cudaGetLastError();
+    return false;
+  }
+  advSolverGen_ = solverGen_;
+  advKey_ = solver_->loopKey();
+  return true;
+}
+
+bool ThermalModel::outerGraphUsable() const {
+  return !advanceFailed_ && opt_.linear.outerOnDevice && !matrixDependsOnT_ && !dSegNorm_ &&
+         opt_.linear.verbosity <= 0 && solver_ && solver_->deviceSolvable();
+}
+
+bool ThermalModel::advanceOnDevice(int niter, AdvanceReport& rep) {
+  if (!outerGraphUsable()) return false;
+  const int cap = std::max(std::max(niter, kOuterHistory), advHistoryCap_);
+  if (!gAdvance_ || advSolverGen_ != solverGen_ || !(advKey_ == solver_->loopKey()) || niter > advHistoryCap_) {
+    if (!buildAdvanceGraph(cap)) {
+      advanceFailed_ = true;
+      if (getenv("FVM_TRACE")) fprintf(stderr, "[fvm advance] the outer-loop graph failed to build: host loop\n");
+      return false;
+    }
+  }
+  OuterState* hs = (OuterState*)hOuter_;
+  hs->initialNorm = initialNorm_;
+  hs->absTol = opt_.absoluteTolerance;
+  hs->relTol = opt_.relativeTolerance;
+  hs->niter = niter;
+  hs->iterations = hs->linearIterations = hs->status = 0;
+  CUDA_OK(cudaMemcpyAsync(dOuter_, hOuter_, sizeof(OuterState), cudaMemcpyHostToDevice, stream_));
+  CUDA_OK(cudaGraphLaunch(gAdvance_, stream_));
+  CUDA_OK(cudaMemcpyAsync(hOuter_, dOuter_, kOuterHead + sizeof(double) * (size_t)std::max(niter, 0),
+                          cudaMemcpyDeviceToHost, stream_));
+  CUDA_OK(cudaStreamSynchronize(stream_));
+  const OuterState s = *hs;
+  const double* hist = (const double*)((const char*)hOuter_ + kOuterHead);
+  for (int i = 0; i < s.iterations; i++) history_.push_back(hist[i]);
+  niters_ += s.iterations;
+  initialNorm_ = s.initialNorm;
+  rep.iterations += s.iterations;
+  rep.linearIterations += s.linearIterations;
+  if (s.iterations > 0) rep.lastNorm = hist[s.iterations - 1];
+  rep.launches += 1 + (long long)s.iterations * advOuterNodes_ + (long long)s.linearIterations * solver_->loopBodyNodes();
+  if (s.status == 2) throw Error(kNaN, "initial residual is not finite");
+  if (s.status == 4) throw Error(kNaN, "residual became non-finite");
+  rep.converged = s.status == 1;
+  rep.outerOnDevice = true;
+  return true;
+}
 
 // Per-block outer test on the L1 norm of this iteration's linear system
 // (b, the residual of the delta form at delta = 0).
@@ -469,12 +666,28 @@ void ThermalModel::ensureMatrix() {
     in.cfCol = dCfCol_;
     in.faceCells = dFaceCells_;
     CUDA_OK(cudaStreamSynchronize(stream_));
-    hier_.buildDevice(in, opt_.linear);
+    hier_.buildDevice(in, opt_.linear, true);
     lap("hierarchy on the device");
     dPerm_ = const_cast<int*>(hier_.finestPermDevice());
     solver_.reset(new LinearSolve(hier_));
+    solverGen_++;
     solver_->setLearned(learned_);
-    lap("solver workspace");
+    // the solve's graphs are built while the GPU computes the coarsest
+    // inverse, the build's last step
+    try {
+      if (outerGraphUsable()) {
+        if (!buildAdvanceGraph(std::max(kOuterHistory, advHistoryCap_))) advanceFailed_ = true;
+      } else {
+        solver_->prebuild(stream_);
+      }
+      hier_.finishBuild();
+    } catch (...) {
+      releaseAdvanceGraph();
+      solver_.reset();
+      hier_.release();
+      throw;
+    }
+    lap("solver workspace and graphs");
     matrixDirty_ = hierarchyDirty_ = false;
     return;
   }
@@ -522,6 +735,7 @@ void ThermalModel::ensureMatrix() {
   CUDA_OK(cudaMemcpyAsync(dPerm_, hier_.packed(0).perm.data(), sizeof(int) * (size_t)n, cudaMemcpyHostToDevice,
                           stream_));
   solver_.reset(new LinearSolve(hier_));
+  solverGen_++;
   solver_->setLearned(learned_);
   lap("solver workspace");
   matrixDirty_ = hierarchyDirty_ = false;
@@ -565,7 +779,9 @@ void ThermalModel::advance(int niter, AdvanceReport& rep) {
   const long long launches0 = solver_->launches;
   HostMesh& m = *mesh_;
   const dev::BoundaryData bd = boundaryData();
-  for (int it = 0; it < niter; it++) {
+  TraceRange traceOuter("outer iterations");
+  const bool onDevice = advanceOnDevice(niter, rep);
+  for (int it = 0; !onDevice && it < niter; it++) {
     if (matrixDependsOnT_ && it > 0) {
       // radiative / mixed conditions: the ghost diagonals follow T, so the
       // matrix and its AMG levels are rebuilt every outer iteration, as the

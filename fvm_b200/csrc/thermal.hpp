@@ -106,6 +106,7 @@ struct AdvanceReport {
   long long launches = 0;
   int learnedSteps = 0;    // learned corrections tried / kept (all outer iterations)
   int learnedAccepted = 0;
+  bool outerOnDevice = false;  // the outer iterations ran as one CUDA graph
 };
 
 class ThermalModel {
@@ -173,6 +174,23 @@ class ThermalModel {
   void ensureMatrix();
   void linearize();
   void freeDevice();
+  // The outer loop of advance() on the device: one CUDA graph whose
+  // conditional while node runs linearize, the CG solve (its own while
+  // node), the convergence test and, under a conditional if node, the
+  // solution update. False (nothing ran) when the graph cannot be built.
+  bool advanceOnDevice(int niter, AdvanceReport& rep);
+  bool outerGraphUsable() const;
+  bool buildAdvanceGraph(int historyCap);
+  void releaseAdvanceGraph();
+  cudaGraphExec_t gAdvance_ = nullptr;
+  bool advanceFailed_ = false;
+  // the solver (counted by its builds) and settings the graph was built for
+  unsigned long long solverGen_ = 0, advSolverGen_ = 0;
+  LinearSolve::LoopKey advKey_{};
+  int advHistoryCap_ = 0;
+  long long advOuterNodes_ = 0;  // graph nodes per outer iteration besides the CG iterations
+  void* dOuter_ = nullptr;       // device: outer-loop state, then the outer norms
+  void* hOuter_ = nullptr;       // pinned copy of the same
 
   std::shared_ptr<HostMesh> mesh_;
   std::vector<GroupBC> bcs_;

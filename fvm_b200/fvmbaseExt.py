@@ -201,6 +201,7 @@ class AMG(LinearSolver):
         self.gsReverse = bool(d.gsReverse)  # Gauss-Seidel sweep: forward + reverse (reference) or forward only
         self.patternOnDevice = bool(d.patternOnDevice)  # finest level of a GPU-built hierarchy packed on the GPU
         self.fuseProlongation = bool(d.fuseProlongation)  # prolongation folded into the first smoothing pass
+        self.outerOnDevice = bool(d.outerOnDevice)  # a thermal advance() as one CUDA graph when it can be
         self.setupOnDevice = bool(d.setupOnDevice)
         self.matchRounds = d.matchRounds
         self.matchBeta = d.matchBeta
@@ -249,6 +250,7 @@ class AMG(LinearSolver):
         o.gsReverse = int(bool(self.gsReverse))
         o.patternOnDevice = int(bool(self.patternOnDevice))
         o.fuseProlongation = int(bool(self.fuseProlongation))
+        o.outerOnDevice = int(bool(self.outerOnDevice))
         o.setupOnDevice = int(bool(self.setupOnDevice))
         o.matchRounds = int(self.matchRounds)
         o.matchBeta = float(self.matchBeta)

@@ -103,6 +103,9 @@ typedef struct fvm_linear_options {
   int fuseProlongation;     /* 1: a zero-guess cycle without pre-smoothing folds each prolongation
                                into the level's first post-smoothing pass (bitwise the same result),
                                0: separate prolongation launches */
+  int outerOnDevice;        /* 1: a thermal model's advance() runs all its outer iterations (linearize,
+                               CG solve, update, convergence test) as one CUDA graph when the solve
+                               needs no host step; 0: one host round trip per outer iteration */
 } fvm_linear_options;
 
 /* ThermalModelOptions (fvmbase/ThermalBC.h:33-67) + volume-condition constants */
@@ -131,6 +134,8 @@ typedef struct fvm_report {
   long long launches;      /* kernels and copies issued (graph nodes counted per replay) */
   int learnedSteps;        /* learned corrections tried (0 without a learned correction) */
   int learnedAccepted;     /* ... and kept because they lowered the FP64 residual */
+  int outerOnDevice;       /* 1: the outer iterations ran as one CUDA graph (linear options'
+                              outerOnDevice), 0: one host round trip per outer iteration */
 } fvm_report;
 
 /* Reference AMG defaults (fvmbase/AMG.cpp:15-22) and LinearSolver defaults. */

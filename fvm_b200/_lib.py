@@ -56,6 +56,7 @@ class LinearOptions(ctypes.Structure):
         ("patternOnDevice", ctypes.c_int),
         ("fuseProlongation", ctypes.c_int),
         ("outerOnDevice", ctypes.c_int),
+        ("outerAcceleration", ctypes.c_int),
     ]
 
 

@@ -113,6 +113,9 @@ SolverOptions to_solver(const fvm_linear_options& o) {
   s.patternOnDevice = o.patternOnDevice != 0;
   s.fuseProlongation = o.fuseProlongation != 0;
   s.outerOnDevice = o.outerOnDevice != 0;
+  FVM_REQUIRE(o.outerAcceleration >= 0 && o.outerAcceleration <= 5, kBadArgument,
+              "outerAcceleration must be in [0, 5]");
+  s.outerAcceleration = o.outerAcceleration;
   FVM_REQUIRE(o.matchRounds >= 1 && o.matchRounds <= 64, kBadArgument, "matchRounds must be in [1, 64]");
   FVM_REQUIRE(o.matchBeta >= 0.0 && o.matchBeta <= 1.0, kBadArgument, "matchBeta must be in [0, 1]");
   s.setupOnDevice = o.setupOnDevice != 0;
@@ -163,6 +166,7 @@ void from_solver(const SolverOptions& s, fvm_linear_options& o) {
   o.patternOnDevice = s.patternOnDevice ? 1 : 0;
   o.fuseProlongation = s.fuseProlongation ? 1 : 0;
   o.outerOnDevice = s.outerOnDevice ? 1 : 0;
+  o.outerAcceleration = s.outerAcceleration;
 }
 
 RefLevel level_from_csr(int n, const int* row, const int* col, const double* diag, const double* off) {

@@ -92,6 +92,9 @@ struct SolverOptions {
   // a thermal model's advance() runs all its outer iterations as one CUDA
   // graph when the solve needs no host step (deviceSolvable)
   bool outerOnDevice = true;
+  // Anderson acceleration of a thermal model's outer iteration: the depth
+  // (pairs of iterates mixed, 1-5); 0 = off, the reference's plain loop
+  int outerAcceleration = 0;
   int postSweeps(int l) const { return l > 0 && coarsePostSweeps >= 0 ? coarsePostSweeps : nPostSweeps; }
   // only the finest level is needed (Jacobi solver or preconditioner)
   bool finestOnly() const { return solver == kSolverJacobi || preconditioner == kPrecJacobi; }

@@ -37,6 +37,7 @@ ThermalModel::ThermalModel(std::shared_ptr<HostMesh> mesh) : mesh_(std::move(mes
 
 ThermalModel::~ThermalModel() {
   releaseAdvanceGraph();
+  releaseAcceleration();
   if (dOuter_) cudaFree(dOuter_);
   if (hOuter_) cudaFreeHost(hOuter_);
   solver_.reset();
@@ -189,6 +190,257 @@ __global__ void k_outer_check(OuterState* s, double* hist, const double* cgIniti
 }
 }  // namespace
 
+namespace {
+// Anderson acceleration (type II, depth m <= kAAMax) of the outer
+// fixed-point iteration x -> G(x), G = linearize at x, solve, update: with
+// f_i = G(x_i) - x_i and the last mk + 1 pairs (G_i, f_i) held,
+// gamma = argmin |f_k - dF gamma|_2 and x_{k+1} = G(x_k) - dG gamma, where
+// the columns of dF and dG are differences of consecutive f_i and G_i
+// (Walker & Ni, SIAM J. Numer. Anal. 49, 2011). x is the whole temperature
+// vector, ghost cells included: a ghost's update is affine in its cell's
+// (CRMatrix::solveBoundary), and the weights of the combination sum to 1.
+// Three kernels: the pair store with the normal equations' partial sums,
+// a one-block solve, the update. Sums in a fixed order: bitwise
+// reproducible. Each returns at once when *stop is set (the outer loop has
+// ended: the last plain update stays).
+constexpr int kAAMax = 5;
+constexpr int kAAQ = kAAMax * (kAAMax + 1) / 2 + kAAMax;  // Gram upper triangle + right-hand side
+constexpr int kAABlock = 256;
+
+struct AAState {
+  int head;   // slot of the next pair
+  int count;  // pairs held before this iteration's
+  int cur;    // slot of this iteration's pair
+  int mk;     // columns used this iteration
+  double gamma[kAAMax];
+};
+
+struct AAVectors {
+  double* F[kAAMax + 1];
+  double* G[kAAMax + 1];
+};
+
+__device__ __forceinline__ double aa_block_sum(double v, double* red) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) red[w] = v;
+  __syncthreads();
+  double s = 0.0;
+  if (threadIdx.x == 0)
+    for (int k = 0; k < kAABlock / 32; k++) s += red[k];
+  return s;  // valid in thread 0
+}
+
+__global__ void __launch_bounds__(kAABlock) k_aa_dots(int n, const double* __restrict__ x, const double* __restrict__ xs,
+                                                      AAVectors v, int m, const AAState* st, const int* stop,
+                                                      double* partials) {
+  if (stop && *stop != 0) return;
+  __shared__ double red[kAABlock / 32];
+  const int head = st->head, mk = min(st->count, m), slots = m + 1;
+  // the held pairs' f vectors, oldest first (the slot table is indexed
+  // once per thread, the vectors with unrolled indices)
+  const double* Fq[kAAMax + 1];
+#pragma unroll
+  for (int j = 0; j <= kAAMax; j++) Fq[j] = v.F[((head - mk + j) % slots + slots) % slots];
+  double* const Gn = v.G[head];
+  double* const Fn = v.F[head];
+  double acc[kAAQ];
+#pragma unroll
+  for (int k = 0; k < kAAQ; k++) acc[k] = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double g = x[i], f = g - xs[i];
+    Gn[i] = g;
+    Fn[i] = f;
+    double d[kAAMax];
+    double prev = mk > 0 ? Fq[0][i] : 0.0;
+#pragma unroll
+    for (int j = 1; j <= kAAMax; j++) {
+      if (j <= mk) {
+        const double c = j == mk ? f : Fq[j][i];
+        d[j - 1] = c - prev;
+        prev = c;
+      } else {
+        d[j - 1] = 0.0;
+      }
+    }
+    int k = 0;
+#pragma unroll
+    for (int a = 0; a < kAAMax; a++)
+#pragma unroll
+      for (int b = a; b < kAAMax; b++) acc[k++] += d[a] * d[b];
+#pragma unroll
+    for (int a = 0; a < kAAMax; a++) acc[k++] += d[a] * f;
+  }
+#pragma unroll
+  for (int k = 0; k < kAAQ; k++) {
+    const double s = aa_block_sum(acc[k], red);
+    if (threadIdx.x == 0) partials[(size_t)blockIdx.x * kAAQ + k] = s;
+  }
+}
+
+// Normal equations (dF^T dF) gamma = dF^T f by Cholesky; a pivot below
+// 1e-12 of its diagonal entry (columns nearly dependent) restarts the
+// history: this iteration takes the plain step and keeps only its own pair.
+__global__ void __launch_bounds__(kAABlock) k_aa_solve(int nb, const double* __restrict__ partials, int m, AAState* st,
+                                                       const int* stop) {
+  if (stop && *stop != 0) return;
+  __shared__ double red[kAABlock / 32];
+  __shared__ double tot[kAAQ];
+  const int mk = min(st->count, m);
+  for (int k = 0; k < kAAQ; k++) {
+    double s = 0.0;
+    for (int b = threadIdx.x; b < nb; b += blockDim.x) s += partials[(size_t)b * kAAQ + k];
+    s = aa_block_sum(s, red);
+    if (threadIdx.x == 0) tot[k] = s;
+  }
+  __syncthreads();
+  if (threadIdx.x != 0) return;
+  double H[kAAMax][kAAMax], r[kAAMax], L[kAAMax][kAAMax];
+  int k = 0;
+  for (int a = 0; a < kAAMax; a++)
+    for (int b = a; b < kAAMax; b++) {
+      H[a][b] = tot[k];
+      H[b][a] = tot[k];
+      k++;
+    }
+  for (int a = 0; a < kAAMax; a++) r[a] = tot[k++];
+  bool ok = true;
+  for (int a = 0; a < mk && ok; a++) {
+    for (int b = 0; b <= a; b++) {
+      double s = H[a][b];
+      for (int c = 0; c < b; c++) s -= L[a][c] * L[b][c];
+      if (a == b) {
+        if (!(s > 1e-12 * H[a][a])) {
+          ok = false;
+          break;
+        }
+        L[a][a] = sqrt(s);
+      } else {
+        L[a][b] = s / L[b][b];
+      }
+    }
+  }
+  double y[kAAMax], gam[kAAMax];
+  int used = 0;
+  if (ok && mk > 0) {
+    for (int a = 0; a < mk; a++) {
+      double s = r[a];
+      for (int c = 0; c < a; c++) s -= L[a][c] * y[c];
+      y[a] = s / L[a][a];
+    }
+    for (int a = mk - 1; a >= 0; a--) {
+      double s = y[a];
+      for (int c = a + 1; c < mk; c++) s -= L[c][a] * gam[c];
+      gam[a] = s / L[a][a];
+    }
+    used = mk;
+    for (int a = 0; a < mk; a++) ok = ok && isfinite(gam[a]);
+    if (!ok) used = 0;
+  }
+  for (int a = 0; a < kAAMax; a++) st->gamma[a] = a < used ? gam[a] : 0.0;
+  st->cur = st->head;
+  st->mk = used;
+  st->head = (st->head + 1) % (m + 1);
+  st->count = used == mk ? min(st->count + 1, m + 1) : 1;
+}
+
+__global__ void __launch_bounds__(kAABlock) k_aa_update(int n, double* __restrict__ x, double* __restrict__ xs,
+                                                        AAVectors v, int m, const AAState* st, const int* stop) {
+  if (stop && *stop != 0) return;
+  const int cur = st->cur, mk = st->mk, slots = m + 1;
+  const double* Gq[kAAMax + 1];
+  double gam[kAAMax];
+#pragma unroll
+  for (int j = 0; j <= kAAMax; j++) Gq[j] = v.G[((cur - mk + j) % slots + slots) % slots];
+#pragma unroll
+  for (int j = 0; j < kAAMax; j++) gam[j] = st->gamma[j];
+  const double* const Gc = v.G[cur];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double g = Gc[i];
+    double s = 0.0;
+    double prev = mk > 0 ? Gq[0][i] : 0.0;
+#pragma unroll
+    for (int j = 1; j <= kAAMax; j++) {
+      if (j <= mk) {
+        const double c = j == mk ? g : Gq[j][i];
+        s += gam[j - 1] * (c - prev);
+        prev = c;
+      }
+    }
+    const double xn = g - s;
+    x[i] = xn;
+    xs[i] = xn;
+  }
+}
+
+__global__ void k_aa_reset(AAState* st) {
+  st->head = 0;
+  st->count = 0;
+  st->cur = 0;
+  st->mk = 0;
+}
+
+int aa_blocks(int n) {
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  return std::max(1, std::min((n + kAABlock - 1) / kAABlock, 8 * sms));
+}
+}  // namespace
+
+// Buffers of the outer acceleration of depth m: (m + 1) pairs of
+// temperature-sized vectors, the previous iterate, the partial sums and
+// the state; allocated on first use, kept while m and the mesh stay.
+void ThermalModel::ensureAcceleration(int m) {
+  const int nAll = mesh_->nTotalCells();
+  if (aaDepth_ == m && aaCells_ == nAll) return;
+  releaseAcceleration();
+  const int nb = aa_blocks(nAll);
+  const size_t vec = sizeof(double) * (size_t)nAll;
+  const size_t bytes = vec * (size_t)(2 * (m + 1) + 1) + sizeof(double) * (size_t)nb * kAAQ + 256;
+  CUDA_OK(cudaMalloc(&dAA_, bytes));
+  aaDepth_ = m;
+  aaCells_ = nAll;
+  aaBlocks_ = nb;
+  aaGen_++;
+}
+
+void ThermalModel::releaseAcceleration() {
+  if (dAA_) cudaFree(dAA_);
+  dAA_ = nullptr;
+  aaDepth_ = 0;
+  aaCells_ = 0;
+}
+
+void ThermalModel::accelerationStart(cudaStream_t st) {
+  const size_t vec = sizeof(double) * (size_t)aaCells_;
+  double* xs = (double*)dAA_;
+  AAState* s = (AAState*)((char*)dAA_ + vec * (size_t)(2 * (aaDepth_ + 1) + 1) +
+                          sizeof(double) * (size_t)aaBlocks_ * kAAQ);
+  k_aa_reset<<<1, 1, 0, st>>>(s);
+  CUDA_OK(cudaGetLastError());
+  CUDA_OK(cudaMemcpyAsync(xs, dT_, vec, cudaMemcpyDeviceToDevice, st));
+}
+
+void ThermalModel::accelerationStep(cudaStream_t st, const int* stop) {
+  const int m = aaDepth_, n = aaCells_;
+  const size_t vec = sizeof(double) * (size_t)n;
+  double* base = (double*)dAA_;
+  double* xs = base;
+  AAVectors v{};
+  for (int j = 0; j <= m; j++) {
+    v.F[j] = base + (size_t)(1 + j) * n;
+    v.G[j] = base + (size_t)(2 + m + j) * n;
+  }
+  double* partials = (double*)((char*)dAA_ + vec * (size_t)(2 * (m + 1) + 1));
+  AAState* s = (AAState*)((char*)partials + sizeof(double) * (size_t)aaBlocks_ * kAAQ);
+  k_aa_dots<<<aaBlocks_, kAABlock, 0, st>>>(n, dT_, xs, v, m, s, stop, partials);
+  k_aa_solve<<<1, kAABlock, 0, st>>>(aaBlocks_, partials, m, s, stop);
+  k_aa_update<<<aaBlocks_, kAABlock, 0, st>>>(n, dT_, xs, v, m, s, stop);
+  CUDA_OK(cudaGetLastError());
+}
+
 void ThermalModel::releaseAdvanceGraph() {
   if (gAdvance_) cudaGraphExecDestroy(gAdvance_);
   gAdvance_ = nullptr;
@@ -247,10 +499,18 @@ bool ThermalModel::buildAdvanceGraph(int historyCap) {
   cudaGraphConditionalHandle hOuter = 0, hUpdate = 0;
   bool ok = cudaGraphCreate(&g, 0) == cudaSuccess &&
             cudaGraphConditionalHandleCreate(&hOuter, g, 0, cudaGraphCondAssignDefault) == cudaSuccess;
+  const int aaM = opt_.linear.outerAcceleration;
+  if (aaM > 0) ensureAcceleration(aaM);
   ok = ok && capture(g, [&] {
     k_outer_init<<<1, 1, 0, stream_>>>(state, hOuter);
     CUDA_OK(cudaGetLastError());
+    if (aaM > 0) accelerationStart(stream_);
   });
+  if (ok) {
+    size_t np = 0;
+    cudaGraphGetNodes(g, nullptr, &np);
+    advPrologueNodes_ = (long long)np;
+  }
   ok = ok && conditional(g, hOuter, cudaGraphCondTypeWhile, &body);
   ok = ok && cudaGraphConditionalHandleCreate(&hUpdate, body, 0, cudaGraphCondAssignDefault) == cudaSuccess;
   ok = ok && capture(body, [&] { linearize(); });
@@ -263,6 +523,9 @@ bool ThermalModel::buildAdvanceGraph(int historyCap) {
   ok = ok && conditional(body, hUpdate, cudaGraphCondTypeIf, &upd);
   ok = ok && capture(upd, [&] {
     dev::update_solution(nCells, dPerm_, hier_.level(0).x, bd, dFaceCells_, dCoeff_, dT_, stream_);
+    // skipped on the device once the loop has ended (converged or out of
+    // iterations), as the host loop skips it
+    if (aaM > 0) accelerationStep(stream_, &state->status);
   });
   if (ok) {
     size_t nb = 0, nu = 0;
@@ -286,6 +549,8 @@ bool ThermalModel::buildAdvanceGraph(int historyCap) {
   }
   advSolverGen_ = solverGen_;
   advKey_ = solver_->loopKey();
+  advAADepth_ = aaM;
+  advAAGen_ = aaGen_;
   return true;
 }
 
@@ -297,7 +562,10 @@ bool ThermalModel::outerGraphUsable() const {
 bool ThermalModel::advanceOnDevice(int niter, AdvanceReport& rep) {
   if (!outerGraphUsable()) return false;
   const int cap = std::max(std::max(niter, kOuterHistory), advHistoryCap_);
-  if (!gAdvance_ || advSolverGen_ != solverGen_ || !(advKey_ == solver_->loopKey()) || niter > advHistoryCap_) {
+  const int aaM = opt_.linear.outerAcceleration;
+  if (aaM > 0) ensureAcceleration(aaM);
+  if (!gAdvance_ || advSolverGen_ != solverGen_ || !(advKey_ == solver_->loopKey()) || niter > advHistoryCap_ ||
+      advAADepth_ != aaM || (aaM > 0 && advAAGen_ != aaGen_)) {
     if (!buildAdvanceGraph(cap)) {
       advanceFailed_ = true;
       if (getenv("FVM_TRACE")) fprintf(stderr, "[fvm advance] the outer-loop graph failed to build: host loop\n");
@@ -323,7 +591,8 @@ bool ThermalModel::advanceOnDevice(int niter, AdvanceReport& rep) {
   rep.iterations += s.iterations;
   rep.linearIterations += s.linearIterations;
   if (s.iterations > 0) rep.lastNorm = hist[s.iterations - 1];
-  rep.launches += 1 + (long long)s.iterations * advOuterNodes_ + (long long)s.linearIterations * solver_->loopBodyNodes();
+  rep.launches += advPrologueNodes_ + (long long)s.iterations * advOuterNodes_ +
+                 (long long)s.linearIterations * solver_->loopBodyNodes();
   if (s.status == 2) throw Error(kNaN, "initial residual is not finite");
   if (s.status == 4) throw Error(kNaN, "residual became non-finite");
   rep.converged = s.status == 1;
@@ -781,6 +1050,12 @@ void ThermalModel::advance(int niter, AdvanceReport& rep) {
   const dev::BoundaryData bd = boundaryData();
   TraceRange traceOuter("outer iterations");
   const bool onDevice = advanceOnDevice(niter, rep);
+  const int aaM = opt_.linear.outerAcceleration;
+  if (!onDevice && aaM > 0 && niter > 0) {
+    ensureAcceleration(aaM);
+    accelerationStart(stream_);
+    rep.launches += 2;
+  }
   for (int it = 0; !onDevice && it < niter; it++) {
     if (matrixDependsOnT_ && it > 0) {
       // radiative / mixed conditions: the ghost diagonals follow T, so the
@@ -823,6 +1098,10 @@ void ThermalModel::advance(int niter, AdvanceReport& rep) {
     if (done) {
       rep.converged = true;
       break;
+    }
+    if (aaM > 0 && it + 1 < niter) {
+      accelerationStep(stream_, nullptr);
+      rep.launches += 3;
     }
   }
   CUDA_OK(cudaEventRecord(e2, stream_));

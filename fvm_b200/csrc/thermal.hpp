@@ -191,6 +191,19 @@ class ThermalModel {
   long long advOuterNodes_ = 0;  // graph nodes per outer iteration besides the CG iterations
   void* dOuter_ = nullptr;       // device: outer-loop state, then the outer norms
   void* hOuter_ = nullptr;       // pinned copy of the same
+  long long advPrologueNodes_ = 0;
+  // Anderson acceleration of the outer iteration (linear options'
+  // outerAcceleration = depth m, 0 off): buffers, the start of a call (state
+  // reset, previous iterate = T) and one step after an update (returns at
+  // once on the device when *stop is non-zero)
+  void ensureAcceleration(int m);
+  void releaseAcceleration();
+  void accelerationStart(cudaStream_t st);
+  void accelerationStep(cudaStream_t st, const int* stop);
+  void* dAA_ = nullptr;
+  int aaDepth_ = 0, aaCells_ = 0, aaBlocks_ = 0;
+  unsigned long long aaGen_ = 0, advAAGen_ = 0;
+  int advAADepth_ = 0;
 
   std::shared_ptr<HostMesh> mesh_;
   std::vector<GroupBC> bcs_;

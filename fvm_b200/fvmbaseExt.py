@@ -202,6 +202,7 @@ class AMG(LinearSolver):
         self.patternOnDevice = bool(d.patternOnDevice)  # finest level of a GPU-built hierarchy packed on the GPU
         self.fuseProlongation = bool(d.fuseProlongation)  # prolongation folded into the first smoothing pass
         self.outerOnDevice = bool(d.outerOnDevice)  # a thermal advance() as one CUDA graph when it can be
+        self.outerAcceleration = d.outerAcceleration  # Anderson depth of the outer iteration (0: off)
         self.setupOnDevice = bool(d.setupOnDevice)
         self.matchRounds = d.matchRounds
         self.matchBeta = d.matchBeta
@@ -251,6 +252,7 @@ class AMG(LinearSolver):
         o.patternOnDevice = int(bool(self.patternOnDevice))
         o.fuseProlongation = int(bool(self.fuseProlongation))
         o.outerOnDevice = int(bool(self.outerOnDevice))
+        o.outerAcceleration = int(self.outerAcceleration)
         o.setupOnDevice = int(bool(self.setupOnDevice))
         o.matchRounds = int(self.matchRounds)
         o.matchBeta = float(self.matchBeta)

@@ -106,6 +106,9 @@ typedef struct fvm_linear_options {
   int outerOnDevice;        /* 1: a thermal model's advance() runs all its outer iterations (linearize,
                                CG solve, update, convergence test) as one CUDA graph when the solve
                                needs no host step; 0: one host round trip per outer iteration */
+  int outerAcceleration;    /* Anderson acceleration of a thermal model's outer iteration, depth 1-5
+                               (that many earlier iterates mixed into each new one); 0: off, the
+                               reference's plain outer loop */
 } fvm_linear_options;
 
 /* ThermalModelOptions (fvmbase/ThermalBC.h:33-67) + volume-condition constants */

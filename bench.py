@@ -905,7 +905,7 @@ def main():
         accel = args.outer_accel
     if args.mixed_inner_rel is not None:
         mixed_inner = args.mixed_inner_rel
-    if accel > 0 and "mixed" in variants and "mixed-plain-outer" not in variants:
+    if accel > 0 and "mixed" in variants and "plain" in variants and "mixed-plain-outer" not in variants:
         variants.insert(variants.index("mixed") + 1, "mixed-plain-outer")  # the same solver, plain outer loop
     lc, learned_info = None, None
     if "learned" in variants:

@@ -940,6 +940,22 @@ __global__ void k_l1_partials(int n, const double* __restrict__ a, double* parti
   s = block_sum(s);
   if (threadIdx.x == 0) partials[blockIdx.x] = s;
 }
+// The start of a CG solve from x = 0: r = b + A x is b itself. r, its FP32
+// copy (the FP32 cycle's right-hand side; null: none) and the |r|_1
+// partials in k_l1_partials' layout, in one pass over b.
+__global__ void k_cg_start(int n, const double* __restrict__ b, double* __restrict__ r, float* __restrict__ rF,
+                           double* partials) {
+  FVM_PDL();
+  double s = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double v = b[i];
+    r[i] = v;
+    if (rF) rF[i] = (float)v;
+    s += fabs(v);
+  }
+  s = block_sum(s);
+  if (threadIdx.x == 0) partials[blockIdx.x] = s;
+}
 __global__ void k_dot_partials(int n, const double* __restrict__ a, const double* __restrict__ b,
                                double* partials) {
   FVM_PDL();
@@ -1974,6 +1990,9 @@ int vec_blocks(int n) {
 }
 void l1_partials(int n, const double* a, double* partials, cudaStream_t st) {
   pdl_launch(k_l1_partials, vec_blocks(n), kBlock, st, n, a, partials);
+}
+void cg_start(int n, const double* b, double* r, float* rF, double* partials, cudaStream_t st) {
+  pdl_launch(k_cg_start, vec_blocks(n), kBlock, st, n, b, r, rF, partials);
 }
 void dot_partials(int n, const double* a, const double* b, double* partials, cudaStream_t st) {
   pdl_launch(k_dot_partials, vec_blocks(n), kBlock, st, n, a, b, partials);

@@ -180,6 +180,9 @@ void l1_partials(int n, const double* a, double* partials, cudaStream_t st);
 void dot_partials(int n, const double* a, const double* b, double* partials, cudaStream_t st);
 // out[0] = sum of the partials in a fixed order
 void sum_partials(int np, const double* partials, double* out, cudaStream_t st);
+// r = b (the residual at x = 0), rF = (float) b when rF is not null, and the
+// |b|_1 partials of l1_partials (vec_blocks(n) of them)
+void cg_start(int n, const double* b, double* r, float* rF, double* partials, cudaStream_t st);
 // scalar recurrences for the Krylov solvers, all on the device:
 // out = num / den (out, num, den are device scalars)
 void scalar_div(const double* num, const double* den, double* out, cudaStream_t st);

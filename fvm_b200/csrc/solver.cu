@@ -1600,9 +1600,9 @@ bool LinearSolve::addCGLoop(cudaGraph_t g, cudaStream_t st, bool flexible, bool 
       CUDA_OK(cudaMemsetAsync(P, 0, sizeof(double) * (size_t)n_, st));
       CUDA_OK(cudaMemsetAsync(Z, 0, sizeof(double) * (size_t)n_, st));
       if (B != d.b) dev::copy_d(n_, d.b, B, st);
-      dev::residual<double>(d.view64(), d.nSlices, X, B, R, nullptr, st);
-      norm_into(R, scal_ + kNorm, st);
-      if (mixedCycle) dev::convert_d2f(n_, R, d.bF, st);  // the FP32 cycle's right-hand side
+      // r = b at x = 0, with its norm and the FP32 cycle's right-hand side
+      dev::cg_start(n_, B, R, mixedCycle ? d.bF : nullptr, partials_, st);
+      dev::sum_partials(dev::vec_blocks(n_), partials_, scal_ + kNorm, st);
       k_cg_loop_init<<<1, 1, 0, st>>>(scal_, loopInt_, history_, o.absoluteTolerance, o.nMaxIterations, h);
     } catch (const Error&) {
       ok = false;
@@ -1655,13 +1655,16 @@ bool LinearSolve::addCGLoop(cudaGraph_t g, cudaStream_t st, bool flexible, bool 
     if (ok) cudaGraphGetNodes(body, nullptr, &nb);
     loopBodyNodes_ = (long long)nb;
   }
-  // epilogue: the true residual's norm, the system restored, the results to
-  // the pinned host scalars
+  // epilogue: the system restored; with hostCopies the true residual's norm
+  // and the results to the pinned host scalars (inside an outer loop nothing
+  // reads that norm)
   ok = ok && cudaStreamBeginCaptureToGraph(st, g, &cnode, nullptr, 1, mode) == cudaSuccess;
   if (ok) {
     try {
-      dev::residual<double>(d.view64(), d.nSlices, X, B, R, nullptr, st);
-      norm_into(R, scal_ + kNorm, st);
+      if (hostCopies) {
+        dev::residual<double>(d.view64(), d.nSlices, X, B, R, nullptr, st);
+        norm_into(R, scal_ + kNorm, st);
+      }
       if (X != d.x) dev::copy_d(n_, X, d.x, st);
       if (B != d.b) dev::copy_d(n_, B, d.b, st);
       if (hostCopies) {

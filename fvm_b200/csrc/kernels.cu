@@ -54,6 +54,14 @@ struct XDirect {
   const T* __restrict__ x;
   __device__ __forceinline__ T operator()(int j) const { return x[j]; }
 };
+// CG's new search direction read where it is needed: p_j = p_old_j * beta +
+// z_j, rounded as k_xpby_dev rounds it (contraction off in this file)
+struct XPby {
+  const double* __restrict__ z;
+  const double* __restrict__ p;
+  double beta;
+  __device__ __forceinline__ double operator()(int j) const { return p[j] * beta + z[j]; }
+};
 template <class T>
 struct XProlonged {
   const T* __restrict__ xc;
@@ -507,6 +515,47 @@ __global__ void __launch_bounds__(kBlock, 8) k_spmv_dot_ell(SellView<double> a, 
   if (threadIdx.x == 0) partials[blockIdx.x] = d;
 }
 
+// q = A p with p = p_old * beta + z formed on the fly (p itself is written
+// by k_cg_update_pby, after every row has read its neighbours' p_old), one
+// partial of p.q per block
+template <int W>
+__global__ void __launch_bounds__(kBlock, 8) k_spmv_dot_pby_ell(SellView<double> a, const double* __restrict__ z,
+                                                                const double* __restrict__ p, const double* beta,
+                                                                double* y, double* partials) {
+  FVM_PDL();
+  const int i = blockIdx.x * kBlock + threadIdx.x;
+  const XPby pg{z, p, beta[0]};
+  double d = 0.0;
+  if (i < a.n) {
+    const double xi = pg(i);
+    const double yi = ell_row_g<double, W>(a, i, pg, a.diag[i] * xi);
+    y[i] = yi;
+    d = xi * yi;
+  }
+  d = block_sum(d);
+  if (threadIdx.x == 0) partials[blockIdx.x] = d;
+}
+
+__global__ void __launch_bounds__(kBlock, 8) k_spmv_dot_pby(SellView<double> a, int nSlices,
+                                                            const double* __restrict__ z, const double* __restrict__ p,
+                                                            const double* beta, double* y, double* partials) {
+  FVM_PDL();
+  const int lane = threadIdx.x & 31;
+  const XPby pg{z, p, beta[0]};
+  double d = 0.0;
+  for (int s = blockIdx.x * kSlicesPerBlock + (threadIdx.x >> 5); s < nSlices; s += gridDim.x * kSlicesPerBlock) {
+    const int4 m = slice_meta(a, s);
+    if (lane >= m.y) continue;
+    const int i = m.x + lane;
+    const double xi = pg(i);
+    const double yi = row_sum_g(a, m, lane, pg, a.diag[i] * xi);
+    y[i] = yi;
+    d += xi * yi;
+  }
+  d = block_sum(d);
+  if (threadIdx.x == 0) partials[blockIdx.x] = d;
+}
+
 // the same over a SELL-32 level (grid-stride over slices)
 __global__ void __launch_bounds__(kBlock, 8) k_spmv_dot(SellView<double> a, int nSlices, const double* __restrict__ x,
                                                         double* y, double* partials) {
@@ -582,6 +631,28 @@ __global__ void k_cg_update(int n, const double* alpha, const double* __restrict
   double l1 = 0.0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     x[i] = x[i] + am * p[i];
+    const double ri = r[i] + am * q[i];
+    r[i] = ri;
+    if (rF) rF[i] = (float)ri;
+    l1 += fabs(ri);
+  }
+  l1 = block_sum(l1);
+  if (threadIdx.x == 0) partials[blockIdx.x] = l1;
+}
+
+// p = p_old * beta + z (written here), x += -alpha p; r += -alpha q; block
+// partials of |r|
+__global__ void k_cg_update_pby(int n, const double* alpha, const double* __restrict__ z, const double* beta,
+                                double* p, const double* __restrict__ q, double* x, double* r, double* partials,
+                                float* rF) {
+  FVM_PDL();
+  const double am = -1.0 * alpha[0];
+  const double b = beta[0];
+  double l1 = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double pi = p[i] * b + z[i];
+    p[i] = pi;
+    x[i] = x[i] + am * pi;
     const double ri = r[i] + am * q[i];
     r[i] = ri;
     if (rF) rF[i] = (float)ri;
@@ -1409,6 +1480,17 @@ void spmv_dot(const SellView<double>& a, int nSlices, const double* x, double* y
   if (a.ellWidth && FVM_ELL_SWITCH(a.ellWidth, FVM_L)) return;
 #undef FVM_L
   pdl_launch(k_spmv_dot, reduce_blocks(nSlices), kBlock, st, a, nSlices, x, y, partials);
+}
+void spmv_dot_pby(const SellView<double>& a, int nSlices, const double* z, const double* p, const double* beta,
+                  double* y, double* partials, cudaStream_t st) {
+#define FVM_L(W) pdl_launch(k_spmv_dot_pby_ell<W>, ceil_div(a.n, kBlock), kBlock, st, a, z, p, beta, y, partials)
+  if (a.ellWidth && FVM_ELL_SWITCH(a.ellWidth, FVM_L)) return;
+#undef FVM_L
+  pdl_launch(k_spmv_dot_pby, reduce_blocks(nSlices), kBlock, st, a, nSlices, z, p, beta, y, partials);
+}
+void cg_update_pby(int n, const double* alpha, const double* z, const double* beta, double* p, const double* q,
+                   double* x, double* r, double* partials, cudaStream_t st, float* rF) {
+  pdl_launch(k_cg_update_pby, vec_blocks(n), kBlock, st, n, alpha, z, beta, p, q, x, r, partials, rF);
 }
 template <class S>
 void cg_take_z(int n, const S* src, const double* r, double* z, double* partials, cudaStream_t st) {

@@ -87,6 +87,12 @@ int reduce_blocks(int nSlices);  // grid of the SELL-32 whole-level row kernels
 // y = A x with one partial of x.y per block (spmv_dot_blocks of them)
 int spmv_dot_blocks(const SellView<double>& a, int nSlices);
 void spmv_dot(const SellView<double>& a, int nSlices, const double* x, double* y, double* partials, cudaStream_t st);
+// the same with p = p_old * beta + z formed on the fly (spmv_dot_blocks
+// partials); cg_update_pby then writes that p and updates x and r
+void spmv_dot_pby(const SellView<double>& a, int nSlices, const double* z, const double* p, const double* beta,
+                  double* y, double* partials, cudaStream_t st);
+void cg_update_pby(int n, const double* alpha, const double* z, const double* beta, double* p, const double* q,
+                   double* x, double* r, double* partials, cudaStream_t st, float* rF = nullptr);
 // z <- src (converted to FP64) with per-block partials of r.z_old and
 // r.z_new (interleaved, vec_blocks(n) pairs)
 template <class S>

@@ -1639,10 +1639,12 @@ bool LinearSolve::addCGLoop(cudaGraph_t g, cudaStream_t st, bool flexible, bool 
       else
         dev::cg_take_z<double>(n_, d.x, R, Z, partials2_, st);
       dev::cg_beta(dev::vec_blocks(n_), partials2_, scal_ + kRho, scal_ + kRhoPrev, scal_ + kBeta, flexible, st);
-      dev::xpby_dev(n_, Z, scal_ + kBeta, P, st);
-      dev::spmv_dot(d.view64(), d.nSlices, P, Q, partials2_, st);
+      // p = p * beta + z is formed by the SpMV where it reads p and written
+      // by the update: no pass of its own
+      dev::spmv_dot_pby(d.view64(), d.nSlices, Z, P, scal_ + kBeta, Q, partials2_, st);
       dev::cg_alpha(dev::spmv_dot_blocks(d.view64(), d.nSlices), partials2_, scal_ + kRho, scal_ + kAlpha, st);
-      dev::cg_update(n_, scal_ + kAlpha, P, Q, X, R, partials_, st, mixedCycle ? d.bF : nullptr);
+      dev::cg_update_pby(n_, scal_ + kAlpha, Z, scal_ + kBeta, P, Q, X, R, partials_, st,
+                         mixedCycle ? d.bF : nullptr);
       dev::sum_partials(dev::vec_blocks(n_), partials_, scal_ + kNorm, st);
       k_cg_loop_check<<<1, 1, 0, st>>>(scal_, loopInt_, history_, o.relativeTolerance, o.absoluteTolerance,
                                        o.nMaxIterations, h);

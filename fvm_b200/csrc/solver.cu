@@ -1411,8 +1411,9 @@ SolveReport LinearSolve::solveCG(cudaStream_t st) {
   CUDA_OK(cudaMemsetAsync(P, 0, sizeof(double) * (size_t)n_, st));
   CUDA_OK(cudaMemsetAsync(Z, 0, sizeof(double) * (size_t)n_, st));  // z_0 enters the first flexible beta
   dev::copy_d(n_, d.b, B, st);
-  dev::residual<double>(d.view64(), d.nSlices, X, B, R, nullptr, st);
-  norm_into(R, scal_ + kNorm, st);
+  // r = b at x = 0, with its norm (the FP32 copy below, when the cycle takes it)
+  dev::cg_start(n_, B, R, nullptr, partials_, st);
+  dev::sum_partials(dev::vec_blocks(n_), partials_, scal_ + kNorm, st);
   {
     const double inf = std::numeric_limits<double>::infinity();
     CUDA_OK(cudaMemcpyAsync(scal_ + kRho, &inf, sizeof(double), cudaMemcpyHostToDevice, st));
@@ -1487,10 +1488,9 @@ SolveReport LinearSolve::solveCG(cudaStream_t st) {
         else
           dev::cg_take_z<double>(n_, d.x, R, Z, partials2_, st);
         dev::cg_beta(dev::vec_blocks(n_), partials2_, scal_ + kRho, scal_ + kRhoPrev, scal_ + kBeta, flexible, st);
-        dev::xpby_dev(n_, Z, scal_ + kBeta, P, st);
-        dev::spmv_dot(d.view64(), d.nSlices, P, Q, partials2_, st);
+        dev::spmv_dot_pby(d.view64(), d.nSlices, Z, P, scal_ + kBeta, Q, partials2_, st);
         dev::cg_alpha(dev::spmv_dot_blocks(d.view64(), d.nSlices), partials2_, scal_ + kRho, scal_ + kAlpha, st);
-        dev::cg_update(n_, scal_ + kAlpha, P, Q, X, R, partials_, st, rF);
+        dev::cg_update_pby(n_, scal_ + kAlpha, Z, scal_ + kBeta, P, Q, X, R, partials_, st, rF);
         dev::sum_partials(dev::vec_blocks(n_), partials_, scal_ + kNorm, st);
         CUDA_OK(cudaMemcpyAsync(hostScal_, scal_ + kNorm, sizeof(double), cudaMemcpyDeviceToHost, st));
       });

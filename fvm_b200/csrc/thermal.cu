@@ -220,42 +220,57 @@ struct AAVectors {
   double* G[kAAMax + 1];
 };
 
-__device__ __forceinline__ double aa_block_sum(double v, double* red) {
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  __syncthreads();
-  if (lane == 0) red[w] = v;
-  __syncthreads();
-  double s = 0.0;
-  if (threadIdx.x == 0)
-    for (int k = 0; k < kAABlock / 32; k++) s += red[k];
-  return s;  // valid in thread 0
+template <int M>
+constexpr int aa_nq() {
+  return M * (M + 1) / 2 + M;  // Gram upper triangle, then the right-hand side
 }
 
+// sums of acc[0..NQ) over the block in a fixed order (each warp's by
+// shuffles, then the warps' sums in warp order), written to out[0..NQ) by
+// threads 0..NQ-1
+template <int NQ>
+__device__ __forceinline__ void aa_block_sums(double (&acc)[NQ], double (*red)[NQ], double* out) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+  for (int q = 0; q < NQ; q++) {
+    double v = acc[q];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (lane == 0) red[w][q] = v;
+  }
+  __syncthreads();
+  if ((int)threadIdx.x < NQ) {
+    double s = 0.0;
+    for (int k = 0; k < kAABlock / 32; k++) s += red[k][threadIdx.x];
+    out[threadIdx.x] = s;
+  }
+}
+
+template <int M>
 __global__ void __launch_bounds__(kAABlock) k_aa_dots(int n, const double* __restrict__ x, const double* __restrict__ xs,
-                                                      AAVectors v, int m, const AAState* st, const int* stop,
+                                                      AAVectors v, const AAState* st, const int* stop,
                                                       double* partials) {
   if (stop && *stop != 0) return;
-  __shared__ double red[kAABlock / 32];
-  const int head = st->head, mk = min(st->count, m), slots = m + 1;
+  constexpr int NQ = aa_nq<M>();
+  __shared__ double red[kAABlock / 32][NQ];
+  const int head = st->head, mk = min(st->count, M), slots = M + 1;
   // the held pairs' f vectors, oldest first (the slot table is indexed
   // once per thread, the vectors with unrolled indices)
-  const double* Fq[kAAMax + 1];
+  const double* Fq[M + 1];
 #pragma unroll
-  for (int j = 0; j <= kAAMax; j++) Fq[j] = v.F[((head - mk + j) % slots + slots) % slots];
+  for (int j = 0; j <= M; j++) Fq[j] = v.F[((head - mk + j) % slots + slots) % slots];
   double* const Gn = v.G[head];
   double* const Fn = v.F[head];
-  double acc[kAAQ];
+  double acc[NQ];
 #pragma unroll
-  for (int k = 0; k < kAAQ; k++) acc[k] = 0.0;
+  for (int k = 0; k < NQ; k++) acc[k] = 0.0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const double g = x[i], f = g - xs[i];
     Gn[i] = g;
     Fn[i] = f;
-    double d[kAAMax];
+    double d[M];
     double prev = mk > 0 ? Fq[0][i] : 0.0;
 #pragma unroll
-    for (int j = 1; j <= kAAMax; j++) {
+    for (int j = 1; j <= M; j++) {
       if (j <= mk) {
         const double c = j == mk ? f : Fq[j][i];
         d[j - 1] = c - prev;
@@ -266,45 +281,45 @@ __global__ void __launch_bounds__(kAABlock) k_aa_dots(int n, const double* __res
     }
     int k = 0;
 #pragma unroll
-    for (int a = 0; a < kAAMax; a++)
+    for (int a = 0; a < M; a++)
 #pragma unroll
-      for (int b = a; b < kAAMax; b++) acc[k++] += d[a] * d[b];
+      for (int b = a; b < M; b++) acc[k++] += d[a] * d[b];
 #pragma unroll
-    for (int a = 0; a < kAAMax; a++) acc[k++] += d[a] * f;
+    for (int a = 0; a < M; a++) acc[k++] += d[a] * f;
   }
-#pragma unroll
-  for (int k = 0; k < kAAQ; k++) {
-    const double s = aa_block_sum(acc[k], red);
-    if (threadIdx.x == 0) partials[(size_t)blockIdx.x * kAAQ + k] = s;
-  }
+  aa_block_sums<NQ>(acc, red, partials + (size_t)blockIdx.x * NQ);
 }
 
 // Normal equations (dF^T dF) gamma = dF^T f by Cholesky; a pivot below
 // 1e-12 of its diagonal entry (columns nearly dependent) restarts the
 // history: this iteration takes the plain step and keeps only its own pair.
-__global__ void __launch_bounds__(kAABlock) k_aa_solve(int nb, const double* __restrict__ partials, int m, AAState* st,
+// The blocks' partials are summed by one warp per quantity, lanes striding
+// over the blocks, then by shuffles: a fixed order.
+template <int M>
+__global__ void __launch_bounds__(kAABlock) k_aa_solve(int nb, const double* __restrict__ partials, AAState* st,
                                                        const int* stop) {
   if (stop && *stop != 0) return;
-  __shared__ double red[kAABlock / 32];
-  __shared__ double tot[kAAQ];
-  const int mk = min(st->count, m);
-  for (int k = 0; k < kAAQ; k++) {
+  constexpr int NQ = aa_nq<M>();
+  __shared__ double tot[NQ];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (int q = w; q < NQ; q += kAABlock / 32) {
     double s = 0.0;
-    for (int b = threadIdx.x; b < nb; b += blockDim.x) s += partials[(size_t)b * kAAQ + k];
-    s = aa_block_sum(s, red);
-    if (threadIdx.x == 0) tot[k] = s;
+    for (int b = lane; b < nb; b += 32) s += partials[(size_t)b * NQ + q];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if (lane == 0) tot[q] = s;
   }
   __syncthreads();
   if (threadIdx.x != 0) return;
-  double H[kAAMax][kAAMax], r[kAAMax], L[kAAMax][kAAMax];
+  const int mk = min(st->count, M);
+  double H[M][M], r[M], L[M][M];
   int k = 0;
-  for (int a = 0; a < kAAMax; a++)
-    for (int b = a; b < kAAMax; b++) {
+  for (int a = 0; a < M; a++)
+    for (int b = a; b < M; b++) {
       H[a][b] = tot[k];
       H[b][a] = tot[k];
       k++;
     }
-  for (int a = 0; a < kAAMax; a++) r[a] = tot[k++];
+  for (int a = 0; a < M; a++) r[a] = tot[k++];
   bool ok = true;
   for (int a = 0; a < mk && ok; a++) {
     for (int b = 0; b <= a; b++) {
@@ -321,7 +336,7 @@ __global__ void __launch_bounds__(kAABlock) k_aa_solve(int nb, const double* __r
       }
     }
   }
-  double y[kAAMax], gam[kAAMax];
+  double y[M], gam[M];
   int used = 0;
   if (ok && mk > 0) {
     for (int a = 0; a < mk; a++) {
@@ -341,27 +356,28 @@ __global__ void __launch_bounds__(kAABlock) k_aa_solve(int nb, const double* __r
   for (int a = 0; a < kAAMax; a++) st->gamma[a] = a < used ? gam[a] : 0.0;
   st->cur = st->head;
   st->mk = used;
-  st->head = (st->head + 1) % (m + 1);
-  st->count = used == mk ? min(st->count + 1, m + 1) : 1;
+  st->head = (st->head + 1) % (M + 1);
+  st->count = used == mk ? min(st->count + 1, M + 1) : 1;
 }
 
+template <int M>
 __global__ void __launch_bounds__(kAABlock) k_aa_update(int n, double* __restrict__ x, double* __restrict__ xs,
-                                                        AAVectors v, int m, const AAState* st, const int* stop) {
+                                                        AAVectors v, const AAState* st, const int* stop) {
   if (stop && *stop != 0) return;
-  const int cur = st->cur, mk = st->mk, slots = m + 1;
-  const double* Gq[kAAMax + 1];
-  double gam[kAAMax];
+  const int cur = st->cur, mk = st->mk, slots = M + 1;
+  const double* Gq[M + 1];
+  double gam[M];
 #pragma unroll
-  for (int j = 0; j <= kAAMax; j++) Gq[j] = v.G[((cur - mk + j) % slots + slots) % slots];
+  for (int j = 0; j <= M; j++) Gq[j] = v.G[((cur - mk + j) % slots + slots) % slots];
 #pragma unroll
-  for (int j = 0; j < kAAMax; j++) gam[j] = st->gamma[j];
+  for (int j = 0; j < M; j++) gam[j] = st->gamma[j];
   const double* const Gc = v.G[cur];
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const double g = Gc[i];
     double s = 0.0;
     double prev = mk > 0 ? Gq[0][i] : 0.0;
 #pragma unroll
-    for (int j = 1; j <= kAAMax; j++) {
+    for (int j = 1; j <= M; j++) {
       if (j <= mk) {
         const double c = j == mk ? g : Gq[j][i];
         s += gam[j - 1] * (c - prev);
@@ -372,6 +388,14 @@ __global__ void __launch_bounds__(kAABlock) k_aa_update(int n, double* __restric
     x[i] = xn;
     xs[i] = xn;
   }
+}
+
+template <int M>
+void aa_step(int n, int nb, double* x, double* xs, const AAVectors& v, AAState* s, const int* stop, double* partials,
+             cudaStream_t st) {
+  k_aa_dots<M><<<nb, kAABlock, 0, st>>>(n, x, xs, v, s, stop, partials);
+  k_aa_solve<M><<<1, kAABlock, 0, st>>>(nb, partials, s, stop);
+  k_aa_update<M><<<nb, kAABlock, 0, st>>>(n, x, xs, v, s, stop);
 }
 
 __global__ void k_aa_reset(AAState* st) {
@@ -385,7 +409,7 @@ int aa_blocks(int n) {
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  return std::max(1, std::min((n + kAABlock - 1) / kAABlock, 8 * sms));
+  return std::max(1, std::min((n + kAABlock - 1) / kAABlock, 4 * sms));
 }
 }  // namespace
 
@@ -435,9 +459,13 @@ void ThermalModel::accelerationStep(cudaStream_t st, const int* stop) {
   }
   double* partials = (double*)((char*)dAA_ + vec * (size_t)(2 * (m + 1) + 1));
   AAState* s = (AAState*)((char*)partials + sizeof(double) * (size_t)aaBlocks_ * kAAQ);
-  k_aa_dots<<<aaBlocks_, kAABlock, 0, st>>>(n, dT_, xs, v, m, s, stop, partials);
-  k_aa_solve<<<1, kAABlock, 0, st>>>(aaBlocks_, partials, m, s, stop);
-  k_aa_update<<<aaBlocks_, kAABlock, 0, st>>>(n, dT_, xs, v, m, s, stop);
+  switch (m) {
+    case 1: aa_step<1>(n, aaBlocks_, dT_, xs, v, s, stop, partials, st); break;
+    case 2: aa_step<2>(n, aaBlocks_, dT_, xs, v, s, stop, partials, st); break;
+    case 3: aa_step<3>(n, aaBlocks_, dT_, xs, v, s, stop, partials, st); break;
+    case 4: aa_step<4>(n, aaBlocks_, dT_, xs, v, s, stop, partials, st); break;
+    default: aa_step<5>(n, aaBlocks_, dT_, xs, v, s, stop, partials, st); break;
+  }
   CUDA_OK(cudaGetLastError());
 }
 

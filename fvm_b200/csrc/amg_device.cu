@@ -291,12 +291,17 @@ __global__ void __launch_bounds__(32 * kGalWarps) k_galerkin(LevelRows a, int nc
   __shared__ int sJ[kGalWarps][kGalerkinCap];
   __shared__ double sV[kGalWarps][kGalerkinCap];
   __shared__ int sOff[kGalWarps][32], sBase[kGalWarps][32], sRow[kGalWarps][32];
+  __shared__ double sDiag[kGalWarps][32];
   const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int I = blockIdx.x * kGalWarps + wid;
   if (I >= nc) return;  // the whole warp leaves together
   int* J = sJ[wid];
   double* V = sV[wid];
   const int f0 = c2fRow[I], f1 = c2fRow[I + 1];
+  // the coarse diagonal (fill pass, lane 0): fine diagonals plus the entries
+  // inside the aggregate, fine rows ascending, entries in stored order,
+  // summed chunk by chunk from the values staged in shared memory
+  double dsum = 0.0;
   // every entry of the aggregate's fine rows, fine rows ascending, entries
   // in stored order; J = coarse column (-1: padding). Up to 32 fine rows at
   // a time: each lane looks up one row's range, a warp scan places the rows,
@@ -309,6 +314,7 @@ __global__ void __launch_bounds__(32 * kGalWarps) k_galerkin(LevelRows a, int nc
     if (lane < nq) {
       f = c2fCol[q0 + lane];
       row_range(a, f, base, w);
+      if (kFill) sDiag[wid][lane] = a.diag[f];
     }
     int incl = w;
     for (int o = 1; o < 32; o <<= 1) {
@@ -339,6 +345,16 @@ __global__ void __launch_bounds__(32 * kGalWarps) k_galerkin(LevelRows a, int nc
       const double v = a.vals[idx];
       J[L + e] = (j == sRow[wid][lo] || v == 0.0) ? -1 : ci[j];
       V[L + e] = v;
+    }
+    __syncwarp();
+    if (kFill && lane == 0) {
+      int e = L;
+      for (int q = 0; q < nq; q++) {
+        dsum += sDiag[wid][q];
+        const int we = (q + 1 < nq ? sOff[wid][q + 1] : tot) - sOff[wid][q];
+        for (int k = 0; k < we; k++, e++)
+          if (J[e] == I) dsum += V[e];
+      }
     }
     __syncwarp();
     L += tot;
@@ -400,19 +416,8 @@ __global__ void __launch_bounds__(32 * kGalWarps) k_galerkin(LevelRows a, int nc
     }
   }
   if (lane == 0) {
-    // diagonal: fine diagonals plus the entries inside the aggregate
-    double d = 0.0;
-    int e = 0;
-    for (int q = f0; q < f1; q++) {
-      const int f = c2fCol[q];
-      int base, w;
-      row_range(a, f, base, w);
-      d += a.diag[f];
-      for (int k = 0; k < w; k++, e++)
-        if (J[e] == I) d += V[e];
-    }
-    cdiag[I] = d;
-    if (cdiagF) cdiagF[I] = (float)d;
+    cdiag[I] = dsum;
+    if (cdiagF) cdiagF[I] = (float)dsum;
   }
 }
 

@@ -909,7 +909,15 @@ def main():
         variants.insert(variants.index("mixed") + 1, "mixed-plain-outer")  # the same solver, plain outer loop
     lc, learned_info = None, None
     if "learned" in variants:
-        lc, learned_info = train_learned(gen, args.inner_rel, steps=args.train_steps)
+        try:
+            lc, learned_info = train_learned(gen, args.inner_rel, steps=args.train_steps)
+        except Exception as e:
+            # the learned correction is an optional step of the mixed solve (it
+            # is used only when its measured residual reduction pays); a failed
+            # training is reported in the line and the mixed solve measured
+            # without it
+            lc, learned_info = None, {"failed": "%s: %s" % (type(e).__name__, e), "used_in_solve": False}
+            variants = [v for v in variants if v != "learned"]
     for variant in variants:
         if variant in ("mixed", "learned"):
             solve = Solve(mesh, fields, variant, mixed_inner, accel=accel)

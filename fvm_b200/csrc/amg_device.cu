@@ -132,6 +132,13 @@ __global__ void k_fill_finest_diag(int n, const int* __restrict__ iperm, const d
 
 __device__ __forceinline__ double strength(double v, double di, double dj) { return fabs(v) / fmax(di, dj); }
 
+// The matching kernels take a row's entries in chunks of kAggChunk: the
+// chunk's column and value loads are issued together, then its neighbour
+// loads (only for the entries that one at a time would load them for), then
+// the entries are taken in stored order, so the result is the one-at-a-time
+// result with a quarter of the dependent round trips to memory.
+constexpr int kAggChunk = 4;
+
 __global__ void k_agg_init(LevelRows a, double* maxw, int* partner) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= a.n) return;
@@ -139,14 +146,74 @@ __global__ void k_agg_init(LevelRows a, double* maxw, int* partner) {
   row_range(a, i, base, w);
   const double di = fabs(a.diag[i]);
   double m = 0.0;
-  for (int k = 0; k < w; k++) {
-    const int j = a.cols[base + 32 * k];
-    const double v = a.vals[base + 32 * k];
-    if (j == i || v == 0.0) continue;
-    m = fmax(m, strength(v, di, fabs(a.diag[j])));
+  for (int k0 = 0; k0 < w; k0 += kAggChunk) {
+    int jj[kAggChunk];
+    double vv[kAggChunk], dj[kAggChunk];
+    bool use[kAggChunk];
+#pragma unroll
+    for (int u = 0; u < kAggChunk; u++) {
+      use[u] = false;
+      if (k0 + u < w) {
+        jj[u] = a.cols[base + 32 * (k0 + u)];
+        vv[u] = a.vals[base + 32 * (k0 + u)];
+        use[u] = !(jj[u] == i || vv[u] == 0.0);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < kAggChunk; u++)
+      if (use[u]) dj[u] = fabs(a.diag[jj[u]]);
+#pragma unroll
+    for (int u = 0; u < kAggChunk; u++)
+      if (use[u]) m = fmax(m, strength(vv[u], di, dj[u]));
   }
   maxw[i] = m;
   partner[i] = -1;
+}
+
+// the strongest candidate of row i among its entries whose neighbour j has
+// (paired ? partner[j] >= 0 : partner[j] == -1), strength at least thr
+// (ties: smaller index); -1 when none
+template <bool Paired>
+__device__ __forceinline__ int agg_strongest(const LevelRows& a, int i, double thr, const int* __restrict__ partner) {
+  int base, w;
+  row_range(a, i, base, w);
+  const double di = fabs(a.diag[i]);
+  int bj = -1;
+  double bw = 0.0;
+  for (int k0 = 0; k0 < w; k0 += kAggChunk) {
+    int jj[kAggChunk];
+    double vv[kAggChunk], dj[kAggChunk];
+    bool use[kAggChunk];
+#pragma unroll
+    for (int u = 0; u < kAggChunk; u++) {
+      use[u] = false;
+      if (k0 + u < w) {
+        jj[u] = a.cols[base + 32 * (k0 + u)];
+        vv[u] = a.vals[base + 32 * (k0 + u)];
+        use[u] = !(jj[u] == i || vv[u] == 0.0);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < kAggChunk; u++)
+      if (use[u]) {
+        const int p = partner[jj[u]];
+        use[u] = Paired ? p >= 0 : p == -1;
+      }
+#pragma unroll
+    for (int u = 0; u < kAggChunk; u++)
+      if (use[u]) dj[u] = fabs(a.diag[jj[u]]);
+#pragma unroll
+    for (int u = 0; u < kAggChunk; u++) {
+      if (!use[u]) continue;
+      const double s = strength(vv[u], di, dj[u]);
+      if (!(s > 0.0) || s < thr) continue;
+      if (s > bw || (s == bw && jj[u] < bj)) {
+        bw = s;
+        bj = jj[u];
+      }
+    }
+  }
+  return bj;
 }
 
 // strongest unpaired candidate of every unpaired row (ties: smaller index)
@@ -158,24 +225,7 @@ __global__ void k_agg_best(LevelRows a, const double* __restrict__ maxw, double 
     best[i] = -1;
     return;
   }
-  int base, w;
-  row_range(a, i, base, w);
-  const double di = fabs(a.diag[i]);
-  const double thr = beta * maxw[i];
-  int bj = -1;
-  double bw = 0.0;
-  for (int k = 0; k < w; k++) {
-    const int j = a.cols[base + 32 * k];
-    const double v = a.vals[base + 32 * k];
-    if (j == i || v == 0.0 || partner[j] != -1) continue;
-    const double s = strength(v, di, fabs(a.diag[j]));
-    if (!(s > 0.0) || s < thr) continue;
-    if (s > bw || (s == bw && j < bj)) {
-      bw = s;
-      bj = j;
-    }
-  }
-  best[i] = bj;
+  best[i] = agg_strongest<false>(a, i, beta * maxw[i], partner);
 }
 
 // handshake: i and j pair when each is the other's strongest candidate
@@ -195,24 +245,7 @@ __global__ void k_agg_join(LevelRows a, const double* __restrict__ maxw, double 
     join[i] = -1;
     return;
   }
-  int base, w;
-  row_range(a, i, base, w);
-  const double di = fabs(a.diag[i]);
-  const double thr = beta * maxw[i];
-  int bj = -1;
-  double bw = 0.0;
-  for (int k = 0; k < w; k++) {
-    const int j = a.cols[base + 32 * k];
-    const double v = a.vals[base + 32 * k];
-    if (j == i || v == 0.0 || partner[j] < 0) continue;
-    const double s = strength(v, di, fabs(a.diag[j]));
-    if (!(s > 0.0) || s < thr) continue;
-    if (s > bw || (s == bw && j < bj)) {
-      bw = s;
-      bj = j;
-    }
-  }
-  join[i] = bj;
+  join[i] = agg_strongest<true>(a, i, beta * maxw[i], partner);
 }
 
 __device__ __forceinline__ bool is_leader(int i, const int* partner, const int* join) {

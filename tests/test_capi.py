@@ -33,6 +33,31 @@ def test_reference_defaults():
     assert t.relativeTolerance == 1e-8 and t.absoluteTolerance == 1e-16
     assert t.initialTemperature == 300.0 and t.timeStep == 1e-7 and t.transient == 0
     assert t.linear.relativeTolerance == 1e-1 and t.linear.nMaxIterations == 20
+    # added knobs: the outer loop as one CUDA graph (bitwise the host loop) on
+    # by default, its Anderson acceleration off (the reference's plain loop)
+    assert o.outerOnDevice == 1 and o.outerAcceleration == 0
+
+
+def test_outer_acceleration_depth_is_checked():
+    """The acceleration depth is checked where the options cross the C ABI
+    (no GPU needed: the host-only hierarchy entry point converts them)."""
+    import numpy as np
+    import pytest
+
+    from fvm_b200 import fvmbaseExt
+
+    row = np.array([0, 1, 3, 4], dtype=np.int32)
+    col = np.array([1, 0, 2, 1], dtype=np.int32)
+    diag = np.full(3, 2.0)
+    off = np.full(4, -1.0)
+    a = fvmbaseExt.AMG()
+    for depth in (-1, 6):
+        a.outerAcceleration = depth
+        with pytest.raises(_lib.FvmError) as e:
+            a.hierarchy_csr(row, col, diag, off)
+        assert "outerAcceleration" in str(e.value)
+    a.outerAcceleration = 5
+    a.hierarchy_csr(row, col, diag, off)
 
 
 def test_errors_are_reported(fvm_lib):
